@@ -1,0 +1,272 @@
+"""Synthetic cases in the reference's input layout.
+
+The reference loads a real reach (Global_Variables.py:27-133): topography ``h``
+(depth below datum, positive down, defined on cell corners), roughness ``hsnham``,
+viscosity ``VISCOINDX``, sediment friction ``Fw``, each transposed, flipped and
+edge-padded to ``(N+3, M+3)``; boundary types per edge (``boundary_type.txt``:
+0 wall, 1 stage Z, 2 discharge Q) and hourly boundary tables per edge segment.
+The generators here build the same arrays from closed-form geometry with a fixed
+seed; no dataset is needed.  A data array ``d`` of shape (N, M) is placed like the
+reference places its input maps: ``np.pad(d, ((1, 2), (1, 2)), 'edge')``.
+"""
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+from .params import default_params, derive, settling_velocity
+
+SEGMENT_LIMIT = 20
+EDGE_UP, EDGE_DOWN, EDGE_LEFT, EDGE_RIGHT = 0, 1, 2, 3
+GRID_FIELDS = ("h", "hsnham", "VISCOIDX", "Fw", "Tsxw", "Tsyw", "u", "v", "z", "FS")
+
+
+@dataclass
+class Case:
+    name: str
+    N: int
+    M: int
+    params: object
+    fields: dict
+    boundary_type: np.ndarray
+    tables: list
+    cc: list
+    total_time: int
+    t_start: float = 0.0
+    nsteps: int = 1
+    notes: dict = field(default_factory=dict)
+
+    @property
+    def shape(self):
+        return (self.N + 3, self.M + 3)
+
+    def nseg(self):
+        return [int(t.shape[0]) for t in self.tables]
+
+    def interior_cells(self):
+        return self.N * self.M
+
+
+def pad_edge(d):
+    """Edge padding of an (N, M) input map to (N+3, M+3) (Global_Variables.py:71-89)."""
+    return np.pad(np.asarray(d, dtype=np.float64), ((1, 2), (1, 2)), "edge")
+
+
+def _prismatic_ends(h):
+    """Make the first two and the last two cross-sections identical.
+
+    The reference weights a discharge edge by pow(face depth, 5/3) of the corner
+    depths on the edge row (support_funcs.cu:451-511); with identical first two rows
+    a cell is wet exactly where its edge face depth is positive, so the weights are
+    finite.  The same is done at the outflow end."""
+    h[0, :] = h[1, :]
+    h[-1, :] = h[-2, :]
+    return h
+
+
+def _heal_faces(h, fill=0.05, max_iter=50):
+    """Raise corner depths so that every cell face between two wet cells has a positive
+    mean corner depth.
+
+    The reference's Manning factor pow(face depth, -2*mu_mn) (support_funcs.cu:53-57) is
+    NaN or infinite on such a face, and a wet cell next to it then produces NaN
+    velocities; measured bathymetry is smooth enough not to contain such faces.
+    Cells are wet when their four-corner mean is positive (support_funcs.cu:42)."""
+    for _ in range(max_iter):
+        H = pad_edge(h)
+        n1, m1 = H.shape
+        cell = np.full(H.shape, -1.0)
+        cell[1:, 1:] = (H[:-1, :-1] + H[:-1, 1:] + H[1:, :-1] + H[1:, 1:]) * 0.25
+        wet = cell > 0
+        bad = np.zeros(H.shape, dtype=bool)
+        # face between (i, j) and (i+1, j): corners H[i, j-1], H[i, j]
+        fu = np.full(H.shape, 1.0)
+        fu[:, 1:] = (H[:, :-1] + H[:, 1:]) * 0.5
+        bu = (fu <= 0) & wet & np.roll(wet, -1, axis=0)
+        # face between (i, j) and (i, j+1): corners H[i-1, j], H[i, j]
+        fv = np.full(H.shape, 1.0)
+        fv[1:, :] = (H[:-1, :] + H[1:, :]) * 0.5
+        bv = (fv <= 0) & wet & np.roll(wet, -1, axis=1)
+        bu[-1, :] = False
+        bv[:, -1] = False
+        if not (bu.any() or bv.any()):
+            return h
+        for i, j in np.argwhere(bu):
+            for jj in (j - 1, j):
+                bad[i, jj] = True
+        for i, j in np.argwhere(bv):
+            for ii in (i - 1, i):
+                bad[ii, j] = True
+        bad &= H <= 0
+        for i, j in np.argwhere(bad):
+            a = min(max(i - 1, 0), h.shape[0] - 1)
+            b = min(max(j - 1, 0), h.shape[1] - 1)
+            h[a, b] = fill
+    return h
+
+
+def _tables(btype_row, values_per_seg, total_time):
+    nseg = max(1, int(np.count_nonzero(btype_row)))
+    t = np.zeros((nseg, total_time), dtype=np.float64)
+    for k in range(nseg):
+        t[k, :] = values_per_seg[k] if k < len(values_per_seg) else values_per_seg[-1]
+    return t
+
+
+def _gaussian_field(rng, shape, sigma_cells, std):
+    """Gaussian-correlated noise (periodic FFT filter), scaled to standard deviation `std`."""
+    w = rng.standard_normal(shape)
+    ky = np.fft.fftfreq(shape[0])[:, None]
+    kx = np.fft.rfftfreq(shape[1])[None, :]
+    filt = np.exp(-2.0 * (math.pi * sigma_cells) ** 2 * (kx ** 2 + ky ** 2))
+    f = np.fft.irfft2(np.fft.rfft2(w) * filt, s=shape)
+    f -= f.mean()
+    s = f.std()
+    return f * (std / s) if s > 0 else f
+
+
+def channel_case(N=400, M=60, dX=5.0, dT=2.0, bank=5, depth=3.0, slope=1e-4, bank_height=2.0,
+                 manning=0.025, Q=150.0, hours=1, z_out=0.0, name="channel"):
+    """Straight channel (the repo's horizontal-channel test): x along i, banks across j.
+
+    Bed z_b = -depth - slope*x (x from upstream), so h = depth + slope*x; the first and
+    last `bank` cross cells are dry banks at +bank_height.  Upstream (left edge, i=2)
+    discharge Q, downstream (right edge, i=N) stage z_out, walls up/down.  No sediment.
+    """
+    p = default_params(dX=dX, dY=dX, dT=dT, sediment_start=1e12, bed_change_start=1e12)
+    derive(p)
+    x = np.arange(N, dtype=np.float64)[:, None] * dX
+    h = np.repeat(depth + slope * x, M, axis=1)
+    h[:, :bank] = -bank_height
+    h[:, M - bank:] = -bank_height
+    shape = (N + 3, M + 3)
+    fields = {
+        "h": pad_edge(h) + p.NANGDAY,
+        "hsnham": pad_edge(np.full((N, M), manning)),
+        "VISCOIDX": pad_edge(np.full((N, M), 1e-6)),
+        "Fw": np.zeros(shape),
+        "Tsxw": np.zeros(shape),
+        "Tsyw": np.zeros(shape),
+        "u": np.zeros(shape),
+        "v": np.zeros(shape),
+        "z": np.zeros(shape),
+        "FS": np.zeros(shape),
+    }
+    bt = np.zeros((4, SEGMENT_LIMIT), dtype=np.int32)
+    bt[EDGE_LEFT, 0] = 2
+    bt[EDGE_RIGHT, 0] = 1
+    total_time = int(hours) + 3
+    tables = [
+        np.zeros((1, total_time)),
+        np.zeros((1, total_time)),
+        _tables(bt[EDGE_LEFT], [Q], total_time),
+        _tables(bt[EDGE_RIGHT], [z_out], total_time),
+    ]
+    cc = [np.zeros((1, total_time)) for _ in range(4)]
+    nsteps = int(round(hours * 3600 / dT))
+    return Case(name, N, M, p, fields, bt, tables, cc, total_time, 0.0, nsteps,
+                notes={"Q": Q, "bank_cells": bank})
+
+
+def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=120.0,
+                 wavelength=1500.0, width=150.0, depth=8.0, floodplain=1.5, noise_sigma=0.2,
+                 noise_len=50.0, manning=0.025, manning_spread=0.10, Q0=2000.0, Q1=3500.0,
+                 tide_amp=1.0, tide_period_h=12.42, d50=1e-4, Sx=2.7125, cc_in=0.2,
+                 sediment_start=1800.0, bed_change_start=3600.0, y_center=None, spinup_h=0.0,
+                 name="meander"):
+    """Seeded meandering reach with a parabolic channel, floodplain and bed noise.
+
+    Centreline y = y_c + amp*sin(2*pi*x/wavelength); parabolic section of `width` and
+    `depth`, floodplain at +floodplain; Gaussian-correlated bed noise (sigma, length);
+    lognormal Manning n.  Upstream (left edge) discharge rising as a half-cosine from
+    Q0 to Q1 over `hours`; downstream (right edge) tidal stage; walls up/down.
+    Single-grain cohesive sediment (d50, Sx chosen so that wss() = 0.0080 m/s),
+    inflow concentration cc_in, sediment from `sediment_start`, bed change from
+    `bed_change_start`.  The reference's hourly tables are linearly interpolated
+    (support_funcs.cu:547-565), so the boundary forcing is given at hourly knots.
+
+    With spinup_h > 0 the discharge first ramps linearly from 0 to Q0 over spinup_h
+    hours (the scheme cannot carry the bore of an impulsive start at Q0 into water at
+    rest), the stated hydrograph follows, and sediment_start is counted from the end of
+    the spin-up.
+    """
+    rng = np.random.default_rng(seed)
+    p = default_params(dX=dX, dY=dX, dT=dT, dm=d50, Sx=Sx, Ks=2.5 * d50,
+                       sediment_start=sediment_start + spinup_h * 3600.0,
+                       bed_change_start=bed_change_start, ketdinh=1)
+    derive(p)
+    x = np.arange(N, dtype=np.float64)[:, None] * dX
+    y = np.arange(M, dtype=np.float64)[None, :] * dX
+    yc = (M * dX / 2.0 if y_center is None else y_center) + amp * np.sin(2 * math.pi * x / wavelength)
+    d = np.abs(y - yc)
+    half = width / 2.0
+    zb = np.where(d <= half, -depth * (1.0 - (d / half) ** 2), floodplain)
+    zb = zb + _gaussian_field(rng, (N, M), noise_len / dX, noise_sigma)
+    h = -zb
+    _prismatic_ends(h)
+    _heal_faces(h)
+    n = manning * np.exp(manning_spread * rng.standard_normal((N, M)))
+    hpos = np.maximum(h, 0.1)
+    fw = np.where(h > 0, p.g * n ** 2 / hpos ** (1.0 / 3.0), 0.0)
+    shape = (N + 3, M + 3)
+    fields = {
+        "h": pad_edge(h) + p.NANGDAY,
+        "hsnham": pad_edge(n),
+        "VISCOIDX": pad_edge(np.full((N, M), 1e-6)),
+        "Fw": pad_edge(fw),
+        "Tsxw": np.zeros(shape),
+        "Tsyw": np.zeros(shape),
+        "u": np.zeros(shape),
+        "v": np.zeros(shape),
+        "z": np.zeros(shape),
+        "FS": np.zeros(shape),
+    }
+    bt = np.zeros((4, SEGMENT_LIMIT), dtype=np.int32)
+    bt[EDGE_LEFT, 0] = 2
+    bt[EDGE_RIGHT, 0] = 1
+    total_time = int(math.ceil(hours + spinup_h)) + 3
+    th = np.arange(total_time, dtype=np.float64)
+    tr = np.clip(th - spinup_h, 0.0, hours)
+    q = Q0 + (Q1 - Q0) * 0.5 * (1.0 - np.cos(math.pi * tr / hours))
+    if spinup_h > 0:
+        q = np.where(th < spinup_h, Q0 * th / spinup_h, q)
+    zt = tide_amp * np.sin(2 * math.pi * th / tide_period_h)
+    tables = [np.zeros((1, total_time)), np.zeros((1, total_time)), q[None, :].copy(), zt[None, :].copy()]
+    cc = [np.zeros((1, total_time)), np.zeros((1, total_time)),
+          np.full((1, total_time), cc_in), np.zeros((1, total_time))]
+    nsteps = int(round((hours + spinup_h) * 3600 / dT))
+    return Case(name, N, M, p, fields, bt, tables, cc, total_time, 0.0, nsteps,
+                notes={"wss": settling_velocity(p), "seed": seed, "spinup_steps": int(round(spinup_h * 3600 / dT))})
+
+
+def islands_case(N=48, M=36, dX=5.0, dT=1.0, seed=7, hours=1.0, sediment_start=0.0,
+                 bed_change_start=10.0, name="islands"):
+    """Small irregular reach for parity tests: random islands give several wet segments
+    per line, single-cell segments, shallow cells that dry and re-wet, a discharge edge
+    and a stage edge; sediment and bed change active within a few steps."""
+    rng = np.random.default_rng(seed)
+    c = meander_case(N=N, M=M, dX=dX, dT=dT, hours=hours, seed=seed, amp=M * dX * 0.15,
+                     wavelength=N * dX * 0.7, width=M * dX * 0.55, depth=3.0, floodplain=1.0,
+                     noise_sigma=0.05, noise_len=3 * dX, Q0=40.0, Q1=60.0, tide_amp=0.3,
+                     tide_period_h=2.0, sediment_start=sediment_start,
+                     bed_change_start=bed_change_start, name=name)
+    h = c.fields["h"][1:N + 1, 1:M + 1].copy()
+    # a shallow shelf that wets and dries with the tide
+    shelf = (h > 0) & (h < 0.8)
+    h[shelf] = 0.03 + 0.02 * rng.random(int(shelf.sum()))
+    # 2x2-corner islands in deep water: each blocks one cell and splits the lines through it
+    k = max(1, (N * M) // 120)
+    ii = rng.integers(4, N - 5, size=k)
+    jj = rng.integers(4, M - 5, size=k)
+    for a, b in zip(ii, jj):
+        if (h[a - 1:a + 3, b - 1:b + 3] > 1.0).all():
+            h[a:a + 2, b:b + 2] = -0.5
+    _prismatic_ends(h)
+    _heal_faces(h)
+    c.fields["h"] = pad_edge(h) + c.params.NANGDAY
+    c.fields["Fw"] = pad_edge(np.where(h > 0, 0.004, 0.0))
+    return c
+
+
+def steps_for(case, hours):
+    return int(round(hours * 3600 / case.params.dT))

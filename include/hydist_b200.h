@@ -1,0 +1,186 @@
+/*
+ * hydist_b200.h — C ABI of the B200 (sm_100a) ADI shallow-water + sediment library.
+ *
+ * The reference (GPU-hydist) has no C ABI: its operator surface is
+ *   (1) the device structs Argument_Pointers / Array_Pointers (constant.cuh:6-29),
+ *   (2) the compile-time case constants of constant.cuh:31-133, and
+ *   (3) the Python host calls rep.gpu_init (rep.py:58-142) and
+ *       Engine.hydraulic_Calculation (Engine.py:49-469).
+ * Every entry point below names the piece of that surface it replaces.
+ *
+ * Conventions
+ *   - All functions return 0 on success and a negative HYD_E* code on failure;
+ *     hyd_last_error() then returns a human-readable message (thread-local).
+ *   - Grid fields are host-owned, C-contiguous (N+3) x (M+3) arrays, row index i
+ *     (x, dX, "N" direction) and column index j (y, dY, "M" direction), exactly
+ *     the layout of Global_Variables.py:92-133.  The library copies them in and
+ *     out; it never keeps host pointers.
+ *   - The library owns all device memory and one CUDA stream per handle.  Calls
+ *     on one handle are not thread-safe; separate handles are independent.
+ */
+#ifndef HYDIST_B200_H
+#define HYDIST_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Maximum wet segments per grid line (constant.cuh:31 `segment_limit`). */
+#define HYD_SEGMENT_LIMIT 20
+
+/* Error codes. */
+#define HYD_OK 0
+#define HYD_EINVAL (-1)   /* bad argument */
+#define HYD_ECUDA (-2)    /* CUDA runtime error */
+#define HYD_ENOMEM (-3)   /* allocation failed */
+#define HYD_ESTATE (-4)   /* call out of order (e.g. step before init) */
+#define HYD_EDEVICE (-5)  /* a device-side check failed (see hyd_last_error) */
+
+/* Boundary edges, in the order of Argument_Pointers' bc_up/bc_down/bc_left/bc_right
+ * and of the rows of boundary_type (support_funcs.cu:632-665):
+ *   up    = column j = M (location of vbt),   down  = column j = 2 (vbd),
+ *   left  = row    i = 2 (ubt),               right = row    i = N (ubp). */
+#define HYD_EDGE_UP 0
+#define HYD_EDGE_DOWN 1
+#define HYD_EDGE_LEFT 2
+#define HYD_EDGE_RIGHT 3
+
+/*
+ * HydCaseParams — every __constant__ of the reference's case header
+ * (constant.cuh:31-118) plus the run options that Engine.hydraulic_Calculation
+ * takes as keywords (Engine.py:49-50).  It replaces "copy constant_<case>.cuh over
+ * constant.cuh and recompile" (readme.md:13-15): the values are uploaded at run time.
+ * The derived members (dXbp ... HaiChiadT) are stored explicitly because the
+ * reference header spells them out as separate literals; hyd_params_derive()
+ * recomputes them from dX, dY, dT.
+ */
+typedef struct HydCaseParams {
+    /* grid spacing and time step (constant.cuh:32-47) */
+    double dX, dY, dT;
+    double dXbp, dX2, dYbp, dY2, dTchia2dX, dTchia2dY, QuyDoiTime, QuyDoiPi, HaiChiadT;
+    /* wet/dry limits, wind, smoothing, friction exponent (constant.cuh:54-66) */
+    double NANGDAY, H_TINH, Wind, huonggio, Zbandau, heso, mu_mn;
+    /* concentrations (constant.cuh:70-74) */
+    double NDnen, NDbphai, NDbtrai, NDbtren, NDbduoi;
+    /* erosion/deposition and grain properties (constant.cuh:80-101) */
+    double Tod, Toe, hstoe, ghtoe, Mbochat, ro, ros, dm, d90, muy, Dorong, Sx;
+    /* depth counts, Coriolis, gravity, roughness height (constant.cuh:104-118) */
+    double sohn, soha, sohn1, CORIOLIS_FORCE, g, Ks;
+    /* run options (Engine.py:49-50, rep.py:152-156) */
+    double sediment_start;   /* s; sediment ADI runs while t >= sediment_start (Engine.py:218,338) */
+    double bed_change_start; /* s; source gate s_start (Engine.py:226,347) and Exner period (Engine.py:364) */
+    int ketdinh;             /* 1 = cohesive source term (Engine.py:49 default True) */
+    int kenhhepd;            /* channel mode, vertical channel (rep.py:37; Engine.py:68,156) */
+    int kenhhepng;           /* channel mode, horizontal channel (rep.py:36; Engine.py:68,277) */
+    int reserved0;
+} HydCaseParams;
+
+/* Fill *p with the values of the reference's constant.cuh (constant.cuh:31-118)
+ * and the Engine.hydraulic_Calculation defaults (Engine.py:49-50). */
+void hyd_params_default(HydCaseParams* p);
+/* Recompute dXbp, dX2, dYbp, dY2, dTchia2dX, dTchia2dY, QuyDoiTime, QuyDoiPi,
+ * HaiChiadT from dX, dY, dT (the relations written out in constant.cuh:36-47). */
+void hyd_params_derive(HydCaseParams* p);
+
+typedef struct HydSim* hyd_handle;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* hyd_last_error(void);
+
+/* Library build string (architecture, precision). */
+const char* hyd_version(void);
+
+/*
+ * Create a simulation of N x M interior cells on CUDA device `device`.
+ * Replaces rep.gpu_init's context creation, Pointers.alloc/alloc_on_device_only
+ * and the PointersStruct packing (rep.py:58-109, Pointers.py:15-81,169-191).
+ * All device fields start zero-filled.
+ */
+int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out);
+
+/* Release all device memory and the stream (replaces ctx.detach, rep.py:171). */
+int hyd_destroy(hyd_handle h);
+
+/*
+ * Copy one field in from the host.  `name` is one of the Argument_Pointers
+ * members that rep.py uploads (rep.py:110-111): "h", "hsnham", "VISCOIDX", "Fw",
+ * "Tsxw", "Tsyw", "u", "v", "z", "FS", plus the state fields "t_u", "t_v", "t_z",
+ * "H_moi", "htaiz", "Htdu", "Htdv", "dH", "tFS", "VTH", "Kx", "Ky", "Qbx", "Qby",
+ * "Kx1", "Ky1" (double, (N+3)*(M+3) values) and "khouot" (int32, (N+3)*(M+3)).
+ * `count` must equal the field's element count.  Replaces Pointers.toDevice
+ * (Pointers.py:110-122).
+ */
+int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count);
+
+/*
+ * Copy one field out to the host (any name accepted by hyd_set_field, plus the
+ * segment tables "daui","cuoii" (int32, (N+2)*20), "moci" (int32, N+2), "dauj",
+ * "cuoij" ((M+2)*20), "mocj" (M+2), and "ubt","ubp" (M+2), "vbt","vbd" (N+2),
+ * "hi" (2*(N+3)+2*(M+3))).  Replaces Pointers.extract (Pointers.py:148-154).
+ */
+int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count);
+
+/*
+ * Boundary tables for all four edges (Global_Variables.py:30-66):
+ *   boundary_type: 4 x HYD_SEGMENT_LIMIT int32 (0 wall, 1 stage Z, 2 discharge Q);
+ *   tables[e]:     nseg[e] x total_time hourly values of Q or Z (bc_up..bc_right);
+ *   cc[e]:         nseg[e] x total_time hourly inflow concentrations (CC_u..CC_r).
+ * bienQ is derived as in Global_Variables.py:56-66.  total_time must cover every
+ * hour index the run reaches plus one (support_funcs.cu:565).
+ */
+int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const* tables,
+                     const double* const* cc, const int* nseg, int total_time);
+
+/*
+ * One-time initialisation (rep.py:126-139): Onetime_init, the wet-segment scans
+ * Find_Calculation_limits_Horizontal/Vertical, Htuongdoi and preprocess_data
+ * (support_funcs.cu:20-58, 230-354, 433-542).  Call after the fields and the
+ * boundary tables are set; sets the simulation time to t_start.
+ */
+int hyd_init(hyd_handle h, double t_start);
+
+/*
+ * Advance `nsteps` full ADI steps (two half-steps each, with the sediment ADI
+ * and the Exner update when their start times are reached): the body of the
+ * time loop of Engine.hydraulic_Calculation (Engine.py:144-366).  On return
+ * *t_out (if not NULL) holds the simulation time.  Work is queued on the
+ * handle's stream; the call returns after the launches are queued unless
+ * `sync` is non-zero.
+ */
+int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out);
+
+/* Current simulation time (host mirror). */
+int hyd_get_time(hyd_handle h, double* t);
+
+/* Wait for all queued work on the handle and report device-side errors. */
+int hyd_synchronize(hyd_handle h);
+
+/*
+ * Domain sums over interior cells i in [2,N], j in [2,M] with khouot == 0, in FP64:
+ *   out[0] = sum(H_moi) * dX * dY   (water volume, m^3)
+ *   out[1] = sum(FS * H_moi) * dX * dY   (suspended mass / ros scale as in FS)
+ *   out[2] = sum(dH) * dX * dY      (accumulated bed change volume)
+ *   out[3] = number of wet cells
+ *   out[4] = number of non-finite values in z/u/v/FS (the reference's hourly NaN check,
+ *            Engine.py:402)
+ * n must be >= 5.
+ */
+int hyd_mass_balance(hyd_handle h, double* out, int n);
+
+/* Size in bytes of a checkpoint image, and checkpoint save/restore (replaces the
+ * text pick-up of rep.py:43-55 with an exact binary image of every prognostic
+ * field, the wet mask, the segment tables and the time). */
+int hyd_state_size(hyd_handle h, size_t* bytes);
+int hyd_get_state(hyd_handle h, void* buf, size_t bytes);
+int hyd_set_state(hyd_handle h, const void* buf, size_t bytes);
+
+/* Number of kernels this handle has launched since creation (instrumentation). */
+int hyd_launch_count(hyd_handle h, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYDIST_B200_H */
