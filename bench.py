@@ -1,0 +1,339 @@
+"""Benchmark: ADI cell-updates/s of the B200 library on the meandering-reach workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (config 2): 1048 x 980 cells, dx = dy = 5 m, dt = 1 s, FP64 hydraulics with the
+suspended-sediment ADI and the Exner update active.  A "step" is one full ADI step (two
+half-steps) of the whole grid; one cell-update is one interior cell advanced one step.
+The state is first spun up (untimed) to t = 3590 s, where sediment is active and the
+Exner update fires every 3600 s.  Per step the fields touched (about 25 arrays of 8.3 MB)
+exceed the 126 MB L2, so no flush is needed between steps.
+
+--impl ours       the CUDA library; prints value (device-resident), e2e (through the C
+                  ABI with host buffers copied in and out every step), roofline of the
+                  dominant phase, cpu_baseline (the oracle port on the host cores).
+--impl reference  the same scheme on the host cores: the reference has no CPU
+                  implementation of this path, so this times the oracle port (a line-for-
+                  line C restatement of the reference's kernels, OpenMP) on a bounded sample.
+Multi-GPU (torchrun): one independent replica of the reach per GPU ("replicas only":
+an ADI line couples the whole domain, so a single reach has no shard).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "gpu-hydist_b200"), os.path.join(ROOT, "oracle")]
+
+SPINUP_STEPS = 3590
+METRIC = "ADI cell-updates/s"
+
+# algorithmic bytes per launch of each phase, per unit (cells of the whole padded grid
+# "grid", interior cells "cells", or wet cells of the swept lines "wet"); the derivation
+# is in DESIGN.md (each field read once and written once)
+PHASE_BYTES = {
+    "smooth": (20, "grid"),        # read t (8) + mask (4), write out (8)
+    "post": (72, "cells"),         # read t_z,t_u,t_v,h (32), write z,u,v,Htdu,Htdv (40)
+    "reset_rows": (28, "cells"),   # read mask, htaiz, t_z (20), write H_moi (8)
+    "reset_cols": (28, "cells"),
+    "scan": (8, "cells"),          # mask read by the row and the column scans
+    "vth_hesok": (80, "cells"),    # read t_u,t_v,H_moi,htaiz,Htdu,Htdv,h (56), write VTH,Kx,Ky (24)
+    "update_fs": (16, "cells"),
+    "sweep_uz": (88, "wet"),       # read u,v,z,Htdu,Htdv,H_moi,VISC,Kx1,Tsxw (72), write t_z,t_u (16)
+    "sweep_vz": (88, "wet"),
+    "explicit_v": (80, "wet"),
+    "explicit_u": (80, "wet"),
+    "fs_sweep_j": (88, "wet"),
+    "fs_sweep_i": (88, "wet"),
+    "boundary": (0, "cells"),
+    "bed": (0, "cells"),
+}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def wet_cells_per_line_sweep(sim):
+    """Cells covered by the wet segments (the units the line sweeps process)."""
+    import numpy as np
+    kh = sim.get("khouot")
+    return int((kh[2:sim.N + 1, 2:sim.M + 1] == 0).sum())
+
+
+def cpu_port_sample(case, state_get, t0, hmax, budget_s=12.0):
+    """Time the oracle port (OpenMP, all host cores) from the GPU's state."""
+    import oracle
+    ora = oracle.OracleSim(case, threads=os.cpu_count() or 1)
+    ora.load_state(state_get, t0, hmax)
+    ora.step(2)  # warm caches / thread pool
+    steps, t_start = 0, time.perf_counter()
+    while True:
+        ora.step(10)
+        steps += 10
+        el = time.perf_counter() - t_start
+        if el >= budget_s:
+            break
+    return steps, el
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    from hydist import cases
+    from hydist.lib import Simulation
+
+    torch.cuda.set_device(local_rank)
+    case = cases.config2_case()
+    N, M = case.N, case.M
+    cells = N * M
+    sim = Simulation.from_case(case, device=local_rank)
+    sim.step(SPINUP_STEPS)
+    ext = torch.cuda.ExternalStream(sim.stream_ptr(), device=local_rank)
+    launches0 = sim.launch_count()
+    # warm-up
+    sim.step(args.warmup, sync=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = sim.launch_count()
+    with ClockSampler(local_rank) as clk:
+        e0.record(ext)
+        sim.step(args.steps, sync=False)
+        e1.record(ext)
+        e1.synchronize()
+    launches = sim.launch_count() - l0
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t_max = torch.tensor([ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t_max, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    ms = float(t_max.item())
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # per-phase device timing (separate pass: events around every phase)
+    sim.set_timing(True)
+    ksteps = max(20, min(args.steps, 200))
+    sim.step(ksteps, sync=True)
+    rep = sim.timing_report()
+    sim.set_timing(False)
+    wet = wet_cells_per_line_sweep(sim)
+    units = {"grid": (N + 3) * (M + 3), "cells": (N + 1) * (M + 1), "wet": wet}
+    total_ms = sum(v[1] for v in rep.values())
+    dom = max(rep.items(), key=lambda kv: kv[1][1])
+    dom_name, (dom_n, dom_ms) = dom
+    per_unit, unit = PHASE_BYTES.get(dom_name, (0, "cells"))
+    bytes_per_launch = per_unit * units[unit]
+    avg_ms = dom_ms / dom_n
+    peak, peak_kind = load_peaks()
+    achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    phases = {k: {"launches": n, "ms_per_launch": t / n, "share": t / total_ms} for k, (n, t) in rep.items()}
+
+    # end to end through the C ABI: host fields in and out every step (pinned buffers)
+    names = ("z", "u", "v", "FS")
+    host = {f: torch.empty((N + 3, M + 3), dtype=torch.float64, pin_memory=True) for f in names}
+    for f in names:
+        sim.get(f, out=host[f].numpy())
+    e2e_steps = max(10, min(args.steps, 100))
+    torch.cuda.synchronize()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(ext)
+    for _ in range(e2e_steps):
+        for f in names:
+            sim.set(f, host[f].numpy())
+        sim.step(1, sync=False)
+        for f in names:
+            sim.get(f, out=host[f].numpy())
+    a1.record(ext)
+    a1.synchronize()
+    e2e_ms = a0.elapsed_time(a1)
+    t_e2e = torch.tensor([e2e_ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t_e2e, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(t_e2e.item())
+    field_bytes = (N + 3) * (M + 3) * 8 * len(names)
+    e2e_value = world * cells * e2e_steps / (e2e_ms / 1e3)
+
+    result = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            st_t = sim.t
+            hmax = sim.get("hmax")
+            snap = {f: sim.get(f) for f in __import__("oracle").OracleSim.STATE_FIELDS}
+            n_cpu, el = cpu_port_sample(case, lambda f: snap[f], st_t, hmax, budget_s=args.cpu_seconds)
+            cpu = {"value": cells * n_cpu / el, "unit": "cell-updates/s", "cores": os.cpu_count(),
+                   "kind": "port",
+                   "sample": "%d ADI steps of the 1048x980 reach from t=%.0f s (the GPU state), oracle port "
+                             "(OpenMP, %d threads), %.1f s wall" % (n_cpu, st_t, os.cpu_count(), el)}
+        clocks = clk.summary()
+        result = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded meandering reach, config-2 shape)",
+            "config": {"workload": "config2_meander 1048x980 dx=5m dt=1s FP64 hydraulics+sediment+Exner, "
+                                   "t=%d..%d s" % (SPINUP_STEPS + args.warmup, SPINUP_STEPS + args.warmup + args.steps),
+                       "grid": [N, M], "cells": cells, "wet_cells": wet,
+                       "parallelism": "replicas%d" % world if world > 1 else "single",
+                       "l2": "per-step working set > 126 MB L2, no flush"},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": field_bytes,
+                    "d2h_bytes_per_step": field_bytes, "steps": e2e_steps,
+                    "api": "hyd_set_field(z,u,v,FS) + hyd_step(1) + hyd_get_field(z,u,v,FS), pinned host buffers"},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "bytes_per_launch": bytes_per_launch, "ms_per_launch": avg_ms},
+            "step_roofline": {"bytes_per_cell_update": 208, "achieved": value * 208 / 1e9 / world, "peak": peak,
+                              "frac": value * 208 / 1e9 / world / peak},
+            "phases": phases,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+    sim.close()
+    return result
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    import numpy as np
+    import oracle
+    from hydist import cases
+    case = cases.config2_case()
+    cells = case.N * case.M
+    ora = oracle.OracleSim(case, threads=os.cpu_count() or 1)
+    ora.init()
+    # the sample starts from the oracle's own spin-up state; spin-up is not timed
+    spin = min(SPINUP_STEPS, args.ref_spinup)
+    if spin:
+        ora.step(spin)
+    ora.step(max(1, args.warmup))
+    per_step = []
+    budget = args.cpu_seconds
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ora.step(1)
+        per_step.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget:
+            break
+    n = len(per_step)
+    el = sum(per_step)
+    value = cells * n / el
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": 0,
+        "steps": n, "warmup": args.warmup, "ms_per_step": el / n * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded meandering reach, config-2 shape)",
+        "config": {"workload": "config2_meander 1048x980 dx=5m dt=1s FP64 hydraulics+sediment+Exner",
+                   "grid": [case.N, case.M], "cells": cells},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "%d ADI steps after %d spin-up steps, oracle port (OpenMP)" % (n, spin)},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-spinup", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        res = run_reference(args, rank)
+        if res is not None:
+            print(json.dumps(res))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        res = run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if res is not None:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,774 @@
+// hydist_api.cu — the C ABI of include/hydist_b200.h.
+//
+// Replaces the reference's Python host (rep.py gpu_init, Pointers.py struct packing,
+// Engine.hydraulic_Calculation's time loop): one handle owns a device arena, a stream
+// and the launch sequence of a full ADI step.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hydist_b200.h"
+#include "hydist_dev.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                           \
+    do {                                                                                         \
+        cudaError_t e_ = (expr);                                                                 \
+        if (e_ != cudaSuccess) return fail(HYD_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr double kPiRef = 3.14159265359;
+
+}  // namespace
+
+long long hyd_kernel_launches_add(long long n) { return g_launches.fetch_add(n) + n; }
+
+struct FieldDesc {
+    const char* name;
+    int kind;     // 0 grid double, 1 grid int, 2 row table int (N+2)*20, 3 col table int (M+2)*20,
+                  // 4 int N+2, 5 int M+2, 6 double M+2, 7 double N+2, 8 hi, 9 hmax[4]
+    size_t off;   // offset of the pointer member in DevGrid
+};
+
+#define FD(n, k) {#n, k, offsetof(DevGrid, n)}
+static const FieldDesc kFieldTable[] = {
+    FD(h, 0),     FD(hsnham, 0), FD(Fw, 0),    FD(Tsxw, 0),    FD(Tsyw, 0),  FD(u, 0),
+    FD(v, 0),     FD(z, 0),      FD(t_u, 0),   FD(t_v, 0),     FD(t_z, 0),   FD(Htdu, 0),
+    FD(Htdv, 0),  FD(H_moi, 0),  FD(htaiz, 0), FD(htaiz_bd, 0), FD(Kx1, 0),  FD(Ky1, 0),
+    FD(FS, 0),    FD(tFS, 0),    FD(VTH, 0),   FD(Kx, 0),      FD(Ky, 0),    FD(Qbx, 0),
+    FD(Qby, 0),   FD(dH, 0),     FD(khouot, 1), FD(daui, 2),   FD(cuoii, 2), FD(moci, 4),
+    FD(dauj, 3),  FD(cuoij, 3),  FD(mocj, 5),  FD(ubt, 6),     FD(ubp, 6),   FD(vbt, 7),
+    FD(vbd, 7),   FD(hi, 8),     FD(hmax, 9),
+};
+#undef FD
+
+struct HydSim {
+    HydCaseParams P;
+    int N, M, pitch;
+    int device;
+    cudaStream_t stream;
+    DevGrid g;
+    DevParams dp;
+    double* scratch_u;  // smoothing ping-pong partners
+    double* scratch_v;
+    void* arena;
+    size_t arena_bytes;
+    std::vector<void*> extra;
+    double t;
+    int have_boundary;
+    int initialized;
+    int solver;
+    int start_idx, end_idx;
+    unsigned* h_status;
+    // phase timing (instrumentation)
+    int timing;
+    struct Mark {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    std::vector<Mark> marks;
+    std::vector<cudaEvent_t> event_pool;
+    double phase_ms[32];
+    long long phase_n[32];
+};
+
+static const char* kPhaseNames[] = {"boundary", "sweep_uz", "sweep_vz", "smooth", "explicit_v", "explicit_u",
+                                    "reset_rows", "reset_cols", "post", "scan", "vth_hesok", "fs_sweep_j",
+                                    "fs_sweep_i", "update_fs", "bed"};
+enum Phase { PH_BOUNDARY, PH_SWEEP_UZ, PH_SWEEP_VZ, PH_SMOOTH, PH_EXPL_V, PH_EXPL_U, PH_RESET_ROWS,
+             PH_RESET_COLS, PH_POST, PH_SCAN, PH_VTH, PH_FS_J, PH_FS_I, PH_UPDATE_FS, PH_BED, PH_COUNT };
+
+namespace {
+cudaEvent_t pool_event(HydSim* s) {
+    if (!s->event_pool.empty()) {
+        cudaEvent_t e = s->event_pool.back();
+        s->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+struct PhaseScope {
+    HydSim* s;
+    int ph;
+    cudaEvent_t a = nullptr;
+    PhaseScope(HydSim* s_, int ph_) : s(s_), ph(ph_) {
+        if (s->timing) {
+            a = pool_event(s);
+            cudaEventRecord(a, s->stream);
+        }
+    }
+    ~PhaseScope() {
+        if (s->timing) {
+            cudaEvent_t b = pool_event(s);
+            cudaEventRecord(b, s->stream);
+            s->marks.push_back({ph, a, b});
+        }
+    }
+};
+}  // namespace
+#define PHASE(ph) PhaseScope phase_scope_##__LINE__(s, ph)
+
+namespace {
+
+size_t field_count(const HydSim* s, int kind) {
+    const size_t N = s->N, M = s->M;
+    switch (kind) {
+        case 0:
+        case 1: return (N + 3) * (M + 3);
+        case 2: return (N + 2) * HYD_SEGL;
+        case 3: return (M + 2) * HYD_SEGL;
+        case 4: return N + 2;
+        case 5: return M + 2;
+        case 6: return M + 2;
+        case 7: return N + 2;
+        case 9: return 4;
+        default: return 2 * (N + 3) + 2 * (M + 3);
+    }
+}
+
+const FieldDesc* find_field(const char* name) {
+    if (!strcmp(name, "VISCOIDX") || !strcmp(name, "VISCOINDX")) {
+        static const FieldDesc visc = {"VISCOIDX", 0, offsetof(DevGrid, VISC)};
+        return &visc;
+    }
+    for (const FieldDesc& f : kFieldTable)
+        if (!strcmp(f.name, name)) return &f;
+    return nullptr;
+}
+
+void* member(HydSim* s, const FieldDesc* f) { return *(void**)((char*)&s->g + f->off); }
+
+DevParams make_dev_params(const HydCaseParams& P) {
+    DevParams d;
+    d.dX = P.dX;
+    d.dY = P.dY;
+    d.dT = P.dT;
+    d.dXbp = P.dXbp;
+    d.dX2 = P.dX2;
+    d.dYbp = P.dYbp;
+    d.dY2 = P.dY2;
+    d.dTchia2dX = P.dTchia2dX;
+    d.dTchia2dY = P.dTchia2dY;
+    d.HaiChiadT = P.HaiChiadT;
+    d.NANGDAY = P.NANGDAY;
+    d.H_TINH = P.H_TINH;
+    d.heso = P.heso;
+    d.mu_mn = P.mu_mn;
+    d.NDnen = P.NDnen;
+    d.Tod = P.Tod;
+    d.Toe = P.Toe;
+    d.hstoe = P.hstoe;
+    d.ghtoe = P.ghtoe;
+    d.Mbochat = P.Mbochat;
+    d.ro = P.ro;
+    d.ros = P.ros;
+    d.dm = P.dm;
+    d.Dorong = P.Dorong;
+    d.Sx = P.Sx;
+    d.CORIOLIS_FORCE = P.CORIOLIS_FORCE;
+    d.g = P.g;
+    d.Ks = P.Ks;
+    // device helpers of constant.cuh:126-133
+    d.windx = 0.0013 * (0.00075 + 0.000067 * std::fabs(P.Wind)) * std::fabs(P.Wind) * P.Wind *
+              std::cos(P.huonggio * (kPiRef / 180));
+    d.windy = 0.0013 * (0.00075 + 0.000067 * std::fabs(P.Wind)) * std::fabs(P.Wind) * P.Wind *
+              std::sin(P.huonggio * (kPiRef / 180));
+    d.ufr = 0.25 * std::pow((P.Sx - 1) * P.g, 8.0 / 15.0) * std::pow(P.dm, 9.0 / 15.0) * std::pow(P.muy, -1.0 / 15.0);
+    d.dxr = P.dm * std::pow(P.g * (P.Sx - 1) / P.muy * P.muy, (1.0 / 3.0));
+    d.wss = 10 * P.muy / P.dm * (std::sqrt(1 + 0.01 * (P.Sx - 1) * 9.81 * std::pow(P.dm, 3) / std::pow(P.muy, 2)) - 1);
+    d.sediment_start = P.sediment_start;
+    d.bed_change_start = P.bed_change_start;
+    d.ketdinh = P.ketdinh;
+    d.kenhhepd = P.kenhhepd;
+    d.kenhhepng = P.kenhhepng;
+    d.channel = (P.kenhhepd || P.kenhhepng) ? 1 : 0;
+    return d;
+}
+
+int check_device_status(HydSim* s) {
+    unsigned st = 0;
+    CUDA_TRY(cudaMemcpyAsync(&st, s->g.status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (st & HYD_ST_SEG_OVERFLOW)
+        return fail(HYD_EDEVICE, "a grid line has more than 20 wet segments (segment_limit)");
+    return HYD_OK;
+}
+
+// mass balance: per-block partial sums, then one block adds them in a fixed order
+__global__ void k_mass_partial(DevGrid g, double* part) {
+    __shared__ double sh[5][256];
+    const int tid = threadIdx.x;
+    double a = 0, b = 0, c = 0, wet = 0, bad = 0;
+    const long long ncell = (long long)(g.N + 3) * (g.M + 3);
+    for (long long q = (long long)blockIdx.x * blockDim.x + tid; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q / (g.M + 3)), j = (int)(q % (g.M + 3));
+        const int gp = i * g.P + j;
+        if (i <= g.N && j <= g.M) {
+            if (!isfinite(g.z[gp]) || !isfinite(g.u[gp]) || !isfinite(g.v[gp]) || !isfinite(g.FS[gp])) bad += 1;
+        }
+        if (i < 2 || j < 2 || i > g.N || j > g.M) continue;
+        if (g.khouot[gp] == 0) {
+            a += g.H_moi[gp];
+            b += g.FS[gp] * g.H_moi[gp];
+            wet += 1;
+        }
+        if (isfinite(g.dH[gp])) c += g.dH[gp];
+    }
+    sh[0][tid] = a;
+    sh[1][tid] = b;
+    sh[2][tid] = c;
+    sh[3][tid] = wet;
+    sh[4][tid] = bad;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (tid < w)
+            for (int k = 0; k < 5; k++) sh[k][tid] += sh[k][tid + w];
+        __syncthreads();
+    }
+    if (tid == 0)
+        for (int k = 0; k < 5; k++) part[blockIdx.x * 5 + k] = sh[k][0];
+}
+
+__global__ void k_mass_final(const double* part, int nblocks, double* out) {
+    if (threadIdx.x != 0) return;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int b = 0; b < nblocks; b++)
+        for (int k = 0; k < 5; k++) acc[k] += part[b * 5 + k];
+    for (int k = 0; k < 5; k++) out[k] = acc[k];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hyd_last_error(void) { return g_last_error.c_str(); }
+
+const char* hyd_version(void) { return "hydist_b200 1.0 (sm_100a, FP64 ADI, partitioned line solver)"; }
+
+void hyd_params_derive(HydCaseParams* p) {
+    p->dXbp = p->dX * p->dX;
+    p->dX2 = 2 * p->dX;
+    p->dYbp = p->dY * p->dY;
+    p->dY2 = 2 * p->dY;
+    p->dTchia2dX = p->dT / (2 * p->dX);
+    p->dTchia2dY = p->dT / (2 * p->dY);
+    p->QuyDoiTime = 1.0 / 3600;
+    p->QuyDoiPi = 1.0 / kPiRef;
+    p->HaiChiadT = 2.0 / p->dT;
+}
+
+void hyd_params_default(HydCaseParams* p) {
+    memset(p, 0, sizeof(*p));
+    p->dX = 10.0;
+    p->dY = 10.0;
+    p->dT = 2.0;
+    p->NANGDAY = 0.0;
+    p->H_TINH = 0.02;
+    p->Wind = 0.0;
+    p->huonggio = 0.0;
+    p->Zbandau = 0.0;
+    p->heso = 0.94;
+    p->mu_mn = 0.2;
+    p->NDnen = 0.0;
+    p->NDbphai = p->NDbtrai = p->NDbtren = p->NDbduoi = 0.5;
+    p->Tod = 0.06;
+    p->Toe = 0.15;
+    p->hstoe = 0;
+    p->ghtoe = 3;
+    p->Mbochat = 0.00001;
+    p->ro = 1000;
+    p->ros = 2000;
+    p->dm = 0.00001;
+    p->d90 = 0.002;
+    p->muy = 1.01e-06;
+    p->Dorong = 0.5;
+    p->Sx = 2;
+    p->sohn = 8;
+    p->soha = 3;
+    p->sohn1 = 3;
+    p->CORIOLIS_FORCE = 0.0;
+    p->g = 9.81;
+    p->Ks = 2.5 * 0.00001;
+    p->sediment_start = 36000;
+    p->bed_change_start = 72000;
+    p->ketdinh = 1;
+    hyd_params_derive(p);
+}
+
+int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out) {
+    if (!p || !out) return fail(HYD_EINVAL, "null argument");
+    if (N < 6 || M < 6) return fail(HYD_EINVAL, "grid too small (N, M >= 6)");
+    if (p->dT <= 0 || p->dX <= 0 || p->dY <= 0) return fail(HYD_EINVAL, "dX, dY, dT must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(HYD_ECUDA, "no CUDA device: this library has no CPU path");
+    if (device < 0 || device >= ndev) return fail(HYD_EINVAL, "bad device index");
+    CUDA_TRY(cudaSetDevice(device));
+    HydSim* s = new HydSim();
+    s->P = *p;
+    s->N = N;
+    s->M = M;
+    s->pitch = ((M + 3) + 31) / 32 * 32;
+    s->device = device;
+    s->t = 0;
+    s->have_boundary = 0;
+    s->initialized = 0;
+    const char* sv = getenv("HYD_SOLVER");
+    s->solver = (sv && !strcmp(sv, "thomas")) ? 1 : 0;
+    s->start_idx = 2;
+    s->end_idx = N;
+    s->timing = 0;
+    for (int k = 0; k < 32; k++) {
+        s->phase_ms[k] = 0;
+        s->phase_n[k] = 0;
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(HYD_ECUDA, std::string("stream: ") + cudaGetErrorString(e));
+    }
+    // arena: grid fields (double and int), smoothing partners, tables, boundary arrays
+    const size_t nrow = (size_t)N + 3;
+    const size_t gbytes = nrow * s->pitch * sizeof(double);
+    const size_t ngrid = 26;  // double grid fields in kFieldTable + VISC
+    const size_t nseg_rows = ((size_t)N + 3) * HYD_SEGL, nseg_cols = ((size_t)M + 3) * HYD_SEGL;
+    auto a256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    size_t total = a256(gbytes) * (ngrid + 1 + 2) + a256(nrow * s->pitch * sizeof(int));
+    total += 2 * a256(nseg_rows * 4) + a256((N + 3) * 4) + 2 * a256(nseg_cols * 4) + a256((M + 3) * 4);
+    total += 2 * a256((M + 3) * 8) + 2 * a256((N + 3) * 8) + a256((2 * (N + 3) + 2 * (M + 3)) * 8);
+    total += a256(4 * 8) + a256(4 * 4) + a256(4 * HYD_SEGL * 4) + a256(64);
+    e = cudaMalloc(&s->arena, total);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return fail(HYD_ENOMEM, std::string("device arena: ") + cudaGetErrorString(e));
+    }
+    s->arena_bytes = total;
+    cudaMemset(s->arena, 0, total);
+    char* cur = (char*)s->arena;
+    auto take = [&](size_t b) {
+        char* q = cur;
+        cur += a256(b);
+        return (void*)q;
+    };
+    DevGrid& g = s->g;
+    memset(&g, 0, sizeof g);
+    g.N = N;
+    g.M = M;
+    g.P = s->pitch;
+    double** gd[] = {&g.h,   &g.hsnham, &g.VISC,  &g.Fw,   &g.Tsxw,  &g.Tsyw,     &g.u,   &g.v,   &g.z,
+                     &g.t_u, &g.t_v,    &g.t_z,   &g.Htdu, &g.Htdv,  &g.H_moi,    &g.htaiz, &g.htaiz_bd,
+                     &g.Kx1, &g.Ky1,    &g.FS,    &g.tFS,  &g.VTH,   &g.Kx,       &g.Ky,  &g.Qbx, &g.Qby,
+                     &g.dH};
+    for (double** q : gd) *q = (double*)take(gbytes);
+    s->scratch_u = (double*)take(gbytes);
+    s->scratch_v = (double*)take(gbytes);
+    g.khouot = (int*)take(nrow * s->pitch * sizeof(int));
+    g.daui = (int*)take(nseg_rows * 4);
+    g.cuoii = (int*)take(nseg_rows * 4);
+    g.moci = (int*)take((N + 3) * 4);
+    g.dauj = (int*)take(nseg_cols * 4);
+    g.cuoij = (int*)take(nseg_cols * 4);
+    g.mocj = (int*)take((M + 3) * 4);
+    g.ubt = (double*)take((M + 3) * 8);
+    g.ubp = (double*)take((M + 3) * 8);
+    g.vbt = (double*)take((N + 3) * 8);
+    g.vbd = (double*)take((N + 3) * 8);
+    g.hi = (double*)take((2 * (N + 3) + 2 * (M + 3)) * 8);
+    g.hmax = (double*)take(4 * 8);
+    g.bienQ = (int*)take(4 * 4);
+    g.btype = (int*)take(4 * HYD_SEGL * 4);
+    g.status = (unsigned*)take(64);
+    if ((size_t)(cur - (char*)s->arena) > total) {
+        cudaFree(s->arena);
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return fail(HYD_ENOMEM, "arena layout overflow");
+    }
+    s->dp = make_dev_params(s->P);
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaFree(s->arena);
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return fail(HYD_ECUDA, std::string("create: ") + cudaGetErrorString(e));
+    }
+    *out = s;
+    return HYD_OK;
+}
+
+int hyd_destroy(hyd_handle h) {
+    if (!h) return HYD_OK;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    for (void* q : h->extra) cudaFree(q);
+    for (auto& m : h->marks) {
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
+    cudaFree(h->arena);
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return HYD_OK;
+}
+
+int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count) {
+    if (!h || !name || !host) return fail(HYD_EINVAL, "null argument");
+    const FieldDesc* f = find_field(name);
+    if (!f) return fail(HYD_EINVAL, std::string("unknown field ") + name);
+    if (count != field_count(h, f->kind)) return fail(HYD_EINVAL, std::string("wrong element count for ") + name);
+    CUDA_TRY(cudaSetDevice(h->device));
+    void* dst = member(h, f);
+    if (f->kind == 0 || f->kind == 1) {
+        const size_t es = f->kind == 0 ? 8 : 4;
+        CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)h->pitch * es, host, (size_t)(h->M + 3) * es, (size_t)(h->M + 3) * es,
+                                   (size_t)h->N + 3, cudaMemcpyHostToDevice, h->stream));
+    } else {
+        const size_t es = (f->kind >= 6) ? 8 : 4;
+        CUDA_TRY(cudaMemcpyAsync(dst, host, count * es, cudaMemcpyHostToDevice, h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HYD_OK;
+}
+
+int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count) {
+    if (!h || !name || !host) return fail(HYD_EINVAL, "null argument");
+    const FieldDesc* f = find_field(name);
+    if (!f) return fail(HYD_EINVAL, std::string("unknown field ") + name);
+    if (count != field_count(h, f->kind)) return fail(HYD_EINVAL, std::string("wrong element count for ") + name);
+    CUDA_TRY(cudaSetDevice(h->device));
+    const void* src = member(h, f);
+    if (f->kind == 0 || f->kind == 1) {
+        const size_t es = f->kind == 0 ? 8 : 4;
+        CUDA_TRY(cudaMemcpy2DAsync(host, (size_t)(h->M + 3) * es, src, (size_t)h->pitch * es, (size_t)(h->M + 3) * es,
+                                   (size_t)h->N + 3, cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        const size_t es = (f->kind >= 6) ? 8 : 4;
+        CUDA_TRY(cudaMemcpyAsync(host, src, count * es, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HYD_OK;
+}
+
+int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const* tables, const double* const* cc,
+                     const int* nseg, int total_time) {
+    if (!h || !boundary_type || !tables || !cc || !nseg) return fail(HYD_EINVAL, "null argument");
+    if (total_time < 2) return fail(HYD_EINVAL, "total_time must be >= 2");
+    CUDA_TRY(cudaSetDevice(h->device));
+    int bienQ[4];
+    for (int e = 0; e < 4; e++) {
+        bienQ[e] = 0;
+        for (int k = 0; k < HYD_SEGL; k++) {
+            const int bt = boundary_type[e * HYD_SEGL + k];
+            if (bt < 0 || bt > 2) return fail(HYD_EINVAL, "boundary_type values must be 0, 1 or 2");
+            if (bt == 2) bienQ[e] = 1;
+        }
+        if (nseg[e] < 0 || nseg[e] > HYD_SEGL) return fail(HYD_EINVAL, "nseg out of range");
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->g.bienQ, bienQ, sizeof bienQ, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->g.btype, boundary_type, 4 * HYD_SEGL * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    for (int e = 0; e < 4; e++) {
+        const size_t n = (size_t)(nseg[e] > 0 ? nseg[e] : 1) * total_time + 2;
+        void* q = nullptr;
+        CUDA_TRY(cudaMalloc(&q, n * 8));
+        h->extra.push_back(q);
+        CUDA_TRY(cudaMemsetAsync(q, 0, n * 8, h->stream));
+        void* q2 = nullptr;
+        CUDA_TRY(cudaMalloc(&q2, n * 8));
+        h->extra.push_back(q2);
+        CUDA_TRY(cudaMemsetAsync(q2, 0, n * 8, h->stream));
+        if (nseg[e] > 0) {
+            if (!tables[e] || !cc[e]) return fail(HYD_EINVAL, "missing boundary table");
+            CUDA_TRY(cudaMemcpyAsync(q, tables[e], (size_t)nseg[e] * total_time * 8, cudaMemcpyHostToDevice, h->stream));
+            CUDA_TRY(cudaMemcpyAsync(q2, cc[e], (size_t)nseg[e] * total_time * 8, cudaMemcpyHostToDevice, h->stream));
+        }
+        h->g.bc[e] = (double*)q;
+        h->g.cc[e] = (double*)q2;
+    }
+    h->g.total_time = total_time;
+    h->have_boundary = 1;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HYD_OK;
+}
+
+int hyd_init(hyd_handle h, double t_start) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    if (!h->have_boundary) return fail(HYD_ESTATE, "hyd_set_boundary must precede hyd_init");
+    CUDA_TRY(cudaSetDevice(h->device));
+    launch_init_kernels(h->g, h->dp, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->t = t_start;
+    h->initialized = 1;
+    return check_device_status(h);
+}
+
+static void half_step_1(HydSim* s, double t) {
+    DevGrid& g = s->g;
+    const DevParams& p = s->dp;
+    cudaStream_t st = s->stream;
+    { PHASE(PH_BOUNDARY); launch_boundary(g, p, t, st); }
+    int start_idx = 2, end_idx = s->M;
+    if (p.channel && s->P.kenhhepd == 1) {
+        start_idx = 3;
+        end_idx = s->M - 1;
+    }
+    { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, start_idx, end_idx, s->solver, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, st); }
+    std::swap(g.t_u, s->scratch_u);
+    { PHASE(PH_EXPL_V); launch_explicit_v(g, p, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, st); }
+    std::swap(g.t_v, s->scratch_v);
+    { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, st); }
+    { PHASE(PH_POST); launch_post(g, p, st); }
+    { PHASE(PH_SCAN); launch_scan_fs_edges(g, p, st); }
+    if (t >= s->P.sediment_start) {
+        { PHASE(PH_VTH); launch_vth_hesok(g, p, st); }
+        { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, t, s->solver, st); }
+        { PHASE(PH_UPDATE_FS); launch_update_fs(g, st); }
+        start_idx = 3;
+        end_idx = s->M - 1;
+    }
+    s->start_idx = start_idx;
+    s->end_idx = end_idx;
+}
+
+static void half_step_2(HydSim* s, double t) {
+    DevGrid& g = s->g;
+    const DevParams& p = s->dp;
+    cudaStream_t st = s->stream;
+    { PHASE(PH_BOUNDARY); launch_boundary(g, p, t, st); }
+    int start_idx = 2, end_idx = s->N;
+    if (p.channel && s->P.kenhhepng == 1) {
+        start_idx = 3;
+        end_idx = s->N;
+    }
+    { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, start_idx, end_idx, s->solver, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, st); }
+    std::swap(g.t_v, s->scratch_v);
+    { PHASE(PH_EXPL_U); launch_explicit_u(g, p, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, st); }
+    std::swap(g.t_u, s->scratch_u);
+    { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, st); }
+    { PHASE(PH_POST); launch_post(g, p, st); }
+    { PHASE(PH_SCAN); launch_scan_fs_edges(g, p, st); }
+    if (t >= s->P.sediment_start) {
+        { PHASE(PH_VTH); launch_vth_hesok(g, p, st); }
+        { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, t, s->solver, st); }
+        { PHASE(PH_UPDATE_FS); launch_update_fs(g, st); }
+        start_idx = 3;
+        end_idx = s->N - 1;
+    }
+    // Engine.py:364-366: int(t) % bed_change_start == 0 and t integral
+    const double it = (double)(long long)t;
+    if (std::fmod(it, s->P.bed_change_start) == 0 && t - it == 0) {
+        PHASE(PH_BED);
+        launch_bed(g, p, start_idx, end_idx, st);
+    }
+    s->start_idx = start_idx;
+    s->end_idx = end_idx;
+}
+
+int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_step");
+    if (nsteps < 0) return fail(HYD_EINVAL, "nsteps < 0");
+    CUDA_TRY(cudaSetDevice(h->device));
+    // the hourly tables must cover the last hour index reached (support_funcs.cu:565)
+    const double t_end = h->t + nsteps * h->P.dT;
+    if ((int)(t_end / 3600) + 1 >= h->g.total_time)
+        return fail(HYD_EINVAL, "boundary tables too short for the requested time span");
+    double t = h->t;
+    for (int n = 0; n < nsteps; n++) {
+        t = t + h->P.dT * 0.5;
+        half_step_1(h, t);
+        t = t + h->P.dT * 0.5;
+        half_step_2(h, t);
+    }
+    h->t = t;
+    CUDA_TRY(cudaGetLastError());
+    if (t_out) *t_out = t;
+    if (sync) return check_device_status(h);
+    return HYD_OK;
+}
+
+int hyd_set_params(hyd_handle h, const HydCaseParams* p) {
+    if (!h || !p) return fail(HYD_EINVAL, "null argument");
+    if (p->dT <= 0 || p->dX <= 0 || p->dY <= 0) return fail(HYD_EINVAL, "dX, dY, dT must be positive");
+    h->P = *p;
+    h->dp = make_dev_params(h->P);
+    return HYD_OK;
+}
+
+int hyd_get_time(hyd_handle h, double* t) {
+    if (!h || !t) return fail(HYD_EINVAL, "null argument");
+    *t = h->t;
+    return HYD_OK;
+}
+
+int hyd_synchronize(hyd_handle h) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    CUDA_TRY(cudaGetLastError());
+    return check_device_status(h);
+}
+
+int hyd_mass_balance(hyd_handle h, double* out, int n) {
+    if (!h || !out || n < 5) return fail(HYD_EINVAL, "need 5 output slots");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int nb = 148;
+    double* part = nullptr;
+    CUDA_TRY(cudaMallocAsync(&part, (size_t)nb * 5 * 8 + 5 * 8, h->stream));
+    k_mass_partial<<<nb, 256, 0, h->stream>>>(h->g, part);
+    k_mass_final<<<1, 32, 0, h->stream>>>(part, nb, part + nb * 5);
+    hyd_kernel_launches_add(2);
+    double r[5];
+    CUDA_TRY(cudaMemcpyAsync(r, part + nb * 5, sizeof r, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaFreeAsync(part, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const double area = h->P.dX * h->P.dY;
+    out[0] = r[0] * area;
+    out[1] = r[1] * area;
+    out[2] = r[2] * area;
+    out[3] = r[3];
+    out[4] = r[4];
+    return HYD_OK;
+}
+
+int hyd_state_size(hyd_handle h, size_t* bytes) {
+    if (!h || !bytes) return fail(HYD_EINVAL, "null argument");
+    size_t b = 64;
+    for (const FieldDesc& f : kFieldTable) {
+        const size_t es = (f.kind == 0 || f.kind >= 6) ? 8 : 4;
+        b += field_count(h, f.kind) * es;
+    }
+    b += (size_t)(h->N + 3) * (h->M + 3) * 8;  // VISCOIDX
+    *bytes = b;
+    return HYD_OK;
+}
+
+int hyd_get_state(hyd_handle h, void* buf, size_t bytes) {
+    size_t need = 0;
+    int rc = hyd_state_size(h, &need);
+    if (rc) return rc;
+    if (!buf || bytes < need) return fail(HYD_EINVAL, "state buffer too small");
+    char* p = (char*)buf;
+    memset(p, 0, 64);
+    memcpy(p, &h->t, 8);
+    memcpy(p + 8, &h->N, 4);
+    memcpy(p + 12, &h->M, 4);
+    memcpy(p + 16, &h->start_idx, 4);
+    memcpy(p + 20, &h->end_idx, 4);
+    p += 64;
+    for (const FieldDesc& f : kFieldTable) {
+        const size_t es = (f.kind == 0 || f.kind >= 6) ? 8 : 4;
+        const size_t n = field_count(h, f.kind);
+        rc = hyd_get_field(h, f.name, p, n);
+        if (rc) return rc;
+        p += n * es;
+    }
+    rc = hyd_get_field(h, "VISCOIDX", p, (size_t)(h->N + 3) * (h->M + 3));
+    if (rc) return rc;
+    return HYD_OK;
+}
+
+int hyd_set_state(hyd_handle h, const void* buf, size_t bytes) {
+    size_t need = 0;
+    int rc = hyd_state_size(h, &need);
+    if (rc) return rc;
+    if (!buf || bytes < need) return fail(HYD_EINVAL, "state buffer too small");
+    const char* p = (const char*)buf;
+    int n0, m0;
+    memcpy(&n0, p + 8, 4);
+    memcpy(&m0, p + 12, 4);
+    if (n0 != h->N || m0 != h->M) return fail(HYD_EINVAL, "state image is for a different grid");
+    memcpy(&h->t, p, 8);
+    memcpy(&h->start_idx, p + 16, 4);
+    memcpy(&h->end_idx, p + 20, 4);
+    p += 64;
+    for (const FieldDesc& f : kFieldTable) {
+        const size_t es = (f.kind == 0 || f.kind >= 6) ? 8 : 4;
+        const size_t n = field_count(h, f.kind);
+        rc = hyd_set_field(h, f.name, p, n);
+        if (rc) return rc;
+        p += n * es;
+    }
+    rc = hyd_set_field(h, "VISCOIDX", p, (size_t)(h->N + 3) * (h->M + 3));
+    if (rc) return rc;
+    h->initialized = 1;
+    return HYD_OK;
+}
+
+int hyd_device_status(hyd_handle h, unsigned* status) {
+    if (!h || !status) return fail(HYD_EINVAL, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaMemcpyAsync(status, h->g.status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HYD_OK;
+}
+
+int hyd_get_stream(hyd_handle h, void** stream) {
+    if (!h || !stream) return fail(HYD_EINVAL, "null argument");
+    *stream = (void*)h->stream;
+    return HYD_OK;
+}
+
+int hyd_set_timing(hyd_handle h, int enable) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    h->timing = enable ? 1 : 0;
+    return HYD_OK;
+}
+
+int hyd_timing_report(hyd_handle h, char* buf, size_t buflen) {
+    if (!h || !buf || buflen == 0) return fail(HYD_EINVAL, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (auto& m : h->marks) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, m.a, m.b);
+        h->phase_ms[m.phase] += ms;
+        h->phase_n[m.phase] += 1;
+        h->event_pool.push_back(m.a);
+        h->event_pool.push_back(m.b);
+    }
+    h->marks.clear();
+    std::string out;
+    char line[128];
+    for (int k = 0; k < PH_COUNT; k++) {
+        if (h->phase_n[k] == 0) continue;
+        snprintf(line, sizeof line, "%s %lld %.6f\n", kPhaseNames[k], h->phase_n[k], h->phase_ms[k]);
+        out += line;
+        h->phase_ms[k] = 0;
+        h->phase_n[k] = 0;
+    }
+    snprintf(buf, buflen, "%s", out.c_str());
+    return HYD_OK;
+}
+
+int hyd_launch_count(hyd_handle h, long long* count) {
+    (void)h;
+    if (!count) return fail(HYD_EINVAL, "null argument");
+    *count = g_launches.load();
+    return HYD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// hydist_dev.cuh — device-side state, parameters and helpers of the B200 ADI library.
+//
+// Layout in HBM: every (N+3) x (M+3) grid field of the reference (Argument_Pointers,
+// constant.cuh:6-20) is stored row-major with a pitch P >= M+3 that is a multiple of
+// 32 doubles (256 B), so every row starts on a 256-byte boundary.  Element (i, j) is
+// at i*P + j; i is the x / "N" direction (u faces, dX), j the y / "M" direction
+// (v faces, dY).  Segment tables keep the reference's [line][20] layout.
+#pragma once
+
+#include <cstdint>
+
+#define HYD_SEGL 20
+
+// Device status bits (read back by hyd_synchronize).
+#define HYD_ST_SEG_OVERFLOW 1u     // more than 20 wet segments on a line
+#define HYD_ST_INTERP_RANGE 2u     // edge FS interpolation index left the grid
+#define HYD_ST_DEGENERATE 4u       // single-cell segment on an open edge (reference reads stale scratch)
+
+struct DevParams {
+    double dX, dY, dT, dXbp, dX2, dYbp, dY2, dTchia2dX, dTchia2dY, HaiChiadT;
+    double NANGDAY, H_TINH, heso, mu_mn, NDnen, Tod, Toe, hstoe, ghtoe, Mbochat, ro, ros, dm,
+        Dorong, Sx, CORIOLIS_FORCE, g, Ks;
+    // device helpers of constant.cuh:126-133, evaluated once
+    double windx, windy, ufr, dxr, wss;
+    double sediment_start, bed_change_start;
+    int ketdinh, kenhhepd, kenhhepng, channel;
+};
+
+struct DevGrid {
+    int N, M, P;
+    int total_time;
+    // grid fields (pitch P)
+    double *h, *hsnham, *VISC, *Fw, *Tsxw, *Tsyw;
+    double *u, *v, *z, *t_u, *t_v, *t_z;
+    double *Htdu, *Htdv, *H_moi, *htaiz, *htaiz_bd, *Kx1, *Ky1;
+    double *FS, *tFS, *VTH, *Kx, *Ky, *Qbx, *Qby, *dH;
+    int* khouot;
+    // segment tables (reference layout)
+    int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
+    // boundary data
+    double *ubt, *ubp, *vbt, *vbd, *hi, *hmax;  // hmax[4]: 1/(ros*hmax) per edge (up, down, left, right)
+    int *bienQ, *btype;                          // bienQ[4], btype[4*20]
+    double *bc[4], *cc[4];                       // [nseg][total_time] per edge
+    unsigned* status;
+};
+
+__device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { atomicOr(g.status, bit); }
+
+// Wall/open flags of a row segment [first, last] (locate_segment_v, constant.cuh:135-154).
+__device__ __forceinline__ void seg_flags_v(const DevGrid& g, const DevParams& p, int row, int first, int last,
+                                            int& br1, int& br2) {
+    const int P = g.P;
+    br1 = (first > 2) ||
+          (first == 2 && (g.h[row * P + first - 1] + g.h[(row - 1) * P + first - 1]) * 0.5 == p.NANGDAY);
+    br2 = (last < g.M) || (last == g.M && (g.h[row * P + last] + g.h[(row - 1) * P + last]) * 0.5 == p.NANGDAY);
+}
+
+// Wall/open flags of a column segment (locate_segment_u, constant.cuh:156-178).
+__device__ __forceinline__ void seg_flags_u(const DevGrid& g, const DevParams& p, int col, int first, int last,
+                                            int& br1, int& br2) {
+    const int P = g.P;
+    br1 = (first > 2) || (first == 2 && (g.h[1 * P + col] + g.h[1 * P + col - 1]) * 0.5 == p.NANGDAY);
+    br2 = (last < g.N) || (last == g.N && (g.h[g.N * P + col] + g.h[g.N * P + col - 1]) * 0.5 == p.NANGDAY);
+}
+
+// Segment of row `row` holding column `col`, -1 if none.
+__device__ __forceinline__ int find_seg_v(const DevGrid& g, int row, int col, int& first, int& last) {
+    const int n = g.moci[row];
+    for (int k = 0; k < n; k++) {
+        const int a = g.daui[row * HYD_SEGL + k], b = g.cuoii[row * HYD_SEGL + k];
+        if (a <= col && col <= b) {
+            first = a;
+            last = b;
+            return k;
+        }
+    }
+    return -1;
+}
+
+// Segment of column `col` holding row `row`, -1 if none.
+__device__ __forceinline__ int find_seg_u(const DevGrid& g, int row, int col, int& first, int& last) {
+    const int n = g.mocj[col];
+    for (int k = 0; k < n; k++) {
+        const int a = g.dauj[col * HYD_SEGL + k], b = g.cuoij[col * HYD_SEGL + k];
+        if (a <= row && row <= b) {
+            first = a;
+            last = b;
+            return k;
+        }
+    }
+    return -1;
+}
+
+// Host launch wrappers (defined in the .cu files, called by hydist_api.cu).
+struct StepLaunch;
+void launch_init_kernels(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_boundary(const DevGrid& g, const DevParams& p, double t, cudaStream_t s);
+void launch_sweep_uz(const DevGrid& g, const DevParams& p, int startidx, int endidx, int solver, cudaStream_t s);
+void launch_sweep_vz(const DevGrid& g, const DevParams& p, int startidx, int endidx, int solver, cudaStream_t s);
+void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, cudaStream_t s);
+void launch_explicit_v(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_explicit_u(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_reset_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_reset_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_post(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_scan_fs_edges(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_vth_hesok(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, double t, int solver, cudaStream_t s);
+void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, double t, int solver, cudaStream_t s);
+void launch_update_fs(const DevGrid& g, cudaStream_t s);
+void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, cudaStream_t s);
+long long hyd_kernel_launches_add(long long n);

@@ -173,7 +173,7 @@ def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=12
                  noise_len=50.0, manning=0.025, manning_spread=0.10, Q0=2000.0, Q1=3500.0,
                  tide_amp=1.0, tide_period_h=12.42, d50=1e-4, Sx=2.7125, cc_in=0.2,
                  sediment_start=1800.0, bed_change_start=3600.0, y_center=None, spinup_h=0.0,
-                 name="meander"):
+                 end_cells=8, name="meander"):
     """Seeded meandering reach with a parabolic channel, floodplain and bed noise.
 
     Centreline y = y_c + amp*sin(2*pi*x/wavelength); parabolic section of `width` and
@@ -185,14 +185,19 @@ def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=12
     `bed_change_start`.  The reference's hourly tables are linearly interpolated
     (support_funcs.cu:547-565), so the boundary forcing is given at hourly knots.
 
+    The first and last `end_cells` cross-sections are rectangular (full depth across
+    the channel width) and blend into the parabola over the next `end_cells`.
+
     With spinup_h > 0 the discharge first ramps linearly from 0 to Q0 over spinup_h
     hours (the scheme cannot carry the bore of an impulsive start at Q0 into water at
-    rest), the stated hydrograph follows, and sediment_start is counted from the end of
-    the spin-up.
+    rest) and the stated hydrograph follows.  sediment_start and bed_change_start are
+    absolute times: the reference's Exner step divides by the speed VTH that only the
+    sediment phase computes (Sediment_Transport.cu:365-374), so the bed must not start
+    changing before the sediment does.
     """
     rng = np.random.default_rng(seed)
     p = default_params(dX=dX, dY=dX, dT=dT, dm=d50, Sx=Sx, Ks=2.5 * d50,
-                       sediment_start=sediment_start + spinup_h * 3600.0,
+                       sediment_start=sediment_start,
                        bed_change_start=bed_change_start, ketdinh=1)
     derive(p)
     x = np.arange(N, dtype=np.float64)[:, None] * dX
@@ -201,6 +206,15 @@ def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=12
     d = np.abs(y - yc)
     half = width / 2.0
     zb = np.where(d <= half, -depth * (1.0 - (d / half) ** 2), floodplain)
+    if end_cells > 0:
+        # rectangular inlet/outlet sections blended into the parabola: the reference
+        # derives the stage-edge velocity from continuity divided by the edge face
+        # depth (UVZSolver_multithread.cu:720), which shallow bank cells make unstable
+        rect = np.where(d <= half, -depth, floodplain)
+        a = np.arange(N, dtype=np.float64)[:, None]
+        dist = np.minimum(a, N - 1 - a)
+        w = np.clip((2.0 * end_cells - dist) / end_cells, 0.0, 1.0)
+        zb = w * rect + (1.0 - w) * zb
     zb = zb + _gaussian_field(rng, (N, M), noise_len / dX, noise_sigma)
     h = -zb
     _prismatic_ends(h)
@@ -270,3 +284,28 @@ def islands_case(N=48, M=36, dX=5.0, dT=1.0, seed=7, hours=1.0, sediment_start=0
 
 def steps_for(case, hours):
     return int(round(hours * 3600 / case.params.dT))
+
+
+# --------------------------------------------------------------------------------
+# Named workloads
+
+def config1_case():
+    """Plain FP64 hydraulics, straight channel 400 x 60, dx = 5 m, dt = 2 s, 1800 steps."""
+    return channel_case(N=400, M=60, dX=5.0, dT=2.0, bank=5, depth=3.0, slope=1e-4, bank_height=2.0,
+                        manning=0.025, Q=150.0, hours=1, z_out=0.0, name="config1_channel")
+
+
+CONFIG2_Q_SCALE = 0.25
+
+
+def config2_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE):
+    """Meandering reach 1048 x 980, dx = 5 m, dt = 1 s, hydraulics + sediment + bed change.
+
+    Stated geometry, grid, time step, roughness, tide, sediment and start times.  Three
+    changes make the run stable under the reference's own scheme (the oracle and the
+    reference's kernels both reach NaN otherwise): a one-hour discharge ramp from rest,
+    rectangular inlet/outlet sections, and the 2000 -> 3500 m3/s hydrograph scaled by
+    `q_scale` (at full scale the explicit central-difference cross-advection develops a
+    2-cell oscillation once velocities pass about 2.5 m/s)."""
+    return meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, spinup_h=spinup_h,
+                        Q0=2000.0 * q_scale, Q1=3500.0 * q_scale, name="config2_meander")

@@ -1,0 +1,219 @@
+"""ctypes binding of libhydist_b200.so (the C ABI declared in include/hydist_b200.h).
+
+There is no CPU fallback: if the library or a CUDA device is missing, every call
+raises.  The shared object is built in-tree by ``make -C gpu-hydist_b200``.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .params import HydCaseParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhydist_b200.so")
+SEGL = 20
+
+_lib = None
+
+
+class HydError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise HydError("libhydist_b200.so not built (run: make -C gpu-hydist_b200)")
+    lib = ctypes.CDLL(LIB_PATH)
+    H = ctypes.c_void_p
+    sig = {
+        "hyd_last_error": (ctypes.c_char_p, []),
+        "hyd_version": (ctypes.c_char_p, []),
+        "hyd_params_default": (None, [ctypes.POINTER(HydCaseParams)]),
+        "hyd_params_derive": (None, [ctypes.POINTER(HydCaseParams)]),
+        "hyd_create": (ctypes.c_int, [ctypes.POINTER(HydCaseParams), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(H)]),
+        "hyd_destroy": (ctypes.c_int, [H]),
+        "hyd_set_field": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]),
+        "hyd_get_field": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]),
+        "hyd_set_boundary": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_int]),
+        "hyd_init": (ctypes.c_int, [H, ctypes.c_double]),
+        "hyd_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+        "hyd_get_time": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double)]),
+        "hyd_set_params": (ctypes.c_int, [H, ctypes.POINTER(HydCaseParams)]),
+        "hyd_synchronize": (ctypes.c_int, [H]),
+        "hyd_mass_balance": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_int]),
+        "hyd_state_size": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_size_t)]),
+        "hyd_get_state": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_size_t]),
+        "hyd_set_state": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_size_t]),
+        "hyd_launch_count": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_longlong)]),
+        "hyd_get_stream": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_void_p)]),
+        "hyd_device_status": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_uint)]),
+        "hyd_set_timing": (ctypes.c_int, [H, ctypes.c_int]),
+        "hyd_timing_report": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_size_t]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise HydError("hydist error %d: %s" % (rc, _lib.hyd_last_error().decode()))
+
+
+def field_shape(name, N, M):
+    if name in ("daui", "cuoii"):
+        return (N + 2, SEGL), np.int32
+    if name in ("dauj", "cuoij"):
+        return (M + 2, SEGL), np.int32
+    if name == "moci":
+        return (N + 2,), np.int32
+    if name == "mocj":
+        return (M + 2,), np.int32
+    if name in ("ubt", "ubp"):
+        return (M + 2,), np.float64
+    if name in ("vbt", "vbd"):
+        return (N + 2,), np.float64
+    if name == "hi":
+        return (2 * (N + 3) + 2 * (M + 3),), np.float64
+    if name == "hmax":
+        return (4,), np.float64
+    if name == "khouot":
+        return (N + 3, M + 3), np.int32
+    return (N + 3, M + 3), np.float64
+
+
+class Simulation:
+    """One device-resident simulation (a hyd_handle)."""
+
+    def __init__(self, params, N, M, device=0):
+        lib = load()
+        self.lib = lib
+        self.N, self.M = int(N), int(M)
+        self._p = params.copy()
+        h = ctypes.c_void_p()
+        _check(lib.hyd_create(ctypes.byref(self._p), self.N, self.M, int(device), ctypes.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_case(cls, case, device=0, init=True):
+        sim = cls(case.params, case.N, case.M, device)
+        for name in ("h", "hsnham", "VISCOIDX", "Fw", "Tsxw", "Tsyw", "u", "v", "z", "FS"):
+            sim.set(name, case.fields[name])
+        sim.set_boundary(case.boundary_type, case.tables, case.cc, case.total_time)
+        if init:
+            sim.init(case.t_start)
+        return sim
+
+    def set(self, name, arr):
+        shape, dt = field_shape(name, self.N, self.M)
+        a = np.ascontiguousarray(arr, dtype=dt)
+        if a.shape != shape:
+            raise ValueError("%s: expected shape %s, got %s" % (name, shape, a.shape))
+        _check(self.lib.hyd_set_field(self.h, name.encode(), a.ctypes.data, a.size))
+
+    def get(self, name, out=None):
+        shape, dt = field_shape(name, self.N, self.M)
+        a = out if out is not None else np.empty(shape, dtype=dt)
+        _check(self.lib.hyd_get_field(self.h, name.encode(), a.ctypes.data, a.size))
+        return a
+
+    def set_boundary(self, boundary_type, tables, cc, total_time):
+        bt = np.ascontiguousarray(boundary_type, dtype=np.int32)
+        tabs = [np.ascontiguousarray(t, dtype=np.float64) for t in tables]
+        ccs = [np.ascontiguousarray(t, dtype=np.float64) for t in cc]
+        PD = ctypes.POINTER(ctypes.c_double)
+        tp = (PD * 4)(*[t.ctypes.data_as(PD) for t in tabs])
+        cp = (PD * 4)(*[t.ctypes.data_as(PD) for t in ccs])
+        ns = (ctypes.c_int * 4)(*[int(t.shape[0]) for t in tabs])
+        _check(self.lib.hyd_set_boundary(self.h, bt.ctypes.data, tp, cp, ns, int(total_time)))
+
+    def set_params(self, params):
+        self._p = params.copy()
+        _check(self.lib.hyd_set_params(self.h, ctypes.byref(self._p)))
+
+    @property
+    def params(self):
+        return self._p.copy()
+
+    def init(self, t_start=0.0):
+        _check(self.lib.hyd_init(self.h, float(t_start)))
+
+    def step(self, n=1, sync=True):
+        t = ctypes.c_double()
+        _check(self.lib.hyd_step(self.h, int(n), 1 if sync else 0, ctypes.byref(t)))
+        return t.value
+
+    def synchronize(self):
+        _check(self.lib.hyd_synchronize(self.h))
+
+    @property
+    def t(self):
+        t = ctypes.c_double()
+        _check(self.lib.hyd_get_time(self.h, ctypes.byref(t)))
+        return t.value
+
+    def mass_balance(self):
+        out = np.zeros(5)
+        _check(self.lib.hyd_mass_balance(self.h, out.ctypes.data, 5))
+        return {"volume": out[0], "suspended": out[1], "bed_change": out[2], "wet_cells": int(out[3]),
+                "nonfinite": int(out[4])}
+
+    def get_state(self):
+        n = ctypes.c_size_t()
+        _check(self.lib.hyd_state_size(self.h, ctypes.byref(n)))
+        buf = np.zeros(n.value, dtype=np.uint8)
+        _check(self.lib.hyd_get_state(self.h, buf.ctypes.data, buf.size))
+        return buf
+
+    def set_state(self, buf):
+        b = np.ascontiguousarray(buf, dtype=np.uint8)
+        _check(self.lib.hyd_set_state(self.h, b.ctypes.data, b.size))
+
+    def launch_count(self):
+        c = ctypes.c_longlong()
+        _check(self.lib.hyd_launch_count(self.h, ctypes.byref(c)))
+        return c.value
+
+    def device_status(self):
+        st = ctypes.c_uint()
+        _check(self.lib.hyd_device_status(self.h, ctypes.byref(st)))
+        return st.value
+
+    def stream_ptr(self):
+        """The library stream (cudaStream_t as an integer) for torch.cuda.ExternalStream."""
+        p = ctypes.c_void_p()
+        _check(self.lib.hyd_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def set_timing(self, enable):
+        _check(self.lib.hyd_set_timing(self.h, 1 if enable else 0))
+
+    def timing_report(self):
+        buf = ctypes.create_string_buffer(8192)
+        _check(self.lib.hyd_timing_report(self.h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, n, ms = line.split()
+            out[name] = (int(n), float(ms))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hyd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

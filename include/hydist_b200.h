@@ -118,7 +118,8 @@ int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count
  * Copy one field out to the host (any name accepted by hyd_set_field, plus the
  * segment tables "daui","cuoii" (int32, (N+2)*20), "moci" (int32, N+2), "dauj",
  * "cuoij" ((M+2)*20), "mocj" (M+2), and "ubt","ubp" (M+2), "vbt","vbd" (N+2),
- * "hi" (2*(N+3)+2*(M+3))).  Replaces Pointers.extract (Pointers.py:148-154).
+ * "hi" (2*(N+3)+2*(M+3)), "hmax" (4: the edge concentration scales 1/(ros*hmax) of
+ * preprocess_data, up/down/left/right)).  Replaces Pointers.extract (Pointers.py:148-154).
  */
 int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count);
 
@@ -151,6 +152,14 @@ int hyd_init(hyd_handle h, double t_start);
  */
 int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out);
 
+/*
+ * Replace the case parameters between steps (the run options of
+ * Engine.hydraulic_Calculation, e.g. sediment_start, bed_change_start, ketdinh, are
+ * keyword arguments there and may differ per call, Engine.py:49-50).  The grid size
+ * cannot change.
+ */
+int hyd_set_params(hyd_handle h, const HydCaseParams* p);
+
 /* Current simulation time (host mirror). */
 int hyd_get_time(hyd_handle h, double* t);
 
@@ -176,8 +185,27 @@ int hyd_state_size(hyd_handle h, size_t* bytes);
 int hyd_get_state(hyd_handle h, void* buf, size_t bytes);
 int hyd_set_state(hyd_handle h, const void* buf, size_t bytes);
 
-/* Number of kernels this handle has launched since creation (instrumentation). */
+/* Device status bits accumulated since creation (waits for the stream):
+ *   1 = a line had more than 20 wet segments (the reference overflows its tables),
+ *   2 = an edge concentration interpolation index left the grid (skipped),
+ *   4 = a single-cell segment on an open edge was met (the reference solves a
+ *       negative-size system on stale scratch there; this library solves nothing). */
+int hyd_device_status(hyd_handle h, unsigned* status);
+
+/* Number of kernels this library has launched in this process (instrumentation). */
 int hyd_launch_count(hyd_handle h, long long* count);
+
+/* The handle's CUDA stream (a cudaStream_t), so that callers can order their own work
+ * and time the library with events on the stream it launches on. */
+int hyd_get_stream(hyd_handle h, void** stream);
+
+/* Per-phase device timing: while enabled, every phase of the step (boundary, the two
+ * line sweeps, smoothing, explicit momentum, resets, state update, scans, sediment, bed)
+ * is bracketed by CUDA events on the handle's stream.  hyd_timing_report() synchronizes
+ * and writes lines "name launches total_ms\n" into buf (NUL-terminated), then clears the
+ * accumulators. */
+int hyd_set_timing(hyd_handle h, int enable);
+int hyd_timing_report(hyd_handle h, char* buf, size_t buflen);
 
 #ifdef __cplusplus
 }

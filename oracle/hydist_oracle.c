@@ -240,6 +240,15 @@ int ora_set_boundary(OraSim* s, const int* boundary_type, const double* const* t
 
 double ora_time(const OraSim* s) { return s->t; }
 
+void ora_set_time(OraSim* s, double t) { s->t = t; }
+
+void ora_set_hmax(OraSim* s, const double* hmax4) {
+    s->hmax_u = hmax4[0];
+    s->hmax_d = hmax4[1];
+    s->hmax_l = hmax4[2];
+    s->hmax_r = hmax4[3];
+}
+
 /* ------------------------------------------------------- segment lookups */
 
 /* locate_segment_v (constant.cuh:135-154): segment of row `row` holding column `col`.
@@ -545,31 +554,33 @@ static void k_boundary(OraSim* s, double t) {
 }
 
 /* Channel-mode analytic seiche boundaries (support_funcs.cu:356-429, Engine.py:29-43).
- * bienQ is read through a bool* there, i.e. the low byte of bienQ[0]'s int32. */
+ * Engine.py passes m_offset = 5 as the kernels' segment_limit parameter, so the segment
+ * tables are indexed with a stride of 5 there; bienQ is read through a bool*, i.e. byte e
+ * of the int32 array. */
 static void k_boundary_channel(OraSim* s, double t) {
     const int N = s->N, M = s->M, W = s->W;
+    const int sl = 5;
     const double dX = s->P.dX, dY = s->P.dY;
     const unsigned char* bq = (const unsigned char*)s->bienQ;
-    /* up: i from dauj[M][0] .. cuoij[M][0] */
-    for (int i = s->dauj[M * SEGL]; i <= s->cuoij[M * SEGL]; i++) {
+    for (int i = s->dauj[M * sl]; i <= s->cuoij[M * sl] && i < s->dauj[M * sl] + N; i++) {
         s->t_z[i * W + M] = 0.01 * cos(2 * PI_REF / 27.750 * t) * cos(2 * (PI_REF / 100) * (100 - dY / 2));
         s->t_z[i * W + M + 1] = 0.01 * cos(2 * PI_REF / 27.75 * t) * cos(2 * (PI_REF / 100) * (100 + dY / 2));
     }
-    for (int i = s->dauj[2 * SEGL]; i <= s->cuoij[2 * SEGL]; i++) {
+    for (int i = s->dauj[2 * sl]; i <= s->cuoij[2 * sl] && i < s->dauj[2 * sl] + N; i++) {
         if (bq[1]) s->vbd[i] = 0;
         else {
             s->t_z[i * W + 2] = 0.01 * cos(2 * PI_REF / 27.75 * t) * cos(2 * (PI_REF / 100) * dY / 2);
             s->t_z[i * W + 1] = 0.01 * cos(2 * PI_REF / 27.75 * t) * cos(2 * (PI_REF / 100) * (-dY) / 2);
         }
     }
-    for (int i = s->daui[2 * SEGL]; i <= s->cuoii[2 * SEGL]; i++) {
+    for (int i = s->daui[2 * sl]; i <= s->cuoii[2 * sl] && i < s->daui[2 * sl] + M; i++) {
         if (bq[2]) s->ubt[i] = 0;
         else {
             s->t_z[2 * W + i] = 0.01 * cos(2 * PI_REF / 27.75 * t) * cos(2 * (PI_REF / 100) * dX / 2);
             s->t_z[1 * W + i] = 0.01 * cos(2 * PI_REF / 27.75 * t) * cos(2 * (PI_REF / 100) * (-dX) / 2);
         }
     }
-    for (int i = s->daui[2 * SEGL]; i <= s->cuoii[N * SEGL]; i++) {
+    for (int i = s->daui[2 * sl]; i <= s->cuoii[N * sl] && i < s->daui[2 * sl] + M; i++) {
         if (bq[3]) s->ubp[i] = 0;
         else {
             s->t_z[N * W + i] = 0.01 * cos(2 * PI_REF / 27.75 * t) * cos(2 * (PI_REF / 100) * (100 - dX / 2));
@@ -1204,10 +1215,12 @@ static void k_reset_vertical(OraSim* s) {
     }
 }
 
-/* update_uvz (support_funcs.cu:671-680); kenhhepd/ng mask the velocities in channel mode */
+/* update_uvz (support_funcs.cu:671-680).  Engine.py:90 passes two arguments fewer than
+ * the kernel declares, so its kenhhepd/kenhhepng parameters never hold the host's flags
+ * and the velocities are copied unmasked. */
 static void k_update_uvz(OraSim* s) {
     const int N = s->N, M = s->M, o = s->W;
-    const int kd = s->P.kenhhepd, kn = s->P.kenhhepng;
+    const int kd = 0, kn = 0;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i <= N; i++)
         for (int j = 0; j <= M; j++) {

@@ -38,6 +38,9 @@ void ora_init(OraSim* s, double t_start);
 /* Engine.py:144-366, nsteps iterations of the while loop */
 void ora_step(OraSim* s, int nsteps);
 double ora_time(const OraSim* s);
+/* Resume support: set the time and the edge concentration scales (hmax_u, _d, _l, _r). */
+void ora_set_time(OraSim* s, double t);
+void ora_set_hmax(OraSim* s, const double* hmax4);
 void ora_set_threads(int n);
 /* Debug aid: print the first non-finite field value after each phase (stderr). */
 void ora_set_trace(int on);

@@ -45,6 +45,8 @@ def field_shape(name, N, M):
         return (N + 2,), np.float64
     if name == "hi":
         return (2 * (N + 3) + 2 * (M + 3),), np.float64
+    if name == "hmax":
+        return (4,), np.float64
     if name == "khouot":
         return (N + 3, M + 3), np.int32
     return (N + 3, M + 3), np.float64
@@ -86,6 +88,8 @@ class OracleSim:
         lib.ora_set_threads.argtypes = [ctypes.c_int]
         lib.ora_tridiag.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 8
         lib.ora_derived_constants.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.ora_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.ora_set_hmax.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         self.lib = lib
         self.case = case
         self.N, self.M = case.N, case.M
@@ -120,6 +124,18 @@ class OracleSim:
 
     def step(self, n):
         self.lib.ora_step(self.h, int(n))
+
+    STATE_FIELDS = ("u", "v", "z", "t_u", "t_v", "t_z", "Htdu", "Htdv", "H_moi", "htaiz", "htaiz_bd", "Kx1", "Ky1",
+                    "FS", "tFS", "VTH", "Kx", "Ky", "Qbx", "Qby", "dH", "khouot", "daui", "cuoii", "moci", "dauj",
+                    "cuoij", "mocj", "ubt", "ubp", "vbt", "vbd", "hi")
+
+    def load_state(self, get, t, hmax4):
+        """Resume from another implementation's state: `get(name)` returns each field."""
+        for f in self.STATE_FIELDS:
+            self.view(f)[...] = get(f)
+        self.lib.ora_set_time(self.h, float(t))
+        hm = np.ascontiguousarray(hmax4, dtype=np.float64)
+        self.lib.ora_set_hmax(self.h, hm.ctypes.data)
 
     @property
     def t(self):
