@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <utility>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -66,6 +67,8 @@ struct HydSim {
     DevParams dp;
     double* scratch_u;  // smoothing ping-pong partners
     double* scratch_v;
+    double* sweep_scratch;  // rows/cells of lines too long for shared memory
+    SweepPlan plan;         // launch shapes of the sweeps
     void* arena;
     size_t arena_bytes;
     std::vector<void*> extra;
@@ -85,6 +88,12 @@ struct HydSim {
     std::vector<cudaEvent_t> event_pool;
     double phase_ms[32];
     long long phase_n[32];
+    // CUDA graphs of one full step, one per variant (bit 0: sediment in half-step 1,
+    // bit 1: sediment in half-step 2, bit 2: Exner update)
+    int use_graphs;
+    int force_rescan;  // the next step rescans every line (mask or segment tables were set)
+    cudaGraphExec_t graph[8];
+    long long graph_kernels[8];
 };
 
 static const char* kPhaseNames[] = {"boundary", "sweep_uz", "sweep_vz", "smooth", "explicit_v", "explicit_u",
@@ -94,6 +103,20 @@ enum Phase { PH_BOUNDARY, PH_SWEEP_UZ, PH_SWEEP_VZ, PH_SMOOTH, PH_EXPL_V, PH_EXP
              PH_RESET_COLS, PH_POST, PH_SCAN, PH_VTH, PH_FS_J, PH_FS_I, PH_UPDATE_FS, PH_BED, PH_COUNT };
 
 namespace {
+void drop_graphs(HydSim* s) {
+    for (int k = 0; k < 8; k++) {
+        if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
+        s->graph[k] = nullptr;
+    }
+}
+
+int set_clock(HydSim* s, double t) {
+    const double c[3] = {t, t, t};
+    cudaError_t e = cudaMemcpyAsync(s->g.clock, c, sizeof c, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? HYD_OK : fail(HYD_ECUDA, std::string("clock: ") + cudaGetErrorString(e));
+}
+
 cudaEvent_t pool_event(HydSim* s) {
     if (!s->event_pool.empty()) {
         cudaEvent_t e = s->event_pool.back();
@@ -192,6 +215,7 @@ DevParams make_dev_params(const HydCaseParams& P) {
               std::sin(P.huonggio * (kPiRef / 180));
     d.ufr = 0.25 * std::pow((P.Sx - 1) * P.g, 8.0 / 15.0) * std::pow(P.dm, 9.0 / 15.0) * std::pow(P.muy, -1.0 / 15.0);
     d.dxr = P.dm * std::pow(P.g * (P.Sx - 1) / P.muy * P.muy, (1.0 / 3.0));
+    d.dxr_m03 = std::pow(d.dxr, -0.3);
     d.wss = 10 * P.muy / P.dm * (std::sqrt(1 + 0.01 * (P.Sx - 1) * 9.81 * std::pow(P.dm, 3) / std::pow(P.muy, 2)) - 1);
     d.sediment_start = P.sediment_start;
     d.bed_change_start = P.bed_change_start;
@@ -315,6 +339,8 @@ void hyd_params_default(HydCaseParams* p) {
 int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out) {
     if (!p || !out) return fail(HYD_EINVAL, "null argument");
     if (N < 6 || M < 6) return fail(HYD_EINVAL, "grid too small (N, M >= 6)");
+    // a line of the grid is staged in shared memory by several kernels (8 B per cell)
+    if (N > HYD_MAX_LINE || M > HYD_MAX_LINE) return fail(HYD_EINVAL, "grid too large (N, M <= 25000)");
     if (p->dT <= 0 || p->dX <= 0 || p->dY <= 0) return fail(HYD_EINVAL, "dX, dY, dT must be positive");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -335,6 +361,14 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     s->start_idx = 2;
     s->end_idx = N;
     s->timing = 0;
+    {
+        const char* gv = getenv("HYD_GRAPHS");
+        s->use_graphs = !(gv && !strcmp(gv, "0"));
+    }
+    for (int k = 0; k < 8; k++) {
+        s->graph[k] = nullptr;
+        s->graph_kernels[k] = 0;
+    }
     for (int k = 0; k < 32; k++) {
         s->phase_ms[k] = 0;
         s->phase_n[k] = 0;
@@ -353,7 +387,9 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     size_t total = a256(gbytes) * (ngrid + 1 + 2) + a256(nrow * s->pitch * sizeof(int));
     total += 2 * a256(nseg_rows * 4) + a256((N + 3) * 4) + 2 * a256(nseg_cols * 4) + a256((M + 3) * 4);
     total += 2 * a256((M + 3) * 8) + 2 * a256((N + 3) * 8) + a256((2 * (N + 3) + 2 * (M + 3)) * 8);
-    total += a256(4 * 8) + a256(4 * 4) + a256(4 * HYD_SEGL * 4) + a256(64);
+    total += a256(4 * 8) + a256(4 * 4) + a256(4 * HYD_SEGL * 4) + a256(64) + a256(64);
+    total += a256(((N > M ? N : M) + 3) * 4) + a256(64);  // long-line list and counters
+    total += 4 * a256((N + 3) * 4) + 4 * a256((M + 3) * 4) + a256(64);  // spans, rescan flags and lists
     e = cudaMalloc(&s->arena, total);
     if (e != cudaSuccess) {
         cudaStreamDestroy(s->stream);
@@ -396,6 +432,18 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.bienQ = (int*)take(4 * 4);
     g.btype = (int*)take(4 * HYD_SEGL * 4);
     g.status = (unsigned*)take(64);
+    g.long_list = (int*)take(((N > M ? N : M) + 3) * 4);
+    g.long_ctr = (unsigned*)take(64);
+    g.rlo = (int*)take((N + 3) * 4);
+    g.rhi = (int*)take((N + 3) * 4);
+    g.dirty_r = (int*)take((N + 3) * 4);
+    g.dlist_r = (int*)take((N + 3) * 4);
+    g.clo = (int*)take((M + 3) * 4);
+    g.chi = (int*)take((M + 3) * 4);
+    g.dirty_c = (int*)take((M + 3) * 4);
+    g.dlist_c = (int*)take((M + 3) * 4);
+    g.dctr = (unsigned*)take(64);
+    g.clock = (double*)take(64);
     if ((size_t)(cur - (char*)s->arena) > total) {
         cudaFree(s->arena);
         cudaStreamDestroy(s->stream);
@@ -403,6 +451,22 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         return fail(HYD_ENOMEM, "arena layout overflow");
     }
     s->dp = make_dev_params(s->P);
+    e = sweep_plan(N, M, &s->plan);
+    if (e == cudaSuccess) e = grid_setup(N, M);
+    if (e != cudaSuccess) {
+        cudaFree(s->arena);
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return fail(HYD_ECUDA, std::string("shared-memory set-up: ") + cudaGetErrorString(e));
+    }
+    s->sweep_scratch = nullptr;
+    e = cudaMalloc(&s->sweep_scratch, s->plan.scratch_doubles * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(s->arena);
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return fail(HYD_ENOMEM, std::string("sweep scratch: ") + cudaGetErrorString(e));
+    }
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         cudaFree(s->arena);
@@ -424,6 +488,8 @@ int hyd_destroy(hyd_handle h) {
         cudaEventDestroy(m.b);
     }
     for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
+    drop_graphs(h);
+    cudaFree(h->sweep_scratch);
     cudaFree(h->arena);
     cudaStreamDestroy(h->stream);
     delete h;
@@ -445,6 +511,15 @@ int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count
         const size_t es = (f->kind >= 6) ? 8 : 4;
         CUDA_TRY(cudaMemcpyAsync(dst, host, count * es, cudaMemcpyHostToDevice, h->stream));
     }
+    if (dst == (void*)h->g.khouot) {
+        // new mask: new spans, and every line is rescanned at the next step
+        launch_spans(h->g, h->stream);
+        clear_rescan_lists(h->g, h->stream);
+        h->force_rescan = 1;
+    } else if (f->kind >= 2 && f->kind <= 5) {
+        h->force_rescan = 1;  // segment tables
+    }
+    CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return HYD_OK;
 }
@@ -505,6 +580,7 @@ int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const
     }
     h->g.total_time = total_time;
     h->have_boundary = 1;
+    drop_graphs(h);
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return HYD_OK;
 }
@@ -518,73 +594,90 @@ int hyd_init(hyd_handle h, double t_start) {
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->t = t_start;
     h->initialized = 1;
+    h->force_rescan = 0;  // the set-up scanned every line
+    int rc = set_clock(h, t_start);
+    if (rc) return rc;
     return check_device_status(h);
 }
 
-static void half_step_1(HydSim* s, double t) {
+// The launch sequence of one full step (Engine.py:144-366).  sed1/sed2: sediment phase
+// active in the first/second half-step (t >= sediment_start); bed: Exner update at the end.
+static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0) {
     DevGrid& g = s->g;
     const DevParams& p = s->dp;
     cudaStream_t st = s->stream;
-    { PHASE(PH_BOUNDARY); launch_boundary(g, p, t, st); }
+    launch_clock(g, p, st);
+    // ---- half-step 1: implicit along i (columns), explicit v
+    { PHASE(PH_BOUNDARY); launch_boundary(g, p, 0, st); }
     int start_idx = 2, end_idx = s->M;
     if (p.channel && s->P.kenhhepd == 1) {
         start_idx = 3;
         end_idx = s->M - 1;
     }
-    { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, start_idx, end_idx, s->solver, st); }
+    { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_EXPL_V); launch_explicit_v(g, p, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, st); }
     std::swap(g.t_v, s->scratch_v);
-    { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, st); }
+    if (force) launch_mark_all_cols(g, st);
+    { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, st); }
     { PHASE(PH_POST); launch_post(g, p, st); }
-    { PHASE(PH_SCAN); launch_scan_fs_edges(g, p, st); }
-    if (t >= s->P.sediment_start) {
+    { PHASE(PH_SCAN); launch_scan_cols(g, p, st); }
+    if (sed1) {
         { PHASE(PH_VTH); launch_vth_hesok(g, p, st); }
-        { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, t, s->solver, st); }
+        { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, st); }
-        start_idx = 3;
-        end_idx = s->M - 1;
     }
-    s->start_idx = start_idx;
-    s->end_idx = end_idx;
-}
-
-static void half_step_2(HydSim* s, double t) {
-    DevGrid& g = s->g;
-    const DevParams& p = s->dp;
-    cudaStream_t st = s->stream;
-    { PHASE(PH_BOUNDARY); launch_boundary(g, p, t, st); }
-    int start_idx = 2, end_idx = s->N;
+    // ---- half-step 2: implicit along j (rows), explicit u
+    { PHASE(PH_BOUNDARY); launch_boundary(g, p, 1, st); }
+    start_idx = 2;
+    end_idx = s->N;
     if (p.channel && s->P.kenhhepng == 1) {
         start_idx = 3;
         end_idx = s->N;
     }
-    { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, start_idx, end_idx, s->solver, st); }
+    { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, st); }
     std::swap(g.t_v, s->scratch_v);
     { PHASE(PH_EXPL_U); launch_explicit_u(g, p, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, st); }
     std::swap(g.t_u, s->scratch_u);
-    { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, st); }
+    { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, st); }
     { PHASE(PH_POST); launch_post(g, p, st); }
-    { PHASE(PH_SCAN); launch_scan_fs_edges(g, p, st); }
-    if (t >= s->P.sediment_start) {
+    { PHASE(PH_SCAN); launch_scan_rows(g, p, st); }
+    if (sed2) {
         { PHASE(PH_VTH); launch_vth_hesok(g, p, st); }
-        { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, t, s->solver, st); }
+        { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, s->plan, 1, s->solver, s->sweep_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, st); }
         start_idx = 3;
         end_idx = s->N - 1;
     }
-    // Engine.py:364-366: int(t) % bed_change_start == 0 and t integral
-    const double it = (double)(long long)t;
-    if (std::fmod(it, s->P.bed_change_start) == 0 && t - it == 0) {
+    if (bed) {
         PHASE(PH_BED);
         launch_bed(g, p, start_idx, end_idx, st);
     }
     s->start_idx = start_idx;
     s->end_idx = end_idx;
+}
+
+// The captured graph of one step variant (built on first use).
+static cudaGraphExec_t step_graph(HydSim* s, int mask) {
+    if (s->graph[mask]) return s->graph[mask];
+    const long long before = hyd_kernel_launches_add(0);
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return nullptr;
+    launch_step(s, mask & 1, (mask >> 1) & 1, (mask >> 2) & 1);
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamEndCapture(s->stream, &graph) != cudaSuccess || !graph) return nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return nullptr;
+    const long long after = hyd_kernel_launches_add(0);
+    s->graph_kernels[mask] = after - before;
+    hyd_kernel_launches_add(-(after - before));
+    s->graph[mask] = exec;
+    return exec;
 }
 
 int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
@@ -598,10 +691,24 @@ int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
         return fail(HYD_EINVAL, "boundary tables too short for the requested time span");
     double t = h->t;
     for (int n = 0; n < nsteps; n++) {
-        t = t + h->P.dT * 0.5;
-        half_step_1(h, t);
-        t = t + h->P.dT * 0.5;
-        half_step_2(h, t);
+        const double t1 = t + h->P.dT * 0.5;
+        const double t2 = t1 + h->P.dT * 0.5;
+        const int sed1 = t1 >= h->P.sediment_start;
+        const int sed2 = t2 >= h->P.sediment_start;
+        // Engine.py:364: int(t) % bed_change_start == 0 and t integral
+        const double it = (double)(long long)t2;
+        const int bed = std::fmod(it, h->P.bed_change_start) == 0 && t2 - it == 0;
+        const int mask = sed1 | (sed2 << 1) | (bed << 2);
+        const int force = h->force_rescan;
+        h->force_rescan = 0;
+        cudaGraphExec_t exec = (h->use_graphs && !h->timing && !force) ? step_graph(h, mask) : nullptr;
+        if (exec) {
+            CUDA_TRY(cudaGraphLaunch(exec, h->stream));
+            hyd_kernel_launches_add(h->graph_kernels[mask]);
+        } else {
+            launch_step(h, sed1, sed2, bed, force);
+        }
+        t = t2;
     }
     h->t = t;
     CUDA_TRY(cudaGetLastError());
@@ -615,6 +722,7 @@ int hyd_set_params(hyd_handle h, const HydCaseParams* p) {
     if (p->dT <= 0 || p->dX <= 0 || p->dY <= 0) return fail(HYD_EINVAL, "dX, dY, dT must be positive");
     h->P = *p;
     h->dp = make_dev_params(h->P);
+    drop_graphs(h);
     return HYD_OK;
 }
 
@@ -715,6 +823,8 @@ int hyd_set_state(hyd_handle h, const void* buf, size_t bytes) {
     rc = hyd_set_field(h, "VISCOIDX", p, (size_t)(h->N + 3) * (h->M + 3));
     if (rc) return rc;
     h->initialized = 1;
+    rc = set_clock(h, h->t);
+    if (rc) return rc;
     return HYD_OK;
 }
 

@@ -10,6 +10,7 @@
 #include <cstdint>
 
 #define HYD_SEGL 20
+#define HYD_MAX_LINE 25000  // largest N or M (a line is staged in shared memory)
 
 // Device status bits (read back by hyd_synchronize).
 #define HYD_ST_SEG_OVERFLOW 1u     // more than 20 wet segments on a line
@@ -22,6 +23,7 @@ struct DevParams {
         Dorong, Sx, CORIOLIS_FORCE, g, Ks;
     // device helpers of constant.cuh:126-133, evaluated once
     double windx, windy, ufr, dxr, wss;
+    double dxr_m03;  // pow(dxr, -0.3), a constant of the source and bed-load formulas
     double sediment_start, bed_change_start;
     int ketdinh, kenhhepd, kenhhepng, channel;
 };
@@ -42,6 +44,14 @@ struct DevGrid {
     int *bienQ, *btype;                          // bienQ[4], btype[4*20]
     double *bc[4], *cc[4];                       // [nseg][total_time] per edge
     unsigned* status;
+    int* long_list;      // lines listed for the long-line sweep kernels
+    unsigned* long_ctr;  // [0] listed lines, [1] CTAs of the long-line kernel done
+    // span of the cells whose mask is not 2 (those never change) per row / column
+    int *rlo, *rhi, *clo, *chi;
+    // lines whose mask changed since their segments were scanned: flags and lists
+    int *dirty_r, *dirty_c, *dlist_r, *dlist_c;
+    unsigned* dctr;  // [0] listed rows, [1] listed columns, [2] [3] CTAs of the rescans done
+    double* clock;  // [0] time of half-step 1, [1] time of half-step 2, [2] time at the step start
 };
 
 __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { atomicOr(g.status, bit); }
@@ -94,19 +104,40 @@ __device__ __forceinline__ int find_seg_u(const DevGrid& g, int row, int col, in
 // Host launch wrappers (defined in the .cu files, called by hydist_api.cu).
 struct StepLaunch;
 void launch_init_kernels(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_boundary(const DevGrid& g, const DevParams& p, double t, cudaStream_t s);
-void launch_sweep_uz(const DevGrid& g, const DevParams& p, int startidx, int endidx, int solver, cudaStream_t s);
-void launch_sweep_vz(const DevGrid& g, const DevParams& p, int startidx, int endidx, int solver, cudaStream_t s);
+void launch_clock(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
+// Launch shapes of the sweeps for one grid (k_sweep.cu).
+struct SweepPlan {
+    size_t smem_lines, smem_fs_lines;  // line kernels (one warp per line)
+    size_t smem_long, smem_fs_long;    // long-line kernels
+    int RB, CB, RBf;                   // rows / cells of a long line held in shared memory
+    int RG, CG, RGf;                   // rows / cells of a CTA's global scratch region
+    int long_grid;                     // CTAs of the long-line kernels
+    int need_global;                   // some line may exceed shared memory
+    size_t scratch_doubles;            // global scratch to allocate
+};
+cudaError_t sweep_plan(int N, int M, SweepPlan* sp);
+cudaError_t grid_setup(int N, int M);
+void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
+                     int solver, double* scratch, cudaStream_t s);
+void launch_sweep_vz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
+                     int solver, double* scratch, cudaStream_t s);
 void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, cudaStream_t s);
 void launch_explicit_v(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_explicit_u(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_reset_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_reset_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, cudaStream_t s);
+void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, cudaStream_t s);
+void launch_spans(const DevGrid& g, cudaStream_t s);
+void clear_rescan_lists(const DevGrid& g, cudaStream_t s);
+void launch_mark_all_cols(const DevGrid& g, cudaStream_t s);
 void launch_post(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_scan_fs_edges(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, double t, int solver, cudaStream_t s);
-void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, double t, int solver, cudaStream_t s);
+void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
+                       double* scratch, cudaStream_t s);
+void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
+                       double* scratch, cudaStream_t s);
 void launch_update_fs(const DevGrid& g, cudaStream_t s);
 void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, cudaStream_t s);
 long long hyd_kernel_launches_add(long long n);

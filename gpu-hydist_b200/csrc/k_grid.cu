@@ -116,6 +116,19 @@ __global__ void k_preprocess(DevGrid g, DevParams p) {
     g.hmax[3] = hr;
 }
 
+// ------------------------------------------------------------------ step clock
+
+// Advances the device copy of the simulation time by one full step exactly as the host
+// loop does (Engine.py:146,260: t = t + dT * 0.5, twice), so that a captured step can be
+// replayed without baking the time into kernel arguments.
+__global__ void k_clock(DevGrid g, double dT) {
+    const double t1 = g.clock[2] + dT * 0.5;
+    const double t2 = t1 + dT * 0.5;
+    g.clock[0] = t1;
+    g.clock[1] = t2;
+    g.clock[2] = t2;
+}
+
 // --------------------------------------------------------------- boundary values
 
 // Boundary_value + FS_boundary for one edge at index i (support_funcs.cu:544-617)
@@ -144,9 +157,14 @@ __device__ void bnd_edge(const DevGrid& g, int i, double t, int isU, int locatio
     g.FS[ii * P + jj] = cv * g.htaiz_bd[ii * P + jj] * hmax;
 }
 
-// Update_Boundary_Value (support_funcs.cu:622-668); edges in the order up, down, left,
-// right, each completed before the next (the order a converged warp applies them).
-__global__ void k_boundary(DevGrid g, DevParams p, double t) {
+// Update_Boundary_Value (support_funcs.cu:622-668).  Each reference thread i applies the
+// up, down, left and right edges in turn; two edges write the same t_z/FS cell only at the
+// corners (2,M), (N,M), (2,2), (N,2).  The edges run one after another here, and the two
+// corners where a later thread of the reference wins over a later edge are re-applied:
+// (N,2) by the down edge (thread N runs after the right edge's thread 2) and (N,M) by the
+// up edge when N > M.
+__global__ void k_boundary(DevGrid g, DevParams p, int half) {
+    const double t = g.clock[half];
     const int N = g.N, M = g.M;
     const int imax = N > M ? N : M;
     const double* hi_up = g.hi;
@@ -170,6 +188,13 @@ __global__ void k_boundary(DevGrid g, DevParams p, double t) {
         }
         __syncthreads();
     }
+    if (threadIdx.x == 0) {
+        bnd_edge(g, N, t, 0, 2, 1, g.btype + 1 * HYD_SEGL, hi_down, g.vbd, g.bc[1], g.cc[1], g.hmax[1], g.mocj, g.dauj,
+                 g.cuoij);
+        if (N > M)
+            bnd_edge(g, N, t, 0, M, M + 1, g.btype + 0 * HYD_SEGL, hi_up, g.vbt, g.bc[0], g.cc[0], g.hmax[0], g.mocj,
+                     g.dauj, g.cuoij);
+    }
 }
 
 // Channel-mode analytic seiche boundaries (support_funcs.cu:356-429, Engine.py:30-43).
@@ -177,7 +202,8 @@ __global__ void k_boundary(DevGrid g, DevParams p, double t) {
 // tables are read with a stride of 5; bienQ is read through a bool pointer, i.e. byte e
 // of the int32 array.  Each edge covers at most N (up/down) or M (left/right) indices,
 // the extent of the reference's launch.
-__global__ void k_boundary_channel(DevGrid g, DevParams p, double t) {
+__global__ void k_boundary_channel(DevGrid g, DevParams p, int half) {
+    const double t = g.clock[half];
     const int N = g.N, M = g.M, P = g.P;
     const int sl = 5;
     const unsigned char* bq = (const unsigned char*)g.bienQ;
@@ -256,10 +282,25 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
 // solveV/vSolver (UVZSolver_multithread.cu:1055-1071, 727-768) on row i, then
 // update_margin_elem_V (1008-1052) for the same row.
 __global__ void k_explicit_v(DevGrid g, DevParams p) {
+    extern __shared__ double sv[];  // the row's t_v over [k0, k1]
+    __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL];
     const int row = 2 + blockIdx.x;
     const int P = g.P, M = g.M;
     const int nseg = g.moci[row];
+    if (nseg == 0) return;
     const double *u = g.u, *v = g.v, *z = g.z, *t_u = g.t_u, *H = g.H_moi;
+    // cells read or written: two before the first segment to one past the last
+    const int k0 = max(g.daui[row * HYD_SEGL] - 2, 0);
+    const int k1 = min(g.cuoii[row * HYD_SEGL + nseg - 1] + 1, M + 2);
+    for (int j = k0 + threadIdx.x; j <= k1; j += blockDim.x) sv[j - k0] = g.t_v[row * P + j];
+    if ((int)threadIdx.x < nseg) {
+        const int i = row, W = P, k = threadIdx.x;
+        const int first = g.daui[i * HYD_SEGL + k], last = g.cuoii[i * HYD_SEGL + k];
+        const double* h = g.h;
+        s_b1[k] = (first > 2) || ((first == 2) && (fabs((h[i * W + first - 1] + h[(i - 1) * W + first - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
+        s_b2[k] = (last < M) || ((last == M) && (fabs((h[i * W + last] + h[(i - 1) * W + last]) * 0.5 - p.NANGDAY) < kEpsRef));
+    }
+    __syncthreads();
     for (int k = 0; k < nseg; k++) {
         const int first = g.daui[row * HYD_SEGL + k], last = g.cuoii[row * HYD_SEGL + k];
         if (first >= last) continue;
@@ -293,22 +334,23 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
             q = (q - p.g * (z[row * o + col + 1] - z[row * o + col]) / p.dY +
                  g.VISC[row * o + col] * (tmp + (v[row * o + col + 1] - 2 * v[row * o + col] + v[row * o + col - 1]) / p.dYbp)) +
                 (p.windy - g.Tsyw[row * o + col]) / g.Htdv[row * o + col];
-            g.t_v[row * o + col] = q / pp;
+            const double tv = q / pp;
+            g.t_v[row * o + col] = tv;
+            sv[col - k0] = tv;
         }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double* t_v = g.t_v;
-        const double* h = g.h;
-        const int i = row, W = P;
+        // segment ends in order, on the staged row (update_margin_elem_V)
+        double* t_v = g.t_v + row * P;
         for (int k = 0; k < nseg; k++) {
-            const int first = g.daui[i * HYD_SEGL + k], last = g.cuoii[i * HYD_SEGL + k];
-            const bool b1 = (first > 2) || ((first == 2) && (fabs((h[i * W + first - 1] + h[(i - 1) * W + first - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
-            const bool b2 = (last < M) || ((last == M) && (fabs((h[i * W + last] + h[(i - 1) * W + last]) * 0.5 - p.NANGDAY) < kEpsRef));
-            if (b1) t_v[i * W + first - 1] = 0;
-            else t_v[i * W + first - 1] = 2 * t_v[i * W + first] - t_v[i * W + first + 1];
-            if (b2) t_v[i * W + last] = 0;
-            else t_v[i * W + last] = 2 * t_v[i * W + last - 1] - t_v[i * W + last - 2];
+            const int first = g.daui[row * HYD_SEGL + k], last = g.cuoii[row * HYD_SEGL + k];
+            const double a = s_b1[k] ? 0.0 : 2 * sv[first - k0] - sv[first + 1 - k0];
+            sv[first - 1 - k0] = a;
+            t_v[first - 1] = a;
+            const double b = s_b2[k] ? 0.0 : 2 * sv[last - 1 - k0] - sv[last - 2 - k0];
+            sv[last - k0] = b;
+            t_v[last] = b;
         }
     }
 }
@@ -316,10 +358,24 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
 // solveU/uSolver (UVZSolver_multithread.cu:947-968, 773-815) on column j, then
 // update_margin_elem_U (970-1006).
 __global__ void k_explicit_u(DevGrid g, DevParams p) {
+    extern __shared__ double su[];  // the column's t_u over [k0, k1]
+    __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL];
     const int col = 2 + blockIdx.x;
     const int P = g.P, N = g.N;
     const int nseg = g.mocj[col];
+    if (nseg == 0) return;
     const double *u = g.u, *v = g.v, *z = g.z, *t_v = g.t_v, *H = g.H_moi;
+    const int k0 = max(g.dauj[col * HYD_SEGL] - 2, 0);
+    const int k1 = min(g.cuoij[col * HYD_SEGL + nseg - 1] + 1, N + 2);
+    for (int i = k0 + threadIdx.x; i <= k1; i += blockDim.x) su[i - k0] = g.t_u[i * P + col];
+    if ((int)threadIdx.x < nseg) {
+        const int j = col, W = P, k = threadIdx.x;
+        const int first = g.dauj[j * HYD_SEGL + k], last = g.cuoij[j * HYD_SEGL + k];
+        const double* h = g.h;
+        s_b1[k] = (first > 2) || ((first == 2) && ((fabs(h[1 * W + j] + h[1 * W + j - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
+        s_b2[k] = (last < N) || ((last == N) && (fabs((h[N * W + j] + h[N * W + j - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
+    }
+    __syncthreads();
     for (int k = 0; k < nseg; k++) {
         const int first = g.dauj[col * HYD_SEGL + k], last = g.cuoij[col * HYD_SEGL + k];
         for (int row = first + threadIdx.x; row < last; row += blockDim.x) {
@@ -352,76 +408,183 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
             q = (q - p.g * (z[(row + 1) * o + col] - z[row * o + col]) / p.dX +
                  g.VISC[row * o + col] * (tmp + (u[(row + 1) * o + col] - 2 * u[row * o + col] + u[(row - 1) * o + col]) / p.dXbp)) +
                 (p.windx - g.Tsxw[row * o + col]) / g.Htdu[row * o + col];
-            g.t_u[row * o + col] = q / pp;
+            const double tu = q / pp;
+            g.t_u[row * o + col] = tu;
+            su[row - k0] = tu;
         }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double* t_u = g.t_u;
-        const double* h = g.h;
-        const int j = col, W = P;
+        // segment ends in order, on the staged column (update_margin_elem_U)
         for (int k = 0; k < nseg; k++) {
-            const int first = g.dauj[j * HYD_SEGL + k], last = g.cuoij[j * HYD_SEGL + k];
-            const bool b1 = (first > 2) || ((first == 2) && ((fabs(h[1 * W + j] + h[1 * W + j - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
-            const bool b2 = (last < N) || ((last == N) && (fabs((h[N * W + j] + h[N * W + j - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
-            if (b1) t_u[(first - 1) * W + j] = 0;
-            else t_u[(first - 1) * W + j] = 2 * t_u[first * W + j] - t_u[(first + 1) * W + j];
-            if (b2) t_u[last * W + j] = 0;
-            else t_u[last * W + j] = 2 * t_u[(last - 1) * W + j] - t_u[(last - 2) * W + j];
+            const int first = g.dauj[col * HYD_SEGL + k], last = g.cuoij[col * HYD_SEGL + k];
+            const double a = s_b1[k] ? 0.0 : 2 * su[first - k0] - su[first + 1 - k0];
+            su[first - 1 - k0] = a;
+            g.t_u[(first - 1) * P + col] = a;
+            const double b = s_b2[k] ? 0.0 : 2 * su[last - 1 - k0] - su[last - 2 - k0];
+            su[last - k0] = b;
+            g.t_u[last * P + col] = b;
         }
     }
 }
 
 // --------------------------------------------------------------- wet/dry resets
 
+// Mark line `line` of the other direction for a segment rescan (once).
+__device__ __forceinline__ void mark_dirty(int* flags, int* list, unsigned* ctr, int line) {
+    if (atomicExch(&flags[line], 1) == 0) list[atomicAdd(ctr, 1u)] = line;
+}
+
+// Wet-segment scan of one line by one warp (Find_Calculation_limits_Horizontal/Vertical,
+// support_funcs.cu:230-335).  The serial while-loop there yields the maximal runs of
+// khouot == 0 within [2, L] in order, except runs starting at L-1 or L, which it skips.
+// Cells a..b are tested with wet(k); every other cell is dry.  The warp packs the wet
+// flags into 32-cell words (words: (b - a) / 32 + 2 entries of shared memory), then
+// lane 0 walks the run starts and ends word by word.
+template <class Wet>
+__device__ void warp_scan_line(const DevGrid& g, Wet wet, int a, int b, int L, unsigned* words, int* dau, int* cuoi,
+                               int* moc) {
+    const int lane = threadIdx.x & 31;
+    if (a < 2) a = 2;
+    if (b > L) b = L;
+    const int w0 = (a - 2) >> 5, w1 = (b - 2) >> 5;
+    for (int w = w0; w <= w1; w++) {
+        const int k = 2 + 32 * w + lane;
+        const bool z = (k >= a && k <= b) ? wet(k) : false;
+        const unsigned bits = __ballot_sync(0xffffffffu, z);
+        if (lane == 0) words[w - w0] = bits;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        int nseg = 0;
+        int open_start = -1;
+        for (int w = w0; w <= w1; w++) {
+            const unsigned cur = words[w - w0];
+            const unsigned prev = w > w0 ? words[w - w0 - 1] : 0u;
+            const unsigned next = w < w1 ? words[w - w0 + 1] : 0u;
+            unsigned starts = cur & ~((cur << 1) | (prev >> 31));
+            unsigned ends = cur & ~((cur >> 1) | (next << 31));
+            const int c0 = 2 + 32 * w;
+            // events in position order; a run's start precedes or equals its end
+            while (starts | ends) {
+                if (open_start < 0) {
+                    if (!starts) break;
+                    open_start = c0 + __ffs(starts) - 1;
+                    starts &= starts - 1;
+                } else {
+                    if (!ends) break;  // the run continues into the next word
+                    const int e = c0 + __ffs(ends) - 1;
+                    ends &= ends - 1;
+                    if (open_start <= L - 2) {
+                        if (nseg < HYD_SEGL) {
+                            dau[nseg] = open_start;
+                            cuoi[nseg] = e;
+                        } else {
+                            flag_status(g, HYD_ST_SEG_OVERFLOW);
+                        }
+                        nseg++;
+                    }
+                    open_start = -1;
+                }
+            }
+        }
+        *moc = nseg < HYD_SEGL ? nseg : HYD_SEGL;
+    }
+    __syncwarp();
+}
+
+struct WetShared {  // staged mask: cell k at kh[k - k0]
+    const signed char* kh;
+    int k0;
+    __device__ bool operator()(int k) const { return kh[k - k0] == 0; }
+};
+
+struct WetGlobal {  // mask in HBM: cell k at kh[base + k * along]
+    const int* kh;
+    int base, along;
+    __device__ bool operator()(int k) const { return kh[base + k * along] == 0; }
+};
+
 // update_h_moi (support_funcs.cu:60-73) and Reset_states_horizontal/_vertical
 // (support_funcs.cu:75-186) for one line.  ROWS: line = row i (1..N), cells j (2..M);
-// otherwise line = column j (1..M), cells i (2..N).  The opening pass is a serial
-// scan in the reference; an iteration can only act next to a cell whose mask is 1
-// at the start of the pass, so warp 0 ballots those candidates and lane 0 runs them
-// in increasing order.
+// otherwise line = column j (1..M), cells i (2..N).
+// Cells whose mask is 2 never change (only 0 <-> 1 transitions exist), so each line is
+// staged in shared memory over its span [lo, hi] of cells that are not 2, widened by one
+// cell: nothing outside can act or be acted on.  The opening pass is a serial scan in the
+// reference; an iteration can only act next to a cell whose mask is 1 at the start of the
+// pass, so warp 0 ballots those candidates and lane 0 runs them in increasing order.
+// A line only changes its own cells, so its segments are rescanned here when a cell
+// changed (or when `force`); every changed cell marks its line of the other direction
+// for the rescan that follows.
 template <int ROWS>
-__global__ void k_reset(DevGrid g, DevParams p) {
+__global__ void k_reset(DevGrid g, DevParams p, int force) {
+    extern __shared__ unsigned char rsm[];
+    __shared__ int s_changed;
     const int line = 1 + blockIdx.x;
     const int P = g.P;
-    const int L = ROWS ? g.M : g.N;           // last cell index of the line
+    const int L = ROWS ? g.M : g.N;  // last cell index of the line
     const int along = ROWS ? 1 : P;
     const int base = ROWS ? line * P : line;
+    const int lo = ROWS ? g.rlo[line] : g.clo[line];
+    const int hi = ROWS ? g.rhi[line] : g.chi[line];
+    int* dau = ROWS ? g.daui + line * HYD_SEGL : g.dauj + line * HYD_SEGL;
+    int* cuoi = ROWS ? g.cuoii + line * HYD_SEGL : g.cuoij + line * HYD_SEGL;
+    int* moc = ROWS ? g.moci + line : g.mocj + line;
+    if (hi < lo) {  // no cell of the line can ever be wet
+        if (force && line >= 2 && threadIdx.x == 0) *moc = 0;
+        return;
+    }
+    int* oflags = ROWS ? g.dirty_c : g.dirty_r;
+    int* olist = ROWS ? g.dlist_c : g.dlist_r;
+    unsigned* octr = g.dctr + (ROWS ? 1 : 0);
+    const int k0 = lo - 1 > 0 ? lo - 1 : 0;
+    const int k1 = hi + 1 < L + 2 ? hi + 1 : L + 2;
+    signed char* khs = (signed char*)rsm;                       // khs[k - k0], k in [k0, k1]
+    unsigned* words = (unsigned*)(rsm + ((L + 3 + 15) & ~15));  // scan words
+    auto khv = [&](int k) -> int { return (k >= k0 && k <= k1) ? khs[k - k0] : 2; };
     double *H = g.H_moi, *t_z = g.t_z, *FS = g.FS;
     int* kh = g.khouot;
-    // update_h_moi for this line (cells 1..L)
-    for (int k = 1 + threadIdx.x; k <= L; k += blockDim.x) {
+    if (threadIdx.x == 0) s_changed = 0;
+    for (int k = k0 + threadIdx.x; k <= k1; k += blockDim.x) {
         const int gp = base + k * along;
-        if (kh[gp] == 0) H[gp] = g.htaiz[gp] + t_z[gp];
+        const int kv = kh[gp];
+        khs[k - k0] = (signed char)kv;
+        if (k >= 1 && k <= L && kv == 0) H[gp] = g.htaiz[gp] + t_z[gp];
     }
     __syncthreads();
     // opening pass (loop 1)
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
-        for (int c0 = 2; c0 <= L; c0 += 32) {
+        const int ka = k0 > 2 ? k0 : 2, kb = k1 < L ? k1 : L;
+        for (int c0 = ka; c0 <= kb; c0 += 32) {
             const int k = c0 + lane;
-            bool cand = false;
-            if (k <= L) cand = (kh[base + (k - 1) * along] == 1) || (kh[base + (k + 1) * along] == 1);
+            const bool cand = (k <= kb) && (khv(k - 1) == 1 || khv(k + 1) == 1);
             unsigned mask = __ballot_sync(0xffffffffu, cand);
             if (lane == 0) {
                 while (mask) {
-                    const int b = __ffs(mask) - 1;
+                    const int kk = c0 + __ffs(mask) - 1;
                     mask &= mask - 1;
-                    const int kk = c0 + b;
                     const int gp = base + kk * along;
                     if (t_z[gp] > g.z[gp]) {
-                        const int gm = gp - along, gq = gp + along;
-                        if (kh[gm] == 1) {
+                        if (khv(kk - 1) == 1) {
+                            const int gm = gp - along;
                             t_z[gm] = t_z[gp];
                             H[gm] = g.htaiz[gm] + t_z[gp];
                             kh[gm] = 0;
+                            khs[kk - 1 - k0] = 0;
                             FS[gm] = FS[gp];
+                            s_changed = 1;
+                            mark_dirty(oflags, olist, octr, kk - 1);
                         }
-                        if (kh[gq] == 1) {
+                        if (khv(kk + 1) == 1) {
+                            const int gq = gp + along;
                             t_z[gq] = t_z[gp];
                             H[gq] = g.htaiz[gq] + t_z[gp];
                             kh[gq] = 0;
+                            khs[kk + 1 - k0] = 0;
                             FS[gq] = FS[gp];
+                            s_changed = 1;
+                            mark_dirty(oflags, olist, octr, kk + 1);
                         }
                     }
                 }
@@ -431,17 +594,52 @@ __global__ void k_reset(DevGrid g, DevParams p) {
     }
     __syncthreads();
     // closing pass (loop 2): independent per cell
-    for (int k = 2 + threadIdx.x; k <= L; k += blockDim.x) {
+    const int ca = lo > 2 ? lo : 2, cb = hi < L ? hi : L;
+    for (int k = ca + threadIdx.x; k <= cb; k += blockDim.x) {
         const int gp = base + k * along;
-        if (kh[gp] == 0 && H[gp] <= p.H_TINH) {
+        if (khs[k - k0] == 0 && H[gp] <= p.H_TINH) {
             g.t_u[gp - P] = 0;
             g.t_u[gp] = 0;
             g.t_v[gp - 1] = 0;
             g.t_v[gp] = 0;
             kh[gp] = 1;
+            khs[k - k0] = 1;
             FS[gp] = 0;
+            s_changed = 1;
+            mark_dirty(oflags, olist, octr, k);
         }
     }
+    __syncthreads();
+    if (threadIdx.x < 32 && line >= 2 && (s_changed || force))
+        warp_scan_line(g, WetShared{khs, k0}, lo, hi, L, words, dau, cuoi, moc);
+}
+
+// Spans of the cells whose mask is not 2: rows [rlo, rhi], columns [clo, chi] (the
+// bounds start at INT_MAX / -1).
+__global__ void k_spans(DevGrid g) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.N + 2 || j > g.M + 2) return;
+    if (g.khouot[i * g.P + j] != 2) {
+        atomicMin(&g.rlo[i], j);
+        atomicMax(&g.rhi[i], j);
+        atomicMin(&g.clo[j], i);
+        atomicMax(&g.chi[j], i);
+    }
+}
+
+// List every row (ROWS) or column of the grid for a segment rescan.
+template <int ROWS>
+__global__ void k_mark_all(DevGrid g) {
+    const int n = ROWS ? g.N + 3 : g.M + 3;
+    int* flags = ROWS ? g.dirty_r : g.dirty_c;
+    int* list = ROWS ? g.dlist_r : g.dlist_c;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        flags[k] = 1;
+        list[k] = k;
+    }
+    if (k == 0) g.dctr[ROWS ? 0 : 1] = n;
 }
 
 // --------------------------------------------------- state update and face depths
@@ -472,80 +670,55 @@ __global__ void k_post(DevGrid g, int with_uvz) {
 
 // ------------------------------------------------------------- wet-segment scans
 
-// Find_Calculation_limits_Horizontal/Vertical (support_funcs.cu:230-335).  The serial
-// while-loop there yields the maximal runs of khouot == 0 within [2, L] in order,
-// except runs starting at L-1 or L, which it skips; one warp per line finds the run
-// starts and ends with ballots.  Blocks [0, N-1) scan rows 2..N, the rest columns 2..M.
-__global__ void k_scan(DevGrid g) {
-    const int lane = threadIdx.x;
-    const int N = g.N, M = g.M, P = g.P;
-    int line, L, along, base;
-    int *dau, *cuoi, *moc;
-    if ((int)blockIdx.x < N - 1) {
-        line = 2 + blockIdx.x;
-        L = M;
-        along = 1;
-        base = line * P;
-        dau = g.daui + line * HYD_SEGL;
-        cuoi = g.cuoii + line * HYD_SEGL;
-        moc = g.moci + line;
+__device__ void fs_edges_block(const DevGrid& g, const DevParams& p);
+
+// Rescan of the listed rows (ROWS) or columns: a line is listed when one of its cells
+// changed since its segments were last scanned, and a line whose mask did not change
+// keeps segments equal to a fresh scan.  Warp w of the scanning CTAs takes listed lines
+// w, w + W, ...; CTA `edges` (or none, -1) runs the edge concentration interpolation of
+// the same reference kernels.  The last CTA to finish empties the list.
+template <int ROWS>
+__global__ void k_scan_dirty(DevGrid g, DevParams p, int edges) {
+    extern __shared__ unsigned swords[];
+    if ((int)blockIdx.x == edges) {
+        fs_edges_block(g, p);
     } else {
-        line = 2 + (blockIdx.x - (N - 1));
-        L = N;
-        along = P;
-        base = line;
-        dau = g.dauj + line * HYD_SEGL;
-        cuoi = g.cuoij + line * HYD_SEGL;
-        moc = g.mocj + line;
-    }
-    const int* kh = g.khouot;
-    int nseg = 0;       // uniform across the warp
-    int open_start = -1;
-    for (int c0 = 2; c0 <= L; c0 += 32) {
-        const int k = c0 + lane;
-        bool isz = false, prevz = false, nextz = false;
-        if (k <= L) {
-            isz = kh[base + k * along] == 0;
-            prevz = (k > 2) && kh[base + (k - 1) * along] == 0;
-            nextz = (k < L) && kh[base + (k + 1) * along] == 0;
-        }
-        unsigned starts = __ballot_sync(0xffffffffu, isz && !prevz);
-        unsigned ends = __ballot_sync(0xffffffffu, isz && !nextz);
-        // walk events in position order; a run's start precedes or equals its end
-        while (starts | ends) {
-            const int bs = starts ? __ffs(starts) - 1 : 64;
-            const int be = ends ? __ffs(ends) - 1 : 64;
-            if (open_start < 0) {
-                // next event must be a start
-                if (!starts) break;
-                open_start = c0 + bs;
-                starts &= starts - 1;
-            } else {
-                if (!ends) break;  // the run continues into the next chunk
-                const int e = c0 + be;
-                ends &= ends - 1;
-                if (open_start <= L - 2) {
-                    if (nseg < HYD_SEGL) {
-                        if (lane == 0) {
-                            dau[nseg] = open_start;
-                            cuoi[nseg] = e;
-                        }
-                    } else if (lane == 0) {
-                        flag_status(g, HYD_ST_SEG_OVERFLOW);
-                    }
-                    nseg++;
-                }
-                open_start = -1;
-            }
+        const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int scanning = gridDim.x - (edges >= 0 ? 1 : 0);
+        const int n = *(volatile unsigned*)&g.dctr[ROWS ? 0 : 1];
+        const int L = ROWS ? g.M : g.N;
+        const int Lines = ROWS ? g.N : g.M;
+        const int nwords = (L + 63) / 32 + 1;
+        unsigned* words = swords + warp * nwords;
+        int* flags = ROWS ? g.dirty_r : g.dirty_c;
+        const int* list = ROWS ? g.dlist_r : g.dlist_c;
+        for (int k = blockIdx.x * warps + warp; k < n; k += scanning * warps) {
+            const int line = list[k];
+            if (lane == 0) flags[line] = 0;
+            if (line < 2 || line > Lines) continue;
+            const int lo = ROWS ? g.rlo[line] : g.clo[line];
+            const int hi = ROWS ? g.rhi[line] : g.chi[line];
+            const WetGlobal wet{g.khouot, ROWS ? line * g.P : line, ROWS ? 1 : g.P};
+            if (ROWS) warp_scan_line(g, wet, lo, hi, L, words, g.daui + line * HYD_SEGL, g.cuoii + line * HYD_SEGL, g.moci + line);
+            else warp_scan_line(g, wet, lo, hi, L, words, g.dauj + line * HYD_SEGL, g.cuoij + line * HYD_SEGL, g.mocj + line);
         }
     }
-    if (lane == 0) *moc = nseg < HYD_SEGL ? nseg : HYD_SEGL;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned* done = &g.dctr[ROWS ? 2 : 3];
+        if (atomicAdd(done, 1u) == gridDim.x - 1) {
+            g.dctr[ROWS ? 0 : 1] = 0;
+            *done = 0;
+            __threadfence();
+        }
+    }
 }
 
 // Interpolate_FS_ng / Interpolate_FS_d (support_funcs.cu:189-229), run by the row-2,
 // row-N and column-M blocks of the scans in the reference.  Rows first (row 2, then
 // row N), then the column.
-__global__ void k_fs_edges(DevGrid g, DevParams p) {
+__device__ void fs_edges_block(const DevGrid& g, const DevParams& p) {
     const int N = g.N, M = g.M, P = g.P;
     const int i_dX = __double2int_rn(p.dX);
     const int j_dY = __double2int_rn(p.dY);
@@ -635,9 +808,9 @@ __global__ void k_qb(DevGrid g, DevParams p) {
         Tob = p.ro * g.Fw[pos] * (g.VTH[pos] * g.VTH[pos]);
         if (g.H_moi[pos] > p.ghtoe) Toee = p.Toe * (1 + p.hstoe * ((g.H_moi[pos] - p.ghtoe)));
         if (Tob > Toee) Tx = Tob / Toee - 1;
-        qx = 0.053 * pow((p.Sx - 1) * p.g, 0.5) * pow(p.dm, 1.5) * pow(Tx, 2.1) * pow(p.dxr, -0.3) *
+        qx = 0.053 * pow((p.Sx - 1) * p.g, 0.5) * pow(p.dm, 1.5) * pow(Tx, 2.1) * p.dxr_m03 *
              (g.t_u[pos] + g.t_u[pos - P]) * 0.5 / g.VTH[pos];
-        qy = 0.053 * pow((p.Sx - 1) * p.g, 0.5) * pow(p.dm, 1.5) * pow(Tx, 2.1) * pow(p.dxr, -0.3) *
+        qy = 0.053 * pow((p.Sx - 1) * p.g, 0.5) * pow(p.dm, 1.5) * pow(Tx, 2.1) * p.dxr_m03 *
              (g.t_v[pos] + g.t_v[pos - 1]) * 0.5 / g.VTH[pos];
     }
     double *Qbx = g.Qbx, *Qby = g.Qby;
@@ -737,14 +910,15 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
     tH = tH + pp;
     const double c = 18 * log(12 * g.H_moi[pos] / p.Ks);
     const double Uf = sqrt(p.g) * fabs(g.VTH[pos]) / c;
-    const double wsm = p.wss * pow((1 - FS[pos]), 4);
+    const double fq = 1 - FS[pos];
+    const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
     double Zf = 0, S = 0;
     if (FS[pos] > 0.0) Zf = wsm / (0.4 * (Uf + 2 * wsm));
     if (p.ketdinh) S = source_chs_g(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], g.H_moi[pos]);
     else {
         const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
         const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
-        const double Cac = 0.015 * p.dm * pow(Tx, 1.5) * pow(p.dxr, (-0.3)) / (0.05 * g.H_moi[pos]);
+        const double Cac = 0.015 * p.dm * pow(Tx, 1.5) * p.dxr_m03 / (0.05 * g.H_moi[pos]);
         S = wsm * (Cac - gamac * FS[pos]);
     }
     g.dH[pos] += p.dT / (1 - p.Dorong) * (S + tH);
@@ -754,19 +928,100 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
 
 // ------------------------------------------------------------------ host wrappers
 
+namespace {
+constexpr int kScanThreads = 256;
+size_t scan_smem(const DevGrid& g) {
+    const int L = g.N > g.M ? g.N : g.M;
+    return sizeof(unsigned) * (kScanThreads / 32) * ((L + 63) / 32 + 1);
+}
+size_t reset_smem(int L) { return ((L + 3 + 15) & ~15) + sizeof(unsigned) * ((L + 63) / 32 + 1); }
+int scan_grid() {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (nsm < 1) nsm = 1;
+    }
+    return nsm;
+}
+void scan_dirty(const DevGrid& g, const DevParams& p, int rows, int with_edges, cudaStream_t s) {
+    const int nb = scan_grid();
+    const int edges = with_edges ? nb : -1;
+    if (rows) k_scan_dirty<1><<<nb + (with_edges ? 1 : 0), kScanThreads, scan_smem(g), s>>>(g, p, edges);
+    else k_scan_dirty<0><<<nb + (with_edges ? 1 : 0), kScanThreads, scan_smem(g), s>>>(g, p, edges);
+}
+}  // namespace
+
+// Allow `f` `bytes` of dynamic shared memory on the current device.
+cudaError_t allow_smem(const void* f, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Opt the kernels that stage a line in shared memory into the dynamic shared memory
+// this grid needs.
+cudaError_t grid_setup(int N, int M) {
+    DevGrid g{};
+    g.N = N;
+    g.M = M;
+    cudaError_t e;
+    if ((e = allow_smem((const void*)k_scan_dirty<1>, scan_smem(g))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_scan_dirty<0>, scan_smem(g))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_u, sizeof(double) * (N + 3))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_v, sizeof(double) * (M + 3))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_reset<1>, reset_smem(M))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_reset<0>, reset_smem(N))) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+// Spans of the never-dry-forever cells of every line, from the current mask.
+void launch_spans(const DevGrid& g, cudaStream_t s) {
+    cudaMemsetAsync(g.rlo, 0x7f, sizeof(int) * (g.N + 3), s);
+    cudaMemsetAsync(g.rhi, 0xff, sizeof(int) * (g.N + 3), s);
+    cudaMemsetAsync(g.clo, 0x7f, sizeof(int) * (g.M + 3), s);
+    cudaMemsetAsync(g.chi, 0xff, sizeof(int) * (g.M + 3), s);
+    const dim3 b(32, 8);
+    k_spans<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g);
+    hyd_kernel_launches_add(1);
+}
+
+// Empty the rescan lists.
+void clear_rescan_lists(const DevGrid& g, cudaStream_t s) {
+    cudaMemsetAsync(g.dirty_r, 0, sizeof(int) * (g.N + 3), s);
+    cudaMemsetAsync(g.dirty_c, 0, sizeof(int) * (g.M + 3), s);
+    cudaMemsetAsync(g.dctr, 0, 4 * sizeof(unsigned), s);
+}
+
+// List every column for the rescan after the next row resets.
+void launch_mark_all_cols(const DevGrid& g, cudaStream_t s) {
+    k_mark_all<0><<<(g.M + 3 + 255) / 256, 256, 0, s>>>(g);
+    hyd_kernel_launches_add(1);
+}
+
 void launch_init_kernels(const DevGrid& g, const DevParams& p, cudaStream_t s) {
     const dim3 b(32, 8);
     k_onetime_init<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p);
-    k_fs_edges<<<1, 512, 0, s>>>(g, p);
-    k_scan<<<(g.N - 1) + (g.M - 1), 32, 0, s>>>(g);
+    hyd_kernel_launches_add(1);
+    launch_spans(g, s);
+    clear_rescan_lists(g, s);
+    k_mark_all<1><<<(g.N + 3 + 255) / 256, 256, 0, s>>>(g);
+    k_mark_all<0><<<(g.M + 3 + 255) / 256, 256, 0, s>>>(g);
+    scan_dirty(g, p, 1, 1, s);
+    scan_dirty(g, p, 0, 0, s);
     k_post<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, 0);
     k_preprocess<<<1, 32, 0, s>>>(g, p);
-    hyd_kernel_launches_add(5);
+    hyd_kernel_launches_add(6);
 }
 
-void launch_boundary(const DevGrid& g, const DevParams& p, double t, cudaStream_t s) {
-    if (p.channel) k_boundary_channel<<<1, 256, 0, s>>>(g, p, t);
-    else k_boundary<<<1, 1024, 0, s>>>(g, p, t);
+void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s) {
+    if (p.channel) k_boundary_channel<<<1, 256, 0, s>>>(g, p, half);
+    else k_boundary<<<1, 1024, 0, s>>>(g, p, half);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_clock(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+    k_clock<<<1, 1, 0, s>>>(g, p.dT);
     hyd_kernel_launches_add(1);
 }
 
@@ -777,22 +1032,22 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, c
 }
 
 void launch_explicit_v(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_explicit_v<<<g.N - 1, 128, 0, s>>>(g, p);
+    k_explicit_v<<<g.N - 1, 128, sizeof(double) * (g.M + 3), s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
 void launch_explicit_u(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_explicit_u<<<g.M - 1, 128, 0, s>>>(g, p);
+    k_explicit_u<<<g.M - 1, 128, sizeof(double) * (g.N + 3), s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
-void launch_reset_rows(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_reset<1><<<g.N, 128, 0, s>>>(g, p);
+void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, cudaStream_t s) {
+    k_reset<1><<<g.N, 128, reset_smem(g.M), s>>>(g, p, force);
     hyd_kernel_launches_add(1);
 }
 
-void launch_reset_cols(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_reset<0><<<g.M, 128, 0, s>>>(g, p);
+void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, cudaStream_t s) {
+    k_reset<0><<<g.M, 128, reset_smem(g.N), s>>>(g, p, force);
     hyd_kernel_launches_add(1);
 }
 
@@ -802,10 +1057,16 @@ void launch_post(const DevGrid& g, const DevParams& p, cudaStream_t s) {
     hyd_kernel_launches_add(1);
 }
 
-void launch_scan_fs_edges(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_fs_edges<<<1, 512, 0, s>>>(g, p);
-    k_scan<<<(g.N - 1) + (g.M - 1), 32, 0, s>>>(g);
-    hyd_kernel_launches_add(2);
+// After the row resets the changed columns are rescanned (and vice versa); the same
+// launch carries the edge concentration interpolation.
+void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+    scan_dirty(g, p, 0, 1, s);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+    scan_dirty(g, p, 1, 1, s);
+    hyd_kernel_launches_add(1);
 }
 
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, cudaStream_t s) {

@@ -1,21 +1,27 @@
 // k_sweep.cu — fused implicit line sweeps of the ADI step.
 //
-// One CTA per grid line does what the reference spreads over five kernels and global
-// scratch (UZSolver_calculate_preindex/_abcd/_matrix_coeff, tridiagSolver,
-// UZSolver_extract_solution, UVZSolver_multithread.cu:881-943 and the VZ twins
-// 818-879; Scan_FS*/tridiagSolver/FS*_extract_solution, Sediment_Transport.cu:570-617):
-//   A  continuity coefficients a2, c2, d2 of every wet cell            -> shared memory
-//   B  momentum coefficients and the interleaved tridiagonal rows       -> shared memory
-//   C  the line's tridiagonal system, solved in shared memory by a
-//      partitioned method: each thread eliminates its chunk of rows,
-//      the 2T interface unknowns are solved by parallel cyclic reduction,
-//      and each thread substitutes back into its chunk (replaces the
-//      reference's serial Thomas sweep, UVZSolver_multithread.cu:203-228)
-//   D  the solution scattered to t_z / t_u (t_v) with the reference's
-//      boundary-case formulas.
-// All wet segments of a line are solved as one system: the rows of a segment
-// are decoupled from their neighbours and every row outside a segment is an
-// identity row.  Each line's fields are read from HBM once.
+// A line's sweep does what the reference spreads over five kernels and global scratch
+// (UZSolver_calculate_preindex/_abcd/_matrix_coeff, tridiagSolver,
+// UZSolver_extract_solution, UVZSolver_multithread.cu:881-943 and the VZ twins 818-879;
+// Scan_FS*/tridiagSolver/FS*_extract_solution, Sediment_Transport.cu:570-617).
+// Only the wet segments of the line are touched: their cells and their tridiagonal rows
+// are packed one segment after another, so a line with a few wet cells costs a few rows
+// however long it is.
+//   A  continuity coefficients a2, c2, d2 of every wet cell
+//   B  momentum coefficients and the interleaved rows of every segment's system
+//   C  all segments of the line solved as one block-decoupled tridiagonal system by a
+//      partitioned method: each thread eliminates a chunk of rows, the chunk-end
+//      unknowns are solved by parallel cyclic reduction, each thread substitutes back
+//      (replaces the reference's serial Thomas sweep, UVZSolver_multithread.cu:203-228)
+//   D  the solution scattered to t_z / t_u (t_v) with the reference's boundary formulas.
+//
+// Two tiers.  The line kernels give every line one warp (four lines per CTA): a short
+// line (at most 3 rows per lane) is swept by its warp alone, in shared memory, with
+// warp-level synchronisation only.  A longer line is appended to a device list and swept
+// afterwards by the long-line kernel, a persistent grid in which a 512-thread CTA takes
+// one line at a time with shared memory sized for the longest line the grid can hold (a
+// global scratch region per CTA beyond that).  The last CTA of the long-line kernel
+// empties the list for the next sweep.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -24,29 +30,87 @@
 
 namespace {
 
-constexpr int kRedBuf = 2 * 4;  // two buffers of (A, B, C, D)
+constexpr int kT = 128;          // threads of a line-kernel CTA; 4 warps
+constexpr int kWarps = kT / 32;  // lines per CTA in the line kernels
+constexpr int kTL = 512;         // threads of a long-line CTA
+constexpr int kRowW = 96;        // rows of a warp-tier line (3 per lane)
+constexpr int kCellW = 48;       // cells of a warp-tier hydrodynamic line
+constexpr int kRowWf = 64;       // rows of a warp-tier sediment line
+constexpr int kRedL = 6 * kTL;   // reduced-system exchange buffer of a long-line CTA
+constexpr int kWarpHydro = 4 * kRowW + 3 * kCellW;  // doubles per warp
+constexpr int kWarpFs = 4 * kRowW;
 
-// Partitioned tridiagonal solve of rows [0, T*m) held in shared memory.
+// A group of threads that sweeps one line: a warp, or a whole long-line CTA.  exchange()
+// gives thread t the values v of threads t - h (lo) and t + h (hi).
+struct WarpG {
+    static constexpr int size = 32;
+    __device__ static __forceinline__ int rank() { return threadIdx.x & 31; }
+    __device__ static __forceinline__ void sync() { __syncwarp(); }
+    __device__ static __forceinline__ void exchange(const double (&v)[6], int h, double (&lo)[6], double (&hi)[6],
+                                                    double*) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            lo[k] = __shfl_up_sync(0xffffffffu, v[k], h);
+            hi[k] = __shfl_down_sync(0xffffffffu, v[k], h);
+        }
+    }
+};
+
+struct BlockG {
+    static constexpr int size = kTL;
+    __device__ static __forceinline__ int rank() { return threadIdx.x; }
+    __device__ static __forceinline__ void sync() { __syncthreads(); }
+    __device__ static __forceinline__ void exchange(const double (&v)[6], int h, double (&lo)[6], double (&hi)[6],
+                                                    double* buf) {
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < 6; k++) buf[k * kTL + t] = v[k];
+        __syncthreads();
+        const int tl = t - h >= 0 ? t - h : t;
+        const int th = t + h < kTL ? t + h : t;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            lo[k] = buf[k * kTL + tl];
+            hi[k] = buf[k * kTL + th];
+        }
+        __syncthreads();
+    }
+};
+
+// Chunk length for R rows over T threads: at least 3 and odd (odd strides keep the
+// chunk-strided shared-memory accesses free of bank conflicts).
+__host__ __device__ inline int chunk_len(int R, int T) {
+    int m = (R + T - 1) / T;
+    if (m < 3) m = 3;
+    if ((m & 1) == 0) m++;
+    return m;
+}
+
+// Partitioned tridiagonal solve of rows [0, T*m) by the T threads of group G.
 // Row r: A[r] x[r-1] + B[r] x[r] + C[r] x[r+1] = D[r]; A[0] and C[last] are ignored.
-// Thread t owns rows [t*m, t*m+m), m >= 3.  On return B[r] holds x[r].
-template <int T>
-__device__ void solve_partitioned(double* A, double* B, double* C, double* D, int m, double* red) {
-    const int t = threadIdx.x;
+// Thread t owns rows [t*m, t*m+m).  The 2T chunk-end unknowns form a tridiagonal system
+// solved by parallel cyclic reduction with every row scaled to a unit diagonal (one
+// reciprocal per row and level), held in registers and exchanged through G (shuffles,
+// or `red`, 6T doubles of shared memory).  On return B[r] holds x[r].
+template <class G>
+__device__ __forceinline__ void solve_partitioned(double* A, double* B, double* C, double* D, int m, double* red) {
+    constexpr int T = G::size;
+    const int t = G::rank();
     const int s = t * m, e = s + m - 1;
     // downward elimination inside the chunk: x_i + c'_i x_{i+1} + a'_i x_s = d'_i
     {
         int i = s + 1;
-        double den = B[i];
-        double cp = C[i] / den, dp = D[i] / den, ap = A[i] / den;
+        double r = 1.0 / B[i];
+        double cp = C[i] * r, dp = D[i] * r, ap = A[i] * r;
         A[i] = ap;
         C[i] = cp;
         D[i] = dp;
         for (i = s + 2; i <= e; i++) {
             const double ai = A[i];
-            den = B[i] - ai * cp;
-            cp = C[i] / den;
-            dp = (D[i] - ai * dp) / den;
-            ap = -(ai * ap) / den;
+            r = 1.0 / (B[i] - ai * cp);
+            cp = C[i] * r;
+            dp = (D[i] - ai * dp) * r;
+            ap = -(ai * ap) * r;
             A[i] = ap;
             C[i] = cp;
             D[i] = dp;
@@ -65,74 +129,76 @@ __device__ void solve_partitioned(double* A, double* B, double* C, double* D, in
             D[i] = dn;
         }
     }
-    // reduced system on the 2T interface unknowns (x_s, x_e of every chunk)
+    // Reduced system on the chunk-end unknowns ordered (x_s, x_e) chunk after chunk, each
+    // row scaled to a unit diagonal: row 2t is (v[0], 1, v[1] | v[2]), row 2t+1 is
+    // (v[3], 1, v[4] | v[5]) as (lower, diagonal, upper | right-hand side).
     constexpr int n = 2 * T;
-    double* rA = red;
-    double* rB = red + n;
-    double* rC = red + 2 * n;
-    double* rD = red + 3 * n;
+    double v[6];
     {
-        const double as = A[s], bs = B[s], cs = C[s], ds = D[s];
-        if (m >= 3) {
-            rA[2 * t] = as;
-            rB[2 * t] = bs - cs * A[s + 1];
-            rC[2 * t] = -cs * C[s + 1];
-            rD[2 * t] = ds - cs * D[s + 1];
-        }
-        rA[2 * t + 1] = A[e];
-        rB[2 * t + 1] = 1.0;
-        rC[2 * t + 1] = C[e];
-        rD[2 * t + 1] = D[e];
+        const double cs = C[s];
+        const double ib = 1.0 / (B[s] - cs * A[s + 1]);
+        v[0] = A[s] * ib;
+        v[1] = -cs * C[s + 1] * ib;
+        v[2] = (D[s] - cs * D[s + 1]) * ib;
+        v[3] = A[e];
+        v[4] = C[e];
+        v[5] = D[e];
     }
-    __syncthreads();
-    // parallel cyclic reduction, ping-pong between the two buffers
-    double* cur = red;
-    double* nxt = red + 4 * n;
+    // parallel cyclic reduction: at distance d row r eliminates rows r - d and r + d
     for (int d = 1; d < n; d <<= 1) {
+        double lo[6], hi[6];
+        const int h = d == 1 ? 1 : d >> 1;
+        G::exchange(v, h, lo, hi, red);
+        double la[2], lc[2], ld[2], ha[2], hc[2], hd[2];
+        bool lv[2], hv[2];
+        if (d == 1) {
+            // row 2t: lo = row 2t-1 (thread t-1, second row), hi = row 2t+1 (own second row)
+            la[0] = lo[3]; lc[0] = lo[4]; ld[0] = lo[5]; lv[0] = t >= 1;
+            ha[0] = v[3]; hc[0] = v[4]; hd[0] = v[5]; hv[0] = true;
+            // row 2t+1: lo = row 2t (own first row), hi = row 2t+2 (thread t+1, first row)
+            la[1] = v[0]; lc[1] = v[1]; ld[1] = v[2]; lv[1] = true;
+            ha[1] = hi[0]; hc[1] = hi[1]; hd[1] = hi[2]; hv[1] = t + 1 < T;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                la[q] = lo[3 * q]; lc[q] = lo[3 * q + 1]; ld[q] = lo[3 * q + 2]; lv[q] = t - h >= 0;
+                ha[q] = hi[3 * q]; hc[q] = hi[3 * q + 1]; hd[q] = hi[3 * q + 2]; hv[q] = t + h < T;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < 2; q++) {
-            const int r = 2 * t + q;
-            const double* cA = cur;
-            const double* cB = cur + n;
-            const double* cC = cur + 2 * n;
-            const double* cD = cur + 3 * n;
-            double nA = 0.0, nB = cB[r], nC = 0.0, nD = cD[r];
-            const int lo = r - d, hi = r + d;
-            if (lo >= 0) {
-                const double k1 = cA[r] / cB[lo];
-                nA = -cA[lo] * k1;
-                nB -= cC[lo] * k1;
-                nD -= cD[lo] * k1;
+            const double a = v[3 * q], c = v[3 * q + 1];
+            double nA = 0.0, nC = 0.0, nB = 1.0, nD = v[3 * q + 2];
+            if (lv[q]) {
+                nA = -la[q] * a;
+                nB -= lc[q] * a;
+                nD -= ld[q] * a;
             }
-            if (hi < n) {
-                const double k2 = cC[r] / cB[hi];
-                nC = -cC[hi] * k2;
-                nB -= cA[hi] * k2;
-                nD -= cD[hi] * k2;
+            if (hv[q]) {
+                nC = -hc[q] * c;
+                nB -= ha[q] * c;
+                nD -= hd[q] * c;
             }
-            nxt[r] = nA;
-            nxt[n + r] = nB;
-            nxt[2 * n + r] = nC;
-            nxt[3 * n + r] = nD;
+            const double ib = 1.0 / nB;
+            v[3 * q] = nA * ib;
+            v[3 * q + 1] = nC * ib;
+            v[3 * q + 2] = nD * ib;
         }
-        __syncthreads();
-        double* tmp = cur;
-        cur = nxt;
-        nxt = tmp;
     }
-    const double xs = cur[3 * n + 2 * t] / cur[n + 2 * t];
-    const double xe = cur[3 * n + 2 * t + 1] / cur[n + 2 * t + 1];
+    const double xs = v[2];
+    const double xe = v[5];
     for (int i = s + 1; i < e; i++) B[i] = D[i] - A[i] * xs - C[i] * xe;
     B[s] = xs;
     B[e] = xe;
-    __syncthreads();
+    G::sync();
 }
 
-// Serial Thomas per line by thread 0, in the reference's operation order
-// (tridiag, UVZSolver_multithread.cu:203-228) applied to the whole decoupled line.
-__device__ void solve_thomas(double* A, double* B, double* C, double* D, int rows) {
-    if (threadIdx.x == 0) {
-        // forward: store Ap in C, Bp in D
+// Serial Thomas over the packed rows by the group's first thread, in the reference's
+// operation order (tridiag, UVZSolver_multithread.cu:203-228); decoupled segments solve
+// exactly as separate systems.  Used to check the partitioned solver.
+template <class G>
+__device__ __forceinline__ void solve_thomas(double* A, double* B, double* C, double* D, int rows) {
+    if (G::rank() == 0 && rows > 0) {
         double Ap = -C[0] / B[0], Bp = D[0] / B[0];
         C[0] = Ap;
         D[0] = Bp;
@@ -150,343 +216,414 @@ __device__ void solve_thomas(double* A, double* B, double* C, double* D, int row
             B[i] = x;
         }
     }
-    __syncthreads();
+    G::sync();
 }
 
-struct SegInfo {
+struct LineShared {
     int first[HYD_SEGL], last[HYD_SEGL];
     int br1[HYD_SEGL], br2[HYD_SEGL];
-    int typeR[HYD_SEGL];  // rows start with continuity (bienrandau) instead of momentum (bienlongdau)
-    int sn[HYD_SEGL];
+    int typeR[HYD_SEGL];     // rows start with continuity (bienrandau) rather than momentum (bienlongdau)
+    int sn[HYD_SEGL];        // last row index of the segment's system (the reference's SN)
+    int lastKind[HYD_SEGL];  // 0 wall end, 1 discharge end, 2 stage end
+    int co[HYD_SEGL + 1];    // packed cell offset of each segment
+    int ro[HYD_SEGL + 1];    // packed row offset of each segment
     double tzl[HYD_SEGL], tzr[HYD_SEGL];
-    int nseg;
+    int nseg, R, C;
 };
 
-// Hydrodynamic sweep.  DIR 0: UZ, line = column j, cells i (t_u, ubt/ubp, bienQ[2]/[3]).
-//                      DIR 1: VZ, line = row i, cells j (t_v, vbd/vbt, bienQ[1]/[0]).
-template <int DIR, int T, int SOLVER>
-__global__ void __launch_bounds__(T) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int m) {
-    extern __shared__ double smem[];
-    __shared__ SegInfo sg;
-    const int line = startidx + blockIdx.x;
-    const int N = g.N, M = g.M, P = g.P;
-    const int L = DIR == 0 ? N : M;
-    const int Lc = L + 3;
-    const int Rpad = T * m;
-    double* A = smem;
-    double* B = A + Rpad;
-    double* C = B + Rpad;
-    double* D = C + Rpad;
-    double* a2 = D + Rpad;
-    double* c2 = a2 + Lc;
-    double* d2 = c2 + Lc;
-    double* red = d2 + Lc;
-    const int tid = threadIdx.x;
-    // cell k of this line -> linear position; stride across the line for the cross neighbour
-    const int along = DIR == 0 ? P : 1;  // offset to the next cell of the line
-    const int cross = DIR == 0 ? 1 : P;  // offset to the neighbouring line
-    const int base = DIR == 0 ? line : line * P;
-    double* tvel = DIR == 0 ? g.t_u : g.t_v;
-    const double bq_first = DIR == 0 ? g.ubt[line] : g.vbd[line];  // ubt_or_vbd
-    const double bq_last = DIR == 0 ? g.ubp[line] : g.vbt[line];   // ubp_or_vbt
-    const int Q1 = DIR == 0 ? g.bienQ[2] : g.bienQ[1];             // dkBienQ_1
-    const int Q2 = DIR == 0 ? g.bienQ[3] : g.bienQ[0];             // dkBienQ_2
+__device__ __forceinline__ int seg_of(const LineShared& sg, int c) {
+    int s = 0;
+    while (s + 1 < sg.nseg && sg.co[s + 1] <= c) s++;
+    return s;
+}
 
-    if (tid == 0) {
-        const int n = DIR == 0 ? g.mocj[line] : g.moci[line];
-        sg.nseg = n;
-    }
-    for (int r = tid; r < Rpad; r += T) {
-        A[r] = 0.0;
-        B[r] = 1.0;
-        C[r] = 0.0;
-        D[r] = 0.0;
-    }
+__device__ __forceinline__ int seg_of_row(const LineShared& sg, int c) {
+    int s = 0;
+    while (s + 1 < sg.nseg && sg.ro[s + 1] <= c) s++;
+    return s;
+}
+
+// Append a line to the long-line list.
+__device__ __forceinline__ void long_push(const DevGrid& g, int line) {
+    const unsigned k = atomicAdd(&g.long_ctr[0], 1u);
+    g.long_list[k] = line;
+}
+
+// Called by every CTA of a long-line kernel at its end: the last CTA to finish empties
+// the list (every CTA read the count before it got here).
+__device__ __forceinline__ void long_release(const DevGrid& g) {
     __syncthreads();
-    const int nseg = sg.nseg;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&g.long_ctr[1], 1u);
+        if (prev == gridDim.x - 1) {
+            g.long_ctr[0] = 0;
+            g.long_ctr[1] = 0;
+            __threadfence();
+        }
+    }
+}
+
+// ---- hydrodynamic sweeps ----------------------------------------------------------
+// DIR 0: UZ, line = column j, cells i (t_u, ubt/ubp, bienQ[2]/[3]).
+// DIR 1: VZ, line = row i, cells j (t_v, vbd/vbt, bienQ[1]/[0]).
+
+// Segments of the line, their system sizes (_calculate_matrix_coeff,
+// UVZSolver_multithread.cu:515-592) and packed offsets, into sg.
+template <int DIR, class G>
+__device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p, int line, LineShared& sg) {
+    const int tid = G::rank();
+    const int L = DIR == 0 ? g.N : g.M;
+    const int along = DIR == 0 ? g.P : 1;
+    const int base = DIR == 0 ? line : line * g.P;
+    const int Q1 = DIR == 0 ? g.bienQ[2] : g.bienQ[1];  // dkBienQ_1
+    const int Q2 = DIR == 0 ? g.bienQ[3] : g.bienQ[0];  // dkBienQ_2
+    const int nseg = DIR == 0 ? g.mocj[line] : g.moci[line];
     if (tid < nseg) {
         const int f = DIR == 0 ? g.dauj[line * HYD_SEGL + tid] : g.daui[line * HYD_SEGL + tid];
         const int l = DIR == 0 ? g.cuoij[line * HYD_SEGL + tid] : g.cuoii[line * HYD_SEGL + tid];
         int b1, b2;
         if (DIR == 0) seg_flags_u(g, p, line, f, l, b1, b2);
         else seg_flags_v(g, p, line, f, l, b1, b2);
+        const int Ls = l - f;
+        const int tR = b1 || (Q1 && f == 2);
+        const int qEnd = Q1 && l == L;
+        int sn, kind;
+        if (b1) {
+            if (!b2) {
+                if (Q2 && l == L) { sn = 2 * Ls; kind = 1; }
+                else { sn = 2 * Ls - 1; kind = 2; }
+            } else { sn = 2 * Ls; kind = 0; }
+        } else if (tR) {
+            if (!b2) {
+                if (qEnd) { sn = 2 * Ls; kind = 1; }
+                else { sn = 2 * Ls - 1; kind = 2; }
+            } else { sn = 2 * Ls; kind = 0; }
+        } else {
+            if (!b2) {
+                if (qEnd) { sn = 2 * Ls - 1; kind = 1; }
+                else { sn = 2 * Ls - 2; kind = 2; }
+            } else { sn = 2 * Ls - 1; kind = 0; }
+        }
         sg.first[tid] = f;
         sg.last[tid] = l;
         sg.br1[tid] = b1;
         sg.br2[tid] = b2;
-        sg.typeR[tid] = b1 || (Q1 && f == 2);
+        sg.typeR[tid] = tR;
+        sg.sn[tid] = sn;
+        sg.lastKind[tid] = kind;
         sg.tzl[tid] = g.t_z[base + f * along];
         sg.tzr[tid] = g.t_z[base + l * along];
     }
-    __syncthreads();
+    G::sync();
+    if (tid == 0) {
+        int c = 0, r = 0;
+        for (int s = 0; s < nseg; s++) {
+            sg.co[s] = c;
+            sg.ro[s] = r;
+            c += sg.last[s] - sg.first[s] + 1;
+            if (sg.sn[s] >= 0) r += sg.sn[s] + 1;
+            else flag_status(g, HYD_ST_DEGENERATE);  // single-cell segment on an open edge
+        }
+        sg.co[nseg] = c;
+        sg.ro[nseg] = r;
+        sg.C = c;
+        sg.R = r;
+        sg.nseg = nseg;
+    }
+    G::sync();
+}
 
-    // ---- A: continuity coefficients (preindex, UVZSolver_multithread.cu:402-406 / 345-349)
-    for (int sI = 0; sI < nseg; sI++) {
-        const int f = sg.first[sI], l = sg.last[sI];
-        for (int k = f + tid; k <= l; k += T) {
-            const int pos = base + k * along;
-            if (DIR == 0) {
-                c2[k] = p.dTchia2dX * g.Htdu[pos];
-                a2[k] = -p.dTchia2dX * g.Htdu[pos - P];
-                d2[k] = g.z[pos] - p.dTchia2dY * (g.Htdv[pos] * g.v[pos] - g.Htdv[pos - 1] * g.v[pos - 1]);
-            } else {
-                c2[k] = p.dTchia2dY * g.Htdv[pos];
-                a2[k] = -p.dTchia2dY * g.Htdv[pos - 1];
-                d2[k] = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
-            }
+// Phases A-D of one line by group G.  Rows A, B, Cc, D hold at least G::size * m
+// entries, cells a2, c2, d2 at least sg.C.
+template <int DIR, int SOLVER, class G>
+__device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p, int line, const LineShared& sg,
+                                           double* A, double* B, double* Cc, double* D, double* a2, double* c2,
+                                           double* d2, double* red, int m) {
+    constexpr int T = G::size;
+    const int tid = G::rank();
+    const int N = g.N, M = g.M, P = g.P;
+    const int L = DIR == 0 ? N : M;
+    (void)M;
+    const int along = DIR == 0 ? P : 1;  // offset to the next cell of the line
+    const int base = DIR == 0 ? line : line * P;
+    double* tvel = DIR == 0 ? g.t_u : g.t_v;
+    const double bq_first = DIR == 0 ? g.ubt[line] : g.vbd[line];  // ubt_or_vbd
+    const double bq_last = DIR == 0 ? g.ubp[line] : g.vbt[line];   // ubp_or_vbt
+    const int nseg = sg.nseg;
+    const int C = sg.C, R = sg.R;
+
+    // ---- A: continuity coefficients of every wet cell (preindex, UVZSolver_multithread.cu:402-406 / 345-349)
+    for (int c = tid; c < C; c += T) {
+        const int sI = seg_of(sg, c);
+        const int k = sg.first[sI] + (c - sg.co[sI]);
+        const int pos = base + k * along;
+        if (DIR == 0) {
+            c2[c] = p.dTchia2dX * g.Htdu[pos];
+            a2[c] = -p.dTchia2dX * g.Htdu[pos - P];
+            d2[c] = g.z[pos] - p.dTchia2dY * (g.Htdv[pos] * g.v[pos] - g.Htdv[pos - 1] * g.v[pos - 1]);
+        } else {
+            c2[c] = p.dTchia2dY * g.Htdv[pos];
+            a2[c] = -p.dTchia2dY * g.Htdv[pos - 1];
+            d2[c] = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
         }
     }
-    __syncthreads();
+    for (int r = R + tid; r < T * m; r += T) {
+        A[r] = 0.0;
+        B[r] = 1.0;
+        Cc[r] = 0.0;
+        D[r] = 0.0;
+    }
+    G::sync();
 
-    // ---- B1: momentum rows (preindex f1..f5, _calculate_abcd 409-466) and the interleaved rows
+    // ---- B1: momentum coefficients (preindex f1..f5, _calculate_abcd 409-466) and the rows
     const double f4 = DIR == 0 ? 2 * p.g * p.dTchia2dX : 2 * p.g * p.dTchia2dY;
-    for (int sI = 0; sI < nseg; sI++) {
+    for (int c = tid; c < C; c += T) {
+        const int sI = seg_of(sg, c);
         const int f = sg.first[sI], l = sg.last[sI];
+        const int k = f + (c - sg.co[sI]);
         const int Ls = l - f;
         const int tR = sg.typeR[sI];
         const int b1f = sg.br1[sI], b2f = sg.br2[sI];
-        for (int k = f + tid; k <= l; k += T) {
-            if (tR) {
-                A[2 * k] = a2[k];
-                B[2 * k] = 1.0;
-                C[2 * k] = c2[k];
-                D[2 * k] = d2[k];
-            }
-            if (k == l) continue;
-            if (Ls <= 1 && k != f) continue;
-            const int pos = base + k * along;
-            double f1, f2, f3, f5;
-            {
-                double pp = 0.0, qq = 0.0;
-                if (DIR == 0) {
-                    const double* u = g.u;
-                    const double* H = g.H_moi;
-                    const double vtb = (g.v[pos - 1] + g.v[pos] + g.v[pos + P - 1] + g.v[pos + P]) * 0.25;
-                    f1 = p.dTchia2dX * u[pos] + g.VISC[pos] * p.dT / p.dXbp;
-                    f2 = -(2 + g.Kx1[pos] * p.dT * sqrt(u[pos] * u[pos] + vtb * vtb) / g.Htdu[pos] +
-                           (2 * p.dT * g.VISC[pos]) / p.dXbp);
-                    f3 = p.dT * g.VISC[pos] / p.dXbp - p.dTchia2dX * u[pos];
-                    if (H[pos - 1] <= p.H_TINH) {
-                        if (vtb < 0) {
-                            pp = vtb * (-3 * u[pos] + 4 * u[pos + 1] - u[pos + 2]) / p.dY2;
-                            qq = (u[pos] - 2 * u[pos + 1] + u[pos + 2]) / p.dYbp;
+        const int sn = sg.sn[sI];
+        const int r0 = sg.ro[sI];
+        const int rel = 2 * (k - f);  // row 2k relative to the segment's first row 2f
+        if (tR && rel <= sn) {
+            A[r0 + rel] = a2[c];
+            B[r0 + rel] = 1.0;
+            Cc[r0 + rel] = c2[c];
+            D[r0 + rel] = d2[c];
+        }
+        if (k == l) continue;
+        if (Ls <= 1 && k != f) continue;
+        const int rm = tR ? rel + 1 : rel;  // the momentum row of this cell
+        if (rm > sn) continue;
+        const int pos = base + k * along;
+        double f1, f2, f3, f5;
+        {
+            double pp = 0.0, qq = 0.0;
+            if (DIR == 0) {
+                const double* u = g.u;
+                const double* H = g.H_moi;
+                const double vtb = (g.v[pos - 1] + g.v[pos] + g.v[pos + P - 1] + g.v[pos + P]) * 0.25;
+                f1 = p.dTchia2dX * u[pos] + g.VISC[pos] * p.dT / p.dXbp;
+                f2 = -(2 + g.Kx1[pos] * p.dT * sqrt(u[pos] * u[pos] + vtb * vtb) / g.Htdu[pos] +
+                       (2 * p.dT * g.VISC[pos]) / p.dXbp);
+                f3 = p.dT * g.VISC[pos] / p.dXbp - p.dTchia2dX * u[pos];
+                if (H[pos - 1] <= p.H_TINH) {
+                    if (vtb < 0) {
+                        pp = vtb * (-3 * u[pos] + 4 * u[pos + 1] - u[pos + 2]) / p.dY2;
+                        qq = (u[pos] - 2 * u[pos + 1] + u[pos + 2]) / p.dYbp;
+                    }
+                } else {
+                    if (H[pos + 1] <= p.H_TINH) {
+                        if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
+                            pp = vtb * (3 * u[pos] - 4 * u[pos - 1] + u[pos - 2]) / p.dY2;
+                            qq = (u[pos] - 2 * u[pos - 1] + u[pos - 2]) / p.dYbp;
                         }
                     } else {
-                        if (H[pos + 1] <= p.H_TINH) {
-                            if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
-                                pp = vtb * (3 * u[pos] - 4 * u[pos - 1] + u[pos - 2]) / p.dY2;
-                                qq = (u[pos] - 2 * u[pos - 1] + u[pos - 2]) / p.dYbp;
-                            }
-                        } else {
-                            pp = vtb * (u[pos + 1] - u[pos - 1]) / p.dY2;
-                            qq = (u[pos + 1] - 2 * u[pos] + u[pos - 1]) / p.dYbp;
-                        }
+                        pp = vtb * (u[pos + 1] - u[pos - 1]) / p.dY2;
+                        qq = (u[pos + 1] - 2 * u[pos] + u[pos - 1]) / p.dYbp;
                     }
-                    f5 = -2 * u[pos] + p.dT * pp - p.dT * p.CORIOLIS_FORCE * vtb - p.dT * g.VISC[pos] * qq -
-                         p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
-                } else {
-                    const double* v = g.v;
-                    const double* H = g.H_moi;
-                    const double utb = (g.u[pos - P] + g.u[pos] + g.u[pos - P + 1] + g.u[pos + 1]) * 0.25;
-                    f1 = p.dTchia2dY * v[pos] + g.VISC[pos] * p.dT / p.dYbp;
-                    f2 = -(2 + g.Ky1[pos] * p.dT * sqrt(v[pos] * v[pos] + utb * utb) / g.Htdv[pos] +
-                           (2 * p.dT * g.VISC[pos]) / p.dYbp);
-                    f3 = p.dT * g.VISC[pos] / p.dYbp - p.dTchia2dY * v[pos];
-                    if (H[pos - P] <= p.H_TINH) {
-                        if (utb < 0) {
-                            qq = utb * (-3 * v[pos] + 4 * v[pos + P] - v[pos + 2 * P]) / p.dX2;
-                            pp = (v[pos] - 2 * v[pos + P] + v[pos + 2 * P]) / p.dXbp;
-                        }
-                    } else {
-                        if (H[pos + P] <= p.H_TINH) {
-                            if ((H[pos - 2 * P] > p.H_TINH) && (utb > 0)) {
-                                qq = utb * (3 * v[pos] - 4 * v[pos - P] + v[pos - 2 * P]) / p.dX2;
-                                pp = (v[pos] - 2 * v[pos - P] + v[pos - 2 * P]) / p.dXbp;
-                            }
-                        } else {
-                            qq = utb * (v[pos + P] - v[pos - P]) / p.dX2;
-                            pp = (v[pos + P] - 2 * v[pos] + v[pos - P]) / p.dXbp;
-                        }
-                    }
-                    f5 = -2 * v[pos] + p.dT * qq + p.dT * p.CORIOLIS_FORCE * utb - p.dT * g.VISC[pos] * pp -
-                         p.dT * (p.windy - g.Tsyw[pos]) / g.Htdv[pos];
                 }
-            }
-            double ra, rb, rc, rd;
-            if (Ls >= 2) {
-                if (k == f && b1f) {
-                    ra = f4;
-                    rb = f2 - (f3 * a2[f + 1] / c2[f + 1]);
-                    rc = -f4 - (f3 / c2[f + 1]);
-                    rd = f5 - (f3 * d2[f + 1] / c2[f + 1]);
-                } else if (k == l - 1 && b2f) {
-                    ra = f4 - f1 / a2[k];
-                    rb = f2 - (f1 * c2[k] / a2[k]);
-                    rc = -f4;
-                    rd = f5 - (f1 * d2[k] / a2[k]);
-                } else {
-                    ra = f4 - f1 / a2[k];
-                    rc = -f4 - (f3 / c2[k + 1]);
-                    rb = f2 - (f1 * c2[k] / a2[k]) - (f3 * a2[k + 1] / c2[k + 1]);
-                    rd = f5 - (f1 * d2[k] / a2[k]) - (f3 * d2[k + 1] / c2[k + 1]);
-                }
+                f5 = -2 * u[pos] + p.dT * pp - p.dT * p.CORIOLIS_FORCE * vtb - p.dT * g.VISC[pos] * qq -
+                     p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
             } else {
-                ra = f4;
-                rb = f2;
-                rd = f5;
-                rc = -f4;
-            }
-            const int r = tR ? 2 * k + 1 : 2 * k;
-            A[r] = ra;
-            B[r] = rb;
-            C[r] = rc;
-            D[r] = rd;
-            if (!tR) {
-                A[2 * k + 1] = a2[k + 1];
-                B[2 * k + 1] = 1.0;
-                C[2 * k + 1] = c2[k + 1];
-                D[2 * k + 1] = d2[k + 1];
+                const double* v = g.v;
+                const double* H = g.H_moi;
+                const double utb = (g.u[pos - P] + g.u[pos] + g.u[pos - P + 1] + g.u[pos + 1]) * 0.25;
+                f1 = p.dTchia2dY * v[pos] + g.VISC[pos] * p.dT / p.dYbp;
+                f2 = -(2 + g.Ky1[pos] * p.dT * sqrt(v[pos] * v[pos] + utb * utb) / g.Htdv[pos] +
+                       (2 * p.dT * g.VISC[pos]) / p.dYbp);
+                f3 = p.dT * g.VISC[pos] / p.dYbp - p.dTchia2dY * v[pos];
+                if (H[pos - P] <= p.H_TINH) {
+                    if (utb < 0) {
+                        qq = utb * (-3 * v[pos] + 4 * v[pos + P] - v[pos + 2 * P]) / p.dX2;
+                        pp = (v[pos] - 2 * v[pos + P] + v[pos + 2 * P]) / p.dXbp;
+                    }
+                } else {
+                    if (H[pos + P] <= p.H_TINH) {
+                        if ((H[pos - 2 * P] > p.H_TINH) && (utb > 0)) {
+                            qq = utb * (3 * v[pos] - 4 * v[pos - P] + v[pos - 2 * P]) / p.dX2;
+                            pp = (v[pos] - 2 * v[pos - P] + v[pos - 2 * P]) / p.dXbp;
+                        }
+                    } else {
+                        qq = utb * (v[pos + P] - v[pos - P]) / p.dX2;
+                        pp = (v[pos + P] - 2 * v[pos] + v[pos - P]) / p.dXbp;
+                    }
+                }
+                f5 = -2 * v[pos] + p.dT * qq + p.dT * p.CORIOLIS_FORCE * utb - p.dT * g.VISC[pos] * pp -
+                     p.dT * (p.windy - g.Tsyw[pos]) / g.Htdv[pos];
             }
         }
+        double ra, rb, rc, rd;
+        if (Ls >= 2) {
+            if (k == f && b1f) {
+                ra = f4;
+                rb = f2 - (f3 * a2[c + 1] / c2[c + 1]);
+                rc = -f4 - (f3 / c2[c + 1]);
+                rd = f5 - (f3 * d2[c + 1] / c2[c + 1]);
+            } else if (k == l - 1 && b2f) {
+                ra = f4 - f1 / a2[c];
+                rb = f2 - (f1 * c2[c] / a2[c]);
+                rc = -f4;
+                rd = f5 - (f1 * d2[c] / a2[c]);
+            } else {
+                ra = f4 - f1 / a2[c];
+                rc = -f4 - (f3 / c2[c + 1]);
+                rb = f2 - (f1 * c2[c] / a2[c]) - (f3 * a2[c + 1] / c2[c + 1]);
+                rd = f5 - (f1 * d2[c] / a2[c]) - (f3 * d2[c + 1] / c2[c + 1]);
+            }
+        } else {
+            ra = f4;
+            rb = f2;
+            rd = f5;
+            rc = -f4;
+        }
+        A[r0 + rm] = ra;
+        B[r0 + rm] = rb;
+        Cc[r0 + rm] = rc;
+        D[r0 + rm] = rd;
+        if (!tR && rel + 1 <= sn) {
+            A[r0 + rel + 1] = a2[c + 1];
+            B[r0 + rel + 1] = 1.0;
+            Cc[r0 + rel + 1] = c2[c + 1];
+            D[r0 + rel + 1] = d2[c + 1];
+        }
     }
-    __syncthreads();
+    G::sync();
 
     // ---- B2: segment end rows (_calculate_matrix_coeff 469-592) and decoupling
-    if (tid < nseg) {
-        const int f = sg.first[tid], l = sg.last[tid];
-        const int Ls = l - f;
-        const int b1f = sg.br1[tid], b2f = sg.br2[tid], tR = sg.typeR[tid];
-        int sn;
-        int lastKind;  // 0 wall (row kept), 1 discharge end (DD -= CC*bq_last), 2 stage end (DD -= CC*TZ_r)
-        const int qEnd = Q1 && l == (DIR == 0 ? N : M);
-        if (b1f) {
-            if (!b2f) {
-                if (Q2 && l == (DIR == 0 ? N : M)) {
-                    sn = 2 * Ls;
-                    lastKind = 1;
-                } else {
-                    sn = 2 * Ls - 1;
-                    lastKind = 2;
-                }
-            } else {
-                sn = 2 * Ls;
-                lastKind = 0;
-            }
-        } else if (tR) {
-            if (!b2f) {
-                if (qEnd) {
-                    sn = 2 * Ls;
-                    lastKind = 1;
-                } else {
-                    sn = 2 * Ls - 1;
-                    lastKind = 2;
-                }
-            } else {
-                sn = 2 * Ls;
-                lastKind = 0;
-            }
-        } else {
-            if (!b2f) {
-                if (qEnd) {
-                    sn = 2 * Ls - 1;
-                    lastKind = 1;
-                } else {
-                    sn = 2 * Ls - 2;
-                    lastKind = 2;
-                }
-            } else {
-                sn = 2 * Ls - 1;
-                lastKind = 0;
-            }
+    if (tid < nseg && sg.sn[tid] >= 0) {
+        const int sn = sg.sn[tid];
+        const int rowF = sg.ro[tid], rowL = rowF + sn;
+        const double oA = A[rowL], oB = B[rowL], oC = Cc[rowL], oD = D[rowL];
+        if (!sg.br1[tid]) {
+            if (sg.typeR[tid]) D[rowF] = D[rowF] - A[rowF] * bq_first;
+            else D[rowF] = D[rowF] - A[rowF] * sg.tzl[tid];
         }
-        sg.sn[tid] = sn;
-        const int rowF = 2 * f;
-        if (sn < 0) {
-            // single-cell segment on an open edge: the reference solves a negative-size
-            // system on stale scratch; nothing is solved here
-            flag_status(g, HYD_ST_DEGENERATE);
-            for (int r = rowF; r <= 2 * l + 1; r++) {
-                A[r] = 0.0;
-                B[r] = 1.0;
-                C[r] = 0.0;
-                D[r] = 0.0;
-            }
-        } else {
-            const int rowL = rowF + sn;
-            const double oA = A[rowL], oB = B[rowL], oC = C[rowL], oD = D[rowL];
-            if (!b1f) {
-                if (tR) D[rowF] = D[rowF] - A[rowF] * bq_first;
-                else D[rowF] = D[rowF] - A[rowF] * sg.tzl[tid];
-            }
-            if (lastKind == 1) {
-                A[rowL] = oA;
-                B[rowL] = oB;
-                D[rowL] = oD - oC * bq_last;
-            } else if (lastKind == 2) {
-                A[rowL] = oA;
-                B[rowL] = oB;
-                D[rowL] = oD - oC * sg.tzr[tid];
-            }
-            A[rowF] = 0.0;
-            C[rowL] = 0.0;
-            for (int r = rowL + 1; r <= 2 * l + 1; r++) {
-                A[r] = 0.0;
-                B[r] = 1.0;
-                C[r] = 0.0;
-                D[r] = 0.0;
-            }
-        }
+        // the end-row statement always rewrites AA, BB, DD of the last row; for a
+        // single-row system that undoes the first-row override (UVZSolver_multithread.cu:574-590)
+        A[rowL] = oA;
+        B[rowL] = oB;
+        const int kind = sg.lastKind[tid];
+        if (kind == 1) D[rowL] = oD - oC * bq_last;
+        else if (kind == 2) D[rowL] = oD - oC * sg.tzr[tid];
+        else D[rowL] = oD;
+        A[rowF] = 0.0;
+        Cc[rowL] = 0.0;
     }
-    __syncthreads();
+    G::sync();
 
     // ---- C: solve
-    if (SOLVER == 0) solve_partitioned<T>(A, B, C, D, m, red);
-    else solve_thomas(A, B, C, D, 2 * L + 4);
+    if (SOLVER == 0) solve_partitioned<G>(A, B, Cc, D, m, red);
+    else solve_thomas<G>(A, B, Cc, D, R);
 
     // ---- D: extract (_uzSolver_extract_solution 668-723 / _vzSolver_extract_solution 595-665)
     const double* x = B;
     const int QF = DIR == 0 ? g.bienQ[2] : g.bienQ[1];
     const int QL = DIR == 0 ? g.bienQ[3] : g.bienQ[0];
-    for (int sI = 0; sI < nseg; sI++) {
+    for (int c = tid; c < C; c += T) {
+        const int sI = seg_of(sg, c);
         const int f = sg.first[sI], l = sg.last[sI];
+        const int k = f + (c - sg.co[sI]);
         const int b1f = sg.br1[sI], b2f = sg.br2[sI];
         const int sn = sg.sn[sI];
+        const int r0 = sg.ro[sI] - 2 * f;  // packed index of global row r is r0 + r
         const int qfirst = !b1f && QF && f == 2;
-        for (int k = f + tid; k <= l; k += T) {
-            const int pos = base + k * along;
-            if (k < l) {
-                if (b1f || qfirst) {
-                    g.t_z[pos] = x[2 * k];
-                    tvel[pos] = x[2 * k + 1];
-                    if (k == f) tvel[pos - along] = b1f ? 0.0 : bq_first;
-                } else {
-                    if (k == f) {
-                        const double tv = x[2 * f];
-                        tvel[pos] = tv;
-                        tvel[pos - along] = (d2[f] - g.t_z[pos] - c2[f] * tv) / a2[f];
-                    } else {
-                        g.t_z[pos] = x[2 * k - 1];
-                        tvel[pos] = x[2 * k];
-                    }
-                }
+        const int pos = base + k * along;
+        if (k < l) {
+            if (b1f || qfirst) {
+                g.t_z[pos] = x[r0 + 2 * k];
+                tvel[pos] = x[r0 + 2 * k + 1];
+                if (k == f) tvel[pos - along] = b1f ? 0.0 : bq_first;
+            } else if (k == f) {
+                const double tv = x[r0 + 2 * f];
+                tvel[pos] = tv;
+                tvel[pos - along] = (d2[c] - g.t_z[pos] - c2[c] * tv) / a2[c];
             } else {
-                const double xl = sn >= 0 ? x[2 * f + sn] : 0.0;
-                if (b2f) {
-                    tvel[pos] = 0.0;
-                    g.t_z[pos] = xl;
-                } else if (QL && l == (DIR == 0 ? N : M)) {
-                    tvel[pos] = bq_last;
-                    g.t_z[pos] = xl;
-                } else {
-                    double tprev;
-                    if (l > f) tprev = (b1f || qfirst) ? x[2 * l - 1] : x[2 * l - 2];
-                    else tprev = tvel[pos - along];
-                    tvel[pos] = (d2[l] - a2[l] * tprev - g.t_z[pos]) / c2[l];
-                }
+                g.t_z[pos] = x[r0 + 2 * k - 1];
+                tvel[pos] = x[r0 + 2 * k];
+            }
+        } else {
+            const double xl = sn >= 0 ? x[r0 + 2 * f + sn] : 0.0;
+            if (b2f) {
+                tvel[pos] = 0.0;
+                g.t_z[pos] = xl;
+            } else if (QL && l == L) {
+                tvel[pos] = bq_last;
+                g.t_z[pos] = xl;
+            } else {
+                double tprev;
+                if (l > f) tprev = (b1f || qfirst) ? x[r0 + 2 * l - 1] : x[r0 + 2 * l - 2];
+                else tprev = tvel[pos - along];
+                tvel[pos] = (d2[c] - a2[c] * tprev - g.t_z[pos]) / c2[c];
             }
         }
     }
-    (void)cross;
+}
+
+// Line kernel: warp w of CTA b sweeps line startidx + 4b + w, or lists it as long.
+template <int DIR, int SOLVER>
+__global__ void __launch_bounds__(kT) k_hydro_lines(DevGrid g, DevParams p, int startidx, int endidx) {
+    extern __shared__ double dyn_smem[];
+    __shared__ LineShared sgw[kWarps];
+    const int w = threadIdx.x >> 5;
+    const int line = startidx + blockIdx.x * kWarps + w;
+    if (line > endidx) return;  // the whole warp; only warp-level barriers follow
+    LineShared& sg = sgw[w];
+    hydro_setup<DIR, WarpG>(g, p, line, sg);
+    if (sg.nseg == 0) return;
+    if (sg.R > kRowW || sg.C > kCellW) {
+        if ((threadIdx.x & 31) == 0) long_push(g, line);
+        return;
+    }
+    double* A = dyn_smem + w * kWarpHydro;
+    double* B = A + kRowW;
+    double* Cc = B + kRowW;
+    double* D = Cc + kRowW;
+    double* a2 = D + kRowW;
+    double* c2 = a2 + kCellW;
+    double* d2 = c2 + kCellW;
+    hydro_body<DIR, SOLVER, WarpG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, nullptr, chunk_len(sg.R, 32));
+}
+
+// Long-line kernel: CTA b sweeps listed lines b, b + gridDim.x, ...  Shared memory holds
+// RB rows and CB cells; a line needing more uses the CTA's global region of RG rows and
+// CG cells.
+template <int DIR, int SOLVER>
+__global__ void __launch_bounds__(kTL) k_hydro_long(DevGrid g, DevParams p, int RB, int CB, double* gscr, int RG,
+                                                   int CG) {
+    extern __shared__ double dyn_smem[];
+    __shared__ LineShared sg;
+    const int n = *(volatile unsigned*)&g.long_ctr[0];
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int line = g.long_list[k];
+        hydro_setup<DIR, BlockG>(g, p, line, sg);
+        const int m = chunk_len(sg.R, kTL);
+        double* red = dyn_smem;
+        if (kTL * m <= RB && sg.C <= CB) {
+            double* A = red + kRedL;
+            double* B = A + RB;
+            double* Cc = B + RB;
+            double* D = Cc + RB;
+            double* a2 = D + RB;
+            double* c2 = a2 + CB;
+            double* d2 = c2 + CB;
+            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, red, m);
+        } else {
+            double* A = gscr + (size_t)blockIdx.x * (4 * (size_t)RG + 3 * (size_t)CG);
+            double* B = A + RG;
+            double* Cc = B + RG;
+            double* D = Cc + RG;
+            double* a2 = D + RG;
+            double* c2 = a2 + CG;
+            double* d2 = c2 + CG;
+            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, red, m);
+        }
+        __syncthreads();  // sg and the buffers are reused by the next line
+    }
+    long_release(g);
 }
 
 // ---- sediment sweeps --------------------------------------------------------------
@@ -514,36 +651,16 @@ __device__ __forceinline__ double source_nchs(const DevParams& p, double wsm, do
     // source_nchs (Sediment_Transport.cu:52-60)
     const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
     const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
-    const double Cac = 0.015 * p.dm * pow(Tx, 1.5) * pow(p.dxr, (-0.3)) / (0.05 * h_moi);
+    const double Cac = 0.015 * p.dm * pow(Tx, 1.5) * p.dxr_m03 / (0.05 * h_moi);
     return wsm * (Cac - gamac * fs);
 }
 
-// Suspended-sediment sweep.  DIR 0: FSj (columns j = 3..M-1, rows i), DIR 1: FSi (rows i = 3..N-1).
-template <int DIR, int T, int SOLVER>
-__global__ void __launch_bounds__(T) k_fs_sweep(DevGrid g, DevParams p, double t, int startidx, int m) {
-    extern __shared__ double smem[];
-    __shared__ SegInfo sg;
-    const int line = startidx + blockIdx.x;
-    const int P = g.P;
-    const int Rpad = T * m;
-    double* A = smem;
-    double* B = A + Rpad;
-    double* C = B + Rpad;
-    double* D = C + Rpad;
-    double* red = D + Rpad;
-    const int tid = threadIdx.x;
-    const int along = DIR == 0 ? P : 1;
-    const int base = DIR == 0 ? line : line * P;
-    const double s_start = p.bed_change_start;
-    if (tid == 0) sg.nseg = DIR == 0 ? g.mocj[line] : g.moci[line];
-    for (int r = tid; r < Rpad; r += T) {
-        A[r] = 0.0;
-        B[r] = 1.0;
-        C[r] = 0.0;
-        D[r] = 0.0;
-    }
-    __syncthreads();
-    const int nseg = sg.nseg;
+// Segments of a sediment line and their row offsets (one row per interior cell
+// first+1..last-1, the reference's SN+1 rows).
+template <int DIR, class G>
+__device__ __forceinline__ void fs_setup(const DevGrid& g, const DevParams& p, int line, LineShared& sg) {
+    const int tid = G::rank();
+    const int nseg = DIR == 0 ? g.mocj[line] : g.moci[line];
     if (tid < nseg) {
         const int f = DIR == 0 ? g.dauj[line * HYD_SEGL + tid] : g.daui[line * HYD_SEGL + tid];
         const int l = DIR == 0 ? g.cuoij[line * HYD_SEGL + tid] : g.cuoii[line * HYD_SEGL + tid];
@@ -555,182 +672,320 @@ __global__ void __launch_bounds__(T) k_fs_sweep(DevGrid g, DevParams p, double t
         sg.br1[tid] = b1;
         sg.br2[tid] = b2;
     }
-    __syncthreads();
+    G::sync();
+    if (tid == 0) {
+        int r = 0;
+        for (int s = 0; s < nseg; s++) {
+            sg.ro[s] = r;
+            const int n = sg.last[s] - sg.first[s] - 1;
+            if (n > 0) r += n;
+        }
+        sg.ro[nseg] = r;
+        sg.R = r;
+        sg.nseg = nseg;
+    }
+    G::sync();
+}
+
+// Rows, solve and extraction of one sediment line (_FSi/_FSj_calculate__mactrix_coeff
+// and _FSi/_FSj_extract_solution, Sediment_Transport.cu:62-340, driven by Scan_FSi/
+// Scan_FSj and FSi/FSj_extract_solution 570-618).  DIR 0: FSj (line = column j, cells
+// i), DIR 1: FSi (line = row i, cells j).
+template <int DIR, int SOLVER, class G>
+__device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, int half, int line,
+                                        const LineShared& sg, double* A, double* B, double* Cc, double* D,
+                                        double* red, int m) {
+    constexpr int T = G::size;
+    const int tid = G::rank();
+    const int P = g.P;
+    const int along = DIR == 0 ? P : 1;
+    const int base = DIR == 0 ? line : line * P;
+    const double s_start = p.bed_change_start;
+    const double t = g.clock[half];
+    const int R = sg.R;
+    for (int r = R + tid; r < T * m; r += T) {
+        A[r] = 0.0;
+        B[r] = 1.0;
+        Cc[r] = 0.0;
+        D[r] = 0.0;
+    }
     const double* FS = g.FS;
     const double* H = g.H_moi;
     const double sqrtg = sqrt(p.g);
-    for (int sI = 0; sI < nseg; sI++) {
+    for (int rr = tid; rr < R; rr += T) {
+        const int sI = seg_of_row(sg, rr);
         const int f = sg.first[sI], l = sg.last[sI];
-        if (l - f < 2) continue;
+        const int k = f + 1 + (rr - sg.ro[sI]);
         const int b1f = sg.br1[sI], b2f = sg.br2[sI];
-        for (int k = f + 1 + tid; k <= l - 1; k += T) {
-            const int pos = base + k * along;
-            const double c = 18 * log(12 * H[pos] / p.Ks);
-            const double Uf = sqrtg * fabs(g.VTH[pos]) / c;
-            const double wsm = p.wss * pow((1 - FS[pos]), 4);
-            double Zf = 0;
-            double S;
-            double gamav;
-            if (DIR == 0) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
-            if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
-            if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], H[pos]);
-            else S = source_nchs(p, wsm, Zf, Uf, H[pos], FS[pos]);
-            if (t < s_start) S = 0;
-            if (DIR == 1) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
-            double aa, bb, cc, dd, pp, qq;
-            if (DIR == 0) {
-                aa = -gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 -
-                     g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
-                cc = gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
-                bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
-                pp = 0;
+        const int pos = base + k * along;
+        const double c = 18 * log(12 * H[pos] / p.Ks);
+        const double Uf = sqrtg * fabs(g.VTH[pos]) / c;
+        const double fq = 1 - FS[pos];
+        const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
+        double Zf = 0;
+        double S;
+        double gamav;
+        if (DIR == 0) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
+        if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+        if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], H[pos]);
+        else S = source_nchs(p, wsm, Zf, Uf, H[pos], FS[pos]);
+        if (t < s_start) S = 0;
+        if (DIR == 1) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
+        double aa, bb, cc, dd, pp, qq;
+        if (DIR == 0) {
+            aa = -gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 -
+                 g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
+            cc = gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
+            bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
+            pp = 0;
+            qq = 0;
+            if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = (FS[pos + 1] - FS[pos]);
+            if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = (FS[pos] - FS[pos - 1]);
+            pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
+            if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
+                qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
+                qq = (g.t_v[pos] + g.t_v[pos - 1]) * 0.5 * qq * gamav;
+            } else
                 qq = 0;
-                if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = (FS[pos + 1] - FS[pos]);
-                if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = (FS[pos] - FS[pos - 1]);
-                pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
-                if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
-                    qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
-                    qq = (g.t_v[pos] + g.t_v[pos - 1]) * 0.5 * qq * gamav;
-                } else
-                    qq = 0;
-                dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
-                if (k == f + 1) {
-                    if (b1f || g.t_u[base + f * along] == 0) bb += aa;
-                    else dd -= aa * FS[base + f * along];
-                }
-                if (k == l - 1) {
-                    if (b2f && g.t_u[base + l * along] == 0) bb += cc;
-                    else dd -= cc * FS[base + l * along];
-                }
-            } else {
-                aa = -gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 -
-                     g.Htdv[pos - 1] * g.Ky[pos - 1] / (H[pos] * p.dYbp);
-                cc = gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos] * g.Ky[pos] / (H[pos] * p.dYbp);
-                bb = p.HaiChiadT + (g.Htdv[pos] * g.Ky[pos] + g.Htdv[pos - 1] * g.Ky[pos - 1]) / (H[pos] * p.dYbp);
-                pp = 0;
-                qq = 0;
-                if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = (FS[pos + P] - FS[pos]);
-                if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = (FS[pos] - FS[pos - P]);
-                pp = (1 / (H[pos] * p.dXbp)) * (g.Htdu[pos] * g.Kx[pos] * pp - g.Htdu[pos - P] * g.Kx[pos - P] * qq);
-                if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
-                    qq = (FS[pos + P] - FS[pos - P]) / p.dX2;
-                    qq = (g.t_u[pos] + g.t_u[pos - P]) * 0.5 * qq * gamav;
-                } else
-                    qq = 0;
-                dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
-                if (k == f + 1) {
-                    if (b1f || g.t_v[base + f * along] == 0) bb = bb + aa;
-                    else dd = dd - aa * FS[base + f * along];
-                }
-                if (k == l - 1) {
-                    if (b2f || g.t_v[base + l * along] == 0) bb = bb + cc;
-                    else dd = dd - cc * FS[base + l * along];
-                }
-            }
-            A[k] = (k == f + 1) ? 0.0 : aa;
-            B[k] = bb;
-            C[k] = (k == l - 1) ? 0.0 : cc;
-            D[k] = dd;
-        }
-    }
-    __syncthreads();
-    if (SOLVER == 0) solve_partitioned<T>(A, B, C, D, m, red);
-    else solve_thomas(A, B, C, D, DIR == 0 ? g.N + 3 : g.M + 3);
-    const double* x = B;
-    double* vel = DIR == 0 ? g.t_u : g.t_v;
-    for (int sI = 0; sI < nseg; sI++) {
-        const int f = sg.first[sI], l = sg.last[sI];
-        if (l - f < 2) continue;
-        const int b1f = sg.br1[sI], b2f = sg.br2[sI];
-        for (int k = f + 1 + tid; k <= l - 1; k += T) {
-            const int pos = base + k * along;
-            double xv = x[k];
-            if (xv < 0) xv = p.NDnen;
-            g.tFS[pos] = xv;
+            dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
             if (k == f + 1) {
-                // FSj: t_u[pos - width]; FSi: t_v[i*width + first]
-                const double vb = DIR == 0 ? vel[pos - P] : vel[base + f * along];
-                g.tFS[base + f * along] = (b1f || vb == 0) ? xv : FS[base + f * along];
+                if (b1f || g.t_u[base + f * along] == 0) bb += aa;
+                else dd -= aa * FS[base + f * along];
             }
             if (k == l - 1) {
-                const double vb = DIR == 0 ? vel[pos + P] : vel[base + l * along];
-                g.tFS[base + l * along] = (b2f || vb == 0) ? xv : FS[base + l * along];
+                if (b2f && g.t_u[base + l * along] == 0) bb += cc;
+                else dd -= cc * FS[base + l * along];
             }
+        } else {
+            aa = -gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 -
+                 g.Htdv[pos - 1] * g.Ky[pos - 1] / (H[pos] * p.dYbp);
+            cc = gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos] * g.Ky[pos] / (H[pos] * p.dYbp);
+            bb = p.HaiChiadT + (g.Htdv[pos] * g.Ky[pos] + g.Htdv[pos - 1] * g.Ky[pos - 1]) / (H[pos] * p.dYbp);
+            pp = 0;
+            qq = 0;
+            if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = (FS[pos + P] - FS[pos]);
+            if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = (FS[pos] - FS[pos - P]);
+            pp = (1 / (H[pos] * p.dXbp)) * (g.Htdu[pos] * g.Kx[pos] * pp - g.Htdu[pos - P] * g.Kx[pos - P] * qq);
+            if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
+                qq = (FS[pos + P] - FS[pos - P]) / p.dX2;
+                qq = (g.t_u[pos] + g.t_u[pos - P]) * 0.5 * qq * gamav;
+            } else
+                qq = 0;
+            dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
+            if (k == f + 1) {
+                if (b1f || g.t_v[base + f * along] == 0) bb = bb + aa;
+                else dd = dd - aa * FS[base + f * along];
+            }
+            if (k == l - 1) {
+                if (b2f || g.t_v[base + l * along] == 0) bb = bb + cc;
+                else dd = dd - cc * FS[base + l * along];
+            }
+        }
+        A[rr] = (k == f + 1) ? 0.0 : aa;
+        B[rr] = bb;
+        Cc[rr] = (k == l - 1) ? 0.0 : cc;
+        D[rr] = dd;
+    }
+    G::sync();
+    if (SOLVER == 0) solve_partitioned<G>(A, B, Cc, D, m, red);
+    else solve_thomas<G>(A, B, Cc, D, R);
+    const double* x = B;
+    double* vel = DIR == 0 ? g.t_u : g.t_v;
+    for (int c = tid; c < R; c += T) {
+        const int sI = seg_of_row(sg, c);
+        const int f = sg.first[sI], l = sg.last[sI];
+        const int k = f + 1 + (c - sg.ro[sI]);
+        const int b1f = sg.br1[sI], b2f = sg.br2[sI];
+        const int pos = base + k * along;
+        double xv = x[c];
+        if (xv < 0) xv = p.NDnen;
+        g.tFS[pos] = xv;
+        if (k == f + 1) {
+            // FSj: t_u[pos - width]; FSi: t_v[i*width + first]
+            const double vb = DIR == 0 ? vel[pos - P] : vel[base + f * along];
+            g.tFS[base + f * along] = (b1f || vb == 0) ? xv : FS[base + f * along];
+        }
+        if (k == l - 1) {
+            const double vb = DIR == 0 ? vel[pos + P] : vel[base + l * along];
+            g.tFS[base + l * along] = (b2f || vb == 0) ? xv : FS[base + l * along];
         }
     }
 }
 
-// --- launch configuration --------------------------------------------------------
-inline int odd_chunk(int rows, int T) {
-    int m = (rows + T - 1) / T;
-    if (m < 3) m = 3;
-    if ((m & 1) == 0) m++;
-    return m;
+template <int DIR, int SOLVER>
+__global__ void __launch_bounds__(kT) k_fs_lines(DevGrid g, DevParams p, int half, int startidx, int endidx) {
+    extern __shared__ double dyn_smem[];
+    __shared__ LineShared sgw[kWarps];
+    const int w = threadIdx.x >> 5;
+    const int line = startidx + blockIdx.x * kWarps + w;
+    if (line > endidx) return;
+    LineShared& sg = sgw[w];
+    fs_setup<DIR, WarpG>(g, p, line, sg);
+    if (sg.R == 0) return;
+    if (sg.R > kRowWf) {
+        if ((threadIdx.x & 31) == 0) long_push(g, line);
+        return;
+    }
+    double* A = dyn_smem + w * kWarpFs;
+    double* B = A + kRowW;
+    double* Cc = B + kRowW;
+    double* D = Cc + kRowW;
+    fs_body<DIR, SOLVER, WarpG>(g, p, half, line, sg, A, B, Cc, D, nullptr, chunk_len(sg.R, 32));
 }
 
-template <int DIR>
-void launch_hydro(const DevGrid& g, const DevParams& p, int startidx, int endidx, int solver, cudaStream_t s) {
-    const int nlines = endidx - startidx + 1;
-    if (nlines <= 0) return;
-    const int L = DIR == 0 ? g.N : g.M;
-    const int rows = 2 * L + 4;
-    const int Lc = L + 3;
-#define HYD_LAUNCH_T(TT)                                                                                     \
-    do {                                                                                                     \
-        const int m = odd_chunk(rows, TT);                                                                   \
-        const size_t sm = sizeof(double) * ((size_t)4 * TT * m + 3 * (size_t)Lc + kRedBuf * 2 * TT);         \
-        if (solver == 0) {                                                                                   \
-            cudaFuncSetAttribute(k_hydro_sweep<DIR, TT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-            k_hydro_sweep<DIR, TT, 0><<<nlines, TT, sm, s>>>(g, p, startidx, m);                             \
-        } else {                                                                                             \
-            cudaFuncSetAttribute(k_hydro_sweep<DIR, TT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-            k_hydro_sweep<DIR, TT, 1><<<nlines, TT, sm, s>>>(g, p, startidx, m);                             \
-        }                                                                                                    \
-    } while (0)
-    if (rows <= 256) HYD_LAUNCH_T(32);
-    else if (rows <= 1024) HYD_LAUNCH_T(64);
-    else HYD_LAUNCH_T(128);
-#undef HYD_LAUNCH_T
-    hyd_kernel_launches_add(1);
+template <int DIR, int SOLVER>
+__global__ void __launch_bounds__(kTL) k_fs_long(DevGrid g, DevParams p, int half, int RB, double* gscr, int RG) {
+    extern __shared__ double dyn_smem[];
+    __shared__ LineShared sg;
+    const int n = *(volatile unsigned*)&g.long_ctr[0];
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int line = g.long_list[k];
+        fs_setup<DIR, BlockG>(g, p, line, sg);
+        const int m = chunk_len(sg.R, kTL);
+        double* red = dyn_smem;
+        if (kTL * m <= RB) {
+            double* A = red + kRedL;
+            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sg, A, A + RB, A + 2 * RB, A + 3 * RB, red, m);
+        } else {
+            double* A = gscr + (size_t)blockIdx.x * 4 * (size_t)RG;
+            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sg, A, A + RG, A + 2 * RG, A + 3 * RG, red, m);
+        }
+        __syncthreads();
+    }
+    long_release(g);
 }
 
-template <int DIR>
-void launch_fs(const DevGrid& g, const DevParams& p, double t, int solver, cudaStream_t s) {
-    const int startidx = 3;
-    const int endidx = DIR == 0 ? g.M - 1 : g.N - 1;
-    const int nlines = endidx - startidx + 1;
-    if (nlines <= 0) return;
-    const int rows = (DIR == 0 ? g.N : g.M) + 3;
-#define HYD_LAUNCH_T(TT)                                                                                  \
-    do {                                                                                                  \
-        const int m = odd_chunk(rows, TT);                                                                \
-        const size_t sm = sizeof(double) * ((size_t)4 * TT * m + kRedBuf * 2 * TT);                       \
-        if (solver == 0) {                                                                                \
-            cudaFuncSetAttribute(k_fs_sweep<DIR, TT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-            k_fs_sweep<DIR, TT, 0><<<nlines, TT, sm, s>>>(g, p, t, startidx, m);                          \
-        } else {                                                                                          \
-            cudaFuncSetAttribute(k_fs_sweep<DIR, TT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-            k_fs_sweep<DIR, TT, 1><<<nlines, TT, sm, s>>>(g, p, t, startidx, m);                          \
-        }                                                                                                 \
-    } while (0)
-    if (rows <= 128) HYD_LAUNCH_T(32);
-    else if (rows <= 512) HYD_LAUNCH_T(64);
-    else HYD_LAUNCH_T(128);
-#undef HYD_LAUNCH_T
-    hyd_kernel_launches_add(1);
+// Largest dynamic shared memory the kernel may be given on this device.
+int max_dyn_smem(const void* f) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, f) != cudaSuccess) return 48 * 1024;
+    return optin - (int)a.sharedSizeBytes;
 }
+
+template <class F>
+cudaError_t allow_all(F* const* fs, int n, int* limit) {
+    int lim = 1 << 30;
+    for (int i = 0; i < n; i++) {
+        const int mx = max_dyn_smem((const void*)fs[i]);
+        const cudaError_t e = cudaFuncSetAttribute((const void*)fs[i], cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        if (e != cudaSuccess) return e;
+        if (mx < lim) lim = mx;
+    }
+    *limit = lim;
+    return cudaSuccess;
+}
+
+using HydroLinesFn = void(DevGrid, DevParams, int, int);
+using HydroLongFn = void(DevGrid, DevParams, int, int, double*, int, int);
+using FsLinesFn = void(DevGrid, DevParams, int, int, int);
+using FsLongFn = void(DevGrid, DevParams, int, int, double*, int);
+
+HydroLinesFn* const kHydroLines[2][2] = {{k_hydro_lines<0, 0>, k_hydro_lines<0, 1>},
+                                         {k_hydro_lines<1, 0>, k_hydro_lines<1, 1>}};
+HydroLongFn* const kHydroLong[2][2] = {{k_hydro_long<0, 0>, k_hydro_long<0, 1>},
+                                       {k_hydro_long<1, 0>, k_hydro_long<1, 1>}};
+FsLinesFn* const kFsLines[2][2] = {{k_fs_lines<0, 0>, k_fs_lines<0, 1>}, {k_fs_lines<1, 0>, k_fs_lines<1, 1>}};
+FsLongFn* const kFsLong[2][2] = {{k_fs_long<0, 0>, k_fs_long<0, 1>}, {k_fs_long<1, 0>, k_fs_long<1, 1>}};
 
 }  // namespace
 
-void launch_sweep_uz(const DevGrid& g, const DevParams& p, int startidx, int endidx, int solver, cudaStream_t s) {
-    launch_hydro<0>(g, p, startidx, endidx, solver, s);
+// Shared-memory sizes and the long-line grid of a grid of N x M cells on the current
+// device; opts the sweep kernels into the shared memory they may need.
+cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
+    cudaError_t e;
+    int lim_lines, lim_long, lim_fsl, lim_fslong;
+    if ((e = allow_all(&kHydroLines[0][0], 4, &lim_lines)) != cudaSuccess) return e;
+    if ((e = allow_all(&kHydroLong[0][0], 4, &lim_long)) != cudaSuccess) return e;
+    if ((e = allow_all(&kFsLines[0][0], 4, &lim_fsl)) != cudaSuccess) return e;
+    if ((e = allow_all(&kFsLong[0][0], 4, &lim_fslong)) != cudaSuccess) return e;
+    sp->smem_lines = sizeof(double) * kWarps * kWarpHydro;
+    sp->smem_fs_lines = sizeof(double) * kWarps * kWarpFs;
+    if ((int)sp->smem_lines > lim_lines || (int)sp->smem_fs_lines > lim_fsl) return cudaErrorInvalidValue;
+    const int L = N > M ? N : M;
+    // every row/cell a line can have: rows <= 2 L + 20, cells <= L + 3
+    sp->RG = kTL * chunk_len(2 * L + HYD_SEGL, kTL);
+    sp->CG = L + 3;
+    const size_t full = sizeof(double) * (kRedL + 4 * (size_t)sp->RG + 3 * (size_t)sp->CG);
+    if ((long long)full <= lim_long) {
+        sp->RB = sp->RG;
+        sp->CB = sp->CG;
+        sp->need_global = 0;
+    } else {
+        // as many rows (and half as many cells) as fit; longer lines use global scratch
+        const int per = 4 * 2 + 3;  // doubles per pair of rows
+        const int pairs = (int)((lim_long / (int)sizeof(double) - kRedL) / per);
+        sp->RB = (2 * pairs) / kTL * kTL;
+        sp->CB = pairs;
+        sp->need_global = 1;
+    }
+    sp->smem_long = sizeof(double) * (kRedL + 4 * (size_t)sp->RB + 3 * (size_t)sp->CB);
+    sp->RGf = kTL * chunk_len(L, kTL);
+    const size_t full_fs = sizeof(double) * (kRedL + 4 * (size_t)sp->RGf);
+    if ((long long)full_fs <= lim_fslong) {
+        sp->RBf = sp->RGf;
+    } else {
+        sp->RBf = (int)((lim_fslong / (int)sizeof(double) - kRedL) / 4) / kTL * kTL;
+        sp->need_global = 1;
+    }
+    sp->smem_fs_long = sizeof(double) * (kRedL + 4 * (size_t)sp->RBf);
+    int dev = 0, nsm = 0, occ = 0, occf = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kHydroLong[0][0], kTL, sp->smem_long)) != cudaSuccess)
+        return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, kFsLong[0][0], kTL, sp->smem_fs_long)) !=
+        cudaSuccess)
+        return e;
+    if (occ < 1) occ = 1;
+    if (occf < 1) occf = 1;
+    sp->long_grid = nsm * (occ < occf ? occ : occf);
+    if (sp->long_grid > L + 3) sp->long_grid = L + 3;
+    sp->scratch_doubles = sp->need_global ? (size_t)sp->long_grid * (4 * (size_t)sp->RG + 3 * (size_t)sp->CG) : 1;
+    return cudaSuccess;
 }
-void launch_sweep_vz(const DevGrid& g, const DevParams& p, int startidx, int endidx, int solver, cudaStream_t s) {
-    launch_hydro<1>(g, p, startidx, endidx, solver, s);
+
+namespace {
+void hydro_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
+                 int solver, double* scratch, cudaStream_t s) {
+    const int nlines = endidx - startidx + 1;
+    if (nlines <= 0) return;
+    const int sv = solver ? 1 : 0;
+    kHydroLines[dir][sv]<<<(nlines + kWarps - 1) / kWarps, kT, sp.smem_lines, s>>>(g, p, startidx, endidx);
+    kHydroLong[dir][sv]<<<sp.long_grid, kTL, sp.smem_long, s>>>(g, p, sp.RB, sp.CB, scratch, sp.RG, sp.CG);
+    hyd_kernel_launches_add(2);
 }
-void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, double t, int solver, cudaStream_t s) {
-    launch_fs<0>(g, p, t, solver, s);
+
+void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int startidx,
+              int endidx, int solver, double* scratch, cudaStream_t s) {
+    const int nlines = endidx - startidx + 1;
+    if (nlines <= 0) return;
+    const int sv = solver ? 1 : 0;
+    kFsLines[dir][sv]<<<(nlines + kWarps - 1) / kWarps, kT, sp.smem_fs_lines, s>>>(g, p, half, startidx, endidx);
+    kFsLong[dir][sv]<<<sp.long_grid, kTL, sp.smem_fs_long, s>>>(g, p, half, sp.RBf, scratch, sp.RGf);
+    hyd_kernel_launches_add(2);
 }
-void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, double t, int solver, cudaStream_t s) {
-    launch_fs<1>(g, p, t, solver, s);
+}  // namespace
+
+void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
+                     int solver, double* scratch, cudaStream_t s) {
+    hydro_sweep(0, g, p, sp, startidx, endidx, solver, scratch, s);
+}
+
+void launch_sweep_vz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
+                     int solver, double* scratch, cudaStream_t s) {
+    hydro_sweep(1, g, p, sp, startidx, endidx, solver, scratch, s);
+}
+
+// FSj over columns 3..M-1 (Engine.py:224-237), FSi over rows 3..N-1 (Engine.py:345-358).
+void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
+                       double* scratch, cudaStream_t s) {
+    fs_sweep(0, g, p, sp, half, 3, g.M - 1, solver, scratch, s);
+}
+
+void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
+                       double* scratch, cudaStream_t s) {
+    fs_sweep(1, g, p, sp, half, 3, g.N - 1, solver, scratch, s);
 }
