@@ -92,6 +92,12 @@ struct HydSim {
     // bit 1: sediment in half-step 2, bit 2: Exner update)
     int use_graphs;
     int force_rescan;  // the next step rescans every line (mask or segment tables were set)
+    // elementwise kernels still owed one whole-grid pass before they may run on the
+    // extended spans: bit 0 hydrodynamics (smoothing, state update), bit 1 sediment
+    int full_pending;
+    // CTA widths of the row and column line kernels, from the longest span of each
+    // direction (about two cells per thread)
+    int thr_r, thr_c;
     cudaGraphExec_t graph[8];
     long long graph_kernels[8];
 };
@@ -109,6 +115,33 @@ void drop_graphs(HydSim* s) {
         s->graph[k] = nullptr;
     }
 }
+
+// Widths of the row / column line kernels from the spans (read back once per mask).
+static int refresh_widths(HydSim* s) {
+    std::vector<int> lo((size_t)(s->N > s->M ? s->N : s->M) + 3), hi(lo.size());
+    auto longest = [&](const int* dlo, const int* dhi, int n) -> int {
+        if (cudaMemcpyAsync(lo.data(), dlo, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaMemcpyAsync(hi.data(), dhi, sizeof(int) * n, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess)
+            return -1;
+        int best = 0;
+        for (int i = 0; i < n; i++)
+            if (hi[i] >= lo[i] && hi[i] - lo[i] + 1 > best) best = hi[i] - lo[i] + 1;
+        return best;
+    };
+    auto pick = [](int len) {
+        int t = ((len + 1) / 2 + 31) / 32 * 32;
+        return t < 64 ? 64 : (t > 512 ? 512 : t);
+    };
+    const int lr = longest(s->g.rlo, s->g.rhi, s->N + 3), lc = longest(s->g.clo, s->g.chi, s->M + 3);
+    if (lr < 0 || lc < 0) return fail(HYD_ECUDA, "reading the spans back failed");
+    const int tr = pick(lr), tc = pick(lc);
+    if (tr != s->thr_r || tc != s->thr_c) drop_graphs(s);
+    s->thr_r = tr;
+    s->thr_c = tc;
+    return HYD_OK;
+}
+
 
 int set_clock(HydSim* s, double t) {
     const double c[3] = {t, t, t};
@@ -348,6 +381,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     if (device < 0 || device >= ndev) return fail(HYD_EINVAL, "bad device index");
     CUDA_TRY(cudaSetDevice(device));
     HydSim* s = new HydSim();
+    s->thr_r = s->thr_c = 128;
     s->P = *p;
     s->N = N;
     s->M = M;
@@ -390,6 +424,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     total += a256(4 * 8) + a256(4 * 4) + a256(4 * HYD_SEGL * 4) + a256(64) + a256(64);
     total += a256(((N > M ? N : M) + 3) * 4) + a256(64);  // long-line list and counters
     total += 4 * a256((N + 3) * 4) + 4 * a256((M + 3) * 4) + a256(64);  // spans, rescan flags and lists
+    total += 2 * a256((N + 3) * 4) + a256(64);                          // extended spans
     e = cudaMalloc(&s->arena, total);
     if (e != cudaSuccess) {
         cudaStreamDestroy(s->stream);
@@ -443,6 +478,9 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.dirty_c = (int*)take((M + 3) * 4);
     g.dlist_c = (int*)take((M + 3) * 4);
     g.dctr = (unsigned*)take(64);
+    g.elo = (int*)take((N + 3) * 4);
+    g.ehi = (int*)take((N + 3) * 4);
+    g.span_wide = (int*)take(64);
     g.clock = (double*)take(64);
     if ((size_t)(cur - (char*)s->arena) > total) {
         cudaFree(s->arena);
@@ -516,9 +554,12 @@ int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count
         launch_spans(h->g, h->stream);
         clear_rescan_lists(h->g, h->stream);
         h->force_rescan = 1;
+        const int rc = refresh_widths(h);
+        if (rc) return rc;
     } else if (f->kind >= 2 && f->kind <= 5) {
         h->force_rescan = 1;  // segment tables
     }
+    h->full_pending = 3;  // any field may feed the elementwise kernels outside the spans
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return HYD_OK;
@@ -595,17 +636,22 @@ int hyd_init(hyd_handle h, double t_start) {
     h->t = t_start;
     h->initialized = 1;
     h->force_rescan = 0;  // the set-up scanned every line
-    int rc = set_clock(h, t_start);
+    h->full_pending = 3;
+    int rc = refresh_widths(h);
+    if (rc) return rc;
+    rc = set_clock(h, t_start);
     if (rc) return rc;
     return check_device_status(h);
 }
 
 // The launch sequence of one full step (Engine.py:144-366).  sed1/sed2: sediment phase
 // active in the first/second half-step (t >= sediment_start); bed: Exner update at the end.
-static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0) {
+static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, int full_h = 0, int full_s = 0) {
     DevGrid& g = s->g;
     const DevParams& p = s->dp;
     cudaStream_t st = s->stream;
+    // channel mode writes levels at table-dependent places: always the whole grid
+    const int fh = full_h || p.channel, fsd = full_s || p.channel;
     launch_clock(g, p, st);
     // ---- half-step 1: implicit along i (columns), explicit v
     { PHASE(PH_BOUNDARY); launch_boundary(g, p, 0, st); }
@@ -615,19 +661,19 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0) {
         end_idx = s->M - 1;
     }
     { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
     std::swap(g.t_u, s->scratch_u);
-    { PHASE(PH_EXPL_V); launch_explicit_v(g, p, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, st); }
+    { PHASE(PH_EXPL_V); launch_explicit_v(g, p, s->thr_r, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, st); }
     std::swap(g.t_v, s->scratch_v);
     if (force) launch_mark_all_cols(g, st);
-    { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, st); }
-    { PHASE(PH_POST); launch_post(g, p, st); }
+    { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, s->thr_r, st); }
+    { PHASE(PH_POST); launch_post(g, p, fh, st); }
     { PHASE(PH_SCAN); launch_scan_cols(g, p, st); }
     if (sed1) {
-        { PHASE(PH_VTH); launch_vth_hesok(g, p, st); }
+        { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
         { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
-        { PHASE(PH_UPDATE_FS); launch_update_fs(g, st); }
+        { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
     }
     // ---- half-step 2: implicit along j (rows), explicit u
     { PHASE(PH_BOUNDARY); launch_boundary(g, p, 1, st); }
@@ -638,18 +684,18 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0) {
         end_idx = s->N;
     }
     { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, st); }
     std::swap(g.t_v, s->scratch_v);
-    { PHASE(PH_EXPL_U); launch_explicit_u(g, p, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, st); }
+    { PHASE(PH_EXPL_U); launch_explicit_u(g, p, s->thr_c, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
     std::swap(g.t_u, s->scratch_u);
-    { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, st); }
-    { PHASE(PH_POST); launch_post(g, p, st); }
+    { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }
+    { PHASE(PH_POST); launch_post(g, p, fh, st); }
     { PHASE(PH_SCAN); launch_scan_rows(g, p, st); }
     if (sed2) {
-        { PHASE(PH_VTH); launch_vth_hesok(g, p, st); }
+        { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
         { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, s->plan, 1, s->solver, s->sweep_scratch, st); }
-        { PHASE(PH_UPDATE_FS); launch_update_fs(g, st); }
+        { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
         start_idx = 3;
         end_idx = s->N - 1;
     }
@@ -657,6 +703,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0) {
         PHASE(PH_BED);
         launch_bed(g, p, start_idx, end_idx, st);
     }
+    if (full_h && !p.channel) launch_widen_spans(g, st);
     s->start_idx = start_idx;
     s->end_idx = end_idx;
 }
@@ -701,12 +748,16 @@ int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
         const int mask = sed1 | (sed2 << 1) | (bed << 2);
         const int force = h->force_rescan;
         h->force_rescan = 0;
-        cudaGraphExec_t exec = (h->use_graphs && !h->timing && !force) ? step_graph(h, mask) : nullptr;
+        const int full_h = h->full_pending & 1;
+        const int full_s = (sed1 || sed2) ? (h->full_pending >> 1) & 1 : 0;
+        h->full_pending &= ~(full_h | (full_s << 1));
+        const int special = force || full_h || full_s;
+        cudaGraphExec_t exec = (h->use_graphs && !h->timing && !special) ? step_graph(h, mask) : nullptr;
         if (exec) {
             CUDA_TRY(cudaGraphLaunch(exec, h->stream));
             hyd_kernel_launches_add(h->graph_kernels[mask]);
         } else {
-            launch_step(h, sed1, sed2, bed, force);
+            launch_step(h, sed1, sed2, bed, force, full_h, full_s);
         }
         t = t2;
     }
@@ -722,6 +773,7 @@ int hyd_set_params(hyd_handle h, const HydCaseParams* p) {
     if (p->dT <= 0 || p->dX <= 0 || p->dY <= 0) return fail(HYD_EINVAL, "dX, dY, dT must be positive");
     h->P = *p;
     h->dp = make_dev_params(h->P);
+    h->full_pending = 3;
     drop_graphs(h);
     return HYD_OK;
 }

@@ -48,6 +48,10 @@ struct DevGrid {
     unsigned* long_ctr;  // [0] listed lines, [1] CTAs of the long-line kernel done
     // span of the cells whose mask is not 2 (those never change) per row / column
     int *rlo, *rhi, *clo, *chi;
+    // extended span per row (every cell within a few cells of those), where the
+    // elementwise kernels run once the whole grid has been brought up to date
+    int *elo, *ehi;
+    int* span_wide;  // set when a velocity lies outside the extended spans
     // lines whose mask changed since their segments were scanned: flags and lists
     int *dirty_r, *dirty_c, *dlist_r, *dlist_c;
     unsigned* dctr;  // [0] listed rows, [1] listed columns, [2] [3] CTAs of the rescans done
@@ -122,22 +126,23 @@ void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, 
                      int solver, double* scratch, cudaStream_t s);
 void launch_sweep_vz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
                      int solver, double* scratch, cudaStream_t s);
-void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, cudaStream_t s);
-void launch_explicit_v(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_explicit_u(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, cudaStream_t s);
-void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, cudaStream_t s);
+void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, cudaStream_t s);
+void launch_widen_spans(const DevGrid& g, cudaStream_t s);
+void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
+void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
+void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
+void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_spans(const DevGrid& g, cudaStream_t s);
 void clear_rescan_lists(const DevGrid& g, cudaStream_t s);
 void launch_mark_all_cols(const DevGrid& g, cudaStream_t s);
-void launch_post(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_post(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
 void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_vth_hesok(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
 void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
                        double* scratch, cudaStream_t s);
 void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
                        double* scratch, cudaStream_t s);
-void launch_update_fs(const DevGrid& g, cudaStream_t s);
+void launch_update_fs(const DevGrid& g, int full, cudaStream_t s);
 void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, cudaStream_t s);
 long long hyd_kernel_launches_add(long long n);

@@ -16,6 +16,7 @@ namespace {
 
 constexpr double kPiRef = 3.14159265359;  // constant.cuh:3
 constexpr double kEpsRef = 1e-16;         // UVZSolver_multithread.cu:12
+constexpr int kSpanHalo = 4;              // extended-span margin, cells
 
 inline dim3 grid2d(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y); }
 
@@ -251,15 +252,17 @@ __global__ void k_boundary_channel(DevGrid g, DevParams p, int half) {
 
 // Normalize + update_buffer (support_funcs.cu:682-729): out = 5-point smoothed velocity on
 // the interior, a copy elsewhere.  isU smooths t_u (neighbours along i, wet check along j).
-__global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+// A nonzero velocity outside the row's extended span is reported in *g.span_wide (the
+// spans then cannot bound the smoothing).
+__device__ __forceinline__ void smooth_cell(const DevGrid& g, const DevParams& p, int isU, double* __restrict__ out,
+                                            int i, int j, bool check_span) {
     const int N = g.N, M = g.M, P = g.P;
     if (i >= N + 3 || j >= M + 3) return;
     const double* val = isU ? g.t_u : g.t_v;
     const int gp = i * P + j;
     const double v0 = val[gp];
     double r = v0;
+    if (check_span && v0 != 0 && (j < g.elo[i] || j > g.ehi[i])) *g.span_wide = 1;
     if (!(i > N || j > M || i < 2 || j < 2) && v0 != 0) {
         const int close_d = isU ? P : 1, far_d = isU ? 1 : P;
         int count = 2;
@@ -277,13 +280,23 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
     out[gp] = r;
 }
 
+__global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
+    smooth_cell(g, p, isU, out, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x, true);
+}
+
+__global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i > g.N + 2) return;
+    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) smooth_cell(g, p, isU, out, i, j, false);
+}
+
 // ----------------------------------------------------------- explicit momentum
 
 // solveV/vSolver (UVZSolver_multithread.cu:1055-1071, 727-768) on row i, then
 // update_margin_elem_V (1008-1052) for the same row.
 __global__ void k_explicit_v(DevGrid g, DevParams p) {
     extern __shared__ double sv[];  // the row's t_v over [k0, k1]
-    __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL];
+    __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL], s_first[HYD_SEGL], s_last[HYD_SEGL], s_off[HYD_SEGL + 1];
     const int row = 2 + blockIdx.x;
     const int P = g.P, M = g.M;
     const int nseg = g.moci[row];
@@ -297,14 +310,27 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
         const int i = row, W = P, k = threadIdx.x;
         const int first = g.daui[i * HYD_SEGL + k], last = g.cuoii[i * HYD_SEGL + k];
         const double* h = g.h;
+        s_first[k] = first;
+        s_last[k] = last;
         s_b1[k] = (first > 2) || ((first == 2) && (fabs((h[i * W + first - 1] + h[(i - 1) * W + first - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
         s_b2[k] = (last < M) || ((last == M) && (fabs((h[i * W + last] + h[(i - 1) * W + last]) * 0.5 - p.NANGDAY) < kEpsRef));
     }
     __syncthreads();
-    for (int k = 0; k < nseg; k++) {
-        const int first = g.daui[row * HYD_SEGL + k], last = g.cuoii[row * HYD_SEGL + k];
-        if (first >= last) continue;
-        for (int col = first + threadIdx.x; col < last; col += blockDim.x) {
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int q = 0; q < nseg; q++) {
+            s_off[q] = off;
+            off += max(s_last[q] - s_first[q], 0);
+        }
+        s_off[nseg] = off;
+    }
+    __syncthreads();
+    // every cell first..last-1 of every segment, packed segment after segment
+    for (int c = threadIdx.x; c < s_off[nseg]; c += blockDim.x) {
+        {
+            int k = 0;
+            while (k + 1 < nseg && s_off[k + 1] <= c) k++;
+            const int col = s_first[k] + (c - s_off[k]);
             const int o = P;
             double pp, q, tmp;
             q = 0;
@@ -344,7 +370,7 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
         // segment ends in order, on the staged row (update_margin_elem_V)
         double* t_v = g.t_v + row * P;
         for (int k = 0; k < nseg; k++) {
-            const int first = g.daui[row * HYD_SEGL + k], last = g.cuoii[row * HYD_SEGL + k];
+            const int first = s_first[k], last = s_last[k];
             const double a = s_b1[k] ? 0.0 : 2 * sv[first - k0] - sv[first + 1 - k0];
             sv[first - 1 - k0] = a;
             t_v[first - 1] = a;
@@ -353,13 +379,14 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
             t_v[last] = b;
         }
     }
+    __syncthreads();  // keep the other warps resident while thread 0 works
 }
 
 // solveU/uSolver (UVZSolver_multithread.cu:947-968, 773-815) on column j, then
 // update_margin_elem_U (970-1006).
 __global__ void k_explicit_u(DevGrid g, DevParams p) {
     extern __shared__ double su[];  // the column's t_u over [k0, k1]
-    __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL];
+    __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL], s_first[HYD_SEGL], s_last[HYD_SEGL], s_off[HYD_SEGL + 1];
     const int col = 2 + blockIdx.x;
     const int P = g.P, N = g.N;
     const int nseg = g.mocj[col];
@@ -372,13 +399,27 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
         const int j = col, W = P, k = threadIdx.x;
         const int first = g.dauj[j * HYD_SEGL + k], last = g.cuoij[j * HYD_SEGL + k];
         const double* h = g.h;
+        s_first[k] = first;
+        s_last[k] = last;
         s_b1[k] = (first > 2) || ((first == 2) && ((fabs(h[1 * W + j] + h[1 * W + j - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
         s_b2[k] = (last < N) || ((last == N) && (fabs((h[N * W + j] + h[N * W + j - 1]) * 0.5 - p.NANGDAY) < kEpsRef));
     }
     __syncthreads();
-    for (int k = 0; k < nseg; k++) {
-        const int first = g.dauj[col * HYD_SEGL + k], last = g.cuoij[col * HYD_SEGL + k];
-        for (int row = first + threadIdx.x; row < last; row += blockDim.x) {
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int q = 0; q < nseg; q++) {
+            s_off[q] = off;
+            off += max(s_last[q] - s_first[q], 0);
+        }
+        s_off[nseg] = off;
+    }
+    __syncthreads();
+    // every cell first..last-1 of every segment, packed segment after segment
+    for (int c = threadIdx.x; c < s_off[nseg]; c += blockDim.x) {
+        {
+            int k = 0;
+            while (k + 1 < nseg && s_off[k + 1] <= c) k++;
+            const int row = s_first[k] + (c - s_off[k]);
             const int o = P;
             double pp, q, tmp;
             pp = 0;
@@ -417,7 +458,7 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
     if (threadIdx.x == 0) {
         // segment ends in order, on the staged column (update_margin_elem_U)
         for (int k = 0; k < nseg; k++) {
-            const int first = g.dauj[col * HYD_SEGL + k], last = g.cuoij[col * HYD_SEGL + k];
+            const int first = s_first[k], last = s_last[k];
             const double a = s_b1[k] ? 0.0 : 2 * su[first - k0] - su[first + 1 - k0];
             su[first - 1 - k0] = a;
             g.t_u[(first - 1) * P + col] = a;
@@ -426,6 +467,7 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
             g.t_u[last * P + col] = b;
         }
     }
+    __syncthreads();  // keep the other warps resident while thread 0 works
 }
 
 // --------------------------------------------------------------- wet/dry resets
@@ -612,6 +654,7 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
     __syncthreads();
     if (threadIdx.x < 32 && line >= 2 && (s_changed || force))
         warp_scan_line(g, WetShared{khs, k0}, lo, hi, L, words, dau, cuoi, moc);
+    __syncthreads();  // keep the other warps resident while warp 0 scans
 }
 
 // Spans of the cells whose mask is not 2: rows [rlo, rhi], columns [clo, chi] (the
@@ -626,6 +669,31 @@ __global__ void k_spans(DevGrid g) {
         atomicMin(&g.clo[j], i);
         atomicMax(&g.chi[j], i);
     }
+}
+
+// Extended span of row i: every cell within H cells (rows and columns) of a cell whose
+// mask is not 2.  Velocities, levels and depths only change within one cell of those
+// cells and the elementwise kernels read one cell around, so outside the extended spans
+// they reproduce what is there.
+__global__ void k_ext_spans(DevGrid g, int H) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > g.N + 2) return;
+    int lo = 0x7fffffff, hi = -1;
+    for (int r = i - H; r <= i + H; r++) {
+        if (r < 0 || r > g.N + 2 || g.rhi[r] < g.rlo[r]) continue;
+        lo = min(lo, g.rlo[r] - H);
+        hi = max(hi, g.rhi[r] + H);
+    }
+    g.elo[i] = max(lo, 0);
+    g.ehi[i] = min(hi, g.M + 2);
+}
+
+// After a full-grid pass found a velocity outside the extended spans: spans = whole rows.
+__global__ void k_widen_spans(DevGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > g.N + 2 || !*g.span_wide) return;
+    g.elo[i] = 0;
+    g.ehi[i] = g.M + 2;
 }
 
 // List every row (ROWS) or column of the grid for a segment rescan.
@@ -647,9 +715,7 @@ __global__ void k_mark_all(DevGrid g) {
 // update_uvz (support_funcs.cu:671-680) and Htuongdoi (338-354) in one pass.  The
 // kernel's kenhhepd/kenhhepng parameters never receive the host's flags (Engine.py:90
 // passes two arguments fewer than it declares), so velocities are copied unmasked.
-__global__ void k_post(DevGrid g, int with_uvz) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void post_cell(const DevGrid& g, int with_uvz, int i, int j) {
     const int N = g.N, M = g.M, P = g.P;
     if (i > N || j > M) return;
     const int gp = i * P + j;
@@ -666,6 +732,16 @@ __global__ void k_post(DevGrid g, int with_uvz) {
     const double* h = g.h;
     g.Htdu[gp] = (h[gp - 1] + h[gp] + z_ip + z_ij) * 0.5;
     g.Htdv[gp] = (h[gp - P] + h[gp] + z_jp + z_ij) * 0.5;
+}
+
+__global__ void k_post(DevGrid g, int with_uvz) {
+    post_cell(g, with_uvz, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void k_post_span(DevGrid g) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i > g.N) return;
+    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) post_cell(g, 1, i, j);
 }
 
 // ------------------------------------------------------------- wet-segment scans
@@ -760,9 +836,7 @@ __device__ void fs_edges_block(const DevGrid& g, const DevParams& p) {
 // --------------------------------------------------------------------- sediment
 
 // Find_VTH (Sediment_Transport.cu:541-568) and hesoK (508-539) in one pass
-__global__ void k_vth_hesok(DevGrid g, DevParams p) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void vth_cell(const DevGrid& g, const DevParams& p, int i, int j) {
     const int N = g.N, M = g.M, P = g.P;
     if (i > N || j > M) return;
     const int pos = i * P + j;
@@ -787,12 +861,37 @@ __global__ void k_vth_hesok(DevGrid g, DevParams p) {
     }
 }
 
+__global__ void k_vth_hesok(DevGrid g, DevParams p) {
+    vth_cell(g, p, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void k_vth_span(DevGrid g, DevParams p) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i > g.N) return;
+    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) vth_cell(g, p, i, j);
+}
+
 // Update_FS (Sediment_Transport.cu:620-629)
 __global__ void k_update_fs(DevGrid g) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int i = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > g.N || j > g.M) return;
     g.FS[i * g.P + j] = g.tFS[i * g.P + j];
+}
+
+// Update_FS over the extended spans, plus rows 2 and N and column M in full (the edge
+// interpolation writes FS there).
+__global__ void k_update_fs_span(DevGrid g) {
+    const int i = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int N = g.N, M = g.M, P = g.P;
+    if (i > N) return;
+    int lo = g.elo[i] > 1 ? g.elo[i] : 1, hi = g.ehi[i] < M ? g.ehi[i] : M;
+    if (i == 2 || i == N) {
+        lo = 1;
+        hi = M;
+    }
+    for (int j = lo + lane; j <= hi; j += 32) g.FS[i * P + j] = g.tFS[i * P + j];
+    if (lane == 0 && (M < lo || M > hi)) g.FS[i * P + M] = g.tFS[i * P + M];
 }
 
 // Calculate_Qb (Sediment_Transport.cu:341-414): bed-load flux, then the edge copies
@@ -981,8 +1080,15 @@ void launch_spans(const DevGrid& g, cudaStream_t s) {
     cudaMemsetAsync(g.rhi, 0xff, sizeof(int) * (g.N + 3), s);
     cudaMemsetAsync(g.clo, 0x7f, sizeof(int) * (g.M + 3), s);
     cudaMemsetAsync(g.chi, 0xff, sizeof(int) * (g.M + 3), s);
+    cudaMemsetAsync(g.span_wide, 0, sizeof(int), s);
     const dim3 b(32, 8);
     k_spans<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g);
+    k_ext_spans<<<(g.N + 3 + 127) / 128, 128, 0, s>>>(g, kSpanHalo);
+    hyd_kernel_launches_add(2);
+}
+
+void launch_widen_spans(const DevGrid& g, cudaStream_t s) {
+    k_widen_spans<<<(g.N + 3 + 127) / 128, 128, 0, s>>>(g);
     hyd_kernel_launches_add(1);
 }
 
@@ -1025,35 +1131,42 @@ void launch_clock(const DevGrid& g, const DevParams& p, cudaStream_t s) {
     hyd_kernel_launches_add(1);
 }
 
-void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, cudaStream_t s) {
+// Elementwise kernels: the whole grid (`full`), or one warp per row over its extended span.
+static int row_warps_blocks(int rows) { return (rows * 32 + 255) / 256; }
+
+void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, cudaStream_t s) {
     const dim3 b(32, 8);
-    k_smooth<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
+    if (full) k_smooth<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
+    else k_smooth_span<<<row_warps_blocks(g.N + 3), 256, 0, s>>>(g, p, isU, out);
     hyd_kernel_launches_add(1);
 }
 
-void launch_explicit_v(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_explicit_v<<<g.N - 1, 128, sizeof(double) * (g.M + 3), s>>>(g, p);
+// The line kernels below take `threads` per CTA (a multiple of 32, at least 64), chosen
+// by the caller from the longest span of the direction.
+void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s) {
+    k_explicit_v<<<g.N - 1, threads, sizeof(double) * (g.M + 3), s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
-void launch_explicit_u(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_explicit_u<<<g.M - 1, 128, sizeof(double) * (g.N + 3), s>>>(g, p);
+void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s) {
+    k_explicit_u<<<g.M - 1, threads, sizeof(double) * (g.N + 3), s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
-void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, cudaStream_t s) {
-    k_reset<1><<<g.N, 128, reset_smem(g.M), s>>>(g, p, force);
+void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s) {
+    k_reset<1><<<g.N, threads, reset_smem(g.M), s>>>(g, p, force);
     hyd_kernel_launches_add(1);
 }
 
-void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, cudaStream_t s) {
-    k_reset<0><<<g.M, 128, reset_smem(g.N), s>>>(g, p, force);
+void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s) {
+    k_reset<0><<<g.M, threads, reset_smem(g.N), s>>>(g, p, force);
     hyd_kernel_launches_add(1);
 }
 
-void launch_post(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+void launch_post(const DevGrid& g, const DevParams& p, int full, cudaStream_t s) {
     const dim3 b(32, 8);
-    k_post<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, 1);
+    if (full) k_post<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, 1);
+    else k_post_span<<<row_warps_blocks(g.N + 1), 256, 0, s>>>(g);
     hyd_kernel_launches_add(1);
 }
 
@@ -1069,15 +1182,17 @@ void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s) {
     hyd_kernel_launches_add(1);
 }
 
-void launch_vth_hesok(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s) {
     const dim3 b(32, 8);
-    k_vth_hesok<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
+    if (full) k_vth_hesok<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
+    else k_vth_span<<<row_warps_blocks(g.N + 1), 256, 0, s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
-void launch_update_fs(const DevGrid& g, cudaStream_t s) {
+void launch_update_fs(const DevGrid& g, int full, cudaStream_t s) {
     const dim3 b(32, 8);
-    k_update_fs<<<grid2d(g.M, g.N, b), b, 0, s>>>(g);
+    if (full) k_update_fs<<<grid2d(g.M, g.N, b), b, 0, s>>>(g);
+    else k_update_fs_span<<<row_warps_blocks(g.N), 256, 0, s>>>(g);
     hyd_kernel_launches_add(1);
 }
 

@@ -564,28 +564,39 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
 }
 
 // Line kernel: warp w of CTA b sweeps line startidx + 4b + w, or lists it as long.
+// All warps of the CTA set up, meet at a barrier, and then sweep; a warp with nothing to
+// sweep waits at the closing barrier instead of exiting.  Without the two barriers the
+// warp-synchronous steps of a lone working warp were measured an order of magnitude
+// slower on B200.
 template <int DIR, int SOLVER>
 __global__ void __launch_bounds__(kT) k_hydro_lines(DevGrid g, DevParams p, int startidx, int endidx) {
     extern __shared__ double dyn_smem[];
     __shared__ LineShared sgw[kWarps];
     const int w = threadIdx.x >> 5;
     const int line = startidx + blockIdx.x * kWarps + w;
-    if (line > endidx) return;  // the whole warp; only warp-level barriers follow
     LineShared& sg = sgw[w];
-    hydro_setup<DIR, WarpG>(g, p, line, sg);
-    if (sg.nseg == 0) return;
-    if (sg.R > kRowW || sg.C > kCellW) {
-        if ((threadIdx.x & 31) == 0) long_push(g, line);
-        return;
+    bool work = line <= endidx;  // warp-uniform
+    if (work) {
+        hydro_setup<DIR, WarpG>(g, p, line, sg);
+        if (sg.nseg == 0) {
+            work = false;
+        } else if (sg.R > kRowW || sg.C > kCellW) {
+            if ((threadIdx.x & 31) == 0) long_push(g, line);
+            work = false;
+        }
     }
-    double* A = dyn_smem + w * kWarpHydro;
-    double* B = A + kRowW;
-    double* Cc = B + kRowW;
-    double* D = Cc + kRowW;
-    double* a2 = D + kRowW;
-    double* c2 = a2 + kCellW;
-    double* d2 = c2 + kCellW;
-    hydro_body<DIR, SOLVER, WarpG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, nullptr, chunk_len(sg.R, 32));
+    __syncthreads();
+    if (work) {
+        double* A = dyn_smem + w * kWarpHydro;
+        double* B = A + kRowW;
+        double* Cc = B + kRowW;
+        double* D = Cc + kRowW;
+        double* a2 = D + kRowW;
+        double* c2 = a2 + kCellW;
+        double* d2 = c2 + kCellW;
+        hydro_body<DIR, SOLVER, WarpG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, nullptr, chunk_len(sg.R, 32));
+    }
+    __syncthreads();
 }
 
 // Long-line kernel: CTA b sweeps listed lines b, b + gridDim.x, ...  Shared memory holds
@@ -812,25 +823,33 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     }
 }
 
+// Sediment line kernel: as k_hydro_lines.
 template <int DIR, int SOLVER>
 __global__ void __launch_bounds__(kT) k_fs_lines(DevGrid g, DevParams p, int half, int startidx, int endidx) {
     extern __shared__ double dyn_smem[];
     __shared__ LineShared sgw[kWarps];
     const int w = threadIdx.x >> 5;
     const int line = startidx + blockIdx.x * kWarps + w;
-    if (line > endidx) return;
     LineShared& sg = sgw[w];
-    fs_setup<DIR, WarpG>(g, p, line, sg);
-    if (sg.R == 0) return;
-    if (sg.R > kRowWf) {
-        if ((threadIdx.x & 31) == 0) long_push(g, line);
-        return;
+    bool work = line <= endidx;  // warp-uniform
+    if (work) {
+        fs_setup<DIR, WarpG>(g, p, line, sg);
+        if (sg.R == 0) {
+            work = false;
+        } else if (sg.R > kRowWf) {
+            if ((threadIdx.x & 31) == 0) long_push(g, line);
+            work = false;
+        }
     }
-    double* A = dyn_smem + w * kWarpFs;
-    double* B = A + kRowW;
-    double* Cc = B + kRowW;
-    double* D = Cc + kRowW;
-    fs_body<DIR, SOLVER, WarpG>(g, p, half, line, sg, A, B, Cc, D, nullptr, chunk_len(sg.R, 32));
+    __syncthreads();
+    if (work) {
+        double* A = dyn_smem + w * kWarpFs;
+        double* B = A + kRowW;
+        double* Cc = B + kRowW;
+        double* D = Cc + kRowW;
+        fs_body<DIR, SOLVER, WarpG>(g, p, half, line, sg, A, B, Cc, D, nullptr, chunk_len(sg.R, 32));
+    }
+    __syncthreads();
 }
 
 template <int DIR, int SOLVER>
