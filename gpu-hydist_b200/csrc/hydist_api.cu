@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 #include <utility>
 #include <cmath>
 #include <cstdio>
@@ -310,6 +311,13 @@ __global__ void k_mass_final(const double* part, int nblocks, double* out) {
         for (int k = 0; k < 5; k++) acc[k] += part[b * 5 + k];
     for (int k = 0; k < 5; k++) out[k] = acc[k];
 }
+
+// Scratch of hyd_mass_balance_noalloc: up to HYD_MASS_NOALLOC_MAX_BLOCKS blocks of five
+// partial sums, then the five totals.  Looked up once per device.
+static __device__ __align__(256) double g_mass_scratch[HYD_MASS_NOALLOC_MAX_BLOCKS * 5 + 5];
+constexpr int kMaxDevices = 64;
+double* g_mass_scratch_ptr[kMaxDevices];
+std::mutex g_mass_scratch_mu;
 
 }  // namespace
 
@@ -804,6 +812,40 @@ int hyd_mass_balance(hyd_handle h, double* out, int n) {
     double r[5];
     CUDA_TRY(cudaMemcpyAsync(r, part + nb * 5, sizeof r, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaFreeAsync(part, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const double area = h->P.dX * h->P.dY;
+    out[0] = r[0] * area;
+    out[1] = r[1] * area;
+    out[2] = r[2] * area;
+    out[3] = r[3];
+    out[4] = r[4];
+    return HYD_OK;
+}
+
+int hyd_mass_balance_noalloc(hyd_handle h, int nblocks, double* out, int n) {
+    if (!h || !out || n < 5) return fail(HYD_EINVAL, "need 5 output slots");
+    if (nblocks < 1 || nblocks > HYD_MASS_NOALLOC_MAX_BLOCKS)
+        return fail(HYD_EINVAL, "nblocks must be in 1.." + std::to_string(HYD_MASS_NOALLOC_MAX_BLOCKS) +
+                                    " (the static scratch holds that many blocks of partial sums)");
+    if (h->device < 0 || h->device >= kMaxDevices) return fail(HYD_EINVAL, "device index beyond the scratch table");
+    CUDA_TRY(cudaSetDevice(h->device));
+    double* part = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mass_scratch_mu);
+        if (!g_mass_scratch_ptr[h->device]) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_mass_scratch);
+            if (e != cudaSuccess) return fail(HYD_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_mass_scratch_ptr[h->device] = (double*)p;
+        }
+        part = g_mass_scratch_ptr[h->device];
+    }
+    k_mass_partial<<<nblocks, 256, 0, h->stream>>>(h->g, part);
+    k_mass_final<<<1, 32, 0, h->stream>>>(part, nblocks, part + nblocks * 5);
+    hyd_kernel_launches_add(2);
+    CUDA_TRY(cudaGetLastError());
+    double r[5];
+    CUDA_TRY(cudaMemcpyAsync(r, part + nblocks * 5, sizeof r, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     const double area = h->P.dX * h->P.dY;
     out[0] = r[0] * area;

@@ -178,6 +178,27 @@ int hyd_synchronize(hyd_handle h);
  */
 int hyd_mass_balance(hyd_handle h, double* out, int n);
 
+/*
+ * hyd_mass_balance_noalloc — the sums of hyd_mass_balance (same out[0..4]) computed
+ * without any allocation: the per-block partial sums live in a fixed device array of
+ * HYD_MASS_NOALLOC_MAX_BLOCKS * 5 + 5 doubles (41 KB) instead of a per-call
+ * cudaMallocAsync.  No counterpart in the reference (its hourly check copies whole
+ * fields to the host, Engine.py:402).  For callers that must not touch the device
+ * allocator between steps, e.g. a monitor running while another allocator (a framework's
+ * caching pool) holds the device memory, where a per-call allocation can fail or force
+ * the pool to trim mid-run.
+ *   nblocks: number of partial-sum blocks, 1..HYD_MASS_NOALLOC_MAX_BLOCKS; HYD_EINVAL
+ *            beyond.  nblocks = 148 sums in the order hyd_mass_balance uses.
+ * Nothing in the array needs to start at zero (every partial is written before it is
+ * read).  The array is one per device and process, shared by all handles on that
+ * device: overlapping calls (from two threads, or on two streams not ordered with each
+ * other) race on it and must be serialised by the caller.  The first call on a device
+ * looks the array up with cudaGetSymbolAddress and must not be made while a stream on
+ * that device is being captured.
+ */
+#define HYD_MASS_NOALLOC_MAX_BLOCKS 1024
+int hyd_mass_balance_noalloc(hyd_handle h, int nblocks, double* out, int n);
+
 /* Size in bytes of a checkpoint image, and checkpoint save/restore (replaces the
  * text pick-up of rep.py:43-55 with an exact binary image of every prognostic
  * field, the wet mask, the segment tables and the time). */
