@@ -634,11 +634,17 @@ int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const
     return HYD_OK;
 }
 
-int hyd_init(hyd_handle h, double t_start) {
-    if (!h) return fail(HYD_EINVAL, "null handle");
+static int init_common(HydSim* h, double t_start, int pickup) {
     if (!h->have_boundary) return fail(HYD_ESTATE, "hyd_set_boundary must precede hyd_init");
     CUDA_TRY(cudaSetDevice(h->device));
-    launch_init_kernels(h->g, h->dp, h->stream);
+    const int* keep = nullptr;
+    if (pickup) {
+        // the caller's mask, parked in a smoothing partner (rewritten by the first step)
+        CUDA_TRY(cudaMemcpyAsync(h->scratch_u, h->g.khouot, sizeof(int) * (size_t)(h->N + 3) * h->pitch,
+                                 cudaMemcpyDeviceToDevice, h->stream));
+        keep = (const int*)h->scratch_u;
+    }
+    launch_init_kernels(h->g, h->dp, keep, h->stream);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->t = t_start;
@@ -650,6 +656,16 @@ int hyd_init(hyd_handle h, double t_start) {
     rc = set_clock(h, t_start);
     if (rc) return rc;
     return check_device_status(h);
+}
+
+int hyd_init(hyd_handle h, double t_start) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    return init_common(h, t_start, 0);
+}
+
+int hyd_init_pickup(hyd_handle h, double t_start) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    return init_common(h, t_start, 1);
 }
 
 // The launch sequence of one full step (Engine.py:144-366).  sed1/sed2: sediment phase

@@ -107,7 +107,7 @@ __device__ __forceinline__ int find_seg_u(const DevGrid& g, int row, int col, in
 
 // Host launch wrappers (defined in the .cu files, called by hydist_api.cu).
 struct StepLaunch;
-void launch_init_kernels(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_mask, cudaStream_t s);
 void launch_clock(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 // Launch shapes of the sweeps for one grid (k_sweep.cu).

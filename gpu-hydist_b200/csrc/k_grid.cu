@@ -1105,10 +1105,14 @@ void launch_mark_all_cols(const DevGrid& g, cudaStream_t s) {
     hyd_kernel_launches_add(1);
 }
 
-void launch_init_kernels(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+// keep_mask: when not null, a saved mask (pitched like khouot) copied over the one
+// Onetime_init derives, before the scans (the pick-up order of rep.py:126-131).
+void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_mask, cudaStream_t s) {
     const dim3 b(32, 8);
     k_onetime_init<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p);
     hyd_kernel_launches_add(1);
+    if (keep_mask)
+        cudaMemcpyAsync(g.khouot, keep_mask, sizeof(int) * (size_t)(g.N + 3) * g.P, cudaMemcpyDeviceToDevice, s);
     launch_spans(g, s);
     clear_rescan_lists(g, s);
     k_mark_all<1><<<(g.N + 3 + 255) / 256, 256, 0, s>>>(g);

@@ -26,7 +26,9 @@ def gpu_init(case, device_no=0, pick_up=False, pickup_dirs=None):
     if pick_up:
         from .io import load_initial_condition
         load_initial_condition(sim, pickup_dirs, case)
-    sim.init(case.t_start)
+        sim.init_pickup(case.t_start)
+    else:
+        sim.init(case.t_start)
     return sim, None, None, None, None
 
 

@@ -43,6 +43,7 @@ def load():
         "hyd_set_boundary": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int]),
         "hyd_init": (ctypes.c_int, [H, ctypes.c_double]),
+        "hyd_init_pickup": (ctypes.c_int, [H, ctypes.c_double]),
         "hyd_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
         "hyd_get_time": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double)]),
         "hyd_set_params": (ctypes.c_int, [H, ctypes.POINTER(HydCaseParams)]),
@@ -147,6 +148,10 @@ class Simulation:
 
     def init(self, t_start=0.0):
         _check(self.lib.hyd_init(self.h, float(t_start)))
+
+    def init_pickup(self, t_start=0.0):
+        """hyd_init keeping the mask set with set("khouot", ...) (rep.py:126-131)."""
+        _check(self.lib.hyd_init_pickup(self.h, float(t_start)))
 
     def step(self, n=1, sync=True):
         t = ctypes.c_double()

@@ -142,6 +142,14 @@ int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const
  */
 int hyd_init(hyd_handle h, double t_start);
 
+/* hyd_init_pickup — hyd_init for a run picked up from saved fields (rep.py:126-131):
+ * the wet/dry mask set with hyd_set_field("khouot", ...) before the call replaces the
+ * one Onetime_init derives from h; then the segment scans, Htuongdoi and
+ * preprocess_data run on it, as in the reference, which loads the pick-up files between
+ * Onetime_init and the scans.  u, v, z, FS set before the call are kept (Onetime_init
+ * does not touch them). */
+int hyd_init_pickup(hyd_handle h, double t_start);
+
 /*
  * Advance `nsteps` full ADI steps (two half-steps each, with the sediment ADI
  * and the Exner update when their start times are reached): the body of the

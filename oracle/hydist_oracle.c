@@ -486,6 +486,22 @@ static void k_preprocess(OraSim* s) {
     if (s->hmax_r != 0) s->hmax_r = 1.0 / (ros * s->hmax_r);
 }
 
+/* rep.py:126-131 with pick_up: the mask loaded from the pick-up files replaces the one
+ * Onetime_init derives, before the segment scans, Htuongdoi and preprocess_data. */
+void ora_init_pickup(OraSim* s, double t_start) {
+    const size_t n = (size_t)(s->N + 3) * (s->M + 3);
+    int* keep = (int*)malloc(n * sizeof(int));
+    memcpy(keep, s->khouot, n * sizeof(int));
+    k_onetime_init(s);
+    memcpy(s->khouot, keep, n * sizeof(int));
+    free(keep);
+    k_limits_horizontal(s);
+    k_limits_vertical(s);
+    k_htuongdoi(s);
+    k_preprocess(s);
+    s->t = t_start;
+}
+
 void ora_init(OraSim* s, double t_start) {
     k_onetime_init(s);
     k_limits_horizontal(s);

@@ -35,6 +35,8 @@ int ora_set_boundary(OraSim* s, const int* boundary_type, const double* const* t
 
 /* rep.py:126-139 */
 void ora_init(OraSim* s, double t_start);
+/* rep.py:126-131 with pick_up: keeps the mask set before the call */
+void ora_init_pickup(OraSim* s, double t_start);
 /* Engine.py:144-366, nsteps iterations of the while loop */
 void ora_step(OraSim* s, int nsteps);
 double ora_time(const OraSim* s);

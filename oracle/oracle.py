@@ -81,6 +81,7 @@ class OracleSim:
         lib.ora_set_boundary.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         lib.ora_init.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.ora_init_pickup.argtypes = [ctypes.c_void_p, ctypes.c_double]
         lib.ora_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.ora_time.restype = ctypes.c_double
         lib.ora_time.argtypes = [ctypes.c_void_p]
@@ -121,6 +122,10 @@ class OracleSim:
 
     def init(self):
         self.lib.ora_init(self.h, float(self.case.t_start))
+
+    def init_pickup(self):
+        """Initialise keeping the mask written into view("khouot") (rep.py:126-131)."""
+        self.lib.ora_init_pickup(self.h, float(self.case.t_start))
 
     def step(self, n):
         self.lib.ora_step(self.h, int(n))
@@ -168,6 +173,7 @@ class RefSim:
         lib.ref_set_boundary.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         lib.ref_init.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.ref_init_pickup.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
         lib.ref_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.ref_time.restype = ctypes.c_double
         lib.ref_time.argtypes = [ctypes.c_void_p]
@@ -200,6 +206,11 @@ class RefSim:
 
     def init(self):
         self._check(self.lib.ref_init(self.h, float(self.case.t_start)))
+
+    def init_pickup(self, mask):
+        """Initialise with a pick-up mask loaded after Onetime_init (rep.py:126-131)."""
+        m = np.ascontiguousarray(mask, dtype=np.int32)
+        self._check(self.lib.ref_init_pickup(self.h, float(self.case.t_start), m.ctypes.data))
 
     def step(self, n):
         self._check(self.lib.ref_step(self.h, int(n)))

@@ -421,6 +421,27 @@ int ref_init(void* h, double t_start) {
     return g_err ? -2 : 0;
 }
 
+/* rep.py:126-131 with pick_up: Onetime_init, then the pick-up mask copied to the device
+ * (load_intial_condition's toDevice), then the scans, Htuongdoi and preprocess_data. */
+int ref_init_pickup(void* h, double t_start, const int* mask) {
+    RefSim* s = (RefSim*)h;
+    const int N = s->N, M = s->M;
+    Argument_Pointers* arg = s->arg;
+    const dim3 b2((unsigned)(M + 3 < 32 ? M + 3 : 32), 1, 1);
+    const dim3 g2((unsigned)((M + 3) / (M + 3 < 32 ? M + 3 : 32) + 1), (unsigned)(N + 3), 1);
+    LAUNCH(Onetime_init, g2, b2, arg);
+    SYNC();
+    ref_copy_in(s->host_arg.khouot, mask, sizeof(int) * (size_t)(N + 3) * (M + 3));
+    LAUNCH(Find_Calculation_limits_Horizontal, dim3(1, N, 1), RED32, arg);
+    LAUNCH(Find_Calculation_limits_Vertical, dim3(1, M, 1), RED32, arg);
+    LAUNCH(Htuongdoi, g2, b2, arg);
+    SYNC();
+    LAUNCH(preprocess_data, dim3(1, 1, 1), RED32, arg);
+    SYNC();
+    s->t = t_start;
+    return g_err ? -2 : 0;
+}
+
 /* Engine.py:144-366, nsteps iterations of the while loop */
 int ref_step(void* h, int nsteps) {
     RefSim* s = (RefSim*)h;

@@ -37,13 +37,29 @@ def golden_cases():
     return [c1, c2, c3, c4, c5]
 
 
-def main():
+# The shipped Tan Chau reach (the reference's Inputs/TanChau), with sediment from 20 s and
+# the bed update at 40 s so that every part of the step runs on the real inputs.  Its
+# fixture keeps the prognostic fields and the segment tables only (size).
+TANCHAU_OUT = ("z", "u", "v", "FS", "dH", "khouot", "daui", "cuoii", "moci", "dauj", "cuoij", "mocj")
+
+
+def tanchau_golden(ref_root):
+    from hydist import io
+    c = io.tanchau_case(os.path.join(ref_root, "Inputs", "TanChau"))
+    c.params.sediment_start = 20.0
+    c.params.bed_change_start = 40.0
+    c.nsteps = 60
+    return c
+
+
+def main(ref_root="/root/reference"):
     oracle.build(("ref_cpu",))
-    for c in golden_cases():
+    todo = [(c, golden.OUT_FIELDS) for c in golden_cases()] + [(tanchau_golden(ref_root), TANCHAU_OUT)]
+    for c, fields in todo:
         r = oracle.RefSim(c)
         r.init()
         r.step(c.nsteps)
-        out = {f: r.get(f) for f in golden.OUT_FIELDS}
+        out = {f: r.get(f) for f in fields}
         path = os.path.join(HERE, c.name + ".npz")
         golden.save(path, c, out)
         print("wrote", path, "t =", r.t, "bytes", os.path.getsize(path))
