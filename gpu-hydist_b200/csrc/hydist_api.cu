@@ -101,6 +101,10 @@ struct HydSim {
     int thr_r, thr_c;
     cudaGraphExec_t graph[8];
     long long graph_kernels[8];
+    // timing with graphs: one graph per variant with the phase events captured in it
+    cudaGraphExec_t tgraph[8];
+    std::vector<Mark> tmarks[8];
+    std::vector<Mark>* mark_sink;  // where PhaseScope files its events (null: marks)
 };
 
 static const char* kPhaseNames[] = {"boundary", "sweep_uz", "sweep_vz", "smooth", "explicit_v", "explicit_u",
@@ -114,6 +118,13 @@ void drop_graphs(HydSim* s) {
     for (int k = 0; k < 8; k++) {
         if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
         s->graph[k] = nullptr;
+        if (s->tgraph[k]) cudaGraphExecDestroy(s->tgraph[k]);
+        s->tgraph[k] = nullptr;
+        for (auto& m : s->tmarks[k]) {
+            cudaEventDestroy(m.a);
+            cudaEventDestroy(m.b);
+        }
+        s->tmarks[k].clear();
     }
 }
 
@@ -165,17 +176,22 @@ struct PhaseScope {
     HydSim* s;
     int ph;
     cudaEvent_t a = nullptr;
+    // inside a capture an event record is an ordering edge unless marked external
+    static void record(HydSim* s, cudaEvent_t e) {
+        if (s->mark_sink) cudaEventRecordWithFlags(e, s->stream, cudaEventRecordExternal);
+        else cudaEventRecord(e, s->stream);
+    }
     PhaseScope(HydSim* s_, int ph_) : s(s_), ph(ph_) {
         if (s->timing) {
             a = pool_event(s);
-            cudaEventRecord(a, s->stream);
+            record(s, a);
         }
     }
     ~PhaseScope() {
         if (s->timing) {
             cudaEvent_t b = pool_event(s);
-            cudaEventRecord(b, s->stream);
-            s->marks.push_back({ph, a, b});
+            record(s, b);
+            (s->mark_sink ? *s->mark_sink : s->marks).push_back({ph, a, b});
         }
     }
 };
@@ -732,12 +748,19 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     s->end_idx = end_idx;
 }
 
-// The captured graph of one step variant (built on first use).
-static cudaGraphExec_t step_graph(HydSim* s, int mask) {
-    if (s->graph[mask]) return s->graph[mask];
+// The captured graph of one step variant (built on first use).  timed: the variant with
+// the phase events captured in it (their pairs are read after each replay).
+static cudaGraphExec_t step_graph(HydSim* s, int mask, int timed = 0) {
+    cudaGraphExec_t* slot = timed ? &s->tgraph[mask] : &s->graph[mask];
+    if (*slot) return *slot;
     const long long before = hyd_kernel_launches_add(0);
-    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return nullptr;
+    if (timed) s->mark_sink = &s->tmarks[mask];
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        s->mark_sink = nullptr;
+        return nullptr;
+    }
     launch_step(s, mask & 1, (mask >> 1) & 1, (mask >> 2) & 1);
+    s->mark_sink = nullptr;
     cudaGraph_t graph = nullptr;
     if (cudaStreamEndCapture(s->stream, &graph) != cudaSuccess || !graph) return nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -747,7 +770,7 @@ static cudaGraphExec_t step_graph(HydSim* s, int mask) {
     const long long after = hyd_kernel_launches_add(0);
     s->graph_kernels[mask] = after - before;
     hyd_kernel_launches_add(-(after - before));
-    s->graph[mask] = exec;
+    *slot = exec;
     return exec;
 }
 
@@ -776,10 +799,20 @@ int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
         const int full_s = (sed1 || sed2) ? (h->full_pending >> 1) & 1 : 0;
         h->full_pending &= ~(full_h | (full_s << 1));
         const int special = force || full_h || full_s;
-        cudaGraphExec_t exec = (h->use_graphs && !h->timing && !special) ? step_graph(h, mask) : nullptr;
+        cudaGraphExec_t exec = (h->use_graphs && !special) ? step_graph(h, mask, h->timing) : nullptr;
         if (exec) {
             CUDA_TRY(cudaGraphLaunch(exec, h->stream));
             hyd_kernel_launches_add(h->graph_kernels[mask]);
+            if (h->timing) {
+                // the replay's phase events, read before the next replay reuses them
+                CUDA_TRY(cudaStreamSynchronize(h->stream));
+                for (auto& m : h->tmarks[mask]) {
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, m.a, m.b);
+                    h->phase_ms[m.phase] += ms;
+                    h->phase_n[m.phase] += 1;
+                }
+            }
         } else {
             launch_step(h, sed1, sed2, bed, force, full_h, full_s);
         }
