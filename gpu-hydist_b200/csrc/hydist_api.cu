@@ -446,7 +446,6 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     total += 2 * a256(nseg_rows * 4) + a256((N + 3) * 4) + 2 * a256(nseg_cols * 4) + a256((M + 3) * 4);
     total += 2 * a256((M + 3) * 8) + 2 * a256((N + 3) * 8) + a256((2 * (N + 3) + 2 * (M + 3)) * 8);
     total += a256(4 * 8) + a256(4 * 4) + a256(4 * HYD_SEGL * 4) + a256(64) + a256(64);
-    total += a256(((N > M ? N : M) + 3) * 4) + a256(64);  // long-line list and counters
     total += 4 * a256((N + 3) * 4) + 4 * a256((M + 3) * 4) + a256(64);  // spans, rescan flags and lists
     total += 2 * a256((N + 3) * 4) + a256(64);                          // extended spans
     e = cudaMalloc(&s->arena, total);
@@ -491,8 +490,6 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.bienQ = (int*)take(4 * 4);
     g.btype = (int*)take(4 * HYD_SEGL * 4);
     g.status = (unsigned*)take(64);
-    g.long_list = (int*)take(((N > M ? N : M) + 3) * 4);
-    g.long_ctr = (unsigned*)take(64);
     g.rlo = (int*)take((N + 3) * 4);
     g.rhi = (int*)take((N + 3) * 4);
     g.dirty_r = (int*)take((N + 3) * 4);
@@ -520,6 +517,15 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         cudaStreamDestroy(s->stream);
         delete s;
         return fail(HYD_ECUDA, std::string("shared-memory set-up: ") + cudaGetErrorString(e));
+    }
+    s->g.LT = (N + 3 + 31) / 32 * 32;
+    s->g.colT_stride = (size_t)(M + 3) * s->g.LT;
+    e = cudaMalloc(&s->g.colT, 7 * s->g.colT_stride * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(s->arena);
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return fail(HYD_ENOMEM, std::string("column-major scratch: ") + cudaGetErrorString(e));
     }
     s->sweep_scratch = nullptr;
     e = cudaMalloc(&s->sweep_scratch, s->plan.scratch_doubles * sizeof(double));
@@ -552,6 +558,7 @@ int hyd_destroy(hyd_handle h) {
     for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
     drop_graphs(h);
     cudaFree(h->sweep_scratch);
+    cudaFree(h->g.colT);
     cudaFree(h->arena);
     cudaStreamDestroy(h->stream);
     delete h;
@@ -700,7 +707,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         start_idx = 3;
         end_idx = s->M - 1;
     }
-    { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
+    { PHASE(PH_SWEEP_UZ); launch_coef_uz(g, p, st); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_EXPL_V); launch_explicit_v(g, p, s->thr_r, st); }
@@ -712,7 +719,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     { PHASE(PH_SCAN); launch_scan_cols(g, p, st); }
     if (sed1) {
         { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
-        { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
+        { PHASE(PH_FS_J); launch_coef_fsj(g, p, 0, st); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
     }
     // ---- half-step 2: implicit along j (rows), explicit u
@@ -726,7 +733,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, st); }
     std::swap(g.t_v, s->scratch_v);
-    { PHASE(PH_EXPL_U); launch_explicit_u(g, p, s->thr_c, st); }
+    { PHASE(PH_EXPL_U); launch_coef_eu(g, p, st); launch_explicit_u(g, p, s->thr_c, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }

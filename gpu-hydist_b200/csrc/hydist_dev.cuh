@@ -44,8 +44,6 @@ struct DevGrid {
     int *bienQ, *btype;                          // bienQ[4], btype[4*20]
     double *bc[4], *cc[4];                       // [nseg][total_time] per edge
     unsigned* status;
-    int* long_list;      // lines listed for the long-line sweep kernels
-    unsigned* long_ctr;  // [0] listed lines, [1] CTAs of the long-line kernel done
     // span of the cells whose mask is not 2 (those never change) per row / column
     int *rlo, *rhi, *clo, *chi;
     // extended span per row (every cell within a few cells of those), where the
@@ -55,10 +53,18 @@ struct DevGrid {
     // lines whose mask changed since their segments were scanned: flags and lists
     int *dirty_r, *dirty_c, *dlist_r, *dlist_c;
     unsigned* dctr;  // [0] listed rows, [1] listed columns, [2] [3] CTAs of the rescans done
+    // column-major copies of per-cell quantities for the column sweeps: 7 arrays of
+    // (M+3) columns x LT rows (LT = N+3 rounded up to 32), array k at colT + k*colT_stride
+    double* colT;
+    size_t colT_stride;
+    int LT;
     double* clock;  // [0] time of half-step 1, [1] time of half-step 2, [2] time at the step start
 };
 
 __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { atomicOr(g.status, bit); }
+
+// Column-major copy k of a per-cell quantity; (row i, column j) is at [j * g.LT + i].
+__device__ __forceinline__ double* colT(const DevGrid& g, int k) { return g.colT + (size_t)k * g.colT_stride; }
 
 // Wall/open flags of a row segment [first, last] (locate_segment_v, constant.cuh:135-154).
 __device__ __forceinline__ void seg_flags_v(const DevGrid& g, const DevParams& p, int row, int first, int last,
@@ -112,11 +118,10 @@ void launch_clock(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 // Launch shapes of the sweeps for one grid (k_sweep.cu).
 struct SweepPlan {
-    size_t smem_lines, smem_fs_lines;  // line kernels (one warp per line)
-    size_t smem_long, smem_fs_long;    // long-line kernels
+    size_t smem_lines, smem_fs_lines;  // dynamic shared memory of the hydrodynamic / sediment sweeps
     int RB, CB, RBf;                   // rows / cells of a long line held in shared memory
     int RG, CG, RGf;                   // rows / cells of a CTA's global scratch region
-    int long_grid;                     // CTAs of the long-line kernels
+    int long_grid;                     // CTAs of the sweeps
     int need_global;                   // some line may exceed shared memory
     size_t scratch_doubles;            // global scratch to allocate
 };
@@ -130,6 +135,7 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
 void launch_widen_spans(const DevGrid& g, cudaStream_t s);
 void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
 void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
+void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_spans(const DevGrid& g, cudaStream_t s);
@@ -139,6 +145,8 @@ void launch_post(const DevGrid& g, const DevParams& p, int full, cudaStream_t s)
 void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
+void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
                        double* scratch, cudaStream_t s);
 void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,

@@ -384,6 +384,55 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
 
 // solveU/uSolver (UVZSolver_multithread.cu:947-968, 773-815) on column j, then
 // update_margin_elem_U (970-1006).
+// uSolver (UVZSolver_multithread.cu:773-815) for one cell: the new u velocity.  Cell-local,
+// so it is computed for every wet cell by a row-major kernel and stored column-major.
+__device__ __forceinline__ double eu_cell(const DevGrid& g, const DevParams& p, int row, int col) {
+    const int P = g.P;
+    const double *u = g.u, *v = g.v, *z = g.z, *t_v = g.t_v, *H = g.H_moi;
+    const int o = P;
+    double pp, q, tmp;
+    pp = 0;
+    q = 0;
+    tmp = 0;
+    const double vtb = (v[row * o + col - 1] + v[row * o + col] + v[(row + 1) * o + col - 1] + v[(row + 1) * o + col]) * 0.25;
+    const double t_vtb = (t_v[row * o + col - 1] + t_v[row * o + col] + t_v[(row + 1) * o + col - 1] + t_v[(row + 1) * o + col]) * 0.25;
+    pp = (u[(row + 1) * o + col] - u[(row - 1) * o + col]) / p.dX2;
+    pp = (p.HaiChiadT + pp + g.Kx1[row * o + col] * sqrt(vtb * vtb + u[row * o + col] * u[row * o + col]) / g.Htdu[row * o + col]);
+    if (H[row * o + col - 1] <= p.H_TINH) {
+        if (vtb < 0) {
+            q = t_vtb * (-3 * u[row * o + col] + 4 * u[row * o + col + 1] - u[row * o + col + 2]) / p.dY2;
+            tmp = (u[row * o + col] - 2 * u[row * o + col + 1] + u[row * o + col + 2]) / p.dYbp;
+        }
+    } else {
+        if (H[row * o + col + 1] <= p.H_TINH) {
+            if ((H[row * o + col - 2] > p.H_TINH) && (vtb > 0)) {
+                q = t_vtb * (3 * u[row * o + col] - 4 * u[row * o + col - 1] + u[row * o + col - 2]) / p.dY2;
+                tmp = (u[row * o + col] - 2 * u[row * o + col - 1] + u[row * o + col - 2]) / p.dYbp;
+            }
+        } else {
+            q = t_vtb * (u[row * o + col + 1] - u[row * o + col - 1]) / p.dY2;
+            tmp = (u[row * o + col + 1] - 2 * u[row * o + col] + u[row * o + col - 1]) / p.dYbp;
+        }
+    }
+    q = p.HaiChiadT * u[row * o + col] - q + p.CORIOLIS_FORCE * t_vtb;
+    q = (q - p.g * (z[(row + 1) * o + col] - z[row * o + col]) / p.dX +
+         g.VISC[row * o + col] * (tmp + (u[(row + 1) * o + col] - 2 * u[row * o + col] + u[(row - 1) * o + col]) / p.dXbp)) +
+        (p.windx - g.Tsxw[row * o + col]) / g.Htdu[row * o + col];
+    return q / pp;
+}
+
+// explicit_u values of every wet cell of rows 2..N-1, columns 2..M, one warp per row over
+// the row's span; written column-major (g.colT array 0).
+__global__ void k_coef_eu(DevGrid g, DevParams p) {
+    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i > g.N - 1) return;
+    const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
+    for (int j = lo + lane; j <= hi; j += 32) {
+        if (g.khouot[i * g.P + j] != 0) continue;
+        colT(g, 0)[(size_t)j * g.LT + i] = eu_cell(g, p, i, j);
+    }
+}
+
 __global__ void k_explicit_u(DevGrid g, DevParams p) {
     extern __shared__ double su[];  // the column's t_u over [k0, k1]
     __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL], s_first[HYD_SEGL], s_last[HYD_SEGL], s_off[HYD_SEGL + 1];
@@ -391,7 +440,6 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
     const int P = g.P, N = g.N;
     const int nseg = g.mocj[col];
     if (nseg == 0) return;
-    const double *u = g.u, *v = g.v, *z = g.z, *t_v = g.t_v, *H = g.H_moi;
     const int k0 = max(g.dauj[col * HYD_SEGL] - 2, 0);
     const int k1 = min(g.cuoij[col * HYD_SEGL + nseg - 1] + 1, N + 2);
     for (int i = k0 + threadIdx.x; i <= k1; i += blockDim.x) su[i - k0] = g.t_u[i * P + col];
@@ -420,37 +468,8 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
             int k = 0;
             while (k + 1 < nseg && s_off[k + 1] <= c) k++;
             const int row = s_first[k] + (c - s_off[k]);
-            const int o = P;
-            double pp, q, tmp;
-            pp = 0;
-            q = 0;
-            tmp = 0;
-            const double vtb = (v[row * o + col - 1] + v[row * o + col] + v[(row + 1) * o + col - 1] + v[(row + 1) * o + col]) * 0.25;
-            const double t_vtb = (t_v[row * o + col - 1] + t_v[row * o + col] + t_v[(row + 1) * o + col - 1] + t_v[(row + 1) * o + col]) * 0.25;
-            pp = (u[(row + 1) * o + col] - u[(row - 1) * o + col]) / p.dX2;
-            pp = (p.HaiChiadT + pp + g.Kx1[row * o + col] * sqrt(vtb * vtb + u[row * o + col] * u[row * o + col]) / g.Htdu[row * o + col]);
-            if (H[row * o + col - 1] <= p.H_TINH) {
-                if (vtb < 0) {
-                    q = t_vtb * (-3 * u[row * o + col] + 4 * u[row * o + col + 1] - u[row * o + col + 2]) / p.dY2;
-                    tmp = (u[row * o + col] - 2 * u[row * o + col + 1] + u[row * o + col + 2]) / p.dYbp;
-                }
-            } else {
-                if (H[row * o + col + 1] <= p.H_TINH) {
-                    if ((H[row * o + col - 2] > p.H_TINH) && (vtb > 0)) {
-                        q = t_vtb * (3 * u[row * o + col] - 4 * u[row * o + col - 1] + u[row * o + col - 2]) / p.dY2;
-                        tmp = (u[row * o + col] - 2 * u[row * o + col - 1] + u[row * o + col - 2]) / p.dYbp;
-                    }
-                } else {
-                    q = t_vtb * (u[row * o + col + 1] - u[row * o + col - 1]) / p.dY2;
-                    tmp = (u[row * o + col + 1] - 2 * u[row * o + col] + u[row * o + col - 1]) / p.dYbp;
-                }
-            }
-            q = p.HaiChiadT * u[row * o + col] - q + p.CORIOLIS_FORCE * t_vtb;
-            q = (q - p.g * (z[(row + 1) * o + col] - z[row * o + col]) / p.dX +
-                 g.VISC[row * o + col] * (tmp + (u[(row + 1) * o + col] - 2 * u[row * o + col] + u[(row - 1) * o + col]) / p.dXbp)) +
-                (p.windx - g.Tsxw[row * o + col]) / g.Htdu[row * o + col];
-            const double tu = q / pp;
-            g.t_u[row * o + col] = tu;
+            const double tu = colT(g, 0)[(size_t)col * g.LT + row];  // k_coef_eu
+            g.t_u[row * P + col] = tu;
             su[row - k0] = tu;
         }
     }
@@ -1149,6 +1168,11 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
 // by the caller from the longest span of the direction.
 void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s) {
     k_explicit_v<<<g.N - 1, threads, sizeof(double) * (g.M + 3), s>>>(g, p);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+    k_coef_eu<<<((g.N - 2) * 32 + 255) / 256, 256, 0, s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 

@@ -15,13 +15,13 @@
 //      (replaces the reference's serial Thomas sweep, UVZSolver_multithread.cu:203-228)
 //   D  the solution scattered to t_z / t_u (t_v) with the reference's boundary formulas.
 //
-// Two tiers.  The line kernels give every line one warp (four lines per CTA): a short
-// line (at most 3 rows per lane) is swept by its warp alone, in shared memory, with
-// warp-level synchronisation only.  A longer line is appended to a device list and swept
-// afterwards by the long-line kernel, a persistent grid in which a 512-thread CTA takes
-// one line at a time with shared memory sized for the longest line the grid can hold (a
-// global scratch region per CTA beyond that).  The last CTA of the long-line kernel
-// empties the list for the next sweep.
+// One persistent kernel per sweep: a 512-thread CTA per SM takes every G-th line, one
+// per warp.  A short line (at most 3 rows per lane) is swept by its warp alone; a long
+// line by the whole CTA in shared memory sized for the longest line the grid can hold (a
+// global scratch region per CTA beyond that).  The solve is always one warp's: lanes
+// eliminate chunks of rows, the chunk ends are solved by shuffle-only cyclic reduction.
+// In the column sweeps the cell-local coefficients come precomputed, stored column-major
+// so that a column reads them contiguously (k_coef_uz, k_coef_fsj).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -30,18 +30,16 @@
 
 namespace {
 
-constexpr int kT = 128;          // threads of a line-kernel CTA; 4 warps
-constexpr int kWarps = kT / 32;  // lines per CTA in the line kernels
-constexpr int kTL = 512;         // threads of a long-line CTA
+constexpr int kTL = 512;         // threads of a sweep CTA
+constexpr int kWL = kTL / 32;    // lines per group (one per warp)
 constexpr int kRowW = 96;        // rows of a warp-tier line (3 per lane)
 constexpr int kCellW = 48;       // cells of a warp-tier hydrodynamic line
 constexpr int kRowWf = 64;       // rows of a warp-tier sediment line
-constexpr int kRedL = 6 * kTL;   // reduced-system exchange buffer of a long-line CTA
 constexpr int kWarpHydro = 4 * kRowW + 3 * kCellW;  // doubles per warp
 constexpr int kWarpFs = 4 * kRowW;
 
-// A group of threads that sweeps one line: a warp, or a whole long-line CTA.  exchange()
-// gives thread t the values v of threads t - h (lo) and t + h (hi).
+// A group of threads that sweeps one line: a warp, or a whole CTA for a long line.
+// WarpG::exchange() gives lane t the values v of lanes t - h (lo) and t + h (hi).
 struct WarpG {
     static constexpr int size = 32;
     __device__ static __forceinline__ int rank() { return threadIdx.x & 31; }
@@ -60,21 +58,6 @@ struct BlockG {
     static constexpr int size = kTL;
     __device__ static __forceinline__ int rank() { return threadIdx.x; }
     __device__ static __forceinline__ void sync() { __syncthreads(); }
-    __device__ static __forceinline__ void exchange(const double (&v)[6], int h, double (&lo)[6], double (&hi)[6],
-                                                    double* buf) {
-        const int t = threadIdx.x;
-#pragma unroll
-        for (int k = 0; k < 6; k++) buf[k * kTL + t] = v[k];
-        __syncthreads();
-        const int tl = t - h >= 0 ? t - h : t;
-        const int th = t + h < kTL ? t + h : t;
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            lo[k] = buf[k * kTL + tl];
-            hi[k] = buf[k * kTL + th];
-        }
-        __syncthreads();
-    }
 };
 
 // Chunk length for R rows over T threads: at least 3 and odd (odd strides keep the
@@ -90,8 +73,8 @@ __host__ __device__ inline int chunk_len(int R, int T) {
 // Row r: A[r] x[r-1] + B[r] x[r] + C[r] x[r+1] = D[r]; A[0] and C[last] are ignored.
 // Thread t owns rows [t*m, t*m+m).  The 2T chunk-end unknowns form a tridiagonal system
 // solved by parallel cyclic reduction with every row scaled to a unit diagonal (one
-// reciprocal per row and level), held in registers and exchanged through G (shuffles,
-// or `red`, 6T doubles of shared memory).  On return B[r] holds x[r].
+// reciprocal per row and level), held in registers and exchanged through G (warp
+// shuffles).  On return B[r] holds x[r].
 template <class G>
 __device__ __forceinline__ void solve_partitioned(double* A, double* B, double* C, double* D, int m, double* red) {
     constexpr int T = G::size;
@@ -219,6 +202,23 @@ __device__ __forceinline__ void solve_thomas(double* A, double* B, double* C, do
     G::sync();
 }
 
+// Solve of a line's packed system by group G: the partitioned solver run by the group's
+// first warp (chunks of m rows per lane, shuffle-only reduction), the other warps waiting.
+// A single warp keeps the reduction free of CTA barriers; m grows with the line instead.
+template <class G, int SOLVER>
+__device__ __forceinline__ void solve_line(double* A, double* B, double* C, double* D, int m, int rows) {
+    if (SOLVER == 0) {
+        if (G::size == 32) {
+            solve_partitioned<WarpG>(A, B, C, D, m, nullptr);
+        } else {
+            if (threadIdx.x < 32) solve_partitioned<WarpG>(A, B, C, D, m, nullptr);
+            G::sync();
+        }
+    } else {
+        solve_thomas<G>(A, B, C, D, rows);
+    }
+}
+
 struct LineShared {
     int first[HYD_SEGL], last[HYD_SEGL];
     int br1[HYD_SEGL], br2[HYD_SEGL];
@@ -241,27 +241,6 @@ __device__ __forceinline__ int seg_of_row(const LineShared& sg, int c) {
     int s = 0;
     while (s + 1 < sg.nseg && sg.ro[s + 1] <= c) s++;
     return s;
-}
-
-// Append a line to the long-line list.
-__device__ __forceinline__ void long_push(const DevGrid& g, int line) {
-    const unsigned k = atomicAdd(&g.long_ctr[0], 1u);
-    g.long_list[k] = line;
-}
-
-// Called by every CTA of a long-line kernel at its end: the last CTA to finish empties
-// the list (every CTA read the count before it got here).
-__device__ __forceinline__ void long_release(const DevGrid& g) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned prev = atomicAdd(&g.long_ctr[1], 1u);
-        if (prev == gridDim.x - 1) {
-            g.long_ctr[0] = 0;
-            g.long_ctr[1] = 0;
-            __threadfence();
-        }
-    }
 }
 
 // ---- hydrodynamic sweeps ----------------------------------------------------------
@@ -334,6 +313,65 @@ __device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p
     G::sync();
 }
 
+// Continuity and momentum coefficients of one wet cell of a UZ line (column j, cell i):
+// a2, c2, d2 (_uzSolver_calculate_preindex, UVZSolver_multithread.cu:402-406) and f1, f2,
+// f3, f5 (352-400).  Cell-local, so they are computed for every wet cell by a row-major
+// kernel and stored column-major for the column sweep.
+__device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& a2, double& c2,
+                                               double& d2, double& f1, double& f2, double& f3, double& f5) {
+    const int P = g.P;
+    c2 = p.dTchia2dX * g.Htdu[pos];
+    a2 = -p.dTchia2dX * g.Htdu[pos - P];
+    d2 = g.z[pos] - p.dTchia2dY * (g.Htdv[pos] * g.v[pos] - g.Htdv[pos - 1] * g.v[pos - 1]);
+    double pp = 0.0, qq = 0.0;
+    const double* u = g.u;
+    const double* H = g.H_moi;
+    const double vtb = (g.v[pos - 1] + g.v[pos] + g.v[pos + P - 1] + g.v[pos + P]) * 0.25;
+    f1 = p.dTchia2dX * u[pos] + g.VISC[pos] * p.dT / p.dXbp;
+    f2 = -(2 + g.Kx1[pos] * p.dT * sqrt(u[pos] * u[pos] + vtb * vtb) / g.Htdu[pos] + (2 * p.dT * g.VISC[pos]) / p.dXbp);
+    f3 = p.dT * g.VISC[pos] / p.dXbp - p.dTchia2dX * u[pos];
+    if (H[pos - 1] <= p.H_TINH) {
+        if (vtb < 0) {
+            pp = vtb * (-3 * u[pos] + 4 * u[pos + 1] - u[pos + 2]) / p.dY2;
+            qq = (u[pos] - 2 * u[pos + 1] + u[pos + 2]) / p.dYbp;
+        }
+    } else {
+        if (H[pos + 1] <= p.H_TINH) {
+            if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
+                pp = vtb * (3 * u[pos] - 4 * u[pos - 1] + u[pos - 2]) / p.dY2;
+                qq = (u[pos] - 2 * u[pos - 1] + u[pos - 2]) / p.dYbp;
+            }
+        } else {
+            pp = vtb * (u[pos + 1] - u[pos - 1]) / p.dY2;
+            qq = (u[pos + 1] - 2 * u[pos] + u[pos - 1]) / p.dYbp;
+        }
+    }
+    f5 = -2 * u[pos] + p.dT * pp - p.dT * p.CORIOLIS_FORCE * vtb - p.dT * g.VISC[pos] * qq -
+         p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
+}
+
+// UZ coefficients of every wet interior cell, one warp per row over the row's span of
+// cells that can be wet; written column-major (g.colT arrays 0..6: a2 c2 d2 f1 f2 f3 f5).
+__global__ void k_coef_uz(DevGrid g, DevParams p) {
+    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i > g.N) return;
+    const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
+    for (int j = lo + lane; j <= hi; j += 32) {
+        const int pos = i * g.P + j;
+        if (g.khouot[pos] != 0) continue;
+        double a2, c2, d2, f1, f2, f3, f5;
+        uz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
+        const size_t t = (size_t)j * g.LT + i;
+        colT(g, 0)[t] = a2;
+        colT(g, 1)[t] = c2;
+        colT(g, 2)[t] = d2;
+        colT(g, 3)[t] = f1;
+        colT(g, 4)[t] = f2;
+        colT(g, 5)[t] = f3;
+        colT(g, 6)[t] = f5;
+    }
+}
+
 // Phases A-D of one line by group G.  Rows A, B, Cc, D hold at least G::size * m
 // entries, cells a2, c2, d2 at least sg.C.
 template <int DIR, int SOLVER, class G>
@@ -359,16 +397,18 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         const int k = sg.first[sI] + (c - sg.co[sI]);
         const int pos = base + k * along;
         if (DIR == 0) {
-            c2[c] = p.dTchia2dX * g.Htdu[pos];
-            a2[c] = -p.dTchia2dX * g.Htdu[pos - P];
-            d2[c] = g.z[pos] - p.dTchia2dY * (g.Htdv[pos] * g.v[pos] - g.Htdv[pos - 1] * g.v[pos - 1]);
+            const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_uz
+            a2[c] = colT(g, 0)[t];
+            c2[c] = colT(g, 1)[t];
+            d2[c] = colT(g, 2)[t];
+            (void)pos;
         } else {
             c2[c] = p.dTchia2dY * g.Htdv[pos];
             a2[c] = -p.dTchia2dY * g.Htdv[pos - 1];
             d2[c] = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
         }
     }
-    for (int r = R + tid; r < T * m; r += T) {
+    for (int r = R + tid; r < 32 * m; r += T) {  // identity rows up to the solver's 32 m
         A[r] = 0.0;
         B[r] = 1.0;
         Cc[r] = 0.0;
@@ -403,31 +443,13 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         {
             double pp = 0.0, qq = 0.0;
             if (DIR == 0) {
-                const double* u = g.u;
-                const double* H = g.H_moi;
-                const double vtb = (g.v[pos - 1] + g.v[pos] + g.v[pos + P - 1] + g.v[pos + P]) * 0.25;
-                f1 = p.dTchia2dX * u[pos] + g.VISC[pos] * p.dT / p.dXbp;
-                f2 = -(2 + g.Kx1[pos] * p.dT * sqrt(u[pos] * u[pos] + vtb * vtb) / g.Htdu[pos] +
-                       (2 * p.dT * g.VISC[pos]) / p.dXbp);
-                f3 = p.dT * g.VISC[pos] / p.dXbp - p.dTchia2dX * u[pos];
-                if (H[pos - 1] <= p.H_TINH) {
-                    if (vtb < 0) {
-                        pp = vtb * (-3 * u[pos] + 4 * u[pos + 1] - u[pos + 2]) / p.dY2;
-                        qq = (u[pos] - 2 * u[pos + 1] + u[pos + 2]) / p.dYbp;
-                    }
-                } else {
-                    if (H[pos + 1] <= p.H_TINH) {
-                        if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
-                            pp = vtb * (3 * u[pos] - 4 * u[pos - 1] + u[pos - 2]) / p.dY2;
-                            qq = (u[pos] - 2 * u[pos - 1] + u[pos - 2]) / p.dYbp;
-                        }
-                    } else {
-                        pp = vtb * (u[pos + 1] - u[pos - 1]) / p.dY2;
-                        qq = (u[pos + 1] - 2 * u[pos] + u[pos - 1]) / p.dYbp;
-                    }
-                }
-                f5 = -2 * u[pos] + p.dT * pp - p.dT * p.CORIOLIS_FORCE * vtb - p.dT * g.VISC[pos] * qq -
-                     p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
+                const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_uz
+                f1 = colT(g, 3)[t];
+                f2 = colT(g, 4)[t];
+                f3 = colT(g, 5)[t];
+                f5 = colT(g, 6)[t];
+                (void)pp;
+                (void)qq;
             } else {
                 const double* v = g.v;
                 const double* H = g.H_moi;
@@ -516,8 +538,8 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     G::sync();
 
     // ---- C: solve
-    if (SOLVER == 0) solve_partitioned<G>(A, B, Cc, D, m, red);
-    else solve_thomas<G>(A, B, Cc, D, R);
+    solve_line<G, SOLVER>(A, B, Cc, D, m, R);
+    (void)red;
 
     // ---- D: extract (_uzSolver_extract_solution 668-723 / _vzSolver_extract_solution 595-665)
     const double* x = B;
@@ -563,78 +585,65 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     }
 }
 
-// Line kernel: warp w of CTA b sweeps line startidx + 4b + w, or lists it as long.
-// All warps of the CTA set up, meet at a barrier, and then sweep; a warp with nothing to
-// sweep waits at the closing barrier instead of exiting.  Without the two barriers the
-// warp-synchronous steps of a lone working warp were measured an order of magnitude
-// slower on B200.
+// Fused sweep of one direction.  CTA b takes lines b, b + G, b + 2G, ... (G = gridDim.x)
+// in groups of 16, one line per warp.  Every warp sets its line up; a warp whose line is
+// short (at most kRowW rows, kCellW cells) sweeps it alone in its own slice of shared
+// memory; then the whole CTA sweeps the group's long lines one after another in the full
+// shared memory (RB rows, CB cells; a CTA's region of global scratch beyond that).
+// Adjacent long lines (a wet band) fall on different CTAs.  Warps with nothing to sweep
+// wait at the CTA barriers rather than exit: the warp-synchronous steps of a warp whose
+// sibling warps had exited were measured an order of magnitude slower on B200.
 template <int DIR, int SOLVER>
-__global__ void __launch_bounds__(kT) k_hydro_lines(DevGrid g, DevParams p, int startidx, int endidx) {
+__global__ void __launch_bounds__(kTL) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB, int CB,
+                                                     double* gscr, int RG, int CG) {
     extern __shared__ double dyn_smem[];
-    __shared__ LineShared sgw[kWarps];
+    __shared__ LineShared sgw[kWL];
+    __shared__ int s_long[kWL];
+    __shared__ int s_nlong;
     const int w = threadIdx.x >> 5;
-    const int line = startidx + blockIdx.x * kWarps + w;
-    LineShared& sg = sgw[w];
-    bool work = line <= endidx;  // warp-uniform
-    if (work) {
-        hydro_setup<DIR, WarpG>(g, p, line, sg);
-        if (sg.nseg == 0) {
-            work = false;
-        } else if (sg.R > kRowW || sg.C > kCellW) {
-            if ((threadIdx.x & 31) == 0) long_push(g, line);
-            work = false;
+    const int nlines = endidx - startidx + 1;
+    const int G = gridDim.x;
+    for (int j0 = 0; (int)blockIdx.x + j0 * G < nlines; j0 += kWL) {
+        const int li = blockIdx.x + (j0 + w) * G;
+        LineShared& sg = sgw[w];
+        if (threadIdx.x == 0) s_nlong = 0;
+        if (li < nlines) hydro_setup<DIR, WarpG>(g, p, startidx + li, sg);  // warp-uniform
+        __syncthreads();
+        if (li < nlines && sg.nseg > 0) {
+            if (sg.R > kRowW || sg.C > kCellW) {
+                if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
+            } else {
+                double* A = dyn_smem + w * kWarpHydro;
+                double* B = A + kRowW;
+                double* Cc = B + kRowW;
+                double* D = Cc + kRowW;
+                double* a2 = D + kRowW;
+                double* c2 = a2 + kCellW;
+                double* d2 = c2 + kCellW;
+                hydro_body<DIR, SOLVER, WarpG>(g, p, startidx + li, sg, A, B, Cc, D, a2, c2, d2, nullptr,
+                                               chunk_len(sg.R, 32));
+            }
+        }
+        __syncthreads();
+        const int nl = s_nlong;
+        for (int q = 0; q < nl; q++) {
+            const int wl = s_long[q];
+            const LineShared& sl = sgw[wl];
+            const int line = startidx + (int)blockIdx.x + (j0 + wl) * G;
+            const int m = chunk_len(sl.R, 32);
+            const bool fits = 32 * m <= RB && sl.C <= CB;
+            const int rs = fits ? RB : RG, cs = fits ? CB : CG;
+            double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * (4 * (size_t)RG + 3 * (size_t)CG);
+            double* B = A + rs;
+            double* Cc = B + rs;
+            double* D = Cc + rs;
+            double* a2 = D + rs;
+            double* c2 = a2 + cs;
+            double* d2 = c2 + cs;
+            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sl, A, B, Cc, D, a2, c2, d2, nullptr, m);
+            __syncthreads();  // the slices and sgw are reused
         }
     }
-    __syncthreads();
-    if (work) {
-        double* A = dyn_smem + w * kWarpHydro;
-        double* B = A + kRowW;
-        double* Cc = B + kRowW;
-        double* D = Cc + kRowW;
-        double* a2 = D + kRowW;
-        double* c2 = a2 + kCellW;
-        double* d2 = c2 + kCellW;
-        hydro_body<DIR, SOLVER, WarpG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, nullptr, chunk_len(sg.R, 32));
-    }
-    __syncthreads();
-}
-
-// Long-line kernel: CTA b sweeps listed lines b, b + gridDim.x, ...  Shared memory holds
-// RB rows and CB cells; a line needing more uses the CTA's global region of RG rows and
-// CG cells.
-template <int DIR, int SOLVER>
-__global__ void __launch_bounds__(kTL) k_hydro_long(DevGrid g, DevParams p, int RB, int CB, double* gscr, int RG,
-                                                   int CG) {
-    extern __shared__ double dyn_smem[];
-    __shared__ LineShared sg;
-    const int n = *(volatile unsigned*)&g.long_ctr[0];
-    for (int k = blockIdx.x; k < n; k += gridDim.x) {
-        const int line = g.long_list[k];
-        hydro_setup<DIR, BlockG>(g, p, line, sg);
-        const int m = chunk_len(sg.R, kTL);
-        double* red = dyn_smem;
-        if (kTL * m <= RB && sg.C <= CB) {
-            double* A = red + kRedL;
-            double* B = A + RB;
-            double* Cc = B + RB;
-            double* D = Cc + RB;
-            double* a2 = D + RB;
-            double* c2 = a2 + CB;
-            double* d2 = c2 + CB;
-            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, red, m);
-        } else {
-            double* A = gscr + (size_t)blockIdx.x * (4 * (size_t)RG + 3 * (size_t)CG);
-            double* B = A + RG;
-            double* Cc = B + RG;
-            double* D = Cc + RG;
-            double* a2 = D + RG;
-            double* c2 = a2 + CG;
-            double* d2 = c2 + CG;
-            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sg, A, B, Cc, D, a2, c2, d2, red, m);
-        }
-        __syncthreads();  // sg and the buffers are reused by the next line
-    }
-    long_release(g);
 }
 
 // ---- sediment sweeps --------------------------------------------------------------
@@ -664,6 +673,84 @@ __device__ __forceinline__ double source_nchs(const DevParams& p, double wsm, do
     const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
     const double Cac = 0.015 * p.dm * pow(Tx, 1.5) * p.dxr_m03 / (0.05 * h_moi);
     return wsm * (Cac - gamac * fs);
+}
+
+// Row of the sediment system for one interior wet cell before the segment-end terms
+// (_FSj/_FSi_calculate__mactrix_coeff, Sediment_Transport.cu:205-302 / 62-165): aa, bb,
+// cc, dd of the row, with the source S gated by t < bed_change_start.
+template <int DIR>
+__device__ __forceinline__ void fs_cell_coeffs(const DevGrid& g, const DevParams& p, double t, int pos, double& aa,
+                                               double& bb, double& cc, double& dd) {
+    const int P = g.P;
+    const double* FS = g.FS;
+    const double* H = g.H_moi;
+    const double s_start = p.bed_change_start;
+    const double sqrtg = sqrt(p.g);
+    const double c = 18 * log(12 * H[pos] / p.Ks);
+    const double Uf = sqrtg * fabs(g.VTH[pos]) / c;
+    const double fq = 1 - FS[pos];
+    const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
+    double Zf = 0;
+    double S;
+    double gamav;
+    if (DIR == 0) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
+    if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+    if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], H[pos]);
+    else S = source_nchs(p, wsm, Zf, Uf, H[pos], FS[pos]);
+    if (t < s_start) S = 0;
+    if (DIR == 1) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
+    double pp, qq;
+    if (DIR == 0) {
+        aa = -gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 - g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
+        cc = gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
+        bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
+        pp = 0;
+        qq = 0;
+        if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = (FS[pos + 1] - FS[pos]);
+        if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = (FS[pos] - FS[pos - 1]);
+        pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
+        if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
+            qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
+            qq = (g.t_v[pos] + g.t_v[pos - 1]) * 0.5 * qq * gamav;
+        } else
+            qq = 0;
+        dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
+    } else {
+        aa = -gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos - 1] * g.Ky[pos - 1] / (H[pos] * p.dYbp);
+        cc = gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos] * g.Ky[pos] / (H[pos] * p.dYbp);
+        bb = p.HaiChiadT + (g.Htdv[pos] * g.Ky[pos] + g.Htdv[pos - 1] * g.Ky[pos - 1]) / (H[pos] * p.dYbp);
+        pp = 0;
+        qq = 0;
+        if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = (FS[pos + P] - FS[pos]);
+        if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = (FS[pos] - FS[pos - P]);
+        pp = (1 / (H[pos] * p.dXbp)) * (g.Htdu[pos] * g.Kx[pos] * pp - g.Htdu[pos - P] * g.Kx[pos - P] * qq);
+        if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
+            qq = (FS[pos + P] - FS[pos - P]) / p.dX2;
+            qq = (g.t_u[pos] + g.t_u[pos - P]) * 0.5 * qq * gamav;
+        } else
+            qq = 0;
+        dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
+    }
+}
+
+// FSj rows of every interior wet cell (columns 3..M-1), one warp per row of the grid over
+// the row's span, written column-major (g.colT arrays 0..3: aa bb cc dd).
+__global__ void k_coef_fsj(DevGrid g, DevParams p, int half) {
+    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i > g.N) return;
+    const double t = g.clock[half];
+    const int lo = max(g.rlo[i], 3), hi = min(g.rhi[i], g.M - 1);
+    for (int j = lo + lane; j <= hi; j += 32) {
+        const int pos = i * g.P + j;
+        if (g.khouot[pos] != 0) continue;
+        double aa, bb, cc, dd;
+        fs_cell_coeffs<0>(g, p, t, pos, aa, bb, cc, dd);
+        const size_t q = (size_t)j * g.LT + i;
+        colT(g, 0)[q] = aa;
+        colT(g, 1)[q] = bb;
+        colT(g, 2)[q] = cc;
+        colT(g, 3)[q] = dd;
+    }
 }
 
 // Segments of a sediment line and their row offsets (one row per interior cell
@@ -711,54 +798,28 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     const int P = g.P;
     const int along = DIR == 0 ? P : 1;
     const int base = DIR == 0 ? line : line * P;
-    const double s_start = p.bed_change_start;
     const double t = g.clock[half];
     const int R = sg.R;
-    for (int r = R + tid; r < T * m; r += T) {
+    for (int r = R + tid; r < 32 * m; r += T) {  // identity rows up to the solver's 32 m
         A[r] = 0.0;
         B[r] = 1.0;
         Cc[r] = 0.0;
         D[r] = 0.0;
     }
     const double* FS = g.FS;
-    const double* H = g.H_moi;
-    const double sqrtg = sqrt(p.g);
     for (int rr = tid; rr < R; rr += T) {
         const int sI = seg_of_row(sg, rr);
         const int f = sg.first[sI], l = sg.last[sI];
         const int k = f + 1 + (rr - sg.ro[sI]);
         const int b1f = sg.br1[sI], b2f = sg.br2[sI];
         const int pos = base + k * along;
-        const double c = 18 * log(12 * H[pos] / p.Ks);
-        const double Uf = sqrtg * fabs(g.VTH[pos]) / c;
-        const double fq = 1 - FS[pos];
-        const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
-        double Zf = 0;
-        double S;
-        double gamav;
-        if (DIR == 0) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
-        if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
-        if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], H[pos]);
-        else S = source_nchs(p, wsm, Zf, Uf, H[pos], FS[pos]);
-        if (t < s_start) S = 0;
-        if (DIR == 1) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
-        double aa, bb, cc, dd, pp, qq;
-        if (DIR == 0) {
-            aa = -gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 -
-                 g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
-            cc = gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
-            bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
-            pp = 0;
-            qq = 0;
-            if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = (FS[pos + 1] - FS[pos]);
-            if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = (FS[pos] - FS[pos - 1]);
-            pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
-            if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
-                qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
-                qq = (g.t_v[pos] + g.t_v[pos - 1]) * 0.5 * qq * gamav;
-            } else
-                qq = 0;
-            dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
+        double aa, bb, cc, dd;
+        if (DIR == 0) {  // precomputed by k_coef_fsj
+            const size_t q = (size_t)line * g.LT + k;
+            aa = colT(g, 0)[q];
+            bb = colT(g, 1)[q];
+            cc = colT(g, 2)[q];
+            dd = colT(g, 3)[q];
             if (k == f + 1) {
                 if (b1f || g.t_u[base + f * along] == 0) bb += aa;
                 else dd -= aa * FS[base + f * along];
@@ -768,21 +829,7 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
                 else dd -= cc * FS[base + l * along];
             }
         } else {
-            aa = -gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 -
-                 g.Htdv[pos - 1] * g.Ky[pos - 1] / (H[pos] * p.dYbp);
-            cc = gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos] * g.Ky[pos] / (H[pos] * p.dYbp);
-            bb = p.HaiChiadT + (g.Htdv[pos] * g.Ky[pos] + g.Htdv[pos - 1] * g.Ky[pos - 1]) / (H[pos] * p.dYbp);
-            pp = 0;
-            qq = 0;
-            if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = (FS[pos + P] - FS[pos]);
-            if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = (FS[pos] - FS[pos - P]);
-            pp = (1 / (H[pos] * p.dXbp)) * (g.Htdu[pos] * g.Kx[pos] * pp - g.Htdu[pos - P] * g.Kx[pos - P] * qq);
-            if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
-                qq = (FS[pos + P] - FS[pos - P]) / p.dX2;
-                qq = (g.t_u[pos] + g.t_u[pos - P]) * 0.5 * qq * gamav;
-            } else
-                qq = 0;
-            dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
+            fs_cell_coeffs<1>(g, p, t, pos, aa, bb, cc, dd);
             if (k == f + 1) {
                 if (b1f || g.t_v[base + f * along] == 0) bb = bb + aa;
                 else dd = dd - aa * FS[base + f * along];
@@ -798,8 +845,8 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
         D[rr] = dd;
     }
     G::sync();
-    if (SOLVER == 0) solve_partitioned<G>(A, B, Cc, D, m, red);
-    else solve_thomas<G>(A, B, Cc, D, R);
+    solve_line<G, SOLVER>(A, B, Cc, D, m, R);
+    (void)red;
     const double* x = B;
     double* vel = DIR == 0 ? g.t_u : g.t_v;
     for (int c = tid; c < R; c += T) {
@@ -823,55 +870,46 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     }
 }
 
-// Sediment line kernel: as k_hydro_lines.
+// Fused sediment sweep of one direction: as k_hydro_sweep, short lines at most kRowWf rows.
 template <int DIR, int SOLVER>
-__global__ void __launch_bounds__(kT) k_fs_lines(DevGrid g, DevParams p, int half, int startidx, int endidx) {
+__global__ void __launch_bounds__(kTL) k_fs_sweep(DevGrid g, DevParams p, int half, int startidx, int endidx, int RB,
+                                                  double* gscr, int RG) {
     extern __shared__ double dyn_smem[];
-    __shared__ LineShared sgw[kWarps];
+    __shared__ LineShared sgw[kWL];
+    __shared__ int s_long[kWL];
+    __shared__ int s_nlong;
     const int w = threadIdx.x >> 5;
-    const int line = startidx + blockIdx.x * kWarps + w;
-    LineShared& sg = sgw[w];
-    bool work = line <= endidx;  // warp-uniform
-    if (work) {
-        fs_setup<DIR, WarpG>(g, p, line, sg);
-        if (sg.R == 0) {
-            work = false;
-        } else if (sg.R > kRowWf) {
-            if ((threadIdx.x & 31) == 0) long_push(g, line);
-            work = false;
-        }
-    }
-    __syncthreads();
-    if (work) {
-        double* A = dyn_smem + w * kWarpFs;
-        double* B = A + kRowW;
-        double* Cc = B + kRowW;
-        double* D = Cc + kRowW;
-        fs_body<DIR, SOLVER, WarpG>(g, p, half, line, sg, A, B, Cc, D, nullptr, chunk_len(sg.R, 32));
-    }
-    __syncthreads();
-}
-
-template <int DIR, int SOLVER>
-__global__ void __launch_bounds__(kTL) k_fs_long(DevGrid g, DevParams p, int half, int RB, double* gscr, int RG) {
-    extern __shared__ double dyn_smem[];
-    __shared__ LineShared sg;
-    const int n = *(volatile unsigned*)&g.long_ctr[0];
-    for (int k = blockIdx.x; k < n; k += gridDim.x) {
-        const int line = g.long_list[k];
-        fs_setup<DIR, BlockG>(g, p, line, sg);
-        const int m = chunk_len(sg.R, kTL);
-        double* red = dyn_smem;
-        if (kTL * m <= RB) {
-            double* A = red + kRedL;
-            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sg, A, A + RB, A + 2 * RB, A + 3 * RB, red, m);
-        } else {
-            double* A = gscr + (size_t)blockIdx.x * 4 * (size_t)RG;
-            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sg, A, A + RG, A + 2 * RG, A + 3 * RG, red, m);
+    const int nlines = endidx - startidx + 1;
+    const int G = gridDim.x;
+    for (int j0 = 0; (int)blockIdx.x + j0 * G < nlines; j0 += kWL) {
+        const int li = blockIdx.x + (j0 + w) * G;
+        LineShared& sg = sgw[w];
+        if (threadIdx.x == 0) s_nlong = 0;
+        if (li < nlines) fs_setup<DIR, WarpG>(g, p, startidx + li, sg);  // warp-uniform
+        __syncthreads();
+        if (li < nlines && sg.R > 0) {
+            if (sg.R > kRowWf) {
+                if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
+            } else {
+                double* A = dyn_smem + w * kWarpFs;
+                fs_body<DIR, SOLVER, WarpG>(g, p, half, startidx + li, sg, A, A + kRowW, A + 2 * kRowW, A + 3 * kRowW,
+                                            nullptr, chunk_len(sg.R, 32));
+            }
         }
         __syncthreads();
+        const int nl = s_nlong;
+        for (int q = 0; q < nl; q++) {
+            const int wl = s_long[q];
+            const LineShared& sl = sgw[wl];
+            const int line = startidx + (int)blockIdx.x + (j0 + wl) * G;
+            const int m = chunk_len(sl.R, 32);
+            const bool fits = 32 * m <= RB;
+            const int rs = fits ? RB : RG;
+            double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * 4 * (size_t)RG;
+            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sl, A, A + rs, A + 2 * rs, A + 3 * rs, nullptr, m);
+            __syncthreads();
+        }
     }
-    long_release(g);
 }
 
 // Largest dynamic shared memory the kernel may be given on this device.
@@ -897,17 +935,12 @@ cudaError_t allow_all(F* const* fs, int n, int* limit) {
     return cudaSuccess;
 }
 
-using HydroLinesFn = void(DevGrid, DevParams, int, int);
-using HydroLongFn = void(DevGrid, DevParams, int, int, double*, int, int);
-using FsLinesFn = void(DevGrid, DevParams, int, int, int);
-using FsLongFn = void(DevGrid, DevParams, int, int, double*, int);
+using HydroSweepFn = void(DevGrid, DevParams, int, int, int, int, double*, int, int);
+using FsSweepFn = void(DevGrid, DevParams, int, int, int, int, double*, int);
 
-HydroLinesFn* const kHydroLines[2][2] = {{k_hydro_lines<0, 0>, k_hydro_lines<0, 1>},
-                                         {k_hydro_lines<1, 0>, k_hydro_lines<1, 1>}};
-HydroLongFn* const kHydroLong[2][2] = {{k_hydro_long<0, 0>, k_hydro_long<0, 1>},
-                                       {k_hydro_long<1, 0>, k_hydro_long<1, 1>}};
-FsLinesFn* const kFsLines[2][2] = {{k_fs_lines<0, 0>, k_fs_lines<0, 1>}, {k_fs_lines<1, 0>, k_fs_lines<1, 1>}};
-FsLongFn* const kFsLong[2][2] = {{k_fs_long<0, 0>, k_fs_long<0, 1>}, {k_fs_long<1, 0>, k_fs_long<1, 1>}};
+HydroSweepFn* const kHydroSweep[2][2] = {{k_hydro_sweep<0, 0>, k_hydro_sweep<0, 1>},
+                                         {k_hydro_sweep<1, 0>, k_hydro_sweep<1, 1>}};
+FsSweepFn* const kFsSweep[2][2] = {{k_fs_sweep<0, 0>, k_fs_sweep<0, 1>}, {k_fs_sweep<1, 0>, k_fs_sweep<1, 1>}};
 
 }  // namespace
 
@@ -915,54 +948,53 @@ FsLongFn* const kFsLong[2][2] = {{k_fs_long<0, 0>, k_fs_long<0, 1>}, {k_fs_long<
 // device; opts the sweep kernels into the shared memory they may need.
 cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
     cudaError_t e;
-    int lim_lines, lim_long, lim_fsl, lim_fslong;
-    if ((e = allow_all(&kHydroLines[0][0], 4, &lim_lines)) != cudaSuccess) return e;
-    if ((e = allow_all(&kHydroLong[0][0], 4, &lim_long)) != cudaSuccess) return e;
-    if ((e = allow_all(&kFsLines[0][0], 4, &lim_fsl)) != cudaSuccess) return e;
-    if ((e = allow_all(&kFsLong[0][0], 4, &lim_fslong)) != cudaSuccess) return e;
-    sp->smem_lines = sizeof(double) * kWarps * kWarpHydro;
-    sp->smem_fs_lines = sizeof(double) * kWarps * kWarpFs;
-    if ((int)sp->smem_lines > lim_lines || (int)sp->smem_fs_lines > lim_fsl) return cudaErrorInvalidValue;
+    int lim_h, lim_f;
+    if ((e = allow_all(&kHydroSweep[0][0], 4, &lim_h)) != cudaSuccess) return e;
+    if ((e = allow_all(&kFsSweep[0][0], 4, &lim_f)) != cudaSuccess) return e;
     const int L = N > M ? N : M;
-    // every row/cell a line can have: rows <= 2 L + 20, cells <= L + 3
-    sp->RG = kTL * chunk_len(2 * L + HYD_SEGL, kTL);
+    const size_t warp_h = (size_t)kWL * kWarpHydro, warp_f = (size_t)kWL * kWarpFs;  // short-line slices
+    if ((long long)(sizeof(double) * warp_h) > lim_h || (long long)(sizeof(double) * warp_f) > lim_f)
+        return cudaErrorInvalidValue;
+    // every row/cell a line can have: rows <= 2 L + 20, cells <= L + 3 (solved by 32 lanes)
+    sp->RG = 32 * chunk_len(2 * L + HYD_SEGL, 32);
     sp->CG = L + 3;
-    const size_t full = sizeof(double) * (kRedL + 4 * (size_t)sp->RG + 3 * (size_t)sp->CG);
-    if ((long long)full <= lim_long) {
+    sp->need_global = 0;
+    if ((long long)(sizeof(double) * (4 * (size_t)sp->RG + 3 * (size_t)sp->CG)) <= lim_h) {
         sp->RB = sp->RG;
         sp->CB = sp->CG;
-        sp->need_global = 0;
-    } else {
-        // as many rows (and half as many cells) as fit; longer lines use global scratch
-        const int per = 4 * 2 + 3;  // doubles per pair of rows
-        const int pairs = (int)((lim_long / (int)sizeof(double) - kRedL) / per);
-        sp->RB = (2 * pairs) / kTL * kTL;
+    } else {  // as many rows (and half as many cells) as fit; longer lines use global scratch
+        const int pairs = (int)((lim_h / (int)sizeof(double)) / (4 * 2 + 3));
+        sp->RB = 2 * pairs;
         sp->CB = pairs;
         sp->need_global = 1;
     }
-    sp->smem_long = sizeof(double) * (kRedL + 4 * (size_t)sp->RB + 3 * (size_t)sp->CB);
-    sp->RGf = kTL * chunk_len(L, kTL);
-    const size_t full_fs = sizeof(double) * (kRedL + 4 * (size_t)sp->RGf);
-    if ((long long)full_fs <= lim_fslong) {
+    size_t big = 4 * (size_t)sp->RB + 3 * (size_t)sp->CB;
+    sp->smem_lines = sizeof(double) * (big > warp_h ? big : warp_h);
+    sp->RGf = 32 * chunk_len(L, 32);
+    if ((long long)(sizeof(double) * 4 * (size_t)sp->RGf) <= lim_f) {
         sp->RBf = sp->RGf;
     } else {
-        sp->RBf = (int)((lim_fslong / (int)sizeof(double) - kRedL) / 4) / kTL * kTL;
+        sp->RBf = (int)((lim_f / (int)sizeof(double)) / 4);
         sp->need_global = 1;
     }
-    sp->smem_fs_long = sizeof(double) * (kRedL + 4 * (size_t)sp->RBf);
+    big = 4 * (size_t)sp->RBf;
+    sp->smem_fs_lines = sizeof(double) * (big > warp_f ? big : warp_f);
     int dev = 0, nsm = 0, occ = 0, occf = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kHydroLong[0][0], kTL, sp->smem_long)) != cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kHydroSweep[0][0], kTL, sp->smem_lines)) !=
+        cudaSuccess)
         return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, kFsLong[0][0], kTL, sp->smem_fs_long)) !=
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, kFsSweep[0][0], kTL, sp->smem_fs_lines)) !=
         cudaSuccess)
         return e;
     if (occ < 1) occ = 1;
     if (occf < 1) occf = 1;
     sp->long_grid = nsm * (occ < occf ? occ : occf);
     if (sp->long_grid > L + 3) sp->long_grid = L + 3;
-    sp->scratch_doubles = sp->need_global ? (size_t)sp->long_grid * (4 * (size_t)sp->RG + 3 * (size_t)sp->CG) : 1;
+    sp->scratch_doubles =
+        sp->need_global ? (size_t)sp->long_grid * (4 * (size_t)(sp->RG > sp->RGf ? sp->RG : sp->RGf) + 3 * (size_t)sp->CG)
+                        : 1;
     return cudaSuccess;
 }
 
@@ -972,9 +1004,9 @@ void hydro_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan&
     const int nlines = endidx - startidx + 1;
     if (nlines <= 0) return;
     const int sv = solver ? 1 : 0;
-    kHydroLines[dir][sv]<<<(nlines + kWarps - 1) / kWarps, kT, sp.smem_lines, s>>>(g, p, startidx, endidx);
-    kHydroLong[dir][sv]<<<sp.long_grid, kTL, sp.smem_long, s>>>(g, p, sp.RB, sp.CB, scratch, sp.RG, sp.CG);
-    hyd_kernel_launches_add(2);
+    kHydroSweep[dir][sv]<<<sp.long_grid, kTL, sp.smem_lines, s>>>(g, p, startidx, endidx, sp.RB, sp.CB, scratch, sp.RG,
+                                                                  sp.CG);
+    hyd_kernel_launches_add(1);
 }
 
 void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int startidx,
@@ -982,11 +1014,21 @@ void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp
     const int nlines = endidx - startidx + 1;
     if (nlines <= 0) return;
     const int sv = solver ? 1 : 0;
-    kFsLines[dir][sv]<<<(nlines + kWarps - 1) / kWarps, kT, sp.smem_fs_lines, s>>>(g, p, half, startidx, endidx);
-    kFsLong[dir][sv]<<<sp.long_grid, kTL, sp.smem_fs_long, s>>>(g, p, half, sp.RBf, scratch, sp.RGf);
-    hyd_kernel_launches_add(2);
+    kFsSweep[dir][sv]<<<sp.long_grid, kTL, sp.smem_fs_lines, s>>>(g, p, half, startidx, endidx, sp.RBf, scratch,
+                                                                   sp.RGf);
+    hyd_kernel_launches_add(1);
 }
 }  // namespace
+
+void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+    k_coef_uz<<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s) {
+    k_coef_fsj<<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p, half);
+    hyd_kernel_launches_add(1);
+}
 
 void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
                      int solver, double* scratch, cudaStream_t s) {
