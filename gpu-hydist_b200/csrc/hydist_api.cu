@@ -699,15 +699,15 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     cudaStream_t st = s->stream;
     // channel mode writes levels at table-dependent places: always the whole grid
     const int fh = full_h || p.channel, fsd = full_s || p.channel;
-    launch_clock(g, p, st);
     // ---- half-step 1: implicit along i (columns), explicit v
-    { PHASE(PH_BOUNDARY); launch_boundary(g, p, 0, st); }
+    // (the first launch advances the clock and applies the boundary values)
     int start_idx = 2, end_idx = s->M;
     if (p.channel && s->P.kenhhepd == 1) {
         start_idx = 3;
         end_idx = s->M - 1;
     }
-    { PHASE(PH_SWEEP_UZ); launch_coef_uz(g, p, st); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
+    { PHASE(PH_BOUNDARY); launch_coef_uz(g, p, st); }
+    { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_EXPL_V); launch_explicit_v(g, p, s->thr_r, st); }
@@ -715,10 +715,18 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     std::swap(g.t_v, s->scratch_v);
     if (force) launch_mark_all_cols(g, st);
     { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, s->thr_r, st); }
-    { PHASE(PH_POST); launch_post(g, p, fh, st); }
-    { PHASE(PH_SCAN); launch_scan_cols(g, p, st); }
+    // after a span-limited pass the update, the column rescan and (with sediment) VTH/K
+    // share one launch; whole-grid passes keep them apart
+    const int fuse1 = !fh && !fsd;
+    if (!fh) {
+        PHASE(PH_POST);
+        launch_post_fused(g, p, 0, sed1 && fuse1, st);
+    } else {
+        { PHASE(PH_POST); launch_post(g, p, fh, st); }
+        { PHASE(PH_SCAN); launch_scan_cols(g, p, st); }
+    }
     if (sed1) {
-        { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
+        if (!(sed1 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
         { PHASE(PH_FS_J); launch_coef_fsj(g, p, 0, st); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
     }
@@ -737,10 +745,15 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }
-    { PHASE(PH_POST); launch_post(g, p, fh, st); }
-    { PHASE(PH_SCAN); launch_scan_rows(g, p, st); }
+    if (!fh) {
+        PHASE(PH_POST);
+        launch_post_fused(g, p, 1, sed2 && fuse1, st);
+    } else {
+        { PHASE(PH_POST); launch_post(g, p, fh, st); }
+        { PHASE(PH_SCAN); launch_scan_rows(g, p, st); }
+    }
     if (sed2) {
-        { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
+        if (!(sed2 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
         { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, s->plan, 1, s->solver, s->sweep_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
         start_idx = 3;

@@ -114,7 +114,6 @@ __device__ __forceinline__ int find_seg_u(const DevGrid& g, int row, int col, in
 // Host launch wrappers (defined in the .cu files, called by hydist_api.cu).
 struct StepLaunch;
 void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_mask, cudaStream_t s);
-void launch_clock(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 // Launch shapes of the sweeps for one grid (k_sweep.cu).
 struct SweepPlan {
@@ -145,6 +144,7 @@ void launch_post(const DevGrid& g, const DevParams& p, int full, cudaStream_t s)
 void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
+void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s);
 void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,

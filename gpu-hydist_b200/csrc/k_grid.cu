@@ -122,89 +122,119 @@ __global__ void k_preprocess(DevGrid g, DevParams p) {
 // Advances the device copy of the simulation time by one full step exactly as the host
 // loop does (Engine.py:146,260: t = t + dT * 0.5, twice), so that a captured step can be
 // replayed without baking the time into kernel arguments.
-__global__ void k_clock(DevGrid g, double dT) {
-    const double t1 = g.clock[2] + dT * 0.5;
-    const double t2 = t1 + dT * 0.5;
-    g.clock[0] = t1;
-    g.clock[1] = t2;
-    g.clock[2] = t2;
-}
 
 // --------------------------------------------------------------- boundary values
 
-// Boundary_value + FS_boundary for one edge at index i (support_funcs.cu:544-617)
-__device__ void bnd_edge(const DevGrid& g, int i, double t, int isU, int location, int location_ext,
-                         const int* btype, const double* hi_e, double* barr, const double* bcv, const double* ccv,
-                         double hmax, const int* moc, const int* dau, const int* cuoi) {
-    const int P = g.P, tt = g.total_time;
-    const int t1 = (int)(t / 3600);
-    const double t2 = (t - (3600.0 * t1)) / 3600.0;
-    int seg_no = -1;
-    if (moc[location] > 0 && dau[location * HYD_SEGL] <= i && i <= cuoi[location * HYD_SEGL]) seg_no = 0;
-    if (seg_no == -1) return;
-    const double value = bcv[seg_no * tt + t1] * (1.0 - t2) + bcv[seg_no * tt + t1 + 1] * t2;
-    if (btype[seg_no] == 2) {
-        barr[i] = value * hi_e[i];
-    } else if (isU) {
-        g.t_z[location * P + i] = value;
-        g.t_z[location_ext * P + i] = value;
-    } else {
-        g.t_z[i * P + location] = value;
-        g.t_z[i * P + location_ext] = value;
-    }
-    if (btype[seg_no] != 2) return;
-    const int ii = isU ? location : i, jj = isU ? i : location;
-    const double cv = ccv[seg_no * tt + t1] * (1.0 - t2) + ccv[seg_no * tt + t1 + 1] * t2;
-    g.FS[ii * P + jj] = cv * g.htaiz_bd[ii * P + jj] * hmax;
-}
+// Boundary_value + FS_boundary for one edge at index i (support_funcs.cu:544-617), split
+// into the computation (BndRec) and the writes it makes (bnd_apply).
+struct BndRec {
+    int kind;  // 0 nothing, 1 discharge edge (velocity table + FS), 2 level edge (two levels)
+    double value, fsv;
+};
 
-// Update_Boundary_Value (support_funcs.cu:622-668).  Each reference thread i applies the
-// up, down, left and right edges in turn; two edges write the same t_z/FS cell only at the
-// corners (2,M), (N,M), (2,2), (N,2).  The edges run one after another here, and the two
-// corners where a later thread of the reference wins over a later edge are re-applied:
-// (N,2) by the down edge (thread N runs after the right edge's thread 2) and (N,M) by the
-// up edge when N > M.
-__global__ void k_boundary(DevGrid g, DevParams p, int half) {
-    const double t = g.clock[half];
+struct EdgeArgs {
+    int isU, location, location_ext;
+    const int* btype;
+    const double *hi_e, *bcv, *ccv;
+    double* barr;
+    double hmax;
+    const int *moc, *dau, *cuoi;
+};
+
+// Edges in the order up (column M), down (column 2), left (row 2), right (row N).
+__device__ __forceinline__ EdgeArgs edge_args(const DevGrid& g, int e) {
     const int N = g.N, M = g.M;
-    const int imax = N > M ? N : M;
     const double* hi_up = g.hi;
     const double* hi_down = hi_up + (N + 3);
     const double* hi_left = hi_down + (N + 3);
     const double* hi_right = hi_left + (M + 3);
-    for (int e = 0; e < 4; e++) {
-        for (int i = 2 + threadIdx.x; i <= imax; i += blockDim.x) {
-            if (e == 0)
-                bnd_edge(g, i, t, 0, M, M + 1, g.btype + 0 * HYD_SEGL, hi_up, g.vbt, g.bc[0], g.cc[0], g.hmax[0], g.mocj,
-                         g.dauj, g.cuoij);
-            else if (e == 1)
-                bnd_edge(g, i, t, 0, 2, 1, g.btype + 1 * HYD_SEGL, hi_down, g.vbd, g.bc[1], g.cc[1], g.hmax[1], g.mocj,
-                         g.dauj, g.cuoij);
-            else if (e == 2)
-                bnd_edge(g, i, t, 1, 2, 1, g.btype + 2 * HYD_SEGL, hi_left, g.ubt, g.bc[2], g.cc[2], g.hmax[2], g.moci,
-                         g.daui, g.cuoii);
-            else
-                bnd_edge(g, i, t, 1, N, N + 1, g.btype + 3 * HYD_SEGL, hi_right, g.ubp, g.bc[3], g.cc[3], g.hmax[3],
-                         g.moci, g.daui, g.cuoii);
-        }
-        __syncthreads();
+    if (e == 0) return {0, M, M + 1, g.btype + 0 * HYD_SEGL, hi_up, g.bc[0], g.cc[0], g.vbt, g.hmax[0], g.mocj, g.dauj, g.cuoij};
+    if (e == 1) return {0, 2, 1, g.btype + 1 * HYD_SEGL, hi_down, g.bc[1], g.cc[1], g.vbd, g.hmax[1], g.mocj, g.dauj, g.cuoij};
+    if (e == 2) return {1, 2, 1, g.btype + 2 * HYD_SEGL, hi_left, g.bc[2], g.cc[2], g.ubt, g.hmax[2], g.moci, g.daui, g.cuoii};
+    return {1, N, N + 1, g.btype + 3 * HYD_SEGL, hi_right, g.bc[3], g.cc[3], g.ubp, g.hmax[3], g.moci, g.daui, g.cuoii};
+}
+
+__device__ BndRec bnd_compute(const DevGrid& g, const EdgeArgs& a, int i, double t) {
+    BndRec r{0, 0.0, 0.0};
+    const int P = g.P, tt = g.total_time;
+    const int t1 = (int)(t / 3600);
+    const double t2 = (t - (3600.0 * t1)) / 3600.0;
+    int seg_no = -1;
+    if (a.moc[a.location] > 0 && a.dau[a.location * HYD_SEGL] <= i && i <= a.cuoi[a.location * HYD_SEGL]) seg_no = 0;
+    if (seg_no == -1) return r;
+    const double value = a.bcv[seg_no * tt + t1] * (1.0 - t2) + a.bcv[seg_no * tt + t1 + 1] * t2;
+    if (a.btype[seg_no] == 2) {
+        r.kind = 1;
+        r.value = value * a.hi_e[i];
+        const int ii = a.isU ? a.location : i, jj = a.isU ? i : a.location;
+        const double cv = a.ccv[seg_no * tt + t1] * (1.0 - t2) + a.ccv[seg_no * tt + t1 + 1] * t2;
+        r.fsv = cv * g.htaiz_bd[ii * P + jj] * a.hmax;
+    } else {
+        r.kind = 2;
+        r.value = value;
     }
-    if (threadIdx.x == 0) {
-        bnd_edge(g, N, t, 0, 2, 1, g.btype + 1 * HYD_SEGL, hi_down, g.vbd, g.bc[1], g.cc[1], g.hmax[1], g.mocj, g.dauj,
-                 g.cuoij);
-        if (N > M)
-            bnd_edge(g, N, t, 0, M, M + 1, g.btype + 0 * HYD_SEGL, hi_up, g.vbt, g.bc[0], g.cc[0], g.hmax[0], g.mocj,
-                     g.dauj, g.cuoij);
+    return r;
+}
+
+__device__ void bnd_apply(const DevGrid& g, const EdgeArgs& a, const BndRec& r, int i) {
+    const int P = g.P;
+    if (r.kind == 1) {
+        a.barr[i] = r.value;
+        const int ii = a.isU ? a.location : i, jj = a.isU ? i : a.location;
+        g.FS[ii * P + jj] = r.fsv;
+    } else if (r.kind == 2) {
+        if (a.isU) {
+            g.t_z[a.location * P + i] = r.value;
+            g.t_z[a.location_ext * P + i] = r.value;
+        } else {
+            g.t_z[i * P + a.location] = r.value;
+            g.t_z[i * P + a.location_ext] = r.value;
+        }
     }
 }
+
+// Update_Boundary_Value (support_funcs.cu:622-668).  The reference applies the edges in
+// the order up, down, left, right (the order a converged warp applies them); two edges
+// only meet at the corner indices (2 and N of the up/down edges, 2 and M of left/right).
+// Here the four edges run at once, each in a quarter of the CTA (blockDim a multiple of
+// 128), holding back their corner writes; thread 0 then applies those in the reference's
+// order, and again the (N, 2) write of the down edge and, when N > M, the (N, M) write of
+// the up edge, which threads past the first warp repeat in the reference.
+__device__ void boundary_body(const DevGrid& g, double t) {
+    __shared__ BndRec s_rec[4][2];
+    const int N = g.N, M = g.M;
+    const int imax = N > M ? N : M;
+    const int Q = blockDim.x / 4, e = threadIdx.x / Q, r = threadIdx.x % Q;
+    if (e < 4) {
+        const EdgeArgs a = edge_args(g, e);
+        const int far = a.isU ? M : N;
+        for (int i = 2 + r; i <= imax; i += Q) {
+            const BndRec rec = bnd_compute(g, a, i, t);
+            if (i == 2) s_rec[e][0] = rec;
+            else if (i == far) s_rec[e][1] = rec;
+            else bnd_apply(g, a, rec, i);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 4; k++) {
+            const EdgeArgs a = edge_args(g, k);
+            bnd_apply(g, a, s_rec[k][0], 2);
+            bnd_apply(g, a, s_rec[k][1], a.isU ? M : N);
+        }
+        bnd_apply(g, edge_args(g, 1), s_rec[1][1], N);
+        if (N > M) bnd_apply(g, edge_args(g, 0), s_rec[0][1], N);
+    }
+}
+
+__global__ void k_boundary(DevGrid g, DevParams p, int half) { boundary_body(g, g.clock[half]); }
 
 // Channel-mode analytic seiche boundaries (support_funcs.cu:356-429, Engine.py:30-43).
 // Engine.py passes m_offset = 5 as the kernels' segment_limit parameter, so the segment
 // tables are read with a stride of 5; bienQ is read through a bool pointer, i.e. byte e
 // of the int32 array.  Each edge covers at most N (up/down) or M (left/right) indices,
 // the extent of the reference's launch.
-__global__ void k_boundary_channel(DevGrid g, DevParams p, int half) {
-    const double t = g.clock[half];
+__device__ void boundary_channel_body(const DevGrid& g, const DevParams& p, double t) {
     const int N = g.N, M = g.M, P = g.P;
     const int sl = 5;
     const unsigned char* bq = (const unsigned char*)g.bienQ;
@@ -245,6 +275,84 @@ __global__ void k_boundary_channel(DevGrid g, DevParams p, int half) {
             }
         }
         __syncthreads();
+    }
+}
+
+__global__ void k_boundary_channel(DevGrid g, DevParams p, int half) { boundary_channel_body(g, p, g.clock[half]); }
+
+// Continuity and momentum coefficients of one wet cell of a UZ line (column j, cell i):
+// a2, c2, d2 (_uzSolver_calculate_preindex, UVZSolver_multithread.cu:402-406) and f1, f2,
+// f3, f5 (352-400).  Cell-local, so they are computed for every wet cell by a row-major
+// kernel and stored column-major for the column sweep.
+__device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& a2, double& c2,
+                                               double& d2, double& f1, double& f2, double& f3, double& f5) {
+    const int P = g.P;
+    c2 = p.dTchia2dX * g.Htdu[pos];
+    a2 = -p.dTchia2dX * g.Htdu[pos - P];
+    d2 = g.z[pos] - p.dTchia2dY * (g.Htdv[pos] * g.v[pos] - g.Htdv[pos - 1] * g.v[pos - 1]);
+    double pp = 0.0, qq = 0.0;
+    const double* u = g.u;
+    const double* H = g.H_moi;
+    const double vtb = (g.v[pos - 1] + g.v[pos] + g.v[pos + P - 1] + g.v[pos + P]) * 0.25;
+    f1 = p.dTchia2dX * u[pos] + g.VISC[pos] * p.dT / p.dXbp;
+    f2 = -(2 + g.Kx1[pos] * p.dT * sqrt(u[pos] * u[pos] + vtb * vtb) / g.Htdu[pos] + (2 * p.dT * g.VISC[pos]) / p.dXbp);
+    f3 = p.dT * g.VISC[pos] / p.dXbp - p.dTchia2dX * u[pos];
+    if (H[pos - 1] <= p.H_TINH) {
+        if (vtb < 0) {
+            pp = vtb * (-3 * u[pos] + 4 * u[pos + 1] - u[pos + 2]) / p.dY2;
+            qq = (u[pos] - 2 * u[pos + 1] + u[pos + 2]) / p.dYbp;
+        }
+    } else {
+        if (H[pos + 1] <= p.H_TINH) {
+            if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
+                pp = vtb * (3 * u[pos] - 4 * u[pos - 1] + u[pos - 2]) / p.dY2;
+                qq = (u[pos] - 2 * u[pos - 1] + u[pos - 2]) / p.dYbp;
+            }
+        } else {
+            pp = vtb * (u[pos + 1] - u[pos - 1]) / p.dY2;
+            qq = (u[pos + 1] - 2 * u[pos] + u[pos - 1]) / p.dYbp;
+        }
+    }
+    f5 = -2 * u[pos] + p.dT * pp - p.dT * p.CORIOLIS_FORCE * vtb - p.dT * g.VISC[pos] * qq -
+         p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
+}
+
+// First launch of a step: UZ coefficients of every wet interior cell, one warp per row
+// over the row's span of cells that can be wet, written column-major (g.colT arrays 0..6:
+// a2 c2 d2 f1 f2 f3 f5); the last CTA advances the step clock and applies the boundary
+// values of the first half-step (neither reads what the other writes).
+__global__ void __launch_bounds__(1024) k_coef_uz(DevGrid g, DevParams p) {
+    if (blockIdx.x == gridDim.x - 1) {
+        __shared__ double s_t;
+        if (threadIdx.x == 0) {  // k_clock
+            const double t1 = g.clock[2] + p.dT * 0.5;
+            const double t2 = t1 + p.dT * 0.5;
+            g.clock[0] = t1;
+            g.clock[1] = t2;
+            g.clock[2] = t2;
+            s_t = t1;
+        }
+        __syncthreads();
+        if (p.channel) boundary_channel_body(g, p, s_t);
+        else boundary_body(g, s_t);
+        return;
+    }
+    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i > g.N) return;
+    const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
+    for (int j = lo + lane; j <= hi; j += 32) {
+        const int pos = i * g.P + j;
+        if (g.khouot[pos] != 0) continue;
+        double a2, c2, d2, f1, f2, f3, f5;
+        uz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
+        const size_t t = (size_t)j * g.LT + i;
+        colT(g, 0)[t] = a2;
+        colT(g, 1)[t] = c2;
+        colT(g, 2)[t] = d2;
+        colT(g, 3)[t] = f1;
+        colT(g, 4)[t] = f2;
+        colT(g, 5)[t] = f3;
+        colT(g, 6)[t] = f5;
     }
 }
 
@@ -765,6 +873,7 @@ __global__ void k_post_span(DevGrid g) {
 
 // ------------------------------------------------------------- wet-segment scans
 
+template <int AFTER_UPDATE = 1>
 __device__ void fs_edges_block(const DevGrid& g, const DevParams& p);
 
 // Rescan of the listed rows (ROWS) or columns: a line is listed when one of its cells
@@ -776,7 +885,7 @@ template <int ROWS>
 __global__ void k_scan_dirty(DevGrid g, DevParams p, int edges) {
     extern __shared__ unsigned swords[];
     if ((int)blockIdx.x == edges) {
-        fs_edges_block(g, p);
+        fs_edges_block<1>(g, p);
     } else {
         const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int scanning = gridDim.x - (edges >= 0 ? 1 : 0);
@@ -813,7 +922,11 @@ __global__ void k_scan_dirty(DevGrid g, DevParams p, int edges) {
 // Interpolate_FS_ng / Interpolate_FS_d (support_funcs.cu:189-229), run by the row-2,
 // row-N and column-M blocks of the scans in the reference.  Rows first (row 2, then
 // row N), then the column.
+// AFTER_UPDATE = 0: run concurrently with the state update, so u and v (which the update
+// sets to t_u and t_v on i <= N, j <= M) are read as t_u and t_v there.
+template <int AFTER_UPDATE>
 __device__ void fs_edges_block(const DevGrid& g, const DevParams& p) {
+    const double* uu = AFTER_UPDATE ? g.u : g.t_u;
     const int N = g.N, M = g.M, P = g.P;
     const int i_dX = __double2int_rn(p.dX);
     const int j_dY = __double2int_rn(p.dY);
@@ -821,7 +934,7 @@ __device__ void fs_edges_block(const DevGrid& g, const DevParams& p) {
         const int location = pass == 0 ? 2 : N, offset = pass == 0 ? 2 : N - 1, sign = pass == 0 ? 1 : -1;
         for (int j = 1 + threadIdx.x; j < M; j += blockDim.x) {
             if (g.t_u[location * P + j] > 0) {
-                const double deltaX = (g.u[location * P + j] + g.t_u[location * P + j]) * 0.25 * p.dT;
+                const double deltaX = (uu[location * P + j] + g.t_u[location * P + j]) * 0.25 * p.dT;
                 const int i = (int)(offset + sign * (deltaX / p.dX));
                 const int i_deltaX = __double2int_rn(deltaX);
                 if (i < 0 || i + 1 > N + 2) {
@@ -838,7 +951,8 @@ __device__ void fs_edges_block(const DevGrid& g, const DevParams& p) {
         const int location = M, offset = M - 1, sign = -1;
         for (int i = 1 + threadIdx.x; i < M && i <= N + 2; i += blockDim.x) {
             if (g.t_v[i * P + location] > 0) {
-                const double deltaY = (g.v[i * P + location] + g.t_v[i * P + location]) * 0.25 * p.dT;
+                const double vv = (AFTER_UPDATE || i > N) ? g.v[i * P + location] : g.t_v[i * P + location];
+                const double deltaY = (vv + g.t_v[i * P + location]) * 0.25 * p.dT;
                 const int j = (int)(offset + sign * (deltaY / p.dY));
                 const int j_deltaY = __double2int_rn(deltaY);
                 if (j < 0 || j + 1 > M + 2) {
@@ -888,6 +1002,62 @@ __global__ void k_vth_span(DevGrid g, DevParams p) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i > g.N) return;
     for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) vth_cell(g, p, i, j);
+}
+
+// After a half-step's reset, in one launch: the state update (update_uvz + Htuongdoi)
+// and, when VTH, Find_VTH + hesoK on the extended spans (CTAs [0, nbp), one warp per
+// row; both only read the cell's own new Htdu/Htdv); the rescan of the changed lines of
+// the other direction (CTAs [nbp, nbp + nbs)); and the edge concentration interpolation
+// (last CTA, reading t_u / t_v where the reference reads u / v after the update).  None of
+// the three writes what another reads.
+template <int ROWS, int VTH>
+__global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
+    extern __shared__ unsigned swords[];
+    const int b = blockIdx.x;
+    if (b < nbp) {
+        const int i = (b * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+        if (i > g.N) return;
+        for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) {
+            post_cell(g, 1, i, j);
+            if (VTH) vth_cell(g, p, i, j);
+        }
+        return;
+    }
+    if (b == (int)gridDim.x - 1) {
+        fs_edges_block<0>(g, p);
+        return;
+    }
+    const int sb = b - nbp;
+    {
+        const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int n = *(volatile unsigned*)&g.dctr[ROWS ? 0 : 1];
+        const int L = ROWS ? g.M : g.N;
+        const int Lines = ROWS ? g.N : g.M;
+        const int nwords = (L + 63) / 32 + 1;
+        unsigned* words = swords + warp * nwords;
+        int* flags = ROWS ? g.dirty_r : g.dirty_c;
+        const int* list = ROWS ? g.dlist_r : g.dlist_c;
+        for (int k = sb * warps + warp; k < n; k += nbs * warps) {
+            const int line = list[k];
+            if (lane == 0) flags[line] = 0;
+            if (line < 2 || line > Lines) continue;
+            const int lo = ROWS ? g.rlo[line] : g.clo[line];
+            const int hi = ROWS ? g.rhi[line] : g.chi[line];
+            const WetGlobal wet{g.khouot, ROWS ? line * g.P : line, ROWS ? 1 : g.P};
+            if (ROWS) warp_scan_line(g, wet, lo, hi, L, words, g.daui + line * HYD_SEGL, g.cuoii + line * HYD_SEGL, g.moci + line);
+            else warp_scan_line(g, wet, lo, hi, L, words, g.dauj + line * HYD_SEGL, g.cuoij + line * HYD_SEGL, g.mocj + line);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // the last rescanning CTA empties the list
+        __threadfence();
+        unsigned* done = &g.dctr[ROWS ? 2 : 3];
+        if (atomicAdd(done, 1u) == (unsigned)nbs - 1) {
+            g.dctr[ROWS ? 0 : 1] = 0;
+            *done = 0;
+            __threadfence();
+        }
+    }
 }
 
 // Update_FS (Sediment_Transport.cu:620-629)
@@ -1086,6 +1256,10 @@ cudaError_t grid_setup(int N, int M) {
     cudaError_t e;
     if ((e = allow_smem((const void*)k_scan_dirty<1>, scan_smem(g))) != cudaSuccess) return e;
     if ((e = allow_smem((const void*)k_scan_dirty<0>, scan_smem(g))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_post_fused<0, 0>, scan_smem(g))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_post_fused<0, 1>, scan_smem(g))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_post_fused<1, 0>, scan_smem(g))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_post_fused<1, 1>, scan_smem(g))) != cudaSuccess) return e;
     if ((e = allow_smem((const void*)k_explicit_u, sizeof(double) * (N + 3))) != cudaSuccess) return e;
     if ((e = allow_smem((const void*)k_explicit_v, sizeof(double) * (M + 3))) != cudaSuccess) return e;
     if ((e = allow_smem((const void*)k_reset<1>, reset_smem(M))) != cudaSuccess) return e;
@@ -1145,12 +1319,13 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
 
 void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s) {
     if (p.channel) k_boundary_channel<<<1, 256, 0, s>>>(g, p, half);
-    else k_boundary<<<1, 1024, 0, s>>>(g, p, half);
+    else k_boundary<<<1, 512, 0, s>>>(g, p, half);
     hyd_kernel_launches_add(1);
 }
 
-void launch_clock(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_clock<<<1, 1, 0, s>>>(g, p.dT);
+// The step's first launch: k_coef_uz with the clock and the first boundary update.
+void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s) {
+    k_coef_uz<<<((g.N - 1) * 32 + 1023) / 1024 + 1, 1024, 0, s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
@@ -1207,6 +1382,21 @@ void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s) {
 
 void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s) {
     scan_dirty(g, p, 1, 1, s);
+    hyd_kernel_launches_add(1);
+}
+
+// The fused update / rescan / interpolation launch (k_post_fused); rows: which direction
+// is rescanned.
+void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s) {
+    const int nbp = (g.N + 1) * 32 / 256 + 1, nbs = 32;
+    const int grid = nbp + nbs + 1;
+    if (rows) {
+        if (vth) k_post_fused<1, 1><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
+        else k_post_fused<1, 0><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
+    } else {
+        if (vth) k_post_fused<0, 1><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
+        else k_post_fused<0, 0><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
+    }
     hyd_kernel_launches_add(1);
 }
 

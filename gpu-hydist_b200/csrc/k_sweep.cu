@@ -313,65 +313,6 @@ __device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p
     G::sync();
 }
 
-// Continuity and momentum coefficients of one wet cell of a UZ line (column j, cell i):
-// a2, c2, d2 (_uzSolver_calculate_preindex, UVZSolver_multithread.cu:402-406) and f1, f2,
-// f3, f5 (352-400).  Cell-local, so they are computed for every wet cell by a row-major
-// kernel and stored column-major for the column sweep.
-__device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& a2, double& c2,
-                                               double& d2, double& f1, double& f2, double& f3, double& f5) {
-    const int P = g.P;
-    c2 = p.dTchia2dX * g.Htdu[pos];
-    a2 = -p.dTchia2dX * g.Htdu[pos - P];
-    d2 = g.z[pos] - p.dTchia2dY * (g.Htdv[pos] * g.v[pos] - g.Htdv[pos - 1] * g.v[pos - 1]);
-    double pp = 0.0, qq = 0.0;
-    const double* u = g.u;
-    const double* H = g.H_moi;
-    const double vtb = (g.v[pos - 1] + g.v[pos] + g.v[pos + P - 1] + g.v[pos + P]) * 0.25;
-    f1 = p.dTchia2dX * u[pos] + g.VISC[pos] * p.dT / p.dXbp;
-    f2 = -(2 + g.Kx1[pos] * p.dT * sqrt(u[pos] * u[pos] + vtb * vtb) / g.Htdu[pos] + (2 * p.dT * g.VISC[pos]) / p.dXbp);
-    f3 = p.dT * g.VISC[pos] / p.dXbp - p.dTchia2dX * u[pos];
-    if (H[pos - 1] <= p.H_TINH) {
-        if (vtb < 0) {
-            pp = vtb * (-3 * u[pos] + 4 * u[pos + 1] - u[pos + 2]) / p.dY2;
-            qq = (u[pos] - 2 * u[pos + 1] + u[pos + 2]) / p.dYbp;
-        }
-    } else {
-        if (H[pos + 1] <= p.H_TINH) {
-            if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
-                pp = vtb * (3 * u[pos] - 4 * u[pos - 1] + u[pos - 2]) / p.dY2;
-                qq = (u[pos] - 2 * u[pos - 1] + u[pos - 2]) / p.dYbp;
-            }
-        } else {
-            pp = vtb * (u[pos + 1] - u[pos - 1]) / p.dY2;
-            qq = (u[pos + 1] - 2 * u[pos] + u[pos - 1]) / p.dYbp;
-        }
-    }
-    f5 = -2 * u[pos] + p.dT * pp - p.dT * p.CORIOLIS_FORCE * vtb - p.dT * g.VISC[pos] * qq -
-         p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
-}
-
-// UZ coefficients of every wet interior cell, one warp per row over the row's span of
-// cells that can be wet; written column-major (g.colT arrays 0..6: a2 c2 d2 f1 f2 f3 f5).
-__global__ void k_coef_uz(DevGrid g, DevParams p) {
-    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (i > g.N) return;
-    const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
-    for (int j = lo + lane; j <= hi; j += 32) {
-        const int pos = i * g.P + j;
-        if (g.khouot[pos] != 0) continue;
-        double a2, c2, d2, f1, f2, f3, f5;
-        uz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
-        const size_t t = (size_t)j * g.LT + i;
-        colT(g, 0)[t] = a2;
-        colT(g, 1)[t] = c2;
-        colT(g, 2)[t] = d2;
-        colT(g, 3)[t] = f1;
-        colT(g, 4)[t] = f2;
-        colT(g, 5)[t] = f3;
-        colT(g, 6)[t] = f5;
-    }
-}
-
 // Phases A-D of one line by group G.  Rows A, B, Cc, D hold at least G::size * m
 // entries, cells a2, c2, d2 at least sg.C.
 template <int DIR, int SOLVER, class G>
@@ -1019,11 +960,6 @@ void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp
     hyd_kernel_launches_add(1);
 }
 }  // namespace
-
-void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_coef_uz<<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p);
-    hyd_kernel_launches_add(1);
-}
 
 void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s) {
     k_coef_fsj<<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p, half);
