@@ -447,7 +447,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     total += 2 * a256((M + 3) * 8) + 2 * a256((N + 3) * 8) + a256((2 * (N + 3) + 2 * (M + 3)) * 8);
     total += a256(4 * 8) + a256(4 * 4) + a256(4 * HYD_SEGL * 4) + a256(64) + a256(64);
     total += 4 * a256((N + 3) * 4) + 4 * a256((M + 3) * 4) + a256(64);  // spans, rescan flags and lists
-    total += 2 * a256((N + 3) * 4) + a256(64);                          // extended spans
+    total += 2 * a256((N + 3) * 4) + 2 * a256(64);                      // extended spans, flags
     e = cudaMalloc(&s->arena, total);
     if (e != cudaSuccess) {
         cudaStreamDestroy(s->stream);
@@ -502,6 +502,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.elo = (int*)take((N + 3) * 4);
     g.ehi = (int*)take((N + 3) * 4);
     g.span_wide = (int*)take(64);
+    g.dflag = (int*)take(64);
     g.clock = (double*)take(64);
     if ((size_t)(cur - (char*)s->arena) > total) {
         cudaFree(s->arena);
@@ -590,7 +591,31 @@ int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count
     } else if (f->kind >= 2 && f->kind <= 5) {
         h->force_rescan = 1;  // segment tables
     }
-    h->full_pending = 3;  // any field may feed the elementwise kernels outside the spans
+    // A field the elementwise kernels may read or bring up to date outside the extended
+    // spans owes whole-grid passes, unless it is one of z, u, v, FS and equals there what
+    // those passes would leave (t_z, t_u, t_v; tFS once a sediment pass has run).
+    const DevGrid& G = h->g;
+    int owed = 3;
+    if (h->initialized) {
+        const double* partner = nullptr;
+        int i0 = 0, j0 = 0;
+        if (dst == (void*)G.u) partner = G.t_u;
+        else if (dst == (void*)G.v) partner = G.t_v;
+        else if (dst == (void*)G.z) partner = G.t_z;
+        else if (dst == (void*)G.FS) {
+            owed = 2;  // read by the sediment kernels only
+            if (!(h->full_pending & 2)) {
+                partner = G.tFS;
+                i0 = j0 = 1;
+            }
+        }
+        if (partner) {
+            const int d = outside_differs(G, (const double*)dst, partner, i0, h->N, j0, h->M, G.dflag, h->stream);
+            if (d < 0) return fail(HYD_ECUDA, "set-field span check failed");
+            if (!d) owed = 0;
+        }
+    }
+    h->full_pending |= owed;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return HYD_OK;

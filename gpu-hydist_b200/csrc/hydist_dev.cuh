@@ -50,6 +50,7 @@ struct DevGrid {
     // elementwise kernels run once the whole grid has been brought up to date
     int *elo, *ehi;
     int* span_wide;  // set when a velocity lies outside the extended spans
+    int* dflag;      // scratch flag of the set-field check
     // lines whose mask changed since their segments were scanned: flags and lists
     int *dirty_r, *dirty_c, *dlist_r, *dlist_c;
     unsigned* dctr;  // [0] listed rows, [1] listed columns, [2] [3] CTAs of the rescans done
@@ -139,6 +140,9 @@ void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, int thre
 void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_spans(const DevGrid& g, cudaStream_t s);
 void clear_rescan_lists(const DevGrid& g, cudaStream_t s);
+// 1 if a and b differ outside the extended spans on [i0, i1] x [j0, j1], 0 if not, -1 on error
+int outside_differs(const DevGrid& g, const double* a, const double* b, int i0, int i1, int j0, int j1, int* dflag,
+                    cudaStream_t s);
 void launch_mark_all_cols(const DevGrid& g, cudaStream_t s);
 void launch_post(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
 void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);

@@ -823,6 +823,18 @@ __global__ void k_widen_spans(DevGrid g) {
     g.ehi[i] = g.M + 2;
 }
 
+// *flag = 1 if a and b differ at a cell of [i0, i1] x [j0, j1] outside the extended span
+// of its row (where the span-limited kernels would not bring them together).
+__global__ void k_outside_diff(DevGrid g, const double* a, const double* b, int i0, int i1, int j0, int j1,
+                               int* flag) {
+    const int j = j0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = i0 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > i1 || j > j1) return;
+    if (j >= g.elo[i] && j <= g.ehi[i]) return;
+    const int pos = i * g.P + j;
+    if (a[pos] != b[pos] && !(a[pos] != a[pos] && b[pos] != b[pos])) *flag = 1;
+}
+
 // List every row (ROWS) or column of the grid for a segment rescan.
 template <int ROWS>
 __global__ void k_mark_all(DevGrid g) {
@@ -1283,6 +1295,18 @@ void launch_spans(const DevGrid& g, cudaStream_t s) {
 void launch_widen_spans(const DevGrid& g, cudaStream_t s) {
     k_widen_spans<<<(g.N + 3 + 127) / 128, 128, 0, s>>>(g);
     hyd_kernel_launches_add(1);
+}
+
+int outside_differs(const DevGrid& g, const double* a, const double* b, int i0, int i1, int j0, int j1, int* dflag,
+                    cudaStream_t s) {
+    int h = 0;
+    if (cudaMemsetAsync(dflag, 0, sizeof(int), s) != cudaSuccess) return -1;
+    const dim3 bl(32, 8);
+    k_outside_diff<<<grid2d(j1 - j0 + 1, i1 - i0 + 1, bl), bl, 0, s>>>(g, a, b, i0, i1, j0, j1, dflag);
+    hyd_kernel_launches_add(1);
+    if (cudaMemcpyAsync(&h, dflag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+    return h;
 }
 
 // Empty the rescan lists.

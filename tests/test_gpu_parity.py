@@ -97,3 +97,51 @@ def test_gpu_config2_first_steps_vs_oracle(oracle_lib, monkeypatch):
         sim.step(k)
         ora.step(k)
         _check(sim, ora.get, "config2 t=%g" % ora.t)
+
+
+def test_gpu_config2_fields_set_mid_run_vs_oracle(oracle_lib, monkeypatch):
+    """Fields written between steps (the host round trip of Engine.py's output loop): an
+    unchanged write keeps the span-limited step; a velocity written on never-wet cells
+    away from every wet run forces whole-grid passes.  Both against the oracle given the
+    same writes."""
+    import oracle
+    from hydist import cases
+    c = cases.config2_case()
+    sim = _sim(c, "partitioned", monkeypatch)
+    sim.step(1850)          # sediment active from t = 1800 s
+    ora = oracle.OracleSim(c)
+    ora.load_state(sim.get, sim.t, sim.get("hmax"))
+    for f in ("z", "u", "v", "FS"):
+        sim.set(f, sim.get(f))
+    sim.step(10)
+    ora.step(10)
+    _check(sim, ora.get, "unchanged writes t=%g" % ora.t)
+    # a never-wet cell at least 8 cells from any cell that can be wet, in its row and column
+    kh = sim.get("khouot")
+    N, M = c.N, c.M
+    open_ = kh != 2
+    i0, j0 = None, None
+    for i in range(2, N - 1):
+        cols = np.flatnonzero(open_[i])
+        for j in range(2, M - 1):
+            if kh[i, j] != 2:
+                continue
+            if cols.size and np.abs(cols - j).min() < 8:
+                continue
+            if open_[max(i - 8, 0):i + 9, j].any():
+                continue
+            i0, j0 = i, j
+            break
+        if i0 is not None:
+            break
+    assert i0 is not None
+    u = sim.get("u")
+    u[i0, j0] = 0.05
+    sim.set("u", u)
+    ora.view("u")[i0, j0] = 0.05
+    sim.step(10)
+    ora.step(10)
+    _check(sim, ora.get, "u written at (%d, %d) t=%g" % (i0, j0, ora.t))
+    sim.step(5)
+    ora.step(5)
+    _check(sim, ora.get, "after the whole-grid pass t=%g" % ora.t)
