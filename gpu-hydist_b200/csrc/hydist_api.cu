@@ -79,8 +79,8 @@ struct HydSim {
     int solver;
     int start_idx, end_idx;
     unsigned* h_status;
-    // phase timing (instrumentation)
-    int timing;
+    // phase timing (instrumentation): bit k set = phase k bracketed by events
+    unsigned timing;
     struct Mark {
         int phase;
         cudaEvent_t a, b;
@@ -109,9 +109,11 @@ struct HydSim {
 
 static const char* kPhaseNames[] = {"boundary", "sweep_uz", "sweep_vz", "smooth", "explicit_v", "explicit_u",
                                     "reset_rows", "reset_cols", "post", "scan", "vth_hesok", "fs_sweep_j",
-                                    "fs_sweep_i", "update_fs", "bed"};
+                                    "fs_sweep_i", "update_fs", "bed", "coef_uz", "coef_fsj", "coef_eu"};
 enum Phase { PH_BOUNDARY, PH_SWEEP_UZ, PH_SWEEP_VZ, PH_SMOOTH, PH_EXPL_V, PH_EXPL_U, PH_RESET_ROWS,
-             PH_RESET_COLS, PH_POST, PH_SCAN, PH_VTH, PH_FS_J, PH_FS_I, PH_UPDATE_FS, PH_BED, PH_COUNT };
+             PH_RESET_COLS, PH_POST, PH_SCAN, PH_VTH, PH_FS_J, PH_FS_I, PH_UPDATE_FS, PH_BED, PH_COEF_UZ,
+             PH_COEF_FSJ, PH_COEF_EU, PH_COUNT };
+static_assert(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]) == PH_COUNT, "one name per phase");
 
 namespace {
 void drop_graphs(HydSim* s) {
@@ -182,13 +184,13 @@ struct PhaseScope {
         else cudaEventRecord(e, s->stream);
     }
     PhaseScope(HydSim* s_, int ph_) : s(s_), ph(ph_) {
-        if (s->timing) {
+        if ((s->timing >> ph) & 1u) {
             a = pool_event(s);
             record(s, a);
         }
     }
     ~PhaseScope() {
-        if (s->timing) {
+        if (a) {
             cudaEvent_t b = pool_event(s);
             record(s, b);
             (s->mark_sink ? *s->mark_sink : s->marks).push_back({ph, a, b});
@@ -521,7 +523,8 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     }
     s->g.LT = (N + 3 + 31) / 32 * 32;
     s->g.colT_stride = (size_t)(M + 3) * s->g.LT;
-    e = cudaMalloc(&s->g.colT, 7 * s->g.colT_stride * sizeof(double));
+    e = cudaMalloc(&s->g.colT, 7 * s->g.colT_stride * sizeof(double) + s->g.colT_stride);
+    s->g.colB = (unsigned char*)(s->g.colT + 7 * s->g.colT_stride);
     if (e != cudaSuccess) {
         cudaFree(s->arena);
         cudaStreamDestroy(s->stream);
@@ -731,12 +734,12 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         start_idx = 3;
         end_idx = s->M - 1;
     }
-    { PHASE(PH_BOUNDARY); launch_coef_uz(g, p, st); }
+    { PHASE(PH_COEF_UZ); launch_coef_uz(g, p, st); }
     { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_EXPL_V); launch_explicit_v(g, p, s->thr_r, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, st); }
     std::swap(g.t_v, s->scratch_v);
     if (force) launch_mark_all_cols(g, st);
     { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, s->thr_r, st); }
@@ -752,7 +755,8 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     }
     if (sed1) {
         if (!(sed1 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
-        { PHASE(PH_FS_J); launch_coef_fsj(g, p, 0, st); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
+        { PHASE(PH_COEF_FSJ); launch_coef_fsj(g, p, 0, st); }
+        { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
     }
     // ---- half-step 2: implicit along j (rows), explicit u
@@ -764,10 +768,11 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         end_idx = s->N;
     }
     { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, st); }
     std::swap(g.t_v, s->scratch_v);
-    { PHASE(PH_EXPL_U); launch_coef_eu(g, p, st); launch_explicit_u(g, p, s->thr_c, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, st); }
+    { PHASE(PH_COEF_EU); launch_coef_eu(g, p, st); }
+    { PHASE(PH_EXPL_U); launch_explicit_u(g, p, s->thr_c, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 1, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }
     if (!fh) {
@@ -1030,9 +1035,32 @@ int hyd_get_stream(hyd_handle h, void** stream) {
     return HYD_OK;
 }
 
-int hyd_set_timing(hyd_handle h, int enable) {
+int hyd_set_timing_phases(hyd_handle h, unsigned phase_mask) {
     if (!h) return fail(HYD_EINVAL, "null handle");
-    h->timing = enable ? 1 : 0;
+    phase_mask &= (1u << PH_COUNT) - 1u;
+    if (phase_mask != h->timing) {
+        // the timed graphs hold the event records of the previous selection
+        CUDA_TRY(cudaSetDevice(h->device));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        for (int k = 0; k < 8; k++) {
+            if (h->tgraph[k]) cudaGraphExecDestroy(h->tgraph[k]);
+            h->tgraph[k] = nullptr;
+            for (auto& m : h->tmarks[k]) {
+                cudaEventDestroy(m.a);
+                cudaEventDestroy(m.b);
+            }
+            h->tmarks[k].clear();
+        }
+    }
+    h->timing = phase_mask;
+    return HYD_OK;
+}
+
+int hyd_set_timing(hyd_handle h, int enable) { return hyd_set_timing_phases(h, enable ? ~0u : 0u); }
+
+int hyd_phase_name(int phase, const char** name) {
+    if (!name || phase < 0 || phase >= PH_COUNT) return fail(HYD_EINVAL, "phase out of range");
+    *name = kPhaseNames[phase];
     return HYD_OK;
 }
 

@@ -57,6 +57,7 @@ struct DevGrid {
     // column-major copies of per-cell quantities for the column sweeps: 7 arrays of
     // (M+3) columns x LT rows (LT = N+3 rounded up to 32), array k at colT + k*colT_stride
     double* colT;
+    unsigned char* colB;  // column-major reset bytes of the column resets (stride LT)
     size_t colT_stride;
     int LT;
     double* clock;  // [0] time of half-step 1, [1] time of half-step 2, [2] time at the step start
@@ -131,11 +132,13 @@ void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, 
                      int solver, double* scratch, cudaStream_t s);
 void launch_sweep_vz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
                      int solver, double* scratch, cudaStream_t s);
-void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, cudaStream_t s);
+// bytes: also write the column reset bytes (the smoothing of u just before the column resets)
+void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, cudaStream_t s);
 void launch_widen_spans(const DevGrid& g, cudaStream_t s);
 void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
 void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
 void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s);
+// threads: a multiple of 32
 void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_spans(const DevGrid& g, cudaStream_t s);

@@ -388,14 +388,41 @@ __device__ __forceinline__ void smooth_cell(const DevGrid& g, const DevParams& p
     out[gp] = r;
 }
 
-__global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
-    smooth_cell(g, p, isU, out, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x, true);
+// The column-major reset byte of cell (i, j) for the column resets that follow (k_reset
+// columns): mask | (t_z > z, rows 2..N) << 2 | (wet with H <= H_TINH, rows 2..N) << 3,
+// after update_h_moi (support_funcs.cu:60-73) on the wet cells of 1..N x 1..M.
+__device__ __forceinline__ void reset_byte_cell(const DevGrid& g, const DevParams& p, int i, int j) {
+    if (i >= g.N + 3 || j >= g.M + 3) return;
+    const int gp = i * g.P + j;
+    const int kv = g.khouot[gp];
+    const double tz = g.t_z[gp];
+    unsigned b = (unsigned)kv;
+    if (i >= 2 && i <= g.N && tz > g.z[gp]) b |= 4u;
+    if (kv == 0 && i >= 1 && i <= g.N && j >= 1 && j <= g.M) {
+        const double hv = g.htaiz[gp] + tz;
+        g.H_moi[gp] = hv;
+        if (i >= 2 && hv <= p.H_TINH) b |= 8u;
+    }
+    g.colB[(size_t)j * g.LT + i] = (unsigned char)b;
 }
 
+// BYTES: also write the column reset bytes (the smoothing of u right before the column
+// resets; H_moi is not read in between).
+template <int BYTES>
+__global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
+    const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    smooth_cell(g, p, isU, out, i, j, true);
+    if (BYTES) reset_byte_cell(g, p, i, j);
+}
+
+template <int BYTES>
 __global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i > g.N + 2) return;
-    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) smooth_cell(g, p, isU, out, i, j, false);
+    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) {
+        smooth_cell(g, p, isU, out, i, j, false);
+        if (BYTES) reset_byte_cell(g, p, i, j);
+    }
 }
 
 // ----------------------------------------------------------- explicit momentum
@@ -674,17 +701,32 @@ struct WetGlobal {  // mask in HBM: cell k at kh[base + k * along]
     __device__ bool operator()(int k) const { return kh[base + k * along] == 0; }
 };
 
+// Words of each k_reset bitset: one bit per cell of a line.
+__host__ __device__ __forceinline__ int reset_words(int L) { return (L + 3) / 32 + 2; }
+
 // update_h_moi (support_funcs.cu:60-73) and Reset_states_horizontal/_vertical
 // (support_funcs.cu:75-186) for one line.  ROWS: line = row i (1..N), cells j (2..M);
 // otherwise line = column j (1..M), cells i (2..N).
 // Cells whose mask is 2 never change (only 0 <-> 1 transitions exist), so each line is
 // staged in shared memory over its span [lo, hi] of cells that are not 2, widened by one
-// cell: nothing outside can act or be acted on.  The opening pass is a serial scan in the
-// reference; an iteration can only act next to a cell whose mask is 1 at the start of the
-// pass, so warp 0 ballots those candidates and lane 0 runs them in increasing order.
+// cell: nothing outside can act or be acted on.
+// The opening pass is a serial scan in the reference.  Iteration k acts when t_z[k] >
+// z[k] and a neighbour's mask is 1; the only value it passes on is through the cell k+1
+// it opens, whose t_z it sets, so iteration k+1 then tests that value (a cascade through
+// a run of 1s).  Every other iteration sees the t_z, z and mask 1s of the start of the
+// pass.  So the CTA tests t_z[k] > z[k] and the mask-1 neighbours for all cells at once
+// (bitsets), and one thread runs only the cells that pass, in increasing order, each
+// with its cascade.  The closing pass closes the cells that are wet after the opening
+// pass with H <= H_TINH: the cells wet from the start (their H is update_h_moi's) and
+// the cells just opened (H stored with the opening), known as a bitset too.
+// Rows stage the mask, t_z and z of the row (coalesced) and apply update_h_moi here.
+// Columns read the column-major byte the preceding smoothing pass wrote per cell (mask,
+// t_z > z, wet with H <= H_TINH; it also applied update_h_moi), so a column is one
+// coalesced byte read instead of strided loads.
 // A line only changes its own cells, so its segments are rescanned here when a cell
 // changed (or when `force`); every changed cell marks its line of the other direction
 // for the rescan that follows.
+// blockDim.x is a multiple of 32: each warp pass covers whole 32-cell words.
 template <int ROWS>
 __global__ void k_reset(DevGrid g, DevParams p, int force) {
     extern __shared__ unsigned char rsm[];
@@ -708,52 +750,101 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
     unsigned* octr = g.dctr + (ROWS ? 1 : 0);
     const int k0 = lo - 1 > 0 ? lo - 1 : 0;
     const int k1 = hi + 1 < L + 2 ? hi + 1 : L + 2;
+    const int nwords = reset_words(L);
     signed char* khs = (signed char*)rsm;                       // khs[k - k0], k in [k0, k1]
-    unsigned* words = (unsigned*)(rsm + ((L + 3 + 15) & ~15));  // scan words
+    unsigned* c0w = (unsigned*)(rsm + ((L + 3 + 15) & ~15));    // t_z > z bits, then scan words
+    unsigned* evw = c0w + nwords;                               // cells the opening pass runs
+    unsigned* clw = evw + nwords;                               // cells the closing pass closes
     auto khv = [&](int k) -> int { return (k >= k0 && k <= k1) ? khs[k - k0] : 2; };
     double *H = g.H_moi, *t_z = g.t_z, *FS = g.FS;
+    const double* z = g.z;
     int* kh = g.khouot;
-    if (threadIdx.x == 0) s_changed = 0;
-    for (int k = k0 + threadIdx.x; k <= k1; k += blockDim.x) {
-        const int gp = base + k * along;
-        const int kv = kh[gp];
-        khs[k - k0] = (signed char)kv;
-        if (k >= 1 && k <= L && kv == 0) H[gp] = g.htaiz[gp] + t_z[gp];
+    const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_changed = 0;
+    // staging: the mask and the bits of every cell of [k0, k1]
+    for (int kb0 = k0; kb0 <= k1; kb0 += T) {  // uniform over the CTA
+        const int k = kb0 + tid;
+        const bool in = k <= k1;
+        bool c0 = false, cl = false;
+        if constexpr (ROWS) {
+            if (in) {
+                const int gp = base + k;
+                const int kv = kh[gp];
+                khs[k - k0] = (signed char)kv;
+                const double tz = t_z[gp];
+                c0 = k >= 2 && k <= L && tz > z[gp];
+                if (k >= 1 && k <= L && kv == 0) {
+                    const double hv = g.htaiz[gp] + tz;
+                    H[gp] = hv;
+                    cl = k >= 2 && hv <= p.H_TINH;
+                }
+            }
+        } else {
+            const unsigned b = in ? g.colB[(size_t)line * g.LT + k] : 2u;
+            if (in) khs[k - k0] = (signed char)(b & 3u);
+            c0 = (b >> 2) & 1u;
+            cl = (b >> 3) & 1u;
+        }
+        const unsigned c0b = __ballot_sync(0xffffffffu, c0), clb = __ballot_sync(0xffffffffu, cl);
+        const int q = (kb0 - k0 + warp * 32) >> 5;
+        if (lane == 0 && kb0 + warp * 32 <= k1) {
+            c0w[q] = c0b;
+            clw[q] = clb;
+        }
     }
     __syncthreads();
-    // opening pass (loop 1)
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        const int ka = k0 > 2 ? k0 : 2, kb = k1 < L ? k1 : L;
-        for (int c0 = ka; c0 <= kb; c0 += 32) {
-            const int k = c0 + lane;
-            const bool cand = (k <= kb) && (khv(k - 1) == 1 || khv(k + 1) == 1);
-            unsigned mask = __ballot_sync(0xffffffffu, cand);
+    // the cells the opening pass runs: t_z > z with a neighbour whose mask is 1
+    const int nq = (k1 - k0) / 32 + 1;
+    int anyev = 0;
+    for (int q = warp; q < nq; q += T >> 5) {
+        const int k = k0 + q * 32 + lane;
+        const bool ev = ((c0w[q] >> lane) & 1u) && (khv(k - 1) == 1 || khv(k + 1) == 1);
+        const unsigned bits = __ballot_sync(0xffffffffu, ev);
+        if (lane == 0) evw[q] = bits;
+        anyev |= bits != 0;
+    }
+    // opening pass (loop 1), serial over those cells
+    if (__syncthreads_or(anyev) && warp == 0) {
+        const int kb = k1 < L ? k1 : L;
+        int done = -1;
+        auto open = [&](int kk, double tzv, double fsv) {
+            const int gq = base + kk * along;
+            const double hv = g.htaiz[gq] + tzv;
+            t_z[gq] = tzv;
+            H[gq] = hv;
+            kh[gq] = 0;
+            khs[kk - k0] = 0;
+            FS[gq] = fsv;
+            if (kk >= 2 && kk <= L && hv <= p.H_TINH) clw[(kk - k0) >> 5] |= 1u << ((kk - k0) & 31);
+            s_changed = 1;
+            mark_dirty(oflags, olist, octr, kk);
+        };
+        for (int q0 = 0; q0 < nq; q0 += 32) {
+            const unsigned wl = q0 + lane < nq ? evw[q0 + lane] : 0u;
+            unsigned nz = __ballot_sync(0xffffffffu, wl != 0);
             if (lane == 0) {
-                while (mask) {
-                    const int kk = c0 + __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const int gp = base + kk * along;
-                    if (t_z[gp] > g.z[gp]) {
-                        if (khv(kk - 1) == 1) {
-                            const int gm = gp - along;
-                            t_z[gm] = t_z[gp];
-                            H[gm] = g.htaiz[gm] + t_z[gp];
-                            kh[gm] = 0;
-                            khs[kk - 1 - k0] = 0;
-                            FS[gm] = FS[gp];
-                            s_changed = 1;
-                            mark_dirty(oflags, olist, octr, kk - 1);
-                        }
-                        if (khv(kk + 1) == 1) {
-                            const int gq = gp + along;
-                            t_z[gq] = t_z[gp];
-                            H[gq] = g.htaiz[gq] + t_z[gp];
-                            kh[gq] = 0;
-                            khs[kk + 1 - k0] = 0;
-                            FS[gq] = FS[gp];
-                            s_changed = 1;
-                            mark_dirty(oflags, olist, octr, kk + 1);
+                while (nz) {
+                    const int q = q0 + __ffs(nz) - 1;
+                    nz &= nz - 1;
+                    unsigned w = evw[q];
+                    while (w) {
+                        int m = k0 + q * 32 + __ffs(w) - 1;
+                        w &= w - 1;
+                        if (m <= done) continue;  // already run inside a cascade
+                        const double tzv = t_z[base + m * along], fsv = FS[base + m * along];
+                        bool act = true;
+                        for (;;) {
+                            done = m;
+                            if (!act) break;
+                            bool right = false;
+                            if (khv(m - 1) == 1) open(m - 1, tzv, fsv);
+                            if (khv(m + 1) == 1) {
+                                open(m + 1, tzv, fsv);
+                                right = true;
+                            }
+                            if (!right || m + 1 > kb) break;
+                            m++;  // the opened cell now holds tzv
+                            act = tzv > z[base + m * along];
                         }
                     }
                 }
@@ -763,25 +854,33 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
     }
     __syncthreads();
     // closing pass (loop 2): independent per cell
-    const int ca = lo > 2 ? lo : 2, cb = hi < L ? hi : L;
-    for (int k = ca + threadIdx.x; k <= cb; k += blockDim.x) {
+    for (int q = warp; q < nq; q += T >> 5) {
+        if (!((clw[q] >> lane) & 1u)) continue;
+        const int k = k0 + q * 32 + lane;
         const int gp = base + k * along;
-        if (khs[k - k0] == 0 && H[gp] <= p.H_TINH) {
-            g.t_u[gp - P] = 0;
-            g.t_u[gp] = 0;
-            g.t_v[gp - 1] = 0;
-            g.t_v[gp] = 0;
-            kh[gp] = 1;
-            khs[k - k0] = 1;
-            FS[gp] = 0;
-            s_changed = 1;
-            mark_dirty(oflags, olist, octr, k);
-        }
+        g.t_u[gp - P] = 0;
+        g.t_u[gp] = 0;
+        g.t_v[gp - 1] = 0;
+        g.t_v[gp] = 0;
+        kh[gp] = 1;
+        khs[k - k0] = 1;
+        FS[gp] = 0;
+        s_changed = 1;
+        mark_dirty(oflags, olist, octr, k);
     }
     __syncthreads();
-    if (threadIdx.x < 32 && line >= 2 && (s_changed || force))
-        warp_scan_line(g, WetShared{khs, k0}, lo, hi, L, words, dau, cuoi, moc);
+    if (tid < 32 && line >= 2 && (s_changed || force))
+        warp_scan_line(g, WetShared{khs, k0}, lo, hi, L, c0w, dau, cuoi, moc);
     __syncthreads();  // keep the other warps resident while warp 0 scans
+}
+
+// Column-major mask bytes of the whole grid (the cells outside the extended spans keep
+// them: their mask is 2 for good).
+__global__ void k_reset_bytes_init(DevGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.N + 3 || j >= g.M + 3) return;
+    g.colB[(size_t)j * g.LT + i] = (unsigned char)g.khouot[i * g.P + j];
 }
 
 // Spans of the cells whose mask is not 2: rows [rlo, rhi], columns [clo, chi] (the
@@ -1234,7 +1333,8 @@ size_t scan_smem(const DevGrid& g) {
     const int L = g.N > g.M ? g.N : g.M;
     return sizeof(unsigned) * (kScanThreads / 32) * ((L + 63) / 32 + 1);
 }
-size_t reset_smem(int L) { return ((L + 3 + 15) & ~15) + sizeof(unsigned) * ((L + 63) / 32 + 1); }
+// dynamic shared memory of k_reset: the line's mask bytes and two bitsets / scan words
+size_t reset_smem(int L) { return ((L + 3 + 15) & ~15) + 3 * sizeof(unsigned) * reset_words(L); }
 int scan_grid() {
     static int nsm = 0;
     if (!nsm) {
@@ -1289,7 +1389,8 @@ void launch_spans(const DevGrid& g, cudaStream_t s) {
     const dim3 b(32, 8);
     k_spans<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g);
     k_ext_spans<<<(g.N + 3 + 127) / 128, 128, 0, s>>>(g, kSpanHalo);
-    hyd_kernel_launches_add(2);
+    k_reset_bytes_init<<<grid2d(g.N + 3, g.M + 3, b), b, 0, s>>>(g);
+    hyd_kernel_launches_add(3);
 }
 
 void launch_widen_spans(const DevGrid& g, cudaStream_t s) {
@@ -1356,10 +1457,15 @@ void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s) {
 // Elementwise kernels: the whole grid (`full`), or one warp per row over its extended span.
 static int row_warps_blocks(int rows) { return (rows * 32 + 255) / 256; }
 
-void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, cudaStream_t s) {
+void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, cudaStream_t s) {
     const dim3 b(32, 8);
-    if (full) k_smooth<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
-    else k_smooth_span<<<row_warps_blocks(g.N + 3), 256, 0, s>>>(g, p, isU, out);
+    if (full) {
+        if (bytes) k_smooth<1><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
+        else k_smooth<0><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
+    } else {
+        if (bytes) k_smooth_span<1><<<row_warps_blocks(g.N + 3), 256, 0, s>>>(g, p, isU, out);
+        else k_smooth_span<0><<<row_warps_blocks(g.N + 3), 256, 0, s>>>(g, p, isU, out);
+    }
     hyd_kernel_launches_add(1);
 }
 

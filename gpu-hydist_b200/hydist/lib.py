@@ -56,6 +56,8 @@ def load():
         "hyd_get_stream": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_void_p)]),
         "hyd_device_status": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_uint)]),
         "hyd_set_timing": (ctypes.c_int, [H, ctypes.c_int]),
+        "hyd_set_timing_phases": (ctypes.c_int, [H, ctypes.c_uint]),
+        "hyd_phase_name": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]),
         "hyd_timing_report": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_size_t]),
     }
     for name, (res, args) in sig.items():
@@ -69,6 +71,16 @@ def load():
 def _check(rc):
     if rc != 0:
         raise HydError("hydist error %d: %s" % (rc, _lib.hyd_last_error().decode()))
+
+
+def phase_ids(lib):
+    """{phase name: bit index} of the library's step phases."""
+    out, k = {}, 0
+    name = ctypes.c_char_p()
+    while lib.hyd_phase_name(k, ctypes.byref(name)) == 0:
+        out[name.value.decode()] = k
+        k += 1
+    return out
 
 
 def field_shape(name, N, M):
@@ -200,8 +212,19 @@ class Simulation:
         _check(self.lib.hyd_get_stream(self.h, ctypes.byref(p)))
         return p.value or 0
 
-    def set_timing(self, enable):
-        _check(self.lib.hyd_set_timing(self.h, 1 if enable else 0))
+    def set_timing(self, enable, phases=None):
+        """Bracket the step's phases with events: every phase, or only those named in
+        `phases` (names as in timing_report)."""
+        if not enable:
+            _check(self.lib.hyd_set_timing(self.h, 0))
+        elif phases is None:
+            _check(self.lib.hyd_set_timing(self.h, 1))
+        else:
+            ids = phase_ids(self.lib)
+            mask = 0
+            for name in phases:
+                mask |= 1 << ids[name]
+            _check(self.lib.hyd_set_timing_phases(self.h, mask))
 
     def timing_report(self):
         buf = ctypes.create_string_buffer(8192)

@@ -229,11 +229,19 @@ int hyd_launch_count(hyd_handle h, long long* count);
 int hyd_get_stream(hyd_handle h, void** stream);
 
 /* Per-phase device timing: while enabled, every phase of the step (boundary, the two
- * line sweeps, smoothing, explicit momentum, resets, state update, scans, sediment, bed)
- * is bracketed by CUDA events on the handle's stream.  hyd_timing_report() synchronizes
- * and writes lines "name launches total_ms\n" into buf (NUL-terminated), then clears the
- * accumulators. */
+ * line sweeps, smoothing, explicit momentum, resets, state update, scans, sediment, bed,
+ * the coefficient passes) is bracketed by CUDA events on the handle's stream.
+ * hyd_timing_report() synchronizes and writes lines "name launches total_ms\n" into buf
+ * (NUL-terminated), then clears the accumulators.  No reference counterpart (the
+ * reference times whole steps on the host).
+ *
+ * hyd_set_timing_phases() brackets only the phases whose bit is set (bit k = phase k,
+ * named by hyd_phase_name(k, &name); 0 turns timing off): each bracket adds two event
+ * records to the step, so timing one phase alone disturbs the others least.
+ * hyd_set_timing(h, 1) selects every phase. */
 int hyd_set_timing(hyd_handle h, int enable);
+int hyd_set_timing_phases(hyd_handle h, unsigned int phase_mask);
+int hyd_phase_name(int phase, const char** name);
 int hyd_timing_report(hyd_handle h, char* buf, size_t buflen);
 
 #ifdef __cplusplus
