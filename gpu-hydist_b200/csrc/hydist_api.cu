@@ -99,6 +99,9 @@ struct HydSim {
     // CTA widths of the row and column line kernels, from the longest span of each
     // direction (about two cells per thread)
     int thr_r, thr_c;
+    // second stream for work that runs beside the main chain (forked and joined by events)
+    cudaStream_t side;
+    cudaEvent_t ev_fork, ev_join;
     cudaGraphExec_t graph[8];
     long long graph_kernels[8];
     // timing with graphs: one graph per variant with the phase events captured in it
@@ -148,11 +151,15 @@ static int refresh_widths(HydSim* s) {
         return t < 64 ? 64 : (t > 512 ? 512 : t);
     };
     const int lr = longest(s->g.rlo, s->g.rhi, s->N + 3), lc = longest(s->g.clo, s->g.chi, s->M + 3);
-    if (lr < 0 || lc < 0) return fail(HYD_ECUDA, "reading the spans back failed");
+    const int le = longest(s->g.elo, s->g.ehi, s->N + 3);
+    if (lr < 0 || lc < 0 || le < 0) return fail(HYD_ECUDA, "reading the spans back failed");
     const int tr = pick(lr), tc = pick(lc);
-    if (tr != s->thr_r || tc != s->thr_c) drop_graphs(s);
+    int wpr = (le + 31) / 32;
+    wpr = wpr < 1 ? 1 : (wpr > 8 ? 8 : wpr);
+    if (tr != s->thr_r || tc != s->thr_c || wpr != s->g.wpr) drop_graphs(s);
     s->thr_r = tr;
     s->thr_c = tc;
+    s->g.wpr = wpr;
     return HYD_OK;
 }
 
@@ -395,6 +402,18 @@ void hyd_params_default(HydCaseParams* p) {
     hyd_params_derive(p);
 }
 
+// Free what a handle holds (any of it may be missing on a failed create) and the handle.
+static void release(HydSim* s) {
+    cudaFree(s->sweep_scratch);
+    cudaFree(s->g.colT);
+    cudaFree(s->arena);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->side) cudaStreamDestroy(s->side);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
 int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out) {
     if (!p || !out) return fail(HYD_EINVAL, "null argument");
     if (N < 6 || M < 6) return fail(HYD_EINVAL, "grid too small (N, M >= 6)");
@@ -434,9 +453,12 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         s->phase_n[k] = 0;
     }
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
-        delete s;
-        return fail(HYD_ECUDA, std::string("stream: ") + cudaGetErrorString(e));
+        release(s);
+        return fail(HYD_ECUDA, std::string("streams: ") + cudaGetErrorString(e));
     }
     // arena: grid fields (double and int), smoothing partners, tables, boundary arrays
     const size_t nrow = (size_t)N + 3;
@@ -452,8 +474,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     total += 2 * a256((N + 3) * 4) + 2 * a256(64);                      // extended spans, flags
     e = cudaMalloc(&s->arena, total);
     if (e != cudaSuccess) {
-        cudaStreamDestroy(s->stream);
-        delete s;
+        release(s);
         return fail(HYD_ENOMEM, std::string("device arena: ") + cudaGetErrorString(e));
     }
     s->arena_bytes = total;
@@ -469,6 +490,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.N = N;
     g.M = M;
     g.P = s->pitch;
+    g.wpr = 1;
     double** gd[] = {&g.h,   &g.hsnham, &g.VISC,  &g.Fw,   &g.Tsxw,  &g.Tsyw,     &g.u,   &g.v,   &g.z,
                      &g.t_u, &g.t_v,    &g.t_z,   &g.Htdu, &g.Htdv,  &g.H_moi,    &g.htaiz, &g.htaiz_bd,
                      &g.Kx1, &g.Ky1,    &g.FS,    &g.tFS,  &g.VTH,   &g.Kx,       &g.Ky,  &g.Qbx, &g.Qby,
@@ -507,18 +529,14 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.dflag = (int*)take(64);
     g.clock = (double*)take(64);
     if ((size_t)(cur - (char*)s->arena) > total) {
-        cudaFree(s->arena);
-        cudaStreamDestroy(s->stream);
-        delete s;
+        release(s);
         return fail(HYD_ENOMEM, "arena layout overflow");
     }
     s->dp = make_dev_params(s->P);
     e = sweep_plan(N, M, &s->plan);
     if (e == cudaSuccess) e = grid_setup(N, M);
     if (e != cudaSuccess) {
-        cudaFree(s->arena);
-        cudaStreamDestroy(s->stream);
-        delete s;
+        release(s);
         return fail(HYD_ECUDA, std::string("shared-memory set-up: ") + cudaGetErrorString(e));
     }
     s->g.LT = (N + 3 + 31) / 32 * 32;
@@ -526,24 +544,18 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     e = cudaMalloc(&s->g.colT, 7 * s->g.colT_stride * sizeof(double) + s->g.colT_stride);
     s->g.colB = (unsigned char*)(s->g.colT + 7 * s->g.colT_stride);
     if (e != cudaSuccess) {
-        cudaFree(s->arena);
-        cudaStreamDestroy(s->stream);
-        delete s;
+        release(s);
         return fail(HYD_ENOMEM, std::string("column-major scratch: ") + cudaGetErrorString(e));
     }
     s->sweep_scratch = nullptr;
     e = cudaMalloc(&s->sweep_scratch, s->plan.scratch_doubles * sizeof(double));
     if (e != cudaSuccess) {
-        cudaFree(s->arena);
-        cudaStreamDestroy(s->stream);
-        delete s;
+        release(s);
         return fail(HYD_ENOMEM, std::string("sweep scratch: ") + cudaGetErrorString(e));
     }
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
-        cudaFree(s->arena);
-        cudaStreamDestroy(s->stream);
-        delete s;
+        release(s);
         return fail(HYD_ECUDA, std::string("create: ") + cudaGetErrorString(e));
     }
     *out = s;
@@ -561,11 +573,7 @@ int hyd_destroy(hyd_handle h) {
     }
     for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
     drop_graphs(h);
-    cudaFree(h->sweep_scratch);
-    cudaFree(h->g.colT);
-    cudaFree(h->arena);
-    cudaStreamDestroy(h->stream);
-    delete h;
+    release(h);
     return HYD_OK;
 }
 
@@ -734,7 +742,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         start_idx = 3;
         end_idx = s->M - 1;
     }
-    { PHASE(PH_COEF_UZ); launch_coef_uz(g, p, st); }
+    { PHASE(PH_COEF_UZ); launch_coef_uz(g, p, st, s->side, s->ev_fork, s->ev_join); }
     { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, st); }
     std::swap(g.t_u, s->scratch_u);

@@ -60,6 +60,7 @@ struct DevGrid {
     unsigned char* colB;  // column-major reset bytes of the column resets (stride LT)
     size_t colT_stride;
     int LT;
+    int wpr;  // warps per row of the extended-span kernels (1 until the spans are known)
     double* clock;  // [0] time of half-step 1, [1] time of half-step 2, [2] time at the step start
 };
 
@@ -152,7 +153,8 @@ void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
 void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s);
-void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s);
+void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                    cudaEvent_t join);
 void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
                        double* scratch, cudaStream_t s);

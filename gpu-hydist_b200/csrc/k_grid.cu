@@ -317,26 +317,28 @@ __device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams
          p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
 }
 
-// First launch of a step: UZ coefficients of every wet interior cell, one warp per row
-// over the row's span of cells that can be wet, written column-major (g.colT arrays 0..6:
-// a2 c2 d2 f1 f2 f3 f5); the last CTA advances the step clock and applies the boundary
-// values of the first half-step (neither reads what the other writes).
-__global__ void __launch_bounds__(1024) k_coef_uz(DevGrid g, DevParams p) {
-    if (blockIdx.x == gridDim.x - 1) {
-        __shared__ double s_t;
-        if (threadIdx.x == 0) {  // k_clock
-            const double t1 = g.clock[2] + p.dT * 0.5;
-            const double t2 = t1 + p.dT * 0.5;
-            g.clock[0] = t1;
-            g.clock[1] = t2;
-            g.clock[2] = t2;
-            s_t = t1;
-        }
-        __syncthreads();
-        if (p.channel) boundary_channel_body(g, p, s_t);
-        else boundary_body(g, s_t);
-        return;
+// First launches of a step, side by side: UZ coefficients of every wet interior cell, one
+// warp per row over the row's span of cells that can be wet, written column-major
+// (g.colT arrays 0..6: a2 c2 d2 f1 f2 f3 f5); and one CTA that advances the step clock
+// and applies the boundary values of the first half-step (neither reads what the other
+// writes).  The column-major stores are one sector per lane, so the coefficients are
+// spread over many small CTAs.
+__global__ void k_clock_boundary(DevGrid g, DevParams p) {
+    __shared__ double s_t;
+    if (threadIdx.x == 0) {  // k_clock
+        const double t1 = g.clock[2] + p.dT * 0.5;
+        const double t2 = t1 + p.dT * 0.5;
+        g.clock[0] = t1;
+        g.clock[1] = t2;
+        g.clock[2] = t2;
+        s_t = t1;
     }
+    __syncthreads();
+    if (p.channel) boundary_channel_body(g, p, s_t);
+    else boundary_body(g, s_t);
+}
+
+__global__ void __launch_bounds__(128) k_coef_uz(DevGrid g, DevParams p) {
     const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i > g.N) return;
     const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
@@ -406,6 +408,19 @@ __device__ __forceinline__ void reset_byte_cell(const DevGrid& g, const DevParam
     g.colB[(size_t)j * g.LT + i] = (unsigned char)b;
 }
 
+// Row-lane mapping of the extended-span kernels: g.wpr warps per row, so that a row's
+// span is covered in one pass.  Thread -> row i0 + (warp / wpr), first cell offset
+// (warp % wpr) * 32 + lane, stride wpr * 32.
+struct RowLane {
+    int i, off, stride;
+    __device__ __forceinline__ RowLane(const DevGrid& g, int i0) {
+        const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        i = i0 + gw / g.wpr;
+        off = (gw % g.wpr) * 32 + (threadIdx.x & 31);
+        stride = g.wpr * 32;
+    }
+};
+
 // BYTES: also write the column reset bytes (the smoothing of u right before the column
 // resets; H_moi is not read in between).
 template <int BYTES>
@@ -417,9 +432,10 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
 
 template <int BYTES>
 __global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const RowLane rl(g, 0);
+    const int i = rl.i;
     if (i > g.N + 2) return;
-    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) {
+    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
         smooth_cell(g, p, isU, out, i, j, false);
         if (BYTES) reset_byte_cell(g, p, i, j);
     }
@@ -977,9 +993,10 @@ __global__ void k_post(DevGrid g, int with_uvz) {
 }
 
 __global__ void k_post_span(DevGrid g) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const RowLane rl(g, 0);
+    const int i = rl.i;
     if (i > g.N) return;
-    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) post_cell(g, 1, i, j);
+    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) post_cell(g, 1, i, j);
 }
 
 // ------------------------------------------------------------- wet-segment scans
@@ -1110,9 +1127,10 @@ __global__ void k_vth_hesok(DevGrid g, DevParams p) {
 }
 
 __global__ void k_vth_span(DevGrid g, DevParams p) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const RowLane rl(g, 0);
+    const int i = rl.i;
     if (i > g.N) return;
-    for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) vth_cell(g, p, i, j);
+    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) vth_cell(g, p, i, j);
 }
 
 // After a half-step's reset, in one launch: the state update (update_uvz + Htuongdoi)
@@ -1126,9 +1144,10 @@ __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
     extern __shared__ unsigned swords[];
     const int b = blockIdx.x;
     if (b < nbp) {
-        const int i = (b * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+        const RowLane rl(g, 0);
+        const int i = rl.i;
         if (i > g.N) return;
-        for (int j = g.elo[i] + lane; j <= g.ehi[i]; j += 32) {
+        for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
             post_cell(g, 1, i, j);
             if (VTH) vth_cell(g, p, i, j);
         }
@@ -1180,18 +1199,21 @@ __global__ void k_update_fs(DevGrid g) {
 }
 
 // Update_FS over the extended spans, plus rows 2 and N and column M in full (the edge
-// interpolation writes FS there).
-__global__ void k_update_fs_span(DevGrid g) {
-    const int i = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+// interpolation writes FS there): CTAs [0, nb) take the rows other than 2 and N, the
+// last two CTAs rows 2 and N.
+__global__ void k_update_fs_span(DevGrid g, int nb) {
     const int N = g.N, M = g.M, P = g.P;
-    if (i > N) return;
-    int lo = g.elo[i] > 1 ? g.elo[i] : 1, hi = g.ehi[i] < M ? g.ehi[i] : M;
-    if (i == 2 || i == N) {
-        lo = 1;
-        hi = M;
+    if ((int)blockIdx.x >= nb) {
+        const int i = (int)blockIdx.x == nb ? 2 : N;
+        for (int j = 1 + threadIdx.x; j <= M; j += blockDim.x) g.FS[i * P + j] = g.tFS[i * P + j];
+        return;
     }
-    for (int j = lo + lane; j <= hi; j += 32) g.FS[i * P + j] = g.tFS[i * P + j];
-    if (lane == 0 && (M < lo || M > hi)) g.FS[i * P + M] = g.tFS[i * P + M];
+    const RowLane rl(g, 1);
+    const int i = rl.i;
+    if (i > N || i == 2 || i == N) return;
+    const int lo = g.elo[i] > 1 ? g.elo[i] : 1, hi = g.ehi[i] < M ? g.ehi[i] : M;
+    for (int j = lo + rl.off; j <= hi; j += rl.stride) g.FS[i * P + j] = g.tFS[i * P + j];
+    if (rl.off == 0 && (M < lo || M > hi)) g.FS[i * P + M] = g.tFS[i * P + M];
 }
 
 // Calculate_Qb (Sediment_Transport.cu:341-414): bed-load flux, then the edge copies
@@ -1448,14 +1470,21 @@ void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_
     hyd_kernel_launches_add(1);
 }
 
-// The step's first launch: k_coef_uz with the clock and the first boundary update.
-void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_coef_uz<<<((g.N - 1) * 32 + 1023) / 1024 + 1, 1024, 0, s>>>(g, p);
-    hyd_kernel_launches_add(1);
+// The step's first launches: k_coef_uz on s, the clock and the first boundary update on
+// `side`, forked from s and joined back into it (a branch of the step graph).
+void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                    cudaEvent_t join) {
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(side, fork, 0);
+    k_clock_boundary<<<1, p.channel ? 256 : 512, 0, side>>>(g, p);
+    cudaEventRecord(join, side);
+    k_coef_uz<<<((g.N - 1) * 32 + 127) / 128, 128, 0, s>>>(g, p);
+    cudaStreamWaitEvent(s, join, 0);
+    hyd_kernel_launches_add(2);
 }
 
 // Elementwise kernels: the whole grid (`full`), or one warp per row over its extended span.
-static int row_warps_blocks(int rows) { return (rows * 32 + 255) / 256; }
+static int row_warps_blocks(const DevGrid& g, int rows) { return (rows * g.wpr * 32 + 255) / 256; }
 
 void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, cudaStream_t s) {
     const dim3 b(32, 8);
@@ -1463,8 +1492,8 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
         if (bytes) k_smooth<1><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         else k_smooth<0><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
     } else {
-        if (bytes) k_smooth_span<1><<<row_warps_blocks(g.N + 3), 256, 0, s>>>(g, p, isU, out);
-        else k_smooth_span<0><<<row_warps_blocks(g.N + 3), 256, 0, s>>>(g, p, isU, out);
+        if (bytes) k_smooth_span<1><<<row_warps_blocks(g, g.N + 3), 256, 0, s>>>(g, p, isU, out);
+        else k_smooth_span<0><<<row_warps_blocks(g, g.N + 3), 256, 0, s>>>(g, p, isU, out);
     }
     hyd_kernel_launches_add(1);
 }
@@ -1499,7 +1528,7 @@ void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int thre
 void launch_post(const DevGrid& g, const DevParams& p, int full, cudaStream_t s) {
     const dim3 b(32, 8);
     if (full) k_post<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, 1);
-    else k_post_span<<<row_warps_blocks(g.N + 1), 256, 0, s>>>(g);
+    else k_post_span<<<row_warps_blocks(g, g.N + 1), 256, 0, s>>>(g);
     hyd_kernel_launches_add(1);
 }
 
@@ -1518,7 +1547,7 @@ void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s) {
 // The fused update / rescan / interpolation launch (k_post_fused); rows: which direction
 // is rescanned.
 void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s) {
-    const int nbp = (g.N + 1) * 32 / 256 + 1, nbs = 32;
+    const int nbp = row_warps_blocks(g, g.N + 1), nbs = 32;
     const int grid = nbp + nbs + 1;
     if (rows) {
         if (vth) k_post_fused<1, 1><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
@@ -1533,14 +1562,17 @@ void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, 
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s) {
     const dim3 b(32, 8);
     if (full) k_vth_hesok<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
-    else k_vth_span<<<row_warps_blocks(g.N + 1), 256, 0, s>>>(g, p);
+    else k_vth_span<<<row_warps_blocks(g, g.N + 1), 256, 0, s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
 void launch_update_fs(const DevGrid& g, int full, cudaStream_t s) {
     const dim3 b(32, 8);
     if (full) k_update_fs<<<grid2d(g.M, g.N, b), b, 0, s>>>(g);
-    else k_update_fs_span<<<row_warps_blocks(g.N), 256, 0, s>>>(g);
+    else {
+        const int nb = row_warps_blocks(g, g.N);
+        k_update_fs_span<<<nb + 2, 256, 0, s>>>(g, nb);
+    }
     hyd_kernel_launches_add(1);
 }
 
