@@ -69,18 +69,16 @@ __host__ __device__ inline int chunk_len(int R, int T) {
     return m;
 }
 
-// Partitioned tridiagonal solve of rows [0, T*m) by the T threads of group G.
-// Row r: A[r] x[r-1] + B[r] x[r] + C[r] x[r+1] = D[r]; A[0] and C[last] are ignored.
-// Thread t owns rows [t*m, t*m+m).  The 2T chunk-end unknowns form a tridiagonal system
-// solved by parallel cyclic reduction with every row scaled to a unit diagonal (one
-// reciprocal per row and level), held in registers and exchanged through G (warp
-// shuffles).  On return B[r] holds x[r].
-template <class G>
-__device__ __forceinline__ void solve_partitioned(double* A, double* B, double* C, double* D, int m, double* red) {
-    constexpr int T = G::size;
-    const int t = G::rank();
-    const int s = t * m, e = s + m - 1;
-    // downward elimination inside the chunk: x_i + c'_i x_{i+1} + a'_i x_s = d'_i
+// Partitioned tridiagonal solve.  Row r: A[r] x[r-1] + B[r] x[r] + C[r] x[r+1] = D[r];
+// A[0] and C[last] are ignored.  Thread t owns the chunk of rows [t*m, t*m+m) (m >= 3).
+//
+// chunk_reduce: downward elimination inside the chunk (x_i + c'_i x_{i+1} + a'_i x_s =
+// d'_i), then upward (x_i = d''_i - a''_i x_s - c''_i x_e for s < i < e), leaving the two
+// chunk-end rows of the reduced system on the chunk-end unknowns, ordered (x_s, x_e)
+// chunk after chunk and scaled to a unit diagonal: row 2t is (v[0], 1, v[1] | v[2]), row
+// 2t+1 is (v[3], 1, v[4] | v[5]) as (lower, diagonal, upper | right-hand side).
+__device__ __forceinline__ void chunk_reduce(double* A, double* B, double* C, double* D, int s, int e,
+                                             double (&v)[6]) {
     {
         int i = s + 1;
         double r = 1.0 / B[i];
@@ -99,7 +97,6 @@ __device__ __forceinline__ void solve_partitioned(double* A, double* B, double* 
             D[i] = dp;
         }
     }
-    // upward: x_i = d''_i - a''_i x_s - c''_i x_e for s < i < e
     {
         double an = A[e - 1], cn = C[e - 1], dn = D[e - 1];
         for (int i = e - 2; i >= s + 1; i--) {
@@ -112,33 +109,42 @@ __device__ __forceinline__ void solve_partitioned(double* A, double* B, double* 
             D[i] = dn;
         }
     }
-    // Reduced system on the chunk-end unknowns ordered (x_s, x_e) chunk after chunk, each
-    // row scaled to a unit diagonal: row 2t is (v[0], 1, v[1] | v[2]), row 2t+1 is
-    // (v[3], 1, v[4] | v[5]) as (lower, diagonal, upper | right-hand side).
-    constexpr int n = 2 * T;
-    double v[6];
-    {
-        const double cs = C[s];
-        const double ib = 1.0 / (B[s] - cs * A[s + 1]);
-        v[0] = A[s] * ib;
-        v[1] = -cs * C[s + 1] * ib;
-        v[2] = (D[s] - cs * D[s + 1]) * ib;
-        v[3] = A[e];
-        v[4] = C[e];
-        v[5] = D[e];
-    }
-    // parallel cyclic reduction: at distance d row r eliminates rows r - d and r + d
+    const double cs = C[s];
+    const double ib = 1.0 / (B[s] - cs * A[s + 1]);
+    v[0] = A[s] * ib;
+    v[1] = -cs * C[s + 1] * ib;
+    v[2] = (D[s] - cs * D[s + 1]) * ib;
+    v[3] = A[e];
+    v[4] = C[e];
+    v[5] = D[e];
+}
+
+// The chunk's inner unknowns from its end values; x goes to B.
+__device__ __forceinline__ void chunk_back(double* A, double* B, double* C, double* D, int s, int e, double xs,
+                                           double xe) {
+    for (int i = s + 1; i < e; i++) B[i] = D[i] - A[i] * xs - C[i] * xe;
+    B[s] = xs;
+    B[e] = xe;
+}
+
+// Parallel cyclic reduction of the 64-row reduced system of a warp (two unit-diagonal
+// rows per lane, in registers, exchanged by shuffles): at distance d row r eliminates rows
+// r - d and r + d, every row rescaled to a unit diagonal (one reciprocal per row and
+// level).  On return v[2] = x_s and v[5] = x_e of the lane's chunk.
+__device__ __forceinline__ void pcr_warp(double (&v)[6]) {
+    constexpr int T = 32, n = 2 * T;
+    const int t = threadIdx.x & 31;
     for (int d = 1; d < n; d <<= 1) {
         double lo[6], hi[6];
         const int h = d == 1 ? 1 : d >> 1;
-        G::exchange(v, h, lo, hi, red);
+        WarpG::exchange(v, h, lo, hi, nullptr);
         double la[2], lc[2], ld[2], ha[2], hc[2], hd[2];
         bool lv[2], hv[2];
         if (d == 1) {
-            // row 2t: lo = row 2t-1 (thread t-1, second row), hi = row 2t+1 (own second row)
+            // row 2t: lo = row 2t-1 (lane t-1, second row), hi = row 2t+1 (own second row)
             la[0] = lo[3]; lc[0] = lo[4]; ld[0] = lo[5]; lv[0] = t >= 1;
             ha[0] = v[3]; hc[0] = v[4]; hd[0] = v[5]; hv[0] = true;
-            // row 2t+1: lo = row 2t (own first row), hi = row 2t+2 (thread t+1, first row)
+            // row 2t+1: lo = row 2t (own first row), hi = row 2t+2 (lane t+1, first row)
             la[1] = v[0]; lc[1] = v[1]; ld[1] = v[2]; lv[1] = true;
             ha[1] = hi[0]; hc[1] = hi[1]; hd[1] = hi[2]; hv[1] = t + 1 < T;
         } else {
@@ -168,12 +174,76 @@ __device__ __forceinline__ void solve_partitioned(double* A, double* B, double* 
             v[3 * q + 2] = nD * ib;
         }
     }
-    const double xs = v[2];
-    const double xe = v[5];
-    for (int i = s + 1; i < e; i++) B[i] = D[i] - A[i] * xs - C[i] * xe;
-    B[s] = xs;
-    B[e] = xe;
-    G::sync();
+}
+
+// One warp: rows [0, 32 m), chunks of m rows per lane, the reduced system by pcr_warp.
+// On return B[r] holds x[r].
+__device__ __forceinline__ void solve_warp(double* A, double* B, double* C, double* D, int m) {
+    const int t = threadIdx.x & 31;
+    const int s = t * m, e = s + m - 1;
+    double v[6];
+    chunk_reduce(A, B, C, D, s, e, v);
+    pcr_warp(v);
+    chunk_back(A, B, C, D, s, e, v[2], v[5]);
+    __syncwarp();
+}
+
+// How a group of threads solves R rows: t1 threads with chunks of m rows.  t1 == 32: one
+// warp (solve_warp).  t1 > 32: two levels (solve_block): the 2 t1 chunk-end rows form a
+// tridiagonal system that one warp solves in chunks of m2 = chunk_len(2 t1, 32) rows.
+// The plan minimises the serial depth, about 3 m + 6 for one warp and 3 m + 3 m2 + 10
+// for two levels (their two CTA barriers counted as two steps each).
+struct SolvePlan {
+    int t1, m;
+};
+constexpr int kRedRows = 32 * 17;  // reduced rows of the largest two-level plan (t1 = 256)
+__host__ __device__ inline SolvePlan solve_plan(int R, int max_t1) {
+    SolvePlan best{32, chunk_len(R, 32)};
+    int depth = 3 * best.m + 6;
+    for (int t1 = 64; t1 <= max_t1 && t1 <= 256; t1 <<= 1) {
+        const int m1 = chunk_len(R, t1), m2 = chunk_len(2 * t1, 32);
+        const int d = 3 * m1 + 3 * m2 + 10;
+        if (d < depth) {
+            depth = d;
+            best = SolvePlan{t1, m1};
+        }
+    }
+    return best;
+}
+
+// Two-level solve by a CTA (rows [0, t1 m)); red holds 4 kRedRows doubles.  Every thread
+// of the CTA calls it.  On return B[r] holds x[r].
+__device__ __forceinline__ void solve_block(double* A, double* B, double* C, double* D, SolvePlan pl, double* red) {
+    const int t = threadIdx.x;
+    const int m2 = chunk_len(2 * pl.t1, 32);
+    double *rA = red, *rB = red + kRedRows, *rC = red + 2 * kRedRows, *rD = red + 3 * kRedRows;
+    if (t < pl.t1) {
+        const int s = t * pl.m, e = s + pl.m - 1;
+        double v[6];
+        chunk_reduce(A, B, C, D, s, e, v);
+        rA[2 * t] = v[0];
+        rB[2 * t] = 1.0;
+        rC[2 * t] = v[1];
+        rD[2 * t] = v[2];
+        rA[2 * t + 1] = v[3];
+        rB[2 * t + 1] = 1.0;
+        rC[2 * t + 1] = v[4];
+        rD[2 * t + 1] = v[5];
+    }
+    for (int r = 2 * pl.t1 + t; r < 32 * m2; r += blockDim.x) {  // identity rows
+        rA[r] = 0.0;
+        rB[r] = 1.0;
+        rC[r] = 0.0;
+        rD[r] = 0.0;
+    }
+    __syncthreads();
+    if (t < 32) solve_warp(rA, rB, rC, rD, m2);
+    __syncthreads();
+    if (t < pl.t1) {
+        const int s = t * pl.m, e = s + pl.m - 1;
+        chunk_back(A, B, C, D, s, e, rB[2 * t], rB[2 * t + 1]);
+    }
+    __syncthreads();
 }
 
 // Serial Thomas over the packed rows by the group's first thread, in the reference's
@@ -202,17 +272,20 @@ __device__ __forceinline__ void solve_thomas(double* A, double* B, double* C, do
     G::sync();
 }
 
-// Solve of a line's packed system by group G: the partitioned solver run by the group's
-// first warp (chunks of m rows per lane, shuffle-only reduction), the other warps waiting.
-// A single warp keeps the reduction free of CTA barriers; m grows with the line instead.
+// Solve of a line's packed system (rows padded with identity rows to pl.t1 * pl.m) by
+// group G: one warp (a warp group, or a CTA's first warp with the others waiting), or
+// the two-level solve of a CTA.
 template <class G, int SOLVER>
-__device__ __forceinline__ void solve_line(double* A, double* B, double* C, double* D, int m, int rows) {
+__device__ __forceinline__ void solve_line(double* A, double* B, double* C, double* D, SolvePlan pl, int rows,
+                                           double* red) {
     if (SOLVER == 0) {
         if (G::size == 32) {
-            solve_partitioned<WarpG>(A, B, C, D, m, nullptr);
-        } else {
-            if (threadIdx.x < 32) solve_partitioned<WarpG>(A, B, C, D, m, nullptr);
+            solve_warp(A, B, C, D, pl.m);
+        } else if (pl.t1 == 32) {
+            if (threadIdx.x < 32) solve_warp(A, B, C, D, pl.m);
             G::sync();
+        } else {
+            solve_block(A, B, C, D, pl, red);
         }
     } else {
         solve_thomas<G>(A, B, C, D, rows);
@@ -231,17 +304,19 @@ struct LineShared {
     int nseg, R, C;
 };
 
-__device__ __forceinline__ int seg_of(const LineShared& sg, int c) {
-    int s = 0;
-    while (s + 1 < sg.nseg && sg.co[s + 1] <= c) s++;
-    return s;
+// The segment holding packed cell (seg_of) or packed row (seg_of_row) c: the last s with
+// off[s] <= c (binary search over at most 20 offsets).
+__device__ __forceinline__ int seg_search(const int* off, int nseg, int c) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
-
-__device__ __forceinline__ int seg_of_row(const LineShared& sg, int c) {
-    int s = 0;
-    while (s + 1 < sg.nseg && sg.ro[s + 1] <= c) s++;
-    return s;
-}
+__device__ __forceinline__ int seg_of(const LineShared& sg, int c) { return seg_search(sg.co, sg.nseg, c); }
+__device__ __forceinline__ int seg_of_row(const LineShared& sg, int c) { return seg_search(sg.ro, sg.nseg, c); }
 
 // ---- hydrodynamic sweeps ----------------------------------------------------------
 // DIR 0: UZ, line = column j, cells i (t_u, ubt/ubp, bienQ[2]/[3]).
@@ -313,12 +388,12 @@ __device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p
     G::sync();
 }
 
-// Phases A-D of one line by group G.  Rows A, B, Cc, D hold at least G::size * m
-// entries, cells a2, c2, d2 at least sg.C.
+// Phases A-D of one line by group G.  Rows A, B, Cc, D hold at least pl.t1 * pl.m
+// entries, cells a2, c2, d2 at least sg.C; red: the two-level solve's reduced rows.
 template <int DIR, int SOLVER, class G>
 __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p, int line, const LineShared& sg,
                                            double* A, double* B, double* Cc, double* D, double* a2, double* c2,
-                                           double* d2, double* red, int m) {
+                                           double* d2, double* red, SolvePlan pl) {
     constexpr int T = G::size;
     const int tid = G::rank();
     const int N = g.N, M = g.M, P = g.P;
@@ -332,32 +407,29 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     const int nseg = sg.nseg;
     const int C = sg.C, R = sg.R;
 
-    // ---- A: continuity coefficients of every wet cell (preindex, UVZSolver_multithread.cu:402-406 / 345-349)
-    for (int c = tid; c < C; c += T) {
-        const int sI = seg_of(sg, c);
-        const int k = sg.first[sI] + (c - sg.co[sI]);
-        const int pos = base + k * along;
+    // ---- A + B1, one pass over the cells: the continuity coefficients of the cell and of
+    // the next one (preindex, UVZSolver_multithread.cu:402-406 / 345-349), the momentum
+    // coefficients (preindex f1..f5, _calculate_abcd 409-466) and the rows.  The cell's own
+    // continuity coefficients are kept for the extraction.
+    auto cont = [&](int k, double& a, double& c, double& d) {
         if (DIR == 0) {
             const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_uz
-            a2[c] = colT(g, 0)[t];
-            c2[c] = colT(g, 1)[t];
-            d2[c] = colT(g, 2)[t];
-            (void)pos;
+            a = colT(g, 0)[t];
+            c = colT(g, 1)[t];
+            d = colT(g, 2)[t];
         } else {
-            c2[c] = p.dTchia2dY * g.Htdv[pos];
-            a2[c] = -p.dTchia2dY * g.Htdv[pos - 1];
-            d2[c] = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
+            const int pos = base + k * along;
+            c = p.dTchia2dY * g.Htdv[pos];
+            a = -p.dTchia2dY * g.Htdv[pos - 1];
+            d = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
         }
-    }
-    for (int r = R + tid; r < 32 * m; r += T) {  // identity rows up to the solver's 32 m
+    };
+    for (int r = R + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
         A[r] = 0.0;
         B[r] = 1.0;
         Cc[r] = 0.0;
         D[r] = 0.0;
     }
-    G::sync();
-
-    // ---- B1: momentum coefficients (preindex f1..f5, _calculate_abcd 409-466) and the rows
     const double f4 = DIR == 0 ? 2 * p.g * p.dTchia2dX : 2 * p.g * p.dTchia2dY;
     for (int c = tid; c < C; c += T) {
         const int sI = seg_of(sg, c);
@@ -369,16 +441,23 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         const int sn = sg.sn[sI];
         const int r0 = sg.ro[sI];
         const int rel = 2 * (k - f);  // row 2k relative to the segment's first row 2f
+        double ac, cc, dc;
+        cont(k, ac, cc, dc);
+        a2[c] = ac;
+        c2[c] = cc;
+        d2[c] = dc;
         if (tR && rel <= sn) {
-            A[r0 + rel] = a2[c];
+            A[r0 + rel] = ac;
             B[r0 + rel] = 1.0;
-            Cc[r0 + rel] = c2[c];
-            D[r0 + rel] = d2[c];
+            Cc[r0 + rel] = cc;
+            D[r0 + rel] = dc;
         }
         if (k == l) continue;
         if (Ls <= 1 && k != f) continue;
         const int rm = tR ? rel + 1 : rel;  // the momentum row of this cell
         if (rm > sn) continue;
+        double an, cn, dn;  // the next cell's
+        cont(k + 1, an, cn, dn);
         const int pos = base + k * along;
         double f1, f2, f3, f5;
         {
@@ -423,19 +502,19 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         if (Ls >= 2) {
             if (k == f && b1f) {
                 ra = f4;
-                rb = f2 - (f3 * a2[c + 1] / c2[c + 1]);
-                rc = -f4 - (f3 / c2[c + 1]);
-                rd = f5 - (f3 * d2[c + 1] / c2[c + 1]);
+                rb = f2 - (f3 * an / cn);
+                rc = -f4 - (f3 / cn);
+                rd = f5 - (f3 * dn / cn);
             } else if (k == l - 1 && b2f) {
-                ra = f4 - f1 / a2[c];
-                rb = f2 - (f1 * c2[c] / a2[c]);
+                ra = f4 - f1 / ac;
+                rb = f2 - (f1 * cc / ac);
                 rc = -f4;
-                rd = f5 - (f1 * d2[c] / a2[c]);
+                rd = f5 - (f1 * dc / ac);
             } else {
-                ra = f4 - f1 / a2[c];
-                rc = -f4 - (f3 / c2[c + 1]);
-                rb = f2 - (f1 * c2[c] / a2[c]) - (f3 * a2[c + 1] / c2[c + 1]);
-                rd = f5 - (f1 * d2[c] / a2[c]) - (f3 * d2[c + 1] / c2[c + 1]);
+                ra = f4 - f1 / ac;
+                rc = -f4 - (f3 / cn);
+                rb = f2 - (f1 * cc / ac) - (f3 * an / cn);
+                rd = f5 - (f1 * dc / ac) - (f3 * dn / cn);
             }
         } else {
             ra = f4;
@@ -448,10 +527,10 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         Cc[r0 + rm] = rc;
         D[r0 + rm] = rd;
         if (!tR && rel + 1 <= sn) {
-            A[r0 + rel + 1] = a2[c + 1];
+            A[r0 + rel + 1] = an;
             B[r0 + rel + 1] = 1.0;
-            Cc[r0 + rel + 1] = c2[c + 1];
-            D[r0 + rel + 1] = d2[c + 1];
+            Cc[r0 + rel + 1] = cn;
+            D[r0 + rel + 1] = dn;
         }
     }
     G::sync();
@@ -479,8 +558,7 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     G::sync();
 
     // ---- C: solve
-    solve_line<G, SOLVER>(A, B, Cc, D, m, R);
-    (void)red;
+    solve_line<G, SOLVER>(A, B, Cc, D, pl, R, red);
 
     // ---- D: extract (_uzSolver_extract_solution 668-723 / _vzSolver_extract_solution 595-665)
     const double* x = B;
@@ -535,12 +613,13 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
 // wait at the CTA barriers rather than exit: the warp-synchronous steps of a warp whose
 // sibling warps had exited were measured an order of magnitude slower on B200.
 template <int DIR, int SOLVER>
-__global__ void __launch_bounds__(kTL) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB, int CB,
+__global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB, int CB,
                                                      double* gscr, int RG, int CG) {
     extern __shared__ double dyn_smem[];
     __shared__ LineShared sgw[kWL];
     __shared__ int s_long[kWL];
     __shared__ int s_nlong;
+    __shared__ double s_red[4 * kRedRows];  // reduced rows of the two-level solve
     const int w = threadIdx.x >> 5;
     const int nlines = endidx - startidx + 1;
     const int G = gridDim.x;
@@ -562,7 +641,7 @@ __global__ void __launch_bounds__(kTL) k_hydro_sweep(DevGrid g, DevParams p, int
                 double* c2 = a2 + kCellW;
                 double* d2 = c2 + kCellW;
                 hydro_body<DIR, SOLVER, WarpG>(g, p, startidx + li, sg, A, B, Cc, D, a2, c2, d2, nullptr,
-                                               chunk_len(sg.R, 32));
+                                               SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
         __syncthreads();
@@ -571,8 +650,8 @@ __global__ void __launch_bounds__(kTL) k_hydro_sweep(DevGrid g, DevParams p, int
             const int wl = s_long[q];
             const LineShared& sl = sgw[wl];
             const int line = startidx + (int)blockIdx.x + (j0 + wl) * G;
-            const int m = chunk_len(sl.R, 32);
-            const bool fits = 32 * m <= RB && sl.C <= CB;
+            const SolvePlan pl = solve_plan(sl.R, SOLVER == 0 ? 256 : 32);
+            const bool fits = pl.t1 * pl.m <= RB && sl.C <= CB;
             const int rs = fits ? RB : RG, cs = fits ? CB : CG;
             double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * (4 * (size_t)RG + 3 * (size_t)CG);
             double* B = A + rs;
@@ -581,7 +660,7 @@ __global__ void __launch_bounds__(kTL) k_hydro_sweep(DevGrid g, DevParams p, int
             double* a2 = D + rs;
             double* c2 = a2 + cs;
             double* d2 = c2 + cs;
-            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sl, A, B, Cc, D, a2, c2, d2, nullptr, m);
+            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sl, A, B, Cc, D, a2, c2, d2, s_red, pl);
             __syncthreads();  // the slices and sgw are reused
         }
     }
@@ -733,7 +812,7 @@ __device__ __forceinline__ void fs_setup(const DevGrid& g, const DevParams& p, i
 template <int DIR, int SOLVER, class G>
 __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, int half, int line,
                                         const LineShared& sg, double* A, double* B, double* Cc, double* D,
-                                        double* red, int m) {
+                                        double* red, SolvePlan pl) {
     constexpr int T = G::size;
     const int tid = G::rank();
     const int P = g.P;
@@ -741,7 +820,7 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     const int base = DIR == 0 ? line : line * P;
     const double t = g.clock[half];
     const int R = sg.R;
-    for (int r = R + tid; r < 32 * m; r += T) {  // identity rows up to the solver's 32 m
+    for (int r = R + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
         A[r] = 0.0;
         B[r] = 1.0;
         Cc[r] = 0.0;
@@ -786,8 +865,7 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
         D[rr] = dd;
     }
     G::sync();
-    solve_line<G, SOLVER>(A, B, Cc, D, m, R);
-    (void)red;
+    solve_line<G, SOLVER>(A, B, Cc, D, pl, R, red);
     const double* x = B;
     double* vel = DIR == 0 ? g.t_u : g.t_v;
     for (int c = tid; c < R; c += T) {
@@ -813,12 +891,13 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
 
 // Fused sediment sweep of one direction: as k_hydro_sweep, short lines at most kRowWf rows.
 template <int DIR, int SOLVER>
-__global__ void __launch_bounds__(kTL) k_fs_sweep(DevGrid g, DevParams p, int half, int startidx, int endidx, int RB,
+__global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int half, int startidx, int endidx, int RB,
                                                   double* gscr, int RG) {
     extern __shared__ double dyn_smem[];
     __shared__ LineShared sgw[kWL];
     __shared__ int s_long[kWL];
     __shared__ int s_nlong;
+    __shared__ double s_red[4 * kRedRows];  // reduced rows of the two-level solve
     const int w = threadIdx.x >> 5;
     const int nlines = endidx - startidx + 1;
     const int G = gridDim.x;
@@ -834,7 +913,7 @@ __global__ void __launch_bounds__(kTL) k_fs_sweep(DevGrid g, DevParams p, int ha
             } else {
                 double* A = dyn_smem + w * kWarpFs;
                 fs_body<DIR, SOLVER, WarpG>(g, p, half, startidx + li, sg, A, A + kRowW, A + 2 * kRowW, A + 3 * kRowW,
-                                            nullptr, chunk_len(sg.R, 32));
+                                            nullptr, SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
         __syncthreads();
@@ -843,11 +922,11 @@ __global__ void __launch_bounds__(kTL) k_fs_sweep(DevGrid g, DevParams p, int ha
             const int wl = s_long[q];
             const LineShared& sl = sgw[wl];
             const int line = startidx + (int)blockIdx.x + (j0 + wl) * G;
-            const int m = chunk_len(sl.R, 32);
-            const bool fits = 32 * m <= RB;
+            const SolvePlan pl = solve_plan(sl.R, SOLVER == 0 ? 256 : 32);
+            const bool fits = pl.t1 * pl.m <= RB;
             const int rs = fits ? RB : RG;
             double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * 4 * (size_t)RG;
-            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sl, A, A + rs, A + 2 * rs, A + 3 * rs, nullptr, m);
+            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sl, A, A + rs, A + 2 * rs, A + 3 * rs, s_red, pl);
             __syncthreads();
         }
     }
@@ -897,7 +976,14 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
     if ((long long)(sizeof(double) * warp_h) > lim_h || (long long)(sizeof(double) * warp_f) > lim_f)
         return cudaErrorInvalidValue;
     // every row/cell a line can have: rows <= 2 L + 20, cells <= L + 3 (solved by 32 lanes)
-    sp->RG = 32 * chunk_len(2 * L + HYD_SEGL, 32);
+    {
+        int rg = 0;
+        for (int t1 = 32; t1 <= 256; t1 <<= 1) {  // the padded rows of any solve plan
+            const int r = t1 * chunk_len(2 * L + HYD_SEGL, t1);
+            if (r > rg) rg = r;
+        }
+        sp->RG = rg;
+    }
     sp->CG = L + 3;
     sp->need_global = 0;
     if ((long long)(sizeof(double) * (4 * (size_t)sp->RG + 3 * (size_t)sp->CG)) <= lim_h) {
@@ -911,7 +997,11 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
     }
     size_t big = 4 * (size_t)sp->RB + 3 * (size_t)sp->CB;
     sp->smem_lines = sizeof(double) * (big > warp_h ? big : warp_h);
-    sp->RGf = 32 * chunk_len(L, 32);
+    sp->RGf = 0;
+    for (int t1 = 32; t1 <= 256; t1 <<= 1) {
+        const int r = t1 * chunk_len(L, t1);
+        if (r > sp->RGf) sp->RGf = r;
+    }
     if ((long long)(sizeof(double) * 4 * (size_t)sp->RGf) <= lim_f) {
         sp->RBf = sp->RGf;
     } else {
