@@ -38,8 +38,8 @@ METRIC = "ADI cell-updates/s"
 
 # algorithmic bytes per launch of each phase, per unit: cells of the extended spans (the
 # cells the elementwise kernels visit once the grid is up to date, "span"), cells of the
-# spans of cells that can be wet ("core"), or wet cells of the swept lines ("wet"); the
-# derivation is in DESIGN.md (each field read once and written once)
+# spans of cells that can be wet ("core"), or wet cells of the swept lines ("wet"): each
+# field the kernel needs read once and each field it produces written once
 PHASE_BYTES = {
     "smooth": (20, "span"),        # read t (8) + mask (4), write out (8)
     "post": (152, "span"),         # update: read t_z,t_u,t_v,h (32), write z,u,v,Htdu,Htdv (40);
@@ -55,8 +55,20 @@ PHASE_BYTES = {
     "explicit_u": (24, "wet"),     # read the precomputed u (8), t_u staged (8), write t_u (8)
     "fs_sweep_j": (40, "wet"),     # read aa,bb,cc,dd (32), write tFS (8)
     "fs_sweep_i": (88, "wet"),
+    "coef_uz": (128, "wet"),       # read u,v,z,Htdu,Htdv,H_moi,VISC,Kx1,Tsxw (72), write 7 coefficients (56)
+    "coef_fsj": (112, "wet"),      # read FS,H_moi,VTH,Fw,t_u,t_v,Htdu,Htdv,Kx,Ky (80), write 4 (32)
+    "coef_eu": (80, "wet"),        # read u,v,t_v,z,Kx1,Htdu,H_moi,VISC,Tsxw (72), write 8
     "boundary": (0, "core"),
     "bed": (0, "core"),
+}
+
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu
+# --set full capture on this reach, with the wet cells of the captured step: scaled to the
+# timed workload by its wet cells (the swept cells set the traffic).  Captured in the
+# fourth step (t = 4 s) of python bench.py --spinup 0 --steps 3 --warmup 3 --no-cpu-baseline
+# (ncu -k regex:k_hydro_sweep -s 6 -c 2: the 7th launch of the sweep kernel, the UZ sweep).
+NCU_TRAFFIC = {
+    "sweep_uz": (2174208, 30650),
 }
 
 
@@ -252,6 +264,10 @@ def run_ours(args, rank, world, local_rank):
     avg_ms = dom_ms / dom_n
     peak, peak_kind = load_peaks()
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    traffic = None
+    if dom_name in NCU_TRAFFIC:
+        tb, tw = NCU_TRAFFIC[dom_name]
+        traffic = int(round(tb * units["wet"] / tw))
     phases = {k: {"launches": n, "ms_per_launch": t / n, "share": t / total_ms} for k, (n, t) in rep.items()}
 
     # end to end through the C ABI: host fields in and out every step (pinned buffers)
@@ -310,7 +326,7 @@ def run_ours(args, rank, world, local_rank):
                     "d2h_bytes_per_step": field_bytes, "steps": e2e_steps,
                     "api": "hyd_set_field(z,u,v,FS) + hyd_step(1) + hyd_get_field(z,u,v,FS), pinned host buffers"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_launch": bytes_per_launch, "bytes_unit": "%d B x %d %s cells" % (
                              per_unit, units[unit], unit),
                          "ms_per_launch": avg_ms, "timed": "events around this phase alone, L2 flushed per step"},
