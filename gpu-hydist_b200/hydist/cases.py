@@ -309,3 +309,37 @@ def config2_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE):
     2-cell oscillation once velocities pass about 2.5 m/s)."""
     return meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, spinup_h=spinup_h,
                         Q0=2000.0 * q_scale, Q1=3500.0 * q_scale, name="config2_meander")
+
+
+def config3_cases(n=96, seed=20261204, nx_range=(128, 1024), ny_range=(64, 512), hours=2.0, spinup_h=0.5):
+    """The ensemble of independent reaches: n seeded meandering channels.
+
+    Per reach: nx log-uniform in nx_range, ny log-uniform in ny_range, dx = dy = 5 m,
+    dt = 1 s; sinuosity amplitude uniform 0-150 m (cut so that the channel stays inside
+    the domain) and wavelength uniform 800-2500 m; Manning n uniform 0.018-0.035;
+    discharge Q uniform 100-3000 m3/s.  Hydraulics + sediment for `hours` after a
+    `spinup_h` discharge ramp (sediment from the end of the ramp, bed change an hour
+    later).  The channel is the meander generator's parabolic section, its width
+    min(150 m, 35 % of the domain width) and depth 4 m + 4 m x width / 150 m; Q is scaled
+    by the width ratio and by the same stability factor as config 2 (the reference's
+    scheme blows up on the full discharges, see config2_case)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx = int(round(math.exp(rng.uniform(math.log(nx_range[0]), math.log(nx_range[1])))))
+        ny = int(round(math.exp(rng.uniform(math.log(ny_range[0]), math.log(ny_range[1])))))
+        dX = 5.0
+        width = min(150.0, 0.35 * ny * dX)
+        depth = 4.0 + 4.0 * width / 150.0
+        amp = min(rng.uniform(0.0, 150.0), max(0.0, (ny * dX - width) / 2.0 - 4 * dX))
+        wavelength = rng.uniform(800.0, 2500.0)
+        manning = rng.uniform(0.018, 0.035)
+        q = rng.uniform(100.0, 3000.0) * CONFIG2_Q_SCALE * width / 150.0
+        c = meander_case(N=nx, M=ny, dX=dX, dT=1.0, hours=hours, seed=seed + 1 + k, amp=amp,
+                         wavelength=wavelength, width=width, depth=depth, manning=manning,
+                         manning_spread=0.0, Q0=q, Q1=q, tide_amp=0.5, spinup_h=spinup_h,
+                         sediment_start=spinup_h * 3600.0, bed_change_start=spinup_h * 3600.0 + 3600.0,
+                         end_cells=min(8, nx // 16), name="config3_reach%02d" % k)
+        c.notes.update({"Q": q, "amp": amp, "wavelength": wavelength, "manning": manning})
+        out.append(c)
+    return out

@@ -1,0 +1,139 @@
+"""Ensembles of independent reaches split across ranks (hydist.ensemble).
+
+CPU: the cost partition, and two ranks over torch.distributed's gloo backend (processes
+on 127.0.0.1) whose reaches step through the oracle: the gathered fields equal one
+process stepping every reach, and the max-over-ranks reduction returns the largest
+rank's value.  GPU: the same reaches stepped through the library on one device, each
+handle on its own stream, equal bit for bit to handles stepped one at a time."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+STEPS = 6
+
+
+def _small_cases(n=5):
+    from hydist import cases
+    return cases.config3_cases(n=n, seed=11, nx_range=(24, 48), ny_range=(16, 32), hours=1.0, spinup_h=0.1)
+
+
+class _OracleStepper:
+    """The stepping interface of a library handle, on the CPU oracle (test only)."""
+
+    def __init__(self, case):
+        import oracle
+        self.o = oracle.OracleSim(case, threads=1)
+        self.o.init()
+
+    def step(self, n=1, sync=True):
+        self.o.step(n)
+
+    def synchronize(self):
+        pass
+
+    def get(self, name):
+        return self.o.get(name)
+
+    def close(self):
+        self.o.close()
+
+
+def test_partition_covers_and_balances():
+    from hydist import cases
+    from hydist.ensemble import partition, reach_cost
+    cs = cases.config3_cases(n=96)
+    costs = [reach_cost(c) for c in cs]
+    for world in (1, 2, 4, 8):
+        parts = partition(costs, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(cs)))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) <= sum(costs) / world + max(costs)
+        assert parts == partition(costs, world)  # deterministic
+    # a reach never splits: world larger than the ensemble leaves ranks empty
+    assert sum(len(p) == 0 for p in partition(costs[:3], 5)) == 2
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, out_dir):
+    import datetime
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    for p in (root, os.path.join(root, "gpu-hydist_b200"), os.path.join(root, "oracle"), here):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import torch.distributed as dist
+    from hydist.ensemble import Ensemble, checksum, max_over_ranks
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        ens = Ensemble(_small_cases(), rank=rank, world=world, factory=_OracleStepper)
+        ens.step(STEPS)
+        got = ens.gather(("z", "u", "v"))
+        mx = max_over_ranks(float(rank + 1) * 1.5)
+        upd = max_over_ranks(ens.cell_updates(STEPS))
+        if rank == 0:
+            np.save(os.path.join(out_dir, "result.npy"),
+                    {"owned": ens.owned, "sums": checksum(got), "max": mx, "upd": upd,
+                     "fields": got}, allow_pickle=True)
+        ens.close()
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_match_one_process(tmp_path, oracle_lib):
+    import torch.multiprocessing as mp
+    from hydist.ensemble import Ensemble, partition, reach_cost
+    world, port = 2, _free_port()
+    mp.spawn(_rank_main, args=(world, port, str(tmp_path)), nprocs=world, join=True)
+    res = np.load(tmp_path / "result.npy", allow_pickle=True).item()
+    cs = _small_cases()
+    parts = partition([reach_cost(c) for c in cs], world)
+    assert res["owned"] == parts[0]
+    assert res["max"] == 3.0
+    assert res["upd"] == max(STEPS * sum(reach_cost(cs[i]) for i in p) for p in parts)
+    ref = Ensemble(cs, rank=0, world=1, factory=_OracleStepper)
+    ref.step(STEPS)
+    want = ref.fields(("z", "u", "v"))
+    ref.close()
+    assert sorted(res["fields"]) == list(range(len(cs)))
+    for i, d in want.items():
+        for f, a in d.items():
+            assert np.array_equal(res["fields"][i][f], a), (i, f)
+            assert np.isfinite(a).all()
+
+
+@pytest.mark.gpu
+def test_gpu_ensemble_streams_match_single_handles(oracle_lib):
+    from helpers import REL_TOL, rel_linf
+    from hydist.ensemble import Ensemble
+    from hydist.lib import Simulation
+    import oracle
+    cs = _small_cases()
+    ens = Ensemble(cs, rank=0, world=1)
+    ens.step(STEPS)
+    got = ens.fields(("z", "u", "v", "FS"))
+    ens.close()
+    for i, c in enumerate(cs):
+        s = Simulation.from_case(c)
+        s.step(STEPS)
+        for f in ("z", "u", "v", "FS"):
+            assert np.array_equal(got[i][f], s.get(f)), (i, f)
+        s.close()
+        o = oracle.OracleSim(c)
+        o.init()
+        o.step(STEPS)
+        for f in ("z", "u", "v"):
+            e = rel_linf(got[i][f], o.get(f))
+            assert e <= REL_TOL, "reach %d %s rel L-inf %.3e" % (i, f, e)
