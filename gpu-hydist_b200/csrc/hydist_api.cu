@@ -69,6 +69,7 @@ struct HydSim {
     double* scratch_u;  // smoothing ping-pong partners
     double* scratch_v;
     double* sweep_scratch;  // rows/cells of lines too long for shared memory
+    double* fs_scratch;     // the same for the sediment sweeps (which may run beside the others)
     SweepPlan plan;         // launch shapes of the sweeps
     void* arena;
     size_t arena_bytes;
@@ -101,7 +102,7 @@ struct HydSim {
     int thr_r, thr_c;
     // second stream for work that runs beside the main chain (forked and joined by events)
     cudaStream_t side;
-    cudaEvent_t ev_fork, ev_join;
+    cudaEvent_t ev_fork, ev_join, ev_fork2, ev_join2;
     cudaGraphExec_t graph[8];
     long long graph_kernels[8];
     // timing with graphs: one graph per variant with the phase events captured in it
@@ -184,28 +185,30 @@ cudaEvent_t pool_event(HydSim* s) {
 struct PhaseScope {
     HydSim* s;
     int ph;
+    cudaStream_t st;  // the stream the phase's launches go to
     cudaEvent_t a = nullptr;
     // inside a capture an event record is an ordering edge unless marked external
-    static void record(HydSim* s, cudaEvent_t e) {
-        if (s->mark_sink) cudaEventRecordWithFlags(e, s->stream, cudaEventRecordExternal);
-        else cudaEventRecord(e, s->stream);
+    void record(cudaEvent_t e) {
+        if (s->mark_sink) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+        else cudaEventRecord(e, st);
     }
-    PhaseScope(HydSim* s_, int ph_) : s(s_), ph(ph_) {
+    PhaseScope(HydSim* s_, int ph_, cudaStream_t st_) : s(s_), ph(ph_), st(st_) {
         if ((s->timing >> ph) & 1u) {
             a = pool_event(s);
-            record(s, a);
+            record(a);
         }
     }
     ~PhaseScope() {
         if (a) {
             cudaEvent_t b = pool_event(s);
-            record(s, b);
+            record(b);
             (s->mark_sink ? *s->mark_sink : s->marks).push_back({ph, a, b});
         }
     }
 };
 }  // namespace
-#define PHASE(ph) PhaseScope phase_scope_##__LINE__(s, ph)
+#define PHASE(ph) PhaseScope phase_scope_##__LINE__(s, ph, s->stream)
+#define PHASE_ON(ph, stream) PhaseScope phase_scope_##__LINE__(s, ph, stream)
 
 namespace {
 
@@ -405,10 +408,13 @@ void hyd_params_default(HydCaseParams* p) {
 // Free what a handle holds (any of it may be missing on a failed create) and the handle.
 static void release(HydSim* s) {
     cudaFree(s->sweep_scratch);
+    cudaFree(s->fs_scratch);
     cudaFree(s->g.colT);
     cudaFree(s->arena);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->ev_fork2) cudaEventDestroy(s->ev_fork2);
+    if (s->ev_join2) cudaEventDestroy(s->ev_join2);
     if (s->side) cudaStreamDestroy(s->side);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -456,6 +462,8 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork2, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join2, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         release(s);
         return fail(HYD_ECUDA, std::string("streams: ") + cudaGetErrorString(e));
@@ -549,6 +557,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     }
     s->sweep_scratch = nullptr;
     e = cudaMalloc(&s->sweep_scratch, s->plan.scratch_doubles * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&s->fs_scratch, s->plan.scratch_doubles * sizeof(double));
     if (e != cudaSuccess) {
         release(s);
         return fail(HYD_ENOMEM, std::string("sweep scratch: ") + cudaGetErrorString(e));
@@ -744,10 +753,10 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     }
     { PHASE(PH_COEF_UZ); launch_coef_uz(g, p, st, s->side, s->ev_fork, s->ev_join); }
     { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, 0, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_EXPL_V); launch_explicit_v(g, p, s->thr_r, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, st); }
     std::swap(g.t_v, s->scratch_v);
     if (force) launch_mark_all_cols(g, st);
     { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, s->thr_r, st); }
@@ -761,14 +770,29 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         { PHASE(PH_POST); launch_post(g, p, fh, st); }
         { PHASE(PH_SCAN); launch_scan_cols(g, p, st); }
     }
-    if (sed1) {
+    // With span-limited passes the first half-step's sediment (FSj coefficients, sweep and
+    // update) runs on the side stream beside the second half-step up to its explicit u: it
+    // reads u, v (equal to t_u, t_v after the update above), FS, H_moi, VTH, K and the
+    // column segments, none of which those launches write, and its coefficients live in
+    // column-major slots they do not use.  The second half-step's boundary then writes
+    // velocities and levels only; its inflow concentrations (FS) follow the join, in the
+    // smoothing launch that precedes the column resets.
+    const int overlap = sed1 && fuse1 && !p.channel;
+    if (overlap) {
+        cudaEventRecord(s->ev_fork2, st);
+        cudaStreamWaitEvent(s->side, s->ev_fork2, 0);
+        { PHASE_ON(PH_COEF_FSJ, s->side); launch_coef_fsj(g, p, 0, s->side); }
+        { PHASE_ON(PH_FS_J, s->side); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->fs_scratch, s->side); }
+        { PHASE_ON(PH_UPDATE_FS, s->side); launch_update_fs(g, fsd, s->side); }
+        cudaEventRecord(s->ev_join2, s->side);
+    } else if (sed1) {
         if (!(sed1 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
         { PHASE(PH_COEF_FSJ); launch_coef_fsj(g, p, 0, st); }
-        { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->sweep_scratch, st); }
+        { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->fs_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
     }
     // ---- half-step 2: implicit along j (rows), explicit u
-    { PHASE(PH_BOUNDARY); launch_boundary(g, p, 1, st); }
+    { PHASE(PH_BOUNDARY); launch_boundary(g, p, 1, overlap ? 1 : 3, st); }
     start_idx = 2;
     end_idx = s->N;
     if (p.channel && s->P.kenhhepng == 1) {
@@ -776,11 +800,12 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         end_idx = s->N;
     }
     { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, st); }
     std::swap(g.t_v, s->scratch_v);
     { PHASE(PH_COEF_EU); launch_coef_eu(g, p, st); }
     { PHASE(PH_EXPL_U); launch_explicit_u(g, p, s->thr_c, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 1, st); }
+    if (overlap) cudaStreamWaitEvent(st, s->ev_join2, 0);
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 1, overlap, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }
     if (!fh) {
@@ -792,7 +817,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     }
     if (sed2) {
         if (!(sed2 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
-        { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, s->plan, 1, s->solver, s->sweep_scratch, st); }
+        { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, s->plan, 1, s->solver, s->fs_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
         start_idx = 3;
         end_idx = s->N - 1;

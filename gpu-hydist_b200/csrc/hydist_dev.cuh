@@ -117,7 +117,8 @@ __device__ __forceinline__ int find_seg_u(const DevGrid& g, int row, int col, in
 // Host launch wrappers (defined in the .cu files, called by hydist_api.cu).
 struct StepLaunch;
 void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_mask, cudaStream_t s);
-void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
+// writes: 1 velocities/levels, 2 inflow concentrations, 3 both (ignored in channel mode)
+void launch_boundary(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s);
 // Launch shapes of the sweeps for one grid (k_sweep.cu).
 struct SweepPlan {
     size_t smem_lines, smem_fs_lines;  // dynamic shared memory of the hydrodynamic / sediment sweeps
@@ -134,7 +135,10 @@ void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, 
 void launch_sweep_vz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
                      int solver, double* scratch, cudaStream_t s);
 // bytes: also write the column reset bytes (the smoothing of u just before the column resets)
-void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, cudaStream_t s);
+// fs_bnd: also apply the concentration part of the second half-step's boundary (span
+// passes only)
+void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, int fs_bnd,
+                   cudaStream_t s);
 void launch_widen_spans(const DevGrid& g, cudaStream_t s);
 void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
 void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);

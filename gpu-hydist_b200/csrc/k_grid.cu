@@ -176,13 +176,17 @@ __device__ BndRec bnd_compute(const DevGrid& g, const EdgeArgs& a, int i, double
     return r;
 }
 
-__device__ void bnd_apply(const DevGrid& g, const EdgeArgs& a, const BndRec& r, int i) {
+// writes: kBndHydro (discharge-edge velocities, stage-edge levels), kBndFS (inflow
+// concentrations), or both.
+constexpr int kBndHydro = 1, kBndFS = 2, kBndAll = 3;
+
+__device__ void bnd_apply(const DevGrid& g, const EdgeArgs& a, const BndRec& r, int i, int writes) {
     const int P = g.P;
     if (r.kind == 1) {
-        a.barr[i] = r.value;
+        if (writes & kBndHydro) a.barr[i] = r.value;
         const int ii = a.isU ? a.location : i, jj = a.isU ? i : a.location;
-        g.FS[ii * P + jj] = r.fsv;
-    } else if (r.kind == 2) {
+        if (writes & kBndFS) g.FS[ii * P + jj] = r.fsv;
+    } else if (r.kind == 2 && (writes & kBndHydro)) {
         if (a.isU) {
             g.t_z[a.location * P + i] = r.value;
             g.t_z[a.location_ext * P + i] = r.value;
@@ -199,8 +203,10 @@ __device__ void bnd_apply(const DevGrid& g, const EdgeArgs& a, const BndRec& r, 
 // Here the four edges run at once, each in a quarter of the CTA (blockDim a multiple of
 // 128), holding back their corner writes; thread 0 then applies those in the reference's
 // order, and again the (N, 2) write of the down edge and, when N > M, the (N, M) write of
-// the up edge, which threads past the first warp repeat in the reference.
-__device__ void boundary_body(const DevGrid& g, double t) {
+// the up edge, which threads past the first warp repeat in the reference.  `writes`
+// selects the arrays written (the same order applies within each array), so the
+// concentration part can run after work that the velocity/level part need not wait for.
+__device__ void boundary_body(const DevGrid& g, double t, int writes = kBndAll) {
     __shared__ BndRec s_rec[4][2];
     const int N = g.N, M = g.M;
     const int imax = N > M ? N : M;
@@ -212,22 +218,22 @@ __device__ void boundary_body(const DevGrid& g, double t) {
             const BndRec rec = bnd_compute(g, a, i, t);
             if (i == 2) s_rec[e][0] = rec;
             else if (i == far) s_rec[e][1] = rec;
-            else bnd_apply(g, a, rec, i);
+            else bnd_apply(g, a, rec, i, writes);
         }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int k = 0; k < 4; k++) {
             const EdgeArgs a = edge_args(g, k);
-            bnd_apply(g, a, s_rec[k][0], 2);
-            bnd_apply(g, a, s_rec[k][1], a.isU ? M : N);
+            bnd_apply(g, a, s_rec[k][0], 2, writes);
+            bnd_apply(g, a, s_rec[k][1], a.isU ? M : N, writes);
         }
-        bnd_apply(g, edge_args(g, 1), s_rec[1][1], N);
-        if (N > M) bnd_apply(g, edge_args(g, 0), s_rec[0][1], N);
+        bnd_apply(g, edge_args(g, 1), s_rec[1][1], N, writes);
+        if (N > M) bnd_apply(g, edge_args(g, 0), s_rec[0][1], N, writes);
     }
 }
 
-__global__ void k_boundary(DevGrid g, DevParams p, int half) { boundary_body(g, g.clock[half]); }
+__global__ void k_boundary(DevGrid g, DevParams p, int half, int writes) { boundary_body(g, g.clock[half], writes); }
 
 // Channel-mode analytic seiche boundaries (support_funcs.cu:356-429, Engine.py:30-43).
 // Engine.py passes m_offset = 5 as the kernels' segment_limit parameter, so the segment
@@ -430,8 +436,15 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
     if (BYTES) reset_byte_cell(g, p, i, j);
 }
 
-template <int BYTES>
+// FSB: one more CTA (the last) applies the concentration part of the second half-step's
+// boundary (kBndFS), when the velocity/level part ran before the first half-step's
+// sediment sweep had finished.
+template <int BYTES, int FSB>
 __global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
+    if (FSB && blockIdx.x == gridDim.x - 1) {
+        boundary_body(g, g.clock[1], kBndFS);
+        return;
+    }
     const RowLane rl(g, 0);
     const int i = rl.i;
     if (i > g.N + 2) return;
@@ -572,15 +585,19 @@ __device__ __forceinline__ double eu_cell(const DevGrid& g, const DevParams& p, 
     return q / pp;
 }
 
+// The column-major slot of the explicit_u values: not one of the FSj coefficients' slots
+// (0..3), which the FSj sweep may still be reading while the next half-step runs.
+constexpr int kEuSlot = 4;
+
 // explicit_u values of every wet cell of rows 2..N-1, columns 2..M, one warp per row over
-// the row's span; written column-major (g.colT array 0).
+// the row's span; written column-major (g.colT array kEuSlot).
 __global__ void k_coef_eu(DevGrid g, DevParams p) {
     const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i > g.N - 1) return;
     const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
     for (int j = lo + lane; j <= hi; j += 32) {
         if (g.khouot[i * g.P + j] != 0) continue;
-        colT(g, 0)[(size_t)j * g.LT + i] = eu_cell(g, p, i, j);
+        colT(g, kEuSlot)[(size_t)j * g.LT + i] = eu_cell(g, p, i, j);
     }
 }
 
@@ -619,7 +636,7 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
             int k = 0;
             while (k + 1 < nseg && s_off[k + 1] <= c) k++;
             const int row = s_first[k] + (c - s_off[k]);
-            const double tu = colT(g, 0)[(size_t)col * g.LT + row];  // k_coef_eu
+            const double tu = colT(g, kEuSlot)[(size_t)col * g.LT + row];  // k_coef_eu
             g.t_u[row * P + col] = tu;
             su[row - k0] = tu;
         }
@@ -1464,9 +1481,9 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
     hyd_kernel_launches_add(6);
 }
 
-void launch_boundary(const DevGrid& g, const DevParams& p, int half, cudaStream_t s) {
+void launch_boundary(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
     if (p.channel) k_boundary_channel<<<1, 256, 0, s>>>(g, p, half);
-    else k_boundary<<<1, 512, 0, s>>>(g, p, half);
+    else k_boundary<<<1, 512, 0, s>>>(g, p, half, writes);
     hyd_kernel_launches_add(1);
 }
 
@@ -1486,14 +1503,17 @@ void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s, cudaSt
 // Elementwise kernels: the whole grid (`full`), or one warp per row over its extended span.
 static int row_warps_blocks(const DevGrid& g, int rows) { return (rows * g.wpr * 32 + 255) / 256; }
 
-void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, cudaStream_t s) {
+void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, int fs_bnd,
+                   cudaStream_t s) {
     const dim3 b(32, 8);
-    if (full) {
+    if (full) {  // callers pass fs_bnd = 0 with full passes
         if (bytes) k_smooth<1><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         else k_smooth<0><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
     } else {
-        if (bytes) k_smooth_span<1><<<row_warps_blocks(g, g.N + 3), 256, 0, s>>>(g, p, isU, out);
-        else k_smooth_span<0><<<row_warps_blocks(g, g.N + 3), 256, 0, s>>>(g, p, isU, out);
+        const int nb = row_warps_blocks(g, g.N + 3);
+        if (bytes && fs_bnd) k_smooth_span<1, 1><<<nb + 1, 256, 0, s>>>(g, p, isU, out);
+        else if (bytes) k_smooth_span<1, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
+        else k_smooth_span<0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
     }
     hyd_kernel_launches_add(1);
 }

@@ -721,8 +721,12 @@ __device__ __forceinline__ void fs_cell_coeffs(const DevGrid& g, const DevParams
     if (DIR == 1) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
     double pp, qq;
     if (DIR == 0) {
-        aa = -gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 - g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
-        cc = gamav * 0.5 * (g.t_u[pos] + g.t_u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
+        // FSj runs right after the half-step's state update, which left u = t_u and v = t_v
+        // on every cell it reads; reading u and v lets it run beside the next half-step's
+        // sweeps, which write t_u and t_v
+        const double *u = g.u, *v = g.v;
+        aa = -gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
+        cc = gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
         bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
         pp = 0;
         qq = 0;
@@ -731,7 +735,7 @@ __device__ __forceinline__ void fs_cell_coeffs(const DevGrid& g, const DevParams
         pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
         if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
             qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
-            qq = (g.t_v[pos] + g.t_v[pos - 1]) * 0.5 * qq * gamav;
+            qq = (v[pos] + v[pos - 1]) * 0.5 * qq * gamav;
         } else
             qq = 0;
         dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
@@ -841,11 +845,11 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
             cc = colT(g, 2)[q];
             dd = colT(g, 3)[q];
             if (k == f + 1) {
-                if (b1f || g.t_u[base + f * along] == 0) bb += aa;
+                if (b1f || g.u[base + f * along] == 0) bb += aa;
                 else dd -= aa * FS[base + f * along];
             }
             if (k == l - 1) {
-                if (b2f && g.t_u[base + l * along] == 0) bb += cc;
+                if (b2f && g.u[base + l * along] == 0) bb += cc;
                 else dd -= cc * FS[base + l * along];
             }
         } else {
@@ -867,7 +871,7 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     G::sync();
     solve_line<G, SOLVER>(A, B, Cc, D, pl, R, red);
     const double* x = B;
-    double* vel = DIR == 0 ? g.t_u : g.t_v;
+    const double* vel = DIR == 0 ? g.u : g.t_v;  // FSj: u = t_u here (see fs_cell_coeffs)
     for (int c = tid; c < R; c += T) {
         const int sI = seg_of_row(sg, c);
         const int f = sg.first[sI], l = sg.last[sI];
