@@ -102,7 +102,7 @@ struct HydSim {
     int thr_r, thr_c;
     // second stream for work that runs beside the main chain (forked and joined by events)
     cudaStream_t side;
-    cudaEvent_t ev_fork, ev_join, ev_fork2, ev_join2;
+    cudaEvent_t ev_fork, ev_join;
     cudaGraphExec_t graph[8];
     long long graph_kernels[8];
     // timing with graphs: one graph per variant with the phase events captured in it
@@ -410,11 +410,10 @@ static void release(HydSim* s) {
     cudaFree(s->sweep_scratch);
     cudaFree(s->fs_scratch);
     cudaFree(s->g.colT);
+    cudaFree(s->g.rowC);
     cudaFree(s->arena);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     if (s->ev_join) cudaEventDestroy(s->ev_join);
-    if (s->ev_fork2) cudaEventDestroy(s->ev_fork2);
-    if (s->ev_join2) cudaEventDestroy(s->ev_join2);
     if (s->side) cudaStreamDestroy(s->side);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -462,8 +461,6 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork2, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join2, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         release(s);
         return fail(HYD_ECUDA, std::string("streams: ") + cudaGetErrorString(e));
@@ -551,6 +548,8 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     s->g.colT_stride = (size_t)(M + 3) * s->g.LT;
     e = cudaMalloc(&s->g.colT, 7 * s->g.colT_stride * sizeof(double) + s->g.colT_stride);
     s->g.colB = (unsigned char*)(s->g.colT + 7 * s->g.colT_stride);
+    s->g.rowC_stride = (size_t)(N + 3) * s->pitch;
+    if (e == cudaSuccess) e = cudaMalloc(&s->g.rowC, 7 * s->g.rowC_stride * sizeof(double));
     if (e != cudaSuccess) {
         release(s);
         return fail(HYD_ENOMEM, std::string("column-major scratch: ") + cudaGetErrorString(e));
@@ -751,7 +750,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         start_idx = 3;
         end_idx = s->M - 1;
     }
-    { PHASE(PH_COEF_UZ); launch_coef_uz(g, p, st, s->side, s->ev_fork, s->ev_join); }
+    { PHASE(PH_COEF_UZ); launch_coef_bnd(g, p, 0, 3, st); }
     { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, 0, st); }
     std::swap(g.t_u, s->scratch_u);
@@ -779,12 +778,12 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     // smoothing launch that precedes the column resets.
     const int overlap = sed1 && fuse1 && !p.channel;
     if (overlap) {
-        cudaEventRecord(s->ev_fork2, st);
-        cudaStreamWaitEvent(s->side, s->ev_fork2, 0);
+        cudaEventRecord(s->ev_fork, st);
+        cudaStreamWaitEvent(s->side, s->ev_fork, 0);
         { PHASE_ON(PH_COEF_FSJ, s->side); launch_coef_fsj(g, p, 0, s->side); }
         { PHASE_ON(PH_FS_J, s->side); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->fs_scratch, s->side); }
         { PHASE_ON(PH_UPDATE_FS, s->side); launch_update_fs(g, fsd, s->side); }
-        cudaEventRecord(s->ev_join2, s->side);
+        cudaEventRecord(s->ev_join, s->side);
     } else if (sed1) {
         if (!(sed1 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
         { PHASE(PH_COEF_FSJ); launch_coef_fsj(g, p, 0, st); }
@@ -792,7 +791,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
     }
     // ---- half-step 2: implicit along j (rows), explicit u
-    { PHASE(PH_BOUNDARY); launch_boundary(g, p, 1, overlap ? 1 : 3, st); }
+    { PHASE(PH_BOUNDARY); launch_coef_bnd(g, p, 1, overlap ? 1 : 3, st); }
     start_idx = 2;
     end_idx = s->N;
     if (p.channel && s->P.kenhhepng == 1) {
@@ -804,7 +803,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     std::swap(g.t_v, s->scratch_v);
     { PHASE(PH_COEF_EU); launch_coef_eu(g, p, st); }
     { PHASE(PH_EXPL_U); launch_explicit_u(g, p, s->thr_c, st); }
-    if (overlap) cudaStreamWaitEvent(st, s->ev_join2, 0);
+    if (overlap) cudaStreamWaitEvent(st, s->ev_join, 0);
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 1, overlap, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }

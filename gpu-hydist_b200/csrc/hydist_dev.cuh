@@ -58,6 +58,8 @@ struct DevGrid {
     // (M+3) columns x LT rows (LT = N+3 rounded up to 32), array k at colT + k*colT_stride
     double* colT;
     unsigned char* colB;  // column-major reset bytes of the column resets (stride LT)
+    double* rowC;         // row-major VZ coefficients, 7 arrays of (N+3) x P
+    size_t rowC_stride;
     size_t colT_stride;
     int LT;
     int wpr;  // warps per row of the extended-span kernels (1 until the spans are known)
@@ -68,6 +70,7 @@ __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { at
 
 // Column-major copy k of a per-cell quantity; (row i, column j) is at [j * g.LT + i].
 __device__ __forceinline__ double* colT(const DevGrid& g, int k) { return g.colT + (size_t)k * g.colT_stride; }
+__device__ __forceinline__ double* rowC(const DevGrid& g, int k) { return g.rowC + (size_t)k * g.rowC_stride; }
 
 // Wall/open flags of a row segment [first, last] (locate_segment_v, constant.cuh:135-154).
 __device__ __forceinline__ void seg_flags_v(const DevGrid& g, const DevParams& p, int row, int first, int last,
@@ -117,8 +120,6 @@ __device__ __forceinline__ int find_seg_u(const DevGrid& g, int row, int col, in
 // Host launch wrappers (defined in the .cu files, called by hydist_api.cu).
 struct StepLaunch;
 void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_mask, cudaStream_t s);
-// writes: 1 velocities/levels, 2 inflow concentrations, 3 both (ignored in channel mode)
-void launch_boundary(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s);
 // Launch shapes of the sweeps for one grid (k_sweep.cu).
 struct SweepPlan {
     size_t smem_lines, smem_fs_lines;  // dynamic shared memory of the hydrodynamic / sediment sweeps
@@ -157,8 +158,11 @@ void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
 void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s);
-void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                    cudaEvent_t join);
+// The first launch of half-step `half`: its line coefficients (UZ column-major / VZ
+// row-major) and its boundary values (`writes`: 1 velocities/levels, 2 inflow
+// concentrations, 3 both; ignored in channel mode and in half-step 1, which writes both
+// and advances the clock).
+void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s);
 void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
                        double* scratch, cudaStream_t s);

@@ -233,7 +233,6 @@ __device__ void boundary_body(const DevGrid& g, double t, int writes = kBndAll) 
     }
 }
 
-__global__ void k_boundary(DevGrid g, DevParams p, int half, int writes) { boundary_body(g, g.clock[half], writes); }
 
 // Channel-mode analytic seiche boundaries (support_funcs.cu:356-429, Engine.py:30-43).
 // Engine.py passes m_offset = 5 as the kernels' segment_limit parameter, so the segment
@@ -284,7 +283,6 @@ __device__ void boundary_channel_body(const DevGrid& g, const DevParams& p, doub
     }
 }
 
-__global__ void k_boundary_channel(DevGrid g, DevParams p, int half) { boundary_channel_body(g, p, g.clock[half]); }
 
 // Continuity and momentum coefficients of one wet cell of a UZ line (column j, cell i):
 // a2, c2, d2 (_uzSolver_calculate_preindex, UVZSolver_multithread.cu:402-406) and f1, f2,
@@ -323,28 +321,71 @@ __device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams
          p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
 }
 
-// First launches of a step, side by side: UZ coefficients of every wet interior cell, one
-// warp per row over the row's span of cells that can be wet, written column-major
-// (g.colT arrays 0..6: a2 c2 d2 f1 f2 f3 f5); and one CTA that advances the step clock
-// and applies the boundary values of the first half-step (neither reads what the other
-// writes).  The column-major stores are one sector per lane, so the coefficients are
-// spread over many small CTAs.
-__global__ void k_clock_boundary(DevGrid g, DevParams p) {
-    __shared__ double s_t;
-    if (threadIdx.x == 0) {  // k_clock
-        const double t1 = g.clock[2] + p.dT * 0.5;
-        const double t2 = t1 + p.dT * 0.5;
-        g.clock[0] = t1;
-        g.clock[1] = t2;
-        g.clock[2] = t2;
-        s_t = t1;
+// Momentum and continuity coefficients of a VZ cell (preindex, _calculate_abcd:
+// UVZSolver_multithread.cu:345-349, 409-466 for the v direction): the terms the VZ sweep
+// combines into its rows, precomputed row-major so that the sweep's row building is loads.
+__device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& a2, double& c2,
+                                               double& d2, double& f1, double& f2, double& f3, double& f5) {
+    const int P = g.P;
+    c2 = p.dTchia2dY * g.Htdv[pos];
+    a2 = -p.dTchia2dY * g.Htdv[pos - 1];
+    d2 = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
+    const double* v = g.v;
+    const double* H = g.H_moi;
+    double pp = 0.0, qq = 0.0;
+    const double utb = (g.u[pos - P] + g.u[pos] + g.u[pos - P + 1] + g.u[pos + 1]) * 0.25;
+    f1 = p.dTchia2dY * v[pos] + g.VISC[pos] * p.dT / p.dYbp;
+    f2 = -(2 + g.Ky1[pos] * p.dT * sqrt(v[pos] * v[pos] + utb * utb) / g.Htdv[pos] + (2 * p.dT * g.VISC[pos]) / p.dYbp);
+    f3 = p.dT * g.VISC[pos] / p.dYbp - p.dTchia2dY * v[pos];
+    if (H[pos - P] <= p.H_TINH) {
+        if (utb < 0) {
+            qq = utb * (-3 * v[pos] + 4 * v[pos + P] - v[pos + 2 * P]) / p.dX2;
+            pp = (v[pos] - 2 * v[pos + P] + v[pos + 2 * P]) / p.dXbp;
+        }
+    } else {
+        if (H[pos + P] <= p.H_TINH) {
+            if ((H[pos - 2 * P] > p.H_TINH) && (utb > 0)) {
+                qq = utb * (3 * v[pos] - 4 * v[pos - P] + v[pos - 2 * P]) / p.dX2;
+                pp = (v[pos] - 2 * v[pos - P] + v[pos - 2 * P]) / p.dXbp;
+            }
+        } else {
+            qq = utb * (v[pos + P] - v[pos - P]) / p.dX2;
+            pp = (v[pos + P] - 2 * v[pos] + v[pos - P]) / p.dXbp;
+        }
     }
-    __syncthreads();
-    if (p.channel) boundary_channel_body(g, p, s_t);
-    else boundary_body(g, s_t);
+    f5 = -2 * v[pos] + p.dT * qq + p.dT * p.CORIOLIS_FORCE * utb - p.dT * g.VISC[pos] * pp -
+         p.dT * (p.windy - g.Tsyw[pos]) / g.Htdv[pos];
 }
 
-__global__ void __launch_bounds__(128) k_coef_uz(DevGrid g, DevParams p) {
+// The first launch of each half-step.  KIND 0 (half-step 1): UZ coefficients of every wet
+// interior cell written column-major (g.colT arrays 0..6: a2 c2 d2 f1 f2 f3 f5), and in
+// the last CTA the clock advance and the boundary values of the half-step.  KIND 1
+// (half-step 2): VZ coefficients written row-major (g.rowC arrays 0..6), and in the last
+// CTA the half-step's boundary values (`writes`).  The coefficients read none of what the
+// boundary writes (edge levels, edge velocity arrays, inflow concentrations).  One warp
+// per row of the grid over the row's span of cells that can be wet; small CTAs, so that
+// the column-major stores (one sector per lane) spread over many SMs.
+template <int KIND>
+__global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int writes) {
+    if (blockIdx.x == gridDim.x - 1) {
+        __shared__ double s_t;
+        if (threadIdx.x == 0) {
+            if (KIND == 0) {  // k_clock
+                const double t1 = g.clock[2] + p.dT * 0.5;
+                const double t2 = t1 + p.dT * 0.5;
+                g.clock[0] = t1;
+                g.clock[1] = t2;
+                g.clock[2] = t2;
+                s_t = t1;
+            } else {
+                s_t = g.clock[1];
+            }
+        }
+        __syncthreads();
+        if (p.channel) boundary_channel_body(g, p, s_t);
+        else boundary_body(g, s_t, writes);
+        return;
+    }
     const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i > g.N) return;
     const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
@@ -352,15 +393,26 @@ __global__ void __launch_bounds__(128) k_coef_uz(DevGrid g, DevParams p) {
         const int pos = i * g.P + j;
         if (g.khouot[pos] != 0) continue;
         double a2, c2, d2, f1, f2, f3, f5;
-        uz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
-        const size_t t = (size_t)j * g.LT + i;
-        colT(g, 0)[t] = a2;
-        colT(g, 1)[t] = c2;
-        colT(g, 2)[t] = d2;
-        colT(g, 3)[t] = f1;
-        colT(g, 4)[t] = f2;
-        colT(g, 5)[t] = f3;
-        colT(g, 6)[t] = f5;
+        if (KIND == 0) {
+            uz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
+            const size_t t = (size_t)j * g.LT + i;
+            colT(g, 0)[t] = a2;
+            colT(g, 1)[t] = c2;
+            colT(g, 2)[t] = d2;
+            colT(g, 3)[t] = f1;
+            colT(g, 4)[t] = f2;
+            colT(g, 5)[t] = f3;
+            colT(g, 6)[t] = f5;
+        } else {
+            vz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
+            rowC(g, 0)[pos] = a2;
+            rowC(g, 1)[pos] = c2;
+            rowC(g, 2)[pos] = d2;
+            rowC(g, 3)[pos] = f1;
+            rowC(g, 4)[pos] = f2;
+            rowC(g, 5)[pos] = f3;
+            rowC(g, 6)[pos] = f5;
+        }
     }
 }
 
@@ -1481,23 +1533,12 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
     hyd_kernel_launches_add(6);
 }
 
-void launch_boundary(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
-    if (p.channel) k_boundary_channel<<<1, 256, 0, s>>>(g, p, half);
-    else k_boundary<<<1, 512, 0, s>>>(g, p, half, writes);
-    hyd_kernel_launches_add(1);
-}
 
-// The step's first launches: k_coef_uz on s, the clock and the first boundary update on
-// `side`, forked from s and joined back into it (a branch of the step graph).
-void launch_coef_uz(const DevGrid& g, const DevParams& p, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                    cudaEvent_t join) {
-    cudaEventRecord(fork, s);
-    cudaStreamWaitEvent(side, fork, 0);
-    k_clock_boundary<<<1, p.channel ? 256 : 512, 0, side>>>(g, p);
-    cudaEventRecord(join, side);
-    k_coef_uz<<<((g.N - 1) * 32 + 127) / 128, 128, 0, s>>>(g, p);
-    cudaStreamWaitEvent(s, join, 0);
-    hyd_kernel_launches_add(2);
+void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
+    const int nb = ((g.N - 1) * 32 + 255) / 256 + 1;
+    if (half == 0) k_coef_bnd<0><<<nb, 256, 0, s>>>(g, p, kBndAll);
+    else k_coef_bnd<1><<<nb, 256, 0, s>>>(g, p, writes);
+    hyd_kernel_launches_add(1);
 }
 
 // Elementwise kernels: the whole grid (`full`), or one warp per row over its extended span.

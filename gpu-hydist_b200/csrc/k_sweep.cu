@@ -21,7 +21,7 @@
 // global scratch region per CTA beyond that).  The solve is always one warp's: lanes
 // eliminate chunks of rows, the chunk ends are solved by shuffle-only cyclic reduction.
 // In the column sweeps the cell-local coefficients come precomputed, stored column-major
-// so that a column reads them contiguously (k_coef_uz, k_coef_fsj).
+// so that a column reads them contiguously (k_coef_bnd<0>, k_coef_fsj).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -413,15 +413,15 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     // continuity coefficients are kept for the extraction.
     auto cont = [&](int k, double& a, double& c, double& d) {
         if (DIR == 0) {
-            const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_uz
+            const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_bnd<0>
             a = colT(g, 0)[t];
             c = colT(g, 1)[t];
             d = colT(g, 2)[t];
         } else {
-            const int pos = base + k * along;
-            c = p.dTchia2dY * g.Htdv[pos];
-            a = -p.dTchia2dY * g.Htdv[pos - 1];
-            d = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
+            const int pos = base + k * along;  // precomputed by k_coef_bnd<1>
+            a = rowC(g, 0)[pos];
+            c = rowC(g, 1)[pos];
+            d = rowC(g, 2)[pos];
         }
     };
     for (int r = R + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
@@ -459,44 +459,18 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         double an, cn, dn;  // the next cell's
         cont(k + 1, an, cn, dn);
         const int pos = base + k * along;
-        double f1, f2, f3, f5;
-        {
-            double pp = 0.0, qq = 0.0;
-            if (DIR == 0) {
-                const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_uz
-                f1 = colT(g, 3)[t];
-                f2 = colT(g, 4)[t];
-                f3 = colT(g, 5)[t];
-                f5 = colT(g, 6)[t];
-                (void)pp;
-                (void)qq;
-            } else {
-                const double* v = g.v;
-                const double* H = g.H_moi;
-                const double utb = (g.u[pos - P] + g.u[pos] + g.u[pos - P + 1] + g.u[pos + 1]) * 0.25;
-                f1 = p.dTchia2dY * v[pos] + g.VISC[pos] * p.dT / p.dYbp;
-                f2 = -(2 + g.Ky1[pos] * p.dT * sqrt(v[pos] * v[pos] + utb * utb) / g.Htdv[pos] +
-                       (2 * p.dT * g.VISC[pos]) / p.dYbp);
-                f3 = p.dT * g.VISC[pos] / p.dYbp - p.dTchia2dY * v[pos];
-                if (H[pos - P] <= p.H_TINH) {
-                    if (utb < 0) {
-                        qq = utb * (-3 * v[pos] + 4 * v[pos + P] - v[pos + 2 * P]) / p.dX2;
-                        pp = (v[pos] - 2 * v[pos + P] + v[pos + 2 * P]) / p.dXbp;
-                    }
-                } else {
-                    if (H[pos + P] <= p.H_TINH) {
-                        if ((H[pos - 2 * P] > p.H_TINH) && (utb > 0)) {
-                            qq = utb * (3 * v[pos] - 4 * v[pos - P] + v[pos - 2 * P]) / p.dX2;
-                            pp = (v[pos] - 2 * v[pos - P] + v[pos - 2 * P]) / p.dXbp;
-                        }
-                    } else {
-                        qq = utb * (v[pos + P] - v[pos - P]) / p.dX2;
-                        pp = (v[pos + P] - 2 * v[pos] + v[pos - P]) / p.dXbp;
-                    }
-                }
-                f5 = -2 * v[pos] + p.dT * qq + p.dT * p.CORIOLIS_FORCE * utb - p.dT * g.VISC[pos] * pp -
-                     p.dT * (p.windy - g.Tsyw[pos]) / g.Htdv[pos];
-            }
+        double f1, f2, f3, f5;  // precomputed by k_coef_bnd (UZ column-major, VZ row-major)
+        if (DIR == 0) {
+            const size_t t = (size_t)line * g.LT + k;
+            f1 = colT(g, 3)[t];
+            f2 = colT(g, 4)[t];
+            f3 = colT(g, 5)[t];
+            f5 = colT(g, 6)[t];
+        } else {
+            f1 = rowC(g, 3)[pos];
+            f2 = rowC(g, 4)[pos];
+            f3 = rowC(g, 5)[pos];
+            f5 = rowC(g, 6)[pos];
         }
         double ra, rb, rc, rd;
         if (Ls >= 2) {
@@ -679,7 +653,9 @@ __device__ __forceinline__ double source_chs(const DevParams& p, double wsm, dou
     if (tob > toee) S = p.Mbochat / p.ros * (tob - toee) / toee;
     else if (tob < todd) {
         const double Pd = 1 - (tob / todd);
-        const double beta = 1 + (Zf / (1.25 + 4.75 * pow(Pd, 2.5)));
+        // Pd^2.5 as Pd^2 sqrt(Pd) (0 < Pd <= 1): the same value to a few ulp, without pow's
+        // general path
+        const double beta = 1 + (Zf / (1.25 + 4.75 * (Pd * Pd * sqrt(Pd))));
         const double Cb = beta * fs;
         S = -wsm * Cb * Pd;
     }
@@ -691,7 +667,7 @@ __device__ __forceinline__ double source_nchs(const DevParams& p, double wsm, do
     // source_nchs (Sediment_Transport.cu:52-60)
     const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
     const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
-    const double Cac = 0.015 * p.dm * pow(Tx, 1.5) * p.dxr_m03 / (0.05 * h_moi);
+    const double Cac = 0.015 * p.dm * (Tx * sqrt(Tx)) * p.dxr_m03 / (0.05 * h_moi);  // Tx^1.5, Tx >= 0
     return wsm * (Cac - gamac * fs);
 }
 
