@@ -785,7 +785,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         { PHASE_ON(PH_UPDATE_FS, s->side); launch_update_fs(g, fsd, s->side); }
         cudaEventRecord(s->ev_join, s->side);
     } else if (sed1) {
-        if (!(sed1 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
+        if (!(sed1 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, 0, st); }
         { PHASE(PH_COEF_FSJ); launch_coef_fsj(g, p, 0, st); }
         { PHASE(PH_FS_J); launch_fs_sweep_j(g, p, s->plan, 0, s->solver, s->fs_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
@@ -815,7 +815,7 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         { PHASE(PH_SCAN); launch_scan_rows(g, p, st); }
     }
     if (sed2) {
-        if (!(sed2 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, st); }
+        if (!(sed2 && fuse1)) { PHASE(PH_VTH); launch_vth_hesok(g, p, fsd, 1, st); }
         { PHASE(PH_FS_I); launch_fs_sweep_i(g, p, s->plan, 1, s->solver, s->fs_scratch, st); }
         { PHASE(PH_UPDATE_FS); launch_update_fs(g, fsd, st); }
         start_idx = 3;

@@ -82,6 +82,36 @@ __device__ __forceinline__ void seg_flags_v(const DevGrid& g, const DevParams& p
 }
 
 // Wall/open flags of a column segment (locate_segment_u, constant.cuh:156-178).
+// Erosion/deposition source terms of the suspended-sediment rows.
+__device__ __forceinline__ double source_chs(const DevParams& p, double wsm, double Zf, double fs, double fw,
+                                             double vth, double h_moi) {
+    // source_chs (Sediment_Transport.cu:12-49)
+    double toee = p.Toe;
+    const double todd = p.Tod;
+    double S = 0;
+    const double tob = p.ro * fw * (vth * vth);
+    if (h_moi > p.ghtoe) toee = p.Toe * (1 + p.hstoe * ((h_moi - p.ghtoe)));
+    if (tob > toee) S = p.Mbochat / p.ros * (tob - toee) / toee;
+    else if (tob < todd) {
+        const double Pd = 1 - (tob / todd);
+        // Pd^2.5 as Pd^2 sqrt(Pd) (0 < Pd <= 1): the same value to a few ulp, without pow's
+        // general path
+        const double beta = 1 + (Zf / (1.25 + 4.75 * (Pd * Pd * sqrt(Pd))));
+        const double Cb = beta * fs;
+        S = -wsm * Cb * Pd;
+    }
+    return S;
+}
+
+__device__ __forceinline__ double source_nchs(const DevParams& p, double wsm, double Zf, double Uf, double h_moi,
+                                              double fs) {
+    // source_nchs (Sediment_Transport.cu:52-60)
+    const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
+    const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
+    const double Cac = 0.015 * p.dm * (Tx * sqrt(Tx)) * p.dxr_m03 / (0.05 * h_moi);  // Tx^1.5, Tx >= 0
+    return wsm * (Cac - gamac * fs);
+}
+
 __device__ __forceinline__ void seg_flags_u(const DevGrid& g, const DevParams& p, int col, int first, int last,
                                             int& br1, int& br2) {
     const int P = g.P;
@@ -156,7 +186,8 @@ void launch_mark_all_cols(const DevGrid& g, cudaStream_t s);
 void launch_post(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
 void launch_scan_cols(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s);
-void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s);
+// fsi: the second half-step's, which also leaves the FSi cell terms
+void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, int fsi, cudaStream_t s);
 void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s);
 // The first launch of half-step `half`: its line coefficients (UZ column-major / VZ
 // row-major) and its boundary values (`writes`: 1 velocities/levels, 2 inflow

@@ -1166,17 +1166,42 @@ __device__ void fs_edges_block(const DevGrid& g, const DevParams& p) {
 // --------------------------------------------------------------------- sediment
 
 // Find_VTH (Sediment_Transport.cu:541-568) and hesoK (508-539) in one pass
+// The FSi row terms of a wet cell that depend on the cell alone
+// (_FSi_calculate__mactrix_coeff, Sediment_Transport.cu:62-165): gamav (evaluated after
+// Zf) and the source S, gated by t < bed_change_start, over the depth; into rowC arrays 0
+// and 1 for the FSi sweep that follows.  vth: the cell's new VTH.
+__device__ __forceinline__ void fsi_cell_terms(const DevGrid& g, const DevParams& p, int pos, double vth, double t) {
+    const double* FS = g.FS;
+    const double H = g.H_moi[pos];
+    const double c = 18 * log(12 * H / p.Ks);
+    const double Uf = sqrt(p.g) * fabs(vth) / c;
+    const double fq = 1 - FS[pos];
+    const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
+    double Zf = 0;
+    double S;
+    if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
+    if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], vth, H);
+    else S = source_nchs(p, wsm, Zf, Uf, H, FS[pos]);
+    if (t < p.bed_change_start) S = 0;
+    rowC(g, 0)[pos] = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
+    rowC(g, 1)[pos] = S / H;
+}
+
+// Find_VTH + hesoK for cell (i, j); FSI: also the FSi terms of the cell when it is wet.
+template <int FSI>
 __device__ __forceinline__ void vth_cell(const DevGrid& g, const DevParams& p, int i, int j) {
     const int N = g.N, M = g.M, P = g.P;
     if (i > N || j > M) return;
     const int pos = i * P + j;
     if (i >= 2 && j >= 2) {
+        double vth = 0;
         if ((g.htaiz[pos] > p.NANGDAY) && (g.H_moi[pos] > p.H_TINH)) {
             const double ut = (g.t_u[pos] + g.t_u[pos - P]) * 0.5;
             const double vt = (g.t_v[pos] + g.t_v[pos - 1]) * 0.5;
-            g.VTH[pos] = sqrt(ut * ut + vt * vt);
-        } else
-            g.VTH[pos] = 0;
+            vth = sqrt(ut * ut + vt * vt);
+        }
+        g.VTH[pos] = vth;
+        if (FSI && i >= 3 && i < N && j <= M && g.khouot[pos] == 0) fsi_cell_terms(g, p, pos, vth, g.clock[1]);
     }
     const double sg = sqrt(p.g);
     if (g.Htdu[pos] > 0 && pos >= 1) {
@@ -1191,15 +1216,17 @@ __device__ __forceinline__ void vth_cell(const DevGrid& g, const DevParams& p, i
     }
 }
 
+template <int FSI>
 __global__ void k_vth_hesok(DevGrid g, DevParams p) {
-    vth_cell(g, p, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+    vth_cell<FSI>(g, p, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+template <int FSI>
 __global__ void k_vth_span(DevGrid g, DevParams p) {
     const RowLane rl(g, 0);
     const int i = rl.i;
     if (i > g.N) return;
-    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) vth_cell(g, p, i, j);
+    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) vth_cell<FSI>(g, p, i, j);
 }
 
 // After a half-step's reset, in one launch: the state update (update_uvz + Htuongdoi)
@@ -1218,7 +1245,7 @@ __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
         if (i > g.N) return;
         for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
             post_cell(g, 1, i, j);
-            if (VTH) vth_cell(g, p, i, j);
+            if (VTH) vth_cell<ROWS>(g, p, i, j);  // rows: the second half-step, before FSi
         }
         return;
     }
@@ -1339,22 +1366,6 @@ __global__ void k_qb(DevGrid g, DevParams p) {
     }
 }
 
-__device__ __forceinline__ double source_chs_g(const DevParams& p, double wsm, double Zf, double fs, double fw,
-                                               double vth, double h_moi) {
-    double toee = p.Toe;
-    double S = 0;
-    const double tob = p.ro * fw * (vth * vth);
-    if (h_moi > p.ghtoe) toee = p.Toe * (1 + p.hstoe * ((h_moi - p.ghtoe)));
-    if (tob > toee) S = p.Mbochat / p.ros * (tob - toee) / toee;
-    else if (tob < p.Tod) {
-        const double Pd = 1 - (tob / p.Tod);
-        const double beta = 1 + (Zf / (1.25 + 4.75 * pow(Pd, 2.5)));
-        const double Cb = beta * fs;
-        S = -wsm * Cb * Pd;
-    }
-    return S;
-}
-
 // BedLoad/_bed_load (Sediment_Transport.cu:630-639, 416-506): Exner increment into dH
 // on rows startidx..endidx-1.
 __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
@@ -1404,13 +1415,8 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
     const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
     double Zf = 0, S = 0;
     if (FS[pos] > 0.0) Zf = wsm / (0.4 * (Uf + 2 * wsm));
-    if (p.ketdinh) S = source_chs_g(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], g.H_moi[pos]);
-    else {
-        const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
-        const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
-        const double Cac = 0.015 * p.dm * pow(Tx, 1.5) * p.dxr_m03 / (0.05 * g.H_moi[pos]);
-        S = wsm * (Cac - gamac * FS[pos]);
-    }
+    if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], g.H_moi[pos]);
+    else S = source_nchs(p, wsm, Zf, Uf, g.H_moi[pos], FS[pos]);
     g.dH[pos] += p.dT / (1 - p.Dorong) * (S + tH);
 }
 
@@ -1620,10 +1626,15 @@ void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, 
     hyd_kernel_launches_add(1);
 }
 
-void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, cudaStream_t s) {
+void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, int fsi, cudaStream_t s) {
     const dim3 b(32, 8);
-    if (full) k_vth_hesok<<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
-    else k_vth_span<<<row_warps_blocks(g, g.N + 1), 256, 0, s>>>(g, p);
+    if (full) {
+        if (fsi) k_vth_hesok<1><<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
+        else k_vth_hesok<0><<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
+    } else {
+        if (fsi) k_vth_span<1><<<row_warps_blocks(g, g.N + 1), 256, 0, s>>>(g, p);
+        else k_vth_span<0><<<row_warps_blocks(g, g.N + 1), 256, 0, s>>>(g, p);
+    }
     hyd_kernel_launches_add(1);
 }
 

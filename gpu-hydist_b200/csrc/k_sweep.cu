@@ -642,41 +642,14 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
 
 // ---- sediment sweeps --------------------------------------------------------------
 
-__device__ __forceinline__ double source_chs(const DevParams& p, double wsm, double Zf, double fs, double fw,
-                                             double vth, double h_moi) {
-    // source_chs (Sediment_Transport.cu:12-49)
-    double toee = p.Toe;
-    const double todd = p.Tod;
-    double S = 0;
-    const double tob = p.ro * fw * (vth * vth);
-    if (h_moi > p.ghtoe) toee = p.Toe * (1 + p.hstoe * ((h_moi - p.ghtoe)));
-    if (tob > toee) S = p.Mbochat / p.ros * (tob - toee) / toee;
-    else if (tob < todd) {
-        const double Pd = 1 - (tob / todd);
-        // Pd^2.5 as Pd^2 sqrt(Pd) (0 < Pd <= 1): the same value to a few ulp, without pow's
-        // general path
-        const double beta = 1 + (Zf / (1.25 + 4.75 * (Pd * Pd * sqrt(Pd))));
-        const double Cb = beta * fs;
-        S = -wsm * Cb * Pd;
-    }
-    return S;
-}
-
-__device__ __forceinline__ double source_nchs(const DevParams& p, double wsm, double Zf, double Uf, double h_moi,
-                                              double fs) {
-    // source_nchs (Sediment_Transport.cu:52-60)
-    const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
-    const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
-    const double Cac = 0.015 * p.dm * (Tx * sqrt(Tx)) * p.dxr_m03 / (0.05 * h_moi);  // Tx^1.5, Tx >= 0
-    return wsm * (Cac - gamac * fs);
-}
-
 // Row of the sediment system for one interior wet cell before the segment-end terms
 // (_FSj/_FSi_calculate__mactrix_coeff, Sediment_Transport.cu:205-302 / 62-165): aa, bb,
 // cc, dd of the row, with the source S gated by t < bed_change_start.
-template <int DIR>
-__device__ __forceinline__ void fs_cell_coeffs(const DevGrid& g, const DevParams& p, double t, int pos, double& aa,
-                                               double& bb, double& cc, double& dd) {
+// Row of the FSj system for one interior wet cell before the segment-end terms
+// (_FSj_calculate__mactrix_coeff, Sediment_Transport.cu:205-302): aa, bb, cc, dd of the row,
+// with the source S gated by t < bed_change_start.
+__device__ __forceinline__ void fsj_cell_coeffs(const DevGrid& g, const DevParams& p, double t, int pos, double& aa,
+                                                double& bb, double& cc, double& dd) {
     const int P = g.P;
     const double* FS = g.FS;
     const double* H = g.H_moi;
@@ -688,49 +661,53 @@ __device__ __forceinline__ void fs_cell_coeffs(const DevGrid& g, const DevParams
     const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
     double Zf = 0;
     double S;
-    double gamav;
-    if (DIR == 0) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
+    const double gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
     if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
     if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], H[pos]);
     else S = source_nchs(p, wsm, Zf, Uf, H[pos], FS[pos]);
     if (t < s_start) S = 0;
-    if (DIR == 1) gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
-    double pp, qq;
-    if (DIR == 0) {
-        // FSj runs right after the half-step's state update, which left u = t_u and v = t_v
-        // on every cell it reads; reading u and v lets it run beside the next half-step's
-        // sweeps, which write t_u and t_v
-        const double *u = g.u, *v = g.v;
-        aa = -gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
-        cc = gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
-        bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
-        pp = 0;
+    // FSj runs right after the half-step's state update, which left u = t_u and v = t_v
+    // on every cell it reads; reading u and v lets it run beside the next half-step's
+    // sweeps, which write t_u and t_v
+    const double *u = g.u, *v = g.v;
+    aa = -gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
+    cc = gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
+    bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
+    double pp = 0, qq = 0;
+    if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = (FS[pos + 1] - FS[pos]);
+    if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = (FS[pos] - FS[pos - 1]);
+    pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
+    if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
+        qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
+        qq = (v[pos] + v[pos - 1]) * 0.5 * qq * gamav;
+    } else
         qq = 0;
-        if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = (FS[pos + 1] - FS[pos]);
-        if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = (FS[pos] - FS[pos - 1]);
-        pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
-        if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
-            qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
-            qq = (v[pos] + v[pos - 1]) * 0.5 * qq * gamav;
-        } else
-            qq = 0;
-        dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
-    } else {
-        aa = -gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos - 1] * g.Ky[pos - 1] / (H[pos] * p.dYbp);
-        cc = gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos] * g.Ky[pos] / (H[pos] * p.dYbp);
-        bb = p.HaiChiadT + (g.Htdv[pos] * g.Ky[pos] + g.Htdv[pos - 1] * g.Ky[pos - 1]) / (H[pos] * p.dYbp);
-        pp = 0;
+    dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
+}
+
+// Row of the FSi system for one interior wet cell before the segment-end terms
+// (_FSi_calculate__mactrix_coeff, Sediment_Transport.cu:62-165).  The terms that depend on
+// the cell alone (gamav and the gated source over the depth, rowC arrays 0 and 1) were
+// computed by the state update that precedes the sweep (fsi_cell_terms).
+__device__ __forceinline__ void fsi_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& aa,
+                                                double& bb, double& cc, double& dd) {
+    const int P = g.P;
+    const double* FS = g.FS;
+    const double* H = g.H_moi;
+    const double gamav = rowC(g, 0)[pos];
+    aa = -gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos - 1] * g.Ky[pos - 1] / (H[pos] * p.dYbp);
+    cc = gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos] * g.Ky[pos] / (H[pos] * p.dYbp);
+    bb = p.HaiChiadT + (g.Htdv[pos] * g.Ky[pos] + g.Htdv[pos - 1] * g.Ky[pos - 1]) / (H[pos] * p.dYbp);
+    double pp = 0, qq = 0;
+    if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = (FS[pos + P] - FS[pos]);
+    if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = (FS[pos] - FS[pos - P]);
+    pp = (1 / (H[pos] * p.dXbp)) * (g.Htdu[pos] * g.Kx[pos] * pp - g.Htdu[pos - P] * g.Kx[pos - P] * qq);
+    if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
+        qq = (FS[pos + P] - FS[pos - P]) / p.dX2;
+        qq = (g.t_u[pos] + g.t_u[pos - P]) * 0.5 * qq * gamav;
+    } else
         qq = 0;
-        if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = (FS[pos + P] - FS[pos]);
-        if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = (FS[pos] - FS[pos - P]);
-        pp = (1 / (H[pos] * p.dXbp)) * (g.Htdu[pos] * g.Kx[pos] * pp - g.Htdu[pos - P] * g.Kx[pos - P] * qq);
-        if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
-            qq = (FS[pos + P] - FS[pos - P]) / p.dX2;
-            qq = (g.t_u[pos] + g.t_u[pos - P]) * 0.5 * qq * gamav;
-        } else
-            qq = 0;
-        dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
-    }
+    dd = FS[pos] / (p.dT * 0.5) - qq + pp + rowC(g, 1)[pos];
 }
 
 // FSj rows of every interior wet cell (columns 3..M-1), one warp per row of the grid over
@@ -744,7 +721,7 @@ __global__ void k_coef_fsj(DevGrid g, DevParams p, int half) {
         const int pos = i * g.P + j;
         if (g.khouot[pos] != 0) continue;
         double aa, bb, cc, dd;
-        fs_cell_coeffs<0>(g, p, t, pos, aa, bb, cc, dd);
+        fsj_cell_coeffs(g, p, t, pos, aa, bb, cc, dd);
         const size_t q = (size_t)j * g.LT + i;
         colT(g, 0)[q] = aa;
         colT(g, 1)[q] = bb;
@@ -798,7 +775,7 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     const int P = g.P;
     const int along = DIR == 0 ? P : 1;
     const int base = DIR == 0 ? line : line * P;
-    const double t = g.clock[half];
+    (void)half;  // both rows are precomputed (k_coef_fsj, the state update's FSi terms)
     const int R = sg.R;
     for (int r = R + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
         A[r] = 0.0;
@@ -829,7 +806,7 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
                 else dd -= cc * FS[base + l * along];
             }
         } else {
-            fs_cell_coeffs<1>(g, p, t, pos, aa, bb, cc, dd);
+            fsi_cell_coeffs(g, p, pos, aa, bb, cc, dd);
             if (k == f + 1) {
                 if (b1f || g.t_v[base + f * along] == 0) bb = bb + aa;
                 else dd = dd - aa * FS[base + f * along];
@@ -847,7 +824,7 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     G::sync();
     solve_line<G, SOLVER>(A, B, Cc, D, pl, R, red);
     const double* x = B;
-    const double* vel = DIR == 0 ? g.u : g.t_v;  // FSj: u = t_u here (see fs_cell_coeffs)
+    const double* vel = DIR == 0 ? g.u : g.t_v;  // FSj: u = t_u here (see fsj_cell_coeffs)
     for (int c = tid; c < R; c += T) {
         const int sI = seg_of_row(sg, c);
         const int f = sg.first[sI], l = sg.last[sI];
