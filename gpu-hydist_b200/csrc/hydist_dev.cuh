@@ -191,8 +191,7 @@ void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, int fsi, c
 void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s);
 // The first launch of half-step `half`: its line coefficients (UZ column-major / VZ
 // row-major) and its boundary values (`writes`: 1 velocities/levels, 2 inflow
-// concentrations, 3 both; ignored in channel mode and in half-step 1, which writes both
-// and advances the clock).
+// concentrations, 3 both; ignored in channel mode).  Half-step 1 also advances the clock.
 void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s);
 void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s);
 void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,

@@ -1542,7 +1542,7 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
 
 void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
     const int nb = ((g.N - 1) * 32 + 255) / 256 + 1;
-    if (half == 0) k_coef_bnd<0><<<nb, 256, 0, s>>>(g, p, kBndAll);
+    if (half == 0) k_coef_bnd<0><<<nb, 256, 0, s>>>(g, p, writes);
     else k_coef_bnd<1><<<nb, 256, 0, s>>>(g, p, writes);
     hyd_kernel_launches_add(1);
 }
