@@ -457,8 +457,12 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         s->phase_ms[k] = 0;
         s->phase_n[k] = 0;
     }
-    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking);
+    // the side stream's work (the first half-step's sediment) has the slack: it runs at a
+    // lower priority than the main chain it runs beside
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    cudaError_t e = cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_lo);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
@@ -846,7 +850,7 @@ static cudaGraphExec_t step_graph(HydSim* s, int mask, int timed = 0) {
     cudaGraph_t graph = nullptr;
     if (cudaStreamEndCapture(s->stream, &graph) != cudaSuccess || !graph) return nullptr;
     cudaGraphExec_t exec = nullptr;
-    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return nullptr;
     const long long after = hyd_kernel_launches_add(0);

@@ -441,8 +441,24 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         const int sn = sg.sn[sI];
         const int r0 = sg.ro[sI];
         const int rel = 2 * (k - f);  // row 2k relative to the segment's first row 2f
-        double ac, cc, dc;
+        // every coefficient the cell may need, loaded at once (the next cell's and f1..f5
+        // are in bounds even where unused: k + 1 <= L + 1 inside the padded line)
+        double ac, cc, dc, an, cn, dn, f1, f2, f3, f5;
         cont(k, ac, cc, dc);
+        cont(k + 1, an, cn, dn);
+        if (DIR == 0) {
+            const size_t t = (size_t)line * g.LT + k;
+            f1 = colT(g, 3)[t];
+            f2 = colT(g, 4)[t];
+            f3 = colT(g, 5)[t];
+            f5 = colT(g, 6)[t];
+        } else {
+            const int pos = base + k * along;
+            f1 = rowC(g, 3)[pos];
+            f2 = rowC(g, 4)[pos];
+            f3 = rowC(g, 5)[pos];
+            f5 = rowC(g, 6)[pos];
+        }
         a2[c] = ac;
         c2[c] = cc;
         d2[c] = dc;
@@ -456,22 +472,6 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         if (Ls <= 1 && k != f) continue;
         const int rm = tR ? rel + 1 : rel;  // the momentum row of this cell
         if (rm > sn) continue;
-        double an, cn, dn;  // the next cell's
-        cont(k + 1, an, cn, dn);
-        const int pos = base + k * along;
-        double f1, f2, f3, f5;  // precomputed by k_coef_bnd (UZ column-major, VZ row-major)
-        if (DIR == 0) {
-            const size_t t = (size_t)line * g.LT + k;
-            f1 = colT(g, 3)[t];
-            f2 = colT(g, 4)[t];
-            f3 = colT(g, 5)[t];
-            f5 = colT(g, 6)[t];
-        } else {
-            f1 = rowC(g, 3)[pos];
-            f2 = rowC(g, 4)[pos];
-            f3 = rowC(g, 5)[pos];
-            f5 = rowC(g, 6)[pos];
-        }
         double ra, rb, rc, rd;
         if (Ls >= 2) {
             if (k == f && b1f) {
