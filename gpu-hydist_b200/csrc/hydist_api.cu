@@ -1133,4 +1133,72 @@ int hyd_launch_count(hyd_handle h, long long* count) {
     return HYD_OK;
 }
 
+// ---- batches of independent reaches (one persistent handle per member)
+
+struct HydBatch {
+    std::vector<hyd_handle> members;
+};
+
+int hyd_batch_create(int count, const HydCaseParams* params, const int* dims, int device, hyd_batch* out) {
+    if (!params || !dims || !out || count < 1) return fail(HYD_EINVAL, "batch: null argument or empty batch");
+    HydBatch* b = new HydBatch();
+    for (int k = 0; k < count; k++) {
+        hyd_handle h = nullptr;
+        const int rc = hyd_create(&params[k], dims[2 * k], dims[2 * k + 1], device, &h);
+        if (rc) {
+            const std::string msg = "batch member " + std::to_string(k) + ": " + hyd_last_error();
+            for (hyd_handle m : b->members) hyd_destroy(m);
+            delete b;
+            return fail(rc, msg);
+        }
+        b->members.push_back(h);
+    }
+    *out = b;
+    return HYD_OK;
+}
+
+int hyd_batch_size(hyd_batch b, int* count) {
+    if (!b || !count) return fail(HYD_EINVAL, "null argument");
+    *count = (int)b->members.size();
+    return HYD_OK;
+}
+
+int hyd_batch_member(hyd_batch b, int k, hyd_handle* h) {
+    if (!b || !h) return fail(HYD_EINVAL, "null argument");
+    if (k < 0 || k >= (int)b->members.size()) return fail(HYD_EINVAL, "batch member index out of range");
+    *h = b->members[k];
+    return HYD_OK;
+}
+
+int hyd_batch_step(hyd_batch b, int nsteps, int sync) {
+    if (!b) return fail(HYD_EINVAL, "null batch");
+    if (nsteps < 0) return fail(HYD_EINVAL, "nsteps < 0");
+    // one step of every member at a time: each member's graphs go to its own stream, so
+    // the device runs the members side by side while the host queues the next round
+    for (int n = 0; n < nsteps; n++) {
+        for (size_t k = 0; k < b->members.size(); k++) {
+            const int rc = hyd_step(b->members[k], 1, 0, nullptr);
+            if (rc) return fail(rc, "batch member " + std::to_string(k) + ": " + hyd_last_error());
+        }
+    }
+    if (sync) {
+        for (size_t k = 0; k < b->members.size(); k++) {
+            const int rc = hyd_synchronize(b->members[k]);
+            if (rc) return fail(rc, "batch member " + std::to_string(k) + ": " + hyd_last_error());
+        }
+    }
+    return HYD_OK;
+}
+
+int hyd_batch_destroy(hyd_batch b) {
+    if (!b) return HYD_OK;
+    int rc = HYD_OK;
+    for (hyd_handle h : b->members) {
+        const int r = hyd_destroy(h);
+        if (r && !rc) rc = r;
+    }
+    delete b;
+    return rc;
+}
+
 }  // extern "C"

@@ -9,7 +9,8 @@ gathered on rank 0.
 
     partition(costs, world)        -> per-rank lists of reach indices (largest first,
                                       each to the least loaded rank)
-    Ensemble(cases, rank, world)   -> the rank's reaches; .step(n), .cell_updates(n)
+    Ensemble(cases, rank, world)   -> the rank's reaches (one library batch); .step(n),
+                                      .cell_updates(n)
     max_over_ranks(x)              -> max of a host float over the process group
 """
 import heapq
@@ -38,35 +39,37 @@ def partition(costs, world):
     return [sorted(v) for v in out]
 
 
-def _default_factory(device):
-    from .lib import Simulation
-
-    def make(case):
-        return Simulation.from_case(case, device=device)
-    return make
-
-
 class Ensemble:
-    """The reaches of one rank.  `factory(case)` builds a stepping object with
-    step(n, sync), synchronize(), get(name) and close() (default: a library handle on
-    `device`, initialised from the case)."""
+    """The reaches of one rank.  By default they form one library batch on `device`
+    (hyd_batch_*: one handle and stream per reach, stepped side by side); `factory(case)`
+    instead builds one stepping object per reach with step(n, sync), synchronize(),
+    get(name) and close()."""
 
     def __init__(self, cases, rank=0, world=1, device=0, factory=None):
         self.cases = list(cases)
         self.rank, self.world = rank, world
         self.owned = partition([reach_cost(c) for c in self.cases], world)[rank]
-        make = factory if factory is not None else _default_factory(device)
         self.sims = {}
+        self.batch = None
         try:
-            for i in self.owned:
-                self.sims[i] = make(self.cases[i])
+            if factory is None:
+                if self.owned:
+                    from .lib import Batch
+                    self.batch = Batch([self.cases[i] for i in self.owned], device=device)
+                    self.sims = dict(zip(self.owned, self.batch.members))
+            else:
+                for i in self.owned:
+                    self.sims[i] = factory(self.cases[i])
         except Exception:
             self.close()
             raise
 
     def step(self, n=1, sync=True):
-        """Advance every owned reach n steps: all launches are queued first (one stream
-        per reach), then the rank waits for all of them."""
+        """Advance every owned reach n steps (their launches queued on one stream per
+        reach, so the reaches run side by side), then, with sync, wait for all."""
+        if self.batch is not None:
+            self.batch.step(n, sync)
+            return
         for i in self.owned:
             self.sims[i].step(n, sync=False)
         if sync:
@@ -101,8 +104,12 @@ class Ensemble:
         return out
 
     def close(self):
-        for s in self.sims.values():
-            s.close()
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None
+        else:
+            for s in self.sims.values():
+                s.close()
         self.sims = {}
 
 

@@ -59,6 +59,12 @@ def load():
         "hyd_set_timing_phases": (ctypes.c_int, [H, ctypes.c_uint]),
         "hyd_phase_name": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]),
         "hyd_timing_report": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_size_t]),
+        "hyd_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+        "hyd_batch_size": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int)]),
+        "hyd_batch_member": (ctypes.c_int, [H, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+        "hyd_batch_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int]),
+        "hyd_batch_destroy": (ctypes.c_int, [H]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -120,12 +126,24 @@ class Simulation:
     @classmethod
     def from_case(cls, case, device=0, init=True):
         sim = cls(case.params, case.N, case.M, device)
-        for name in ("h", "hsnham", "VISCOIDX", "Fw", "Tsxw", "Tsyw", "u", "v", "z", "FS"):
-            sim.set(name, case.fields[name])
-        sim.set_boundary(case.boundary_type, case.tables, case.cc, case.total_time)
-        if init:
-            sim.init(case.t_start)
+        sim.load_case(case, init)
         return sim
+
+    @classmethod
+    def _member(cls, lib, handle, params, N, M):
+        """A view of a batch member's handle (owned by the batch, not closed by the view)."""
+        sim = cls.__new__(cls)
+        sim.lib, sim.h, sim.N, sim.M, sim._p = lib, handle, int(N), int(M), params.copy()
+        sim._owned = False
+        return sim
+
+    def load_case(self, case, init=True):
+        """Fields and boundary tables of `case` (and hyd_init unless init is False)."""
+        for name in ("h", "hsnham", "VISCOIDX", "Fw", "Tsxw", "Tsyw", "u", "v", "z", "FS"):
+            self.set(name, case.fields[name])
+        self.set_boundary(case.boundary_type, case.tables, case.cc, case.total_time)
+        if init:
+            self.init(case.t_start)
 
     def set(self, name, arr):
         shape, dt = field_shape(name, self.N, self.M)
@@ -236,9 +254,51 @@ class Simulation:
         return out
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self, "_owned", True):
             self.lib.hyd_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent reaches on one device (hyd_batch_*): member k is a Simulation view of
+    the batch's handle k; step() advances all of them, side by side on the device."""
+
+    def __init__(self, cases, device=0, init=True):
+        lib = load()
+        self.lib = lib
+        n = len(cases)
+        params = (HydCaseParams * n)(*[c.params.copy() for c in cases])
+        dims = (ctypes.c_int * (2 * n))(*[v for c in cases for v in (c.N, c.M)])
+        b = ctypes.c_void_p()
+        _check(lib.hyd_batch_create(n, ctypes.cast(params, ctypes.c_void_p), ctypes.cast(dims, ctypes.c_void_p),
+                                    int(device), ctypes.byref(b)))
+        self.b = b
+        self.members = []
+        for k, c in enumerate(cases):
+            h = ctypes.c_void_p()
+            _check(lib.hyd_batch_member(b, k, ctypes.byref(h)))
+            self.members.append(Simulation._member(lib, h, c.params, c.N, c.M))
+        for sim, c in zip(self.members, cases):
+            sim.load_case(c, init)
+
+    def step(self, n=1, sync=True):
+        _check(self.lib.hyd_batch_step(self.b, int(n), 1 if sync else 0))
+
+    def synchronize(self):
+        for s in self.members:
+            s.synchronize()
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.hyd_batch_destroy(self.b)
+            self.b = None
+            self.members = []
 
     def __del__(self):
         try:

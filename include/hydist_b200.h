@@ -85,6 +85,7 @@ void hyd_params_default(HydCaseParams* p);
 void hyd_params_derive(HydCaseParams* p);
 
 typedef struct HydSim* hyd_handle;
+typedef struct HydBatch* hyd_batch;
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* hyd_last_error(void);
@@ -243,6 +244,21 @@ int hyd_set_timing(hyd_handle h, int enable);
 int hyd_set_timing_phases(hyd_handle h, unsigned int phase_mask);
 int hyd_phase_name(int phase, const char** name);
 int hyd_timing_report(hyd_handle h, char* buf, size_t buflen);
+
+/* Batches of independent reaches (the batched variant of the operator surface: a config-3
+ * ensemble on one device).  hyd_batch_create makes `count` handles on `device`, member k
+ * with params[k] and dims[2k] x dims[2k+1] cells; each member is then set up through its
+ * own handle (hyd_batch_member: fields, boundary tables, hyd_init) like a single reach.
+ * hyd_batch_step advances every member nsteps steps, one step of every member at a time;
+ * the members' launches go to their own streams, so they run side by side on the device.
+ * With sync, it waits for all members and reports the first device status error.  The
+ * handles belong to the batch: hyd_batch_destroy frees them (do not hyd_destroy them).
+ * No reference counterpart (the reference runs one reach per process). */
+int hyd_batch_create(int count, const HydCaseParams* params, const int* dims, int device, hyd_batch* out);
+int hyd_batch_size(hyd_batch b, int* count);
+int hyd_batch_member(hyd_batch b, int k, hyd_handle* h);
+int hyd_batch_step(hyd_batch b, int nsteps, int sync);
+int hyd_batch_destroy(hyd_batch b);
 
 #ifdef __cplusplus
 }
