@@ -76,6 +76,13 @@ struct HydSim {
     std::vector<void*> extra;
     double t;
     int have_boundary;
+    int bnd_nseg[4];  // segments per edge of the boundary tables
+    // the eight tables in one device block (bc 0-3, cc 0-3), a pinned staging copy for
+    // hyd_update_boundary and the event of its last upload
+    double* bnd_block;
+    double* bnd_stage;
+    size_t bnd_doubles;
+    cudaEvent_t ev_bnd;
     int initialized;
     int solver;
     int start_idx, end_idx;
@@ -103,6 +110,11 @@ struct HydSim {
     // second stream for work that runs beside the main chain (forked and joined by events)
     cudaStream_t side;
     cudaEvent_t ev_fork, ev_join;
+    // asynchronous field reads: two device snapshots, copied out on their own stream
+    cudaStream_t copy_stream;
+    cudaEvent_t ev_snap, ev_copied[2];
+    void* snap[2];
+    int snap_i;
     cudaGraphExec_t graph[8];
     long long graph_kernels[8];
     // timing with graphs: one graph per variant with the phase events captured in it
@@ -414,6 +426,16 @@ static void release(HydSim* s) {
     cudaFree(s->arena);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+    cudaFree(s->snap[0]);
+    cudaFree(s->snap[1]);
+    if (s->ev_snap) cudaEventDestroy(s->ev_snap);
+    if (s->ev_copied[0]) cudaEventDestroy(s->ev_copied[0]);
+    if (s->ev_copied[1]) cudaEventDestroy(s->ev_copied[1]);
+    if (s->ev_bnd) cudaEventDestroy(s->ev_bnd);
+    cudaFree(s->bnd_block);
+    if (s->bnd_stage) cudaFreeHost(s->bnd_stage);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->side) cudaStreamDestroy(s->side);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -465,6 +487,11 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_lo);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_snap, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_copied[0], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_copied[1], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_bnd, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         release(s);
         return fail(HYD_ECUDA, std::string("streams: ") + cudaGetErrorString(e));
@@ -663,6 +690,36 @@ int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count) {
     return HYD_OK;
 }
 
+int hyd_get_field_async(hyd_handle h, const char* name, void* host, size_t count) {
+    if (!h || !name || !host) return fail(HYD_EINVAL, "null argument");
+    const FieldDesc* f = find_field(name);
+    if (!f) return fail(HYD_EINVAL, std::string("unknown field ") + name);
+    if (f->kind != 0) return fail(HYD_EINVAL, std::string("asynchronous reads take grid fields of doubles: ") + name);
+    if (count != field_count(h, f->kind)) return fail(HYD_EINVAL, std::string("wrong element count for ") + name);
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t row = (size_t)(h->M + 3) * sizeof(double);
+    const int i = h->snap_i;
+    if (!h->snap[i]) CUDA_TRY(cudaMalloc(&h->snap[i], row * (h->N + 3)));
+    // the read two calls back must have left this snapshot before it is overwritten
+    CUDA_TRY(cudaEventSynchronize(h->ev_copied[i]));
+    // packed on the device (the host copy is then one contiguous transfer)
+    launch_pack_rows((const double*)member(h, f), h->pitch, (double*)h->snap[i], h->N + 3, h->M + 3, h->stream);
+    CUDA_TRY(cudaEventRecord(h->ev_snap, h->stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev_snap, 0));
+    CUDA_TRY(cudaMemcpyAsync(host, h->snap[i], row * (h->N + 3), cudaMemcpyDeviceToHost, h->copy_stream));
+    CUDA_TRY(cudaEventRecord(h->ev_copied[i], h->copy_stream));
+    h->snap_i = i ^ 1;
+    return HYD_OK;
+}
+
+int hyd_wait_fields(hyd_handle h) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaEventSynchronize(h->ev_copied[0]));
+    CUDA_TRY(cudaEventSynchronize(h->ev_copied[1]));
+    return HYD_OK;
+}
+
 int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const* tables, const double* const* cc,
                      const int* nseg, int total_time) {
     if (!h || !boundary_type || !tables || !cc || !nseg) return fail(HYD_EINVAL, "null argument");
@@ -680,28 +737,64 @@ int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const
     }
     CUDA_TRY(cudaMemcpyAsync(h->g.bienQ, bienQ, sizeof bienQ, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(cudaMemcpyAsync(h->g.btype, boundary_type, 4 * HYD_SEGL * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    // one block for the eight tables (each padded as the reference's reads allow: an edge
+    // without segments still gets one zero row, and two spare values)
+    size_t off[8], total = 0;
+    for (int q = 0; q < 8; q++) {
+        const int e = q & 3;
+        off[q] = total;
+        total += ((size_t)(nseg[e] > 0 ? nseg[e] : 1) * total_time + 2 + 31) / 32 * 32;
+    }
+    for (int e = 0; e < 4; e++)
+        if (nseg[e] > 0 && (!tables[e] || !cc[e])) return fail(HYD_EINVAL, "missing boundary table");
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->bnd_block) {
+        cudaFree(h->bnd_block);
+        h->bnd_block = nullptr;
+    }
+    if (h->bnd_stage) {
+        cudaFreeHost(h->bnd_stage);
+        h->bnd_stage = nullptr;
+    }
+    CUDA_TRY(cudaMalloc(&h->bnd_block, total * sizeof(double)));
+    CUDA_TRY(cudaMallocHost(&h->bnd_stage, total * sizeof(double)));
+    h->bnd_doubles = total;
+    memset(h->bnd_stage, 0, total * sizeof(double));
     for (int e = 0; e < 4; e++) {
-        const size_t n = (size_t)(nseg[e] > 0 ? nseg[e] : 1) * total_time + 2;
-        void* q = nullptr;
-        CUDA_TRY(cudaMalloc(&q, n * 8));
-        h->extra.push_back(q);
-        CUDA_TRY(cudaMemsetAsync(q, 0, n * 8, h->stream));
-        void* q2 = nullptr;
-        CUDA_TRY(cudaMalloc(&q2, n * 8));
-        h->extra.push_back(q2);
-        CUDA_TRY(cudaMemsetAsync(q2, 0, n * 8, h->stream));
-        if (nseg[e] > 0) {
-            if (!tables[e] || !cc[e]) return fail(HYD_EINVAL, "missing boundary table");
-            CUDA_TRY(cudaMemcpyAsync(q, tables[e], (size_t)nseg[e] * total_time * 8, cudaMemcpyHostToDevice, h->stream));
-            CUDA_TRY(cudaMemcpyAsync(q2, cc[e], (size_t)nseg[e] * total_time * 8, cudaMemcpyHostToDevice, h->stream));
-        }
-        h->g.bc[e] = (double*)q;
-        h->g.cc[e] = (double*)q2;
+        if (nseg[e] <= 0) continue;
+        memcpy(h->bnd_stage + off[e], tables[e], (size_t)nseg[e] * total_time * 8);
+        memcpy(h->bnd_stage + off[4 + e], cc[e], (size_t)nseg[e] * total_time * 8);
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->bnd_block, h->bnd_stage, total * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    for (int e = 0; e < 4; e++) {
+        h->g.bc[e] = h->bnd_block + off[e];
+        h->g.cc[e] = h->bnd_block + off[4 + e];
     }
     h->g.total_time = total_time;
+    for (int e = 0; e < 4; e++) h->bnd_nseg[e] = nseg[e];
     h->have_boundary = 1;
     drop_graphs(h);
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HYD_OK;
+}
+
+int hyd_update_boundary(hyd_handle h, const double* const* tables, const double* const* cc) {
+    if (!h || !tables || !cc) return fail(HYD_EINVAL, "null argument");
+    if (!h->have_boundary) return fail(HYD_ESTATE, "hyd_set_boundary must precede hyd_update_boundary");
+    for (int e = 0; e < 4; e++)
+        if (h->bnd_nseg[e] > 0 && (!tables[e] || !cc[e])) return fail(HYD_EINVAL, "missing boundary table");
+    CUDA_TRY(cudaSetDevice(h->device));
+    // the staging copy is reused: the previous upload must have left it
+    CUDA_TRY(cudaEventSynchronize(h->ev_bnd));
+    for (int e = 0; e < 4; e++) {
+        if (h->bnd_nseg[e] <= 0) continue;
+        const size_t n = (size_t)h->bnd_nseg[e] * h->g.total_time;
+        memcpy(h->bnd_stage + (h->g.bc[e] - h->bnd_block), tables[e], n * 8);
+        memcpy(h->bnd_stage + (h->g.cc[e] - h->bnd_block), cc[e], n * 8);
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->bnd_block, h->bnd_stage, h->bnd_doubles * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    CUDA_TRY(cudaEventRecord(h->ev_bnd, h->stream));
     return HYD_OK;
 }
 

@@ -178,6 +178,8 @@ void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_spans(const DevGrid& g, cudaStream_t s);
+// rows x cols doubles of a pitched array into a packed one
+void launch_pack_rows(const double* src, int pitch, double* dst, int rows, int cols, cudaStream_t s);
 void clear_rescan_lists(const DevGrid& g, cudaStream_t s);
 // 1 if a and b differ outside the extended spans on [i0, i1] x [j0, j1], 0 if not, -1 on error
 int outside_differs(const DevGrid& g, const double* a, const double* b, int i0, int i1, int j0, int j1, int* dflag,

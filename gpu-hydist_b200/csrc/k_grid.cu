@@ -1422,6 +1422,17 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
 
 }  // namespace
 
+// Pitched (N+3) x pitch rows into a packed (N+3) x (M+3) array (a field snapshot for an
+// asynchronous host read).
+__global__ void k_pack_rows(const double* __restrict__ src, int pitch, double* __restrict__ dst, int rows,
+                            int cols) {
+    const long long n = (long long)rows * cols;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(q / cols), c = (int)(q - (long long)r * cols);
+        dst[q] = src[(long long)r * pitch + c];
+    }
+}
+
 // ------------------------------------------------------------------ host wrappers
 
 namespace {
@@ -1653,4 +1664,9 @@ void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, 
     k_qb<<<grid2d(g.M - 1, g.N - 1, b), b, 0, s>>>(g, p);
     if (endidx > startidx) k_bedload<<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
     hyd_kernel_launches_add(2);
+}
+
+void launch_pack_rows(const double* src, int pitch, double* dst, int rows, int cols, cudaStream_t s) {
+    k_pack_rows<<<4 * 148, 256, 0, s>>>(src, pitch, dst, rows, cols);
+    hyd_kernel_launches_add(1);
 }

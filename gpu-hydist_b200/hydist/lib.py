@@ -43,6 +43,9 @@ def load():
         "hyd_set_boundary": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_int]),
         "hyd_init": (ctypes.c_int, [H, ctypes.c_double]),
+        "hyd_get_field_async": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]),
+        "hyd_wait_fields": (ctypes.c_int, [H]),
+        "hyd_update_boundary": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
         "hyd_init_pickup": (ctypes.c_int, [H, ctypes.c_double]),
         "hyd_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
         "hyd_get_time": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double)]),
@@ -167,6 +170,27 @@ class Simulation:
         cp = (PD * 4)(*[t.ctypes.data_as(PD) for t in ccs])
         ns = (ctypes.c_int * 4)(*[int(t.shape[0]) for t in tabs])
         _check(self.lib.hyd_set_boundary(self.h, bt.ctypes.data, tp, cp, ns, int(total_time)))
+
+    def get_async(self, name, out):
+        """Start reading a grid field of doubles into `out` (a C-contiguous (N+3)x(M+3)
+        float64 array, ideally a view of pinned memory) while later steps run; complete
+        after wait_fields() or once the second get_async() after it has returned."""
+        shape, dt = field_shape(name, self.N, self.M)
+        if out.shape != shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("%s: expected a C-contiguous float64 array of shape %s" % (name, shape))
+        _check(self.lib.hyd_get_field_async(self.h, name.encode(), out.ctypes.data, out.size))
+
+    def wait_fields(self):
+        _check(self.lib.hyd_wait_fields(self.h))
+
+    def update_boundary(self, tables, cc):
+        """New values for the boundary tables of set_boundary (same shapes); uploaded in
+        order with the steps (the arrays are free again on return)."""
+        PD = ctypes.POINTER(ctypes.c_double)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in list(tables) + list(cc)]
+        tp = (PD * 4)(*[a.ctypes.data_as(PD) for a in arrs[:4]])
+        cp = (PD * 4)(*[a.ctypes.data_as(PD) for a in arrs[4:]])
+        _check(self.lib.hyd_update_boundary(self.h, tp, cp))
 
     def set_params(self, params):
         self._p = params.copy()

@@ -125,6 +125,19 @@ int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count
 int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count);
 
 /*
+ * Asynchronous read of a grid field of doubles ((N+3)x(M+3), e.g. "z" after a step): the
+ * field is snapshotted on the device in order with the steps (two snapshots in turn),
+ * and the snapshot is copied to `host` on a separate stream while later steps run, the
+ * copies in call order.  `host` should be pinned (cudaHostAlloc / a pinned tensor) for
+ * the copy to overlap, and must stay valid and untouched until the read is complete:
+ * once hyd_wait_fields returns, or once the second hyd_get_field_async call after it has
+ * returned.  No reference counterpart (the reference copies its output fields
+ * synchronously, Engine.py:377-468).
+ */
+int hyd_get_field_async(hyd_handle h, const char* name, void* host, size_t count);
+int hyd_wait_fields(hyd_handle h);
+
+/*
  * Boundary tables for all four edges (Global_Variables.py:30-66):
  *   boundary_type: 4 x HYD_SEGMENT_LIMIT int32 (0 wall, 1 stage Z, 2 discharge Q);
  *   tables[e]:     nseg[e] x total_time hourly values of Q or Z (bc_up..bc_right);
@@ -134,6 +147,17 @@ int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count);
  */
 int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const* tables,
                      const double* const* cc, const int* nseg, int total_time);
+
+/*
+ * New values for the boundary tables set by hyd_set_boundary, of the same shapes
+ * (tables[e], cc[e]: nseg[e] x total_time; edges with nseg 0 are skipped): a host that
+ * drives the forcing as the run goes (a coupled model updating discharges, levels or
+ * inflow concentrations) sends them here between steps.  The values are copied into the
+ * library's pinned staging block at once (the caller's arrays are free on return) and
+ * uploaded in one transfer queued on the handle's stream, in order with the steps.  No
+ * reference counterpart (the reference loads its tables once, Global_Variables.py:39-47).
+ */
+int hyd_update_boundary(hyd_handle h, const double* const* tables, const double* const* cc);
 
 /*
  * One-time initialisation (rep.py:126-139): Onetime_init, the wet-segment scans

@@ -59,3 +59,47 @@ def test_step_argument_errors():
         a.step(10 ** 9)   # beyond the boundary tables
     with pytest.raises((HydError, ValueError)):
         a.set("z", np.zeros((3, 3)))
+
+
+def test_async_level_reads_match_sync_reads():
+    """hyd_get_field_async snapshots the field in order with the steps: each buffer holds
+    the levels of the step it followed, although later steps run during the copies."""
+    from hydist.lib import Simulation
+    c = _config2()
+    a = Simulation.from_case(c)
+    b = Simulation.from_case(c)
+    shape = (c.N + 3, c.M + 3)
+    bufs = [np.empty(shape) for _ in range(5)]
+    want = []
+    for k in range(5):
+        a.step(3, sync=False)
+        a.get_async("z", bufs[k])
+        b.step(3)
+        want.append(b.get("z"))
+        if k >= 2:  # two later calls have returned: the read of call k - 2 is complete
+            assert np.array_equal(bufs[k - 2], want[k - 2]), k - 2
+    a.wait_fields()
+    for k in range(5):
+        assert np.array_equal(bufs[k], want[k]), k
+    with pytest.raises(Exception):
+        a.get_async("khouot", np.empty(shape))
+    a.close()
+    b.close()
+
+
+def test_update_boundary_changes_forcing():
+    """Tables sent between steps drive the following steps like tables set at the start."""
+    from hydist.lib import Simulation
+    c = _config2()
+    tabs2 = [t * 1.1 for t in c.tables]
+    a = Simulation.from_case(c)
+    a.update_boundary(tabs2, c.cc)
+    a.step(20)
+    c2 = _config2()
+    c2.tables = tabs2
+    b = Simulation.from_case(c2)
+    b.step(20)
+    for f in ("z", "u", "v"):
+        assert np.array_equal(a.get(f), b.get(f)), f
+    a.close()
+    b.close()
