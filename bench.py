@@ -72,7 +72,7 @@ SIDE_PHASES = ("coef_fsj", "fs_sweep_j")
 # fourth step (t = 4 s) of python bench.py --spinup 0 --steps 3 --warmup 3 --no-cpu-baseline
 # (ncu -k regex:k_hydro_sweep -s 6 -c 2: the 7th launch of the sweep kernel, the UZ sweep).
 NCU_TRAFFIC = {
-    "sweep_uz": (2174208, 30650),
+    "sweep_uz": (2192640, 30650),
 }
 
 
