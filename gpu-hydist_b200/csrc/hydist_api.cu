@@ -1244,6 +1244,8 @@ int hyd_batch_create(int count, const HydCaseParams* params, const int* dims, in
             delete b;
             return fail(rc, msg);
         }
+        // the members run side by side: sweeps sized by their lines, not the device
+        sweep_plan_throughput(h->N, h->M, &h->plan);
         b->members.push_back(h);
     }
     *out = b;

@@ -160,6 +160,10 @@ struct SweepPlan {
     size_t scratch_doubles;            // global scratch to allocate
 };
 cudaError_t sweep_plan(int N, int M, SweepPlan* sp);
+// Throughput sizing for reaches that share the device with others: as many sweep CTAs as
+// give every line of the longer direction its own warp in one pass (each CTA sweeps one
+// line per warp), instead of one CTA per SM.
+void sweep_plan_throughput(int N, int M, SweepPlan* sp);
 cudaError_t grid_setup(int N, int M);
 void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
                      int solver, double* scratch, cudaStream_t s);

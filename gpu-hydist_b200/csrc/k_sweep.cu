@@ -986,6 +986,12 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
     return cudaSuccess;
 }
 
+void sweep_plan_throughput(int N, int M, SweepPlan* sp) {
+    const int L = N > M ? N : M;
+    const int g = (L + 3 + kWL - 1) / kWL;
+    if (sp->long_grid > g) sp->long_grid = g;
+}
+
 namespace {
 void hydro_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,
                  int solver, double* scratch, cudaStream_t s) {
