@@ -3,7 +3,8 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload (config 2): 1048 x 980 cells, dx = dy = 5 m, dt = 1 s, FP64 hydraulics with the
-suspended-sediment ADI and the Exner update active.  A "step" is one full ADI step (two
+suspended-sediment ADI and the Exner update active (--workload config4: the 4096 x 2048
+reach at 2.5 m, same physics).  A "step" is one full ADI step (two
 half-steps) of the whole grid; one cell-update is one interior cell advanced one step.
 The state is first spun up (untimed) to t = 3590 s, where sediment is active and the
 Exner update fires every 3600 s.  The span-limited kernels touch only the cells near
@@ -36,6 +37,13 @@ sys.path[:0] = [os.path.join(ROOT, "gpu-hydist_b200"), os.path.join(ROOT, "oracl
 
 SPINUP_STEPS = 3590
 METRIC = "ADI cell-updates/s"
+# --workload: name -> (case builder in hydist.cases, description, data)
+WORKLOADS = {
+    "config2": ("config2_case", "config2_meander 1048x980 dx=5m dt=1s FP64 hydraulics+sediment+Exner",
+                "synthetic (seeded meandering reach, config-2 shape)"),
+    "config4": ("config4_case", "config4_large_meander 4096x2048 dx=2.5m dt=1s FP64 hydraulics+sediment+Exner",
+                "synthetic (seeded meandering reach, config-4 shape)"),
+}
 
 # algorithmic bytes per launch of each phase, per unit: cells of the extended spans (the
 # cells the elementwise kernels visit once the grid is up to date, "span"), cells of the
@@ -72,7 +80,7 @@ SIDE_PHASES = ("coef_fsj", "fs_sweep_j")
 # fourth step (t = 4 s) of python bench.py --spinup 0 --steps 3 --warmup 3 --no-cpu-baseline
 # (ncu -k regex:k_hydro_sweep -s 6 -c 2: the 7th launch of the sweep kernel, the UZ sweep).
 NCU_TRAFFIC = {
-    "sweep_uz": (2192640, 30650),
+    "config2": {"sweep_uz": (2192640, 30650)},
 }
 
 
@@ -195,7 +203,7 @@ def run_ours(args, rank, world, local_rank):
     from hydist.lib import Simulation
 
     torch.cuda.set_device(local_rank)
-    case = cases.config2_case()
+    case = getattr(cases, WORKLOADS[args.workload][0])()
     N, M = case.N, case.M
     cells = N * M
     sim = Simulation.from_case(case, device=local_rank)
@@ -277,8 +285,9 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = load_peaks()
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
     traffic = None
-    if dom_name in NCU_TRAFFIC:
-        tb, tw = NCU_TRAFFIC[dom_name]
+    captured = NCU_TRAFFIC.get(args.workload, {})
+    if dom_name in captured:
+        tb, tw = captured[dom_name]
         traffic = int(round(tb * units["wet"] / tw))
     phases = {k: {"launches": n, "ms_per_launch": t / n, "share": t / total_ms} for k, (n, t) in rep.items()}
 
@@ -363,16 +372,16 @@ def run_ours(args, rank, world, local_rank):
             n_cpu, el = cpu_port_sample(case, lambda f: snap[f], st_t, hmax, budget_s=args.cpu_seconds)
             cpu = {"value": cells * n_cpu / el, "unit": "cell-updates/s", "cores": os.cpu_count(),
                    "kind": "port",
-                   "sample": "%d ADI steps of the 1048x980 reach from t=%.0f s (the GPU state), oracle port "
-                             "(OpenMP, %d threads), %.1f s wall" % (n_cpu, st_t, os.cpu_count(), el)}
+                   "sample": "%d ADI steps of the %dx%d reach from t=%.0f s (the GPU state), oracle port "
+                             "(OpenMP, %d threads), %.1f s wall" % (n_cpu, N, M, st_t, os.cpu_count(), el)}
         clocks = clk.summary()
         result = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded meandering reach, config-2 shape)",
-            "config": {"workload": "config2_meander 1048x980 dx=5m dt=1s FP64 hydraulics+sediment+Exner, "
-                                   "t=%d..%d s" % (args.spinup + args.warmup, args.spinup + args.warmup + args.steps),
+            "data": WORKLOADS[args.workload][2],
+            "config": {"workload": "%s, t=%d..%d s" % (WORKLOADS[args.workload][1], args.spinup + args.warmup,
+                                                        args.spinup + args.warmup + args.steps),
                        "grid": [N, M], "cells": cells, "wet_cells": wet,
                        "parallelism": "replicas%d" % world if world > 1 else "single",
                        "core_cells": core, "span_cells": span,
@@ -409,7 +418,7 @@ def run_reference(args, rank):
     import numpy as np
     import oracle
     from hydist import cases
-    case = cases.config2_case()
+    case = getattr(cases, WORKLOADS[args.workload][0])()
     cells = case.N * case.M
     ora = oracle.OracleSim(case, threads=os.cpu_count() or 1)
     ora.init()
@@ -434,8 +443,8 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": 0,
         "steps": n, "warmup": args.warmup, "ms_per_step": el / n * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded meandering reach, config-2 shape)",
-        "config": {"workload": "config2_meander 1048x980 dx=5m dt=1s FP64 hydraulics+sediment+Exner",
+        "data": WORKLOADS[args.workload][2],
+        "config": {"workload": WORKLOADS[args.workload][1],
                    "grid": [case.N, case.M], "cells": cells},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": "%d ADI steps after %d spin-up steps, oracle port (OpenMP)" % (n, spin)},
@@ -454,6 +463,8 @@ def main():
     ap.add_argument("--spinup", type=int, default=SPINUP_STEPS,
                     help="untimed steps before the warm-up (default: to t = 3590 s, sediment active)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS),
+                    help="config2 (the default: the 1048x980 reach) or config4 (the 4096x2048 reach)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

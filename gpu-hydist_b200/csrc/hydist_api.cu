@@ -569,7 +569,12 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         return fail(HYD_ENOMEM, "arena layout overflow");
     }
     s->dp = make_dev_params(s->P);
-    e = sweep_plan(N, M, &s->plan);
+    {
+        // HYD_SWEEP_ROWS caps the rows a long line keeps in shared memory, so that tests can
+        // send lines of a moderate grid through the global-scratch sweeps
+        const char* rv = getenv("HYD_SWEEP_ROWS");
+        e = sweep_plan(N, M, &s->plan, rv ? atoi(rv) : 0);
+    }
     if (e == cudaSuccess) e = grid_setup(N, M);
     if (e != cudaSuccess) {
         release(s);

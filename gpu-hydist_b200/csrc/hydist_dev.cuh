@@ -153,16 +153,19 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
 // Launch shapes of the sweeps for one grid (k_sweep.cu).
 struct SweepPlan {
     size_t smem_lines, smem_fs_lines;  // dynamic shared memory of the hydrodynamic / sediment sweeps
-    int RB, CB, RBf;                   // rows / cells of a long line held in shared memory
-    int RG, CG, RGf;                   // rows / cells of a CTA's global scratch region
+    int RB, RBf;                       // rows of a long line held in shared memory
+    int RG, RGf;                       // rows of a CTA's global scratch region
     int long_grid;                     // CTAs of the sweeps
     int need_global;                   // some line may exceed shared memory
+    int wide;                          // warps sweep every line their slice holds (throughput sizing)
     size_t scratch_doubles;            // global scratch to allocate
 };
-cudaError_t sweep_plan(int N, int M, SweepPlan* sp);
+// max_rows > 0: at most that many rows of a long line in shared memory (0: as many as fit)
+cudaError_t sweep_plan(int N, int M, SweepPlan* sp, int max_rows);
 // Throughput sizing for reaches that share the device with others: as many sweep CTAs as
 // give every line of the longer direction its own warp in one pass (each CTA sweeps one
-// line per warp), instead of one CTA per SM.
+// line per warp), instead of one CTA per SM, and every line a warp's slice holds swept
+// by its warp.
 void sweep_plan_throughput(int N, int M, SweepPlan* sp);
 cudaError_t grid_setup(int N, int M);
 void launch_sweep_uz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int startidx, int endidx,

@@ -7,7 +7,8 @@
 // Only the wet segments of the line are touched: their cells and their tridiagonal rows
 // are packed one segment after another, so a line with a few wet cells costs a few rows
 // however long it is.
-//   A  continuity coefficients a2, c2, d2 of every wet cell
+//   A  continuity coefficients a2, c2, d2 of every wet cell (those of the segment ends
+//      kept for D)
 //   B  momentum coefficients and the interleaved rows of every segment's system
 //   C  all segments of the line solved as one block-decoupled tridiagonal system by a
 //      partitioned method: each thread eliminates a chunk of rows, the chunk-end
@@ -18,8 +19,10 @@
 // One persistent kernel per sweep: a 512-thread CTA per SM takes every G-th line, one
 // per warp.  A short line (at most 3 rows per lane) is swept by its warp alone; a long
 // line by the whole CTA in shared memory sized for the longest line the grid can hold (a
-// global scratch region per CTA beyond that).  The solve is always one warp's: lanes
-// eliminate chunks of rows, the chunk ends are solved by shuffle-only cyclic reduction.
+// global scratch region per CTA beyond that).  A short line's solve is its warp's: lanes
+// eliminate chunks of rows, the chunk ends are solved by shuffle-only cyclic reduction; a
+// long line's adds a level (up to 256 threads eliminate chunks, one warp solves the
+// chunk-end system as above).
 // In the column sweeps the cell-local coefficients come precomputed, stored column-major
 // so that a column reads them contiguously (k_coef_bnd<0>, k_coef_fsj).
 #include <cuda_runtime.h>
@@ -32,11 +35,20 @@ namespace {
 
 constexpr int kTL = 512;         // threads of a sweep CTA
 constexpr int kWL = kTL / 32;    // lines per group (one per warp)
-constexpr int kRowW = 96;        // rows of a warp-tier line (3 per lane)
-constexpr int kCellW = 48;       // cells of a warp-tier hydrodynamic line
-constexpr int kRowWf = 64;       // rows of a warp-tier sediment line
-constexpr int kWarpHydro = 4 * kRowW + 3 * kCellW;  // doubles per warp
+// A warp's shared-memory slice holds kRowW rows (9 per lane).  Which lines a warp sweeps
+// alone is chosen per launch: with at most one group of lines per CTA, lines of at most
+// kRowShort rows (kRowShortF for sediment), the rest by the whole CTA (a long line then
+// costs the CTA less time than a warp would take); with more lines than that, every line
+// that fits the slice, so that a CTA's many medium lines run side by side.
+constexpr int kRowW = 288;
+constexpr int kRowShort = 96;
+constexpr int kRowShortF = 64;
+// continuity coefficients (a, c, d) of the first and last cell of every segment of a
+// hydrodynamic line, kept for the extraction: 6 doubles per segment
+constexpr int kEnds = 6 * HYD_SEGL;
+constexpr int kWarpHydro = 4 * kRowW + kEnds;  // doubles per warp
 constexpr int kWarpFs = 4 * kRowW;
+static_assert(kRowW % 32 == 0 && (kRowW / 32) % 2 == 1, "a warp solve pads R <= kRowW rows to 32 chunk_len(R, 32) <= kRowW");
 
 // A group of threads that sweeps one line: a warp, or a whole CTA for a long line.
 // WarpG::exchange() gives lane t the values v of lanes t - h (lo) and t + h (hi).
@@ -389,11 +401,11 @@ __device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p
 }
 
 // Phases A-D of one line by group G.  Rows A, B, Cc, D hold at least pl.t1 * pl.m
-// entries, cells a2, c2, d2 at least sg.C; red: the two-level solve's reduced rows.
+// entries, ends kEnds; red: the two-level solve's reduced rows.
 template <int DIR, int SOLVER, class G>
 __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p, int line, const LineShared& sg,
-                                           double* A, double* B, double* Cc, double* D, double* a2, double* c2,
-                                           double* d2, double* red, SolvePlan pl) {
+                                           double* A, double* B, double* Cc, double* D, double* ends, double* red,
+                                           SolvePlan pl) {
     constexpr int T = G::size;
     const int tid = G::rank();
     const int N = g.N, M = g.M, P = g.P;
@@ -409,8 +421,8 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
 
     // ---- A + B1, one pass over the cells: the continuity coefficients of the cell and of
     // the next one (preindex, UVZSolver_multithread.cu:402-406 / 345-349), the momentum
-    // coefficients (preindex f1..f5, _calculate_abcd 409-466) and the rows.  The cell's own
-    // continuity coefficients are kept for the extraction.
+    // coefficients (preindex f1..f5, _calculate_abcd 409-466) and the rows.  The continuity
+    // coefficients of each segment's first and last cell are kept for the extraction.
     auto cont = [&](int k, double& a, double& c, double& d) {
         if (DIR == 0) {
             const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_bnd<0>
@@ -459,9 +471,16 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
             f3 = rowC(g, 5)[pos];
             f5 = rowC(g, 6)[pos];
         }
-        a2[c] = ac;
-        c2[c] = cc;
-        d2[c] = dc;
+        if (k == f) {
+            ends[6 * sI] = ac;
+            ends[6 * sI + 1] = cc;
+            ends[6 * sI + 2] = dc;
+        }
+        if (k == l) {
+            ends[6 * sI + 3] = ac;
+            ends[6 * sI + 4] = cc;
+            ends[6 * sI + 5] = dc;
+        }
         if (tR && rel <= sn) {
             A[r0 + rel] = ac;
             B[r0 + rel] = 1.0;
@@ -555,7 +574,7 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
             } else if (k == f) {
                 const double tv = x[r0 + 2 * f];
                 tvel[pos] = tv;
-                tvel[pos - along] = (d2[c] - g.t_z[pos] - c2[c] * tv) / a2[c];
+                tvel[pos - along] = (ends[6 * sI + 2] - g.t_z[pos] - ends[6 * sI + 1] * tv) / ends[6 * sI];
             } else {
                 g.t_z[pos] = x[r0 + 2 * k - 1];
                 tvel[pos] = x[r0 + 2 * k];
@@ -572,7 +591,7 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
                 double tprev;
                 if (l > f) tprev = (b1f || qfirst) ? x[r0 + 2 * l - 1] : x[r0 + 2 * l - 2];
                 else tprev = tvel[pos - along];
-                tvel[pos] = (d2[c] - a2[c] * tprev - g.t_z[pos]) / c2[c];
+                tvel[pos] = (ends[6 * sI + 5] - ends[6 * sI + 3] * tprev - g.t_z[pos]) / ends[6 * sI + 4];
             }
         }
     }
@@ -580,15 +599,15 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
 
 // Fused sweep of one direction.  CTA b takes lines b, b + G, b + 2G, ... (G = gridDim.x)
 // in groups of 16, one line per warp.  Every warp sets its line up; a warp whose line is
-// short (at most kRowW rows, kCellW cells) sweeps it alone in its own slice of shared
-// memory; then the whole CTA sweeps the group's long lines one after another in the full
-// shared memory (RB rows, CB cells; a CTA's region of global scratch beyond that).
+// short (at most roww rows) sweeps it alone in its own slice of shared memory; then the
+// whole CTA sweeps the group's long lines one after another in the full shared memory
+// (RB rows; a CTA's region of global scratch beyond that).
 // Adjacent long lines (a wet band) fall on different CTAs.  Warps with nothing to sweep
 // wait at the CTA barriers rather than exit: the warp-synchronous steps of a warp whose
 // sibling warps had exited were measured an order of magnitude slower on B200.
 template <int DIR, int SOLVER>
-__global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB, int CB,
-                                                     double* gscr, int RG, int CG) {
+__global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB,
+                                                     double* gscr, int RG, int roww) {
     extern __shared__ double dyn_smem[];
     __shared__ LineShared sgw[kWL];
     __shared__ int s_long[kWL];
@@ -604,17 +623,14 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
         if (li < nlines) hydro_setup<DIR, WarpG>(g, p, startidx + li, sg);  // warp-uniform
         __syncthreads();
         if (li < nlines && sg.nseg > 0) {
-            if (sg.R > kRowW || sg.C > kCellW) {
+            if (sg.R > roww) {
                 if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
             } else {
                 double* A = dyn_smem + w * kWarpHydro;
                 double* B = A + kRowW;
                 double* Cc = B + kRowW;
                 double* D = Cc + kRowW;
-                double* a2 = D + kRowW;
-                double* c2 = a2 + kCellW;
-                double* d2 = c2 + kCellW;
-                hydro_body<DIR, SOLVER, WarpG>(g, p, startidx + li, sg, A, B, Cc, D, a2, c2, d2, nullptr,
+                hydro_body<DIR, SOLVER, WarpG>(g, p, startidx + li, sg, A, B, Cc, D, D + kRowW, nullptr,
                                                SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
@@ -625,16 +641,13 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
             const LineShared& sl = sgw[wl];
             const int line = startidx + (int)blockIdx.x + (j0 + wl) * G;
             const SolvePlan pl = solve_plan(sl.R, SOLVER == 0 ? 256 : 32);
-            const bool fits = pl.t1 * pl.m <= RB && sl.C <= CB;
-            const int rs = fits ? RB : RG, cs = fits ? CB : CG;
-            double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * (4 * (size_t)RG + 3 * (size_t)CG);
+            const bool fits = pl.t1 * pl.m <= RB;
+            const int rs = fits ? RB : RG;
+            double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * (4 * (size_t)RG + kEnds);
             double* B = A + rs;
             double* Cc = B + rs;
             double* D = Cc + rs;
-            double* a2 = D + rs;
-            double* c2 = a2 + cs;
-            double* d2 = c2 + cs;
-            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sl, A, B, Cc, D, a2, c2, d2, s_red, pl);
+            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sl, A, B, Cc, D, D + rs, s_red, pl);
             __syncthreads();  // the slices and sgw are reused
         }
     }
@@ -846,10 +859,10 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
     }
 }
 
-// Fused sediment sweep of one direction: as k_hydro_sweep, short lines at most kRowWf rows.
+// Fused sediment sweep of one direction: as k_hydro_sweep.
 template <int DIR, int SOLVER>
 __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int half, int startidx, int endidx, int RB,
-                                                  double* gscr, int RG) {
+                                                  double* gscr, int RG, int roww) {
     extern __shared__ double dyn_smem[];
     __shared__ LineShared sgw[kWL];
     __shared__ int s_long[kWL];
@@ -865,7 +878,7 @@ __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int
         if (li < nlines) fs_setup<DIR, WarpG>(g, p, startidx + li, sg);  // warp-uniform
         __syncthreads();
         if (li < nlines && sg.R > 0) {
-            if (sg.R > kRowWf) {
+            if (sg.R > roww) {
                 if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
             } else {
                 double* A = dyn_smem + w * kWarpFs;
@@ -912,8 +925,8 @@ cudaError_t allow_all(F* const* fs, int n, int* limit) {
     return cudaSuccess;
 }
 
-using HydroSweepFn = void(DevGrid, DevParams, int, int, int, int, double*, int, int);
-using FsSweepFn = void(DevGrid, DevParams, int, int, int, int, double*, int);
+using HydroSweepFn = void(DevGrid, DevParams, int, int, int, double*, int, int);
+using FsSweepFn = void(DevGrid, DevParams, int, int, int, int, double*, int, int);
 
 HydroSweepFn* const kHydroSweep[2][2] = {{k_hydro_sweep<0, 0>, k_hydro_sweep<0, 1>},
                                          {k_hydro_sweep<1, 0>, k_hydro_sweep<1, 1>}};
@@ -922,8 +935,9 @@ FsSweepFn* const kFsSweep[2][2] = {{k_fs_sweep<0, 0>, k_fs_sweep<0, 1>}, {k_fs_s
 }  // namespace
 
 // Shared-memory sizes and the long-line grid of a grid of N x M cells on the current
-// device; opts the sweep kernels into the shared memory they may need.
-cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
+// device; opts the sweep kernels into the shared memory they may need.  max_rows > 0 caps
+// the rows a long line may hold in shared memory (longer lines then run in global scratch).
+cudaError_t sweep_plan(int N, int M, SweepPlan* sp, int max_rows) {
     cudaError_t e;
     int lim_h, lim_f;
     if ((e = allow_all(&kHydroSweep[0][0], 4, &lim_h)) != cudaSuccess) return e;
@@ -932,7 +946,7 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
     const size_t warp_h = (size_t)kWL * kWarpHydro, warp_f = (size_t)kWL * kWarpFs;  // short-line slices
     if ((long long)(sizeof(double) * warp_h) > lim_h || (long long)(sizeof(double) * warp_f) > lim_f)
         return cudaErrorInvalidValue;
-    // every row/cell a line can have: rows <= 2 L + 20, cells <= L + 3 (solved by 32 lanes)
+    // every row a line can have: rows <= 2 L + 20 (solved by 32 lanes)
     {
         int rg = 0;
         for (int t1 = 32; t1 <= 256; t1 <<= 1) {  // the padded rows of any solve plan
@@ -941,18 +955,19 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
         }
         sp->RG = rg;
     }
-    sp->CG = L + 3;
     sp->need_global = 0;
-    if ((long long)(sizeof(double) * (4 * (size_t)sp->RG + 3 * (size_t)sp->CG)) <= lim_h) {
+    sp->wide = 0;
+    if ((long long)(sizeof(double) * (4 * (size_t)sp->RG + kEnds)) <= lim_h) {
         sp->RB = sp->RG;
-        sp->CB = sp->CG;
-    } else {  // as many rows (and half as many cells) as fit; longer lines use global scratch
-        const int pairs = (int)((lim_h / (int)sizeof(double)) / (4 * 2 + 3));
-        sp->RB = 2 * pairs;
-        sp->CB = pairs;
+    } else {  // as many rows as fit; longer lines use global scratch
+        sp->RB = (int)((lim_h / (int)sizeof(double) - kEnds) / 4);
         sp->need_global = 1;
     }
-    size_t big = 4 * (size_t)sp->RB + 3 * (size_t)sp->CB;
+    if (max_rows > 0 && sp->RB > max_rows) {
+        sp->RB = max_rows;
+        sp->need_global = 1;
+    }
+    size_t big = 4 * (size_t)sp->RB + kEnds;
     sp->smem_lines = sizeof(double) * (big > warp_h ? big : warp_h);
     sp->RGf = 0;
     for (int t1 = 32; t1 <= 256; t1 <<= 1) {
@@ -963,6 +978,10 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
         sp->RBf = sp->RGf;
     } else {
         sp->RBf = (int)((lim_f / (int)sizeof(double)) / 4);
+        sp->need_global = 1;
+    }
+    if (max_rows > 0 && sp->RBf > max_rows) {
+        sp->RBf = max_rows;
         sp->need_global = 1;
     }
     big = 4 * (size_t)sp->RBf;
@@ -981,8 +1000,7 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp) {
     sp->long_grid = nsm * (occ < occf ? occ : occf);
     if (sp->long_grid > L + 3) sp->long_grid = L + 3;
     sp->scratch_doubles =
-        sp->need_global ? (size_t)sp->long_grid * (4 * (size_t)(sp->RG > sp->RGf ? sp->RG : sp->RGf) + 3 * (size_t)sp->CG)
-                        : 1;
+        sp->need_global ? (size_t)sp->long_grid * (4 * (size_t)(sp->RG > sp->RGf ? sp->RG : sp->RGf) + kEnds) : 1;
     return cudaSuccess;
 }
 
@@ -990,6 +1008,7 @@ void sweep_plan_throughput(int N, int M, SweepPlan* sp) {
     const int L = N > M ? N : M;
     const int g = (L + 3 + kWL - 1) / kWL;
     if (sp->long_grid > g) sp->long_grid = g;
+    sp->wide = 1;
 }
 
 namespace {
@@ -998,8 +1017,8 @@ void hydro_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan&
     const int nlines = endidx - startidx + 1;
     if (nlines <= 0) return;
     const int sv = solver ? 1 : 0;
-    kHydroSweep[dir][sv]<<<sp.long_grid, kTL, sp.smem_lines, s>>>(g, p, startidx, endidx, sp.RB, sp.CB, scratch, sp.RG,
-                                                                  sp.CG);
+    const int roww = (sp.wide || nlines > kWL * sp.long_grid) ? kRowW : kRowShort;
+    kHydroSweep[dir][sv]<<<sp.long_grid, kTL, sp.smem_lines, s>>>(g, p, startidx, endidx, sp.RB, scratch, sp.RG, roww);
     hyd_kernel_launches_add(1);
 }
 
@@ -1008,8 +1027,9 @@ void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp
     const int nlines = endidx - startidx + 1;
     if (nlines <= 0) return;
     const int sv = solver ? 1 : 0;
+    const int roww = (sp.wide || nlines > kWL * sp.long_grid) ? kRowW : kRowShortF;
     kFsSweep[dir][sv]<<<sp.long_grid, kTL, sp.smem_fs_lines, s>>>(g, p, half, startidx, endidx, sp.RBf, scratch,
-                                                                   sp.RGf);
+                                                                   sp.RGf, roww);
     hyd_kernel_launches_add(1);
 }
 }  // namespace

@@ -173,7 +173,7 @@ def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=12
                  noise_len=50.0, manning=0.025, manning_spread=0.10, Q0=2000.0, Q1=3500.0,
                  tide_amp=1.0, tide_period_h=12.42, d50=1e-4, Sx=2.7125, cc_in=0.2,
                  sediment_start=1800.0, bed_change_start=3600.0, y_center=None, spinup_h=0.0,
-                 end_cells=8, name="meander"):
+                 end_cells=8, tide_delay_h=0.0, name="meander"):
     """Seeded meandering reach with a parabolic channel, floodplain and bed noise.
 
     Centreline y = y_c + amp*sin(2*pi*x/wavelength); parabolic section of `width` and
@@ -190,7 +190,8 @@ def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=12
 
     With spinup_h > 0 the discharge first ramps linearly from 0 to Q0 over spinup_h
     hours (the scheme cannot carry the bore of an impulsive start at Q0 into water at
-    rest) and the stated hydrograph follows.  sediment_start and bed_change_start are
+    rest) and the stated hydrograph follows.  With tide_delay_h > 0 the stage stays at 0
+    for that many hours and the tide starts from there.  sediment_start and bed_change_start are
     absolute times: the reference's Exner step divides by the speed VTH that only the
     sediment phase computes (Sediment_Transport.cu:365-374), so the bed must not start
     changing before the sediment does.
@@ -244,7 +245,7 @@ def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=12
     q = Q0 + (Q1 - Q0) * 0.5 * (1.0 - np.cos(math.pi * tr / hours))
     if spinup_h > 0:
         q = np.where(th < spinup_h, Q0 * th / spinup_h, q)
-    zt = tide_amp * np.sin(2 * math.pi * th / tide_period_h)
+    zt = np.where(th >= tide_delay_h, tide_amp * np.sin(2 * math.pi * (th - tide_delay_h) / tide_period_h), 0.0)
     tables = [np.zeros((1, total_time)), np.zeros((1, total_time)), q[None, :].copy(), zt[None, :].copy()]
     cc = [np.zeros((1, total_time)), np.zeros((1, total_time)),
           np.full((1, total_time), cc_in), np.zeros((1, total_time))]
@@ -309,6 +310,36 @@ def config2_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE):
     2-cell oscillation once velocities pass about 2.5 m/s)."""
     return meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, spinup_h=spinup_h,
                         Q0=2000.0 * q_scale, Q1=3500.0 * q_scale, name="config2_meander")
+
+
+def config4_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE, hours=24.0, dT=1.0, end_cells=32, tide_delay_h=None):
+    """Large single reach 4096 x 2048, dx = 2.5 m, hydraulics + sediment + bed change.
+
+    The config-2 meander scaled x2 in length and width: centreline amplitude 240 m,
+    wavelength 3000 m, channel width 300 m (depth 8 m and floodplain +1.5 m unchanged),
+    bed-noise correlation length 100 m, rectangular end sections of 32 cells (80 m).
+    The hydrograph is config 2's (with its stability scale) times 2, the channel width
+    ratio, so that velocities match config 2's.  Sediment from t = 1800 s, bed change
+    from t = 3600 s, as in config 2.
+
+    No time step is stated for this workload; dt = 1 s as in config 2.  One change keeps
+    the reference's own scheme finite here: the tide starts after the discharge ramp
+    (tide_delay_h = spinup_h).  Started with the ramp, the rising tide of this 4x larger
+    reach pours more water in at the stage edge than the ramped discharge carries out,
+    and under that inflow the scheme's stage-edge velocity at the channel's bank cell
+    grows without bound: the oracle reaches NaN by t = 1100 s (at dt = 0.5 s by
+    t = 1600 s).  With the delay the run stays finite (checked for 4 h at dt = 1 s and
+    dt = 0.5 s).  The morphological factor 10 of this workload is not a
+    library parameter: the Exner step accumulates dH without feeding it back into the
+    bed (the reference's behaviour), so the factor scales the reported bed change only
+    and is kept in notes["morfac"]."""
+    c = meander_case(N=4096, M=2048, dX=2.5, dT=dT, hours=hours, spinup_h=spinup_h, amp=240.0,
+                     wavelength=3000.0, width=300.0, noise_len=100.0,
+                     Q0=2000.0 * q_scale * 2.0, Q1=3500.0 * q_scale * 2.0, end_cells=end_cells,
+                     tide_delay_h=spinup_h if tide_delay_h is None else tide_delay_h,
+                     name="config4_large_meander")
+    c.notes["morfac"] = 10.0
+    return c
 
 
 def config3_cases(n=96, seed=20261204, nx_range=(128, 1024), ny_range=(64, 512), hours=2.0, spinup_h=0.5):

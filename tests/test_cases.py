@@ -42,3 +42,19 @@ def test_islands_wellposed():
     for seed in (7, 11, 23):
         c = cases.islands_case(seed=seed)
         assert _bad_faces(c.fields["h"]) == 0
+
+
+def test_config4_layout_and_wellposed():
+    """The 4096 x 2048 reach at 2.5 m: config 2's meander scaled x2, dt = 1 s, the tide
+    held at 0 through the discharge ramp and then starting from 0."""
+    c = cases.config4_case()
+    assert (c.N, c.M) == (4096, 2048) and c.params.dX == 2.5 and c.params.dT == 1.0
+    assert c.fields["h"].shape == (4099, 2051)
+    assert _bad_faces(c.fields["h"] - c.params.NANGDAY) == 0
+    zt = c.tables[cases.EDGE_RIGHT][0]
+    assert zt[0] == 0 and zt[1] == 0 and zt[2] > 0.4
+    q = c.tables[cases.EDGE_LEFT][0]
+    assert q[0] == 0 and q[1] == 2 * 2000.0 * cases.CONFIG2_Q_SCALE
+    assert c.notes["morfac"] == 10.0
+    wet = (c.fields["h"][2:-1, 2:-1] - c.params.NANGDAY) > 0
+    assert 0.04 < wet.mean() < 0.08
