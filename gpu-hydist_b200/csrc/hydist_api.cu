@@ -581,6 +581,8 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         return fail(HYD_ECUDA, std::string("shared-memory set-up: ") + cudaGetErrorString(e));
     }
     s->g.LT = (N + 3 + 31) / 32 * 32;
+    // the seven column-major coefficient arrays outgrow L2 from about 4M cells
+    s->g.tile_cols = (size_t)N * M >= ((size_t)1 << 22);
     s->g.colT_stride = (size_t)(M + 3) * s->g.LT;
     e = cudaMalloc(&s->g.colT, 7 * s->g.colT_stride * sizeof(double) + s->g.colT_stride);
     s->g.colB = (unsigned char*)(s->g.colT + 7 * s->g.colT_stride);

@@ -63,6 +63,10 @@ struct DevGrid {
     size_t colT_stride;
     int LT;
     int wpr;  // warps per row of the extended-span kernels (1 until the spans are known)
+    // column-major stores through shared-memory tiles (colmajor_tile): set for grids whose
+    // column-major arrays are too large to stay in L2, where one 32-byte sector per stored
+    // value costs DRAM traffic; smaller grids store straight from the per-row warps
+    int tile_cols;
     double* clock;  // [0] time of half-step 1, [1] time of half-step 2, [2] time at the step start
 };
 
@@ -71,6 +75,60 @@ __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { at
 // Column-major copy k of a per-cell quantity; (row i, column j) is at [j * g.LT + i].
 __device__ __forceinline__ double* colT(const DevGrid& g, int k) { return g.colT + (size_t)k * g.colT_stride; }
 __device__ __forceinline__ double* rowC(const DevGrid& g, int k) { return g.rowC + (size_t)k * g.rowC_stride; }
+
+// Per-cell values of a row-major sweep over the grid stored column-major through a
+// shared-memory tile.  The CTA (256 threads) takes rows i0..i0+7, one warp per row as the
+// per-row kernels do, and walks the union of those rows' spans (rlo..rhi clipped to
+// [jmin, jmax]; rows past ilast have none) in chunks of 32 columns.  cell(i, j, v) fills
+// the K values of cell (i, j) and returns whether the cell is stored; the stored values
+// of a chunk go out column by column, the 8 rows of a column as one contiguous run, in
+// place of one 32-byte sector per cell.  dst[k][j * g.LT + i] receives value k.
+constexpr int kTileRows = 8;
+template <int K, class Cell>
+__device__ __forceinline__ void colmajor_tile(const DevGrid& g, int i0, int ilast, int jmin, int jmax, Cell cell,
+                                              double* const (&dst)[K]) {
+    __shared__ double s_v[K][kTileRows][33];
+    __shared__ unsigned s_m[kTileRows];
+    __shared__ int s_lo[kTileRows], s_hi[kTileRows];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = i0 + w;
+    int lo = 1 << 30, hi = -1;
+    if (i <= ilast) {
+        lo = max(g.rlo[i], jmin);
+        hi = min(g.rhi[i], jmax);
+    }
+    if (lane == 0) {
+        s_lo[w] = lo;
+        s_hi[w] = hi;
+    }
+    __syncthreads();
+    int ulo = 1 << 30, uhi = -1;
+#pragma unroll
+    for (int r = 0; r < kTileRows; r++) {
+        ulo = min(ulo, s_lo[r]);
+        uhi = max(uhi, s_hi[r]);
+    }
+    const int sc = threadIdx.x / kTileRows, sr = threadIdx.x % kTileRows;  // store: column, row
+    for (int jc = ulo; jc <= uhi; jc += 32) {
+        const int j = jc + lane;
+        double v[K];
+        bool wr = false;
+        if (j >= lo && j <= hi) wr = cell(i, j, v);
+        const unsigned m = __ballot_sync(0xffffffffu, wr);
+        if (wr) {
+#pragma unroll
+            for (int k = 0; k < K; k++) s_v[k][w][lane] = v[k];
+        }
+        if (lane == 0) s_m[w] = m;
+        __syncthreads();
+        if ((s_m[sr] >> sc) & 1u) {
+            const size_t q = (size_t)(jc + sc) * g.LT + i0 + sr;
+#pragma unroll
+            for (int k = 0; k < K; k++) dst[k][q] = s_v[k][sr][sc];
+        }
+        __syncthreads();
+    }
+}
 
 // Wall/open flags of a row segment [first, last] (locate_segment_v, constant.cuh:135-154).
 __device__ __forceinline__ void seg_flags_v(const DevGrid& g, const DevParams& p, int row, int first, int last,

@@ -364,8 +364,11 @@ __device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams
 // CTA the half-step's boundary values (`writes`).  The coefficients read none of what the
 // boundary writes (edge levels, edge velocity arrays, inflow concentrations).  One warp
 // per row of the grid over the row's span of cells that can be wet; small CTAs, so that
-// the column-major stores (one sector per lane) spread over many SMs.
-template <int KIND>
+// the stores spread over many SMs; TILE (large grids, g.tile_cols) stores KIND 0 through a
+// shared-memory tile (colmajor_tile), 8 rows of a column at a time.  The variants are
+// separate kernels: the tile's shared memory would otherwise shrink the L1 share of the
+// small grids' launches, whose stencil loads it serves.
+template <int KIND, int TILE>
 __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int writes) {
     if (blockIdx.x == gridDim.x - 1) {
         __shared__ double s_t;
@@ -384,6 +387,19 @@ __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int wr
         __syncthreads();
         if (p.channel) boundary_channel_body(g, p, s_t);
         else boundary_body(g, s_t, writes);
+        return;
+    }
+    if constexpr (KIND == 0 && TILE) {
+        double* const dst[7] = {colT(g, 0), colT(g, 1), colT(g, 2), colT(g, 3), colT(g, 4), colT(g, 5), colT(g, 6)};
+        colmajor_tile<7>(
+            g, 2 + kTileRows * blockIdx.x, g.N, 2, g.M,
+            [&](int i, int j, double* v) {
+                const int pos = i * g.P + j;
+                if (g.khouot[pos] != 0) return false;
+                uz_cell_coeffs(g, p, pos, v[0], v[1], v[2], v[3], v[4], v[5], v[6]);
+                return true;
+            },
+            dst);
         return;
     }
     const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
@@ -642,14 +658,27 @@ __device__ __forceinline__ double eu_cell(const DevGrid& g, const DevParams& p, 
 constexpr int kEuSlot = 4;
 
 // explicit_u values of every wet cell of rows 2..N-1, columns 2..M, one warp per row over
-// the row's span; written column-major (g.colT array kEuSlot).
-__global__ void k_coef_eu(DevGrid g, DevParams p) {
-    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (i > g.N - 1) return;
-    const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
-    for (int j = lo + lane; j <= hi; j += 32) {
-        if (g.khouot[i * g.P + j] != 0) continue;
-        colT(g, kEuSlot)[(size_t)j * g.LT + i] = eu_cell(g, p, i, j);
+// the row's span; written column-major (g.colT array kEuSlot), with TILE through a tile.
+template <int TILE>
+__global__ void __launch_bounds__(256) k_coef_eu(DevGrid g, DevParams p) {
+    if constexpr (!TILE) {
+        const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+        if (i > g.N - 1) return;
+        const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
+        for (int j = lo + lane; j <= hi; j += 32) {
+            if (g.khouot[i * g.P + j] != 0) continue;
+            colT(g, kEuSlot)[(size_t)j * g.LT + i] = eu_cell(g, p, i, j);
+        }
+    } else {
+        double* const dst[1] = {colT(g, kEuSlot)};
+        colmajor_tile<1>(
+            g, 2 + kTileRows * blockIdx.x, g.N - 1, 2, g.M,
+            [&](int i, int j, double* v) {
+                if (g.khouot[i * g.P + j] != 0) return false;
+                v[0] = eu_cell(g, p, i, j);
+                return true;
+            },
+            dst);
     }
 }
 
@@ -1553,8 +1582,9 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
 
 void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
     const int nb = ((g.N - 1) * 32 + 255) / 256 + 1;
-    if (half == 0) k_coef_bnd<0><<<nb, 256, 0, s>>>(g, p, writes);
-    else k_coef_bnd<1><<<nb, 256, 0, s>>>(g, p, writes);
+    if (half == 1) k_coef_bnd<1, 0><<<nb, 256, 0, s>>>(g, p, writes);
+    else if (g.tile_cols) k_coef_bnd<0, 1><<<nb, 256, 0, s>>>(g, p, writes);
+    else k_coef_bnd<0, 0><<<nb, 256, 0, s>>>(g, p, writes);
     hyd_kernel_launches_add(1);
 }
 
@@ -1584,7 +1614,8 @@ void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaSt
 }
 
 void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    k_coef_eu<<<((g.N - 2) * 32 + 255) / 256, 256, 0, s>>>(g, p);
+    if (g.tile_cols) k_coef_eu<1><<<((g.N - 2) * 32 + 255) / 256, 256, 0, s>>>(g, p);
+    else k_coef_eu<0><<<((g.N - 2) * 32 + 255) / 256, 256, 0, s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 

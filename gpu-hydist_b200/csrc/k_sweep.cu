@@ -724,22 +724,37 @@ __device__ __forceinline__ void fsi_cell_coeffs(const DevGrid& g, const DevParam
 }
 
 // FSj rows of every interior wet cell (columns 3..M-1), one warp per row of the grid over
-// the row's span, written column-major (g.colT arrays 0..3: aa bb cc dd).
-__global__ void k_coef_fsj(DevGrid g, DevParams p, int half) {
-    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (i > g.N) return;
+// the row's span, written column-major (g.colT arrays 0..3: aa bb cc dd), with TILE
+// through a tile.
+template <int TILE>
+__global__ void __launch_bounds__(256) k_coef_fsj(DevGrid g, DevParams p, int half) {
     const double t = g.clock[half];
-    const int lo = max(g.rlo[i], 3), hi = min(g.rhi[i], g.M - 1);
-    for (int j = lo + lane; j <= hi; j += 32) {
-        const int pos = i * g.P + j;
-        if (g.khouot[pos] != 0) continue;
-        double aa, bb, cc, dd;
-        fsj_cell_coeffs(g, p, t, pos, aa, bb, cc, dd);
-        const size_t q = (size_t)j * g.LT + i;
-        colT(g, 0)[q] = aa;
-        colT(g, 1)[q] = bb;
-        colT(g, 2)[q] = cc;
-        colT(g, 3)[q] = dd;
+    if constexpr (!TILE) {
+        const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+        if (i > g.N) return;
+        const int lo = max(g.rlo[i], 3), hi = min(g.rhi[i], g.M - 1);
+        for (int j = lo + lane; j <= hi; j += 32) {
+            const int pos = i * g.P + j;
+            if (g.khouot[pos] != 0) continue;
+            double aa, bb, cc, dd;
+            fsj_cell_coeffs(g, p, t, pos, aa, bb, cc, dd);
+            const size_t q = (size_t)j * g.LT + i;
+            colT(g, 0)[q] = aa;
+            colT(g, 1)[q] = bb;
+            colT(g, 2)[q] = cc;
+            colT(g, 3)[q] = dd;
+        }
+    } else {
+        double* const dst[4] = {colT(g, 0), colT(g, 1), colT(g, 2), colT(g, 3)};
+        colmajor_tile<4>(
+            g, 2 + kTileRows * blockIdx.x, g.N, 3, g.M - 1,
+            [&](int i, int j, double* v) {
+                const int pos = i * g.P + j;
+                if (g.khouot[pos] != 0) return false;
+                fsj_cell_coeffs(g, p, t, pos, v[0], v[1], v[2], v[3]);
+                return true;
+            },
+            dst);
     }
 }
 
@@ -1035,7 +1050,8 @@ void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp
 }  // namespace
 
 void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s) {
-    k_coef_fsj<<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p, half);
+    if (g.tile_cols) k_coef_fsj<1><<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p, half);
+    else k_coef_fsj<0><<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p, half);
     hyd_kernel_launches_add(1);
 }
 
