@@ -154,24 +154,45 @@ __device__ __forceinline__ EdgeArgs edge_args(const DevGrid& g, int e) {
     return {1, N, N + 1, g.btype + 3 * HYD_SEGL, hi_right, g.bc[3], g.cc[3], g.ubp, g.hmax[3], g.moci, g.daui, g.cuoii};
 }
 
-__device__ BndRec bnd_compute(const DevGrid& g, const EdgeArgs& a, int i, double t) {
-    BndRec r{0, 0.0, 0.0};
-    const int P = g.P, tt = g.total_time;
+// What an edge applies at time t, the same for every index of the edge: the open segment
+// (the edge line's first wet segment, [lo, hi]; empty when the line has none), its kind
+// and the table values interpolated at t.
+struct BndSeg {
+    int lo, hi, kind;
+    double value, cv;
+};
+
+__device__ __forceinline__ BndSeg bnd_segment(const DevGrid& g, const EdgeArgs& a, double t) {
+    BndSeg s{1, 0, 0, 0.0, 0.0};
+    if (a.moc[a.location] <= 0) return s;
+    const int tt = g.total_time;
     const int t1 = (int)(t / 3600);
     const double t2 = (t - (3600.0 * t1)) / 3600.0;
-    int seg_no = -1;
-    if (a.moc[a.location] > 0 && a.dau[a.location * HYD_SEGL] <= i && i <= a.cuoi[a.location * HYD_SEGL]) seg_no = 0;
-    if (seg_no == -1) return r;
-    const double value = a.bcv[seg_no * tt + t1] * (1.0 - t2) + a.bcv[seg_no * tt + t1 + 1] * t2;
+    const int seg_no = 0;
+    s.lo = a.dau[a.location * HYD_SEGL];
+    s.hi = a.cuoi[a.location * HYD_SEGL];
+    s.value = a.bcv[seg_no * tt + t1] * (1.0 - t2) + a.bcv[seg_no * tt + t1 + 1] * t2;
     if (a.btype[seg_no] == 2) {
-        r.kind = 1;
-        r.value = value * a.hi_e[i];
-        const int ii = a.isU ? a.location : i, jj = a.isU ? i : a.location;
-        const double cv = a.ccv[seg_no * tt + t1] * (1.0 - t2) + a.ccv[seg_no * tt + t1 + 1] * t2;
-        r.fsv = cv * g.htaiz_bd[ii * P + jj] * a.hmax;
+        s.kind = 1;
+        s.cv = a.ccv[seg_no * tt + t1] * (1.0 - t2) + a.ccv[seg_no * tt + t1 + 1] * t2;
     } else {
-        r.kind = 2;
-        r.value = value;
+        s.kind = 2;
+    }
+    return s;
+}
+
+// The record of index i of the edge (the body of Boundary_value / FS_boundary for one
+// thread, support_funcs.cu:544-617).
+__device__ __forceinline__ BndRec bnd_at(const DevGrid& g, const EdgeArgs& a, const BndSeg& s, int i) {
+    BndRec r{0, 0.0, 0.0};
+    if (i < s.lo || i > s.hi) return r;
+    r.kind = s.kind;
+    if (s.kind == 1) {
+        r.value = s.value * a.hi_e[i];
+        const int ii = a.isU ? a.location : i, jj = a.isU ? i : a.location;
+        r.fsv = s.cv * g.htaiz_bd[ii * g.P + jj] * a.hmax;
+    } else {
+        r.value = s.value;
     }
     return r;
 }
@@ -214,11 +235,21 @@ __device__ void boundary_body(const DevGrid& g, double t, int writes = kBndAll) 
     if (e < 4) {
         const EdgeArgs a = edge_args(g, e);
         const int far = a.isU ? M : N;
-        for (int i = 2 + r; i <= imax; i += Q) {
-            const BndRec rec = bnd_compute(g, a, i, t);
-            if (i == 2) s_rec[e][0] = rec;
-            else if (i == far) s_rec[e][1] = rec;
-            else bnd_apply(g, a, rec, i, writes);
+        const BndSeg sg = bnd_segment(g, a, t);
+        // four indices at a time: their loads issue before any of their stores
+        constexpr int U = 4;
+        for (int i0 = 2 + r; i0 <= imax; i0 += U * Q) {
+            BndRec rec[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) rec[u] = bnd_at(g, a, sg, i0 + u * Q);
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int i = i0 + u * Q;
+                if (i > imax) break;
+                if (i == 2) s_rec[e][0] = rec[u];
+                else if (i == far) s_rec[e][1] = rec[u];
+                else bnd_apply(g, a, rec[u], i, writes);
+            }
         }
     }
     __syncthreads();
