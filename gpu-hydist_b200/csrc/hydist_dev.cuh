@@ -16,6 +16,7 @@
 #define HYD_ST_SEG_OVERFLOW 1u     // more than 20 wet segments on a line
 #define HYD_ST_INTERP_RANGE 2u     // edge FS interpolation index left the grid
 #define HYD_ST_DEGENERATE 4u       // single-cell segment on an open edge (reference reads stale scratch)
+#define HYD_ST_EDGE_REACH 8u       // an edge FS interpolation read the opposite edge row (order-dependent)
 
 struct DevParams {
     double dX, dY, dT, dXbp, dX2, dYbp, dY2, dTchia2dX, dTchia2dY, HaiChiadT;

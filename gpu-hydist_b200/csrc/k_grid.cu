@@ -1130,8 +1130,8 @@ __global__ void k_post_span(DevGrid g) {
 
 // ------------------------------------------------------------- wet-segment scans
 
-template <int AFTER_UPDATE = 1>
-__device__ void fs_edges_block(const DevGrid& g, const DevParams& p);
+template <int AFTER_UPDATE>
+__device__ void fs_edges_part(const DevGrid& g, const DevParams& p, int part, int parts);
 
 // Rescan of the listed rows (ROWS) or columns: a line is listed when one of its cells
 // changed since its segments were last scanned, and a line whose mask did not change
@@ -1142,7 +1142,7 @@ template <int ROWS>
 __global__ void k_scan_dirty(DevGrid g, DevParams p, int edges) {
     extern __shared__ unsigned swords[];
     if ((int)blockIdx.x == edges) {
-        fs_edges_block<1>(g, p);
+        fs_edges_part<1>(g, p, 0, 1);
     } else {
         const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int scanning = gridDim.x - (edges >= 0 ? 1 : 0);
@@ -1177,50 +1177,85 @@ __global__ void k_scan_dirty(DevGrid g, DevParams p, int edges) {
 }
 
 // Interpolate_FS_ng / Interpolate_FS_d (support_funcs.cu:189-229), run by the row-2,
-// row-N and column-M blocks of the scans in the reference.  Rows first (row 2, then
-// row N), then the column.
+// row-N and column-M blocks of the scans in the reference: row 2, then row N, then column
+// M.  One item is one index of one of the three passes: pass 0 (row 2) and pass 1 (row N)
+// at column j, pass 2 (column M) at row i.
 // AFTER_UPDATE = 0: run concurrently with the state update, so u and v (which the update
 // sets to t_u and t_v on i <= N, j <= M) are read as t_u and t_v there.
-template <int AFTER_UPDATE>
-__device__ void fs_edges_block(const DevGrid& g, const DevParams& p) {
+// CG: FS read through L2 only (values other CTAs of the launch wrote).
+template <int AFTER_UPDATE, int CG>
+__device__ __forceinline__ void fs_edge_item(const DevGrid& g, const DevParams& p, int pass, int idx) {
     const double* uu = AFTER_UPDATE ? g.u : g.t_u;
     const int N = g.N, M = g.M, P = g.P;
-    const int i_dX = __double2int_rn(p.dX);
-    const int j_dY = __double2int_rn(p.dY);
-    for (int pass = 0; pass < 2; pass++) {
+    auto fs = [&](size_t q) { return CG ? __ldcg(g.FS + q) : g.FS[q]; };
+    if (pass < 2) {
+        const int j = idx;
         const int location = pass == 0 ? 2 : N, offset = pass == 0 ? 2 : N - 1, sign = pass == 0 ? 1 : -1;
-        for (int j = 1 + threadIdx.x; j < M; j += blockDim.x) {
-            if (g.t_u[location * P + j] > 0) {
-                const double deltaX = (uu[location * P + j] + g.t_u[location * P + j]) * 0.25 * p.dT;
-                const int i = (int)(offset + sign * (deltaX / p.dX));
-                const int i_deltaX = __double2int_rn(deltaX);
-                if (i < 0 || i + 1 > N + 2) {
-                    flag_status(g, HYD_ST_INTERP_RANGE);
-                    continue;
-                }
-                g.FS[location * P + j] = g.FS[i * P + j] + sign * (g.FS[(i + 1) * P + j] - g.FS[i * P + j]) *
-                                                               (deltaX / p.dX - i_deltaX / i_dX);
+        if (g.t_u[location * P + j] > 0) {
+            const double deltaX = (uu[location * P + j] + g.t_u[location * P + j]) * 0.25 * p.dT;
+            const int i = (int)(offset + sign * (deltaX / p.dX));
+            const int i_deltaX = __double2int_rn(deltaX);
+            if (i < 0 || i + 1 > N + 2) {
+                flag_status(g, HYD_ST_INTERP_RANGE);
+                return;
             }
+            // the two row passes run side by side: a pass reading the other's edge row
+            // would see it in either state
+            if (pass == 0 ? i + 1 >= N : i <= 2) flag_status(g, HYD_ST_EDGE_REACH);
+            const int i_dX = __double2int_rn(p.dX);
+            g.FS[location * P + j] =
+                fs((size_t)i * P + j) + sign * (fs((size_t)(i + 1) * P + j) - fs((size_t)i * P + j)) *
+                                            (deltaX / p.dX - i_deltaX / i_dX);
         }
-        __syncthreads();
-    }
-    {
+    } else {
+        const int i = idx;
         const int location = M, offset = M - 1, sign = -1;
-        for (int i = 1 + threadIdx.x; i < M && i <= N + 2; i += blockDim.x) {
-            if (g.t_v[i * P + location] > 0) {
-                const double vv = (AFTER_UPDATE || i > N) ? g.v[i * P + location] : g.t_v[i * P + location];
-                const double deltaY = (vv + g.t_v[i * P + location]) * 0.25 * p.dT;
-                const int j = (int)(offset + sign * (deltaY / p.dY));
-                const int j_deltaY = __double2int_rn(deltaY);
-                if (j < 0 || j + 1 > M + 2) {
-                    flag_status(g, HYD_ST_INTERP_RANGE);
-                    continue;
-                }
-                g.FS[i * P + location] = g.FS[i * P + j + 1] + (g.FS[i * P + j + 1] - g.FS[i * P + j]) *
-                                                                   (deltaY / p.dY - j_deltaY / j_dY);
+        if (g.t_v[i * P + location] > 0) {
+            const double vv = (AFTER_UPDATE || i > N) ? g.v[i * P + location] : g.t_v[i * P + location];
+            const double deltaY = (vv + g.t_v[i * P + location]) * 0.25 * p.dT;
+            const int j = (int)(offset + sign * (deltaY / p.dY));
+            const int j_deltaY = __double2int_rn(deltaY);
+            if (j < 0 || j + 1 > M + 2) {
+                flag_status(g, HYD_ST_INTERP_RANGE);
+                return;
             }
+            const int j_dY = __double2int_rn(p.dY);
+            g.FS[i * P + location] = fs((size_t)i * P + j + 1) + (fs((size_t)i * P + j + 1) - fs((size_t)i * P + j)) *
+                                                                    (deltaY / p.dY - j_deltaY / j_dY);
         }
     }
+}
+
+// The edge interpolation by `parts` CTAs (this one is `part`).  Items are independent but
+// for the column pass at rows 2 and N, which reads the row passes' results in row 2 and
+// row N: every other item runs first, spread over the CTAs; the last CTA to finish them
+// (counter g.dctr[4], reset by that CTA) then runs those two.
+template <int AFTER_UPDATE>
+__device__ void fs_edges_part(const DevGrid& g, const DevParams& p, int part, int parts) {
+    const int N = g.N, M = g.M;
+    const int nrow = M - 1;                       // j = 1 .. M-1
+    const int ncol = min(M - 1, N + 2);           // i = 1 .. ncol
+    const int K = 2 * nrow + ncol;
+    for (int k = part * blockDim.x + threadIdx.x; k < K; k += parts * blockDim.x) {
+        if (k < 2 * nrow) {
+            fs_edge_item<AFTER_UPDATE, 0>(g, p, k < nrow ? 0 : 1, 1 + (k < nrow ? k : k - nrow));
+        } else {
+            const int i = 1 + k - 2 * nrow;
+            if (i != 2 && i != N) fs_edge_item<AFTER_UPDATE, 0>(g, p, 2, i);
+        }
+    }
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&g.dctr[4], 1u) == (unsigned)parts - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0 && 2 <= ncol) fs_edge_item<AFTER_UPDATE, 1>(g, p, 2, 2);
+    if (threadIdx.x == 32 && N <= ncol && N != 2) fs_edge_item<AFTER_UPDATE, 1>(g, p, 2, N);
+    if (threadIdx.x == 0) g.dctr[4] = 0;
 }
 
 // --------------------------------------------------------------------- sediment
@@ -1293,8 +1328,9 @@ __global__ void k_vth_span(DevGrid g, DevParams p) {
 // and, when VTH, Find_VTH + hesoK on the extended spans (CTAs [0, nbp), one warp per
 // row; both only read the cell's own new Htdu/Htdv); the rescan of the changed lines of
 // the other direction (CTAs [nbp, nbp + nbs)); and the edge concentration interpolation
-// (last CTA, reading t_u / t_v where the reference reads u / v after the update).  None of
-// the three writes what another reads.
+// (the last kEdgeParts CTAs, reading t_u / t_v where the reference reads u / v after the
+// update).  None of the three writes what another reads.
+constexpr int kEdgeParts = 8;
 template <int ROWS, int VTH>
 __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
     extern __shared__ unsigned swords[];
@@ -1309,8 +1345,8 @@ __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
         }
         return;
     }
-    if (b == (int)gridDim.x - 1) {
-        fs_edges_block<0>(g, p);
+    if (b >= (int)gridDim.x - kEdgeParts) {
+        fs_edges_part<0>(g, p, b - ((int)gridDim.x - kEdgeParts), kEdgeParts);
         return;
     }
     const int sb = b - nbp;
@@ -1582,7 +1618,7 @@ int outside_differs(const DevGrid& g, const double* a, const double* b, int i0, 
 void clear_rescan_lists(const DevGrid& g, cudaStream_t s) {
     cudaMemsetAsync(g.dirty_r, 0, sizeof(int) * (g.N + 3), s);
     cudaMemsetAsync(g.dirty_c, 0, sizeof(int) * (g.M + 3), s);
-    cudaMemsetAsync(g.dctr, 0, 4 * sizeof(unsigned), s);
+    cudaMemsetAsync(g.dctr, 0, 5 * sizeof(unsigned), s);
 }
 
 // List every column for the rescan after the next row resets.
@@ -1688,7 +1724,7 @@ void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s) {
 // is rescanned.
 void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s) {
     const int nbp = row_warps_blocks(g, g.N + 1), nbs = 32;
-    const int grid = nbp + nbs + 1;
+    const int grid = nbp + nbs + kEdgeParts;
     if (rows) {
         if (vth) k_post_fused<1, 1><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
         else k_post_fused<1, 0><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
