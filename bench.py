@@ -380,8 +380,8 @@ def run_ours(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": WORKLOADS[args.workload][2],
-            "config": {"workload": "%s, t=%d..%d s" % (WORKLOADS[args.workload][1], args.spinup + args.warmup,
-                                                        args.spinup + args.warmup + args.steps),
+            "config": {"workload": "%s, t=%d..%d s" % (WORKLOADS[args.workload][1], args.spinup + 2 * args.warmup,
+                                                        args.spinup + 2 * args.warmup + args.steps),
                        "grid": [N, M], "cells": cells, "wet_cells": wet,
                        "parallelism": "replicas%d" % world if world > 1 else "single",
                        "core_cells": core, "span_cells": span,
