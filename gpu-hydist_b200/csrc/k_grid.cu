@@ -1055,6 +1055,13 @@ __global__ void k_ext_spans(DevGrid g, int H) {
         lo = min(lo, g.rlo[r] - H);
         hi = max(hi, g.rhi[r] + H);
     }
+    if (hi < lo) {
+        // nothing within H rows can change: an empty span of small bounds (the row
+        // kernels start at elo plus a lane offset, which must not overflow)
+        g.elo[i] = 1;
+        g.ehi[i] = 0;
+        return;
+    }
     g.elo[i] = max(lo, 0);
     g.ehi[i] = min(hi, g.M + 2);
 }
