@@ -293,9 +293,11 @@ def run_ours(args, rank, world, local_rank):
 
     # end to end through the C ABI, host buffers in pinned memory: every step the boundary
     # forcing (the Q/Z and inflow-concentration tables of the open edges) in through
-    # hyd_update_boundary, hyd_step(1), and the water level z out through
-    # hyd_get_field_async (the reference's per-step data flow: forcing in, levels out; the
-    # state stays on the device)
+    # hyd_update_boundary, hyd_step(1), and the water level z out (the reference's data
+    # flow: forcing in, levels out; the state stays on the device).  The levels reach the
+    # host through the library's mirror (hyd_mirror_update_async: a full host copy of z
+    # after every step, of which only the box of cells a step can change crosses PCIe);
+    # e2e_full_field copies every cell of z every step instead (hyd_get_field_async)
     e2e_steps = max(10, min(args.steps, 100))
 
     def pinned(a):
@@ -309,30 +311,51 @@ def run_ours(args, rank, world, local_rank):
     # library's copy stream) while step k + 1 runs
     z_host = [torch.empty((N + 3, M + 3), dtype=torch.float64, pin_memory=True) for _ in range(2)]
 
-    def e2e_loop(n):
+    def timed_max(fn):
+        """Run fn between events on the library's stream; (device ms, max over ranks, and
+        fn's result)."""
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(ext)
+        res = fn()
+        a1.record(ext)
+        a1.synchronize()
+        t = torch.tensor([a0.elapsed_time(a1)], device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item()), res
+
+    def mirror_loop(n):
+        moved = 0
+        view = None
+        for _ in range(n):
+            sim.update_boundary([t.numpy() for t in tabs], [t.numpy() for t in ccs])
+            sim.step(1, sync=False)
+            view, b = sim.mirror_update()
+            moved += b
+        sim.wait_fields()
+        return view, moved
+
+    def full_loop(n):
         for k in range(n):
             sim.update_boundary([t.numpy() for t in tabs], [t.numpy() for t in ccs])
             sim.step(1, sync=False)
             sim.get_async("z", z_host[k % 2].numpy())
         sim.wait_fields()
 
-    # untimed warm-up of the same loop (first use of the snapshots and host buffers)
-    e2e_loop(max(args.warmup, 3))
-    torch.cuda.synchronize()
-    a0 = torch.cuda.Event(enable_timing=True)
-    a1 = torch.cuda.Event(enable_timing=True)
-    a0.record(ext)
-    e2e_loop(e2e_steps)
-    a1.record(ext)
-    a1.synchronize()
-    e2e_ms = a0.elapsed_time(a1)
-    t_e2e = torch.tensor([e2e_ms], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t_e2e, op=torch.distributed.ReduceOp.MAX)
-    e2e_ms = float(t_e2e.item())
     h2d_bytes = sum(t.numel() * 8 for t in tabs + ccs)
-    d2h_bytes = (N + 3) * (M + 3) * 8
+    sim.mirror_open("z")
+    # untimed warm-up of the same loops (first use of the snapshots and host buffers)
+    mirror_loop(max(args.warmup, 3))
+    e2e_ms, (view, moved) = timed_max(lambda: mirror_loop(e2e_steps))
+    mirror_exact = bool(np.array_equal(view, sim.get("z")))
+    sim.mirror_close()
+    d2h_bytes = moved / e2e_steps
     e2e_value = world * cells * e2e_steps / (e2e_ms / 1e3)
+    full_loop(max(args.warmup, 3))
+    full_ms, _ = timed_max(lambda: full_loop(e2e_steps))
+    full_value = world * cells * e2e_steps / (full_ms / 1e3)
 
     # the heavier round trip for reference: the whole state (z, u, v, FS) in and out
     names = ("z", "u", "v", "FS")
@@ -349,16 +372,7 @@ def run_ours(args, rank, world, local_rank):
                 sim.get(f, out=host[f].numpy())
 
     roundtrip_loop(max(args.warmup, 3))
-    torch.cuda.synchronize()
-    a0.record(ext)
-    roundtrip_loop(e2e_steps)
-    a1.record(ext)
-    a1.synchronize()
-    rt_ms = a0.elapsed_time(a1)
-    t_rt = torch.tensor([rt_ms], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t_rt, op=torch.distributed.ReduceOp.MAX)
-    rt_ms = float(t_rt.item())
+    rt_ms, _ = timed_max(lambda: roundtrip_loop(e2e_steps))
     field_bytes = (N + 3) * (M + 3) * 8 * len(names)
     rt_value = world * cells * e2e_steps / (rt_ms / 1e3)
 
@@ -391,7 +405,13 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d_bytes,
                     "d2h_bytes_per_step": d2h_bytes, "steps": e2e_steps,
                     "api": "hyd_update_boundary(Q/Z + concentration tables) + hyd_step(1) + "
-                           "hyd_get_field_async(z) (copied out while the next step runs), pinned host buffers"},
+                           "hyd_mirror_update_async(z): a full host copy of z after every step (checked equal "
+                           "to hyd_get_field at the end: %s), only the box of cells a step can change copied, "
+                           "while the next step runs" % mirror_exact},
+            "e2e_full_field": {"value": full_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d_bytes,
+                               "d2h_bytes_per_step": (N + 3) * (M + 3) * 8, "steps": e2e_steps,
+                               "api": "as e2e, with every cell of z copied every step (hyd_get_field_async into "
+                                      "two pinned buffers in turn)"},
             "e2e_state_roundtrip": {"value": rt_value, "unit": "cell-updates/s", "h2d_bytes_per_step": field_bytes,
                                     "d2h_bytes_per_step": field_bytes, "steps": e2e_steps,
                                     "api": "hyd_set_field(z,u,v,FS) + hyd_step(1) + hyd_get_field(z,u,v,FS), "

@@ -5,6 +5,7 @@
 // and the launch sequence of a full ADI step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <utility>
@@ -115,6 +116,21 @@ struct HydSim {
     cudaEvent_t ev_snap, ev_copied[2];
     void* snap[2];
     int snap_i;
+    // whole-grid events (set-up, field writes, whole-grid steps): after one, any cell of a
+    // field may have changed; between them only the cells of the extended spans can
+    unsigned long long epoch;
+    // rows [box_r0, box_r1] x columns [box_c0, box_c1]: every cell with a non-empty
+    // extended span, as of whole-grid event count box_epoch
+    unsigned long long box_epoch;
+    int box_r0, box_r1, box_c0, box_c1;
+    // host mirror of one grid field (hyd_mirror_*): two pinned copies handed out in turn,
+    // each up to date as of whole-grid event count mir_epoch[k]; device staging of a copy
+    const FieldDesc* mir_f;
+    double* mir[2];
+    void* mir_snap[2];
+    unsigned long long mir_epoch[2];
+    cudaEvent_t ev_mir[2];
+    int mir_i, mir_open;
     cudaGraphExec_t graph[8];
     long long graph_kernels[8];
     // timing with graphs: one graph per variant with the phase events captured in it
@@ -429,6 +445,15 @@ static void release(HydSim* s) {
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     cudaFree(s->snap[0]);
     cudaFree(s->snap[1]);
+    for (int k = 0; k < 2; k++) {
+        if (s->mir[k]) cudaFreeHost(s->mir[k]);
+        cudaFree(s->mir_snap[k]);
+        if (s->ev_mir[k]) cudaEventDestroy(s->ev_mir[k]);
+        s->mir[k] = nullptr;
+        s->mir_snap[k] = nullptr;
+        s->ev_mir[k] = nullptr;
+    }
+    s->mir_open = 0;
     if (s->ev_snap) cudaEventDestroy(s->ev_snap);
     if (s->ev_copied[0]) cudaEventDestroy(s->ev_copied[0]);
     if (s->ev_copied[1]) cudaEventDestroy(s->ev_copied[1]);
@@ -673,6 +698,7 @@ int hyd_set_field(hyd_handle h, const char* name, const void* host, size_t count
         }
     }
     h->full_pending |= owed;
+    h->epoch++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return HYD_OK;
@@ -724,6 +750,119 @@ int hyd_wait_fields(hyd_handle h) {
     CUDA_TRY(cudaSetDevice(h->device));
     CUDA_TRY(cudaEventSynchronize(h->ev_copied[0]));
     CUDA_TRY(cudaEventSynchronize(h->ev_copied[1]));
+    if (h->mir_open) {
+        CUDA_TRY(cudaEventSynchronize(h->ev_mir[0]));
+        CUDA_TRY(cudaEventSynchronize(h->ev_mir[1]));
+    }
+    return HYD_OK;
+}
+
+// The box of the extended spans, read back from the device (waits for the queued steps).
+static int mirror_box(HydSim* h) {
+    const int n = h->N + 3;
+    std::vector<int> lo(n), hi(n);
+    CUDA_TRY(cudaMemcpyAsync(lo.data(), h->g.elo, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(hi.data(), h->g.ehi, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    int r0 = n, r1 = -1, c0 = h->M + 3, c1 = -1;
+    for (int i = 0; i < n; i++) {
+        if (hi[i] < lo[i]) continue;
+        r0 = std::min(r0, i);
+        r1 = std::max(r1, i);
+        c0 = std::min(c0, lo[i]);
+        c1 = std::max(c1, hi[i]);
+    }
+    h->box_r0 = r0;
+    h->box_r1 = r1;
+    h->box_c0 = c0;
+    h->box_c1 = c1;
+    h->box_epoch = h->epoch;
+    return HYD_OK;
+}
+
+int hyd_mirror_open(hyd_handle h, const char* name) {
+    if (!h || !name) return fail(HYD_EINVAL, "null argument");
+    if (strcmp(name, "z") && strcmp(name, "u") && strcmp(name, "v"))
+        return fail(HYD_EINVAL, std::string("mirrors hold z, u or v: ") + name);
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_mirror_open");
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (h->mir_open) {
+        const int rc = hyd_mirror_close(h);
+        if (rc) return rc;
+    }
+    const size_t count = (size_t)(h->N + 3) * (h->M + 3);
+    for (int k = 0; k < 2; k++) {
+        CUDA_TRY(cudaMallocHost(&h->mir[k], count * sizeof(double)));
+        CUDA_TRY(cudaMalloc(&h->mir_snap[k], count * sizeof(double)));
+        CUDA_TRY(cudaEventCreateWithFlags(&h->ev_mir[k], cudaEventDisableTiming));
+    }
+    h->mir_open = 1;
+    h->mir_f = find_field(name);
+    int rc = hyd_get_field(h, name, h->mir[0], count);
+    if (rc) return rc;
+    memcpy(h->mir[1], h->mir[0], count * sizeof(double));
+    h->mir_epoch[0] = h->mir_epoch[1] = h->epoch;
+    h->mir_i = 0;
+    return HYD_OK;
+}
+
+int hyd_mirror_update_async(hyd_handle h, const double** view, size_t* bytes) {
+    if (!h || !view) return fail(HYD_EINVAL, "null argument");
+    if (!h->mir_open) return fail(HYD_ESTATE, "hyd_mirror_open must precede hyd_mirror_update_async");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int k = h->mir_i;
+    // the previous call's copy is complete on return (its view may be read from then on),
+    // and the copy before it, in the slot reused here, with it (the copies run in order)
+    CUDA_TRY(cudaEventSynchronize(h->ev_mir[k ^ 1]));
+    const int W = h->M + 3;
+    const double* src = (const double*)member(h, h->mir_f);
+    size_t moved = 0;
+    if (h->mir_epoch[k] != h->epoch) {
+        // a whole-grid event since this copy was last brought up to date: all of it
+        launch_pack_rows(src, h->pitch, (double*)h->mir_snap[k], h->N + 3, W, h->stream);
+        CUDA_TRY(cudaEventRecord(h->ev_snap, h->stream));
+        CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev_snap, 0));
+        moved = sizeof(double) * (size_t)(h->N + 3) * W;
+        CUDA_TRY(cudaMemcpyAsync(h->mir[k], h->mir_snap[k], moved, cudaMemcpyDeviceToHost, h->copy_stream));
+    } else {
+        if (h->box_epoch != h->epoch || h->box_r1 < 0) {
+            const int rc = mirror_box(h);
+            if (rc) return rc;
+        }
+        if (h->box_r1 >= h->box_r0 && h->box_c1 >= h->box_c0) {
+            const int nr = h->box_r1 - h->box_r0 + 1, nc = h->box_c1 - h->box_c0 + 1;
+            launch_pack_rows(src + (size_t)h->box_r0 * h->pitch + h->box_c0, h->pitch, (double*)h->mir_snap[k], nr, nc,
+                             h->stream);
+            CUDA_TRY(cudaEventRecord(h->ev_snap, h->stream));
+            CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev_snap, 0));
+            CUDA_TRY(cudaMemcpy2DAsync(h->mir[k] + (size_t)h->box_r0 * W + h->box_c0, sizeof(double) * W,
+                                       h->mir_snap[k], sizeof(double) * nc, sizeof(double) * nc, nr,
+                                       cudaMemcpyDeviceToHost, h->copy_stream));
+            moved = sizeof(double) * (size_t)nr * nc;
+        }
+    }
+    CUDA_TRY(cudaEventRecord(h->ev_mir[k], h->copy_stream));
+    h->mir_epoch[k] = h->epoch;
+    h->mir_i = k ^ 1;
+    *view = h->mir[k];
+    if (bytes) *bytes = moved;
+    return HYD_OK;
+}
+
+int hyd_mirror_close(hyd_handle h) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    if (!h->mir_open) return HYD_OK;
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->copy_stream));
+    for (int k = 0; k < 2; k++) {
+        cudaFreeHost(h->mir[k]);
+        cudaFree(h->mir_snap[k]);
+        cudaEventDestroy(h->ev_mir[k]);
+        h->mir[k] = nullptr;
+        h->mir_snap[k] = nullptr;
+        h->ev_mir[k] = nullptr;
+    }
+    h->mir_open = 0;
     return HYD_OK;
 }
 
@@ -822,6 +961,7 @@ static int init_common(HydSim* h, double t_start, int pickup) {
     h->initialized = 1;
     h->force_rescan = 0;  // the set-up scanned every line
     h->full_pending = 3;
+    h->epoch++;
     int rc = refresh_widths(h);
     if (rc) return rc;
     rc = set_clock(h, t_start);
@@ -985,6 +1125,8 @@ int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
         const int full_s = (sed1 || sed2) ? (h->full_pending >> 1) & 1 : 0;
         h->full_pending &= ~(full_h | (full_s << 1));
         const int special = force || full_h || full_s;
+        // channel mode writes levels at table-dependent places every step
+        if (special || h->dp.channel) h->epoch++;
         cudaGraphExec_t exec = (h->use_graphs && !special) ? step_graph(h, mask, h->timing) : nullptr;
         if (exec) {
             CUDA_TRY(cudaGraphLaunch(exec, h->stream));
@@ -1017,6 +1159,7 @@ int hyd_set_params(hyd_handle h, const HydCaseParams* p) {
     h->P = *p;
     h->dp = make_dev_params(h->P);
     h->full_pending = 3;
+    h->epoch++;
     drop_graphs(h);
     return HYD_OK;
 }

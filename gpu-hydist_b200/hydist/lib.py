@@ -45,6 +45,10 @@ def load():
         "hyd_init": (ctypes.c_int, [H, ctypes.c_double]),
         "hyd_get_field_async": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]),
         "hyd_wait_fields": (ctypes.c_int, [H]),
+        "hyd_mirror_open": (ctypes.c_int, [H, ctypes.c_char_p]),
+        "hyd_mirror_update_async": (ctypes.c_int, [H, ctypes.POINTER(ctypes.POINTER(ctypes.c_double)),
+                                                   ctypes.POINTER(ctypes.c_size_t)]),
+        "hyd_mirror_close": (ctypes.c_int, [H]),
         "hyd_update_boundary": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
         "hyd_init_pickup": (ctypes.c_int, [H, ctypes.c_double]),
         "hyd_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
@@ -182,6 +186,23 @@ class Simulation:
 
     def wait_fields(self):
         _check(self.lib.hyd_wait_fields(self.h))
+
+    def mirror_open(self, name="z"):
+        """Keep a host mirror of z, u or v (two library-owned pinned copies, in turn)."""
+        _check(self.lib.hyd_mirror_open(self.h, name.encode()))
+        self._mirror_name = name
+
+    def mirror_update(self):
+        """Bring the next mirror copy up to date after the queued steps; returns (view,
+        bytes moved).  The (N+3)x(M+3) view is complete once the next mirror_update() (or
+        wait_fields()) has returned, and valid until the second later mirror_update()."""
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        n = ctypes.c_size_t()
+        _check(self.lib.hyd_mirror_update_async(self.h, ctypes.byref(ptr), ctypes.byref(n)))
+        return np.ctypeslib.as_array(ptr, shape=(self.N + 3, self.M + 3)), n.value
+
+    def mirror_close(self):
+        _check(self.lib.hyd_mirror_close(self.h))
 
     def update_boundary(self, tables, cc):
         """New values for the boundary tables of set_boundary (same shapes); uploaded in

@@ -138,6 +138,25 @@ int hyd_get_field_async(hyd_handle h, const char* name, void* host, size_t count
 int hyd_wait_fields(hyd_handle h);
 
 /*
+ * Host mirror of "z", "u" or "v": the library keeps two pinned host copies of the field
+ * ((N+3)x(M+3) doubles, row-major like hyd_get_field) and hands them out in turn.
+ * hyd_mirror_open fills both with the field as it is now.  hyd_mirror_update_async,
+ * called after queued steps, brings the next copy up to date on the copy stream while
+ * later steps run and returns it in *view: the copy is complete once the next update
+ * call (or hyd_wait_fields) has returned, and stays valid until the second later update
+ * call.  Between whole-grid events (the
+ * set-up, any hyd_set_field / hyd_set_state / hyd_set_params, a step that ran whole-grid
+ * passes, channel mode) a step changes the field only inside the rows x columns box of
+ * the extended spans, so only that box is copied (*bytes, if given, receives the bytes
+ * moved); after one, the whole field.  One mirror per handle; opening another closes
+ * the first.  No reference counterpart (the reference keeps hourly host lists of u, v,
+ * z, Engine.py:418-420).
+ */
+int hyd_mirror_open(hyd_handle h, const char* name);
+int hyd_mirror_update_async(hyd_handle h, const double** view, size_t* bytes);
+int hyd_mirror_close(hyd_handle h);
+
+/*
  * Boundary tables for all four edges (Global_Variables.py:30-66):
  *   boundary_type: 4 x HYD_SEGMENT_LIMIT int32 (0 wall, 1 stage Z, 2 discharge Q);
  *   tables[e]:     nseg[e] x total_time hourly values of Q or Z (bc_up..bc_right);

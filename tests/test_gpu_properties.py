@@ -103,3 +103,42 @@ def test_update_boundary_changes_forcing():
         assert np.array_equal(a.get(f), b.get(f)), f
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("name", ["z", "u"])
+def test_mirror_matches_sync_reads(name):
+    """hyd_mirror_update_async keeps a host copy equal to the field after every step while
+    copying only the box of cells a span-limited step can change: across whole-grid steps
+    (the first ones, and after a field write) and span-limited ones, with sediment and the
+    Exner update (bed change from t = 10 s on this reach)."""
+    from hydist import cases
+    from hydist.lib import Simulation
+    c = cases.islands_case(N=96, M=72, seed=11, bed_change_start=10.0)
+    a = Simulation.from_case(c)
+    b = Simulation.from_case(c)
+    a.mirror_open(name)
+    full = (c.N + 3) * (c.M + 3) * 8
+    moved = []
+    views = []
+    for k in range(24):
+        a.step(1, sync=False)
+        view, n = a.mirror_update()
+        moved.append(n)
+        b.step(1)
+        want = b.get(name)
+        views.append((view, want))
+        if k >= 1:  # the next update has returned: the copy of update k - 1 is complete
+            v, w = views[k - 1]
+            assert np.array_equal(v, w), (name, k - 1)
+        if k == 12:  # a field write (whole-grid event) in both
+            u = b.get("u")
+            a.set("u", u)
+            b.set("u", u)
+    a.wait_fields()
+    v, w = views[-1]
+    assert np.array_equal(v, w)
+    # whole copies after the set-up and the write, boxes in between
+    assert moved[0] == full and min(moved[3:12]) < full
+    a.mirror_close()
+    a.close()
+    b.close()
