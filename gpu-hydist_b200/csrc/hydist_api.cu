@@ -938,9 +938,14 @@ int hyd_update_boundary(hyd_handle h, const double* const* tables, const double*
         memcpy(h->bnd_stage + (h->g.bc[e] - h->bnd_block), tables[e], n * 8);
         memcpy(h->bnd_stage + (h->g.cc[e] - h->bnd_block), cc[e], n * 8);
     }
-    CUDA_TRY(cudaMemcpyAsync(h->bnd_block, h->bnd_stage, h->bnd_doubles * sizeof(double), cudaMemcpyHostToDevice,
-                             h->stream));
-    CUDA_TRY(cudaEventRecord(h->ev_bnd, h->stream));
+    // small tables travel in a kernel's parameters (no copy engine, and the staging copy is
+    // free again at once); larger ones as one copy, which the next call waits for
+    if (!launch_put_doubles(h->bnd_block, h->bnd_stage, (int)h->bnd_doubles, h->stream)) {
+        CUDA_TRY(cudaMemcpyAsync(h->bnd_block, h->bnd_stage, h->bnd_doubles * sizeof(double), cudaMemcpyHostToDevice,
+                                 h->stream));
+        CUDA_TRY(cudaEventRecord(h->ev_bnd, h->stream));
+    }
+    CUDA_TRY(cudaGetLastError());
     return HYD_OK;
 }
 

@@ -244,6 +244,10 @@ void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s);
 void launch_reset_rows(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_reset_cols(const DevGrid& g, const DevParams& p, int force, int threads, cudaStream_t s);
 void launch_spans(const DevGrid& g, cudaStream_t s);
+// n <= kPutDoubles values from host memory to dst through the launch parameters (returns
+// 0, launching nothing, when n is out of range)
+constexpr int kPutDoubles = 480;
+int launch_put_doubles(double* dst, const double* src, int n, cudaStream_t s);
 // rows x cols doubles of a pitched array into a packed one
 void launch_pack_rows(const double* src, int pitch, double* dst, int rows, int cols, cudaStream_t s);
 void clear_rescan_lists(const DevGrid& g, cudaStream_t s);

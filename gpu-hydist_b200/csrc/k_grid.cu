@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 
 #include "hydist_dev.cuh"
 
@@ -1769,6 +1770,25 @@ void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, 
     k_qb<<<grid2d(g.M - 1, g.N - 1, b), b, 0, s>>>(g, p);
     if (endidx > startidx) k_bedload<<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
     hyd_kernel_launches_add(2);
+}
+
+// Up to kPutDoubles values carried in the launch's parameters into dst[0..n): a small
+// upload in order with the stream's kernels that takes no copy engine (those may be busy
+// with a device-to-host copy of an earlier step).
+struct PutDoubles {
+    double v[kPutDoubles];
+};
+__global__ void k_put_doubles(double* __restrict__ dst, int n, PutDoubles pl) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = pl.v[i];
+}
+
+int launch_put_doubles(double* dst, const double* src, int n, cudaStream_t s) {
+    if (n < 0 || n > kPutDoubles) return 0;
+    PutDoubles pl;
+    memcpy(pl.v, src, sizeof(double) * n);
+    k_put_doubles<<<1, 256, 0, s>>>(dst, n, pl);
+    hyd_kernel_launches_add(1);
+    return 1;
 }
 
 void launch_pack_rows(const double* src, int pitch, double* dst, int rows, int cols, cudaStream_t s) {
