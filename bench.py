@@ -180,6 +180,27 @@ def span_cells(sim, halo=4):
     return core, span
 
 
+def reference_kernels_sample(case, spin, n):
+    """The reference's own kernels on this GPU (oracle/_ref/libhydref_gpu.so: its kernel
+    sources built for sm_100a, launched as its host launches them): spun up untimed, then
+    n steps timed by the harness's CUDA events.  None when that build is absent."""
+    import oracle
+    path = os.path.join(ROOT, "oracle", "_ref", "libhydref_gpu.so")
+    if not os.path.exists(path):
+        return None
+    rs = oracle.RefSim(case, gpu=True)
+    try:
+        rs.init()
+        rs.step(spin)
+        t0 = rs.t
+        rs.step(n)
+        return {"value": case.N * case.M * n / (rs.last_ms / 1e3), "unit": "cell-updates/s", "steps": n,
+                "sample": "the reference's kernels (its sources built for sm_100a, launched as Engine.py launches "
+                          "them) on this GPU, %d steps from t=%.0f s after an untimed spin-up" % (n, t0)}
+    finally:
+        rs.close()
+
+
 def cpu_port_sample(case, state_get, t0, hmax, budget_s=12.0):
     """Time the oracle port (OpenMP, all host cores) from the GPU's state."""
     import oracle
@@ -388,6 +409,10 @@ def run_ours(args, rank, world, local_rank):
                    "kind": "port",
                    "sample": "%d ADI steps of the %dx%d reach from t=%.0f s (the GPU state), oracle port "
                              "(OpenMP, %d threads), %.1f s wall" % (n_cpu, N, M, st_t, os.cpu_count(), el)}
+        ref_gpu = None
+        if world == 1 and not args.no_reference_gpu:
+            # sediment active from t = 1800 s, as in the timed steps
+            ref_gpu = reference_kernels_sample(case, int(round(1800 / case.params.dT)) + 5, 20)
         clocks = clk.summary()
         result = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -425,6 +450,7 @@ def run_ours(args, rank, world, local_rank):
                               "frac": value * 208 / 1e9 / world / peak},
             "phases": phases,
             "cpu_baseline": cpu,
+            "reference_kernels_gpu": ref_gpu,
             "clocks": clocks,
             "gpu_launches": launches,
         }
@@ -483,6 +509,8 @@ def main():
     ap.add_argument("--spinup", type=int, default=SPINUP_STEPS,
                     help="untimed steps before the warm-up (default: to t = 3590 s, sediment active)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own kernels on the GPU (oracle/_ref/libhydref_gpu.so)")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS),
                     help="config2 (the default: the 1048x980 reach) or config4 (the 4096x2048 reach)")
     args = ap.parse_args()
