@@ -15,8 +15,11 @@ steps without the flush (how a simulation runs) is reported beside it.
 
 --impl ours       the CUDA library; prints value (device-resident), e2e (through the C
                   ABI from pinned host buffers: the boundary forcing in and the water
-                  level out every step; the whole-state round trip beside it), roofline
-                  of the dominant phase, cpu_baseline (the oracle port on the host cores).
+                  level out every step, through the library's host mirror of z;
+                  e2e_full_field copies every cell of z instead, e2e_state_roundtrip the
+                  whole state both ways), roofline of the dominant phase, cpu_baseline
+                  (the oracle port on the host cores) and reference_kernels_gpu (the
+                  reference's own kernels, built for sm_100a, on the same GPU).
 --impl reference  the same scheme on the host cores: the reference has no CPU
                   implementation of this path, so this times the oracle port (a line-for-
                   line C restatement of the reference's kernels, OpenMP) on a bounded sample.
