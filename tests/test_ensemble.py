@@ -137,3 +137,25 @@ def test_gpu_ensemble_streams_match_single_handles(oracle_lib):
         for f in ("z", "u", "v"):
             e = rel_linf(got[i][f], o.get(f))
             assert e <= REL_TOL, "reach %d %s rel L-inf %.3e" % (i, f, e)
+
+
+def test_gpu_batch_realistic_reaches_vs_oracle(oracle_lib):
+    """Batch members sized for throughput sweep every line of up to 288 rows by a warp,
+    where a lone handle hands lines over 96 rows to the whole CTA: reaches of config 3's
+    sizes (lines of a few hundred rows) against the oracle within 1e-9."""
+    from helpers import REL_TOL, rel_linf
+    from hydist import cases
+    from hydist.ensemble import Ensemble
+    import oracle
+    cs = cases.config3_cases(n=3, seed=17, nx_range=(300, 500), ny_range=(150, 260), hours=1.0, spinup_h=0.1)
+    ens = Ensemble(cs, rank=0, world=1)
+    ens.step(20)
+    got = ens.fields(("z", "u", "v", "FS"))
+    ens.close()
+    for i, c in enumerate(cs):
+        o = oracle.OracleSim(c)
+        o.init()
+        o.step(20)
+        for f in ("z", "u", "v", "FS"):
+            e = rel_linf(got[i][f], o.get(f))
+            assert e <= REL_TOL, "reach %d %s rel L-inf %.3e" % (i, f, e)
