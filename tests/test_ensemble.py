@@ -139,6 +139,7 @@ def test_gpu_ensemble_streams_match_single_handles(oracle_lib):
             assert e <= REL_TOL, "reach %d %s rel L-inf %.3e" % (i, f, e)
 
 
+@pytest.mark.gpu
 def test_gpu_batch_realistic_reaches_vs_oracle(oracle_lib):
     """Batch members sized for throughput sweep every line of up to 288 rows by a warp,
     where a lone handle hands lines over 96 rows to the whole CTA: reaches of config 3's
