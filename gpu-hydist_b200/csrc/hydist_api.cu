@@ -72,6 +72,7 @@ struct HydSim {
     double* sweep_scratch;  // rows/cells of lines too long for shared memory
     double* fs_scratch;     // the same for the sediment sweeps (which may run beside the others)
     SweepPlan plan;         // launch shapes of the sweeps
+    int plan_grid;          // the sweeps' CTAs as planned at creation (the most allowed)
     void* arena;
     size_t arena_bytes;
     std::vector<void*> extra;
@@ -599,6 +600,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         // send lines of a moderate grid through the global-scratch sweeps
         const char* rv = getenv("HYD_SWEEP_ROWS");
         e = sweep_plan(N, M, &s->plan, rv ? atoi(rv) : 0);
+        s->plan_grid = s->plan.long_grid;
     }
     if (e == cudaSuccess) e = grid_setup(N, M);
     if (e != cudaSuccess) {
@@ -1386,6 +1388,25 @@ int hyd_launch_count(hyd_handle h, long long* count) {
 struct HydBatch {
     std::vector<hyd_handle> members;
 };
+
+int hyd_set_sweep_shape(hyd_handle h, int ctas, int wide) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    if (ctas < 0 || (wide != 0 && wide != 1)) return fail(HYD_EINVAL, "ctas must be >= 0 and wide 0 or 1");
+    const int g = ctas == 0 || ctas > h->plan_grid ? h->plan_grid : ctas;
+    if (g != h->plan.long_grid || wide != h->plan.wide) {
+        h->plan.long_grid = g;
+        h->plan.wide = wide;
+        drop_graphs(h);
+    }
+    return HYD_OK;
+}
+
+int hyd_get_sweep_shape(hyd_handle h, int* ctas, int* wide) {
+    if (!h || !ctas || !wide) return fail(HYD_EINVAL, "null argument");
+    *ctas = h->plan.long_grid;
+    *wide = h->plan.wide;
+    return HYD_OK;
+}
 
 int hyd_batch_create(int count, const HydCaseParams* params, const int* dims, int device, hyd_batch* out) {
     if (!params || !dims || !out || count < 1) return fail(HYD_EINVAL, "batch: null argument or empty batch");

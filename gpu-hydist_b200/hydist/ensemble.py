@@ -10,7 +10,7 @@ gathered on rank 0.
     partition(costs, world)        -> per-rank lists of reach indices (largest first,
                                       each to the least loaded rank)
     Ensemble(cases, rank, world)   -> the rank's reaches (one library batch); .step(n),
-                                      .cell_updates(n)
+                                      .cell_updates(n), .tune(steps) (hydist.tune)
     max_over_ranks(x)              -> max of a host float over the process group
 """
 import heapq
@@ -63,6 +63,14 @@ class Ensemble:
         except Exception:
             self.close()
             raise
+
+    def tune(self, steps=20, candidates=None):
+        """Pick the batch's sweep launch shape by timing (hydist.tune.tune_batch); the
+        tuning steps advance the reaches like step().  Returns (policy, timings)."""
+        if self.batch is None:
+            return None, {}
+        from .tune import DEFAULT_CANDIDATES, tune_batch
+        return tune_batch(self.batch, candidates or DEFAULT_CANDIDATES, steps)
 
     def step(self, n=1, sync=True):
         """Advance every owned reach n steps (their launches queued on one stream per

@@ -72,6 +72,8 @@ def load():
         "hyd_batch_member": (ctypes.c_int, [H, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
         "hyd_batch_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int]),
         "hyd_batch_destroy": (ctypes.c_int, [H]),
+        "hyd_set_sweep_shape": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int]),
+        "hyd_get_sweep_shape": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -203,6 +205,15 @@ class Simulation:
 
     def mirror_close(self):
         _check(self.lib.hyd_mirror_close(self.h))
+
+    def set_sweep_shape(self, ctas, wide):
+        """Sweep CTAs (0: one per SM) and whether warps take every line up to 288 rows."""
+        _check(self.lib.hyd_set_sweep_shape(self.h, int(ctas), int(wide)))
+
+    def sweep_shape(self):
+        c, w = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.hyd_get_sweep_shape(self.h, ctypes.byref(c), ctypes.byref(w)))
+        return c.value, w.value
 
     def update_boundary(self, tables, cc):
         """New values for the boundary tables of set_boundary (same shapes); uploaded in

@@ -303,6 +303,18 @@ int hyd_batch_member(hyd_batch b, int k, hyd_handle* h);
 int hyd_batch_step(hyd_batch b, int nsteps, int sync);
 int hyd_batch_destroy(hyd_batch b);
 
+/*
+ * Launch shape of a handle's line sweeps: `ctas` persistent CTAs (0 or more than planned:
+ * the planned number, one per SM), and with `wide` = 1 every line a warp's shared-memory
+ * slice holds (up to 288 rows) swept by a warp rather than only lines of up to 96 rows.
+ * Batch members start at ceil((max(N, M) + 3) / 16) CTAs, wide.  Changing the shape
+ * drops the captured step graphs (the next step captures anew).  Results do not depend
+ * on the shape beyond rounding (within the parity tolerance).  No reference counterpart
+ * (the reference launches one block per line); hydist.tune picks shapes by timing.
+ */
+int hyd_set_sweep_shape(hyd_handle h, int ctas, int wide);
+int hyd_get_sweep_shape(hyd_handle h, int* ctas, int* wide);
+
 #ifdef __cplusplus
 }
 #endif

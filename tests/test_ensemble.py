@@ -160,3 +160,69 @@ def test_gpu_batch_realistic_reaches_vs_oracle(oracle_lib):
         for f in ("z", "u", "v", "FS"):
             e = rel_linf(got[i][f], o.get(f))
             assert e <= REL_TOL, "reach %d %s rel L-inf %.3e" % (i, f, e)
+
+
+def test_tune_policy_shapes_on_cpu_fake():
+    """The tuner's bookkeeping with a fake batch: each candidate sets every member's shape,
+    the fastest (by the injected clock) is applied last and returned."""
+    from hydist import tune
+
+    class FakeSim:
+        def __init__(self, N, M):
+            self.N, self.M, self.shape = N, M, None
+
+        def set_sweep_shape(self, ctas, wide):
+            self.shape = (ctas, wide)
+
+    class FakeBatch:
+        def __init__(self):
+            self.members = [FakeSim(100, 60), FakeSim(40, 300)]
+            self.log = []
+
+        def step(self, n, sync=True):
+            self.log.append((n, self.members[0].shape))
+
+    costs = {(16, 1): 3.0, (8, 1): 1.0, (16, 0): 2.0}
+    b = FakeBatch()
+    t = [0.0]
+
+    def clock():
+        # advance by the cost of the shape the last timed step ran with
+        if b.log and b.log[-1][0] == 5:
+            d = next(p for p in costs if b.members[0].shape == (max(1, -(-103 // p[0])), p[1]))
+            t[0] += costs[d] * 5
+        return t[0]
+
+    best, times = tune.tune_batch(b, candidates=list(costs), steps=5, warm=1, clock=clock)
+    assert best == (8, 1)
+    assert b.members[0].shape == (13, 1) and b.members[1].shape == (38, 1)  # ceil(103/8), ceil(303/8)
+    assert abs(times[(8, 1)] - 1.0) < 1e-12 and abs(times[(16, 1)] - 3.0) < 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_tuned_batch_vs_oracle(oracle_lib):
+    """The online tuner steps the batch under several sweep shapes and keeps one; the
+    reaches still match the oracle within 1e-9 after the tuning steps and more."""
+    from helpers import REL_TOL, rel_linf
+    from hydist import cases
+    from hydist.ensemble import Ensemble
+    import oracle
+    cs = cases.config3_cases(n=3, seed=17, nx_range=(300, 500), ny_range=(150, 260), hours=1.0, spinup_h=0.1)
+    ens = Ensemble(cs, rank=0, world=1)
+    best, times = ens.tune(steps=3, candidates=((16, 1), (4, 0)))
+    assert best in times and len(times) == 2
+    n_tuned = 2 * (2 + 3)  # warm + timed steps per candidate
+    ens.step(4)
+    got = ens.fields(("z", "u", "v", "FS"))
+    shapes = [m.sweep_shape() for m in ens.batch.members]
+    ens.close()
+    d, wide = best
+    for c, sh in zip(cs, shapes):
+        assert sh == (min(sh[0], -(-(max(c.N, c.M) + 3) // d)), wide)
+    for i, c in enumerate(cs):
+        o = oracle.OracleSim(c)
+        o.init()
+        o.step(n_tuned + 4)
+        for f in ("z", "u", "v", "FS"):
+            e = rel_linf(got[i][f], o.get(f))
+            assert e <= REL_TOL, "reach %d %s rel L-inf %.3e" % (i, f, e)
