@@ -1,7 +1,7 @@
 """Comparison helpers shared by the parity tests."""
 import numpy as np
 
-# north_star tolerance for the plain FP64 form: relative L-infinity against the reference
+# parity tolerance of the plain FP64 form: relative L-infinity against the reference
 REL_TOL = 1e-9
 PARITY_FIELDS = ("z", "u", "v", "t_z", "t_u", "t_v", "FS", "dH", "H_moi", "Htdu", "Htdv")
 EXACT_FIELDS = ("khouot", "moci", "mocj", "daui", "cuoii", "dauj", "cuoij")
