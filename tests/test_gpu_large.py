@@ -74,6 +74,26 @@ def test_gpu_config4_resume_vs_oracle(oracle_lib, config4, monkeypatch):
         sim.close()
 
 
+def test_gpu_config4_bed_update_vs_oracle(oracle_lib, config4, monkeypatch):
+    """The bench's window on config 4: the GPU runs to t = 3590 s, the oracle resumes from
+    the GPU's state and both run across the Exner update at t = 3600 s."""
+    import oracle
+    from hydist.lib import Simulation
+    monkeypatch.delenv("HYD_SWEEP_ROWS", raising=False)
+    monkeypatch.delenv("HYD_SOLVER", raising=False)
+    sim = Simulation.from_case(config4)
+    try:
+        sim.step(3590)
+        ora = oracle.OracleSim(config4)
+        ora.load_state(sim.get, sim.t, sim.get("hmax"))
+        sim.step(12)
+        ora.step(12)
+        _check(sim, ora, "config4 t=%g" % ora.t)
+        assert np.abs(sim.get("dH")).max() > 0  # the bed update ran
+    finally:
+        sim.close()
+
+
 def test_gpu_global_scratch_sweeps_vs_oracle(oracle_lib, monkeypatch):
     """Config 2 with at most 512 rows of a line in shared memory: its long columns (up to
     about 1,300 rows) and long sediment lines run in the sweep CTAs' global scratch
