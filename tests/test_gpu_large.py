@@ -89,7 +89,8 @@ def test_gpu_config4_bed_update_vs_oracle(oracle_lib, config4, monkeypatch):
         sim.step(12)
         ora.step(12)
         _check(sim, ora, "config4 t=%g" % ora.t)
-        assert np.abs(sim.get("dH")).max() > 0  # the bed update ran
+        dH = sim.get("dH")
+        assert np.abs(dH[np.isfinite(dH)]).max() > 0  # the bed update ran
     finally:
         sim.close()
 
