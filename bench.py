@@ -84,6 +84,9 @@ SIDE_PHASES = ("coef_fsj", "fs_sweep_j")
 # (ncu -k regex:k_hydro_sweep -s 6 -c 2: the 7th launch of the sweep kernel, the UZ sweep).
 NCU_TRAFFIC = {
     "config2": {"sweep_uz": (2192640, 30650)},
+    # config 4: the VZ sweep of the fourth step of python bench.py --workload config4
+    # --spinup 0 --steps 3 --warmup 3 --no-cpu-baseline (ncu -k regex:k_hydro_sweep -s 6 -c 2)
+    "config4": {"sweep_vz": (32254200 + 61696, 486100)},
 }
 
 
