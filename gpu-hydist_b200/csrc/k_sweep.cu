@@ -46,8 +46,11 @@ constexpr int kRowShortF = 64;
 // continuity coefficients (a, c, d) of the first and last cell of every segment of a
 // hydrodynamic line, kept for the extraction: 6 doubles per segment
 constexpr int kEnds = 6 * HYD_SEGL;
-constexpr int kWarpHydro = 4 * kRowW + kEnds;  // doubles per warp
+constexpr int kWarpHydro = 4 * kRowW + kEnds;  // doubles per warp (the largest slice)
 constexpr int kWarpFs = 4 * kRowW;
+constexpr int kRowSlice = 96;  // rows of a slice when warps take lines of up to kRowShort (kRowShortF) rows
+// rows of a warp's slice for a launch whose warps take lines of up to roww rows
+__host__ __device__ inline int slice_rows(int roww) { return roww > kRowSlice ? kRowW : kRowSlice; }
 static_assert(kRowW % 32 == 0 && (kRowW / 32) % 2 == 1, "a warp solve pads R <= kRowW rows to 32 chunk_len(R, 32) <= kRowW");
 
 // A group of threads that sweeps one line: a warp, or a whole CTA for a long line.
@@ -626,11 +629,12 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
             if (sg.R > roww) {
                 if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
             } else {
-                double* A = dyn_smem + w * kWarpHydro;
-                double* B = A + kRowW;
-                double* Cc = B + kRowW;
-                double* D = Cc + kRowW;
-                hydro_body<DIR, SOLVER, WarpG>(g, p, startidx + li, sg, A, B, Cc, D, D + kRowW, nullptr,
+                const int wr = slice_rows(roww);
+                double* A = dyn_smem + w * (4 * wr + kEnds);
+                double* B = A + wr;
+                double* Cc = B + wr;
+                double* D = Cc + wr;
+                hydro_body<DIR, SOLVER, WarpG>(g, p, startidx + li, sg, A, B, Cc, D, D + wr, nullptr,
                                                SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
@@ -896,8 +900,9 @@ __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int
             if (sg.R > roww) {
                 if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
             } else {
-                double* A = dyn_smem + w * kWarpFs;
-                fs_body<DIR, SOLVER, WarpG>(g, p, half, startidx + li, sg, A, A + kRowW, A + 2 * kRowW, A + 3 * kRowW,
+                const int wr = slice_rows(roww);
+                double* A = dyn_smem + w * 4 * wr;
+                fs_body<DIR, SOLVER, WarpG>(g, p, half, startidx + li, sg, A, A + wr, A + 2 * wr, A + 3 * wr,
                                             nullptr, SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
@@ -1033,7 +1038,11 @@ void hydro_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan&
     if (nlines <= 0) return;
     const int sv = solver ? 1 : 0;
     const int roww = (sp.wide || nlines > kWL * sp.long_grid) ? kRowW : kRowShort;
-    kHydroSweep[dir][sv]<<<sp.long_grid, kTL, sp.smem_lines, s>>>(g, p, startidx, endidx, sp.RB, scratch, sp.RG, roww);
+    // the long-line rows or the warps' slices, whichever is larger (a smaller request
+    // leaves more of the SM's on-chip memory to L1)
+    const size_t big = 4 * (size_t)sp.RB + kEnds, slices = (size_t)kWL * (4 * slice_rows(roww) + kEnds);
+    const size_t smem = sizeof(double) * (big > slices ? big : slices);
+    kHydroSweep[dir][sv]<<<sp.long_grid, kTL, smem, s>>>(g, p, startidx, endidx, sp.RB, scratch, sp.RG, roww);
     hyd_kernel_launches_add(1);
 }
 
@@ -1043,7 +1052,9 @@ void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp
     if (nlines <= 0) return;
     const int sv = solver ? 1 : 0;
     const int roww = (sp.wide || nlines > kWL * sp.long_grid) ? kRowW : kRowShortF;
-    kFsSweep[dir][sv]<<<sp.long_grid, kTL, sp.smem_fs_lines, s>>>(g, p, half, startidx, endidx, sp.RBf, scratch,
+    const size_t big = 4 * (size_t)sp.RBf, slices = (size_t)kWL * 4 * slice_rows(roww);
+    const size_t smem = sizeof(double) * (big > slices ? big : slices);
+    kFsSweep[dir][sv]<<<sp.long_grid, kTL, smem, s>>>(g, p, half, startidx, endidx, sp.RBf, scratch,
                                                                    sp.RGf, roww);
     hyd_kernel_launches_add(1);
 }
