@@ -145,3 +145,22 @@ def test_gpu_config2_fields_set_mid_run_vs_oracle(oracle_lib, monkeypatch):
     sim.step(5)
     ora.step(5)
     _check(sim, ora.get, "after the whole-grid pass t=%g" % ora.t)
+
+
+def test_gpu_config2_full_horizon_vs_oracle(oracle_lib, monkeypatch):
+    """Config 2 over its whole stated horizon (the 1 h ramp and 6 h: 25 200 steps, sediment
+    from t = 1800 s, seven Exner updates) against the oracle on all host cores, compared
+    every two simulated hours and at the end (about two minutes, mostly the oracle)."""
+    import os
+    import oracle
+    from hydist import cases
+    c = cases.config2_case()
+    sim = _sim(c, "partitioned", monkeypatch)
+    ora = oracle.OracleSim(c, threads=os.cpu_count() or 1)
+    ora.init()
+    for n in (7200, 7200, 7200, 3600):
+        sim.step(n)
+        ora.step(n)
+        _check(sim, ora.get, "config2 t=%g" % ora.t, fields=("z", "u", "v", "t_z", "t_u", "t_v", "H_moi", "FS",
+                                                               "dH", "khouot", "moci", "mocj"))
+    sim.close()
