@@ -89,6 +89,12 @@ NCU_TRAFFIC = {
     "config4": {"sweep_vz": (32254200 + 61696, 486100)},
 }
 
+# DRAM bytes of one whole timed step (dram__bytes_read.sum + dram__bytes_write.sum summed
+# over the step's launches, the L2-flush kernels left out) from an ncu launch list of the
+# timed steps; the summary, with its command, is the file named in "source".  Filled from
+# captures of the current kernels; absent workloads print no step_dram.
+STEP_DRAM = {}
+
 
 def load_peaks():
     try:
@@ -223,14 +229,17 @@ def cpu_port_sample(case, state_get, t0, hmax, budget_s=12.0):
     return steps, el
 
 
-def run_ours(args, rank, world, local_rank):
+def run_ours(args, rank, world, local_rank, workload, secondary=False):
+    """One workload's measurement.  secondary: the extra workload printed beside the
+    default one (its value, back-to-back rate, roofline, level-mirror e2e and a short CPU
+    sample; not the heavier e2e variants nor the reference's kernels)."""
     import numpy as np
     import torch
     from hydist import cases
     from hydist.lib import Simulation
 
     torch.cuda.set_device(local_rank)
-    case = getattr(cases, WORKLOADS[args.workload][0])()
+    case = getattr(cases, WORKLOADS[workload][0])()
     N, M = case.N, case.M
     cells = N * M
     sim = Simulation.from_case(case, device=local_rank)
@@ -312,7 +321,7 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = load_peaks()
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
     traffic = None
-    captured = NCU_TRAFFIC.get(args.workload, {})
+    captured = NCU_TRAFFIC.get(workload, {})
     if dom_name in captured:
         tb, tw = captured[dom_name]
         traffic = int(round(tb * units["wet"] / tw))
@@ -380,28 +389,30 @@ def run_ours(args, rank, world, local_rank):
     sim.mirror_close()
     d2h_bytes = moved / e2e_steps
     e2e_value = world * cells * e2e_steps / (e2e_ms / 1e3)
-    full_loop(max(args.warmup, 3))
-    full_ms, _ = timed_max(lambda: full_loop(e2e_steps))
-    full_value = world * cells * e2e_steps / (full_ms / 1e3)
+    full_value = rt_value = None
+    field_bytes = (N + 3) * (M + 3) * 8 * 4
+    if not secondary:
+        full_loop(max(args.warmup, 3))
+        full_ms, _ = timed_max(lambda: full_loop(e2e_steps))
+        full_value = world * cells * e2e_steps / (full_ms / 1e3)
 
-    # the heavier round trip for reference: the whole state (z, u, v, FS) in and out
-    names = ("z", "u", "v", "FS")
-    host = {f: torch.empty((N + 3, M + 3), dtype=torch.float64, pin_memory=True) for f in names}
-    for f in names:
-        sim.get(f, out=host[f].numpy())
+        # the heavier round trip for reference: the whole state (z, u, v, FS) in and out
+        names = ("z", "u", "v", "FS")
+        host = {f: torch.empty((N + 3, M + 3), dtype=torch.float64, pin_memory=True) for f in names}
+        for f in names:
+            sim.get(f, out=host[f].numpy())
 
-    def roundtrip_loop(n):
-        for _ in range(n):
-            for f in names:
-                sim.set(f, host[f].numpy())
-            sim.step(1, sync=False)
-            for f in names:
-                sim.get(f, out=host[f].numpy())
+        def roundtrip_loop(n):
+            for _ in range(n):
+                for f in names:
+                    sim.set(f, host[f].numpy())
+                sim.step(1, sync=False)
+                for f in names:
+                    sim.get(f, out=host[f].numpy())
 
-    roundtrip_loop(max(args.warmup, 3))
-    rt_ms, _ = timed_max(lambda: roundtrip_loop(e2e_steps))
-    field_bytes = (N + 3) * (M + 3) * 8 * len(names)
-    rt_value = world * cells * e2e_steps / (rt_ms / 1e3)
+        roundtrip_loop(max(args.warmup, 3))
+        rt_ms, _ = timed_max(lambda: roundtrip_loop(e2e_steps))
+        rt_value = world * cells * e2e_steps / (rt_ms / 1e3)
 
     result = None
     if rank == 0:
@@ -410,13 +421,14 @@ def run_ours(args, rank, world, local_rank):
             st_t = sim.t
             hmax = sim.get("hmax")
             snap = {f: sim.get(f) for f in __import__("oracle").OracleSim.STATE_FIELDS}
-            n_cpu, el = cpu_port_sample(case, lambda f: snap[f], st_t, hmax, budget_s=args.cpu_seconds)
+            budget = args.cpu_seconds if not secondary else min(args.cpu_seconds, 6.0)
+            n_cpu, el = cpu_port_sample(case, lambda f: snap[f], st_t, hmax, budget_s=budget)
             cpu = {"value": cells * n_cpu / el, "unit": "cell-updates/s", "cores": os.cpu_count(),
                    "kind": "port",
                    "sample": "%d ADI steps of the %dx%d reach from t=%.0f s (the GPU state), oracle port "
                              "(OpenMP, %d threads), %.1f s wall" % (n_cpu, N, M, st_t, os.cpu_count(), el)}
         ref_gpu = None
-        if world == 1 and not args.no_reference_gpu:
+        if world == 1 and not args.no_reference_gpu and not secondary:
             # sediment active from t = 1800 s, as in the timed steps
             ref_gpu = reference_kernels_sample(case, int(round(1800 / case.params.dT)) + 5, 20)
         clocks = clk.summary()
@@ -424,12 +436,13 @@ def run_ours(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": WORKLOADS[args.workload][2],
-            "config": {"workload": "%s, t=%d..%d s" % (WORKLOADS[args.workload][1], args.spinup + 2 * args.warmup,
+            "data": WORKLOADS[workload][2],
+            "config": {"workload": "%s, t=%d..%d s" % (WORKLOADS[workload][1], args.spinup + 2 * args.warmup,
                                                         args.spinup + 2 * args.warmup + args.steps),
                        "grid": [N, M], "cells": cells, "wet_cells": wet,
                        "parallelism": "replicas%d" % world if world > 1 else "single",
                        "core_cells": core, "span_cells": span,
+                       "touched_fraction": span / cells,
                        "l2": "256 MB written before every timed step (flush); steps timed one by one"},
             "back_to_back": {"value": world * cells * args.steps / (warm_ms / 1e3), "ms_per_step": warm_ms / args.steps,
                              "l2": "no flush between steps"},
@@ -439,14 +452,6 @@ def run_ours(args, rank, world, local_rank):
                            "hyd_mirror_update_async(z): a full host copy of z after every step (checked equal "
                            "to hyd_get_field at the end: %s), only the box of cells a step can change copied, "
                            "while the next step runs" % mirror_exact},
-            "e2e_full_field": {"value": full_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d_bytes,
-                               "d2h_bytes_per_step": (N + 3) * (M + 3) * 8, "steps": e2e_steps,
-                               "api": "as e2e, with every cell of z copied every step (hyd_get_field_async into "
-                                      "two pinned buffers in turn)"},
-            "e2e_state_roundtrip": {"value": rt_value, "unit": "cell-updates/s", "h2d_bytes_per_step": field_bytes,
-                                    "d2h_bytes_per_step": field_bytes, "steps": e2e_steps,
-                                    "api": "hyd_set_field(z,u,v,FS) + hyd_step(1) + hyd_get_field(z,u,v,FS), "
-                                           "pinned host buffers"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_launch": bytes_per_launch, "bytes_unit": "%d B x %d %s cells" % (
@@ -460,6 +465,30 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clocks,
             "gpu_launches": launches,
         }
+        if full_value is not None:
+            result.update({
+                    "e2e_full_field": {"value": full_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d_bytes,
+                                       "d2h_bytes_per_step": (N + 3) * (M + 3) * 8, "steps": e2e_steps,
+                                       "api": "as e2e, with every cell of z copied every step (hyd_get_field_async into "
+                                              "two pinned buffers in turn)"},
+                    "e2e_state_roundtrip": {"value": rt_value, "unit": "cell-updates/s", "h2d_bytes_per_step": field_bytes,
+                                            "d2h_bytes_per_step": field_bytes, "steps": e2e_steps,
+                                            "api": "hyd_set_field(z,u,v,FS) + hyd_step(1) + hyd_get_field(z,u,v,FS), "
+                                                   "pinned host buffers"},
+            })
+        dram = STEP_DRAM.get(workload)
+        if dram:
+            # the whole step's DRAM bytes as ncu counted them (every launch of a timed step),
+            # against the step time of this run: what the step moves, not what it models
+            b = dram["bytes_per_step"]
+            result["step_dram"] = {"bytes_per_step": b, "achieved": b / (ms / args.steps / 1e3) / 1e9,
+                                   "peak": peak, "unit": "GB/s",
+                                   "frac": b / (ms / args.steps / 1e3) / 1e9 / peak,
+                                   "source": dram["source"]}
+        result["step_roofline"]["note"] = (
+            "modelled: 208 B per cell-update charged to all %d cells, while the step's kernels touch "
+            "%d cells (%.1f %%, touched_fraction); step_dram is the measured traffic" % (cells, span, 100.0 * span / cells))
+        result["roofline"]["traffic_kind"] = "modelled from the ncu capture in NCU_TRAFFIC, scaled by wet cells"
     sim.close()
     return result
 
@@ -504,6 +533,18 @@ def run_reference(args, rank):
     }
 
 
+def relaunch_under_torchrun(n):
+    """--gpus N > 1 without a launcher: run this command under torch.distributed.run with N
+    ranks (one per GPU), so that the flag is never silently ignored."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -519,10 +560,18 @@ def main():
                     help="skip timing the reference's own kernels on the GPU (oracle/_ref/libhydref_gpu.so)")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS),
                     help="config2 (the default: the 1048x980 reach) or config4 (the 4096x2048 reach)")
+    ap.add_argument("--secondary", default="config4", choices=sorted(WORKLOADS) + ["none"],
+                    help="a second workload measured in the same run and printed under 'workloads' "
+                         "(default config4; 'none' skips it)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(relaunch_under_torchrun(args.gpus))
+    if args.gpus != world:
+        sys.stderr.write("bench.py: --gpus %d but WORLD_SIZE=%d ranks; launch one rank per GPU\n" % (args.gpus, world))
+        sys.exit(2)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -535,7 +584,11 @@ def main():
         import torch
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        res = run_ours(args, rank, world, local_rank)
+        res = run_ours(args, rank, world, local_rank, args.workload)
+        if args.secondary not in ("none", args.workload):
+            res2 = run_ours(args, rank, world, local_rank, args.secondary, secondary=True)
+            if res is not None:
+                res["workloads"] = {args.secondary: res2}
     finally:
         if world > 1:
             import torch

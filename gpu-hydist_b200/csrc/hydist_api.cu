@@ -376,6 +376,22 @@ constexpr int kMaxDevices = 64;
 double* g_mass_scratch_ptr[kMaxDevices];
 std::mutex g_mass_scratch_mu;
 
+// The device address of g_mass_scratch on `device` (current), looked up once per device.
+// The lookup loads this file's module on that device (with lazy module loading it is not
+// loaded before), which places the array in device memory: hyd_create does it, so that a
+// later hyd_mass_balance_noalloc call finds the module loaded and allocates nothing.
+cudaError_t mass_scratch_address(int device, double** out) {
+    std::lock_guard<std::mutex> lock(g_mass_scratch_mu);
+    if (!g_mass_scratch_ptr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_mass_scratch);
+        if (e != cudaSuccess) return e;
+        g_mass_scratch_ptr[device] = (double*)p;
+    }
+    *out = g_mass_scratch_ptr[device];
+    return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
@@ -603,6 +619,12 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
         s->plan_grid = s->plan.long_grid;
     }
     if (e == cudaSuccess) e = grid_setup(N, M);
+    if (e == cudaSuccess && device < kMaxDevices) {
+        // the fixed scratch of hyd_mass_balance_noalloc: its module is loaded now, while
+        // creating a handle allocates anyway
+        double* scratch = nullptr;
+        e = mass_scratch_address(device, &scratch);
+    }
     if (e != cudaSuccess) {
         release(s);
         return fail(HYD_ECUDA, std::string("shared-memory set-up: ") + cudaGetErrorString(e));
@@ -1216,14 +1238,9 @@ int hyd_mass_balance_noalloc(hyd_handle h, int nblocks, double* out, int n) {
     CUDA_TRY(cudaSetDevice(h->device));
     double* part = nullptr;
     {
-        std::lock_guard<std::mutex> lock(g_mass_scratch_mu);
-        if (!g_mass_scratch_ptr[h->device]) {
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_mass_scratch);
-            if (e != cudaSuccess) return fail(HYD_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_mass_scratch_ptr[h->device] = (double*)p;
-        }
-        part = g_mass_scratch_ptr[h->device];
+        // found by hyd_create already; looked up here only if that failed
+        const cudaError_t e = mass_scratch_address(h->device, &part);
+        if (e != cudaSuccess) return fail(HYD_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     }
     k_mass_partial<<<nblocks, 256, 0, h->stream>>>(h->g, part);
     k_mass_final<<<1, 32, 0, h->stream>>>(part, nblocks, part + nblocks * 5);

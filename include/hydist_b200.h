@@ -244,9 +244,12 @@ int hyd_mass_balance(hyd_handle h, double* out, int n);
  * Nothing in the array needs to start at zero (every partial is written before it is
  * read).  The array is one per device and process, shared by all handles on that
  * device: overlapping calls (from two threads, or on two streams not ordered with each
- * other) race on it and must be serialised by the caller.  The first call on a device
- * looks the array up with cudaGetSymbolAddress and must not be made while a stream on
- * that device is being captured.
+ * other) race on it and must be serialised by the caller.  hyd_create looks the array up
+ * with cudaGetSymbolAddress on its device, which loads the module that holds it (with
+ * CUDA's lazy module loading nothing loads it earlier), so calls on a handle's device
+ * allocate nothing.  Only if that lookup was not possible there does the first call on
+ * the device look it up and load the module itself (an allocation by the driver); such a
+ * first call must not be made while a stream on that device is being captured.
  */
 #define HYD_MASS_NOALLOC_MAX_BLOCKS 1024
 int hyd_mass_balance_noalloc(hyd_handle h, int nblocks, double* out, int n);

@@ -10,7 +10,8 @@ for p in (ROOT, os.path.join(ROOT, "gpu-hydist_b200"), os.path.join(ROOT, "oracl
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE_TREE = "/root/reference"
+# the reference tree (read-only, absent on GPU machines): $HYDIST_REFERENCE, default below
+REFERENCE_TREE = os.environ.get("HYDIST_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

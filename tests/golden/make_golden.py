@@ -52,7 +52,7 @@ def tanchau_golden(ref_root):
     return c
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=os.environ.get("HYDIST_REFERENCE", "/root/reference")):
     oracle.build(("ref_cpu",))
     todo = [(c, golden.OUT_FIELDS) for c in golden_cases()] + [(tanchau_golden(ref_root), TANCHAU_OUT)]
     for c, fields in todo:

@@ -23,3 +23,12 @@ def test_reference_arm_json_line():
     assert d["config"]["workload"].startswith("config2_meander")
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_gpus_flag_must_match_the_ranks():
+    """--gpus N run as fewer ranks than N is refused, not silently measured on one GPU."""
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                          "--steps", "1"], capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
+    assert out.returncode == 2
+    assert "WORLD_SIZE=1" in out.stderr and not out.stdout.strip()

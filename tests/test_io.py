@@ -12,7 +12,7 @@ import pytest
 
 from hydist import io
 
-REF_TANCHAU = "/root/reference/Inputs/TanChau"
+REF_TANCHAU = os.path.join(os.environ.get("HYDIST_REFERENCE", "/root/reference"), "Inputs", "TanChau")
 
 
 def _write_case_dir(d, N=7, M=5, nseg_up=2, hours=6, seed=3):
