@@ -314,6 +314,9 @@ DevParams make_dev_params(const HydCaseParams& P) {
     d.kenhhepd = P.kenhhepd;
     d.kenhhepng = P.kenhhepng;
     d.channel = (P.kenhhepd || P.kenhhepng) ? 1 : 0;
+    d.bed_feedback = P.bed_feedback ? 1 : 0;
+    d.morfac = P.morfac;
+    d.bed_period = P.bed_period > 0 ? P.bed_period : P.bed_change_start;
     return d;
 }
 
@@ -447,6 +450,10 @@ void hyd_params_default(HydCaseParams* p) {
     p->sediment_start = 36000;
     p->bed_change_start = 72000;
     p->ketdinh = 1;
+    p->precision_mode = HYD_PRECISION_FP64;
+    p->morfac = 1.0;
+    p->bed_period = 0.0;
+    p->bed_feedback = 0;
     hyd_params_derive(p);
 }
 
@@ -489,6 +496,9 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     // a line of the grid is staged in shared memory by several kernels (8 B per cell)
     if (N > HYD_MAX_LINE || M > HYD_MAX_LINE) return fail(HYD_EINVAL, "grid too large (N, M <= 25000)");
     if (p->dT <= 0 || p->dX <= 0 || p->dY <= 0) return fail(HYD_EINVAL, "dX, dY, dT must be positive");
+    if (p->precision_mode != HYD_PRECISION_FP64 && p->precision_mode != HYD_PRECISION_MIXED)
+        return fail(HYD_EINVAL, "precision_mode must be HYD_PRECISION_FP64 or HYD_PRECISION_MIXED");
+    if (p->bed_feedback && !(p->morfac > 0)) return fail(HYD_EINVAL, "bed_feedback needs morfac > 0");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(HYD_ECUDA, "no CUDA device: this library has no CPU path");
@@ -541,7 +551,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     // arena: grid fields (double and int), smoothing partners, tables, boundary arrays
     const size_t nrow = (size_t)N + 3;
     const size_t gbytes = nrow * s->pitch * sizeof(double);
-    const size_t ngrid = 26;  // double grid fields in kFieldTable + VISC
+    const size_t ngrid = 28;  // double grid fields in kFieldTable + VISC, h0, dHc
     const size_t nseg_rows = ((size_t)N + 3) * HYD_SEGL, nseg_cols = ((size_t)M + 3) * HYD_SEGL;
     auto a256 = [](size_t b) { return (b + 255) / 256 * 256; };
     size_t total = a256(gbytes) * (ngrid + 1 + 2) + a256(nrow * s->pitch * sizeof(int));
@@ -550,6 +560,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     total += a256(4 * 8) + a256(4 * 4) + a256(4 * HYD_SEGL * 4) + a256(64) + a256(64);
     total += 4 * a256((N + 3) * 4) + 4 * a256((M + 3) * 4) + a256(64);  // spans, rescan flags and lists
     total += 2 * a256((N + 3) * 4) + 2 * a256(64);                      // extended spans, flags
+    total += a256(kBudSlots * 8);                                       // water budget
     e = cudaMalloc(&s->arena, total);
     if (e != cudaSuccess) {
         release(s);
@@ -572,7 +583,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     double** gd[] = {&g.h,   &g.hsnham, &g.VISC,  &g.Fw,   &g.Tsxw,  &g.Tsyw,     &g.u,   &g.v,   &g.z,
                      &g.t_u, &g.t_v,    &g.t_z,   &g.Htdu, &g.Htdv,  &g.H_moi,    &g.htaiz, &g.htaiz_bd,
                      &g.Kx1, &g.Ky1,    &g.FS,    &g.tFS,  &g.VTH,   &g.Kx,       &g.Ky,  &g.Qbx, &g.Qby,
-                     &g.dH};
+                     &g.dH,  &g.h0,     &g.dHc};
     for (double** q : gd) *q = (double*)take(gbytes);
     s->scratch_u = (double*)take(gbytes);
     s->scratch_v = (double*)take(gbytes);
@@ -606,6 +617,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.span_wide = (int*)take(64);
     g.dflag = (int*)take(64);
     g.clock = (double*)take(64);
+    g.budget = (double*)take(kBudSlots * 8);
     if ((size_t)(cur - (char*)s->arena) > total) {
         release(s);
         return fail(HYD_ENOMEM, "arena layout overflow");
@@ -984,6 +996,8 @@ static int init_common(HydSim* h, double t_start, int pickup) {
         keep = (const int*)h->scratch_u;
     }
     launch_init_kernels(h->g, h->dp, keep, h->stream);
+    CUDA_TRY(cudaMemsetAsync(h->g.budget, 0, kBudSlots * sizeof(double), h->stream));
+    launch_bed_reset(h->g, h->stream);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->t = t_start;
@@ -1025,10 +1039,10 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     }
     { PHASE(PH_COEF_UZ); launch_coef_bnd(g, p, 0, 3, st); }
     { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, 0, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, 0, 1, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_EXPL_V); launch_explicit_v(g, p, s->thr_r, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, 0, st); }
     std::swap(g.t_v, s->scratch_v);
     if (force) launch_mark_all_cols(g, st);
     { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, s->thr_r, st); }
@@ -1072,12 +1086,12 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         end_idx = s->N;
     }
     { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, 1, st); }
     std::swap(g.t_v, s->scratch_v);
     { PHASE(PH_COEF_EU); launch_coef_eu(g, p, st); }
     { PHASE(PH_EXPL_U); launch_explicit_u(g, p, s->thr_c, st); }
     if (overlap) cudaStreamWaitEvent(st, s->ev_join, 0);
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 1, overlap, st); }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 1, overlap, 0, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }
     if (!fh) {
@@ -1144,9 +1158,12 @@ int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
         const double t2 = t1 + h->P.dT * 0.5;
         const int sed1 = t1 >= h->P.sediment_start;
         const int sed2 = t2 >= h->P.sediment_start;
-        // Engine.py:364: int(t) % bed_change_start == 0 and t integral
+        // Engine.py:364: int(t) % bed_change_start == 0 and t integral; with a bed period,
+        // every bed_period s from bed_change_start on
         const double it = (double)(long long)t2;
-        const int bed = std::fmod(it, h->P.bed_change_start) == 0 && t2 - it == 0;
+        const int bed = h->P.bed_period > 0
+                            ? (t2 - it == 0 && t2 >= h->P.bed_change_start && std::fmod(it, h->P.bed_period) == 0)
+                            : (std::fmod(it, h->P.bed_change_start) == 0 && t2 - it == 0);
         const int mask = sed1 | (sed2 << 1) | (bed << 2);
         const int force = h->force_rescan;
         h->force_rescan = 0;
@@ -1185,11 +1202,23 @@ int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
 int hyd_set_params(hyd_handle h, const HydCaseParams* p) {
     if (!h || !p) return fail(HYD_EINVAL, "null argument");
     if (p->dT <= 0 || p->dX <= 0 || p->dY <= 0) return fail(HYD_EINVAL, "dX, dY, dT must be positive");
+    if (p->precision_mode != HYD_PRECISION_FP64 && p->precision_mode != HYD_PRECISION_MIXED)
+        return fail(HYD_EINVAL, "precision_mode must be HYD_PRECISION_FP64 or HYD_PRECISION_MIXED");
+    if (p->precision_mode != h->P.precision_mode)
+        return fail(HYD_EINVAL, "precision_mode is fixed when the handle is created");
+    if (p->bed_feedback && !(p->morfac > 0)) return fail(HYD_EINVAL, "bed_feedback needs morfac > 0");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int feedback_on = p->bed_feedback && !h->P.bed_feedback;
     h->P = *p;
     h->dp = make_dev_params(h->P);
     h->full_pending = 3;
     h->epoch++;
     drop_graphs(h);
+    if (feedback_on && h->initialized) {  // the applied changes start from the bed as it is
+        launch_bed_reset(h->g, h->stream);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
     return HYD_OK;
 }
 
@@ -1226,6 +1255,30 @@ int hyd_mass_balance(hyd_handle h, double* out, int n) {
     out[2] = r[2] * area;
     out[3] = r[3];
     out[4] = r[4];
+    return HYD_OK;
+}
+
+int hyd_mass_budget(hyd_handle h, double* out, int n) {
+    if (!h || !out || n < HYD_BUDGET_SLOTS) return fail(HYD_EINVAL, "need HYD_BUDGET_SLOTS output slots");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_mass_budget");
+    CUDA_TRY(cudaSetDevice(h->device));
+    double b[kBudSlots];
+    CUDA_TRY(cudaMemcpyAsync(b, h->g.budget, sizeof b, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const double area = h->P.dX * h->P.dY;
+    double net = 0, gin = 0, gout = 0;
+    for (int e = 0; e < 4; e++) {
+        net += b[kBudNet + e];
+        gin += b[kBudIn + e];
+        gout += b[kBudOut + e];
+        out[6 + e] = b[kBudNet + e];
+    }
+    out[0] = net;
+    out[1] = gin;
+    out[2] = gout;
+    out[3] = b[kBudOpen] * area;
+    out[4] = b[kBudClose] * area;
+    out[5] = b[kBudBed] * area;
     return HYD_OK;
 }
 
@@ -1319,6 +1372,8 @@ int hyd_set_state(hyd_handle h, const void* buf, size_t bytes) {
     rc = hyd_set_field(h, "VISCOIDX", p, (size_t)(h->N + 3) * (h->M + 3));
     if (rc) return rc;
     h->initialized = 1;
+    launch_bed_reset(h->g, h->stream);  // h0 = h - dH for the restored bed
+    CUDA_TRY(cudaGetLastError());
     rc = set_clock(h, h->t);
     if (rc) return rc;
     return HYD_OK;

@@ -27,6 +27,10 @@ struct DevParams {
     double dxr_m03;  // pow(dxr, -0.3), a constant of the source and bed-load formulas
     double sediment_start, bed_change_start;
     int ketdinh, kenhhepd, kenhhepng, channel;
+    // morphodynamic feedback (off: the reference's step): each Exner update's bed change,
+    // morfac x bed_period / (1 - Dorong) x rate, is applied to h and the depths re-derived
+    int bed_feedback;
+    double morfac, bed_period;  // bed_period: the Exner period in s (bed_change_start if unset)
 };
 
 struct DevGrid {
@@ -37,6 +41,7 @@ struct DevGrid {
     double *u, *v, *z, *t_u, *t_v, *t_z;
     double *Htdu, *Htdv, *H_moi, *htaiz, *htaiz_bd, *Kx1, *Ky1;
     double *FS, *tFS, *VTH, *Kx, *Ky, *Qbx, *Qby, *dH;
+    double *h0, *dHc;  // feedback: h at set-up (h = h0 + dH) and dH's Kahan compensation
     int* khouot;
     // segment tables (reference layout)
     int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
@@ -69,7 +74,16 @@ struct DevGrid {
     // value costs DRAM traffic; smaller grids store straight from the per-row warps
     int tile_cols;
     double* clock;  // [0] time of half-step 1, [1] time of half-step 2, [2] time at the step start
+    // water volume budget since hyd_init (kBud* slots): per edge the net, gross inflow and
+    // gross outflow volumes through its faces as the sweeps' continuity rows used them, each
+    // a Kahan sum with its compensation; the volumes of cells opened and closed by the
+    // wet/dry resets (depth sums, atomically added)
+    double* budget;
 };
+
+// Slots of DevGrid::budget.  Edge e = 0 up, 1 down, 2 left, 3 right.
+constexpr int kBudNet = 0, kBudNetC = 4, kBudIn = 8, kBudInC = 12, kBudOut = 16, kBudOutC = 20;
+constexpr int kBudOpen = 24, kBudClose = 25, kBudBed = 26, kBudSlots = 32;
 
 __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { atomicOr(g.status, bit); }
 
@@ -234,8 +248,10 @@ void launch_sweep_vz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, 
 // bytes: also write the column reset bytes (the smoothing of u just before the column resets)
 // fs_bnd: also apply the concentration part of the second half-step's boundary (span
 // passes only)
+// budget: also add the half-step's open-edge volumes to the budget (the first smoothing
+// after each sweep: isU = 1 after the UZ sweep, isU = 0 after the VZ sweep)
 void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, int fs_bnd,
-                   cudaStream_t s);
+                   int budget, cudaStream_t s);
 void launch_widen_spans(const DevGrid& g, cudaStream_t s);
 void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
 void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s);
@@ -272,4 +288,6 @@ void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, const SweepPlan& sp
                        double* scratch, cudaStream_t s);
 void launch_update_fs(const DevGrid& g, int full, cudaStream_t s);
 void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, cudaStream_t s);
+// feedback: h0 = h (the bed the applied changes start from), dH and its compensation zeroed
+void launch_bed_reset(const DevGrid& g, cudaStream_t s);
 long long hyd_kernel_launches_add(long long n);

@@ -527,6 +527,75 @@ struct RowLane {
     }
 };
 
+// The open-edge part of the water budget for one half-step, by one CTA for edge e (0 up:
+// faces j = M, 1 down: faces j = 1, 2 left: faces i = 1, 3 right: faces i = N), run right
+// after the half-step's sweep.  A sweep's continuity row of cell (i, j) reads
+//   z' = z - dT/(2 dX) (Htdu[i,j] u[i,j] - Htdu[i-1,j] u[i-1,j])
+//          - dT/(2 dY) (Htdv[i,j] v[i,j] - Htdv[i,j-1] v[i,j-1])
+// (_uzSolver/_vzSolver_calculate_preindex, UVZSolver_multithread.cu:345-349, 402-406),
+// with the implicit component new (t_u in the UZ sweep, t_v in the VZ sweep) and the other
+// as it stood; summed over the cells the sweep solved, the inner faces cancel and the
+// volume change is the flux through the domain's edge faces.  So the CTA adds, for every
+// edge cell the sweep solved (the cell lies in a segment of the sweep's lines), its edge
+// face's volume flux over the half-step, dT/2 x face depth x velocity x face width, signed
+// into the domain, to the edge's Kahan sums (one writer per edge: the CTA's thread 0).
+// half1: the UZ sweep (x faces t_u, y faces v); otherwise the VZ sweep (x faces u, y faces
+// t_v).
+__device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int e) {
+    __shared__ double s_in[32], s_out[32];
+    const int N = g.N, M = g.M, P = g.P;
+    const int n = e >= 2 ? M : N;  // edge cells j = 2..M (left/right) or i = 2..N (up/down)
+    double vin = 0.0, vout = 0.0;
+    for (int k = 2 + threadIdx.x; k <= n; k += blockDim.x) {
+        int i, j, fp;
+        double sgn;
+        if (e == 0) { i = k; j = M; fp = i * P + M; sgn = -1.0; }
+        else if (e == 1) { i = k; j = 2; fp = i * P + 1; sgn = 1.0; }
+        else if (e == 2) { i = 2; j = k; fp = 1 * P + j; sgn = 1.0; }
+        else { i = N; j = k; fp = N * P + j; sgn = -1.0; }
+        if (g.khouot[i * P + j] != 0) continue;
+        int f, l;
+        const int seg = half1 ? find_seg_u(g, i, j, f, l) : find_seg_v(g, i, j, f, l);
+        if (seg < 0) continue;
+        double q;
+        if (e >= 2) q = g.Htdu[fp] * (half1 ? g.t_u[fp] : g.u[fp]) * p.dY;
+        else q = g.Htdv[fp] * (half1 ? g.v[fp] : g.t_v[fp]) * p.dX;
+        const double vol = sgn * q * (p.dT * 0.5);
+        if (vol > 0) vin += vol;
+        else vout -= vol;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        vin += __shfl_down_sync(0xffffffffu, vin, o);
+        vout += __shfl_down_sync(0xffffffffu, vout, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        s_in[w] = vin;
+        s_out[w] = vout;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
+            a += s_in[q];
+            b += s_out[q];
+        }
+        double* B = g.budget;
+        auto kahan = [&](int sum, int comp, double x) {
+            const double y = x - B[comp];
+            const double t = B[sum] + y;
+            B[comp] = (t - B[sum]) - y;
+            B[sum] = t;
+        };
+        kahan(kBudNet + e, kBudNetC + e, a - b);
+        kahan(kBudIn + e, kBudInC + e, a);
+        kahan(kBudOut + e, kBudOutC + e, b);
+    }
+}
+
+// The edge budget alone (after a whole-grid smoothing pass): CTA e takes edge e.
+__global__ void k_edge_budget(DevGrid g, DevParams p, int half1) { edge_budget(g, p, half1, blockIdx.x); }
+
 // BYTES: also write the column reset bytes (the smoothing of u right before the column
 // resets; H_moi is not read in between).
 template <int BYTES>
@@ -539,8 +608,14 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
 // FSB: one more CTA (the last) applies the concentration part of the second half-step's
 // boundary (kBndFS), when the velocity/level part ran before the first half-step's
 // sediment sweep had finished.
-template <int BYTES, int FSB>
+// BUD: four more CTAs (the last) add the half-step's open-edge volumes to the budget
+// (edge_budget; the smoothing of the swept velocity, isU = the UZ sweep's half-step).
+template <int BYTES, int FSB, int BUD>
 __global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
+    if (BUD && (int)blockIdx.x >= (int)gridDim.x - 4) {
+        edge_budget(g, p, isU, blockIdx.x - (gridDim.x - 4));
+        return;
+    }
     if (FSB && blockIdx.x == gridDim.x - 1) {
         boundary_body(g, g.clock[1], kBndFS);
         return;
@@ -950,6 +1025,9 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
         anyev |= bits != 0;
     }
     // opening pass (loop 1), serial over those cells
+    // interior cells opened / closed here change the domain's water volume (the budget)
+    const bool interior_line = line >= 2 && line <= (ROWS ? g.N : g.M);
+    double opened = 0.0;
     if (__syncthreads_or(anyev) && warp == 0) {
         const int kb = k1 < L ? k1 : L;
         int done = -1;
@@ -962,6 +1040,7 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
             khs[kk - k0] = 0;
             FS[gq] = fsv;
             if (kk >= 2 && kk <= L && hv <= p.H_TINH) clw[(kk - k0) >> 5] |= 1u << ((kk - k0) & 31);
+            if (interior_line && kk >= 2 && kk <= L) opened += hv;
             s_changed = 1;
             mark_dirty(oflags, olist, octr, kk);
         };
@@ -998,12 +1077,15 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
             __syncwarp();
         }
     }
+    if (opened != 0.0) atomicAdd(&g.budget[kBudOpen], opened);
     __syncthreads();
     // closing pass (loop 2): independent per cell
+    double closed = 0.0;
     for (int q = warp; q < nq; q += T >> 5) {
         if (!((clw[q] >> lane) & 1u)) continue;
         const int k = k0 + q * 32 + lane;
         const int gp = base + k * along;
+        if (interior_line) closed += H[gp];
         g.t_u[gp - P] = 0;
         g.t_u[gp] = 0;
         g.t_v[gp - 1] = 0;
@@ -1014,6 +1096,7 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
         s_changed = 1;
         mark_dirty(oflags, olist, octr, k);
     }
+    if (closed != 0.0) atomicAdd(&g.budget[kBudClose], closed);
     __syncthreads();
     if (tid < 32 && line >= 2 && (s_changed || force))
         warp_scan_line(g, WetShared{khs, k0}, lo, hi, L, c0w, dau, cuoi, moc);
@@ -1416,7 +1499,11 @@ __global__ void k_update_fs_span(DevGrid g, int nb) {
     if (rl.off == 0 && (M < lo || M > hi)) g.FS[i * P + M] = g.tFS[i * P + M];
 }
 
-// Calculate_Qb (Sediment_Transport.cu:341-414): bed-load flux, then the edge copies
+// Calculate_Qb (Sediment_Transport.cu:341-414): bed-load flux, then the edge copies.
+// FB (morphodynamic feedback, no reference counterpart): the flux is evaluated where the
+// speed is positive, the formula's evident intent; the reference evaluates it only where
+// VTH == 0 (quirk Q3, reproduced with FB = 0), dividing by that zero.
+template <int FB>
 __global__ void k_qb(DevGrid g, DevParams p) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
     const int i = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -1425,7 +1512,7 @@ __global__ void k_qb(DevGrid g, DevParams p) {
     const int pos = i * P + j;
     double Tob, Toee = p.Toe, Tx = 0;
     double qx = 0, qy = 0;
-    if ((!g.VTH[pos]) && (g.khouot[pos] == 0)) {
+    if ((FB ? g.VTH[pos] > 0 : !g.VTH[pos]) && (g.khouot[pos] == 0)) {
         Tob = p.ro * g.Fw[pos] * (g.VTH[pos] * g.VTH[pos]);
         if (g.H_moi[pos] > p.ghtoe) Toee = p.Toe * (1 + p.hstoe * ((g.H_moi[pos] - p.ghtoe)));
         if (Tob > Toee) Tx = Tob / Toee - 1;
@@ -1471,7 +1558,11 @@ __global__ void k_qb(DevGrid g, DevParams p) {
 }
 
 // BedLoad/_bed_load (Sediment_Transport.cu:630-639, 416-506): Exner increment into dH
-// on rows startidx..endidx-1.
+// on rows startidx..endidx-1.  FB (morphodynamic feedback, no reference counterpart): the
+// increment covers the Exner period times the morphological factor, is added to dH as a
+// Kahan sum (dHc) and applied to the bed, h = h0 + dH; the upwind test the reference
+// writes as t_u[pos > 0] (quirk Q4, reproduced with FB = 0) reads t_u[pos] > 0.
+template <int FB>
 __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
     const int i = blockIdx.y * blockDim.y + threadIdx.y + startidx;
@@ -1488,7 +1579,8 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
         if (g.t_u[pos] < 0) pp = (-3 * Qbx[pos] + 4 * Qbx[pos + width] - Qbx[pos + 2 * width]) / p.dX2;
     } else {
         if (kh[pos + width] == 1) {
-            if (g.t_u[1]) pp = (3 * Qbx[pos] - 4 * Qbx[pos - width] + Qbx[pos - 2 * width]) / p.dX2;
+            if (FB ? g.t_u[pos] > 0 : g.t_u[1] != 0)
+                pp = (3 * Qbx[pos] - 4 * Qbx[pos - width] + Qbx[pos - 2 * width]) / p.dX2;
         } else
             pp = (Qbx[pos + width] - Qbx[pos - width]) / p.dX2;
     }
@@ -1521,7 +1613,59 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
     if (FS[pos] > 0.0) Zf = wsm / (0.4 * (Uf + 2 * wsm));
     if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], g.H_moi[pos]);
     else S = source_nchs(p, wsm, Zf, Uf, g.H_moi[pos], FS[pos]);
-    g.dH[pos] += p.dT / (1 - p.Dorong) * (S + tH);
+    if (!FB) {
+        g.dH[pos] += p.dT / (1 - p.Dorong) * (S + tH);
+        return;
+    }
+    const double x = p.morfac * p.bed_period / (1 - p.Dorong) * (S + tH);
+    const double y = x - g.dHc[pos];
+    const double sum = g.dH[pos] + y;
+    g.dHc[pos] = (sum - g.dH[pos]) - y;
+    g.dH[pos] = sum;
+    g.h[pos] = g.h0[pos] + sum;
+}
+
+// After a fed-back bed change: what the set-up derived from h, re-derived for the new bed
+// (Onetime_init, support_funcs.cu:20-58: htaiz, htaiz_bd, Kx1, Ky1; update_h_moi 60-73 on
+// the wet cells; Htuongdoi 338-354), and the water the bed moved into or out of the wet
+// interior cells' depths added to the budget.  Indexing as k_onetime_init.
+__global__ void k_bed_derive(DevGrid g, DevParams p) {
+    const int j0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = blockIdx.y * blockDim.y + threadIdx.y;
+    const int N = g.N, M = g.M, P = g.P;
+    const int i = i0 + 1, j = j0 + 1;
+    double dv = 0.0;
+    if (i <= N && j <= M) {
+        const double* h = g.h;
+        const int pos = i * P + j;
+        const double ht = (h[(i - 1) * P + j - 1] + h[(i - 1) * P + j] + h[pos - 1] + h[pos]) * 0.25;
+        const double old = g.htaiz[pos];
+        g.htaiz[pos] = ht;
+        g.htaiz_bd[pos] = ht;
+        if (h[pos - 1] + h[pos] != 0)
+            g.Kx1[pos] = p.g * pow((h[pos - 1] + h[pos]) * 0.5, -2 * p.mu_mn) *
+                         pow((g.hsnham[pos - 1] + g.hsnham[pos]) * 0.5, 2);
+        if (h[pos - P] + h[pos] != 0)
+            g.Ky1[pos] = p.g * pow((h[pos - P] + h[pos]) * 0.5, -2 * p.mu_mn) *
+                         pow((g.hsnham[pos - P] + g.hsnham[pos]) * 0.5, 2);
+        if (g.khouot[pos] == 0) {
+            g.H_moi[pos] = ht + g.z[pos];
+            if (i >= 2 && j >= 2) dv = ht - old;
+        }
+        post_cell(g, 0, i, j);
+    }
+    for (int o = 16; o > 0; o >>= 1) dv += __shfl_down_sync(0xffffffffu, dv, o);
+    if ((threadIdx.x & 31) == 0 && dv != 0.0) atomicAdd(&g.budget[kBudBed], dv);
+}
+
+// Feedback set-up: h0 = h - dH (so that h = h0 + dH holds now), no compensation yet.
+__global__ void k_bed_reset(DevGrid g) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.N + 3 || j >= g.M + 3) return;
+    const int pos = i * g.P + j;
+    g.h0[pos] = g.h[pos] - g.dH[pos];
+    g.dHc[pos] = 0.0;
 }
 
 }  // namespace
@@ -1667,16 +1811,21 @@ void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes,
 static int row_warps_blocks(const DevGrid& g, int rows) { return (rows * g.wpr * 32 + 255) / 256; }
 
 void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, int fs_bnd,
-                   cudaStream_t s) {
+                   int budget, cudaStream_t s) {
     const dim3 b(32, 8);
     if (full) {  // callers pass fs_bnd = 0 with full passes
         if (bytes) k_smooth<1><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         else k_smooth<0><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
+        if (budget) {  // the smoothing reads the swept velocity and writes elsewhere
+            k_edge_budget<<<4, 256, 0, s>>>(g, p, isU);
+            hyd_kernel_launches_add(1);
+        }
     } else {
         const int nb = row_warps_blocks(g, g.N + 3);
-        if (bytes && fs_bnd) k_smooth_span<1, 1><<<nb + 1, 256, 0, s>>>(g, p, isU, out);
-        else if (bytes) k_smooth_span<1, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
-        else k_smooth_span<0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
+        if (bytes && fs_bnd) k_smooth_span<1, 1, 0><<<nb + 1, 256, 0, s>>>(g, p, isU, out);
+        else if (bytes) k_smooth_span<1, 0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
+        else if (budget) k_smooth_span<0, 0, 1><<<nb + 4, 256, 0, s>>>(g, p, isU, out);
+        else k_smooth_span<0, 0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
     }
     hyd_kernel_launches_add(1);
 }
@@ -1767,9 +1916,23 @@ void launch_update_fs(const DevGrid& g, int full, cudaStream_t s) {
 
 void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, cudaStream_t s) {
     const dim3 b(32, 8);
-    k_qb<<<grid2d(g.M - 1, g.N - 1, b), b, 0, s>>>(g, p);
-    if (endidx > startidx) k_bedload<<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
-    hyd_kernel_launches_add(2);
+    if (!p.bed_feedback) {
+        k_qb<0><<<grid2d(g.M - 1, g.N - 1, b), b, 0, s>>>(g, p);
+        if (endidx > startidx) k_bedload<0><<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
+        hyd_kernel_launches_add(2);
+        return;
+    }
+    k_qb<1><<<grid2d(g.M - 1, g.N - 1, b), b, 0, s>>>(g, p);
+    if (endidx > startidx) k_bedload<1><<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
+    k_bed_derive<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p);
+    k_preprocess<<<1, 32, 0, s>>>(g, p);
+    hyd_kernel_launches_add(4);
+}
+
+void launch_bed_reset(const DevGrid& g, cudaStream_t s) {
+    const dim3 b(32, 8);
+    k_bed_reset<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g);
+    hyd_kernel_launches_add(1);
 }
 
 // Up to kPutDoubles values carried in the launch's parameters into dst[0..n): a small

@@ -56,6 +56,7 @@ def load():
         "hyd_set_params": (ctypes.c_int, [H, ctypes.POINTER(HydCaseParams)]),
         "hyd_synchronize": (ctypes.c_int, [H]),
         "hyd_mass_balance": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_int]),
+        "hyd_mass_budget": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_int]),
         "hyd_state_size": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_size_t)]),
         "hyd_get_state": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_size_t]),
         "hyd_set_state": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_size_t]),
@@ -258,6 +259,16 @@ class Simulation:
         _check(self.lib.hyd_mass_balance(self.h, out.ctypes.data, 5))
         return {"volume": out[0], "suspended": out[1], "bed_change": out[2], "wet_cells": int(out[3]),
                 "nonfinite": int(out[4])}
+
+    def mass_budget(self):
+        """The water volume budget since init (hyd_mass_budget), m^3: net, gross in and out
+        through the edges, volumes of the cells opened and closed by the wet/dry resets, the
+        volume fed-back bed changes added to the depths, and the net per edge (up, down,
+        left, right)."""
+        out = np.zeros(10)
+        _check(self.lib.hyd_mass_budget(self.h, out.ctypes.data, 10))
+        return {"net_in": out[0], "gross_in": out[1], "gross_out": out[2], "opened": out[3], "closed": out[4],
+                "bed": out[5], "edge_net": out[6:10].copy()}
 
     def get_state(self):
         n = ctypes.c_size_t()

@@ -20,11 +20,18 @@ _DOUBLE_FIELDS = [
     "sohn", "soha", "sohn1", "CORIOLIS_FORCE", "g", "Ks",
     "sediment_start", "bed_change_start",
 ]
-_INT_FIELDS = ["ketdinh", "kenhhepd", "kenhhepng", "reserved0"]
+_INT_FIELDS = ["ketdinh", "kenhhepd", "kenhhepng", "precision_mode"]
+# morphodynamic feedback (no reference counterpart), after the reference's constants
+_MORPHO_FIELDS = [("morfac", ctypes.c_double), ("bed_period", ctypes.c_double), ("bed_feedback", ctypes.c_int),
+                  ("reserved1", ctypes.c_int)]
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
 
 
 class HydCaseParams(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_double) for n in _DOUBLE_FIELDS] + [(n, ctypes.c_int) for n in _INT_FIELDS]
+    _fields_ = ([(n, ctypes.c_double) for n in _DOUBLE_FIELDS] + [(n, ctypes.c_int) for n in _INT_FIELDS] +
+                _MORPHO_FIELDS)
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -60,7 +67,8 @@ def default_params(**overrides):
         dm=0.00001, d90=0.002, muy=1.01e-06, Dorong=0.5, Sx=2.0,
         sohn=8.0, soha=3.0, sohn1=3.0, CORIOLIS_FORCE=0.0, g=9.81, Ks=2.5 * 0.00001,
         sediment_start=36000.0, bed_change_start=72000.0,
-        ketdinh=1, kenhhepd=0, kenhhepng=0, reserved0=0,
+        ketdinh=1, kenhhepd=0, kenhhepng=0, precision_mode=PRECISION_FP64,
+        morfac=1.0, bed_period=0.0, bed_feedback=0, reserved1=0,
     )
     vals.update(overrides)
     for k, v in vals.items():

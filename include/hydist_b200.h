@@ -74,8 +74,20 @@ typedef struct HydCaseParams {
     int ketdinh;             /* 1 = cohesive source term (Engine.py:49 default True) */
     int kenhhepd;            /* channel mode, vertical channel (rep.py:37; Engine.py:68,156) */
     int kenhhepng;           /* channel mode, horizontal channel (rep.py:36; Engine.py:68,277) */
-    int reserved0;
+    int precision_mode;      /* HYD_PRECISION_FP64 (the reference's arithmetic) or HYD_PRECISION_MIXED */
+    /* Morphodynamic feedback: no reference counterpart (the reference accumulates dH and
+     * never applies it, Sediment_Transport.cu:504).  With bed_feedback = 0 every value
+     * below is ignored but bed_period, and the step is the reference's. */
+    double morfac;           /* morphological factor of each applied bed change */
+    double bed_period;       /* s; Exner update every bed_period s from bed_change_start on;
+                                0 = every bed_change_start s (Engine.py:364) */
+    int bed_feedback;        /* 1 = apply each bed change to h and re-derive the depths */
+    int reserved1;
 } HydCaseParams;
+
+/* precision_mode values */
+#define HYD_PRECISION_FP64 0
+#define HYD_PRECISION_MIXED 1
 
 /* Fill *p with the values of the reference's constant.cuh (constant.cuh:31-118)
  * and the Engine.hydraulic_Calculation defaults (Engine.py:49-50). */
@@ -229,6 +241,29 @@ int hyd_synchronize(hyd_handle h);
  * n must be >= 5.
  */
 int hyd_mass_balance(hyd_handle h, double* out, int n);
+
+/*
+ * Water volume budget since hyd_init, in FP64 (the reference has none: it only checks
+ * for NaN once an hour, Engine.py:402-412).  Both sweeps' continuity
+ * rows are in flux form (_uzSolver/_vzSolver_calculate_preindex,
+ * UVZSolver_multithread.cu:345-349, 402-406): summed over the cells a sweep solves, the
+ * faces between two solved cells cancel, so the domain's volume changes by the fluxes
+ * through its edge faces and by the cells the wet/dry resets open and close
+ * (support_funcs.cu:75-186).  The library accumulates exactly those terms on the device
+ * every half-step (edge volumes as Kahan sums, one writer per edge):
+ *   out[0] net volume into the domain through the four edges (m^3)
+ *   out[1] gross inflow volume, out[2] gross outflow volume (m^3)
+ *   out[3] volume of the cells opened by the wetting pass (m^3)
+ *   out[4] volume of the cells closed by the drying pass (m^3)
+ *   out[5] water volume the fed-back bed changes added to the wet cells' depths (m^3;
+ *          0 without bed_feedback)
+ *   out[6..9] net volume in through the up, down, left, right edge (m^3)
+ * Closure: between two times, the change of hyd_mass_balance's out[0] equals
+ * d(out[0]) + d(out[3]) - d(out[4]) + d(out[5]).  n must be >= HYD_BUDGET_SLOTS.  No
+ * reference counterpart.
+ */
+#define HYD_BUDGET_SLOTS 10
+int hyd_mass_budget(hyd_handle h, double* out, int n);
 
 /*
  * hyd_mass_balance_noalloc — the sums of hyd_mass_balance (same out[0..4]) computed

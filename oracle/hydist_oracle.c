@@ -44,6 +44,7 @@ struct OraSim {
     size_t nf;
     double *h, *hsnham, *VISCOIDX, *Fw, *Tsxw, *Tsyw, *u, *v, *z, *t_u, *t_v, *t_z, *Htdu, *Htdv,
         *H_moi, *htaiz, *htaiz_bd, *Kx1, *Ky1, *FS, *tFS, *VTH, *Kx, *Ky, *Qbx, *Qby, *dH;
+    double *h0, *dHc; /* morphodynamic feedback: h = h0 + dH, dH's Kahan compensation */
     int* khouot;
     int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
     double *ubt, *ubp, *vbt, *vbd, *hi;
@@ -110,7 +111,7 @@ OraSim* ora_create(const HydCaseParams* p, int N, int M) {
                          &s->u,     &s->v,      &s->z,        &s->t_u,   &s->t_v,      &s->t_z,
                          &s->Htdu,  &s->Htdv,   &s->H_moi,    &s->htaiz, &s->htaiz_bd, &s->Kx1,
                          &s->Ky1,   &s->FS,     &s->tFS,      &s->VTH,   &s->Kx,       &s->Ky,
-                         &s->Qbx,   &s->Qby,    &s->dH};
+                         &s->Qbx,   &s->Qby,    &s->dH,       &s->h0,    &s->dHc};
     for (size_t k = 0; k < sizeof(fields) / sizeof(fields[0]); k++) {
         *fields[k] = (double*)ora_alloc(s, nf, sizeof(double), G);
         if (!*fields[k]) goto fail;
@@ -486,6 +487,14 @@ static void k_preprocess(OraSim* s) {
     if (s->hmax_r != 0) s->hmax_r = 1.0 / (ros * s->hmax_r);
 }
 
+/* Morphodynamic feedback set-up (no reference counterpart): h0 = h - dH, no compensation. */
+static void bed_feedback_reset(OraSim* s) {
+    for (size_t q = 0; q < s->nf; q++) {
+        s->h0[q] = s->h[q] - s->dH[q];
+        s->dHc[q] = 0.0;
+    }
+}
+
 /* rep.py:126-131 with pick_up: the mask loaded from the pick-up files replaces the one
  * Onetime_init derives, before the segment scans, Htuongdoi and preprocess_data. */
 void ora_init_pickup(OraSim* s, double t_start) {
@@ -499,6 +508,7 @@ void ora_init_pickup(OraSim* s, double t_start) {
     k_limits_vertical(s);
     k_htuongdoi(s);
     k_preprocess(s);
+    bed_feedback_reset(s);
     s->t = t_start;
 }
 
@@ -508,6 +518,7 @@ void ora_init(OraSim* s, double t_start) {
     k_limits_vertical(s);
     k_htuongdoi(s);
     k_preprocess(s);
+    bed_feedback_reset(s);
     s->t = t_start;
 }
 
@@ -1525,7 +1536,9 @@ static void sediment_fsi(OraSim* s, double t, double s_start) {
     k_update_fs(s);
 }
 
-/* Calculate_Qb (Sediment_Transport.cu:341-414) */
+/* Calculate_Qb (Sediment_Transport.cu:341-414).  With the library's bed_feedback option
+ * (no reference counterpart) the flux is evaluated where VTH > 0 instead of VTH == 0
+ * (quirk Q3). */
 static void k_calculate_qb(OraSim* s) {
     const int N = s->N, M = s->M, width = s->W;
     const HydCaseParams* P = &s->P;
@@ -1537,7 +1550,7 @@ static void k_calculate_qb(OraSim* s) {
             double Toee = P->Toe;
             double Tx = 0;
             const int pos = i * width + j;
-            if ((!s->VTH[pos]) && (s->khouot[pos] == 0)) {
+            if ((P->bed_feedback ? s->VTH[pos] > 0 : !s->VTH[pos]) && (s->khouot[pos] == 0)) {
                 Tob = P->ro * s->Fw[pos] * (s->VTH[pos] * s->VTH[pos]);
                 if (s->H_moi[pos] > P->ghtoe) Toee = P->Toe * (1 + P->hstoe * ((s->H_moi[pos] - P->ghtoe)));
                 if (Tob > Toee) Tx = Tob / Toee - 1;
@@ -1585,7 +1598,10 @@ static void k_calculate_qb(OraSim* s) {
         }
 }
 
-/* BedLoad + _bed_load (Sediment_Transport.cu:630-639, 416-506): rows startidx..endidx-1 */
+/* BedLoad + _bed_load (Sediment_Transport.cu:630-639, 416-506): rows startidx..endidx-1.
+ * With the library's bed_feedback option (no reference counterpart): the upwind test reads
+ * t_u[pos] > 0 (quirk Q4), the increment is morfac * bed_period / (1 - Dorong) * rate,
+ * added to dH as a Kahan sum and applied to the bed, h = h0 + dH. */
 static void k_bedload(OraSim* s, int startidx, int endidx) {
     const int N = s->N, M = s->M, width = s->W;
     const HydCaseParams* P = &s->P;
@@ -1607,7 +1623,8 @@ static void k_bedload(OraSim* s, int startidx, int endidx) {
                 if (t_u[pos] < 0) p = (-3 * Qbx[pos] + 4 * Qbx[pos + width] - Qbx[pos + 2 * width]) / dX2;
             } else {
                 if (khouot[pos + width] == 1) {
-                    if (t_u[pos > 0]) p = (3 * Qbx[pos] - 4 * Qbx[pos - width] + Qbx[pos - 2 * width]) / dX2;
+                    if (P->bed_feedback ? t_u[pos] > 0 : t_u[pos > 0] != 0)
+                        p = (3 * Qbx[pos] - 4 * Qbx[pos - width] + Qbx[pos - 2 * width]) / dX2;
                 } else
                     p = (Qbx[pos + width] - Qbx[pos - width]) / dX2;
             }
@@ -1642,8 +1659,45 @@ static void k_bedload(OraSim* s, int startidx, int endidx) {
             if (FS[pos] > 0.0) Zf = wsm / (0.4 * (Uf + 2 * wsm));
             if (P->ketdinh) S = source_chs(P, wsm, Zf, FS[pos], Fw[pos], VTH[pos], H_moi[pos]);
             else S = source_nchs(P, wsm, Zf, s->dxr, s->ufr, Uf, H_moi[pos], FS[pos]);
-            s->dH[pos] += P->dT / (1 - P->Dorong) * (S + tH);
+            if (!P->bed_feedback) {
+                s->dH[pos] += P->dT / (1 - P->Dorong) * (S + tH);
+                continue;
+            }
+            {
+                const double period = P->bed_period > 0 ? P->bed_period : P->bed_change_start;
+                const double x = P->morfac * period / (1 - P->Dorong) * (S + tH);
+                const double y = x - s->dHc[pos];
+                const double sum = s->dH[pos] + y;
+                s->dHc[pos] = (sum - s->dH[pos]) - y;
+                s->dH[pos] = sum;
+                s->h[pos] = s->h0[pos] + sum;
+            }
         }
+}
+
+/* After a fed-back bed change (no reference counterpart): what the set-up derived from h
+ * re-derived for the new bed: htaiz, htaiz_bd, Kx1, Ky1 (Onetime_init,
+ * support_funcs.cu:20-58), H_moi of the wet cells (update_h_moi, 60-73), Htuongdoi and
+ * preprocess_data. */
+static void bed_feedback_derive(OraSim* s) {
+    const int N = s->N, M = s->M, W = s->W;
+    const HydCaseParams* P = &s->P;
+    const double* h = s->h;
+    for (int i = 1; i <= N; i++)
+        for (int j = 1; j <= M; j++) {
+            const size_t ij = (size_t)i * W + j;
+            s->htaiz[ij] = (h[(i - 1) * W + j - 1] + h[(i - 1) * W + j] + h[i * W + j - 1] + h[i * W + j]) * 0.25;
+            s->htaiz_bd[ij] = s->htaiz[ij];
+            if (h[i * W + j - 1] + h[i * W + j] != 0)
+                s->Kx1[ij] = P->g * pow((h[i * W + j - 1] + h[i * W + j]) * 0.5, -2 * P->mu_mn) *
+                             pow((s->hsnham[i * W + j - 1] + s->hsnham[i * W + j]) * 0.5, 2);
+            if (h[(i - 1) * W + j] + h[i * W + j] != 0)
+                s->Ky1[ij] = P->g * pow((h[(i - 1) * W + j] + h[i * W + j]) * 0.5, -2 * P->mu_mn) *
+                             pow((s->hsnham[(i - 1) * W + j] + s->hsnham[i * W + j]) * 0.5, 2);
+            if (s->khouot[ij] == 0) s->H_moi[ij] = s->htaiz[ij] + s->z[ij];
+        }
+    k_htuongdoi(s);
+    k_preprocess(s);
 }
 
 /* ---------------------------------------------------------- time loop */
@@ -1729,12 +1783,17 @@ static void full_step(OraSim* s) {
         end_idx = N - 1;
         sediment_fsi(s, t, P->bed_change_start); TRACE("sediment_fsi");
     }
-    /* Engine.py:364: int(t) % bed_change_start == 0 and t integral */
+    /* Engine.py:364: int(t) % bed_change_start == 0 and t integral; with the library's
+       bed_period, every bed_period s from bed_change_start on */
     {
         const double it = (double)(long long)t;
-        if (fmod(it, P->bed_change_start) == 0 && t - it == 0) {
+        const int bed = P->bed_period > 0
+                            ? (t - it == 0 && t >= P->bed_change_start && fmod(it, P->bed_period) == 0)
+                            : (fmod(it, P->bed_change_start) == 0 && t - it == 0);
+        if (bed) {
             k_calculate_qb(s);
             k_bedload(s, start_idx, end_idx);
+            if (P->bed_feedback) bed_feedback_derive(s);
         }
     }
     s->start_idx = start_idx;

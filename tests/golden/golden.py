@@ -35,8 +35,12 @@ def load(name):
     from hydist.cases import Case
     from hydist.params import HydCaseParams
     z = np.load(os.path.join(HERE, name + ".npz"))
-    p = HydCaseParams()
-    ctypes.memmove(ctypes.addressof(p), z["params"].tobytes(), ctypes.sizeof(p))
+    from hydist.params import default_params
+    # fixtures store the struct as it was when they were made: the reference's constants
+    # and run options; fields added since (the morphodynamic options) keep their defaults
+    p = default_params()
+    raw = z["params"].tobytes()
+    ctypes.memmove(ctypes.addressof(p), raw, min(len(raw), ctypes.sizeof(p)))
     fields = {k[3:]: z[k] for k in z.files if k.startswith("in_")}
     case = Case(name, int(z["N"]), int(z["M"]), p, fields, z["boundary_type"],
                 [z["table_%d" % e] for e in range(4)], [z["cc_%d" % e] for e in range(4)],

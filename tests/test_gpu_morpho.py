@@ -1,0 +1,104 @@
+"""Morphodynamic feedback (GPU): the bed change applied to the bed, against the oracle and
+over the large reach's stated 24 hours.
+
+The reference accumulates dH and never applies it (Sediment_Transport.cu:504, quirk Q5);
+with bed_feedback = 0 the library reproduces that (every parity test runs that way).
+With bed_feedback = 1 each Exner update (every bed_period s from bed_change_start on)
+adds morfac x bed_period / (1 - Dorong) x rate to dH as a Kahan sum and sets
+h = h0 + dH, and the set-up's depth-derived fields are re-derived.  The oracle restates
+the same option, so the GPU is held to the parity tolerance against it.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from helpers import REL_TOL, rel_linf
+
+pytestmark = pytest.mark.gpu
+
+
+def _feedback(case, morfac, period):
+    p = case.params.copy()
+    p.bed_feedback = 1
+    p.morfac = float(morfac)
+    p.bed_period = float(period)
+    case.params = p
+    return case
+
+
+def test_feedback_matches_oracle(oracle_lib):
+    """Islands reach with sediment from t = 0 and a fed-back bed update every 10 s at
+    morfac 10: 240 steps (23 updates) on the GPU and on the oracle."""
+    import oracle
+    from hydist import cases
+    from hydist.lib import Simulation
+    c = _feedback(cases.islands_case(), 10.0, 10.0)
+    n = 240
+    sim = Simulation.from_case(c)
+    h_start = sim.get("h")
+    sim.step(n)
+    ora = oracle.OracleSim(c)
+    ora.init()
+    ora.step(n)
+    for f in ("z", "u", "v", "FS", "dH", "h", "htaiz", "H_moi", "Htdu", "Htdv", "Kx1", "Ky1", "hi"):
+        e = rel_linf(sim.get(f), ora.get(f))
+        assert e <= REL_TOL, "%s rel L-inf %.3e" % (f, e)
+    for f in ("khouot", "moci", "mocj"):
+        assert np.array_equal(sim.get(f), ora.get(f)), f
+    # the bed moved, by dH
+    h = sim.get("h")
+    dH = sim.get("dH")
+    assert np.isfinite(dH).all()
+    assert np.abs(h - h_start).max() > 0
+    assert np.allclose(h - h_start, dH, rtol=0, atol=1e-12)
+    sim.close()
+
+
+def test_feedback_off_keeps_the_bed():
+    """Without feedback the bed never changes and dH only accumulates (quirk Q5)."""
+    from hydist import cases
+    from hydist.lib import Simulation
+    c = cases.islands_case()
+    sim = Simulation.from_case(c)
+    h0 = sim.get("h")
+    sim.step(120)
+    assert np.array_equal(sim.get("h"), h0)
+    assert np.nanmax(np.abs(sim.get("dH"))) > 0
+    sim.close()
+
+
+def test_config4_24h_morfac10():
+    """The 4096 x 2048 reach over its stated 24 h (86 400 steps of 1 s) with hydraulics,
+    sediment and the bed change fed back at morphological factor 10, the bed updated every
+    10 min: finite throughout, the water budget closed with the bed's share, and the
+    simulated hours per wall second reported."""
+    from hydist import cases
+    from hydist.lib import Simulation
+    c = _feedback(cases.config4_case(), 10.0, 600.0)
+    sim = Simulation.from_case(c)
+    sim.step(1)
+    v0 = sim.mass_balance()["volume"]
+    b0 = sim.mass_budget()
+    t0 = time.perf_counter()
+    worst = 0.0
+    for hour in range(24):
+        sim.step(3600 if hour < 23 else 3599)
+        mb = sim.mass_balance()
+        assert mb["nonfinite"] == 0, "non-finite values by hour %d" % (hour + 1)
+        b = sim.mass_budget()
+        dv = mb["volume"] - v0
+        pred = (b["net_in"] - b0["net_in"]) + (b["opened"] - b0["opened"]) - (b["closed"] - b0["closed"]) + (
+            b["bed"] - b0["bed"])
+        worst = max(worst, abs(dv - pred) / mb["volume"])
+    wall = time.perf_counter() - t0
+    assert sim.t == 86400.0
+    dH = sim.get("dH")
+    assert np.isfinite(dH).all()
+    mx = float(np.abs(dH).max())
+    b = sim.mass_budget()
+    print("config4 24 h morfac 10: %.1f s wall, %.2f sim-h/wall-s, max |dH| %.4f m, bed volume to the water "
+          "column %.1f m3, closure worst rel %.2e" % (wall, 24.0 / wall, mx, b["bed"], worst))
+    assert 0 < mx < 2.0
+    assert worst <= 1e-9
+    sim.close()
