@@ -89,6 +89,7 @@ struct HydSim {
     int solver;
     int start_idx, end_idx;
     unsigned* h_status;
+    double* run_part;  // hyd_run's non-finite check: partial sums, allocated at its first use
     // phase timing (instrumentation): bit k set = phase k bracketed by events
     unsigned timing;
     struct Mark {
@@ -459,6 +460,7 @@ void hyd_params_default(HydCaseParams* p) {
 
 // Free what a handle holds (any of it may be missing on a failed create) and the handle.
 static void release(HydSim* s) {
+    cudaFree(s->run_part);
     cudaFree(s->sweep_scratch);
     cudaFree(s->fs_scratch);
     cudaFree(s->g.colT);
@@ -1196,6 +1198,62 @@ int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out) {
     CUDA_TRY(cudaGetLastError());
     if (t_out) *t_out = t;
     if (sync) return check_device_status(h);
+    return HYD_OK;
+}
+
+// Non-finite values in z, u, v, FS (the mass-balance kernels' count), on the handle's
+// stream; -1 on error.
+static long long count_nonfinite(HydSim* h) {
+    const int nb = 148;
+    if (!h->run_part && cudaMalloc(&h->run_part, ((size_t)nb * 5 + 5) * sizeof(double)) != cudaSuccess) return -1;
+    k_mass_partial<<<nb, 256, 0, h->stream>>>(h->g, h->run_part);
+    k_mass_final<<<1, 32, 0, h->stream>>>(h->run_part, nb, h->run_part + nb * 5);
+    hyd_kernel_launches_add(2);
+    double r[5];
+    if (cudaMemcpyAsync(r, h->run_part + nb * 5, sizeof r, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return -1;
+    return (long long)r[4];
+}
+
+// An output time of hyd_run: t integral and a whole multiple of interval (Engine.py:398).
+static bool run_output_time(double t, double interval) {
+    if (!(interval > 0)) return false;
+    const double it = (double)(long long)t;
+    return t - it == 0 && std::fmod(it, interval) == 0;
+}
+
+int hyd_run(hyd_handle h, double Tmax, double interval, hyd_run_callback cb, void* user, double* t_out) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_run");
+    CUDA_TRY(cudaSetDevice(h->device));
+    double t = h->t;
+    while (t < Tmax) {
+        // the steps up to the next output time or the end (the host's time arithmetic:
+        // two half-step increments per step, Engine.py:146,260)
+        int n = 0;
+        double tn = t;
+        do {
+            tn = tn + h->P.dT * 0.5;
+            tn = tn + h->P.dT * 0.5;
+            n++;
+        } while (tn < Tmax && !run_output_time(tn, interval));
+        int rc = hyd_step(h, n, 0, &t);
+        if (rc) return rc;
+        if (run_output_time(t, interval) || t >= Tmax) {
+            const long long bad = count_nonfinite(h);
+            if (bad < 0) return fail(HYD_ECUDA, "hyd_run: the non-finite check failed");
+            rc = check_device_status(h);
+            if (rc) return rc;
+            if (bad > 0) {
+                if (t_out) *t_out = t;
+                return fail(HYD_EDEVICE, "non-finite values in z, u, v or FS at t = " + std::to_string(t) + " s (" +
+                                             std::to_string(bad) + " values)");
+            }
+            if (cb && cb(h, t, user)) break;
+        }
+    }
+    if (t_out) *t_out = t;
     return HYD_OK;
 }
 

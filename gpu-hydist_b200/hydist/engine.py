@@ -47,8 +47,8 @@ def hydraulic_Calculation(Tmax, pointers, arg_struct_ptr=None, arr_struct_ptr=No
     p.ketdinh = 1 if ketdinh else 0
     p.sediment_start = float(sediment_start)
     p.bed_change_start = float(bed_change_start)
-    p.kenhhepd = int(kenhhepd) if kenhhepd in (0, 1, True, False) else 1
-    p.kenhhepng = int(kenhhepng) if kenhhepng in (0, 1, True, False) else 1
+    p.kenhhepd = _channel_flag(kenhhepd)
+    p.kenhhepng = _channel_flag(kenhhepng)
     sim.set_params(p)
     u_list, v_list, z_list, fslist = [], [], [], []
     dT = p.dT
@@ -77,6 +77,16 @@ def hydraulic_Calculation(Tmax, pointers, arg_struct_ptr=None, arr_struct_ptr=No
             from .io import export_velocity_and_level
             export_velocity_and_level(sim, t, out_dir)
     return u_list, v_list, z_list, fslist
+
+
+def _channel_flag(v):
+    """Engine.py's use of kenhhepd / kenhhepng: a true value selects the channel-mode
+    boundaries (Engine.py:68), and only a value equal to 1 also shifts the sweep ranges
+    (Engine.py:156,277).  A string (rep.py's argparse value) is true but never equal to 1
+    (quirk Q11), so it maps to 2: channel mode without the shift."""
+    if isinstance(v, (bool, int, np.integer)):
+        return int(v)
+    return 2 if v else 0
 
 
 def _host_event(t, interval, save_grid, sediment_start, export):

@@ -16,6 +16,9 @@ SEGL = 20
 
 _lib = None
 
+# int (*hyd_run_callback)(hyd_handle h, double t, void* user)
+RUN_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p)
+
 
 class HydError(RuntimeError):
     pass
@@ -52,6 +55,8 @@ def load():
         "hyd_update_boundary": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
         "hyd_init_pickup": (ctypes.c_int, [H, ctypes.c_double]),
         "hyd_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+        "hyd_run": (ctypes.c_int, [H, ctypes.c_double, ctypes.c_double, RUN_CALLBACK, ctypes.c_void_p,
+                                   ctypes.POINTER(ctypes.c_double)]),
         "hyd_get_time": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double)]),
         "hyd_set_params": (ctypes.c_int, [H, ctypes.POINTER(HydCaseParams)]),
         "hyd_synchronize": (ctypes.c_int, [H]),
@@ -247,6 +252,18 @@ class Simulation:
 
     def synchronize(self):
         _check(self.lib.hyd_synchronize(self.h))
+
+    def run(self, Tmax, interval=0.0, callback=None):
+        """hyd_run: step while t < Tmax; at every whole multiple of `interval` s (and at the
+        end) check for non-finite values (HydError if any) and call callback(t), whose true
+        return ends the run.  Returns the time reached."""
+        t = ctypes.c_double()
+        if callback is None:
+            cb = RUN_CALLBACK()
+        else:
+            cb = RUN_CALLBACK(lambda h, tt, user: 1 if callback(tt) else 0)
+        _check(self.lib.hyd_run(self.h, float(Tmax), float(interval), cb, None, ctypes.byref(t)))
+        return t.value
 
     @property
     def t(self):

@@ -217,6 +217,21 @@ int hyd_init_pickup(hyd_handle h, double t_start);
 int hyd_step(hyd_handle h, int nsteps, int sync, double* t_out);
 
 /*
+ * hyd_run — the time loop of Engine.hydraulic_Calculation (Engine.py:49-50, 144-412):
+ * steps of dT while t < Tmax, and at every output time, a time t that is a whole multiple
+ * of `interval` s (the reference's `int(t) % interval == 0` with t integral,
+ * Engine.py:398; interval <= 0: only at the end), the reference's check of z, u, v (and
+ * FS) for non-finite values (Engine.py:402-412), then cb(h, t, user) if cb is not NULL
+ * (where the reference appends u, v, z to its output lists, the host reads fields with
+ * hyd_get_field).  A non-finite value ends the run with HYD_EDEVICE and the time in the
+ * message, the state left as it was then (the reference returns its lists there).  A
+ * nonzero cb return ends the run with HYD_OK.  *t_out (if not NULL) receives the time
+ * reached.  The run ends at the first step end with t >= Tmax, as the reference's loop.
+ */
+typedef int (*hyd_run_callback)(hyd_handle h, double t, void* user);
+int hyd_run(hyd_handle h, double Tmax, double interval, hyd_run_callback cb, void* user, double* t_out);
+
+/*
  * Replace the case parameters between steps (the run options of
  * Engine.hydraulic_Calculation, e.g. sediment_start, bed_change_start, ketdinh, are
  * keyword arguments there and may differ per call, Engine.py:49-50).  The grid size
