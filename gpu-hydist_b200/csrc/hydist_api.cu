@@ -318,6 +318,7 @@ DevParams make_dev_params(const HydCaseParams& P) {
     d.bed_feedback = P.bed_feedback ? 1 : 0;
     d.morfac = P.morfac;
     d.bed_period = P.bed_period > 0 ? P.bed_period : P.bed_change_start;
+    d.mixed = P.precision_mode == HYD_PRECISION_MIXED ? 1 : 0;
     return d;
 }
 
@@ -402,7 +403,9 @@ extern "C" {
 
 const char* hyd_last_error(void) { return g_last_error.c_str(); }
 
-const char* hyd_version(void) { return "hydist_b200 1.0 (sm_100a, FP64 ADI, partitioned line solver)"; }
+const char* hyd_version(void) {
+    return "hydist_b200 1.1 (sm_100a, FP64 ADI and FP32-bulk mixed form, partitioned line solver)";
+}
 
 void hyd_params_derive(HydCaseParams* p) {
     p->dXbp = p->dX * p->dX;
@@ -465,6 +468,8 @@ static void release(HydSim* s) {
     cudaFree(s->fs_scratch);
     cudaFree(s->g.colT);
     cudaFree(s->g.rowC);
+    cudaFree(s->g.colTf);
+    cudaFree(s->g.rowCf);
     cudaFree(s->arena);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     if (s->ev_join) cudaEventDestroy(s->ev_join);
@@ -651,6 +656,11 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     s->g.colB = (unsigned char*)(s->g.colT + 7 * s->g.colT_stride);
     s->g.rowC_stride = (size_t)(N + 3) * s->pitch;
     if (e == cudaSuccess) e = cudaMalloc(&s->g.rowC, 7 * s->g.rowC_stride * sizeof(double));
+    if (e == cudaSuccess && p->precision_mode == HYD_PRECISION_MIXED) {
+        // the mixed form's FP32 coefficient arrays (the FP64 ones stay for the set-up paths)
+        e = cudaMalloc(&s->g.colTf, 7 * s->g.colT_stride * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&s->g.rowCf, 7 * s->g.rowC_stride * sizeof(float));
+    }
     if (e != cudaSuccess) {
         release(s);
         return fail(HYD_ENOMEM, std::string("column-major scratch: ") + cudaGetErrorString(e));

@@ -31,6 +31,10 @@ struct DevParams {
     // morfac x bed_period / (1 - Dorong) x rate, is applied to h and the depths re-derived
     int bed_feedback;
     double morfac, bed_period;  // bed_period: the Exner period in s (bed_change_start if unset)
+    // precision_mode MIXED: coefficient assembly, the line sweeps, the explicit momentum and
+    // the sediment transport in FP32; the water level's continuity update, the mass sums
+    // and the Exner accumulation in FP64
+    int mixed;
 };
 
 struct DevGrid {
@@ -65,6 +69,9 @@ struct DevGrid {
     double* colT;
     unsigned char* colB;  // column-major reset bytes of the column resets (stride LT)
     double* rowC;         // row-major VZ coefficients, 7 arrays of (N+3) x P
+    // the mixed form's FP32 copies of colT and rowC (same layout and strides; null in FP64)
+    float* colTf;
+    float* rowCf;
     size_t rowC_stride;
     size_t colT_stride;
     int LT;
@@ -90,6 +97,19 @@ __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { at
 // Column-major copy k of a per-cell quantity; (row i, column j) is at [j * g.LT + i].
 __device__ __forceinline__ double* colT(const DevGrid& g, int k) { return g.colT + (size_t)k * g.colT_stride; }
 __device__ __forceinline__ double* rowC(const DevGrid& g, int k) { return g.rowC + (size_t)k * g.rowC_stride; }
+// The same arrays in the arithmetic type R of a kernel instantiation (float: the mixed form's copies).
+template <class R>
+__device__ __forceinline__ R* colTr(const DevGrid& g, int k);
+template <>
+__device__ __forceinline__ double* colTr<double>(const DevGrid& g, int k) { return colT(g, k); }
+template <>
+__device__ __forceinline__ float* colTr<float>(const DevGrid& g, int k) { return g.colTf + (size_t)k * g.colT_stride; }
+template <class R>
+__device__ __forceinline__ R* rowCr(const DevGrid& g, int k);
+template <>
+__device__ __forceinline__ double* rowCr<double>(const DevGrid& g, int k) { return rowC(g, k); }
+template <>
+__device__ __forceinline__ float* rowCr<float>(const DevGrid& g, int k) { return g.rowCf + (size_t)k * g.rowC_stride; }
 
 // Per-cell values of a row-major sweep over the grid stored column-major through a
 // shared-memory tile.  The CTA (256 threads) takes rows i0..i0+7, one warp per row as the
@@ -99,10 +119,10 @@ __device__ __forceinline__ double* rowC(const DevGrid& g, int k) { return g.rowC
 // of a chunk go out column by column, the 8 rows of a column as one contiguous run, in
 // place of one 32-byte sector per cell.  dst[k][j * g.LT + i] receives value k.
 constexpr int kTileRows = 8;
-template <int K, class Cell>
+template <int K, class T, class Cell>
 __device__ __forceinline__ void colmajor_tile(const DevGrid& g, int i0, int ilast, int jmin, int jmax, Cell cell,
-                                              double* const (&dst)[K]) {
-    __shared__ double s_v[K][kTileRows][33];
+                                              T* const (&dst)[K]) {
+    __shared__ T s_v[K][kTileRows][33];
     __shared__ unsigned s_m[kTileRows];
     __shared__ int s_lo[kTileRows], s_hi[kTileRows];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -126,7 +146,7 @@ __device__ __forceinline__ void colmajor_tile(const DevGrid& g, int i0, int ilas
     const int sc = threadIdx.x / kTileRows, sr = threadIdx.x % kTileRows;  // store: column, row
     for (int jc = ulo; jc <= uhi; jc += 32) {
         const int j = jc + lane;
-        double v[K];
+        T v[K];
         bool wr = false;
         if (j >= lo && j <= hi) wr = cell(i, j, v);
         const unsigned m = __ballot_sync(0xffffffffu, wr);
@@ -154,37 +174,45 @@ __device__ __forceinline__ void seg_flags_v(const DevGrid& g, const DevParams& p
     br2 = (last < g.M) || (last == g.M && (g.h[row * P + last] + g.h[(row - 1) * P + last]) * 0.5 == p.NANGDAY);
 }
 
-// Wall/open flags of a column segment (locate_segment_u, constant.cuh:156-178).
-// Erosion/deposition source terms of the suspended-sediment rows.
-__device__ __forceinline__ double source_chs(const DevParams& p, double wsm, double Zf, double fs, double fw,
-                                             double vth, double h_moi) {
+// Minimum / maximum in the arithmetic type of a kernel instantiation.
+__device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double rmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float rmin(float a, float b) { return fminf(a, b); }
+
+// Erosion/deposition source terms of the suspended-sediment rows, in the arithmetic type R
+// (double: the FP64 form; float: the mixed form's sediment transport).
+template <class R>
+__device__ __forceinline__ R source_chs(const DevParams& p, R wsm, R Zf, R fs, R fw, R vth, R h_moi) {
     // source_chs (Sediment_Transport.cu:12-49)
-    double toee = p.Toe;
-    const double todd = p.Tod;
-    double S = 0;
-    const double tob = p.ro * fw * (vth * vth);
-    if (h_moi > p.ghtoe) toee = p.Toe * (1 + p.hstoe * ((h_moi - p.ghtoe)));
-    if (tob > toee) S = p.Mbochat / p.ros * (tob - toee) / toee;
+    R toee = R(p.Toe);
+    const R todd = R(p.Tod);
+    R S = 0;
+    const R tob = R(p.ro) * fw * (vth * vth);
+    if (h_moi > R(p.ghtoe)) toee = R(p.Toe) * (1 + R(p.hstoe) * ((h_moi - R(p.ghtoe))));
+    if (tob > toee) S = R(p.Mbochat) / R(p.ros) * (tob - toee) / toee;
     else if (tob < todd) {
-        const double Pd = 1 - (tob / todd);
+        const R Pd = 1 - (tob / todd);
         // Pd^2.5 as Pd^2 sqrt(Pd) (0 < Pd <= 1): the same value to a few ulp, without pow's
         // general path
-        const double beta = 1 + (Zf / (1.25 + 4.75 * (Pd * Pd * sqrt(Pd))));
-        const double Cb = beta * fs;
+        const R beta = 1 + (Zf / (R(1.25) + R(4.75) * (Pd * Pd * sqrt(Pd))));
+        const R Cb = beta * fs;
         S = -wsm * Cb * Pd;
     }
     return S;
 }
 
-__device__ __forceinline__ double source_nchs(const DevParams& p, double wsm, double Zf, double Uf, double h_moi,
-                                              double fs) {
+template <class R>
+__device__ __forceinline__ R source_nchs(const DevParams& p, R wsm, R Zf, R Uf, R h_moi, R fs) {
     // source_nchs (Sediment_Transport.cu:52-60)
-    const double gamac = 0.434 + 5.975 * Zf + 2.888 * Zf * Zf;
-    const double Tx = fmax(0.0, (Uf * Uf - p.ufr * p.ufr) / (p.ufr * p.ufr));
-    const double Cac = 0.015 * p.dm * (Tx * sqrt(Tx)) * p.dxr_m03 / (0.05 * h_moi);  // Tx^1.5, Tx >= 0
+    const R gamac = R(0.434) + R(5.975) * Zf + R(2.888) * Zf * Zf;
+    const R ufr = R(p.ufr);
+    const R Tx = rmax(R(0), (Uf * Uf - ufr * ufr) / (ufr * ufr));
+    const R Cac = R(0.015) * R(p.dm) * (Tx * sqrt(Tx)) * R(p.dxr_m03) / (R(0.05) * h_moi);  // Tx^1.5, Tx >= 0
     return wsm * (Cac - gamac * fs);
 }
 
+// Wall/open flags of a column segment (locate_segment_u, constant.cuh:156-178).
 __device__ __forceinline__ void seg_flags_u(const DevGrid& g, const DevParams& p, int col, int first, int last,
                                             int& br1, int& br2) {
     const int P = g.P;

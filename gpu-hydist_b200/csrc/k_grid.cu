@@ -316,77 +316,101 @@ __device__ void boundary_channel_body(const DevGrid& g, const DevParams& p, doub
 }
 
 
+// The coefficient kernels below and the explicit momentum are templates on the arithmetic
+// type R: double for the FP64 form (the reference's operation order term by term), float for
+// the mixed form.  Every operand is read in FP64 and taken to R at its use; water-level
+// differences are taken in FP64 first (z is a datum plus small changes); the wet/dry tests
+// compare the stored FP64 depths, so both forms take the same branches.
+
 // Continuity and momentum coefficients of one wet cell of a UZ line (column j, cell i):
 // a2, c2, d2 (_uzSolver_calculate_preindex, UVZSolver_multithread.cu:402-406) and f1, f2,
 // f3, f5 (352-400).  Cell-local, so they are computed for every wet cell by a row-major
-// kernel and stored column-major for the column sweep.
-__device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& a2, double& c2,
-                                               double& d2, double& f1, double& f2, double& f3, double& f5) {
+// kernel and stored column-major for the column sweep.  Mixed form (R = float): the rows
+// of the level increment z' - z, i.e. d2 - z and f5 - f4 (z_i - z_i+1), f4 = 2 g dT / 2dX.
+template <class R>
+__device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, R& a2, R& c2, R& d2,
+                                               R& f1, R& f2, R& f3, R& f5) {
+    constexpr bool MIX = sizeof(R) == sizeof(float);
     const int P = g.P;
-    c2 = p.dTchia2dX * g.Htdu[pos];
-    a2 = -p.dTchia2dX * g.Htdu[pos - P];
-    d2 = g.z[pos] - p.dTchia2dY * (g.Htdv[pos] * g.v[pos] - g.Htdv[pos - 1] * g.v[pos - 1]);
-    double pp = 0.0, qq = 0.0;
+    auto L = [](const double* a, int q) { return R(a[q]); };
+    const R dTx = R(p.dTchia2dX), dTy = R(p.dTchia2dY), dT = R(p.dT), dXbp = R(p.dXbp), dY2 = R(p.dY2),
+            dYbp = R(p.dYbp);
+    c2 = dTx * L(g.Htdu, pos);
+    a2 = -dTx * L(g.Htdu, pos - P);
+    const R ydiv = dTy * (L(g.Htdv, pos) * L(g.v, pos) - L(g.Htdv, pos - 1) * L(g.v, pos - 1));
+    d2 = MIX ? -ydiv : R(g.z[pos]) - ydiv;
+    R pp = 0.0, qq = 0.0;
     const double* u = g.u;
     const double* H = g.H_moi;
-    const double vtb = (g.v[pos - 1] + g.v[pos] + g.v[pos + P - 1] + g.v[pos + P]) * 0.25;
-    f1 = p.dTchia2dX * u[pos] + g.VISC[pos] * p.dT / p.dXbp;
-    f2 = -(2 + g.Kx1[pos] * p.dT * sqrt(u[pos] * u[pos] + vtb * vtb) / g.Htdu[pos] + (2 * p.dT * g.VISC[pos]) / p.dXbp);
-    f3 = p.dT * g.VISC[pos] / p.dXbp - p.dTchia2dX * u[pos];
+    const R u0 = L(u, pos);
+    const R vtb = (L(g.v, pos - 1) + L(g.v, pos) + L(g.v, pos + P - 1) + L(g.v, pos + P)) * R(0.25);
+    f1 = dTx * u0 + L(g.VISC, pos) * dT / dXbp;
+    f2 = -(2 + L(g.Kx1, pos) * dT * sqrt(u0 * u0 + vtb * vtb) / L(g.Htdu, pos) + (2 * dT * L(g.VISC, pos)) / dXbp);
+    f3 = dT * L(g.VISC, pos) / dXbp - dTx * u0;
     if (H[pos - 1] <= p.H_TINH) {
         if (vtb < 0) {
-            pp = vtb * (-3 * u[pos] + 4 * u[pos + 1] - u[pos + 2]) / p.dY2;
-            qq = (u[pos] - 2 * u[pos + 1] + u[pos + 2]) / p.dYbp;
+            pp = vtb * (-3 * u0 + 4 * L(u, pos + 1) - L(u, pos + 2)) / dY2;
+            qq = (u0 - 2 * L(u, pos + 1) + L(u, pos + 2)) / dYbp;
         }
     } else {
         if (H[pos + 1] <= p.H_TINH) {
             if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
-                pp = vtb * (3 * u[pos] - 4 * u[pos - 1] + u[pos - 2]) / p.dY2;
-                qq = (u[pos] - 2 * u[pos - 1] + u[pos - 2]) / p.dYbp;
+                pp = vtb * (3 * u0 - 4 * L(u, pos - 1) + L(u, pos - 2)) / dY2;
+                qq = (u0 - 2 * L(u, pos - 1) + L(u, pos - 2)) / dYbp;
             }
         } else {
-            pp = vtb * (u[pos + 1] - u[pos - 1]) / p.dY2;
-            qq = (u[pos + 1] - 2 * u[pos] + u[pos - 1]) / p.dYbp;
+            pp = vtb * (L(u, pos + 1) - L(u, pos - 1)) / dY2;
+            qq = (L(u, pos + 1) - 2 * u0 + L(u, pos - 1)) / dYbp;
         }
     }
-    f5 = -2 * u[pos] + p.dT * pp - p.dT * p.CORIOLIS_FORCE * vtb - p.dT * g.VISC[pos] * qq -
-         p.dT * (p.windx - g.Tsxw[pos]) / g.Htdu[pos];
+    f5 = -2 * u0 + dT * pp - dT * R(p.CORIOLIS_FORCE) * vtb - dT * L(g.VISC, pos) * qq -
+         dT * (R(p.windx) - L(g.Tsxw, pos)) / L(g.Htdu, pos);
+    if (MIX) f5 -= R(2 * p.g * p.dTchia2dX) * R(g.z[pos] - g.z[pos + P]);
 }
 
 // Momentum and continuity coefficients of a VZ cell (preindex, _calculate_abcd:
 // UVZSolver_multithread.cu:345-349, 409-466 for the v direction): the terms the VZ sweep
 // combines into its rows, precomputed row-major so that the sweep's row building is loads.
-__device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& a2, double& c2,
-                                               double& d2, double& f1, double& f2, double& f3, double& f5) {
+// Mixed form as uz_cell_coeffs, with f4 = 2 g dT / 2dY and z_j+1.
+template <class R>
+__device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, R& a2, R& c2, R& d2,
+                                               R& f1, R& f2, R& f3, R& f5) {
+    constexpr bool MIX = sizeof(R) == sizeof(float);
     const int P = g.P;
-    c2 = p.dTchia2dY * g.Htdv[pos];
-    a2 = -p.dTchia2dY * g.Htdv[pos - 1];
-    d2 = g.z[pos] - p.dTchia2dX * (g.Htdu[pos] * g.u[pos] - g.Htdu[pos - P] * g.u[pos - P]);
+    auto L = [](const double* a, int q) { return R(a[q]); };
+    const R dTx = R(p.dTchia2dX), dTy = R(p.dTchia2dY), dT = R(p.dT), dX2 = R(p.dX2), dXbp = R(p.dXbp),
+            dYbp = R(p.dYbp);
+    c2 = dTy * L(g.Htdv, pos);
+    a2 = -dTy * L(g.Htdv, pos - 1);
+    const R xdiv = dTx * (L(g.Htdu, pos) * L(g.u, pos) - L(g.Htdu, pos - P) * L(g.u, pos - P));
+    d2 = MIX ? -xdiv : R(g.z[pos]) - xdiv;
     const double* v = g.v;
     const double* H = g.H_moi;
-    double pp = 0.0, qq = 0.0;
-    const double utb = (g.u[pos - P] + g.u[pos] + g.u[pos - P + 1] + g.u[pos + 1]) * 0.25;
-    f1 = p.dTchia2dY * v[pos] + g.VISC[pos] * p.dT / p.dYbp;
-    f2 = -(2 + g.Ky1[pos] * p.dT * sqrt(v[pos] * v[pos] + utb * utb) / g.Htdv[pos] + (2 * p.dT * g.VISC[pos]) / p.dYbp);
-    f3 = p.dT * g.VISC[pos] / p.dYbp - p.dTchia2dY * v[pos];
+    R pp = 0.0, qq = 0.0;
+    const R v0 = L(v, pos);
+    const R utb = (L(g.u, pos - P) + L(g.u, pos) + L(g.u, pos - P + 1) + L(g.u, pos + 1)) * R(0.25);
+    f1 = dTy * v0 + L(g.VISC, pos) * dT / dYbp;
+    f2 = -(2 + L(g.Ky1, pos) * dT * sqrt(v0 * v0 + utb * utb) / L(g.Htdv, pos) + (2 * dT * L(g.VISC, pos)) / dYbp);
+    f3 = dT * L(g.VISC, pos) / dYbp - dTy * v0;
     if (H[pos - P] <= p.H_TINH) {
         if (utb < 0) {
-            qq = utb * (-3 * v[pos] + 4 * v[pos + P] - v[pos + 2 * P]) / p.dX2;
-            pp = (v[pos] - 2 * v[pos + P] + v[pos + 2 * P]) / p.dXbp;
+            qq = utb * (-3 * v0 + 4 * L(v, pos + P) - L(v, pos + 2 * P)) / dX2;
+            pp = (v0 - 2 * L(v, pos + P) + L(v, pos + 2 * P)) / dXbp;
         }
     } else {
         if (H[pos + P] <= p.H_TINH) {
             if ((H[pos - 2 * P] > p.H_TINH) && (utb > 0)) {
-                qq = utb * (3 * v[pos] - 4 * v[pos - P] + v[pos - 2 * P]) / p.dX2;
-                pp = (v[pos] - 2 * v[pos - P] + v[pos - 2 * P]) / p.dXbp;
+                qq = utb * (3 * v0 - 4 * L(v, pos - P) + L(v, pos - 2 * P)) / dX2;
+                pp = (v0 - 2 * L(v, pos - P) + L(v, pos - 2 * P)) / dXbp;
             }
         } else {
-            qq = utb * (v[pos + P] - v[pos - P]) / p.dX2;
-            pp = (v[pos + P] - 2 * v[pos] + v[pos - P]) / p.dXbp;
+            qq = utb * (L(v, pos + P) - L(v, pos - P)) / dX2;
+            pp = (L(v, pos + P) - 2 * v0 + L(v, pos - P)) / dXbp;
         }
     }
-    f5 = -2 * v[pos] + p.dT * qq + p.dT * p.CORIOLIS_FORCE * utb - p.dT * g.VISC[pos] * pp -
-         p.dT * (p.windy - g.Tsyw[pos]) / g.Htdv[pos];
+    f5 = -2 * v0 + dT * qq + dT * R(p.CORIOLIS_FORCE) * utb - dT * L(g.VISC, pos) * pp -
+         dT * (R(p.windy) - L(g.Tsyw, pos)) / L(g.Htdv, pos);
+    if (MIX) f5 -= R(2 * p.g * p.dTchia2dY) * R(g.z[pos] - g.z[pos + 1]);
 }
 
 // The first launch of each half-step.  KIND 0 (half-step 1): UZ coefficients of every wet
@@ -400,7 +424,7 @@ __device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams
 // shared-memory tile (colmajor_tile), 8 rows of a column at a time.  The variants are
 // separate kernels: the tile's shared memory would otherwise shrink the L1 share of the
 // small grids' launches, whose stencil loads it serves.
-template <int KIND, int TILE>
+template <int KIND, int TILE, class R>
 __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int writes) {
     if (blockIdx.x == gridDim.x - 1) {
         __shared__ double s_t;
@@ -422,13 +446,14 @@ __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int wr
         return;
     }
     if constexpr (KIND == 0 && TILE) {
-        double* const dst[7] = {colT(g, 0), colT(g, 1), colT(g, 2), colT(g, 3), colT(g, 4), colT(g, 5), colT(g, 6)};
+        R* const dst[7] = {colTr<R>(g, 0), colTr<R>(g, 1), colTr<R>(g, 2), colTr<R>(g, 3),
+                           colTr<R>(g, 4), colTr<R>(g, 5), colTr<R>(g, 6)};
         colmajor_tile<7>(
             g, 2 + kTileRows * blockIdx.x, g.N, 2, g.M,
-            [&](int i, int j, double* v) {
+            [&](int i, int j, R* v) {
                 const int pos = i * g.P + j;
                 if (g.khouot[pos] != 0) return false;
-                uz_cell_coeffs(g, p, pos, v[0], v[1], v[2], v[3], v[4], v[5], v[6]);
+                uz_cell_coeffs<R>(g, p, pos, v[0], v[1], v[2], v[3], v[4], v[5], v[6]);
                 return true;
             },
             dst);
@@ -440,26 +465,26 @@ __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int wr
     for (int j = lo + lane; j <= hi; j += 32) {
         const int pos = i * g.P + j;
         if (g.khouot[pos] != 0) continue;
-        double a2, c2, d2, f1, f2, f3, f5;
+        R a2, c2, d2, f1, f2, f3, f5;
         if (KIND == 0) {
-            uz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
+            uz_cell_coeffs<R>(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
             const size_t t = (size_t)j * g.LT + i;
-            colT(g, 0)[t] = a2;
-            colT(g, 1)[t] = c2;
-            colT(g, 2)[t] = d2;
-            colT(g, 3)[t] = f1;
-            colT(g, 4)[t] = f2;
-            colT(g, 5)[t] = f3;
-            colT(g, 6)[t] = f5;
+            colTr<R>(g, 0)[t] = a2;
+            colTr<R>(g, 1)[t] = c2;
+            colTr<R>(g, 2)[t] = d2;
+            colTr<R>(g, 3)[t] = f1;
+            colTr<R>(g, 4)[t] = f2;
+            colTr<R>(g, 5)[t] = f3;
+            colTr<R>(g, 6)[t] = f5;
         } else {
-            vz_cell_coeffs(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
-            rowC(g, 0)[pos] = a2;
-            rowC(g, 1)[pos] = c2;
-            rowC(g, 2)[pos] = d2;
-            rowC(g, 3)[pos] = f1;
-            rowC(g, 4)[pos] = f2;
-            rowC(g, 5)[pos] = f3;
-            rowC(g, 6)[pos] = f5;
+            vz_cell_coeffs<R>(g, p, pos, a2, c2, d2, f1, f2, f3, f5);
+            rowCr<R>(g, 0)[pos] = a2;
+            rowCr<R>(g, 1)[pos] = c2;
+            rowCr<R>(g, 2)[pos] = d2;
+            rowCr<R>(g, 3)[pos] = f1;
+            rowCr<R>(g, 4)[pos] = f2;
+            rowCr<R>(g, 5)[pos] = f3;
+            rowCr<R>(g, 6)[pos] = f5;
         }
     }
 }
@@ -631,8 +656,48 @@ __global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restric
 
 // ----------------------------------------------------------- explicit momentum
 
+// vSolver (UVZSolver_multithread.cu:727-768) for one cell in the arithmetic type R: the new
+// v velocity.
+template <class R>
+__device__ __forceinline__ R ev_cell(const DevGrid& g, const DevParams& p, int row, int col) {
+    const int o = g.P;
+    const double *u = g.u, *v = g.v, *z = g.z, *t_u = g.t_u, *H = g.H_moi;
+    auto L = [](const double* a, int q) { return R(a[q]); };
+    R pp, q, tmp;
+    q = 0;
+    pp = 0;
+    tmp = 0;
+    const R v0 = L(v, row * o + col);
+    const R utb = (L(u, (row - 1) * o + col) + L(u, row * o + col) + L(u, (row - 1) * o + col + 1) + L(u, row * o + col + 1)) * R(0.25);
+    const R t_utb = (L(t_u, (row - 1) * o + col) + L(t_u, row * o + col) + L(t_u, (row - 1) * o + col + 1) + L(t_u, row * o + col + 1)) * R(0.25);
+    pp = (L(v, row * o + col + 1) - L(v, row * o + col - 1)) / R(p.dY2);
+    pp = R(p.HaiChiadT) + pp + L(g.Ky1, row * o + col) * sqrt(utb * utb + v0 * v0) / L(g.Htdv, row * o + col);
+    if (H[(row - 1) * o + col] <= p.H_TINH) {
+        if (utb < 0) {
+            q = t_utb * (-3 * v0 + 4 * L(v, (row + 1) * o + col) - L(v, (row + 2) * o + col)) / R(p.dX2);
+            tmp = (v0 - 2 * L(v, (row + 1) * o + col) + L(v, (row + 2) * o + col)) / R(p.dXbp);
+        }
+    } else {
+        if (H[(row + 1) * o + col] <= p.H_TINH) {
+            if ((H[(row - 2) * o + col] > p.H_TINH) && (utb > 0)) {
+                q = t_utb * (3 * v0 - 4 * L(v, (row - 1) * o + col) + L(v, (row - 2) * o + col)) / R(p.dX2);
+                tmp = (v0 - 2 * L(v, (row - 1) * o + col) + L(v, (row - 2) * o + col)) / R(p.dXbp);
+            }
+        } else {
+            q = t_utb * (L(v, (row + 1) * o + col) - L(v, (row - 1) * o + col)) / R(p.dX2);
+            tmp = (L(v, (row + 1) * o + col) - 2 * v0 + L(v, (row - 1) * o + col)) / R(p.dXbp);
+        }
+    }
+    q = R(p.HaiChiadT) * v0 - q - R(p.CORIOLIS_FORCE) * t_utb;
+    q = (q - R(p.g) * R(z[row * o + col + 1] - z[row * o + col]) / R(p.dY) +
+         L(g.VISC, row * o + col) * (tmp + (L(v, row * o + col + 1) - 2 * v0 + L(v, row * o + col - 1)) / R(p.dYbp))) +
+        (R(p.windy) - L(g.Tsyw, row * o + col)) / L(g.Htdv, row * o + col);
+    return q / pp;
+}
+
 // solveV/vSolver (UVZSolver_multithread.cu:1055-1071, 727-768) on row i, then
 // update_margin_elem_V (1008-1052) for the same row.
+template <class R>
 __global__ void k_explicit_v(DevGrid g, DevParams p) {
     extern __shared__ double sv[];  // the row's t_v over [k0, k1]
     __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL], s_first[HYD_SEGL], s_last[HYD_SEGL], s_off[HYD_SEGL + 1];
@@ -640,7 +705,6 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
     const int P = g.P, M = g.M;
     const int nseg = g.moci[row];
     if (nseg == 0) return;
-    const double *u = g.u, *v = g.v, *z = g.z, *t_u = g.t_u, *H = g.H_moi;
     // cells read or written: two before the first segment to one past the last
     const int k0 = max(g.daui[row * HYD_SEGL] - 2, 0);
     const int k1 = min(g.cuoii[row * HYD_SEGL + nseg - 1] + 1, M + 2);
@@ -666,43 +730,12 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
     __syncthreads();
     // every cell first..last-1 of every segment, packed segment after segment
     for (int c = threadIdx.x; c < s_off[nseg]; c += blockDim.x) {
-        {
-            int k = 0;
-            while (k + 1 < nseg && s_off[k + 1] <= c) k++;
-            const int col = s_first[k] + (c - s_off[k]);
-            const int o = P;
-            double pp, q, tmp;
-            q = 0;
-            pp = 0;
-            tmp = 0;
-            const double utb = (u[(row - 1) * o + col] + u[row * o + col] + u[(row - 1) * o + col + 1] + u[row * o + col + 1]) * 0.25;
-            const double t_utb = (t_u[(row - 1) * o + col] + t_u[row * o + col] + t_u[(row - 1) * o + col + 1] + t_u[row * o + col + 1]) * 0.25;
-            pp = (v[row * o + col + 1] - v[row * o + col - 1]) / p.dY2;
-            pp = p.HaiChiadT + pp + g.Ky1[row * o + col] * sqrt(utb * utb + v[row * o + col] * v[row * o + col]) / g.Htdv[row * o + col];
-            if (H[(row - 1) * o + col] <= p.H_TINH) {
-                if (utb < 0) {
-                    q = t_utb * (-3 * v[row * o + col] + 4 * v[(row + 1) * o + col] - v[(row + 2) * o + col]) / p.dX2;
-                    tmp = (v[row * o + col] - 2 * v[(row + 1) * o + col] + v[(row + 2) * o + col]) / p.dXbp;
-                }
-            } else {
-                if (H[(row + 1) * o + col] <= p.H_TINH) {
-                    if ((H[(row - 2) * o + col] > p.H_TINH) && (utb > 0)) {
-                        q = t_utb * (3 * v[row * o + col] - 4 * v[(row - 1) * o + col] + v[(row - 2) * o + col]) / p.dX2;
-                        tmp = (v[row * o + col] - 2 * v[(row - 1) * o + col] + v[(row - 2) * o + col]) / p.dXbp;
-                    }
-                } else {
-                    q = t_utb * (v[(row + 1) * o + col] - v[(row - 1) * o + col]) / p.dX2;
-                    tmp = (v[(row + 1) * o + col] - 2 * v[row * o + col] + v[(row - 1) * o + col]) / p.dXbp;
-                }
-            }
-            q = p.HaiChiadT * v[row * o + col] - q - p.CORIOLIS_FORCE * t_utb;
-            q = (q - p.g * (z[row * o + col + 1] - z[row * o + col]) / p.dY +
-                 g.VISC[row * o + col] * (tmp + (v[row * o + col + 1] - 2 * v[row * o + col] + v[row * o + col - 1]) / p.dYbp)) +
-                (p.windy - g.Tsyw[row * o + col]) / g.Htdv[row * o + col];
-            const double tv = q / pp;
-            g.t_v[row * o + col] = tv;
-            sv[col - k0] = tv;
-        }
+        int k = 0;
+        while (k + 1 < nseg && s_off[k + 1] <= c) k++;
+        const int col = s_first[k] + (c - s_off[k]);
+        const double tv = ev_cell<R>(g, p, row, col);
+        g.t_v[row * P + col] = tv;
+        sv[col - k0] = tv;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -721,42 +754,44 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
     __syncthreads();  // keep the other warps resident while thread 0 works
 }
 
-// solveU/uSolver (UVZSolver_multithread.cu:947-968, 773-815) on column j, then
-// update_margin_elem_U (970-1006).
-// uSolver (UVZSolver_multithread.cu:773-815) for one cell: the new u velocity.  Cell-local,
-// so it is computed for every wet cell by a row-major kernel and stored column-major.
-__device__ __forceinline__ double eu_cell(const DevGrid& g, const DevParams& p, int row, int col) {
+// uSolver (UVZSolver_multithread.cu:773-815) for one cell in the arithmetic type R: the new
+// u velocity.  Cell-local, so it is computed for every wet cell by a row-major kernel and
+// stored column-major.
+template <class R>
+__device__ __forceinline__ R eu_cell(const DevGrid& g, const DevParams& p, int row, int col) {
     const int P = g.P;
     const double *u = g.u, *v = g.v, *z = g.z, *t_v = g.t_v, *H = g.H_moi;
+    auto L = [](const double* a, int q) { return R(a[q]); };
     const int o = P;
-    double pp, q, tmp;
+    R pp, q, tmp;
     pp = 0;
     q = 0;
     tmp = 0;
-    const double vtb = (v[row * o + col - 1] + v[row * o + col] + v[(row + 1) * o + col - 1] + v[(row + 1) * o + col]) * 0.25;
-    const double t_vtb = (t_v[row * o + col - 1] + t_v[row * o + col] + t_v[(row + 1) * o + col - 1] + t_v[(row + 1) * o + col]) * 0.25;
-    pp = (u[(row + 1) * o + col] - u[(row - 1) * o + col]) / p.dX2;
-    pp = (p.HaiChiadT + pp + g.Kx1[row * o + col] * sqrt(vtb * vtb + u[row * o + col] * u[row * o + col]) / g.Htdu[row * o + col]);
+    const R u0 = L(u, row * o + col);
+    const R vtb = (L(v, row * o + col - 1) + L(v, row * o + col) + L(v, (row + 1) * o + col - 1) + L(v, (row + 1) * o + col)) * R(0.25);
+    const R t_vtb = (L(t_v, row * o + col - 1) + L(t_v, row * o + col) + L(t_v, (row + 1) * o + col - 1) + L(t_v, (row + 1) * o + col)) * R(0.25);
+    pp = (L(u, (row + 1) * o + col) - L(u, (row - 1) * o + col)) / R(p.dX2);
+    pp = (R(p.HaiChiadT) + pp + L(g.Kx1, row * o + col) * sqrt(vtb * vtb + u0 * u0) / L(g.Htdu, row * o + col));
     if (H[row * o + col - 1] <= p.H_TINH) {
         if (vtb < 0) {
-            q = t_vtb * (-3 * u[row * o + col] + 4 * u[row * o + col + 1] - u[row * o + col + 2]) / p.dY2;
-            tmp = (u[row * o + col] - 2 * u[row * o + col + 1] + u[row * o + col + 2]) / p.dYbp;
+            q = t_vtb * (-3 * u0 + 4 * L(u, row * o + col + 1) - L(u, row * o + col + 2)) / R(p.dY2);
+            tmp = (u0 - 2 * L(u, row * o + col + 1) + L(u, row * o + col + 2)) / R(p.dYbp);
         }
     } else {
         if (H[row * o + col + 1] <= p.H_TINH) {
             if ((H[row * o + col - 2] > p.H_TINH) && (vtb > 0)) {
-                q = t_vtb * (3 * u[row * o + col] - 4 * u[row * o + col - 1] + u[row * o + col - 2]) / p.dY2;
-                tmp = (u[row * o + col] - 2 * u[row * o + col - 1] + u[row * o + col - 2]) / p.dYbp;
+                q = t_vtb * (3 * u0 - 4 * L(u, row * o + col - 1) + L(u, row * o + col - 2)) / R(p.dY2);
+                tmp = (u0 - 2 * L(u, row * o + col - 1) + L(u, row * o + col - 2)) / R(p.dYbp);
             }
         } else {
-            q = t_vtb * (u[row * o + col + 1] - u[row * o + col - 1]) / p.dY2;
-            tmp = (u[row * o + col + 1] - 2 * u[row * o + col] + u[row * o + col - 1]) / p.dYbp;
+            q = t_vtb * (L(u, row * o + col + 1) - L(u, row * o + col - 1)) / R(p.dY2);
+            tmp = (L(u, row * o + col + 1) - 2 * u0 + L(u, row * o + col - 1)) / R(p.dYbp);
         }
     }
-    q = p.HaiChiadT * u[row * o + col] - q + p.CORIOLIS_FORCE * t_vtb;
-    q = (q - p.g * (z[(row + 1) * o + col] - z[row * o + col]) / p.dX +
-         g.VISC[row * o + col] * (tmp + (u[(row + 1) * o + col] - 2 * u[row * o + col] + u[(row - 1) * o + col]) / p.dXbp)) +
-        (p.windx - g.Tsxw[row * o + col]) / g.Htdu[row * o + col];
+    q = R(p.HaiChiadT) * u0 - q + R(p.CORIOLIS_FORCE) * t_vtb;
+    q = (q - R(p.g) * R(z[(row + 1) * o + col] - z[row * o + col]) / R(p.dX) +
+         L(g.VISC, row * o + col) * (tmp + (L(u, (row + 1) * o + col) - 2 * u0 + L(u, (row - 1) * o + col)) / R(p.dXbp))) +
+        (R(p.windx) - L(g.Tsxw, row * o + col)) / L(g.Htdu, row * o + col);
     return q / pp;
 }
 
@@ -766,7 +801,7 @@ constexpr int kEuSlot = 4;
 
 // explicit_u values of every wet cell of rows 2..N-1, columns 2..M, one warp per row over
 // the row's span; written column-major (g.colT array kEuSlot), with TILE through a tile.
-template <int TILE>
+template <int TILE, class R>
 __global__ void __launch_bounds__(256) k_coef_eu(DevGrid g, DevParams p) {
     if constexpr (!TILE) {
         const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
@@ -774,21 +809,24 @@ __global__ void __launch_bounds__(256) k_coef_eu(DevGrid g, DevParams p) {
         const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
         for (int j = lo + lane; j <= hi; j += 32) {
             if (g.khouot[i * g.P + j] != 0) continue;
-            colT(g, kEuSlot)[(size_t)j * g.LT + i] = eu_cell(g, p, i, j);
+            colTr<R>(g, kEuSlot)[(size_t)j * g.LT + i] = eu_cell<R>(g, p, i, j);
         }
     } else {
-        double* const dst[1] = {colT(g, kEuSlot)};
+        R* const dst[1] = {colTr<R>(g, kEuSlot)};
         colmajor_tile<1>(
             g, 2 + kTileRows * blockIdx.x, g.N - 1, 2, g.M,
-            [&](int i, int j, double* v) {
+            [&](int i, int j, R* v) {
                 if (g.khouot[i * g.P + j] != 0) return false;
-                v[0] = eu_cell(g, p, i, j);
+                v[0] = eu_cell<R>(g, p, i, j);
                 return true;
             },
             dst);
     }
 }
 
+// solveU/uSolver (UVZSolver_multithread.cu:947-968, 773-815) on column j from the values
+// k_coef_eu stored, then update_margin_elem_U (970-1006).
+template <class R>
 __global__ void k_explicit_u(DevGrid g, DevParams p) {
     extern __shared__ double su[];  // the column's t_u over [k0, k1]
     __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL], s_first[HYD_SEGL], s_last[HYD_SEGL], s_off[HYD_SEGL + 1];
@@ -824,7 +862,7 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
             int k = 0;
             while (k + 1 < nseg && s_off[k + 1] <= c) k++;
             const int row = s_first[k] + (c - s_off[k]);
-            const double tu = colT(g, kEuSlot)[(size_t)col * g.LT + row];  // k_coef_eu
+            const double tu = colTr<R>(g, kEuSlot)[(size_t)col * g.LT + row];  // k_coef_eu
             g.t_u[row * P + col] = tu;
             su[row - k0] = tu;
         }
@@ -1351,68 +1389,70 @@ __device__ void fs_edges_part(const DevGrid& g, const DevParams& p, int part, in
 
 // --------------------------------------------------------------------- sediment
 
-// Find_VTH (Sediment_Transport.cu:541-568) and hesoK (508-539) in one pass
 // The FSi row terms of a wet cell that depend on the cell alone
 // (_FSi_calculate__mactrix_coeff, Sediment_Transport.cu:62-165): gamav (evaluated after
 // Zf) and the source S, gated by t < bed_change_start, over the depth; into rowC arrays 0
-// and 1 for the FSi sweep that follows.  vth: the cell's new VTH.
-__device__ __forceinline__ void fsi_cell_terms(const DevGrid& g, const DevParams& p, int pos, double vth, double t) {
+// and 1 (in the arithmetic type R) for the FSi sweep that follows.  vth: the cell's new VTH.
+template <class R>
+__device__ __forceinline__ void fsi_cell_terms(const DevGrid& g, const DevParams& p, int pos, R vth, double t) {
     const double* FS = g.FS;
-    const double H = g.H_moi[pos];
-    const double c = 18 * log(12 * H / p.Ks);
-    const double Uf = sqrt(p.g) * fabs(vth) / c;
-    const double fq = 1 - FS[pos];
-    const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
-    double Zf = 0;
-    double S;
-    if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
-    if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], vth, H);
-    else S = source_nchs(p, wsm, Zf, Uf, H, FS[pos]);
+    const R H = R(g.H_moi[pos]);
+    const R FSp = R(FS[pos]);
+    const R c = 18 * log(12 * H / R(p.Ks));
+    const R Uf = sqrt(R(p.g)) * fabs(vth) / c;
+    const R fq = 1 - FSp;
+    const R wsm = R(p.wss) * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
+    R Zf = 0;
+    R S;
+    if (FS[pos] > 0.00001) Zf = wsm / (R(0.4) * (Uf + 2 * wsm));
+    if (p.ketdinh) S = source_chs<R>(p, wsm, Zf, FSp, R(g.Fw[pos]), vth, H);
+    else S = source_nchs<R>(p, wsm, Zf, Uf, H, FSp);
     if (t < p.bed_change_start) S = 0;
-    rowC(g, 0)[pos] = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;
-    rowC(g, 1)[pos] = S / H;
+    rowCr<R>(g, 0)[pos] = R(0.98) - R(0.198) * Zf + R(0.032) * Zf * Zf;
+    rowCr<R>(g, 1)[pos] = S / H;
 }
 
-// Find_VTH + hesoK for cell (i, j); FSI: also the FSi terms of the cell when it is wet.
-template <int FSI>
+// Find_VTH (Sediment_Transport.cu:541-568) and hesoK (508-539) for cell (i, j), in the
+// arithmetic type R; FSI: also the FSi terms of the cell when it is wet.
+template <int FSI, class R>
 __device__ __forceinline__ void vth_cell(const DevGrid& g, const DevParams& p, int i, int j) {
     const int N = g.N, M = g.M, P = g.P;
     if (i > N || j > M) return;
     const int pos = i * P + j;
     if (i >= 2 && j >= 2) {
-        double vth = 0;
+        R vth = 0;
         if ((g.htaiz[pos] > p.NANGDAY) && (g.H_moi[pos] > p.H_TINH)) {
-            const double ut = (g.t_u[pos] + g.t_u[pos - P]) * 0.5;
-            const double vt = (g.t_v[pos] + g.t_v[pos - 1]) * 0.5;
+            const R ut = (R(g.t_u[pos]) + R(g.t_u[pos - P])) * R(0.5);
+            const R vt = (R(g.t_v[pos]) + R(g.t_v[pos - 1])) * R(0.5);
             vth = sqrt(ut * ut + vt * vt);
         }
         g.VTH[pos] = vth;
-        if (FSI && i >= 3 && i < N && j <= M && g.khouot[pos] == 0) fsi_cell_terms(g, p, pos, vth, g.clock[1]);
+        if (FSI && i >= 3 && i < N && j <= M && g.khouot[pos] == 0) fsi_cell_terms<R>(g, p, pos, vth, g.clock[1]);
     }
-    const double sg = sqrt(p.g);
+    const R sg = sqrt(R(p.g));
     if (g.Htdu[pos] > 0 && pos >= 1) {
-        const double Cz = 18 * log(12 * g.Htdu[pos] / p.Ks);
-        const double kx = 5.93 * sg * (g.h[pos - 1] + g.h[pos]) * 0.25 * fabs(g.t_u[pos]) / Cz;
-        g.Kx[pos] = fmin(100.0, fmax(5.0, kx));
+        const R Cz = 18 * log(12 * R(g.Htdu[pos]) / R(p.Ks));
+        const R kx = R(5.93) * sg * (R(g.h[pos - 1]) + R(g.h[pos])) * R(0.25) * fabs(R(g.t_u[pos])) / Cz;
+        g.Kx[pos] = rmin(R(100.0), rmax(R(5.0), kx));
     }
     if (g.Htdv[pos] > 0 && pos >= P) {
-        const double Cz = 18 * log(12 * g.Htdv[pos] / p.Ks);
-        const double ky = 5.93 * sg * (g.h[pos - P] + g.h[pos]) * 0.25 * fabs(g.t_v[pos]) / Cz;
-        g.Ky[pos] = fmin(100.0, fmax(5.0, ky));
+        const R Cz = 18 * log(12 * R(g.Htdv[pos]) / R(p.Ks));
+        const R ky = R(5.93) * sg * (R(g.h[pos - P]) + R(g.h[pos])) * R(0.25) * fabs(R(g.t_v[pos])) / Cz;
+        g.Ky[pos] = rmin(R(100.0), rmax(R(5.0), ky));
     }
 }
 
-template <int FSI>
+template <int FSI, class R>
 __global__ void k_vth_hesok(DevGrid g, DevParams p) {
-    vth_cell<FSI>(g, p, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+    vth_cell<FSI, R>(g, p, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-template <int FSI>
+template <int FSI, class R>
 __global__ void k_vth_span(DevGrid g, DevParams p) {
     const RowLane rl(g, 0);
     const int i = rl.i;
     if (i > g.N) return;
-    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) vth_cell<FSI>(g, p, i, j);
+    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) vth_cell<FSI, R>(g, p, i, j);
 }
 
 // After a half-step's reset, in one launch: the state update (update_uvz + Htuongdoi)
@@ -1422,7 +1462,7 @@ __global__ void k_vth_span(DevGrid g, DevParams p) {
 // (the last kEdgeParts CTAs, reading t_u / t_v where the reference reads u / v after the
 // update).  None of the three writes what another reads.
 constexpr int kEdgeParts = 8;
-template <int ROWS, int VTH>
+template <int ROWS, int VTH, class R>
 __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
     extern __shared__ unsigned swords[];
     const int b = blockIdx.x;
@@ -1432,7 +1472,7 @@ __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
         if (i > g.N) return;
         for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
             post_cell(g, 1, i, j);
-            if (VTH) vth_cell<ROWS>(g, p, i, j);  // rows: the second half-step, before FSi
+            if (VTH) vth_cell<ROWS, R>(g, p, i, j);  // rows: the second half-step, before FSi
         }
         return;
     }
@@ -1724,12 +1764,16 @@ cudaError_t grid_setup(int N, int M) {
     cudaError_t e;
     if ((e = allow_smem((const void*)k_scan_dirty<1>, scan_smem(g))) != cudaSuccess) return e;
     if ((e = allow_smem((const void*)k_scan_dirty<0>, scan_smem(g))) != cudaSuccess) return e;
-    if ((e = allow_smem((const void*)k_post_fused<0, 0>, scan_smem(g))) != cudaSuccess) return e;
-    if ((e = allow_smem((const void*)k_post_fused<0, 1>, scan_smem(g))) != cudaSuccess) return e;
-    if ((e = allow_smem((const void*)k_post_fused<1, 0>, scan_smem(g))) != cudaSuccess) return e;
-    if ((e = allow_smem((const void*)k_post_fused<1, 1>, scan_smem(g))) != cudaSuccess) return e;
-    if ((e = allow_smem((const void*)k_explicit_u, sizeof(double) * (N + 3))) != cudaSuccess) return e;
-    if ((e = allow_smem((const void*)k_explicit_v, sizeof(double) * (M + 3))) != cudaSuccess) return e;
+    const void* fused[] = {(const void*)k_post_fused<0, 0, double>, (const void*)k_post_fused<0, 1, double>,
+                           (const void*)k_post_fused<1, 0, double>, (const void*)k_post_fused<1, 1, double>,
+                           (const void*)k_post_fused<0, 0, float>,  (const void*)k_post_fused<0, 1, float>,
+                           (const void*)k_post_fused<1, 0, float>,  (const void*)k_post_fused<1, 1, float>};
+    for (const void* f : fused)
+        if ((e = allow_smem(f, scan_smem(g))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_u<double>, sizeof(double) * (N + 3))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_v<double>, sizeof(double) * (M + 3))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_u<float>, sizeof(double) * (N + 3))) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_v<float>, sizeof(double) * (M + 3))) != cudaSuccess) return e;
     if ((e = allow_smem((const void*)k_reset<1>, reset_smem(M))) != cudaSuccess) return e;
     if ((e = allow_smem((const void*)k_reset<0>, reset_smem(N))) != cudaSuccess) return e;
     return cudaSuccess;
@@ -1801,9 +1845,15 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
 
 void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
     const int nb = ((g.N - 1) * 32 + 255) / 256 + 1;
-    if (half == 1) k_coef_bnd<1, 0><<<nb, 256, 0, s>>>(g, p, writes);
-    else if (g.tile_cols) k_coef_bnd<0, 1><<<nb, 256, 0, s>>>(g, p, writes);
-    else k_coef_bnd<0, 0><<<nb, 256, 0, s>>>(g, p, writes);
+    if (p.mixed) {
+        if (half == 1) k_coef_bnd<1, 0, float><<<nb, 256, 0, s>>>(g, p, writes);
+        else if (g.tile_cols) k_coef_bnd<0, 1, float><<<nb, 256, 0, s>>>(g, p, writes);
+        else k_coef_bnd<0, 0, float><<<nb, 256, 0, s>>>(g, p, writes);
+    } else {
+        if (half == 1) k_coef_bnd<1, 0, double><<<nb, 256, 0, s>>>(g, p, writes);
+        else if (g.tile_cols) k_coef_bnd<0, 1, double><<<nb, 256, 0, s>>>(g, p, writes);
+        else k_coef_bnd<0, 0, double><<<nb, 256, 0, s>>>(g, p, writes);
+    }
     hyd_kernel_launches_add(1);
 }
 
@@ -1833,18 +1883,26 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
 // The line kernels below take `threads` per CTA (a multiple of 32, at least 64), chosen
 // by the caller from the longest span of the direction.
 void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s) {
-    k_explicit_v<<<g.N - 1, threads, sizeof(double) * (g.M + 3), s>>>(g, p);
+    if (p.mixed) k_explicit_v<float><<<g.N - 1, threads, sizeof(double) * (g.M + 3), s>>>(g, p);
+    else k_explicit_v<double><<<g.N - 1, threads, sizeof(double) * (g.M + 3), s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
 void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s) {
-    if (g.tile_cols) k_coef_eu<1><<<((g.N - 2) * 32 + 255) / 256, 256, 0, s>>>(g, p);
-    else k_coef_eu<0><<<((g.N - 2) * 32 + 255) / 256, 256, 0, s>>>(g, p);
+    const int nb = ((g.N - 2) * 32 + 255) / 256;
+    if (p.mixed) {
+        if (g.tile_cols) k_coef_eu<1, float><<<nb, 256, 0, s>>>(g, p);
+        else k_coef_eu<0, float><<<nb, 256, 0, s>>>(g, p);
+    } else {
+        if (g.tile_cols) k_coef_eu<1, double><<<nb, 256, 0, s>>>(g, p);
+        else k_coef_eu<0, double><<<nb, 256, 0, s>>>(g, p);
+    }
     hyd_kernel_launches_add(1);
 }
 
 void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s) {
-    k_explicit_u<<<g.M - 1, threads, sizeof(double) * (g.N + 3), s>>>(g, p);
+    if (p.mixed) k_explicit_u<float><<<g.M - 1, threads, sizeof(double) * (g.N + 3), s>>>(g, p);
+    else k_explicit_u<double><<<g.M - 1, threads, sizeof(double) * (g.N + 3), s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
@@ -1882,12 +1940,16 @@ void launch_scan_rows(const DevGrid& g, const DevParams& p, cudaStream_t s) {
 void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, cudaStream_t s) {
     const int nbp = row_warps_blocks(g, g.N + 1), nbs = 32;
     const int grid = nbp + nbs + kEdgeParts;
-    if (rows) {
-        if (vth) k_post_fused<1, 1><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
-        else k_post_fused<1, 0><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
+    const size_t sm = scan_smem(g);
+    if (!vth) {  // no sediment terms: the FP64 kernel in both forms
+        if (rows) k_post_fused<1, 0, double><<<grid, 256, sm, s>>>(g, p, nbp, nbs);
+        else k_post_fused<0, 0, double><<<grid, 256, sm, s>>>(g, p, nbp, nbs);
+    } else if (p.mixed) {
+        if (rows) k_post_fused<1, 1, float><<<grid, 256, sm, s>>>(g, p, nbp, nbs);
+        else k_post_fused<0, 1, float><<<grid, 256, sm, s>>>(g, p, nbp, nbs);
     } else {
-        if (vth) k_post_fused<0, 1><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
-        else k_post_fused<0, 0><<<grid, 256, scan_smem(g), s>>>(g, p, nbp, nbs);
+        if (rows) k_post_fused<1, 1, double><<<grid, 256, sm, s>>>(g, p, nbp, nbs);
+        else k_post_fused<0, 1, double><<<grid, 256, sm, s>>>(g, p, nbp, nbs);
     }
     hyd_kernel_launches_add(1);
 }
@@ -1895,11 +1957,23 @@ void launch_post_fused(const DevGrid& g, const DevParams& p, int rows, int vth, 
 void launch_vth_hesok(const DevGrid& g, const DevParams& p, int full, int fsi, cudaStream_t s) {
     const dim3 b(32, 8);
     if (full) {
-        if (fsi) k_vth_hesok<1><<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
-        else k_vth_hesok<0><<<grid2d(g.M + 1, g.N + 1, b), b, 0, s>>>(g, p);
+        const dim3 gr = grid2d(g.M + 1, g.N + 1, b);
+        if (p.mixed) {
+            if (fsi) k_vth_hesok<1, float><<<gr, b, 0, s>>>(g, p);
+            else k_vth_hesok<0, float><<<gr, b, 0, s>>>(g, p);
+        } else {
+            if (fsi) k_vth_hesok<1, double><<<gr, b, 0, s>>>(g, p);
+            else k_vth_hesok<0, double><<<gr, b, 0, s>>>(g, p);
+        }
     } else {
-        if (fsi) k_vth_span<1><<<row_warps_blocks(g, g.N + 1), 256, 0, s>>>(g, p);
-        else k_vth_span<0><<<row_warps_blocks(g, g.N + 1), 256, 0, s>>>(g, p);
+        const int nb = row_warps_blocks(g, g.N + 1);
+        if (p.mixed) {
+            if (fsi) k_vth_span<1, float><<<nb, 256, 0, s>>>(g, p);
+            else k_vth_span<0, float><<<nb, 256, 0, s>>>(g, p);
+        } else {
+            if (fsi) k_vth_span<1, double><<<nb, 256, 0, s>>>(g, p);
+            else k_vth_span<0, double><<<nb, 256, 0, s>>>(g, p);
+        }
     }
     hyd_kernel_launches_add(1);
 }

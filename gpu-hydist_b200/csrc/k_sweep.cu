@@ -59,8 +59,8 @@ struct WarpG {
     static constexpr int size = 32;
     __device__ static __forceinline__ int rank() { return threadIdx.x & 31; }
     __device__ static __forceinline__ void sync() { __syncwarp(); }
-    __device__ static __forceinline__ void exchange(const double (&v)[6], int h, double (&lo)[6], double (&hi)[6],
-                                                    double*) {
+    template <class R>
+    __device__ static __forceinline__ void exchange(const R (&v)[6], int h, R (&lo)[6], R (&hi)[6]) {
 #pragma unroll
         for (int k = 0; k < 6; k++) {
             lo[k] = __shfl_up_sync(0xffffffffu, v[k], h);
@@ -92,18 +92,20 @@ __host__ __device__ inline int chunk_len(int R, int T) {
 // chunk-end rows of the reduced system on the chunk-end unknowns, ordered (x_s, x_e)
 // chunk after chunk and scaled to a unit diagonal: row 2t is (v[0], 1, v[1] | v[2]), row
 // 2t+1 is (v[3], 1, v[4] | v[5]) as (lower, diagonal, upper | right-hand side).
-__device__ __forceinline__ void chunk_reduce(double* A, double* B, double* C, double* D, int s, int e,
-                                             double (&v)[6]) {
+// Every solver function is a template on the arithmetic type R: double for the FP64 form,
+// float for the mixed form (the FP64 instantiation is the same code with R = double).
+template <class R>
+__device__ __forceinline__ void chunk_reduce(R* A, R* B, R* C, R* D, int s, int e, R (&v)[6]) {
     {
         int i = s + 1;
-        double r = 1.0 / B[i];
-        double cp = C[i] * r, dp = D[i] * r, ap = A[i] * r;
+        R r = R(1) / B[i];
+        R cp = C[i] * r, dp = D[i] * r, ap = A[i] * r;
         A[i] = ap;
         C[i] = cp;
         D[i] = dp;
         for (i = s + 2; i <= e; i++) {
-            const double ai = A[i];
-            r = 1.0 / (B[i] - ai * cp);
+            const R ai = A[i];
+            r = R(1) / (B[i] - ai * cp);
             cp = C[i] * r;
             dp = (D[i] - ai * dp) * r;
             ap = -(ai * ap) * r;
@@ -113,9 +115,9 @@ __device__ __forceinline__ void chunk_reduce(double* A, double* B, double* C, do
         }
     }
     {
-        double an = A[e - 1], cn = C[e - 1], dn = D[e - 1];
+        R an = A[e - 1], cn = C[e - 1], dn = D[e - 1];
         for (int i = e - 2; i >= s + 1; i--) {
-            const double ci = C[i];
+            const R ci = C[i];
             dn = D[i] - ci * dn;
             an = A[i] - ci * an;
             cn = -ci * cn;
@@ -124,8 +126,8 @@ __device__ __forceinline__ void chunk_reduce(double* A, double* B, double* C, do
             D[i] = dn;
         }
     }
-    const double cs = C[s];
-    const double ib = 1.0 / (B[s] - cs * A[s + 1]);
+    const R cs = C[s];
+    const R ib = R(1) / (B[s] - cs * A[s + 1]);
     v[0] = A[s] * ib;
     v[1] = -cs * C[s + 1] * ib;
     v[2] = (D[s] - cs * D[s + 1]) * ib;
@@ -135,8 +137,8 @@ __device__ __forceinline__ void chunk_reduce(double* A, double* B, double* C, do
 }
 
 // The chunk's inner unknowns from its end values; x goes to B.
-__device__ __forceinline__ void chunk_back(double* A, double* B, double* C, double* D, int s, int e, double xs,
-                                           double xe) {
+template <class R>
+__device__ __forceinline__ void chunk_back(R* A, R* B, R* C, R* D, int s, int e, R xs, R xe) {
     for (int i = s + 1; i < e; i++) B[i] = D[i] - A[i] * xs - C[i] * xe;
     B[s] = xs;
     B[e] = xe;
@@ -146,14 +148,15 @@ __device__ __forceinline__ void chunk_back(double* A, double* B, double* C, doub
 // rows per lane, in registers, exchanged by shuffles): at distance d row r eliminates rows
 // r - d and r + d, every row rescaled to a unit diagonal (one reciprocal per row and
 // level).  On return v[2] = x_s and v[5] = x_e of the lane's chunk.
-__device__ __forceinline__ void pcr_warp(double (&v)[6]) {
+template <class R>
+__device__ __forceinline__ void pcr_warp(R (&v)[6]) {
     constexpr int T = 32, n = 2 * T;
     const int t = threadIdx.x & 31;
     for (int d = 1; d < n; d <<= 1) {
-        double lo[6], hi[6];
+        R lo[6], hi[6];
         const int h = d == 1 ? 1 : d >> 1;
-        WarpG::exchange(v, h, lo, hi, nullptr);
-        double la[2], lc[2], ld[2], ha[2], hc[2], hd[2];
+        WarpG::exchange(v, h, lo, hi);
+        R la[2], lc[2], ld[2], ha[2], hc[2], hd[2];
         bool lv[2], hv[2];
         if (d == 1) {
             // row 2t: lo = row 2t-1 (lane t-1, second row), hi = row 2t+1 (own second row)
@@ -171,8 +174,8 @@ __device__ __forceinline__ void pcr_warp(double (&v)[6]) {
         }
 #pragma unroll
         for (int q = 0; q < 2; q++) {
-            const double a = v[3 * q], c = v[3 * q + 1];
-            double nA = 0.0, nC = 0.0, nB = 1.0, nD = v[3 * q + 2];
+            const R a = v[3 * q], c = v[3 * q + 1];
+            R nA = R(0), nC = R(0), nB = R(1), nD = v[3 * q + 2];
             if (lv[q]) {
                 nA = -la[q] * a;
                 nB -= lc[q] * a;
@@ -183,7 +186,7 @@ __device__ __forceinline__ void pcr_warp(double (&v)[6]) {
                 nB -= ha[q] * c;
                 nD -= hd[q] * c;
             }
-            const double ib = 1.0 / nB;
+            const R ib = R(1) / nB;
             v[3 * q] = nA * ib;
             v[3 * q + 1] = nC * ib;
             v[3 * q + 2] = nD * ib;
@@ -193,10 +196,11 @@ __device__ __forceinline__ void pcr_warp(double (&v)[6]) {
 
 // One warp: rows [0, 32 m), chunks of m rows per lane, the reduced system by pcr_warp.
 // On return B[r] holds x[r].
-__device__ __forceinline__ void solve_warp(double* A, double* B, double* C, double* D, int m) {
+template <class R>
+__device__ __forceinline__ void solve_warp(R* A, R* B, R* C, R* D, int m) {
     const int t = threadIdx.x & 31;
     const int s = t * m, e = s + m - 1;
-    double v[6];
+    R v[6];
     chunk_reduce(A, B, C, D, s, e, v);
     pcr_warp(v);
     chunk_back(A, B, C, D, s, e, v[2], v[5]);
@@ -228,28 +232,29 @@ __host__ __device__ inline SolvePlan solve_plan(int R, int max_t1) {
 
 // Two-level solve by a CTA (rows [0, t1 m)); red holds 4 kRedRows doubles.  Every thread
 // of the CTA calls it.  On return B[r] holds x[r].
-__device__ __forceinline__ void solve_block(double* A, double* B, double* C, double* D, SolvePlan pl, double* red) {
+template <class R>
+__device__ __forceinline__ void solve_block(R* A, R* B, R* C, R* D, SolvePlan pl, R* red) {
     const int t = threadIdx.x;
     const int m2 = chunk_len(2 * pl.t1, 32);
-    double *rA = red, *rB = red + kRedRows, *rC = red + 2 * kRedRows, *rD = red + 3 * kRedRows;
+    R *rA = red, *rB = red + kRedRows, *rC = red + 2 * kRedRows, *rD = red + 3 * kRedRows;
     if (t < pl.t1) {
         const int s = t * pl.m, e = s + pl.m - 1;
-        double v[6];
+        R v[6];
         chunk_reduce(A, B, C, D, s, e, v);
         rA[2 * t] = v[0];
-        rB[2 * t] = 1.0;
+        rB[2 * t] = R(1);
         rC[2 * t] = v[1];
         rD[2 * t] = v[2];
         rA[2 * t + 1] = v[3];
-        rB[2 * t + 1] = 1.0;
+        rB[2 * t + 1] = R(1);
         rC[2 * t + 1] = v[4];
         rD[2 * t + 1] = v[5];
     }
     for (int r = 2 * pl.t1 + t; r < 32 * m2; r += blockDim.x) {  // identity rows
-        rA[r] = 0.0;
-        rB[r] = 1.0;
-        rC[r] = 0.0;
-        rD[r] = 0.0;
+        rA[r] = R(0);
+        rB[r] = R(1);
+        rC[r] = R(0);
+        rD[r] = R(0);
     }
     __syncthreads();
     if (t < 32) solve_warp(rA, rB, rC, rD, m2);
@@ -264,20 +269,20 @@ __device__ __forceinline__ void solve_block(double* A, double* B, double* C, dou
 // Serial Thomas over the packed rows by the group's first thread, in the reference's
 // operation order (tridiag, UVZSolver_multithread.cu:203-228); decoupled segments solve
 // exactly as separate systems.  Used to check the partitioned solver.
-template <class G>
-__device__ __forceinline__ void solve_thomas(double* A, double* B, double* C, double* D, int rows) {
+template <class G, class R>
+__device__ __forceinline__ void solve_thomas(R* A, R* B, R* C, R* D, int rows) {
     if (G::rank() == 0 && rows > 0) {
-        double Ap = -C[0] / B[0], Bp = D[0] / B[0];
+        R Ap = -C[0] / B[0], Bp = D[0] / B[0];
         C[0] = Ap;
         D[0] = Bp;
         for (int i = 1; i < rows; i++) {
-            const double ep = A[i] * Ap + B[i];
+            const R ep = A[i] * Ap + B[i];
             Ap = -C[i] / ep;
             Bp = (D[i] - (A[i] * Bp)) / ep;
             C[i] = Ap;
             D[i] = Bp;
         }
-        double x = D[rows - 1];
+        R x = D[rows - 1];
         B[rows - 1] = x;
         for (int i = rows - 2; i >= 0; i--) {
             x = D[i] + (C[i] * x);
@@ -290,9 +295,8 @@ __device__ __forceinline__ void solve_thomas(double* A, double* B, double* C, do
 // Solve of a line's packed system (rows padded with identity rows to pl.t1 * pl.m) by
 // group G: one warp (a warp group, or a CTA's first warp with the others waiting), or
 // the two-level solve of a CTA.
-template <class G, int SOLVER>
-__device__ __forceinline__ void solve_line(double* A, double* B, double* C, double* D, SolvePlan pl, int rows,
-                                           double* red) {
+template <class G, int SOLVER, class R>
+__device__ __forceinline__ void solve_line(R* A, R* B, R* C, R* D, SolvePlan pl, int rows, R* red) {
     if (SOLVER == 0) {
         if (G::size == 32) {
             solve_warp(A, B, C, D, pl.m);
@@ -303,7 +307,7 @@ __device__ __forceinline__ void solve_line(double* A, double* B, double* C, doub
             solve_block(A, B, C, D, pl, red);
         }
     } else {
-        solve_thomas<G>(A, B, C, D, rows);
+        solve_thomas<G, R>(A, B, C, D, rows);
     }
 }
 
@@ -316,6 +320,7 @@ struct LineShared {
     int co[HYD_SEGL + 1];    // packed cell offset of each segment
     int ro[HYD_SEGL + 1];    // packed row offset of each segment
     double tzl[HYD_SEGL], tzr[HYD_SEGL];
+    double zl[HYD_SEGL], zr[HYD_SEGL];  // mixed form: z at the segment ends (the increments' base)
     int nseg, R, C;
 };
 
@@ -339,7 +344,7 @@ __device__ __forceinline__ int seg_of_row(const LineShared& sg, int c) { return 
 
 // Segments of the line, their system sizes (_calculate_matrix_coeff,
 // UVZSolver_multithread.cu:515-592) and packed offsets, into sg.
-template <int DIR, class G>
+template <int DIR, class G, bool MIX>
 __device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p, int line, LineShared& sg) {
     const int tid = G::rank();
     const int L = DIR == 0 ? g.N : g.M;
@@ -383,6 +388,10 @@ __device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p
         sg.lastKind[tid] = kind;
         sg.tzl[tid] = g.t_z[base + f * along];
         sg.tzr[tid] = g.t_z[base + l * along];
+        if (MIX) {
+            sg.zl[tid] = g.z[base + f * along];
+            sg.zr[tid] = g.z[base + l * along];
+        }
     }
     G::sync();
     if (tid == 0) {
@@ -405,10 +414,14 @@ __device__ __forceinline__ void hydro_setup(const DevGrid& g, const DevParams& p
 
 // Phases A-D of one line by group G.  Rows A, B, Cc, D hold at least pl.t1 * pl.m
 // entries, ends kEnds; red: the two-level solve's reduced rows.
-template <int DIR, int SOLVER, class G>
+// R = float: the mixed form.  Its coefficients (k_coef_bnd's FP32 arrays) are those of the
+// level increment dz = z' - z: the continuity right-hand side d2 - z and the momentum
+// f5 - f4 (z_k - z_k+1), so that the same rows solve for (dz, u) in FP32; the prescribed
+// levels enter as increments, and the new level is z + dz in FP64.
+template <int DIR, int SOLVER, class G, class R>
 __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p, int line, const LineShared& sg,
-                                           double* A, double* B, double* Cc, double* D, double* ends, double* red,
-                                           SolvePlan pl) {
+                                           R* A, R* B, R* Cc, R* D, R* ends, R* red, SolvePlan pl) {
+    constexpr bool MIX = sizeof(R) == sizeof(float);
     constexpr int T = G::size;
     const int tid = G::rank();
     const int N = g.N, M = g.M, P = g.P;
@@ -417,35 +430,35 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     const int along = DIR == 0 ? P : 1;  // offset to the next cell of the line
     const int base = DIR == 0 ? line : line * P;
     double* tvel = DIR == 0 ? g.t_u : g.t_v;
-    const double bq_first = DIR == 0 ? g.ubt[line] : g.vbd[line];  // ubt_or_vbd
-    const double bq_last = DIR == 0 ? g.ubp[line] : g.vbt[line];   // ubp_or_vbt
+    const R bq_first = R(DIR == 0 ? g.ubt[line] : g.vbd[line]);  // ubt_or_vbd
+    const R bq_last = R(DIR == 0 ? g.ubp[line] : g.vbt[line]);   // ubp_or_vbt
     const int nseg = sg.nseg;
-    const int C = sg.C, R = sg.R;
+    const int C = sg.C, Rn = sg.R;
 
     // ---- A + B1, one pass over the cells: the continuity coefficients of the cell and of
     // the next one (preindex, UVZSolver_multithread.cu:402-406 / 345-349), the momentum
     // coefficients (preindex f1..f5, _calculate_abcd 409-466) and the rows.  The continuity
     // coefficients of each segment's first and last cell are kept for the extraction.
-    auto cont = [&](int k, double& a, double& c, double& d) {
+    auto cont = [&](int k, R& a, R& c, R& d) {
         if (DIR == 0) {
             const size_t t = (size_t)line * g.LT + k;  // precomputed by k_coef_bnd<0>
-            a = colT(g, 0)[t];
-            c = colT(g, 1)[t];
-            d = colT(g, 2)[t];
+            a = colTr<R>(g, 0)[t];
+            c = colTr<R>(g, 1)[t];
+            d = colTr<R>(g, 2)[t];
         } else {
             const int pos = base + k * along;  // precomputed by k_coef_bnd<1>
-            a = rowC(g, 0)[pos];
-            c = rowC(g, 1)[pos];
-            d = rowC(g, 2)[pos];
+            a = rowCr<R>(g, 0)[pos];
+            c = rowCr<R>(g, 1)[pos];
+            d = rowCr<R>(g, 2)[pos];
         }
     };
-    for (int r = R + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
-        A[r] = 0.0;
-        B[r] = 1.0;
-        Cc[r] = 0.0;
-        D[r] = 0.0;
+    for (int r = Rn + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
+        A[r] = R(0);
+        B[r] = R(1);
+        Cc[r] = R(0);
+        D[r] = R(0);
     }
-    const double f4 = DIR == 0 ? 2 * p.g * p.dTchia2dX : 2 * p.g * p.dTchia2dY;
+    const R f4 = R(DIR == 0 ? 2 * p.g * p.dTchia2dX : 2 * p.g * p.dTchia2dY);
     for (int c = tid; c < C; c += T) {
         const int sI = seg_of(sg, c);
         const int f = sg.first[sI], l = sg.last[sI];
@@ -458,21 +471,21 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         const int rel = 2 * (k - f);  // row 2k relative to the segment's first row 2f
         // every coefficient the cell may need, loaded at once (the next cell's and f1..f5
         // are in bounds even where unused: k + 1 <= L + 1 inside the padded line)
-        double ac, cc, dc, an, cn, dn, f1, f2, f3, f5;
+        R ac, cc, dc, an, cn, dn, f1, f2, f3, f5;
         cont(k, ac, cc, dc);
         cont(k + 1, an, cn, dn);
         if (DIR == 0) {
             const size_t t = (size_t)line * g.LT + k;
-            f1 = colT(g, 3)[t];
-            f2 = colT(g, 4)[t];
-            f3 = colT(g, 5)[t];
-            f5 = colT(g, 6)[t];
+            f1 = colTr<R>(g, 3)[t];
+            f2 = colTr<R>(g, 4)[t];
+            f3 = colTr<R>(g, 5)[t];
+            f5 = colTr<R>(g, 6)[t];
         } else {
             const int pos = base + k * along;
-            f1 = rowC(g, 3)[pos];
-            f2 = rowC(g, 4)[pos];
-            f3 = rowC(g, 5)[pos];
-            f5 = rowC(g, 6)[pos];
+            f1 = rowCr<R>(g, 3)[pos];
+            f2 = rowCr<R>(g, 4)[pos];
+            f3 = rowCr<R>(g, 5)[pos];
+            f5 = rowCr<R>(g, 6)[pos];
         }
         if (k == f) {
             ends[6 * sI] = ac;
@@ -486,7 +499,7 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         }
         if (tR && rel <= sn) {
             A[r0 + rel] = ac;
-            B[r0 + rel] = 1.0;
+            B[r0 + rel] = R(1);
             Cc[r0 + rel] = cc;
             D[r0 + rel] = dc;
         }
@@ -494,7 +507,7 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         if (Ls <= 1 && k != f) continue;
         const int rm = tR ? rel + 1 : rel;  // the momentum row of this cell
         if (rm > sn) continue;
-        double ra, rb, rc, rd;
+        R ra, rb, rc, rd;
         if (Ls >= 2) {
             if (k == f && b1f) {
                 ra = f4;
@@ -524,7 +537,7 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         D[r0 + rm] = rd;
         if (!tR && rel + 1 <= sn) {
             A[r0 + rel + 1] = an;
-            B[r0 + rel + 1] = 1.0;
+            B[r0 + rel + 1] = R(1);
             Cc[r0 + rel + 1] = cn;
             D[r0 + rel + 1] = dn;
         }
@@ -535,10 +548,13 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     if (tid < nseg && sg.sn[tid] >= 0) {
         const int sn = sg.sn[tid];
         const int rowF = sg.ro[tid], rowL = rowF + sn;
-        const double oA = A[rowL], oB = B[rowL], oC = Cc[rowL], oD = D[rowL];
+        const R oA = A[rowL], oB = B[rowL], oC = Cc[rowL], oD = D[rowL];
+        // the prescribed end levels (increments over z in the mixed form)
+        const R tzl = MIX ? R(sg.tzl[tid] - sg.zl[tid]) : R(sg.tzl[tid]);
+        const R tzr = MIX ? R(sg.tzr[tid] - sg.zr[tid]) : R(sg.tzr[tid]);
         if (!sg.br1[tid]) {
             if (sg.typeR[tid]) D[rowF] = D[rowF] - A[rowF] * bq_first;
-            else D[rowF] = D[rowF] - A[rowF] * sg.tzl[tid];
+            else D[rowF] = D[rowF] - A[rowF] * tzl;
         }
         // the end-row statement always rewrites AA, BB, DD of the last row; for a
         // single-row system that undoes the first-row override (UVZSolver_multithread.cu:574-590)
@@ -546,18 +562,22 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         B[rowL] = oB;
         const int kind = sg.lastKind[tid];
         if (kind == 1) D[rowL] = oD - oC * bq_last;
-        else if (kind == 2) D[rowL] = oD - oC * sg.tzr[tid];
+        else if (kind == 2) D[rowL] = oD - oC * tzr;
         else D[rowL] = oD;
-        A[rowF] = 0.0;
-        Cc[rowL] = 0.0;
+        A[rowF] = R(0);
+        Cc[rowL] = R(0);
     }
     G::sync();
 
     // ---- C: solve
-    solve_line<G, SOLVER>(A, B, Cc, D, pl, R, red);
+    solve_line<G, SOLVER, R>(A, B, Cc, D, pl, Rn, red);
 
     // ---- D: extract (_uzSolver_extract_solution 668-723 / _vzSolver_extract_solution 595-665)
-    const double* x = B;
+    const R* x = B;
+    // a solved level: the unknown itself, or z + the increment in FP64 (mixed form); a
+    // prescribed level as the rows use it
+    auto put_z = [&](int pos, R xz) { g.t_z[pos] = MIX ? g.z[pos] + (double)xz : (double)xz; };
+    auto row_z = [&](int pos) { return MIX ? R(g.t_z[pos] - g.z[pos]) : R(g.t_z[pos]); };
     const int QF = DIR == 0 ? g.bienQ[2] : g.bienQ[1];
     const int QL = DIR == 0 ? g.bienQ[3] : g.bienQ[0];
     for (int c = tid; c < C; c += T) {
@@ -571,30 +591,30 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
         const int pos = base + k * along;
         if (k < l) {
             if (b1f || qfirst) {
-                g.t_z[pos] = x[r0 + 2 * k];
+                put_z(pos, x[r0 + 2 * k]);
                 tvel[pos] = x[r0 + 2 * k + 1];
-                if (k == f) tvel[pos - along] = b1f ? 0.0 : bq_first;
+                if (k == f) tvel[pos - along] = b1f ? R(0) : bq_first;
             } else if (k == f) {
-                const double tv = x[r0 + 2 * f];
+                const R tv = x[r0 + 2 * f];
                 tvel[pos] = tv;
-                tvel[pos - along] = (ends[6 * sI + 2] - g.t_z[pos] - ends[6 * sI + 1] * tv) / ends[6 * sI];
+                tvel[pos - along] = (ends[6 * sI + 2] - row_z(pos) - ends[6 * sI + 1] * tv) / ends[6 * sI];
             } else {
-                g.t_z[pos] = x[r0 + 2 * k - 1];
+                put_z(pos, x[r0 + 2 * k - 1]);
                 tvel[pos] = x[r0 + 2 * k];
             }
         } else {
-            const double xl = sn >= 0 ? x[r0 + 2 * f + sn] : 0.0;
+            const R xl = sn >= 0 ? x[r0 + 2 * f + sn] : R(0);
             if (b2f) {
-                tvel[pos] = 0.0;
-                g.t_z[pos] = xl;
+                tvel[pos] = R(0);
+                put_z(pos, xl);
             } else if (QL && l == L) {
                 tvel[pos] = bq_last;
-                g.t_z[pos] = xl;
+                put_z(pos, xl);
             } else {
-                double tprev;
+                R tprev;
                 if (l > f) tprev = (b1f || qfirst) ? x[r0 + 2 * l - 1] : x[r0 + 2 * l - 2];
-                else tprev = tvel[pos - along];
-                tvel[pos] = (ends[6 * sI + 5] - ends[6 * sI + 3] * tprev - g.t_z[pos]) / ends[6 * sI + 4];
+                else tprev = R(tvel[pos - along]);
+                tvel[pos] = (ends[6 * sI + 5] - ends[6 * sI + 3] * tprev - row_z(pos)) / ends[6 * sI + 4];
             }
         }
     }
@@ -608,14 +628,17 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
 // Adjacent long lines (a wet band) fall on different CTAs.  Warps with nothing to sweep
 // wait at the CTA barriers rather than exit: the warp-synchronous steps of a warp whose
 // sibling warps had exited were measured an order of magnitude slower on B200.
-template <int DIR, int SOLVER>
+template <int DIR, int SOLVER, class R>
 __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB,
-                                                     double* gscr, int RG, int roww) {
-    extern __shared__ double dyn_smem[];
+                                                     double* gscr_d, int RG, int roww) {
+    constexpr bool MIX = sizeof(R) == sizeof(float);
+    extern __shared__ double dyn_smem_d[];
+    R* dyn_smem = reinterpret_cast<R*>(dyn_smem_d);
+    R* gscr = reinterpret_cast<R*>(gscr_d);
     __shared__ LineShared sgw[kWL];
     __shared__ int s_long[kWL];
     __shared__ int s_nlong;
-    __shared__ double s_red[4 * kRedRows];  // reduced rows of the two-level solve
+    __shared__ R s_red[4 * kRedRows];  // reduced rows of the two-level solve
     const int w = threadIdx.x >> 5;
     const int nlines = endidx - startidx + 1;
     const int G = gridDim.x;
@@ -623,19 +646,19 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
         const int li = blockIdx.x + (j0 + w) * G;
         LineShared& sg = sgw[w];
         if (threadIdx.x == 0) s_nlong = 0;
-        if (li < nlines) hydro_setup<DIR, WarpG>(g, p, startidx + li, sg);  // warp-uniform
+        if (li < nlines) hydro_setup<DIR, WarpG, MIX>(g, p, startidx + li, sg);  // warp-uniform
         __syncthreads();
         if (li < nlines && sg.nseg > 0) {
             if (sg.R > roww) {
                 if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
             } else {
                 const int wr = slice_rows(roww);
-                double* A = dyn_smem + w * (4 * wr + kEnds);
-                double* B = A + wr;
-                double* Cc = B + wr;
-                double* D = Cc + wr;
-                hydro_body<DIR, SOLVER, WarpG>(g, p, startidx + li, sg, A, B, Cc, D, D + wr, nullptr,
-                                               SolvePlan{32, chunk_len(sg.R, 32)});
+                R* A = dyn_smem + w * (4 * wr + kEnds);
+                R* B = A + wr;
+                R* Cc = B + wr;
+                R* D = Cc + wr;
+                hydro_body<DIR, SOLVER, WarpG, R>(g, p, startidx + li, sg, A, B, Cc, D, D + wr, nullptr,
+                                                  SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
         __syncthreads();
@@ -647,11 +670,11 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
             const SolvePlan pl = solve_plan(sl.R, SOLVER == 0 ? 256 : 32);
             const bool fits = pl.t1 * pl.m <= RB;
             const int rs = fits ? RB : RG;
-            double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * (4 * (size_t)RG + kEnds);
-            double* B = A + rs;
-            double* Cc = B + rs;
-            double* D = Cc + rs;
-            hydro_body<DIR, SOLVER, BlockG>(g, p, line, sl, A, B, Cc, D, D + rs, s_red, pl);
+            R* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * (4 * (size_t)RG + kEnds);
+            R* B = A + rs;
+            R* Cc = B + rs;
+            R* D = Cc + rs;
+            hydro_body<DIR, SOLVER, BlockG, R>(g, p, line, sl, A, B, Cc, D, D + rs, s_red, pl);
             __syncthreads();  // the slices and sgw are reused
         }
     }
@@ -659,78 +682,87 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
 
 // ---- sediment sweeps --------------------------------------------------------------
 
-// Row of the sediment system for one interior wet cell before the segment-end terms
-// (_FSj/_FSi_calculate__mactrix_coeff, Sediment_Transport.cu:205-302 / 62-165): aa, bb,
-// cc, dd of the row, with the source S gated by t < bed_change_start.
+// The sediment rows in the arithmetic type R (double: the FP64 form; float: the mixed
+// form).  Every operand is read in FP64 and taken to R at its use; the wet/dry tests on
+// the depths compare the stored FP64 values, so both forms take the same branches.
+
 // Row of the FSj system for one interior wet cell before the segment-end terms
 // (_FSj_calculate__mactrix_coeff, Sediment_Transport.cu:205-302): aa, bb, cc, dd of the row,
 // with the source S gated by t < bed_change_start.
-__device__ __forceinline__ void fsj_cell_coeffs(const DevGrid& g, const DevParams& p, double t, int pos, double& aa,
-                                                double& bb, double& cc, double& dd) {
+template <class R>
+__device__ __forceinline__ void fsj_cell_coeffs(const DevGrid& g, const DevParams& p, double t, int pos, R& aa, R& bb,
+                                                R& cc, R& dd) {
     const int P = g.P;
     const double* FS = g.FS;
     const double* H = g.H_moi;
+    auto L = [](const double* a, int q) { return R(a[q]); };
+    const R Hp = L(H, pos), FSp = L(FS, pos), VTHp = L(g.VTH, pos);
     const double s_start = p.bed_change_start;
-    const double sqrtg = sqrt(p.g);
-    const double c = 18 * log(12 * H[pos] / p.Ks);
-    const double Uf = sqrtg * fabs(g.VTH[pos]) / c;
-    const double fq = 1 - FS[pos];
-    const double wsm = p.wss * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
-    double Zf = 0;
-    double S;
-    const double gamav = 0.98 - 0.198 * Zf + 0.032 * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
-    if (FS[pos] > 0.00001) Zf = wsm / (0.4 * (Uf + 2 * wsm));
-    if (p.ketdinh) S = source_chs(p, wsm, Zf, FS[pos], g.Fw[pos], g.VTH[pos], H[pos]);
-    else S = source_nchs(p, wsm, Zf, Uf, H[pos], FS[pos]);
+    const R sqrtg = sqrt(R(p.g));
+    const R c = 18 * log(12 * Hp / R(p.Ks));
+    const R Uf = sqrtg * fabs(VTHp) / c;
+    const R fq = 1 - FSp;
+    const R wsm = R(p.wss) * ((fq * fq) * (fq * fq));  // wss (1 - FS)^4
+    R Zf = 0;
+    R S;
+    const R gamav = R(0.98) - R(0.198) * Zf + R(0.032) * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
+    if (FS[pos] > 0.00001) Zf = wsm / (R(0.4) * (Uf + 2 * wsm));
+    if (p.ketdinh) S = source_chs<R>(p, wsm, Zf, FSp, L(g.Fw, pos), VTHp, Hp);
+    else S = source_nchs<R>(p, wsm, Zf, Uf, Hp, FSp);
     if (t < s_start) S = 0;
     // FSj runs right after the half-step's state update, which left u = t_u and v = t_v
     // on every cell it reads; reading u and v lets it run beside the next half-step's
     // sweeps, which write t_u and t_v
     const double *u = g.u, *v = g.v;
-    aa = -gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos - P] * g.Kx[pos - P] / (H[pos] * (p.dXbp));
-    cc = gamav * 0.5 * (u[pos] + u[pos - P]) / p.dX2 - g.Htdu[pos] * g.Kx[pos] / (H[pos] * (p.dXbp));
-    bb = p.HaiChiadT + (g.Htdu[pos] * g.Kx[pos] + g.Htdu[pos - P] * g.Kx[pos - P]) / (H[pos] * (p.dXbp));
-    double pp = 0, qq = 0;
-    if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = (FS[pos + 1] - FS[pos]);
-    if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = (FS[pos] - FS[pos - 1]);
-    pp = (1 / (H[pos] * p.dYbp)) * (g.Htdv[pos] * g.Ky[pos] * pp - g.Htdv[pos - 1] * g.Ky[pos - 1] * qq);
+    aa = -gamav * R(0.5) * (L(u, pos) + L(u, pos - P)) / R(p.dX2) -
+         L(g.Htdu, pos - P) * L(g.Kx, pos - P) / (Hp * (R(p.dXbp)));
+    cc = gamav * R(0.5) * (L(u, pos) + L(u, pos - P)) / R(p.dX2) - L(g.Htdu, pos) * L(g.Kx, pos) / (Hp * (R(p.dXbp)));
+    bb = R(p.HaiChiadT) + (L(g.Htdu, pos) * L(g.Kx, pos) + L(g.Htdu, pos - P) * L(g.Kx, pos - P)) / (Hp * (R(p.dXbp)));
+    R pp = 0, qq = 0;
+    if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = R(FS[pos + 1] - FS[pos]);
+    if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = R(FS[pos] - FS[pos - 1]);
+    pp = (1 / (Hp * R(p.dYbp))) * (L(g.Htdv, pos) * L(g.Ky, pos) * pp - L(g.Htdv, pos - 1) * L(g.Ky, pos - 1) * qq);
     if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
-        qq = (FS[pos + 1] - FS[pos - 1]) / p.dY2;
-        qq = (v[pos] + v[pos - 1]) * 0.5 * qq * gamav;
+        qq = R(FS[pos + 1] - FS[pos - 1]) / R(p.dY2);
+        qq = (L(v, pos) + L(v, pos - 1)) * R(0.5) * qq * gamav;
     } else
         qq = 0;
-    dd = FS[pos] / (p.dT * 0.5) - qq + pp + (S / H[pos]);
+    dd = FSp / (R(p.dT) * R(0.5)) - qq + pp + (S / Hp);
 }
 
 // Row of the FSi system for one interior wet cell before the segment-end terms
 // (_FSi_calculate__mactrix_coeff, Sediment_Transport.cu:62-165).  The terms that depend on
 // the cell alone (gamav and the gated source over the depth, rowC arrays 0 and 1) were
 // computed by the state update that precedes the sweep (fsi_cell_terms).
-__device__ __forceinline__ void fsi_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, double& aa,
-                                                double& bb, double& cc, double& dd) {
+template <class R>
+__device__ __forceinline__ void fsi_cell_coeffs(const DevGrid& g, const DevParams& p, int pos, R& aa, R& bb, R& cc,
+                                                R& dd) {
     const int P = g.P;
     const double* FS = g.FS;
     const double* H = g.H_moi;
-    const double gamav = rowC(g, 0)[pos];
-    aa = -gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos - 1] * g.Ky[pos - 1] / (H[pos] * p.dYbp);
-    cc = gamav * 0.5 * (g.t_v[pos - 1] + g.t_v[pos]) / p.dY2 - g.Htdv[pos] * g.Ky[pos] / (H[pos] * p.dYbp);
-    bb = p.HaiChiadT + (g.Htdv[pos] * g.Ky[pos] + g.Htdv[pos - 1] * g.Ky[pos - 1]) / (H[pos] * p.dYbp);
-    double pp = 0, qq = 0;
-    if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = (FS[pos + P] - FS[pos]);
-    if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = (FS[pos] - FS[pos - P]);
-    pp = (1 / (H[pos] * p.dXbp)) * (g.Htdu[pos] * g.Kx[pos] * pp - g.Htdu[pos - P] * g.Kx[pos - P] * qq);
+    auto L = [](const double* a, int q) { return R(a[q]); };
+    const R Hp = L(H, pos);
+    const R gamav = rowCr<R>(g, 0)[pos];
+    aa = -gamav * R(0.5) * (L(g.t_v, pos - 1) + L(g.t_v, pos)) / R(p.dY2) -
+         L(g.Htdv, pos - 1) * L(g.Ky, pos - 1) / (Hp * R(p.dYbp));
+    cc = gamav * R(0.5) * (L(g.t_v, pos - 1) + L(g.t_v, pos)) / R(p.dY2) - L(g.Htdv, pos) * L(g.Ky, pos) / (Hp * R(p.dYbp));
+    bb = R(p.HaiChiadT) + (L(g.Htdv, pos) * L(g.Ky, pos) + L(g.Htdv, pos - 1) * L(g.Ky, pos - 1)) / (Hp * R(p.dYbp));
+    R pp = 0, qq = 0;
+    if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = R(FS[pos + P] - FS[pos]);
+    if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = R(FS[pos] - FS[pos - P]);
+    pp = (1 / (Hp * R(p.dXbp))) * (L(g.Htdu, pos) * L(g.Kx, pos) * pp - L(g.Htdu, pos - P) * L(g.Kx, pos - P) * qq);
     if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
-        qq = (FS[pos + P] - FS[pos - P]) / p.dX2;
-        qq = (g.t_u[pos] + g.t_u[pos - P]) * 0.5 * qq * gamav;
+        qq = R(FS[pos + P] - FS[pos - P]) / R(p.dX2);
+        qq = (L(g.t_u, pos) + L(g.t_u, pos - P)) * R(0.5) * qq * gamav;
     } else
         qq = 0;
-    dd = FS[pos] / (p.dT * 0.5) - qq + pp + rowC(g, 1)[pos];
+    dd = L(FS, pos) / (R(p.dT) * R(0.5)) - qq + pp + rowCr<R>(g, 1)[pos];
 }
 
 // FSj rows of every interior wet cell (columns 3..M-1), one warp per row of the grid over
-// the row's span, written column-major (g.colT arrays 0..3: aa bb cc dd), with TILE
+// the row's span, written column-major (colT arrays 0..3 in R: aa bb cc dd), with TILE
 // through a tile.
-template <int TILE>
+template <int TILE, class R>
 __global__ void __launch_bounds__(256) k_coef_fsj(DevGrid g, DevParams p, int half) {
     const double t = g.clock[half];
     if constexpr (!TILE) {
@@ -740,22 +772,22 @@ __global__ void __launch_bounds__(256) k_coef_fsj(DevGrid g, DevParams p, int ha
         for (int j = lo + lane; j <= hi; j += 32) {
             const int pos = i * g.P + j;
             if (g.khouot[pos] != 0) continue;
-            double aa, bb, cc, dd;
-            fsj_cell_coeffs(g, p, t, pos, aa, bb, cc, dd);
+            R aa, bb, cc, dd;
+            fsj_cell_coeffs<R>(g, p, t, pos, aa, bb, cc, dd);
             const size_t q = (size_t)j * g.LT + i;
-            colT(g, 0)[q] = aa;
-            colT(g, 1)[q] = bb;
-            colT(g, 2)[q] = cc;
-            colT(g, 3)[q] = dd;
+            colTr<R>(g, 0)[q] = aa;
+            colTr<R>(g, 1)[q] = bb;
+            colTr<R>(g, 2)[q] = cc;
+            colTr<R>(g, 3)[q] = dd;
         }
     } else {
-        double* const dst[4] = {colT(g, 0), colT(g, 1), colT(g, 2), colT(g, 3)};
+        R* const dst[4] = {colTr<R>(g, 0), colTr<R>(g, 1), colTr<R>(g, 2), colTr<R>(g, 3)};
         colmajor_tile<4>(
             g, 2 + kTileRows * blockIdx.x, g.N, 3, g.M - 1,
-            [&](int i, int j, double* v) {
+            [&](int i, int j, R* v) {
                 const int pos = i * g.P + j;
                 if (g.khouot[pos] != 0) return false;
-                fsj_cell_coeffs(g, p, t, pos, v[0], v[1], v[2], v[3]);
+                fsj_cell_coeffs<R>(g, p, t, pos, v[0], v[1], v[2], v[3]);
                 return true;
             },
             dst);
@@ -798,66 +830,65 @@ __device__ __forceinline__ void fs_setup(const DevGrid& g, const DevParams& p, i
 // and _FSi/_FSj_extract_solution, Sediment_Transport.cu:62-340, driven by Scan_FSi/
 // Scan_FSj and FSi/FSj_extract_solution 570-618).  DIR 0: FSj (line = column j, cells
 // i), DIR 1: FSi (line = row i, cells j).
-template <int DIR, int SOLVER, class G>
+template <int DIR, int SOLVER, class G, class R>
 __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, int half, int line,
-                                        const LineShared& sg, double* A, double* B, double* Cc, double* D,
-                                        double* red, SolvePlan pl) {
+                                        const LineShared& sg, R* A, R* B, R* Cc, R* D, R* red, SolvePlan pl) {
     constexpr int T = G::size;
     const int tid = G::rank();
     const int P = g.P;
     const int along = DIR == 0 ? P : 1;
     const int base = DIR == 0 ? line : line * P;
     (void)half;  // both rows are precomputed (k_coef_fsj, the state update's FSi terms)
-    const int R = sg.R;
-    for (int r = R + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
-        A[r] = 0.0;
-        B[r] = 1.0;
-        Cc[r] = 0.0;
-        D[r] = 0.0;
+    const int Rn = sg.R;
+    for (int r = Rn + tid; r < pl.t1 * pl.m; r += T) {  // identity rows up to the solver's rows
+        A[r] = R(0);
+        B[r] = R(1);
+        Cc[r] = R(0);
+        D[r] = R(0);
     }
     const double* FS = g.FS;
-    for (int rr = tid; rr < R; rr += T) {
+    for (int rr = tid; rr < Rn; rr += T) {
         const int sI = seg_of_row(sg, rr);
         const int f = sg.first[sI], l = sg.last[sI];
         const int k = f + 1 + (rr - sg.ro[sI]);
         const int b1f = sg.br1[sI], b2f = sg.br2[sI];
         const int pos = base + k * along;
-        double aa, bb, cc, dd;
+        R aa, bb, cc, dd;
         if (DIR == 0) {  // precomputed by k_coef_fsj
             const size_t q = (size_t)line * g.LT + k;
-            aa = colT(g, 0)[q];
-            bb = colT(g, 1)[q];
-            cc = colT(g, 2)[q];
-            dd = colT(g, 3)[q];
+            aa = colTr<R>(g, 0)[q];
+            bb = colTr<R>(g, 1)[q];
+            cc = colTr<R>(g, 2)[q];
+            dd = colTr<R>(g, 3)[q];
             if (k == f + 1) {
                 if (b1f || g.u[base + f * along] == 0) bb += aa;
-                else dd -= aa * FS[base + f * along];
+                else dd -= aa * R(FS[base + f * along]);
             }
             if (k == l - 1) {
                 if (b2f && g.u[base + l * along] == 0) bb += cc;
-                else dd -= cc * FS[base + l * along];
+                else dd -= cc * R(FS[base + l * along]);
             }
         } else {
-            fsi_cell_coeffs(g, p, pos, aa, bb, cc, dd);
+            fsi_cell_coeffs<R>(g, p, pos, aa, bb, cc, dd);
             if (k == f + 1) {
                 if (b1f || g.t_v[base + f * along] == 0) bb = bb + aa;
-                else dd = dd - aa * FS[base + f * along];
+                else dd = dd - aa * R(FS[base + f * along]);
             }
             if (k == l - 1) {
                 if (b2f || g.t_v[base + l * along] == 0) bb = bb + cc;
-                else dd = dd - cc * FS[base + l * along];
+                else dd = dd - cc * R(FS[base + l * along]);
             }
         }
-        A[rr] = (k == f + 1) ? 0.0 : aa;
+        A[rr] = (k == f + 1) ? R(0) : aa;
         B[rr] = bb;
-        Cc[rr] = (k == l - 1) ? 0.0 : cc;
+        Cc[rr] = (k == l - 1) ? R(0) : cc;
         D[rr] = dd;
     }
     G::sync();
-    solve_line<G, SOLVER>(A, B, Cc, D, pl, R, red);
-    const double* x = B;
+    solve_line<G, SOLVER, R>(A, B, Cc, D, pl, Rn, red);
+    const R* x = B;
     const double* vel = DIR == 0 ? g.u : g.t_v;  // FSj: u = t_u here (see fsj_cell_coeffs)
-    for (int c = tid; c < R; c += T) {
+    for (int c = tid; c < Rn; c += T) {
         const int sI = seg_of_row(sg, c);
         const int f = sg.first[sI], l = sg.last[sI];
         const int k = f + 1 + (c - sg.ro[sI]);
@@ -879,14 +910,16 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
 }
 
 // Fused sediment sweep of one direction: as k_hydro_sweep.
-template <int DIR, int SOLVER>
+template <int DIR, int SOLVER, class R>
 __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int half, int startidx, int endidx, int RB,
-                                                  double* gscr, int RG, int roww) {
-    extern __shared__ double dyn_smem[];
+                                                  double* gscr_d, int RG, int roww) {
+    extern __shared__ double dyn_smem_d[];
+    R* dyn_smem = reinterpret_cast<R*>(dyn_smem_d);
+    R* gscr = reinterpret_cast<R*>(gscr_d);
     __shared__ LineShared sgw[kWL];
     __shared__ int s_long[kWL];
     __shared__ int s_nlong;
-    __shared__ double s_red[4 * kRedRows];  // reduced rows of the two-level solve
+    __shared__ R s_red[4 * kRedRows];  // reduced rows of the two-level solve
     const int w = threadIdx.x >> 5;
     const int nlines = endidx - startidx + 1;
     const int G = gridDim.x;
@@ -901,9 +934,9 @@ __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int
                 if ((threadIdx.x & 31) == 0) s_long[atomicAdd(&s_nlong, 1)] = w;
             } else {
                 const int wr = slice_rows(roww);
-                double* A = dyn_smem + w * 4 * wr;
-                fs_body<DIR, SOLVER, WarpG>(g, p, half, startidx + li, sg, A, A + wr, A + 2 * wr, A + 3 * wr,
-                                            nullptr, SolvePlan{32, chunk_len(sg.R, 32)});
+                R* A = dyn_smem + w * 4 * wr;
+                fs_body<DIR, SOLVER, WarpG, R>(g, p, half, startidx + li, sg, A, A + wr, A + 2 * wr, A + 3 * wr,
+                                               nullptr, SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
         __syncthreads();
@@ -915,8 +948,8 @@ __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int
             const SolvePlan pl = solve_plan(sl.R, SOLVER == 0 ? 256 : 32);
             const bool fits = pl.t1 * pl.m <= RB;
             const int rs = fits ? RB : RG;
-            double* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * 4 * (size_t)RG;
-            fs_body<DIR, SOLVER, BlockG>(g, p, half, line, sl, A, A + rs, A + 2 * rs, A + 3 * rs, s_red, pl);
+            R* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * 4 * (size_t)RG;
+            fs_body<DIR, SOLVER, BlockG, R>(g, p, half, line, sl, A, A + rs, A + 2 * rs, A + 3 * rs, s_red, pl);
             __syncthreads();
         }
     }
@@ -948,9 +981,15 @@ cudaError_t allow_all(F* const* fs, int n, int* limit) {
 using HydroSweepFn = void(DevGrid, DevParams, int, int, int, double*, int, int);
 using FsSweepFn = void(DevGrid, DevParams, int, int, int, int, double*, int, int);
 
-HydroSweepFn* const kHydroSweep[2][2] = {{k_hydro_sweep<0, 0>, k_hydro_sweep<0, 1>},
-                                         {k_hydro_sweep<1, 0>, k_hydro_sweep<1, 1>}};
-FsSweepFn* const kFsSweep[2][2] = {{k_fs_sweep<0, 0>, k_fs_sweep<0, 1>}, {k_fs_sweep<1, 0>, k_fs_sweep<1, 1>}};
+// [precision: 0 FP64, 1 mixed][direction][solver]
+HydroSweepFn* const kHydroSweep[2][2][2] = {
+    {{k_hydro_sweep<0, 0, double>, k_hydro_sweep<0, 1, double>},
+     {k_hydro_sweep<1, 0, double>, k_hydro_sweep<1, 1, double>}},
+    {{k_hydro_sweep<0, 0, float>, k_hydro_sweep<0, 1, float>},
+     {k_hydro_sweep<1, 0, float>, k_hydro_sweep<1, 1, float>}}};
+FsSweepFn* const kFsSweep[2][2][2] = {
+    {{k_fs_sweep<0, 0, double>, k_fs_sweep<0, 1, double>}, {k_fs_sweep<1, 0, double>, k_fs_sweep<1, 1, double>}},
+    {{k_fs_sweep<0, 0, float>, k_fs_sweep<0, 1, float>}, {k_fs_sweep<1, 0, float>, k_fs_sweep<1, 1, float>}}};
 
 }  // namespace
 
@@ -960,8 +999,10 @@ FsSweepFn* const kFsSweep[2][2] = {{k_fs_sweep<0, 0>, k_fs_sweep<0, 1>}, {k_fs_s
 cudaError_t sweep_plan(int N, int M, SweepPlan* sp, int max_rows) {
     cudaError_t e;
     int lim_h, lim_f;
-    if ((e = allow_all(&kHydroSweep[0][0], 4, &lim_h)) != cudaSuccess) return e;
-    if ((e = allow_all(&kFsSweep[0][0], 4, &lim_f)) != cudaSuccess) return e;
+    // the row counts below are planned for FP64 rows; the mixed form's FP32 rows take half
+    // the bytes of the same plan
+    if ((e = allow_all(&kHydroSweep[0][0][0], 8, &lim_h)) != cudaSuccess) return e;
+    if ((e = allow_all(&kFsSweep[0][0][0], 8, &lim_f)) != cudaSuccess) return e;
     const int L = N > M ? N : M;
     const size_t warp_h = (size_t)kWL * kWarpHydro, warp_f = (size_t)kWL * kWarpFs;  // short-line slices
     if ((long long)(sizeof(double) * warp_h) > lim_h || (long long)(sizeof(double) * warp_f) > lim_f)
@@ -1009,10 +1050,10 @@ cudaError_t sweep_plan(int N, int M, SweepPlan* sp, int max_rows) {
     int dev = 0, nsm = 0, occ = 0, occf = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kHydroSweep[0][0], kTL, sp->smem_lines)) !=
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kHydroSweep[0][0][0], kTL, sp->smem_lines)) !=
         cudaSuccess)
         return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, kFsSweep[0][0], kTL, sp->smem_fs_lines)) !=
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occf, kFsSweep[0][0][0], kTL, sp->smem_fs_lines)) !=
         cudaSuccess)
         return e;
     if (occ < 1) occ = 1;
@@ -1041,8 +1082,10 @@ void hydro_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan&
     // the long-line rows or the warps' slices, whichever is larger (a smaller request
     // leaves more of the SM's on-chip memory to L1)
     const size_t big = 4 * (size_t)sp.RB + kEnds, slices = (size_t)kWL * (4 * slice_rows(roww) + kEnds);
-    const size_t smem = sizeof(double) * (big > slices ? big : slices);
-    kHydroSweep[dir][sv]<<<sp.long_grid, kTL, smem, s>>>(g, p, startidx, endidx, sp.RB, scratch, sp.RG, roww);
+    const size_t esz = p.mixed ? sizeof(float) : sizeof(double);
+    const size_t smem = esz * (big > slices ? big : slices);
+    kHydroSweep[p.mixed ? 1 : 0][dir][sv]<<<sp.long_grid, kTL, smem, s>>>(g, p, startidx, endidx, sp.RB, scratch,
+                                                                         sp.RG, roww);
     hyd_kernel_launches_add(1);
 }
 
@@ -1053,16 +1096,23 @@ void fs_sweep(int dir, const DevGrid& g, const DevParams& p, const SweepPlan& sp
     const int sv = solver ? 1 : 0;
     const int roww = (sp.wide || nlines > kWL * sp.long_grid) ? kRowW : kRowShortF;
     const size_t big = 4 * (size_t)sp.RBf, slices = (size_t)kWL * 4 * slice_rows(roww);
-    const size_t smem = sizeof(double) * (big > slices ? big : slices);
-    kFsSweep[dir][sv]<<<sp.long_grid, kTL, smem, s>>>(g, p, half, startidx, endidx, sp.RBf, scratch,
-                                                                   sp.RGf, roww);
+    const size_t esz = p.mixed ? sizeof(float) : sizeof(double);
+    const size_t smem = esz * (big > slices ? big : slices);
+    kFsSweep[p.mixed ? 1 : 0][dir][sv]<<<sp.long_grid, kTL, smem, s>>>(g, p, half, startidx, endidx, sp.RBf, scratch,
+                                                                      sp.RGf, roww);
     hyd_kernel_launches_add(1);
 }
 }  // namespace
 
 void launch_coef_fsj(const DevGrid& g, const DevParams& p, int half, cudaStream_t s) {
-    if (g.tile_cols) k_coef_fsj<1><<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p, half);
-    else k_coef_fsj<0><<<((g.N - 1) * 32 + 255) / 256, 256, 0, s>>>(g, p, half);
+    const int nb = ((g.N - 1) * 32 + 255) / 256;
+    if (p.mixed) {
+        if (g.tile_cols) k_coef_fsj<1, float><<<nb, 256, 0, s>>>(g, p, half);
+        else k_coef_fsj<0, float><<<nb, 256, 0, s>>>(g, p, half);
+    } else {
+        if (g.tile_cols) k_coef_fsj<1, double><<<nb, 256, 0, s>>>(g, p, half);
+        else k_coef_fsj<0, double><<<nb, 256, 0, s>>>(g, p, half);
+    }
     hyd_kernel_launches_add(1);
 }
 
