@@ -93,7 +93,12 @@ NCU_TRAFFIC = {
 # over the step's launches, the L2-flush kernels left out) from an ncu launch list of the
 # timed steps; the summary, with its command, is the file named in "source".  Filled from
 # captures of the current kernels; absent workloads print no step_dram.
-STEP_DRAM = {}
+STEP_DRAM = {
+    "config2": {"bytes_per_step": 44.53e6, "source": "profiles/step_dram_config2_config4.md (ncu, every launch of "
+                "a timed step run cold: an upper bound)"},
+    "config4": {"bytes_per_step": 501.47e6, "source": "profiles/step_dram_config2_config4.md (ncu, every launch "
+                "of a timed step run cold: an upper bound)"},
+}
 
 
 def load_peaks():
@@ -248,17 +253,37 @@ def run_ours(args, rank, world, local_rank, workload, secondary=False):
     # a buffer twice the L2, written (on the library's stream) before every timed step
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    def flushed_steps(n):
-        """Run n steps, each after an L2 flush; the summed device time of the steps (ms)."""
+    def flushed_steps(n, s=None, st=None):
+        """Run n steps of simulation s (default: the measured one) on its stream st, each
+        after an L2 flush; the summed device time of the steps (ms)."""
+        s = sim if s is None else s
+        st = ext if st is None else st
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
-        with torch.cuda.stream(ext):
+        with torch.cuda.stream(st):
             for a, b in ev:
                 flush.zero_()
-                a.record(ext)
-                sim.step(1, sync=False)
-                b.record(ext)
+                a.record(st)
+                s.step(1, sync=False)
+                b.record(st)
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in ev)
+
+    def back_to_back(n, s, st):
+        """n steps of s queued back to back on its stream st; device ms."""
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        s.step(n, sync=False)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def max_ranks(v):
+        t = torch.tensor([v], device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
 
     # warm-up
     sim.step(args.warmup, sync=True)
@@ -293,6 +318,54 @@ def run_ours(args, rank, world, local_rank, workload, secondary=False):
     if world > 1:
         torch.distributed.all_reduce(t_warm, op=torch.distributed.ReduceOp.MAX)
     warm_ms = float(t_warm.item())
+
+    # the FP32-bulk mixed form of the same workload (precision_mode MIXED: coefficient
+    # assembly, line sweeps, explicit momentum and sediment in FP32; the level's continuity
+    # update, mass sums and Exner sums in FP64), spun up to the same time and timed the
+    # same way
+    from hydist.params import PRECISION_MIXED
+    pm = case.params.copy()
+    pm.precision_mode = PRECISION_MIXED
+    simm = Simulation(pm, N, M, device=local_rank)
+    simm.load_case(case)
+    simm.step(args.spinup)
+    extm = torch.cuda.ExternalStream(simm.stream_ptr(), device=local_rank)
+    simm.step(args.warmup, sync=True)
+    flushed_steps(args.warmup, simm, extm)
+    mixed_ms = max_ranks(flushed_steps(args.steps, simm, extm))
+    mixed_b2b = max_ranks(back_to_back(args.steps, simm, extm))
+    simm.close()
+    mixed = {"value": world * cells * args.steps / (mixed_ms / 1e3), "ms_per_step": mixed_ms / args.steps,
+             "back_to_back": {"value": world * cells * args.steps / (mixed_b2b / 1e3),
+                              "ms_per_step": mixed_b2b / args.steps},
+             "speedup_vs_fp64": ms / mixed_ms, "dtype": "f32 bulk, f64 z update / mass sums / Exner",
+             "model_bytes_per_cell_update": 116,
+             "l2": "flushed before every timed step, as value"}
+
+    # simulated hours per wall second of a morphodynamic run on this reach: hydraulics,
+    # sediment and the bed change fed back every 10 min (bed_feedback, morfac 1,
+    # bed_period 600 s), 2 simulated hours back to back from the spun-up state, FP64 and
+    # mixed (the 30-day config-5 shape on the config-2 geometry)
+    morpho = None
+    if not secondary:
+        morpho = {"sim_hours": 2.0, "bed_period_s": 600.0, "morfac": 1.0}
+        for label, prec in (("fp64", 0), ("mixed", PRECISION_MIXED)):
+            pq = case.params.copy()
+            pq.precision_mode = prec
+            pq.bed_feedback = 1
+            pq.morfac = 1.0
+            pq.bed_period = 600.0
+            sq = Simulation(pq, N, M, device=local_rank)
+            sq.load_case(case)
+            sq.step(args.spinup)
+            stq = torch.cuda.ExternalStream(sq.stream_ptr(), device=local_rank)
+            nq = int(round(2 * 3600 / case.params.dT))
+            sq.step(10, sync=True)
+            mq = max_ranks(back_to_back(nq, sq, stq))
+            assert sq.mass_balance()["nonfinite"] == 0
+            morpho[label] = {"sim_h_per_wall_s": 2.0 / (mq / 1e3), "ms_per_step": mq / nq}
+            sq.close()
+        morpho["mixed_over_fp64"] = morpho["mixed"]["sim_h_per_wall_s"] / morpho["fp64"]["sim_h_per_wall_s"]
 
     # per-phase device timing: events around every phase (the shares), then around the
     # dominant phase alone (its launch time, disturbed least by the events)
@@ -459,6 +532,8 @@ def run_ours(args, rank, world, local_rank, workload, secondary=False):
                          "ms_per_launch": avg_ms, "timed": "events around this phase alone, L2 flushed per step"},
             "step_roofline": {"bytes_per_cell_update": 208, "achieved": value * 208 / 1e9 / world, "peak": peak,
                               "frac": value * 208 / 1e9 / world / peak},
+            "mixed": mixed,
+            "morpho": morpho,
             "phases": phases,
             "cpu_baseline": cpu,
             "reference_kernels_gpu": ref_gpu,

@@ -368,6 +368,47 @@ int hyd_batch_destroy(hyd_batch b);
 int hyd_set_sweep_shape(hyd_handle h, int ctas, int wide);
 int hyd_get_sweep_shape(hyd_handle h, int* ctas, int* wide);
 
+/*
+ * Convolution kernels of the learned surrogate (BF16 operands on the tensor cores, FP32
+ * accumulation in tensor memory).  No reference counterpart: the reference has no learned
+ * part.  A layer is a 3x3 convolution over NHWC BF16 activations, output pixel p and tap
+ * t = 3 (dy + 1) + (dx + 1) reading input pixel:
+ *   HYD_CONV_SAME      (y + dy, x + dx)             same size
+ *   HYD_CONV_SAME_ADJ  (y - dy, x - dx)             the adjoint of SAME
+ *   HYD_CONV_DOWN      (2y + dy, 2x + dx)           stride 2 down
+ *   HYD_CONV_UP        ((y - dy)/2, (x - dx)/2)     stride 2 up (where both are even),
+ *                                                   the adjoint of DOWN
+ * and zero outside the input.  The data gradient of a layer is hyd_conv_forward with the
+ * adjoint mapping, the channel-transposed weights and the output gradient as input.
+ *
+ * hyd_conv_forward: y[p][n] = act(sum_{t,c} x[map(p,t)][c] w[n][t][c] + bias[n]), n < nout,
+ *   times (mask[p][n] > 0) when mask is not null (the ReLU derivative of a data gradient).
+ *   cin (16 or 48) channels per input pixel; ncol (16 or 48) the padded output channels the
+ *   packed weights hold: w_packed is the tensor cores' shared-memory image, for K step
+ *   s = (t cin + c) / 16 a block of ncol x 16 BF16 in which element (n, k) lies at byte
+ *   (n / 8) 256 + (k / 8) 128 + (n % 8) 16 + (k % 8) 2.  relu: max(0, .); out_f32: FP32
+ *   output instead of BF16.  *err is set to 1 if a wait on the tensor cores timed out.
+ * hyd_conv_wgrad: dw[n][t][c] += sum_p dy[p][n] x[map(p,t)][c] (FP32, n < nout), dy with
+ *   ncol channels per pixel; map is the layer's forward mapping.
+ * hyd_bias_grad: db[n] += sum_p dy[p][n].
+ * hyd_mse_grad: loss += scale sum_p w[p] |pred[p] - target[p]|^2 over nc channels (FP32),
+ *   dy[p][c] = 2 scale w[p] (pred - target) as BF16 with ncol channels (zero beyond nc).
+ * All run on `stream` (a cudaStream_t) and return after queuing; pointers are device
+ * memory, 16-byte aligned.
+ */
+#define HYD_CONV_SAME 0
+#define HYD_CONV_SAME_ADJ 1
+#define HYD_CONV_DOWN 2
+#define HYD_CONV_UP 3
+int hyd_conv_forward(const void* x, int B, int Hin, int Win, int cin, const void* w_packed, const float* bias,
+                     int ncol, int nout, int mode, int relu, const void* mask, void* y, int Hout, int Wout,
+                     int out_f32, int* err, void* stream);
+int hyd_conv_wgrad(const void* x, int B, int Hin, int Win, int cin, int mode, const void* dy, int Hout, int Wout,
+                   int ncol, int nout, float* dw, int* err, void* stream);
+int hyd_bias_grad(const void* dy, long long npix, int ncol, int nout, float* db, void* stream);
+int hyd_mse_grad(const float* pred, const float* target, const float* weight, long long npix, int nc, int ncol,
+                 float scale, void* dy, float* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
