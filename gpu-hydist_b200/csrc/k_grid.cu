@@ -18,6 +18,8 @@ namespace {
 constexpr double kPiRef = 3.14159265359;  // constant.cuh:3
 constexpr double kEpsRef = 1e-16;         // UVZSolver_multithread.cu:12
 constexpr int kSpanHalo = 4;              // extended-span margin, cells
+constexpr double kBedLimit = 0.1;         // fed-back bed change per update: at most this fraction of the depth
+constexpr double kBedCap = 0.05;          // and at most this many metres
 
 inline dim3 grid2d(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y); }
 
@@ -960,6 +962,15 @@ struct WetGlobal {  // mask in HBM: cell k at kh[base + k * along]
     __device__ bool operator()(int k) const { return kh[base + k * along] == 0; }
 };
 
+// A column's mask from its column-major reset bytes (g.colB, low two bits): one coalesced
+// byte per cell instead of one 32-byte sector per 4-byte mask value of the pitched grid.
+// The resets keep those bits equal to the mask (they write the byte of every cell they
+// open or close; the smoothing pass before the column resets rewrites every byte).
+struct WetBytes {
+    const unsigned char* col;
+    __device__ bool operator()(int k) const { return (col[k] & 3u) == 0; }
+};
+
 // Words of each k_reset bitset: one bit per cell of a line.
 __host__ __device__ __forceinline__ int reset_words(int L) { return (L + 3) / 32 + 2; }
 
@@ -1075,6 +1086,7 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
             t_z[gq] = tzv;
             H[gq] = hv;
             kh[gq] = 0;
+            g.colB[ROWS ? (size_t)kk * g.LT + line : (size_t)line * g.LT + kk] = 0;  // mask bits of the byte
             khs[kk - k0] = 0;
             FS[gq] = fsv;
             if (kk >= 2 && kk <= L && hv <= p.H_TINH) clw[(kk - k0) >> 5] |= 1u << ((kk - k0) & 31);
@@ -1129,6 +1141,7 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
         g.t_v[gp - 1] = 0;
         g.t_v[gp] = 0;
         kh[gp] = 1;
+        g.colB[ROWS ? (size_t)k * g.LT + line : (size_t)line * g.LT + k] = 1;
         khs[k - k0] = 1;
         FS[gp] = 0;
         s_changed = 1;
@@ -1496,9 +1509,13 @@ __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
             if (line < 2 || line > Lines) continue;
             const int lo = ROWS ? g.rlo[line] : g.clo[line];
             const int hi = ROWS ? g.rhi[line] : g.chi[line];
-            const WetGlobal wet{g.khouot, ROWS ? line * g.P : line, ROWS ? 1 : g.P};
-            if (ROWS) warp_scan_line(g, wet, lo, hi, L, words, g.daui + line * HYD_SEGL, g.cuoii + line * HYD_SEGL, g.moci + line);
-            else warp_scan_line(g, wet, lo, hi, L, words, g.dauj + line * HYD_SEGL, g.cuoij + line * HYD_SEGL, g.mocj + line);
+            if (ROWS) {
+                const WetGlobal wet{g.khouot, line * g.P, 1};
+                warp_scan_line(g, wet, lo, hi, L, words, g.daui + line * HYD_SEGL, g.cuoii + line * HYD_SEGL, g.moci + line);
+            } else {
+                const WetBytes wet{g.colB + (size_t)line * g.LT};
+                warp_scan_line(g, wet, lo, hi, L, words, g.dauj + line * HYD_SEGL, g.cuoij + line * HYD_SEGL, g.mocj + line);
+            }
         }
     }
     __syncthreads();
@@ -1657,7 +1674,14 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
         g.dH[pos] += p.dT / (1 - p.Dorong) * (S + tH);
         return;
     }
-    const double x = p.morfac * p.bed_period / (1 - p.Dorong) * (S + tH);
+    // the period's change, limited to kBedLimit of the water depth and to kBedCap metres
+    // (the explicit Exner step with central and one-sided bed-load differences is unstable
+    // for large morphological steps; the limit keeps each update's bed change small
+    // against the depth it acts on)
+    double x = p.morfac * p.bed_period / (1 - p.Dorong) * (S + tH);
+    if (!isfinite(x)) x = 0.0;
+    const double lim = fmin(kBedLimit * g.H_moi[pos], kBedCap);
+    x = fmin(fmax(x, -lim), lim);
     const double y = x - g.dHc[pos];
     const double sum = g.dH[pos] + y;
     g.dHc[pos] = (sum - g.dH[pos]) - y;
@@ -1682,11 +1706,13 @@ __global__ void k_bed_derive(DevGrid g, DevParams p) {
         const double old = g.htaiz[pos];
         g.htaiz[pos] = ht;
         g.htaiz_bd[pos] = ht;
+        // the face depths below datum taken no smaller than H_TINH: a raised bed must not
+        // give the friction factor a negative base (the set-up's formula is otherwise kept)
         if (h[pos - 1] + h[pos] != 0)
-            g.Kx1[pos] = p.g * pow((h[pos - 1] + h[pos]) * 0.5, -2 * p.mu_mn) *
+            g.Kx1[pos] = p.g * pow(fmax((h[pos - 1] + h[pos]) * 0.5, p.H_TINH), -2 * p.mu_mn) *
                          pow((g.hsnham[pos - 1] + g.hsnham[pos]) * 0.5, 2);
         if (h[pos - P] + h[pos] != 0)
-            g.Ky1[pos] = p.g * pow((h[pos - P] + h[pos]) * 0.5, -2 * p.mu_mn) *
+            g.Ky1[pos] = p.g * pow(fmax((h[pos - P] + h[pos]) * 0.5, p.H_TINH), -2 * p.mu_mn) *
                          pow((g.hsnham[pos - P] + g.hsnham[pos]) * 0.5, 2);
         if (g.khouot[pos] == 0) {
             g.H_moi[pos] = ht + g.z[pos];

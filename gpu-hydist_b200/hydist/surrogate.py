@@ -5,7 +5,8 @@ runs Adam and drives the loop; it computes none of the convolutions.  No referen
 counterpart (the reference has no learned part).
 
 Network (width 48, 3 x 3 kernels, NHWC BF16 activations, FP32 accumulation):
-    L1  same size   4 -> 48  ReLU        input: bed, roughness, upstream Q, downstream stage
+    L1  same size   6 -> 48  ReLU        input: bed, roughness, upstream Q, downstream stage,
+                                          and the cell's along-flow and cross coordinates
     L2  stride-2 down  48 -> 48  ReLU
     L3  same size  48 -> 48  ReLU       (half resolution)
     L4  stride-2 up    48 -> 48  ReLU
@@ -24,7 +25,9 @@ from . import lib as hlib
 
 CONV_SAME, CONV_SAME_ADJ, CONV_DOWN, CONV_UP = 0, 1, 2, 3
 ADJOINT = {CONV_SAME: CONV_SAME_ADJ, CONV_DOWN: CONV_UP, CONV_UP: CONV_DOWN}
-IN_CH, OUT_CH, WIDTH = 4, 3, 48
+# inputs: bed, roughness, upstream Q, downstream stage, and the along-flow and cross
+# coordinates (the levels depend on the distance to the stage edge); outputs u, v, z
+IN_CH, OUT_CH, WIDTH = 6, 3, 48
 CIN_PAD = 16  # input channels padded to the kernels' 16-channel K step
 
 # (mode, cin, cout, relu): the six layers
@@ -135,7 +138,7 @@ class Surrogate:
         return y
 
     def forward(self, x):
-        """x: BF16 [B][H][W][16] (4 input channels, zero padded).  Returns the FP32 output
+        """x: BF16 [B][H][W][16] (IN_CH input channels, zero padded).  Returns the FP32 output
         [B][H][W][3] and the activations the backward pass needs."""
         B, H, W, _ = x.shape
         acts, dims = [x], [(H, W)]

@@ -37,6 +37,8 @@
 #define SEGL HYD_SEGMENT_LIMIT
 #define PI_REF 3.14159265359 /* constant.cuh:3 */
 #define EPS_REF 1e-16        /* UVZSolver_multithread.cu:12 */
+#define BED_LIMIT 0.1        /* the library's fed-back bed change limit, a fraction of the depth */
+#define BED_CAP 0.05         /* and in metres */
 
 struct OraSim {
     HydCaseParams P;
@@ -1600,8 +1602,9 @@ static void k_calculate_qb(OraSim* s) {
 
 /* BedLoad + _bed_load (Sediment_Transport.cu:630-639, 416-506): rows startidx..endidx-1.
  * With the library's bed_feedback option (no reference counterpart): the upwind test reads
- * t_u[pos] > 0 (quirk Q4), the increment is morfac * bed_period / (1 - Dorong) * rate,
- * added to dH as a Kahan sum and applied to the bed, h = h0 + dH. */
+ * t_u[pos] > 0 (quirk Q4), the increment is morfac * bed_period / (1 - Dorong) * rate
+ * (0 if not finite) limited to BED_LIMIT of the depth and BED_CAP metres, added to dH as a Kahan sum and
+ * applied to the bed, h = h0 + dH. */
 static void k_bedload(OraSim* s, int startidx, int endidx) {
     const int N = s->N, M = s->M, width = s->W;
     const HydCaseParams* P = &s->P;
@@ -1665,7 +1668,12 @@ static void k_bedload(OraSim* s, int startidx, int endidx) {
             }
             {
                 const double period = P->bed_period > 0 ? P->bed_period : P->bed_change_start;
-                const double x = P->morfac * period / (1 - P->Dorong) * (S + tH);
+                double x = P->morfac * period / (1 - P->Dorong) * (S + tH);
+                if (!isfinite(x)) x = 0.0;
+                {
+                    const double lim = fmin(BED_LIMIT * H_moi[pos], BED_CAP);
+                    x = fmin(fmax(x, -lim), lim);
+                }
                 const double y = x - s->dHc[pos];
                 const double sum = s->dH[pos] + y;
                 s->dHc[pos] = (sum - s->dH[pos]) - y;
@@ -1676,7 +1684,8 @@ static void k_bedload(OraSim* s, int startidx, int endidx) {
 }
 
 /* After a fed-back bed change (no reference counterpart): what the set-up derived from h
- * re-derived for the new bed: htaiz, htaiz_bd, Kx1, Ky1 (Onetime_init,
+ * re-derived for the new bed: htaiz, htaiz_bd, Kx1, Ky1 (face depths no smaller than H_TINH)
+ * (Onetime_init,
  * support_funcs.cu:20-58), H_moi of the wet cells (update_h_moi, 60-73), Htuongdoi and
  * preprocess_data. */
 static void bed_feedback_derive(OraSim* s) {
@@ -1689,10 +1698,10 @@ static void bed_feedback_derive(OraSim* s) {
             s->htaiz[ij] = (h[(i - 1) * W + j - 1] + h[(i - 1) * W + j] + h[i * W + j - 1] + h[i * W + j]) * 0.25;
             s->htaiz_bd[ij] = s->htaiz[ij];
             if (h[i * W + j - 1] + h[i * W + j] != 0)
-                s->Kx1[ij] = P->g * pow((h[i * W + j - 1] + h[i * W + j]) * 0.5, -2 * P->mu_mn) *
+                s->Kx1[ij] = P->g * pow(fmax((h[i * W + j - 1] + h[i * W + j]) * 0.5, P->H_TINH), -2 * P->mu_mn) *
                              pow((s->hsnham[i * W + j - 1] + s->hsnham[i * W + j]) * 0.5, 2);
             if (h[(i - 1) * W + j] + h[i * W + j] != 0)
-                s->Ky1[ij] = P->g * pow((h[(i - 1) * W + j] + h[i * W + j]) * 0.5, -2 * P->mu_mn) *
+                s->Ky1[ij] = P->g * pow(fmax((h[(i - 1) * W + j] + h[i * W + j]) * 0.5, P->H_TINH), -2 * P->mu_mn) *
                              pow((s->hsnham[(i - 1) * W + j] + s->hsnham[i * W + j]) * 0.5, 2);
             if (s->khouot[ij] == 0) s->H_moi[ij] = s->htaiz[ij] + s->z[ij];
         }
