@@ -568,6 +568,53 @@ def run_ours(args, rank, world, local_rank, workload, secondary=False):
     return result
 
 
+def run_ensemble(args, local_rank):
+    """Config 3: the 96-reach ensemble on one GPU as one batch, stepped with batched
+    launches (every phase one launch for all reaches, the batch step one CUDA graph) and,
+    for comparison, member by member (one graph and stream per reach).  Spun up past the
+    discharge ramp and the sediment start, then timed by CUDA events back to back."""
+    import torch
+    from hydist import cases
+    from hydist.lib import Batch
+    cs = cases.config3_cases()
+    cells = sum(c.N * c.M for c in cs)
+    b = Batch(cs, device=local_rank)
+    b.set_fused(True)
+    b.step(1805, sync=True)  # past the 0.5 h ramp; sediment active from 1800 s
+    streams = [torch.cuda.ExternalStream(m.stream_ptr(), device=local_rank) for m in b.members]
+
+    def timed(n):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(streams[0])
+        for st in streams[1:]:
+            st.wait_event(e0)
+        b.step(n, sync=False)
+        for st in streams[1:]:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            streams[0].wait_event(ev)
+        e1.record(streams[0])
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    out = {"workload": "config3 ensemble: 96 reaches (nx 128-1024, ny 64-512, dx=5m), dt=1s, FP64 "
+                       "hydraulics+sediment, t=1810.. s", "reaches": len(cs), "cells": cells,
+           "l2": "no flush (the reaches' fields, %d cells, exceed L2)" % cells}
+    for label, fused in (("batched", True), ("per_member", False)):
+        b.set_fused(fused)
+        b.step(max(args.warmup, 3), sync=True)
+        f0 = b.fused_steps()
+        ms = timed(args.steps)
+        out[label] = {"value": cells * args.steps / (ms / 1e3), "unit": "cell-updates/s",
+                      "ms_per_step": ms / args.steps, "batched_steps": b.fused_steps() - f0}
+    out["value"] = out["batched"]["value"]
+    out["speedup_vs_per_member"] = out["per_member"]["ms_per_step"] / out["batched"]["ms_per_step"]
+    b.close()
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return None
@@ -635,6 +682,7 @@ def main():
                     help="skip timing the reference's own kernels on the GPU (oracle/_ref/libhydref_gpu.so)")
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS),
                     help="config2 (the default: the 1048x980 reach) or config4 (the 4096x2048 reach)")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the config-3 ensemble line")
     ap.add_argument("--secondary", default="config4", choices=sorted(WORKLOADS) + ["none"],
                     help="a second workload measured in the same run and printed under 'workloads' "
                          "(default config4; 'none' skips it)")
@@ -663,7 +711,11 @@ def main():
         if args.secondary not in ("none", args.workload):
             res2 = run_ours(args, rank, world, local_rank, args.secondary, secondary=True)
             if res is not None:
-                res["workloads"] = {args.secondary: res2}
+                res.setdefault("workloads", {})[args.secondary] = res2
+        if not args.no_ensemble and args.secondary != "none":
+            ens = run_ensemble(args, local_rank)
+            if res is not None:
+                res.setdefault("workloads", {})["config3"] = ens
     finally:
         if world > 1:
             import torch

@@ -967,6 +967,7 @@ int hyd_set_boundary(hyd_handle h, const int* boundary_type, const double* const
     h->g.total_time = total_time;
     for (int e = 0; e < 4; e++) h->bnd_nseg[e] = nseg[e];
     h->have_boundary = 1;
+    h->epoch++;  // the tables moved
     drop_graphs(h);
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return HYD_OK;
@@ -1525,8 +1526,45 @@ int hyd_launch_count(hyd_handle h, long long* count) {
 
 // ---- batches of independent reaches (one persistent handle per member)
 
+// Phases of a batched step with their own per-member CTA counts.
+enum BatchPhase { BP_CB, BP_SM_BUD, BP_SM, BP_SM_FSB, BP_EV, BP_CEU, BP_EU, BP_RR, BP_RC, BP_PF, BP_FSJC, BP_UFS,
+                  BP_COUNT };
+// Line lists of the batched sweeps.
+enum BatchLineSet { BL_UZ, BL_VZ, BL_FSJ, BL_FSI, BL_COUNT };
+
+// The batched form of a batch step: every phase of the step one launch for all members
+// (each CTA working for one member), the whole step one CUDA graph per step variant.
+struct BatchFused {
+    int nm = 0, mixed = 0, solver = 0;
+    void* dev = nullptr;    // the device tables below, one allocation
+    DevGrid* gS[3] = {};    // the members' grids as the step sees them: t_u / t_v as at the
+                            // step start (S0), after the first smoothing of u (S1), and of v (S2)
+    DevParams* p = nullptr;
+    double** outs[4] = {};  // smoothing outputs: half-step 1 u, v; half-step 2 v, u
+    int* bst[BP_COUNT] = {};
+    int ctas[BP_COUNT] = {};
+    int* lst[BL_COUNT] = {};
+    int* lfirst[BL_COUNT] = {};
+    SweepPlan plan{};
+    int grid = 0;
+    double* gscr = nullptr;     // sweep rows of lines too long for shared memory (if any)
+    double* gscr_fs = nullptr;  // the same for the sediment sweep beside the main chain
+    int thr_r = 64, thr_c = 64;
+    size_t sm_ev = 0, sm_eu = 0, sm_rr = 0, sm_rc = 0, sm_pf = 0;
+    cudaStream_t st = nullptr, side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, done = nullptr;
+    std::vector<cudaEvent_t> mev;  // per member: its stream's work before a batched run
+    std::vector<unsigned long long> epochs;  // the members' whole-grid event counts the tables were built at
+    cudaGraphExec_t graph[8] = {};
+    long long graph_kernels[8] = {};
+    long long steps = 0;
+    int built = 0;
+};
+
 struct HydBatch {
     std::vector<hyd_handle> members;
+    int fused = 0;
+    BatchFused bf;
 };
 
 int hyd_set_sweep_shape(hyd_handle h, int ctas, int wide) {
@@ -1581,9 +1619,361 @@ int hyd_batch_member(hyd_batch b, int k, hyd_handle* h) {
     return HYD_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+void fused_release(BatchFused& f) {
+    for (int k = 0; k < 8; k++) {
+        if (f.graph[k]) cudaGraphExecDestroy(f.graph[k]);
+        f.graph[k] = nullptr;
+    }
+    if (f.st) cudaStreamSynchronize(f.st);
+    if (f.side) cudaStreamSynchronize(f.side);
+    cudaFree(f.dev);
+    cudaFree(f.gscr);
+    cudaFree(f.gscr_fs);
+    f.dev = nullptr;
+    f.gscr = f.gscr_fs = nullptr;
+    for (cudaEvent_t e : f.mev) cudaEventDestroy(e);
+    f.mev.clear();
+    if (f.fork) cudaEventDestroy(f.fork);
+    if (f.join) cudaEventDestroy(f.join);
+    if (f.done) cudaEventDestroy(f.done);
+    f.fork = f.join = f.done = nullptr;
+    if (f.side) cudaStreamDestroy(f.side);
+    if (f.st) cudaStreamDestroy(f.st);
+    f.st = f.side = nullptr;
+    f.built = 0;
+}
+
+// Whether the batch can take its next step as batched launches: every member initialised,
+// at the same time with the same step and schedule, in the same precision, none in
+// channel mode, owed whole-grid passes or a rescan of every line (those steps run per
+// member first), none timed, and no grid large enough for the tiled column-major stores.
+bool fused_eligible(HydBatch* b, int sed) {
+    const HydSim* a = b->members[0];
+    for (HydSim* s : b->members) {
+        if (!s->initialized || s->dp.channel || s->force_rescan || s->timing || s->g.tile_cols) return false;
+        if (s->full_pending & 1) return false;
+        if (sed && (s->full_pending & 2)) return false;
+        if (s->device != a->device || s->t != a->t || s->P.dT != a->P.dT ||
+            s->P.sediment_start != a->P.sediment_start || s->P.bed_change_start != a->P.bed_change_start ||
+            s->P.bed_period != a->P.bed_period || s->dp.mixed != a->dp.mixed || s->solver != a->solver)
+            return false;
+    }
+    return true;
+}
+
+// The device tables of the batched form (from the members' current pointers: a step
+// leaves them as it found them).
+int fused_build(HydBatch* b) {
+    BatchFused& f = b->bf;
+    const int nm = (int)b->members.size();
+    f.nm = nm;
+    const HydSim* a0 = b->members[0];
+    f.mixed = a0->dp.mixed;
+    f.solver = a0->solver;
+    std::vector<DevGrid> gs[3];
+    std::vector<DevParams> ps;
+    std::vector<double*> outs[4];
+    std::vector<int> counts[BP_COUNT];
+    std::vector<int> lines[BL_COUNT], firsts[BL_COUNT];
+    int Nmax = 0, Mmax = 0;
+    for (HydSim* s : b->members) {
+        const DevGrid g0 = s->g;
+        double *A = g0.t_u, *Bu = s->scratch_u, *C = g0.t_v, *D = s->scratch_v;
+        DevGrid g1 = g0, g2 = g0;
+        g1.t_u = Bu;
+        g2.t_u = Bu;
+        g2.t_v = D;
+        gs[0].push_back(g0);
+        gs[1].push_back(g1);
+        gs[2].push_back(g2);
+        ps.push_back(s->dp);
+        outs[0].push_back(Bu);
+        outs[1].push_back(D);
+        outs[2].push_back(C);
+        outs[3].push_back(A);
+        const int N = s->N, M = s->M;
+        const int rw = row_warp_ctas(g0, N + 3);
+        counts[BP_CB].push_back(((N - 1) * 32 + 255) / 256 + 1);
+        counts[BP_SM_BUD].push_back(rw + 4);
+        counts[BP_SM].push_back(rw);
+        counts[BP_SM_FSB].push_back(rw + 1);
+        counts[BP_EV].push_back(N - 1);
+        counts[BP_CEU].push_back(((N - 2) * 32 + 255) / 256);
+        counts[BP_EU].push_back(M - 1);
+        counts[BP_RR].push_back(N);
+        counts[BP_RC].push_back(M);
+        counts[BP_PF].push_back(row_warp_ctas(g0, N + 1) + 32 + 8);
+        counts[BP_FSJC].push_back(((N - 1) * 32 + 255) / 256);
+        counts[BP_UFS].push_back(row_warp_ctas(g0, N) + 2);
+        lines[BL_UZ].push_back(M - 1);
+        firsts[BL_UZ].push_back(2);
+        lines[BL_VZ].push_back(N - 1);
+        firsts[BL_VZ].push_back(2);
+        lines[BL_FSJ].push_back(M - 3);
+        firsts[BL_FSJ].push_back(3);
+        lines[BL_FSI].push_back(N - 3);
+        firsts[BL_FSI].push_back(3);
+        Nmax = std::max(Nmax, N);
+        Mmax = std::max(Mmax, M);
+        f.thr_r = std::max(f.thr_r, s->thr_r);
+        f.thr_c = std::max(f.thr_c, s->thr_c);
+        size_t ev, eu, rr, rc, pf;
+        line_smem(N, M, &ev, &eu, &rr, &rc, &pf);
+        f.sm_ev = std::max(f.sm_ev, ev);
+        f.sm_eu = std::max(f.sm_eu, eu);
+        f.sm_rr = std::max(f.sm_rr, rr);
+        f.sm_rc = std::max(f.sm_rc, rc);
+        f.sm_pf = std::max(f.sm_pf, pf);
+    }
+    // one device block: grids, parameters, output pointers, CTA starts, line lists
+    auto a8 = [](size_t x) { return (x + 255) / 256 * 256; };
+    size_t off = 0;
+    size_t o_g[3], o_p, o_out[4], o_b[BP_COUNT], o_ls[BL_COUNT], o_lf[BL_COUNT];
+    for (int k = 0; k < 3; k++) { o_g[k] = off; off += a8(sizeof(DevGrid) * nm); }
+    o_p = off;
+    off += a8(sizeof(DevParams) * nm);
+    for (int k = 0; k < 4; k++) { o_out[k] = off; off += a8(sizeof(double*) * nm); }
+    for (int k = 0; k < BP_COUNT; k++) { o_b[k] = off; off += a8(sizeof(int) * (nm + 1)); }
+    for (int k = 0; k < BL_COUNT; k++) {
+        o_ls[k] = off;
+        off += a8(sizeof(int) * (nm + 1));
+        o_lf[k] = off;
+        off += a8(sizeof(int) * nm);
+    }
+    std::vector<char> host(off, 0);
+    for (int k = 0; k < 3; k++) memcpy(host.data() + o_g[k], gs[k].data(), sizeof(DevGrid) * nm);
+    memcpy(host.data() + o_p, ps.data(), sizeof(DevParams) * nm);
+    for (int k = 0; k < 4; k++) memcpy(host.data() + o_out[k], outs[k].data(), sizeof(double*) * nm);
+    for (int k = 0; k < BP_COUNT; k++) {
+        int* q = (int*)(host.data() + o_b[k]);
+        q[0] = 0;
+        for (int m = 0; m < nm; m++) q[m + 1] = q[m] + counts[k][m];
+        f.ctas[k] = q[nm];
+    }
+    for (int k = 0; k < BL_COUNT; k++) {
+        int* q = (int*)(host.data() + o_ls[k]);
+        q[0] = 0;
+        for (int m = 0; m < nm; m++) q[m + 1] = q[m] + std::max(lines[k][m], 0);
+        memcpy(host.data() + o_lf[k], firsts[k].data(), sizeof(int) * nm);
+    }
+    CUDA_TRY(cudaSetDevice(a0->device));
+    CUDA_TRY(cudaMalloc(&f.dev, off));
+    CUDA_TRY(cudaMemcpy(f.dev, host.data(), off, cudaMemcpyHostToDevice));
+    char* d = (char*)f.dev;
+    for (int k = 0; k < 3; k++) f.gS[k] = (DevGrid*)(d + o_g[k]);
+    f.p = (DevParams*)(d + o_p);
+    for (int k = 0; k < 4; k++) f.outs[k] = (double**)(d + o_out[k]);
+    for (int k = 0; k < BP_COUNT; k++) f.bst[k] = (int*)(d + o_b[k]);
+    for (int k = 0; k < BL_COUNT; k++) {
+        f.lst[k] = (int*)(d + o_ls[k]);
+        f.lfirst[k] = (int*)(d + o_lf[k]);
+    }
+    // the sweeps' plan for the largest member, one persistent CTA per SM
+    CUDA_TRY(sweep_plan(Nmax, Mmax, &f.plan, 0));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, a0->device);
+    f.grid = nsm;
+    if (f.plan.need_global) {
+        const size_t rows = 4 * (size_t)std::max(f.plan.RG, f.plan.RGf) + 6 * HYD_SEGL;
+        CUDA_TRY(cudaMalloc(&f.gscr, rows * f.grid * sizeof(double)));
+        CUDA_TRY(cudaMalloc(&f.gscr_fs, rows * f.grid * sizeof(double)));
+    }
+    CUDA_TRY(batch_sweep_setup());
+    CUDA_TRY(batch_grid_setup(f.sm_ev, f.sm_eu, f.sm_rr, f.sm_rc, f.sm_pf));
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    CUDA_TRY(cudaStreamCreateWithPriority(&f.st, cudaStreamNonBlocking, prio_hi));
+    CUDA_TRY(cudaStreamCreateWithPriority(&f.side, cudaStreamNonBlocking, prio_lo));
+    CUDA_TRY(cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming));
+    f.mev.resize(nm);
+    for (int m = 0; m < nm; m++) CUDA_TRY(cudaEventCreateWithFlags(&f.mev[m], cudaEventDisableTiming));
+    f.epochs.clear();
+    for (HydSim* s : b->members) f.epochs.push_back(s->epoch);
+    f.built = 1;
+    return HYD_OK;
+}
+
+// The launch sequence of one batched step (launch_step's span-limited sequence, every
+// phase one launch for all members).
+void fused_launch_step(HydBatch* b, int sed1, int sed2, int bed) {
+    BatchFused& f = b->bf;
+    const int nm = f.nm, mx = f.mixed;
+    auto BR = [&](int state, int ph) { return BatchRef{f.gS[state], f.p, f.bst[ph], nm}; };
+    auto BL = [&](int state, int set) { return BatchLines{f.gS[state], f.p, f.lst[set], f.lfirst[set], nm}; };
+    cudaStream_t st = f.st;
+    // ---- half-step 1
+    launch_coef_bnd_batch(BR(0, BP_CB), f.ctas[BP_CB], 0, 3, mx, st);
+    launch_sweep_batch(0, BL(0, BL_UZ), f.plan, f.solver, mx, f.gscr, f.grid, st);
+    launch_smooth_batch(BR(0, BP_SM_BUD), f.ctas[BP_SM_BUD], 1, f.outs[0], 0, 0, 1, st);
+    launch_explicit_v_batch(BR(1, BP_EV), f.ctas[BP_EV], f.thr_r, f.sm_ev, mx, st);
+    launch_smooth_batch(BR(1, BP_SM), f.ctas[BP_SM], 0, f.outs[1], 0, 0, 0, st);
+    launch_reset_batch(BR(2, BP_RR), f.ctas[BP_RR], 1, f.thr_r, f.sm_rr, st);
+    launch_post_fused_batch(BR(2, BP_PF), f.ctas[BP_PF], 0, sed1, mx, f.sm_pf, st);
+    if (sed1) {  // the first half-step's sediment beside the second half-step (as launch_step)
+        cudaEventRecord(f.fork, st);
+        cudaStreamWaitEvent(f.side, f.fork, 0);
+        launch_coef_fsj_batch(BR(2, BP_FSJC), f.ctas[BP_FSJC], 0, mx, f.side);
+        launch_fs_sweep_batch(0, BL(2, BL_FSJ), f.plan, 0, f.solver, mx, f.gscr_fs, f.grid, f.side);
+        launch_update_fs_batch(BR(2, BP_UFS), f.ctas[BP_UFS], f.side);
+        cudaEventRecord(f.join, f.side);
+    }
+    // ---- half-step 2
+    launch_coef_bnd_batch(BR(2, BP_CB), f.ctas[BP_CB], 1, sed1 ? 1 : 3, mx, st);
+    launch_sweep_batch(1, BL(2, BL_VZ), f.plan, f.solver, mx, f.gscr, f.grid, st);
+    launch_smooth_batch(BR(2, BP_SM_BUD), f.ctas[BP_SM_BUD], 0, f.outs[2], 0, 0, 1, st);
+    launch_coef_eu_batch(BR(1, BP_CEU), f.ctas[BP_CEU], mx, st);
+    launch_explicit_u_batch(BR(1, BP_EU), f.ctas[BP_EU], f.thr_c, f.sm_eu, mx, st);
+    if (sed1) cudaStreamWaitEvent(st, f.join, 0);
+    launch_smooth_batch(BR(1, sed1 ? BP_SM_FSB : BP_SM), f.ctas[sed1 ? BP_SM_FSB : BP_SM], 1, f.outs[3], 1, sed1, 0,
+                        st);
+    launch_reset_batch(BR(0, BP_RC), f.ctas[BP_RC], 0, f.thr_c, f.sm_rc, st);
+    launch_post_fused_batch(BR(0, BP_PF), f.ctas[BP_PF], 1, sed2, mx, f.sm_pf, st);
+    if (sed2) {
+        launch_fs_sweep_batch(1, BL(0, BL_FSI), f.plan, 1, f.solver, mx, f.gscr, f.grid, st);
+        launch_update_fs_batch(BR(0, BP_UFS), f.ctas[BP_UFS], st);
+    }
+    if (bed) {  // once per bed period: the members' own launches, inside the step's graph
+        for (HydSim* s : b->members) {
+            const int start = sed2 ? 3 : 2, end = sed2 ? s->N - 1 : s->N;
+            launch_bed(s->g, s->dp, start, end, st);
+        }
+    }
+}
+
+cudaGraphExec_t fused_graph(HydBatch* b, int mask) {
+    BatchFused& f = b->bf;
+    if (f.graph[mask]) return f.graph[mask];
+    const long long before = hyd_kernel_launches_add(0);
+    if (cudaStreamBeginCapture(f.st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return nullptr;
+    fused_launch_step(b, mask & 1, (mask >> 1) & 1, (mask >> 2) & 1);
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamEndCapture(f.st, &graph) != cudaSuccess || !graph) return nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return nullptr;
+    const long long after = hyd_kernel_launches_add(0);
+    f.graph_kernels[mask] = after - before;
+    hyd_kernel_launches_add(-(after - before));
+    f.graph[mask] = exec;
+    return exec;
+}
+
+// One batched step of every member; HYD_ESTATE (nothing done) when the batch is not
+// eligible for it now.
+int fused_step(HydBatch* b) {
+    HydSim* a = b->members[0];
+    const double t1 = a->t + a->P.dT * 0.5;
+    const double t2 = t1 + a->P.dT * 0.5;
+    const int sed1 = t1 >= a->P.sediment_start;
+    const int sed2 = t2 >= a->P.sediment_start;
+    if (!fused_eligible(b, sed1 || sed2)) return HYD_ESTATE;
+    for (HydSim* s : b->members)
+        if ((int)(t2 / 3600) + 1 >= s->g.total_time) return fail(HYD_EINVAL, "boundary tables too short");
+    const double it = (double)(long long)t2;
+    const int bed = a->P.bed_period > 0 ? (t2 - it == 0 && t2 >= a->P.bed_change_start &&
+                                           std::fmod(it, a->P.bed_period) == 0)
+                                        : (std::fmod(it, a->P.bed_change_start) == 0 && t2 - it == 0);
+    BatchFused& f = b->bf;
+    if (!f.built) {
+        const int rc = fused_build(b);
+        if (rc) return rc;
+    }
+    const int mask = sed1 | (sed2 << 1) | (bed << 2);
+    cudaGraphExec_t exec = fused_graph(b, mask);
+    if (!exec) return fail(HYD_ECUDA, "batched step: graph capture failed");
+    CUDA_TRY(cudaGraphLaunch(exec, f.st));
+    hyd_kernel_launches_add(f.graph_kernels[mask]);
+    for (HydSim* s : b->members) {
+        s->t = t2;
+        s->start_idx = sed2 ? 3 : 2;
+        s->end_idx = sed2 ? s->N - 1 : s->N;
+    }
+    f.steps++;
+    return HYD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hyd_batch_set_fused(hyd_batch b, int on) {
+    if (!b) return fail(HYD_EINVAL, "null batch");
+    b->fused = on ? 1 : 0;
+    return HYD_OK;
+}
+
+int hyd_batch_fused_steps(hyd_batch b, long long* steps) {
+    if (!b || !steps) return fail(HYD_EINVAL, "null argument");
+    *steps = b->bf.steps;
+    return HYD_OK;
+}
+
 int hyd_batch_step(hyd_batch b, int nsteps, int sync) {
     if (!b) return fail(HYD_EINVAL, "null batch");
     if (nsteps < 0) return fail(HYD_EINVAL, "nsteps < 0");
+    if (b->fused && nsteps > 0) {
+        // batched steps while the members allow them (a member owing whole-grid passes or
+        // a full rescan takes that step on its own first); the members' streams and the
+        // batch stream are ordered both ways around the batched run
+        BatchFused& f = b->bf;
+        int n = 0;
+        int ordered = 0;
+        while (n < nsteps) {
+            HydSim* a = b->members[0];
+            const double t1 = a->t + a->P.dT * 0.5, t2 = t1 + a->P.dT * 0.5;
+            if (!fused_eligible(b, t1 >= a->P.sediment_start || t2 >= a->P.sediment_start)) {
+                if (ordered) {  // the batched steps before this one come first
+                    CUDA_TRY(cudaEventRecord(f.done, f.st));
+                    for (HydSim* s : b->members) CUDA_TRY(cudaStreamWaitEvent(s->stream, f.done, 0));
+                    ordered = 0;
+                }
+                for (size_t k = 0; k < b->members.size(); k++) {
+                    const int rc = hyd_step(b->members[k], 1, 0, nullptr);
+                    if (rc) return fail(rc, "batch member " + std::to_string(k) + ": " + hyd_last_error());
+                }
+                n++;
+                continue;
+            }
+            if (!ordered) {
+                // tables built before a member's parameters, fields or spans changed are stale
+                bool stale = !f.built;
+                for (size_t k = 0; f.built && k < b->members.size(); k++)
+                    if (b->members[k]->epoch != f.epochs[k]) stale = true;
+                if (stale) {
+                    if (f.built) fused_release(f);
+                    const int rc = fused_build(b);
+                    if (rc) return rc;
+                }
+                for (size_t k = 0; k < b->members.size(); k++) {
+                    CUDA_TRY(cudaEventRecord(f.mev[k], b->members[k]->stream));
+                    CUDA_TRY(cudaStreamWaitEvent(f.st, f.mev[k], 0));
+                }
+                ordered = 1;
+            }
+            const int rc = fused_step(b);
+            if (rc) return rc;
+            n++;
+        }
+        if (ordered) {
+            CUDA_TRY(cudaEventRecord(f.done, f.st));
+            for (HydSim* s : b->members) CUDA_TRY(cudaStreamWaitEvent(s->stream, f.done, 0));
+        }
+        CUDA_TRY(cudaGetLastError());
+        if (sync) {
+            for (size_t k = 0; k < b->members.size(); k++) {
+                const int rc = hyd_synchronize(b->members[k]);
+                if (rc) return fail(rc, "batch member " + std::to_string(k) + ": " + hyd_last_error());
+            }
+        }
+        return HYD_OK;
+    }
     // one step of every member at a time: each member's graphs go to its own stream, so
     // the device runs the members side by side while the host queues the next round
     for (int n = 0; n < nsteps; n++) {
@@ -1603,6 +1993,10 @@ int hyd_batch_step(hyd_batch b, int nsteps, int sync) {
 
 int hyd_batch_destroy(hyd_batch b) {
     if (!b) return HYD_OK;
+    if (!b->members.empty()) {
+        cudaSetDevice(b->members[0]->device);
+        fused_release(b->bf);
+    }
     int rc = HYD_OK;
     for (hyd_handle h : b->members) {
         const int r = hyd_destroy(h);

@@ -94,6 +94,66 @@ constexpr int kBudOpen = 24, kBudClose = 25, kBudBed = 26, kBudSlots = 32;
 
 __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { atomicOr(g.status, bit); }
 
+// CTAs of 256 threads that give each of `rows` rows g.wpr warps (the extended-span kernels).
+__host__ __device__ __forceinline__ int row_warp_ctas(const DevGrid& g, int rows) {
+    return (rows * g.wpr * 32 + 255) / 256;
+}
+
+// A batch of reaches stepped by batched launches: member m's grid and parameters (device
+// arrays), and for one launch the first CTA of each member's share (bstart[m], with
+// bstart[nm] the launch's CTAs).  Every CTA of a batched launch works for one member.
+struct BatchRef {
+    const DevGrid* g;
+    const DevParams* p;
+    const int* bstart;
+    int nm;
+};
+
+// The last m with bstart[m] <= b.
+__device__ __forceinline__ int batch_member_of(const int* bstart, int nm, int b) {
+    int lo = 0, hi = nm - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (bstart[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The lines of a batched sweep: every member's lines in one list (member m's at list
+// positions lstart[m] .. lstart[m + 1] - 1, its lines first[m] onwards).
+struct BatchLines {
+    const DevGrid* g;
+    const DevParams* p;
+    const int* lstart;
+    const int* first;
+    int nm;
+    __device__ __forceinline__ int count() const;
+    __device__ __forceinline__ void at(int li, int& m, int& line) const;
+    __device__ __forceinline__ const DevGrid& grid(int m) const { return g[m]; }
+    __device__ __forceinline__ const DevParams& params(int m) const { return p[m]; }
+};
+
+__device__ __forceinline__ int BatchLines::count() const { return lstart[nm]; }
+__device__ __forceinline__ void BatchLines::at(int li, int& m, int& line) const {
+    m = batch_member_of(lstart, nm, li);
+    line = first[m] + (li - lstart[m]);
+}
+
+// This CTA's member, and its index bx among the member's gx CTAs (what blockIdx.x and
+// gridDim.x are in a launch for that member alone).
+struct BatchMember {
+    int m, bx, gx;
+    const DevGrid& g;
+    const DevParams& p;
+    __device__ __forceinline__ explicit BatchMember(const BatchRef& br)
+        : m(batch_member_of(br.bstart, br.nm, (int)blockIdx.x)),
+          bx((int)blockIdx.x - br.bstart[m]),
+          gx(br.bstart[m + 1] - br.bstart[m]),
+          g(br.g[m]),
+          p(br.p[m]) {}
+};
+
 // Column-major copy k of a per-cell quantity; (row i, column j) is at [j * g.LT + i].
 __device__ __forceinline__ double* colT(const DevGrid& g, int k) { return g.colT + (size_t)k * g.colT_stride; }
 __device__ __forceinline__ double* rowC(const DevGrid& g, int k) { return g.rowC + (size_t)k * g.rowC_stride; }
@@ -319,3 +379,23 @@ void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, 
 // feedback: h0 = h (the bed the applied changes start from), dH and its compensation zeroed
 void launch_bed_reset(const DevGrid& g, cudaStream_t s);
 long long hyd_kernel_launches_add(long long n);
+
+// Batched launches (k_grid.cu, k_sweep.cu): one launch for every member of a batch, each
+// CTA working for one member; `ctas` = the members' CTAs together.
+void launch_coef_bnd_batch(const BatchRef& br, int ctas, int half, int writes, int mixed, cudaStream_t s);
+void launch_smooth_batch(const BatchRef& br, int ctas, int isU, double* const* outs, int bytes, int fs_bnd, int budget,
+                         cudaStream_t s);
+void launch_explicit_v_batch(const BatchRef& br, int ctas, int threads, size_t smem, int mixed, cudaStream_t s);
+void launch_coef_eu_batch(const BatchRef& br, int ctas, int mixed, cudaStream_t s);
+void launch_explicit_u_batch(const BatchRef& br, int ctas, int threads, size_t smem, int mixed, cudaStream_t s);
+void launch_reset_batch(const BatchRef& br, int ctas, int rows, int threads, size_t smem, cudaStream_t s);
+void launch_post_fused_batch(const BatchRef& br, int ctas, int rows, int vth, int mixed, size_t smem, cudaStream_t s);
+void launch_update_fs_batch(const BatchRef& br, int ctas, cudaStream_t s);
+void launch_coef_fsj_batch(const BatchRef& br, int ctas, int half, int mixed, cudaStream_t s);
+void launch_sweep_batch(int dir, const BatchLines& bl, const SweepPlan& sp, int solver, int mixed, double* scratch,
+                        int grid, cudaStream_t s);
+void launch_fs_sweep_batch(int dir, const BatchLines& bl, const SweepPlan& sp, int half, int solver, int mixed,
+                           double* scratch, int grid, cudaStream_t s);
+cudaError_t batch_grid_setup(size_t smem_ev, size_t smem_eu, size_t smem_rr, size_t smem_rc, size_t smem_pf);
+cudaError_t batch_sweep_setup();
+void line_smem(int N, int M, size_t* ev, size_t* eu, size_t* rr, size_t* rc, size_t* pf);

@@ -426,9 +426,11 @@ __device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams
 // shared-memory tile (colmajor_tile), 8 rows of a column at a time.  The variants are
 // separate kernels: the tile's shared memory would otherwise shrink the L1 share of the
 // small grids' launches, whose stencil loads it serves.
+// bx, gx: the CTA's index among the launch's CTAs of this grid and their count (blockIdx.x
+// and gridDim.x of a launch for one grid; a member's share of a batched launch).
 template <int KIND, int TILE, class R>
-__global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int writes) {
-    if (blockIdx.x == gridDim.x - 1) {
+__device__ __forceinline__ void coef_bnd_body(const DevGrid& g, const DevParams& p, int writes, int bx, int gx) {
+    if (bx == gx - 1) {
         __shared__ double s_t;
         if (threadIdx.x == 0) {
             if (KIND == 0) {  // k_clock
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int wr
         R* const dst[7] = {colTr<R>(g, 0), colTr<R>(g, 1), colTr<R>(g, 2), colTr<R>(g, 3),
                            colTr<R>(g, 4), colTr<R>(g, 5), colTr<R>(g, 6)};
         colmajor_tile<7>(
-            g, 2 + kTileRows * blockIdx.x, g.N, 2, g.M,
+            g, 2 + kTileRows * bx, g.N, 2, g.M,
             [&](int i, int j, R* v) {
                 const int pos = i * g.P + j;
                 if (g.khouot[pos] != 0) return false;
@@ -461,7 +463,7 @@ __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int wr
             dst);
         return;
     }
-    const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int i = 2 + ((bx * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i > g.N) return;
     const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
     for (int j = lo + lane; j <= hi; j += 32) {
@@ -489,6 +491,16 @@ __global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int wr
             rowCr<R>(g, 6)[pos] = f5;
         }
     }
+}
+
+template <int KIND, int TILE, class R>
+__global__ void __launch_bounds__(256) k_coef_bnd(DevGrid g, DevParams p, int writes) {
+    coef_bnd_body<KIND, TILE, R>(g, p, writes, blockIdx.x, gridDim.x);
+}
+template <int KIND, int TILE, class R>
+__global__ void __launch_bounds__(256) k_coef_bnd_b(BatchRef br, int writes) {
+    const BatchMember bm(br);
+    coef_bnd_body<KIND, TILE, R>(bm.g, bm.p, writes, bm.bx, bm.gx);
 }
 
 // ------------------------------------------------------------------- smoothing
@@ -546,8 +558,8 @@ __device__ __forceinline__ void reset_byte_cell(const DevGrid& g, const DevParam
 // (warp % wpr) * 32 + lane, stride wpr * 32.
 struct RowLane {
     int i, off, stride;
-    __device__ __forceinline__ RowLane(const DevGrid& g, int i0) {
-        const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    __device__ __forceinline__ RowLane(const DevGrid& g, int i0, int bx) {
+        const int gw = (bx * blockDim.x + threadIdx.x) >> 5;
         i = i0 + gw / g.wpr;
         off = (gw % g.wpr) * 32 + (threadIdx.x & 31);
         stride = g.wpr * 32;
@@ -638,22 +650,34 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
 // BUD: four more CTAs (the last) add the half-step's open-edge volumes to the budget
 // (edge_budget; the smoothing of the swept velocity, isU = the UZ sweep's half-step).
 template <int BYTES, int FSB, int BUD>
-__global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
-    if (BUD && (int)blockIdx.x >= (int)gridDim.x - 4) {
-        edge_budget(g, p, isU, blockIdx.x - (gridDim.x - 4));
+__device__ __forceinline__ void smooth_span_body(const DevGrid& g, const DevParams& p, int isU,
+                                                 double* __restrict__ out, int bx, int gx) {
+    if (BUD && bx >= gx - 4) {
+        edge_budget(g, p, isU, bx - (gx - 4));
         return;
     }
-    if (FSB && blockIdx.x == gridDim.x - 1) {
+    if (FSB && bx == gx - 1) {
         boundary_body(g, g.clock[1], kBndFS);
         return;
     }
-    const RowLane rl(g, 0);
+    const RowLane rl(g, 0, bx);
     const int i = rl.i;
     if (i > g.N + 2) return;
     for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
         smooth_cell(g, p, isU, out, i, j, false);
         if (BYTES) reset_byte_cell(g, p, i, j);
     }
+}
+
+template <int BYTES, int FSB, int BUD>
+__global__ void k_smooth_span(DevGrid g, DevParams p, int isU, double* __restrict__ out) {
+    smooth_span_body<BYTES, FSB, BUD>(g, p, isU, out, blockIdx.x, gridDim.x);
+}
+// outs[m]: member m's output array
+template <int BYTES, int FSB, int BUD>
+__global__ void k_smooth_span_b(BatchRef br, int isU, double* const* outs) {
+    const BatchMember bm(br);
+    smooth_span_body<BYTES, FSB, BUD>(bm.g, bm.p, isU, outs[bm.m], bm.bx, bm.gx);
 }
 
 // ----------------------------------------------------------- explicit momentum
@@ -700,10 +724,10 @@ __device__ __forceinline__ R ev_cell(const DevGrid& g, const DevParams& p, int r
 // solveV/vSolver (UVZSolver_multithread.cu:1055-1071, 727-768) on row i, then
 // update_margin_elem_V (1008-1052) for the same row.
 template <class R>
-__global__ void k_explicit_v(DevGrid g, DevParams p) {
+__device__ __forceinline__ void explicit_v_body(const DevGrid& g, const DevParams& p, int bx) {
     extern __shared__ double sv[];  // the row's t_v over [k0, k1]
     __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL], s_first[HYD_SEGL], s_last[HYD_SEGL], s_off[HYD_SEGL + 1];
-    const int row = 2 + blockIdx.x;
+    const int row = 2 + bx;
     const int P = g.P, M = g.M;
     const int nseg = g.moci[row];
     if (nseg == 0) return;
@@ -756,6 +780,16 @@ __global__ void k_explicit_v(DevGrid g, DevParams p) {
     __syncthreads();  // keep the other warps resident while thread 0 works
 }
 
+template <class R>
+__global__ void k_explicit_v(DevGrid g, DevParams p) {
+    explicit_v_body<R>(g, p, blockIdx.x);
+}
+template <class R>
+__global__ void k_explicit_v_b(BatchRef br) {
+    const BatchMember bm(br);
+    explicit_v_body<R>(bm.g, bm.p, bm.bx);
+}
+
 // uSolver (UVZSolver_multithread.cu:773-815) for one cell in the arithmetic type R: the new
 // u velocity.  Cell-local, so it is computed for every wet cell by a row-major kernel and
 // stored column-major.
@@ -804,9 +838,9 @@ constexpr int kEuSlot = 4;
 // explicit_u values of every wet cell of rows 2..N-1, columns 2..M, one warp per row over
 // the row's span; written column-major (g.colT array kEuSlot), with TILE through a tile.
 template <int TILE, class R>
-__global__ void __launch_bounds__(256) k_coef_eu(DevGrid g, DevParams p) {
+__device__ __forceinline__ void coef_eu_body(const DevGrid& g, const DevParams& p, int bx) {
     if constexpr (!TILE) {
-        const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+        const int i = 2 + ((bx * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
         if (i > g.N - 1) return;
         const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
         for (int j = lo + lane; j <= hi; j += 32) {
@@ -816,7 +850,7 @@ __global__ void __launch_bounds__(256) k_coef_eu(DevGrid g, DevParams p) {
     } else {
         R* const dst[1] = {colTr<R>(g, kEuSlot)};
         colmajor_tile<1>(
-            g, 2 + kTileRows * blockIdx.x, g.N - 1, 2, g.M,
+            g, 2 + kTileRows * bx, g.N - 1, 2, g.M,
             [&](int i, int j, R* v) {
                 if (g.khouot[i * g.P + j] != 0) return false;
                 v[0] = eu_cell<R>(g, p, i, j);
@@ -826,13 +860,23 @@ __global__ void __launch_bounds__(256) k_coef_eu(DevGrid g, DevParams p) {
     }
 }
 
+template <int TILE, class R>
+__global__ void __launch_bounds__(256) k_coef_eu(DevGrid g, DevParams p) {
+    coef_eu_body<TILE, R>(g, p, blockIdx.x);
+}
+template <int TILE, class R>
+__global__ void __launch_bounds__(256) k_coef_eu_b(BatchRef br) {
+    const BatchMember bm(br);
+    coef_eu_body<TILE, R>(bm.g, bm.p, bm.bx);
+}
+
 // solveU/uSolver (UVZSolver_multithread.cu:947-968, 773-815) on column j from the values
 // k_coef_eu stored, then update_margin_elem_U (970-1006).
 template <class R>
-__global__ void k_explicit_u(DevGrid g, DevParams p) {
+__device__ __forceinline__ void explicit_u_body(const DevGrid& g, const DevParams& p, int bx) {
     extern __shared__ double su[];  // the column's t_u over [k0, k1]
     __shared__ int s_b1[HYD_SEGL], s_b2[HYD_SEGL], s_first[HYD_SEGL], s_last[HYD_SEGL], s_off[HYD_SEGL + 1];
-    const int col = 2 + blockIdx.x;
+    const int col = 2 + bx;
     const int P = g.P, N = g.N;
     const int nseg = g.mocj[col];
     if (nseg == 0) return;
@@ -883,6 +927,16 @@ __global__ void k_explicit_u(DevGrid g, DevParams p) {
         }
     }
     __syncthreads();  // keep the other warps resident while thread 0 works
+}
+
+template <class R>
+__global__ void k_explicit_u(DevGrid g, DevParams p) {
+    explicit_u_body<R>(g, p, blockIdx.x);
+}
+template <class R>
+__global__ void k_explicit_u_b(BatchRef br) {
+    const BatchMember bm(br);
+    explicit_u_body<R>(bm.g, bm.p, bm.bx);
 }
 
 // --------------------------------------------------------------- wet/dry resets
@@ -998,10 +1052,10 @@ __host__ __device__ __forceinline__ int reset_words(int L) { return (L + 3) / 32
 // for the rescan that follows.
 // blockDim.x is a multiple of 32: each warp pass covers whole 32-cell words.
 template <int ROWS>
-__global__ void k_reset(DevGrid g, DevParams p, int force) {
+__device__ __forceinline__ void reset_body(const DevGrid& g, const DevParams& p, int force, int bx) {
     extern __shared__ unsigned char rsm[];
     __shared__ int s_changed;
-    const int line = 1 + blockIdx.x;
+    const int line = 1 + bx;
     const int P = g.P;
     const int L = ROWS ? g.M : g.N;  // last cell index of the line
     const int along = ROWS ? 1 : P;
@@ -1154,6 +1208,16 @@ __global__ void k_reset(DevGrid g, DevParams p, int force) {
     __syncthreads();  // keep the other warps resident while warp 0 scans
 }
 
+template <int ROWS>
+__global__ void k_reset(DevGrid g, DevParams p, int force) {
+    reset_body<ROWS>(g, p, force, blockIdx.x);
+}
+template <int ROWS>
+__global__ void k_reset_b(BatchRef br, int force) {
+    const BatchMember bm(br);
+    reset_body<ROWS>(bm.g, bm.p, force, bm.bx);
+}
+
 // Column-major mask bytes of the whole grid (the cells outside the extended spans keep
 // them: their mask is 2 for good).
 __global__ void k_reset_bytes_init(DevGrid g) {
@@ -1264,7 +1328,7 @@ __global__ void k_post(DevGrid g, int with_uvz) {
 }
 
 __global__ void k_post_span(DevGrid g) {
-    const RowLane rl(g, 0);
+    const RowLane rl(g, 0, blockIdx.x);
     const int i = rl.i;
     if (i > g.N) return;
     for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) post_cell(g, 1, i, j);
@@ -1462,7 +1526,7 @@ __global__ void k_vth_hesok(DevGrid g, DevParams p) {
 
 template <int FSI, class R>
 __global__ void k_vth_span(DevGrid g, DevParams p) {
-    const RowLane rl(g, 0);
+    const RowLane rl(g, 0, blockIdx.x);
     const int i = rl.i;
     if (i > g.N) return;
     for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) vth_cell<FSI, R>(g, p, i, j);
@@ -1476,11 +1540,12 @@ __global__ void k_vth_span(DevGrid g, DevParams p) {
 // update).  None of the three writes what another reads.
 constexpr int kEdgeParts = 8;
 template <int ROWS, int VTH, class R>
-__global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
+__device__ __forceinline__ void post_fused_body(const DevGrid& g, const DevParams& p, int nbp, int nbs, int bx,
+                                                int gx) {
     extern __shared__ unsigned swords[];
-    const int b = blockIdx.x;
+    const int b = bx;
     if (b < nbp) {
-        const RowLane rl(g, 0);
+        const RowLane rl(g, 0, bx);
         const int i = rl.i;
         if (i > g.N) return;
         for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
@@ -1489,8 +1554,8 @@ __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
         }
         return;
     }
-    if (b >= (int)gridDim.x - kEdgeParts) {
-        fs_edges_part<0>(g, p, b - ((int)gridDim.x - kEdgeParts), kEdgeParts);
+    if (b >= gx - kEdgeParts) {
+        fs_edges_part<0>(g, p, b - (gx - kEdgeParts), kEdgeParts);
         return;
     }
     const int sb = b - nbp;
@@ -1530,6 +1595,17 @@ __global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
     }
 }
 
+template <int ROWS, int VTH, class R>
+__global__ void k_post_fused(DevGrid g, DevParams p, int nbp, int nbs) {
+    post_fused_body<ROWS, VTH, R>(g, p, nbp, nbs, blockIdx.x, gridDim.x);
+}
+template <int ROWS, int VTH, class R>
+__global__ void k_post_fused_b(BatchRef br) {
+    const BatchMember bm(br);
+    const int nbp = row_warp_ctas(bm.g, bm.g.N + 1);
+    post_fused_body<ROWS, VTH, R>(bm.g, bm.p, nbp, bm.gx - nbp - kEdgeParts, bm.bx, bm.gx);
+}
+
 // Update_FS (Sediment_Transport.cu:620-629)
 __global__ void k_update_fs(DevGrid g) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -1541,19 +1617,25 @@ __global__ void k_update_fs(DevGrid g) {
 // Update_FS over the extended spans, plus rows 2 and N and column M in full (the edge
 // interpolation writes FS there): CTAs [0, nb) take the rows other than 2 and N, the
 // last two CTAs rows 2 and N.
-__global__ void k_update_fs_span(DevGrid g, int nb) {
+__device__ __forceinline__ void update_fs_span_body(const DevGrid& g, int nb, int bx) {
     const int N = g.N, M = g.M, P = g.P;
-    if ((int)blockIdx.x >= nb) {
-        const int i = (int)blockIdx.x == nb ? 2 : N;
+    if (bx >= nb) {
+        const int i = bx == nb ? 2 : N;
         for (int j = 1 + threadIdx.x; j <= M; j += blockDim.x) g.FS[i * P + j] = g.tFS[i * P + j];
         return;
     }
-    const RowLane rl(g, 1);
+    const RowLane rl(g, 1, bx);
     const int i = rl.i;
     if (i > N || i == 2 || i == N) return;
     const int lo = g.elo[i] > 1 ? g.elo[i] : 1, hi = g.ehi[i] < M ? g.ehi[i] : M;
     for (int j = lo + rl.off; j <= hi; j += rl.stride) g.FS[i * P + j] = g.tFS[i * P + j];
     if (rl.off == 0 && (M < lo || M > hi)) g.FS[i * P + M] = g.tFS[i * P + M];
+}
+
+__global__ void k_update_fs_span(DevGrid g, int nb) { update_fs_span_body(g, nb, blockIdx.x); }
+__global__ void k_update_fs_span_b(BatchRef br) {
+    const BatchMember bm(br);
+    update_fs_span_body(bm.g, row_warp_ctas(bm.g, bm.g.N), bm.bx);
 }
 
 // Calculate_Qb (Sediment_Transport.cu:341-414): bed-load flux, then the edge copies.
@@ -1884,7 +1966,7 @@ void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes,
 }
 
 // Elementwise kernels: the whole grid (`full`), or one warp per row over its extended span.
-static int row_warps_blocks(const DevGrid& g, int rows) { return (rows * g.wpr * 32 + 255) / 256; }
+static int row_warps_blocks(const DevGrid& g, int rows) { return row_warp_ctas(g, rows); }
 
 void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, int fs_bnd,
                    int budget, cudaStream_t s) {
@@ -2057,4 +2139,102 @@ int launch_put_doubles(double* dst, const double* src, int n, cudaStream_t s) {
 void launch_pack_rows(const double* src, int pitch, double* dst, int rows, int cols, cudaStream_t s) {
     k_pack_rows<<<4 * 148, 256, 0, s>>>(src, pitch, dst, rows, cols);
     hyd_kernel_launches_add(1);
+}
+
+// ------------------------------------------------------------- batched launches
+// One launch for every member of a batch: `ctas` CTAs, member m's share starting at
+// br.bstart[m] (the CTAs its own launch would have), each CTA working for one member.
+
+void launch_coef_bnd_batch(const BatchRef& br, int ctas, int half, int writes, int mixed, cudaStream_t s) {
+    if (mixed) {
+        if (half == 1) k_coef_bnd_b<1, 0, float><<<ctas, 256, 0, s>>>(br, writes);
+        else k_coef_bnd_b<0, 0, float><<<ctas, 256, 0, s>>>(br, writes);
+    } else {
+        if (half == 1) k_coef_bnd_b<1, 0, double><<<ctas, 256, 0, s>>>(br, writes);
+        else k_coef_bnd_b<0, 0, double><<<ctas, 256, 0, s>>>(br, writes);
+    }
+    hyd_kernel_launches_add(1);
+}
+
+void launch_smooth_batch(const BatchRef& br, int ctas, int isU, double* const* outs, int bytes, int fs_bnd, int budget,
+                         cudaStream_t s) {
+    if (bytes && fs_bnd) k_smooth_span_b<1, 1, 0><<<ctas, 256, 0, s>>>(br, isU, outs);
+    else if (bytes) k_smooth_span_b<1, 0, 0><<<ctas, 256, 0, s>>>(br, isU, outs);
+    else if (budget) k_smooth_span_b<0, 0, 1><<<ctas, 256, 0, s>>>(br, isU, outs);
+    else k_smooth_span_b<0, 0, 0><<<ctas, 256, 0, s>>>(br, isU, outs);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_explicit_v_batch(const BatchRef& br, int ctas, int threads, size_t smem, int mixed, cudaStream_t s) {
+    if (mixed) k_explicit_v_b<float><<<ctas, threads, smem, s>>>(br);
+    else k_explicit_v_b<double><<<ctas, threads, smem, s>>>(br);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_coef_eu_batch(const BatchRef& br, int ctas, int mixed, cudaStream_t s) {
+    if (mixed) k_coef_eu_b<0, float><<<ctas, 256, 0, s>>>(br);
+    else k_coef_eu_b<0, double><<<ctas, 256, 0, s>>>(br);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_explicit_u_batch(const BatchRef& br, int ctas, int threads, size_t smem, int mixed, cudaStream_t s) {
+    if (mixed) k_explicit_u_b<float><<<ctas, threads, smem, s>>>(br);
+    else k_explicit_u_b<double><<<ctas, threads, smem, s>>>(br);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_reset_batch(const BatchRef& br, int ctas, int rows, int threads, size_t smem, cudaStream_t s) {
+    if (rows) k_reset_b<1><<<ctas, threads, smem, s>>>(br, 0);
+    else k_reset_b<0><<<ctas, threads, smem, s>>>(br, 0);
+    hyd_kernel_launches_add(1);
+}
+
+void launch_post_fused_batch(const BatchRef& br, int ctas, int rows, int vth, int mixed, size_t smem, cudaStream_t s) {
+    if (!vth) {
+        if (rows) k_post_fused_b<1, 0, double><<<ctas, 256, smem, s>>>(br);
+        else k_post_fused_b<0, 0, double><<<ctas, 256, smem, s>>>(br);
+    } else if (mixed) {
+        if (rows) k_post_fused_b<1, 1, float><<<ctas, 256, smem, s>>>(br);
+        else k_post_fused_b<0, 1, float><<<ctas, 256, smem, s>>>(br);
+    } else {
+        if (rows) k_post_fused_b<1, 1, double><<<ctas, 256, smem, s>>>(br);
+        else k_post_fused_b<0, 1, double><<<ctas, 256, smem, s>>>(br);
+    }
+    hyd_kernel_launches_add(1);
+}
+
+void launch_update_fs_batch(const BatchRef& br, int ctas, cudaStream_t s) {
+    k_update_fs_span_b<<<ctas, 256, 0, s>>>(br);
+    hyd_kernel_launches_add(1);
+}
+
+// Opt the batched kernels that stage a line in shared memory into `bytes` of it (the
+// largest any member needs).
+cudaError_t batch_grid_setup(size_t smem_ev, size_t smem_eu, size_t smem_rr, size_t smem_rc, size_t smem_pf) {
+    cudaError_t e;
+    const void* pf[] = {(const void*)k_post_fused_b<0, 0, double>, (const void*)k_post_fused_b<0, 1, double>,
+                        (const void*)k_post_fused_b<1, 0, double>, (const void*)k_post_fused_b<1, 1, double>,
+                        (const void*)k_post_fused_b<0, 1, float>, (const void*)k_post_fused_b<1, 1, float>};
+    for (const void* f : pf)
+        if ((e = allow_smem(f, smem_pf)) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_v_b<double>, smem_ev)) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_v_b<float>, smem_ev)) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_u_b<double>, smem_eu)) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_explicit_u_b<float>, smem_eu)) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_reset_b<1>, smem_rr)) != cudaSuccess) return e;
+    if ((e = allow_smem((const void*)k_reset_b<0>, smem_rc)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+// Shared memory the line kernels of one grid need (k_explicit_v / _u, k_reset rows /
+// columns, k_post_fused).
+void line_smem(int N, int M, size_t* ev, size_t* eu, size_t* rr, size_t* rc, size_t* pf) {
+    DevGrid g{};
+    g.N = N;
+    g.M = M;
+    *ev = sizeof(double) * (M + 3);
+    *eu = sizeof(double) * (N + 3);
+    *rr = reset_smem(M);
+    *rc = reset_smem(N);
+    *pf = scan_smem(g);
 }

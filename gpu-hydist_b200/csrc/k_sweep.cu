@@ -620,6 +620,22 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
     }
 }
 
+// The lines a sweep launch covers: lines start .. start + n - 1 of one grid, or the lines of
+// every member of a batch in one list (member m's at list positions lstart[m] ..
+// lstart[m + 1] - 1, its lines first[m] onwards).
+struct OneGridLines {
+    DevGrid g;
+    DevParams p;
+    int start, n;
+    __device__ __forceinline__ int count() const { return n; }
+    __device__ __forceinline__ void at(int li, int& m, int& line) const {
+        m = 0;
+        line = start + li;
+    }
+    __device__ __forceinline__ const DevGrid& grid(int) const { return g; }
+    __device__ __forceinline__ const DevParams& params(int) const { return p; }
+};
+
 // Fused sweep of one direction.  CTA b takes lines b, b + G, b + 2G, ... (G = gridDim.x)
 // in groups of 16, one line per warp.  Every warp sets its line up; a warp whose line is
 // short (at most roww rows) sweeps it alone in its own slice of shared memory; then the
@@ -628,25 +644,30 @@ __device__ __forceinline__ void hydro_body(const DevGrid& g, const DevParams& p,
 // Adjacent long lines (a wet band) fall on different CTAs.  Warps with nothing to sweep
 // wait at the CTA barriers rather than exit: the warp-synchronous steps of a warp whose
 // sibling warps had exited were measured an order of magnitude slower on B200.
-template <int DIR, int SOLVER, class R>
-__global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB,
-                                                     double* gscr_d, int RG, int roww) {
+template <int DIR, int SOLVER, class R, class Lines>
+__device__ __forceinline__ void hydro_sweep_loop(const Lines& lines, int RB, double* gscr_d, int RG, int roww) {
     constexpr bool MIX = sizeof(R) == sizeof(float);
     extern __shared__ double dyn_smem_d[];
     R* dyn_smem = reinterpret_cast<R*>(dyn_smem_d);
     R* gscr = reinterpret_cast<R*>(gscr_d);
     __shared__ LineShared sgw[kWL];
-    __shared__ int s_long[kWL];
+    __shared__ int s_long[kWL], s_mem[kWL], s_line[kWL];
     __shared__ int s_nlong;
     __shared__ R s_red[4 * kRedRows];  // reduced rows of the two-level solve
     const int w = threadIdx.x >> 5;
-    const int nlines = endidx - startidx + 1;
+    const int nlines = lines.count();
     const int G = gridDim.x;
     for (int j0 = 0; (int)blockIdx.x + j0 * G < nlines; j0 += kWL) {
         const int li = blockIdx.x + (j0 + w) * G;
         LineShared& sg = sgw[w];
+        int m = 0, line = 0;
+        if (li < nlines) lines.at(li, m, line);
         if (threadIdx.x == 0) s_nlong = 0;
-        if (li < nlines) hydro_setup<DIR, WarpG, MIX>(g, p, startidx + li, sg);  // warp-uniform
+        if ((threadIdx.x & 31) == 0) {
+            s_mem[w] = m;
+            s_line[w] = line;
+        }
+        if (li < nlines) hydro_setup<DIR, WarpG, MIX>(lines.grid(m), lines.params(m), line, sg);  // warp-uniform
         __syncthreads();
         if (li < nlines && sg.nseg > 0) {
             if (sg.R > roww) {
@@ -657,8 +678,8 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
                 R* B = A + wr;
                 R* Cc = B + wr;
                 R* D = Cc + wr;
-                hydro_body<DIR, SOLVER, WarpG, R>(g, p, startidx + li, sg, A, B, Cc, D, D + wr, nullptr,
-                                                  SolvePlan{32, chunk_len(sg.R, 32)});
+                hydro_body<DIR, SOLVER, WarpG, R>(lines.grid(m), lines.params(m), line, sg, A, B, Cc, D, D + wr,
+                                                  nullptr, SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
         __syncthreads();
@@ -666,7 +687,7 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
         for (int q = 0; q < nl; q++) {
             const int wl = s_long[q];
             const LineShared& sl = sgw[wl];
-            const int line = startidx + (int)blockIdx.x + (j0 + wl) * G;
+            const int lm = s_mem[wl];
             const SolvePlan pl = solve_plan(sl.R, SOLVER == 0 ? 256 : 32);
             const bool fits = pl.t1 * pl.m <= RB;
             const int rs = fits ? RB : RG;
@@ -674,10 +695,21 @@ __global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, 
             R* B = A + rs;
             R* Cc = B + rs;
             R* D = Cc + rs;
-            hydro_body<DIR, SOLVER, BlockG, R>(g, p, line, sl, A, B, Cc, D, D + rs, s_red, pl);
+            hydro_body<DIR, SOLVER, BlockG, R>(lines.grid(lm), lines.params(lm), s_line[wl], sl, A, B, Cc, D, D + rs,
+                                               s_red, pl);
             __syncthreads();  // the slices and sgw are reused
         }
     }
+}
+
+template <int DIR, int SOLVER, class R>
+__global__ void __launch_bounds__(kTL, 1) k_hydro_sweep(DevGrid g, DevParams p, int startidx, int endidx, int RB,
+                                                     double* gscr_d, int RG, int roww) {
+    hydro_sweep_loop<DIR, SOLVER, R>(OneGridLines{g, p, startidx, endidx - startidx + 1}, RB, gscr_d, RG, roww);
+}
+template <int DIR, int SOLVER, class R>
+__global__ void __launch_bounds__(kTL, 1) k_hydro_sweep_b(BatchLines bl, int RB, double* gscr_d, int RG, int roww) {
+    hydro_sweep_loop<DIR, SOLVER, R>(bl, RB, gscr_d, RG, roww);
 }
 
 // ---- sediment sweeps --------------------------------------------------------------
@@ -763,10 +795,10 @@ __device__ __forceinline__ void fsi_cell_coeffs(const DevGrid& g, const DevParam
 // the row's span, written column-major (colT arrays 0..3 in R: aa bb cc dd), with TILE
 // through a tile.
 template <int TILE, class R>
-__global__ void __launch_bounds__(256) k_coef_fsj(DevGrid g, DevParams p, int half) {
+__device__ __forceinline__ void coef_fsj_body(const DevGrid& g, const DevParams& p, int half, int bx) {
     const double t = g.clock[half];
     if constexpr (!TILE) {
-        const int i = 2 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+        const int i = 2 + ((bx * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
         if (i > g.N) return;
         const int lo = max(g.rlo[i], 3), hi = min(g.rhi[i], g.M - 1);
         for (int j = lo + lane; j <= hi; j += 32) {
@@ -783,7 +815,7 @@ __global__ void __launch_bounds__(256) k_coef_fsj(DevGrid g, DevParams p, int ha
     } else {
         R* const dst[4] = {colTr<R>(g, 0), colTr<R>(g, 1), colTr<R>(g, 2), colTr<R>(g, 3)};
         colmajor_tile<4>(
-            g, 2 + kTileRows * blockIdx.x, g.N, 3, g.M - 1,
+            g, 2 + kTileRows * bx, g.N, 3, g.M - 1,
             [&](int i, int j, R* v) {
                 const int pos = i * g.P + j;
                 if (g.khouot[pos] != 0) return false;
@@ -792,6 +824,16 @@ __global__ void __launch_bounds__(256) k_coef_fsj(DevGrid g, DevParams p, int ha
             },
             dst);
     }
+}
+
+template <int TILE, class R>
+__global__ void __launch_bounds__(256) k_coef_fsj(DevGrid g, DevParams p, int half) {
+    coef_fsj_body<TILE, R>(g, p, half, blockIdx.x);
+}
+template <int TILE, class R>
+__global__ void __launch_bounds__(256) k_coef_fsj_b(BatchRef br, int half) {
+    const BatchMember bm(br);
+    coef_fsj_body<TILE, R>(bm.g, bm.p, half, bm.bx);
 }
 
 // Segments of a sediment line and their row offsets (one row per interior cell
@@ -910,24 +952,29 @@ __device__ __forceinline__ void fs_body(const DevGrid& g, const DevParams& p, in
 }
 
 // Fused sediment sweep of one direction: as k_hydro_sweep.
-template <int DIR, int SOLVER, class R>
-__global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int half, int startidx, int endidx, int RB,
-                                                  double* gscr_d, int RG, int roww) {
+template <int DIR, int SOLVER, class R, class Lines>
+__device__ __forceinline__ void fs_sweep_loop(const Lines& lines, int half, int RB, double* gscr_d, int RG, int roww) {
     extern __shared__ double dyn_smem_d[];
     R* dyn_smem = reinterpret_cast<R*>(dyn_smem_d);
     R* gscr = reinterpret_cast<R*>(gscr_d);
     __shared__ LineShared sgw[kWL];
-    __shared__ int s_long[kWL];
+    __shared__ int s_long[kWL], s_mem[kWL], s_line[kWL];
     __shared__ int s_nlong;
     __shared__ R s_red[4 * kRedRows];  // reduced rows of the two-level solve
     const int w = threadIdx.x >> 5;
-    const int nlines = endidx - startidx + 1;
+    const int nlines = lines.count();
     const int G = gridDim.x;
     for (int j0 = 0; (int)blockIdx.x + j0 * G < nlines; j0 += kWL) {
         const int li = blockIdx.x + (j0 + w) * G;
         LineShared& sg = sgw[w];
+        int m = 0, line = 0;
+        if (li < nlines) lines.at(li, m, line);
         if (threadIdx.x == 0) s_nlong = 0;
-        if (li < nlines) fs_setup<DIR, WarpG>(g, p, startidx + li, sg);  // warp-uniform
+        if ((threadIdx.x & 31) == 0) {
+            s_mem[w] = m;
+            s_line[w] = line;
+        }
+        if (li < nlines) fs_setup<DIR, WarpG>(lines.grid(m), lines.params(m), line, sg);  // warp-uniform
         __syncthreads();
         if (li < nlines && sg.R > 0) {
             if (sg.R > roww) {
@@ -935,8 +982,8 @@ __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int
             } else {
                 const int wr = slice_rows(roww);
                 R* A = dyn_smem + w * 4 * wr;
-                fs_body<DIR, SOLVER, WarpG, R>(g, p, half, startidx + li, sg, A, A + wr, A + 2 * wr, A + 3 * wr,
-                                               nullptr, SolvePlan{32, chunk_len(sg.R, 32)});
+                fs_body<DIR, SOLVER, WarpG, R>(lines.grid(m), lines.params(m), half, line, sg, A, A + wr, A + 2 * wr,
+                                               A + 3 * wr, nullptr, SolvePlan{32, chunk_len(sg.R, 32)});
             }
         }
         __syncthreads();
@@ -944,15 +991,27 @@ __global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int
         for (int q = 0; q < nl; q++) {
             const int wl = s_long[q];
             const LineShared& sl = sgw[wl];
-            const int line = startidx + (int)blockIdx.x + (j0 + wl) * G;
+            const int lm = s_mem[wl];
             const SolvePlan pl = solve_plan(sl.R, SOLVER == 0 ? 256 : 32);
             const bool fits = pl.t1 * pl.m <= RB;
             const int rs = fits ? RB : RG;
             R* A = fits ? dyn_smem : gscr + (size_t)blockIdx.x * 4 * (size_t)RG;
-            fs_body<DIR, SOLVER, BlockG, R>(g, p, half, line, sl, A, A + rs, A + 2 * rs, A + 3 * rs, s_red, pl);
+            fs_body<DIR, SOLVER, BlockG, R>(lines.grid(lm), lines.params(lm), half, s_line[wl], sl, A, A + rs,
+                                            A + 2 * rs, A + 3 * rs, s_red, pl);
             __syncthreads();
         }
     }
+}
+
+template <int DIR, int SOLVER, class R>
+__global__ void __launch_bounds__(kTL, 1) k_fs_sweep(DevGrid g, DevParams p, int half, int startidx, int endidx, int RB,
+                                                  double* gscr_d, int RG, int roww) {
+    fs_sweep_loop<DIR, SOLVER, R>(OneGridLines{g, p, startidx, endidx - startidx + 1}, half, RB, gscr_d, RG, roww);
+}
+template <int DIR, int SOLVER, class R>
+__global__ void __launch_bounds__(kTL, 1) k_fs_sweep_b(BatchLines bl, int half, int RB, double* gscr_d, int RG,
+                                                    int roww) {
+    fs_sweep_loop<DIR, SOLVER, R>(bl, half, RB, gscr_d, RG, roww);
 }
 
 // Largest dynamic shared memory the kernel may be given on this device.
@@ -980,6 +1039,8 @@ cudaError_t allow_all(F* const* fs, int n, int* limit) {
 
 using HydroSweepFn = void(DevGrid, DevParams, int, int, int, double*, int, int);
 using FsSweepFn = void(DevGrid, DevParams, int, int, int, int, double*, int, int);
+using HydroSweepBFn = void(BatchLines, int, double*, int, int);
+using FsSweepBFn = void(BatchLines, int, int, double*, int, int);
 
 // [precision: 0 FP64, 1 mixed][direction][solver]
 HydroSweepFn* const kHydroSweep[2][2][2] = {
@@ -1135,4 +1196,80 @@ void launch_fs_sweep_j(const DevGrid& g, const DevParams& p, const SweepPlan& sp
 void launch_fs_sweep_i(const DevGrid& g, const DevParams& p, const SweepPlan& sp, int half, int solver,
                        double* scratch, cudaStream_t s) {
     fs_sweep(1, g, p, sp, half, 3, g.N - 1, solver, scratch, s);
+}
+
+// ---- batched sweeps: every member's lines in one persistent launch (the common plan of
+// the batch: rows kept in shared memory, warp tier wide)
+void launch_sweep_batch(int dir, const BatchLines& bl, const SweepPlan& sp, int solver, int mixed, double* scratch,
+                        int grid, cudaStream_t s) {
+    const int sv = solver ? 1 : 0;
+    const int roww = kRowW;
+    const size_t big = 4 * (size_t)sp.RB + kEnds, slices = (size_t)kWL * (4 * slice_rows(roww) + kEnds);
+    const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * (big > slices ? big : slices);
+    if (mixed) {
+        if (dir == 0) {
+            if (sv) k_hydro_sweep_b<0, 1, float><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+            else k_hydro_sweep_b<0, 0, float><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+        } else {
+            if (sv) k_hydro_sweep_b<1, 1, float><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+            else k_hydro_sweep_b<1, 0, float><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+        }
+    } else {
+        if (dir == 0) {
+            if (sv) k_hydro_sweep_b<0, 1, double><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+            else k_hydro_sweep_b<0, 0, double><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+        } else {
+            if (sv) k_hydro_sweep_b<1, 1, double><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+            else k_hydro_sweep_b<1, 0, double><<<grid, kTL, smem, s>>>(bl, sp.RB, scratch, sp.RG, roww);
+        }
+    }
+    hyd_kernel_launches_add(1);
+}
+
+void launch_fs_sweep_batch(int dir, const BatchLines& bl, const SweepPlan& sp, int half, int solver, int mixed,
+                           double* scratch, int grid, cudaStream_t s) {
+    const int sv = solver ? 1 : 0;
+    const int roww = kRowW;
+    const size_t big = 4 * (size_t)sp.RBf, slices = (size_t)kWL * 4 * slice_rows(roww);
+    const size_t smem = (mixed ? sizeof(float) : sizeof(double)) * (big > slices ? big : slices);
+    if (mixed) {
+        if (dir == 0) {
+            if (sv) k_fs_sweep_b<0, 1, float><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+            else k_fs_sweep_b<0, 0, float><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+        } else {
+            if (sv) k_fs_sweep_b<1, 1, float><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+            else k_fs_sweep_b<1, 0, float><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+        }
+    } else {
+        if (dir == 0) {
+            if (sv) k_fs_sweep_b<0, 1, double><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+            else k_fs_sweep_b<0, 0, double><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+        } else {
+            if (sv) k_fs_sweep_b<1, 1, double><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+            else k_fs_sweep_b<1, 0, double><<<grid, kTL, smem, s>>>(bl, half, sp.RBf, scratch, sp.RGf, roww);
+        }
+    }
+    hyd_kernel_launches_add(1);
+}
+
+void launch_coef_fsj_batch(const BatchRef& br, int ctas, int half, int mixed, cudaStream_t s) {
+    if (mixed) k_coef_fsj_b<0, float><<<ctas, 256, 0, s>>>(br, half);
+    else k_coef_fsj_b<0, double><<<ctas, 256, 0, s>>>(br, half);
+    hyd_kernel_launches_add(1);
+}
+
+// The batched sweeps may use all the shared memory the device allows (their row plans
+// are the largest member's).
+cudaError_t batch_sweep_setup() {
+    HydroSweepBFn* const hb[8] = {k_hydro_sweep_b<0, 0, double>, k_hydro_sweep_b<0, 1, double>,
+                                 k_hydro_sweep_b<1, 0, double>, k_hydro_sweep_b<1, 1, double>,
+                                 k_hydro_sweep_b<0, 0, float>,  k_hydro_sweep_b<0, 1, float>,
+                                 k_hydro_sweep_b<1, 0, float>,  k_hydro_sweep_b<1, 1, float>};
+    FsSweepBFn* const fb[8] = {k_fs_sweep_b<0, 0, double>, k_fs_sweep_b<0, 1, double>, k_fs_sweep_b<1, 0, double>,
+                              k_fs_sweep_b<1, 1, double>, k_fs_sweep_b<0, 0, float>,  k_fs_sweep_b<0, 1, float>,
+                              k_fs_sweep_b<1, 0, float>,  k_fs_sweep_b<1, 1, float>};
+    int lim;
+    cudaError_t e = allow_all(hb, 8, &lim);
+    if (e == cudaSuccess) e = allow_all(fb, 8, &lim);
+    return e;
 }

@@ -78,6 +78,8 @@ def load():
         "hyd_batch_member": (ctypes.c_int, [H, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
         "hyd_batch_step": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int]),
         "hyd_batch_destroy": (ctypes.c_int, [H]),
+        "hyd_batch_set_fused": (ctypes.c_int, [H, ctypes.c_int]),
+        "hyd_batch_fused_steps": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_longlong)]),
         "hyd_set_sweep_shape": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int]),
         "hyd_get_sweep_shape": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     }
@@ -373,6 +375,16 @@ class Batch:
 
     def step(self, n=1, sync=True):
         _check(self.lib.hyd_batch_step(self.b, int(n), 1 if sync else 0))
+
+    def set_fused(self, on=True):
+        """Batched launches: every phase of a batch step one launch for all members, the
+        step one CUDA graph (hyd_batch_set_fused)."""
+        _check(self.lib.hyd_batch_set_fused(self.b, 1 if on else 0))
+
+    def fused_steps(self):
+        n = ctypes.c_longlong()
+        _check(self.lib.hyd_batch_fused_steps(self.b, ctypes.byref(n)))
+        return n.value
 
     def synchronize(self):
         for s in self.members:

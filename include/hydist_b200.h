@@ -357,6 +357,22 @@ int hyd_batch_step(hyd_batch b, int nsteps, int sync);
 int hyd_batch_destroy(hyd_batch b);
 
 /*
+ * Batched launches (no reference counterpart): with hyd_batch_set_fused(b, 1) a batch
+ * step whose members all allow it runs every phase of the step as ONE launch for all
+ * members, each CTA working for one member (the line sweeps as one persistent launch over
+ * every member's lines, one CTA per SM), the whole batch step captured as one CUDA graph
+ * per step variant: about 20 launches per batch step instead of 20 per member.  The
+ * members must be initialised, at the same time with the same time step and sediment /
+ * bed schedule and precision, outside channel mode; a step that a member must take on its
+ * own (whole-grid passes after a field was set, a rescan of every line) runs per member
+ * and the batched form resumes after it.  Results are the same as the members' own steps
+ * (every line and cell is computed by the same code).  hyd_batch_fused_steps reports how
+ * many batch steps ran batched.
+ */
+int hyd_batch_set_fused(hyd_batch b, int on);
+int hyd_batch_fused_steps(hyd_batch b, long long* steps);
+
+/*
  * Launch shape of a handle's line sweeps: `ctas` persistent CTAs (0 or more than planned:
  * the planned number, one per SM), and with `wide` = 1 every line a warp's shared-memory
  * slice holds (up to 288 rows) swept by a warp rather than only lines of up to 96 rows.

@@ -226,3 +226,60 @@ def test_gpu_tuned_batch_vs_oracle(oracle_lib):
         for f in ("z", "u", "v", "FS"):
             e = rel_linf(got[i][f], o.get(f))
             assert e <= REL_TOL, "reach %d %s rel L-inf %.3e" % (i, f, e)
+
+
+def _batched_cases():
+    """Six reaches of config 3's generator (uneven sizes), sediment from t = 60 s and the
+    Exner update every 120 s, so that the batched steps cover every step variant."""
+    from hydist import cases
+    cs = cases.config3_cases(n=6, seed=23, nx_range=(128, 420), ny_range=(64, 220), hours=1.0, spinup_h=0.02)
+    for c in cs:
+        p = c.params.copy()
+        p.sediment_start = 60.0
+        p.bed_change_start = 120.0
+        c.params = p
+    return cs
+
+
+@pytest.mark.gpu
+def test_gpu_batched_launches_match_member_steps():
+    """The batched form (every phase one launch for all members, one graph per batch step)
+    against the same batch stepped member by member: every field, the mask and the segment
+    tables bit for bit after 300 steps (sediment from 60 s, two Exner updates)."""
+    from hydist.lib import Batch
+    cs = _batched_cases()
+    a = Batch(cs)
+    a.set_fused(True)
+    a.step(300)
+    assert a.fused_steps() >= 290  # the first step and the first sediment step run per member
+    b = Batch(cs)
+    b.step(300)
+    for k, (ma, mb) in enumerate(zip(a.members, b.members)):
+        assert ma.t == mb.t == 300.0
+        for f in ("z", "u", "v", "t_z", "t_u", "t_v", "FS", "dH", "H_moi", "Htdu", "Htdv", "khouot", "daui", "cuoii",
+                  "moci", "dauj", "cuoij", "mocj"):
+            assert np.array_equal(ma.get(f), mb.get(f), equal_nan=True), (k, f)
+        ba, bb = ma.mass_budget(), mb.mass_budget()
+        assert abs(ba["net_in"] - bb["net_in"]) <= 1e-9 * max(abs(bb["net_in"]), 1.0)
+    a.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_gpu_batched_launches_vs_oracle(oracle_lib):
+    """Two reaches of the batched form against the oracle within 1e-9."""
+    from helpers import REL_TOL, rel_linf
+    from hydist.lib import Batch
+    import oracle
+    cs = _batched_cases()[:2]
+    a = Batch(cs)
+    a.set_fused(True)
+    a.step(150)
+    for m, c in zip(a.members, cs):
+        o = oracle.OracleSim(c)
+        o.init()
+        o.step(150)
+        for f in ("z", "u", "v", "FS", "dH"):
+            e = rel_linf(m.get(f), o.get(f))
+            assert e <= REL_TOL, "%s rel L-inf %.3e" % (f, e)
+    a.close()
