@@ -103,9 +103,9 @@ __host__ __device__ __forceinline__ int row_warp_ctas(const DevGrid& g, int rows
 // arrays), and for one launch the first CTA of each member's share (bstart[m], with
 // bstart[nm] the launch's CTAs).  Every CTA of a batched launch works for one member.
 struct BatchRef {
-    const DevGrid* g;
-    const DevParams* p;
-    const int* bstart;
+    const DevGrid* __restrict__ g;  // read-only during a launch: loads of it need not be repeated
+    const DevParams* __restrict__ p;
+    const int* __restrict__ bstart;
     int nm;
 };
 
@@ -123,10 +123,10 @@ __device__ __forceinline__ int batch_member_of(const int* bstart, int nm, int b)
 // The lines of a batched sweep: every member's lines in one list (member m's at list
 // positions lstart[m] .. lstart[m + 1] - 1, its lines first[m] onwards).
 struct BatchLines {
-    const DevGrid* g;
-    const DevParams* p;
-    const int* lstart;
-    const int* first;
+    const DevGrid* __restrict__ g;
+    const DevParams* __restrict__ p;
+    const int* __restrict__ lstart;
+    const int* __restrict__ first;
     int nm;
     __device__ __forceinline__ int count() const;
     __device__ __forceinline__ void at(int li, int& m, int& line) const;

@@ -100,6 +100,7 @@ def generate(seeds, levels_per_reach, settle=1500, device=0, seed=11):
     rng = np.random.default_rng(seed)
     cs = [reach_case(s) for s in seeds]
     batch = Batch(cs, device=device)
+    batch.set_fused(True)  # the reaches share sizes and schedule: batched launches
     batch.step(int(round(0.25 * 3600)) + 300)  # the ramp, then a settling margin
     X, Y, W, R = [], [], [], []
     plans = [forcing_levels(rng, levels_per_reach) for _ in cs]
