@@ -139,6 +139,16 @@ struct HydSim {
     cudaGraphExec_t tgraph[8];
     std::vector<Mark> tmarks[8];
     std::vector<Mark>* mark_sink;  // where PhaseScope files its events (null: marks)
+    // hyd_checkpoint: a device copy of the arena and the column-major mask bytes, with the
+    // host-side step state at the time (allocated at the first save)
+    void* ck_arena;
+    int ck_valid;
+    double ck_t;
+    int ck_start, ck_end, ck_full, ck_force;
+    // hyd_steady_residual: snapshot of u, v, z (three pitched grid fields), per-CTA sums and
+    // the totals (allocated at the first call)
+    double* res_buf;
+    int res_valid;
 };
 
 static const char* kPhaseNames[] = {"boundary", "sweep_uz", "sweep_vz", "smooth", "explicit_v", "explicit_u",
@@ -316,6 +326,7 @@ DevParams make_dev_params(const HydCaseParams& P) {
     d.kenhhepng = P.kenhhepng;
     d.channel = (P.kenhhepd || P.kenhhepng) ? 1 : 0;
     d.bed_feedback = P.bed_feedback ? 1 : 0;
+    d.bed_fixed = P.bed_fixed > 0 ? P.bed_fixed : 0;
     d.morfac = P.morfac;
     d.bed_period = P.bed_period > 0 ? P.bed_period : P.bed_change_start;
     d.mixed = P.precision_mode == HYD_PRECISION_MIXED ? 1 : 0;
@@ -464,6 +475,8 @@ void hyd_params_default(HydCaseParams* p) {
 // Free what a handle holds (any of it may be missing on a failed create) and the handle.
 static void release(HydSim* s) {
     cudaFree(s->run_part);
+    cudaFree(s->ck_arena);
+    cudaFree(s->res_buf);
     cudaFree(s->sweep_scratch);
     cudaFree(s->fs_scratch);
     cudaFree(s->g.colT);
@@ -558,7 +571,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     // arena: grid fields (double and int), smoothing partners, tables, boundary arrays
     const size_t nrow = (size_t)N + 3;
     const size_t gbytes = nrow * s->pitch * sizeof(double);
-    const size_t ngrid = 28;  // double grid fields in kFieldTable + VISC, h0, dHc
+    const size_t ngrid = 29;  // double grid fields in kFieldTable + VISC, h0, dHc, dHinc
     const size_t nseg_rows = ((size_t)N + 3) * HYD_SEGL, nseg_cols = ((size_t)M + 3) * HYD_SEGL;
     auto a256 = [](size_t b) { return (b + 255) / 256 * 256; };
     size_t total = a256(gbytes) * (ngrid + 1 + 2) + a256(nrow * s->pitch * sizeof(int));
@@ -590,7 +603,7 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     double** gd[] = {&g.h,   &g.hsnham, &g.VISC,  &g.Fw,   &g.Tsxw,  &g.Tsyw,     &g.u,   &g.v,   &g.z,
                      &g.t_u, &g.t_v,    &g.t_z,   &g.Htdu, &g.Htdv,  &g.H_moi,    &g.htaiz, &g.htaiz_bd,
                      &g.Kx1, &g.Ky1,    &g.FS,    &g.tFS,  &g.VTH,   &g.Kx,       &g.Ky,  &g.Qbx, &g.Qby,
-                     &g.dH,  &g.h0,     &g.dHc};
+                     &g.dH,  &g.h0,     &g.dHc,    &g.dHinc};
     for (double** q : gd) *q = (double*)take(gbytes);
     s->scratch_u = (double*)take(gbytes);
     s->scratch_v = (double*)take(gbytes);
@@ -766,6 +779,25 @@ int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count) {
     } else {
         const size_t es = (f->kind >= 6) ? 8 : 4;
         CUDA_TRY(cudaMemcpyAsync(host, src, count * es, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HYD_OK;
+}
+
+int hyd_get_field_device(hyd_handle h, const char* name, void* dst, size_t count) {
+    if (!h || !name || !dst) return fail(HYD_EINVAL, "null argument");
+    const FieldDesc* f = find_field(name);
+    if (!f) return fail(HYD_EINVAL, std::string("unknown field ") + name);
+    if (count != field_count(h, f->kind)) return fail(HYD_EINVAL, std::string("wrong element count for ") + name);
+    CUDA_TRY(cudaSetDevice(h->device));
+    const void* src = member(h, f);
+    if (f->kind == 0 || f->kind == 1) {
+        const size_t es = f->kind == 0 ? 8 : 4;
+        CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)(h->M + 3) * es, src, (size_t)h->pitch * es, (size_t)(h->M + 3) * es,
+                                   (size_t)h->N + 3, cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        const size_t es = (f->kind >= 6) ? 8 : 4;
+        CUDA_TRY(cudaMemcpyAsync(dst, src, count * es, cudaMemcpyDeviceToDevice, h->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return HYD_OK;
@@ -1297,6 +1329,91 @@ int hyd_get_time(hyd_handle h, double* t) {
     return HYD_OK;
 }
 
+int hyd_set_time(hyd_handle h, double t) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_set_time");
+    if (!(t >= 0.0)) return fail(HYD_EINVAL, "t must be >= 0");
+    if ((int)(t / 3600) + 1 >= h->g.total_time) return fail(HYD_EINVAL, "boundary tables too short for t");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->t = t;
+    return set_clock(h, t);
+}
+
+int hyd_checkpoint(hyd_handle h, int restore) {
+    if (!h) return fail(HYD_EINVAL, "null handle");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_checkpoint");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t bytes = h->arena_bytes + h->g.colT_stride;  // arena, then the mask bytes
+    unsigned char* colB = h->g.colB;
+    if (!restore) {
+        if (!h->ck_arena) CUDA_TRY(cudaMalloc(&h->ck_arena, bytes));
+        char* dst = (char*)h->ck_arena;
+        CUDA_TRY(cudaMemcpyAsync(dst, h->arena, h->arena_bytes, cudaMemcpyDeviceToDevice, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(dst + h->arena_bytes, colB, h->g.colT_stride, cudaMemcpyDeviceToDevice, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->ck_t = h->t;
+        h->ck_start = h->start_idx;
+        h->ck_end = h->end_idx;
+        h->ck_full = h->full_pending;
+        h->ck_force = h->force_rescan;
+        h->ck_valid = 1;
+        return HYD_OK;
+    }
+    if (!h->ck_valid) return fail(HYD_ESTATE, "no checkpoint saved on this handle");
+    const char* src = (const char*)h->ck_arena;
+    CUDA_TRY(cudaMemcpyAsync(h->arena, src, h->arena_bytes, cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(colB, src + h->arena_bytes, h->g.colT_stride, cudaMemcpyDeviceToDevice, h->stream));
+    h->t = h->ck_t;
+    h->start_idx = h->ck_start;
+    h->end_idx = h->ck_end;
+    h->full_pending = h->ck_full;
+    h->force_rescan = h->ck_force;
+    h->epoch++;
+    return set_clock(h, h->t);  // synchronises the stream
+}
+
+int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n) {
+    if (!h || !out || n < 2) return fail(HYD_EINVAL, "need 2 output slots");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_steady_residual");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t field = (size_t)(h->N + 3) * h->pitch;
+    const int nb = 2 * 148;
+    if (!h->res_buf) {
+        CUDA_TRY(cudaMalloc(&h->res_buf, (3 * field + (size_t)nb * 4 + 4) * sizeof(double)));
+        h->res_valid = 0;
+    }
+    double *u0 = h->res_buf, *v0 = u0 + field, *z0 = v0 + field, *part = z0 + field, *tot = part + (size_t)nb * 4;
+    launch_steady_residual(h->g, u0, v0, z0, snapshot, part, nb, tot, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    double sums[4];
+    CUDA_TRY(cudaMemcpyAsync(sums, tot, sizeof sums, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (!h->res_valid) {
+        out[0] = out[1] = HUGE_VAL;
+    } else {
+        out[0] = sums[1] > 0 ? std::sqrt(sums[0] / sums[1]) : (sums[0] > 0 ? HUGE_VAL : 0.0);
+        out[1] = sums[3] > 0 ? std::sqrt(sums[2] / sums[3]) : (sums[2] > 0 ? HUGE_VAL : 0.0);
+    }
+    if (snapshot) h->res_valid = 1;
+    return HYD_OK;
+}
+
+int hyd_add_levels(hyd_handle h, const float* du, const float* dv, const float* dz, int i0, int j0, int rows,
+                   int cols, long long ld) {
+    if (!h || !du || !dv || !dz) return fail(HYD_EINVAL, "null argument");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_add_levels");
+    if (rows < 0 || cols < 0 || ld < cols || i0 < 0 || j0 < 0 || i0 + rows > h->N + 3 || j0 + cols > h->M + 3)
+        return fail(HYD_EINVAL, "rectangle outside the grid");
+    if (!rows || !cols) return HYD_OK;
+    CUDA_TRY(cudaSetDevice(h->device));
+    launch_add_levels(h->g, h->dp, du, dv, dz, i0, j0, rows, cols, ld, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->epoch++;
+    return HYD_OK;
+}
+
 int hyd_synchronize(hyd_handle h) {
     if (!h) return fail(HYD_EINVAL, "null handle");
     CUDA_TRY(cudaSetDevice(h->device));
@@ -1328,7 +1445,7 @@ int hyd_mass_balance(hyd_handle h, double* out, int n) {
 }
 
 int hyd_mass_budget(hyd_handle h, double* out, int n) {
-    if (!h || !out || n < HYD_BUDGET_SLOTS) return fail(HYD_EINVAL, "need HYD_BUDGET_SLOTS output slots");
+    if (!h || !out || n < 10) return fail(HYD_EINVAL, "need at least 10 output slots");
     if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_mass_budget");
     CUDA_TRY(cudaSetDevice(h->device));
     double b[kBudSlots];
@@ -1348,6 +1465,7 @@ int hyd_mass_budget(hyd_handle h, double* out, int n) {
     out[3] = b[kBudOpen] * area;
     out[4] = b[kBudClose] * area;
     out[5] = b[kBudBed] * area;
+    if (n > 10) out[10] = b[kBudJump] * area;
     return HYD_OK;
 }
 
@@ -1698,7 +1816,7 @@ int fused_build(HydBatch* b) {
         const int N = s->N, M = s->M;
         const int rw = row_warp_ctas(g0, N + 3);
         counts[BP_CB].push_back(((N - 1) * 32 + 255) / 256 + 1);
-        counts[BP_SM_BUD].push_back(rw + 4);
+        counts[BP_SM_BUD].push_back(rw + 4 * kEdgeCtas);
         counts[BP_SM].push_back(rw);
         counts[BP_SM_FSB].push_back(rw + 1);
         counts[BP_EV].push_back(N - 1);

@@ -30,6 +30,7 @@ struct DevParams {
     // morphodynamic feedback (off: the reference's step): each Exner update's bed change,
     // morfac x bed_period / (1 - Dorong) x rate, is applied to h and the depths re-derived
     int bed_feedback;
+    int bed_fixed;  // the bed stays fixed within bed_fixed cells of the grid's edges
     double morfac, bed_period;  // bed_period: the Exner period in s (bed_change_start if unset)
     // precision_mode MIXED: coefficient assembly, the line sweeps, the explicit momentum and
     // the sediment transport in FP32; the water level's continuity update, the mass sums
@@ -46,6 +47,7 @@ struct DevGrid {
     double *Htdu, *Htdv, *H_moi, *htaiz, *htaiz_bd, *Kx1, *Ky1;
     double *FS, *tFS, *VTH, *Kx, *Ky, *Qbx, *Qby, *dH;
     double *h0, *dHc;  // feedback: h at set-up (h = h0 + dH) and dH's Kahan compensation
+    double* dHinc;     // feedback: an update's unfiltered bed change (NaN where none)
     int* khouot;
     // segment tables (reference layout)
     int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
@@ -88,9 +90,13 @@ struct DevGrid {
     double* budget;
 };
 
-// Slots of DevGrid::budget.  Edge e = 0 up, 1 down, 2 left, 3 right.
+// Slots of DevGrid::budget.  Edge e = 0 up, 1 down, 2 left, 3 right.  An edge's half-step
+// volumes are summed by kEdgeCtas CTAs, each writing its (in, out) partial to kBudPart +
+// 2 (e kEdgeCtas + c); the last CTA of the edge to finish (counted in the unsigned words
+// at kBudCount) adds the partials in CTA order to the edge's Kahan sums.
 constexpr int kBudNet = 0, kBudNetC = 4, kBudIn = 8, kBudInC = 12, kBudOut = 16, kBudOutC = 20;
-constexpr int kBudOpen = 24, kBudClose = 25, kBudBed = 26, kBudSlots = 32;
+constexpr int kBudOpen = 24, kBudClose = 25, kBudBed = 26, kBudJump = 27;
+constexpr int kEdgeCtas = 8, kBudPart = 32, kBudCount = kBudPart + 8 * kEdgeCtas, kBudSlots = kBudCount + 4;
 
 __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { atomicOr(g.status, bit); }
 
@@ -378,6 +384,14 @@ void launch_update_fs(const DevGrid& g, int full, cudaStream_t s);
 void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, cudaStream_t s);
 // feedback: h0 = h (the bed the applied changes start from), dH and its compensation zeroed
 void launch_bed_reset(const DevGrid& g, cudaStream_t s);
+// hyd_add_levels: increments added to z, u, v on the wet cells of rows i0.. x columns j0..,
+// the depths and face depths re-derived around them
+void launch_add_levels(const DevGrid& g, const DevParams& p, const float* du, const float* dv, const float* dz,
+                       int i0, int j0, int rows, int cols, long long ld, cudaStream_t s);
+// hyd_steady_residual: per-CTA sums over the wet cells (4 per CTA), then the totals in
+// out[0..3] added in CTA order; snapshot: u0, v0, z0 = u, v, z afterwards
+void launch_steady_residual(const DevGrid& g, double* u0, double* v0, double* z0, int snapshot, double* part,
+                            int nblocks, double* out, cudaStream_t s);
 long long hyd_kernel_launches_add(long long n);
 
 // Batched launches (k_grid.cu, k_sweep.cu): one launch for every member of a batch, each

@@ -566,26 +566,30 @@ struct RowLane {
     }
 };
 
-// The open-edge part of the water budget for one half-step, by one CTA for edge e (0 up:
-// faces j = M, 1 down: faces j = 1, 2 left: faces i = 1, 3 right: faces i = N), run right
-// after the half-step's sweep.  A sweep's continuity row of cell (i, j) reads
+// The open-edge part of the water budget for one half-step, by kEdgeCtas CTAs for edge e
+// (0 up: faces j = M, 1 down: faces j = 1, 2 left: faces i = 1, 3 right: faces i = N), run
+// right after the half-step's sweep.  A sweep's continuity row of cell (i, j) reads
 //   z' = z - dT/(2 dX) (Htdu[i,j] u[i,j] - Htdu[i-1,j] u[i-1,j])
 //          - dT/(2 dY) (Htdv[i,j] v[i,j] - Htdv[i,j-1] v[i,j-1])
 // (_uzSolver/_vzSolver_calculate_preindex, UVZSolver_multithread.cu:345-349, 402-406),
 // with the implicit component new (t_u in the UZ sweep, t_v in the VZ sweep) and the other
 // as it stood; summed over the cells the sweep solved, the inner faces cancel and the
-// volume change is the flux through the domain's edge faces.  So the CTA adds, for every
-// edge cell the sweep solved (the cell lies in a segment of the sweep's lines), its edge
-// face's volume flux over the half-step, dT/2 x face depth x velocity x face width, signed
-// into the domain, to the edge's Kahan sums (one writer per edge: the CTA's thread 0).
+// volume change is the flux through the domain's edge faces.  So for every edge cell the
+// sweep solved (the cell lies in a segment of the sweep's lines) its edge face's volume
+// flux over the half-step, dT/2 x face depth x velocity x face width, signed into the
+// domain, is added to the edge's inflow or outflow.  CTA c of the edge takes the cells
+// k = 2 + c blockDim + t (stride kEdgeCtas blockDim) and writes its partial sums; the last
+// CTA to finish adds the kEdgeCtas partials in CTA order to the edge's Kahan sums, so the
+// result does not depend on the CTAs' order.
 // half1: the UZ sweep (x faces t_u, y faces v); otherwise the VZ sweep (x faces u, y faces
 // t_v).
-__device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int e) {
+__device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int e, int c) {
     __shared__ double s_in[32], s_out[32];
+    __shared__ int s_last;
     const int N = g.N, M = g.M, P = g.P;
     const int n = e >= 2 ? M : N;  // edge cells j = 2..M (left/right) or i = 2..N (up/down)
     double vin = 0.0, vout = 0.0;
-    for (int k = 2 + threadIdx.x; k <= n; k += blockDim.x) {
+    for (int k = 2 + c * blockDim.x + threadIdx.x; k <= n; k += kEdgeCtas * blockDim.x) {
         int i, j, fp;
         double sgn;
         if (e == 0) { i = k; j = M; fp = i * P + M; sgn = -1.0; }
@@ -613,27 +617,44 @@ __device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int
         s_out[w] = vout;
     }
     __syncthreads();
+    double* B = g.budget;
+    unsigned* count = reinterpret_cast<unsigned*>(B + kBudCount) + e;
     if (threadIdx.x == 0) {
         double a = 0.0, b = 0.0;
         for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
             a += s_in[q];
             b += s_out[q];
         }
-        double* B = g.budget;
-        auto kahan = [&](int sum, int comp, double x) {
-            const double y = x - B[comp];
-            const double t = B[sum] + y;
-            B[comp] = (t - B[sum]) - y;
-            B[sum] = t;
-        };
-        kahan(kBudNet + e, kBudNetC + e, a - b);
-        kahan(kBudIn + e, kBudInC + e, a);
-        kahan(kBudOut + e, kBudOutC + e, b);
+        B[kBudPart + 2 * (e * kEdgeCtas + c)] = a;
+        B[kBudPart + 2 * (e * kEdgeCtas + c) + 1] = b;
+        __threadfence();
+        s_last = atomicAdd(count, 1u) == (unsigned)(kEdgeCtas - 1);
     }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    const volatile double* V = B;
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < kEdgeCtas; q++) {
+        a += V[kBudPart + 2 * (e * kEdgeCtas + q)];
+        b += V[kBudPart + 2 * (e * kEdgeCtas + q) + 1];
+    }
+    auto kahan = [&](int sum, int comp, double x) {
+        const double y = x - B[comp];
+        const double t = B[sum] + y;
+        B[comp] = (t - B[sum]) - y;
+        B[sum] = t;
+    };
+    kahan(kBudNet + e, kBudNetC + e, a - b);
+    kahan(kBudIn + e, kBudInC + e, a);
+    kahan(kBudOut + e, kBudOutC + e, b);
+    *count = 0u;  // ready for the next half-step (stream order separates the launches)
 }
 
-// The edge budget alone (after a whole-grid smoothing pass): CTA e takes edge e.
-__global__ void k_edge_budget(DevGrid g, DevParams p, int half1) { edge_budget(g, p, half1, blockIdx.x); }
+// The edge budget alone (after a whole-grid smoothing pass): kEdgeCtas CTAs per edge.
+__global__ void k_edge_budget(DevGrid g, DevParams p, int half1) {
+    edge_budget(g, p, half1, blockIdx.x / kEdgeCtas, blockIdx.x % kEdgeCtas);
+}
 
 // BYTES: also write the column reset bytes (the smoothing of u right before the column
 // resets; H_moi is not read in between).
@@ -647,13 +668,14 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
 // FSB: one more CTA (the last) applies the concentration part of the second half-step's
 // boundary (kBndFS), when the velocity/level part ran before the first half-step's
 // sediment sweep had finished.
-// BUD: four more CTAs (the last) add the half-step's open-edge volumes to the budget
-// (edge_budget; the smoothing of the swept velocity, isU = the UZ sweep's half-step).
+// BUD: 4 kEdgeCtas more CTAs (the last) add the half-step's open-edge volumes to the
+// budget (edge_budget; the smoothing of the swept velocity, isU = the UZ sweep's half-step).
 template <int BYTES, int FSB, int BUD>
 __device__ __forceinline__ void smooth_span_body(const DevGrid& g, const DevParams& p, int isU,
                                                  double* __restrict__ out, int bx, int gx) {
-    if (BUD && bx >= gx - 4) {
-        edge_budget(g, p, isU, bx - (gx - 4));
+    if (BUD && bx >= gx - 4 * kEdgeCtas) {
+        const int q = bx - (gx - 4 * kEdgeCtas);
+        edge_budget(g, p, isU, q / kEdgeCtas, q % kEdgeCtas);
         return;
     }
     if (FSB && bx == gx - 1) {
@@ -1707,6 +1729,7 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
     const int i = blockIdx.y * blockDim.y + threadIdx.y + startidx;
     const int N = g.N, M = g.M, width = g.P;
     if (i >= endidx || j > M) return;
+    if (FB) g.dHinc[i * width + j] = __longlong_as_double(0x7ff8000000000000LL);  // not computed
     int first = 0, last = 0;
     find_seg_v(g, i, j, first, last);
     if (last - first < 2 || j < first || j > last) return;
@@ -1756,12 +1779,47 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
         g.dH[pos] += p.dT / (1 - p.Dorong) * (S + tH);
         return;
     }
-    // the period's change, limited to kBedLimit of the water depth and to kBedCap metres
-    // (the explicit Exner step with central and one-sided bed-load differences is unstable
-    // for large morphological steps; the limit keeps each update's bed change small
-    // against the depth it acts on)
+    // the period's raw change, filtered and applied by k_bed_apply
     double x = p.morfac * p.bed_period / (1 - p.Dorong) * (S + tH);
     if (!isfinite(x)) x = 0.0;
+    g.dHinc[pos] = x;
+}
+
+// The fed-back bed change of one update.  The explicit Exner rate from central bed-load and
+// diffusion differences carries a grid-scale (2 dx) oscillation, which a morphological step
+// of many minutes turns into a checkerboard bed that the hydraulics do not survive; so the
+// raw change is filtered by the 3 x 3 binomial kernel (weights 1 2 1 x 1 2 1, renormalised
+// over the computed neighbours in rows startidx..endidx-1, columns 2..M), which removes the
+// 2 dx mode exactly and keeps smooth changes, then limited to kBedLimit of the water depth
+// and kBedCap metres (the step stays small against the depth it acts on), added to dH as a
+// Kahan sum and applied to the bed, h = h0 + dH.  Cells within bed_fixed cells of the
+// grid's edges (the inlet and outlet sections of the open boundaries) keep their bed.
+// Indexing as k_bedload.
+__global__ void k_bed_apply(DevGrid g, DevParams p, int startidx, int endidx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y + startidx;
+    const int N = g.N, M = g.M, width = g.P;
+    if (i >= endidx || j > M) return;
+    const int F = p.bed_fixed;
+    if (i < 2 + F || i > N - F || j < 2 + F || j > M - F) return;
+    const int pos = i * width + j;
+    const double* __restrict__ inc = g.dHinc;
+    if (!isfinite(inc[pos])) return;
+    double num = 0.0, den = 0.0;
+    for (int di = -1; di <= 1; di++) {
+        const int ii = i + di;
+        if (ii < startidx || ii >= endidx) continue;
+        for (int dj = -1; dj <= 1; dj++) {
+            const int jj = j + dj;
+            if (jj < 2 || jj > M) continue;
+            const double v = inc[ii * width + jj];
+            if (!isfinite(v)) continue;
+            const double w = (di == 0 ? 2.0 : 1.0) * (dj == 0 ? 2.0 : 1.0);
+            num += w * v;
+            den += w;
+        }
+    }
+    double x = num / den;
     const double lim = fmin(kBedLimit * g.H_moi[pos], kBedCap);
     x = fmin(fmax(x, -lim), lim);
     const double y = x - g.dHc[pos];
@@ -1804,6 +1862,97 @@ __global__ void k_bed_derive(DevGrid g, DevParams p) {
     }
     for (int o = 16; o > 0; o >>= 1) dv += __shfl_down_sync(0xffffffffu, dv, o);
     if ((threadIdx.x & 31) == 0 && dv != 0.0) atomicAdd(&g.budget[kBudBed], dv);
+}
+
+// ------------------------------------------------------- quasi-steady support
+
+// hyd_add_levels, pass 1: the increments of cell (i0 + r, j0 + c) (element r ld + c of each
+// array) added to z, u, v and their swept copies on the wet interior cells, H_moi = htaiz +
+// z (update_h_moi, support_funcs.cu:60-73); a cell whose new depth would not exceed H_TINH
+// keeps its level.  The water added goes to the budget's kBudJump slot (depth units).
+__global__ void k_add_levels(DevGrid g, DevParams p, const float* __restrict__ du, const float* __restrict__ dv,
+                             const float* __restrict__ dz, int i0, int j0, int rows, int cols, long long ld) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    double dvol = 0.0;
+    const int i = i0 + r, j = j0 + c;
+    if (r < rows && c < cols && i >= 2 && i <= g.N && j >= 2 && j <= g.M) {
+        const int pos = i * g.P + j;
+        const long long q = (long long)r * ld + c;
+        if (g.khouot[pos] == 0) {
+            const double zn = g.z[pos] + (double)dz[q];
+            if (g.htaiz[pos] + zn > p.H_TINH) {
+                dvol = zn - g.z[pos];
+                g.z[pos] = zn;
+                g.t_z[pos] = zn;
+                g.H_moi[pos] = g.htaiz[pos] + zn;
+            }
+            const double un = g.u[pos] + (double)du[q], vn = g.v[pos] + (double)dv[q];
+            g.u[pos] = un;
+            g.t_u[pos] = un;
+            g.v[pos] = vn;
+            g.t_v[pos] = vn;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) dvol += __shfl_down_sync(0xffffffffu, dvol, o);
+    if ((threadIdx.x & 31) == 0 && dvol != 0.0) atomicAdd(&g.budget[kBudJump], dvol);
+}
+
+// hyd_add_levels, pass 2: Htuongdoi (support_funcs.cu:338-354) over the rectangle grown by
+// one cell, for the new levels.
+__global__ void k_add_levels_faces(DevGrid g, int i0, int j0, int rows, int cols) {
+    const int i = i0 - 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int j = j0 - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 1 || j < 1 || i > i0 + rows || j > j0 + cols) return;
+    post_cell(g, 0, i, j);
+}
+
+// hyd_steady_residual: sums over the wet cells of 2..N x 2..M of (u - u0)^2 + (v - v0)^2,
+// u^2 + v^2, (z - z0)^2 and H_moi^2, per CTA; with snapshot, the cell's u, v, z are copied
+// to u0, v0, z0 after they are read.
+__global__ void k_resid_partial(DevGrid g, double* __restrict__ u0, double* __restrict__ v0, double* __restrict__ z0,
+                                int snapshot, double* __restrict__ part) {
+    __shared__ double sh[4][256];
+    const int tid = threadIdx.x;
+    double a = 0, b = 0, c = 0, d = 0;
+    const int W = g.M - 1;
+    const long long ncell = (long long)(g.N - 1) * W;
+    for (long long q = (long long)blockIdx.x * blockDim.x + tid; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+        const int i = 2 + (int)(q / W), j = 2 + (int)(q % W);
+        const int gp = i * g.P + j;
+        if (g.khouot[gp] != 0) continue;
+        const double u = g.u[gp], v = g.v[gp], z = g.z[gp], H = g.H_moi[gp];
+        const double du = u - u0[gp], dv = v - v0[gp], dz = z - z0[gp];
+        a += du * du + dv * dv;
+        b += u * u + v * v;
+        c += dz * dz;
+        d += H * H;
+        if (snapshot) {
+            u0[gp] = u;
+            v0[gp] = v;
+            z0[gp] = z;
+        }
+    }
+    sh[0][tid] = a;
+    sh[1][tid] = b;
+    sh[2][tid] = c;
+    sh[3][tid] = d;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (tid < w)
+            for (int k = 0; k < 4; k++) sh[k][tid] += sh[k][tid + w];
+        __syncthreads();
+    }
+    if (tid == 0)
+        for (int k = 0; k < 4; k++) part[blockIdx.x * 4 + k] = sh[k][0];
+}
+
+__global__ void k_resid_final(const double* __restrict__ part, int nblocks, double* __restrict__ out) {
+    if (threadIdx.x != 0) return;
+    double acc[4] = {0, 0, 0, 0};
+    for (int b = 0; b < nblocks; b++)
+        for (int k = 0; k < 4; k++) acc[k] += part[b * 4 + k];
+    for (int k = 0; k < 4; k++) out[k] = acc[k];
 }
 
 // Feedback set-up: h0 = h - dH (so that h = h0 + dH holds now), no compensation yet.
@@ -1975,14 +2124,14 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
         if (bytes) k_smooth<1><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         else k_smooth<0><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         if (budget) {  // the smoothing reads the swept velocity and writes elsewhere
-            k_edge_budget<<<4, 256, 0, s>>>(g, p, isU);
+            k_edge_budget<<<4 * kEdgeCtas, 256, 0, s>>>(g, p, isU);
             hyd_kernel_launches_add(1);
         }
     } else {
         const int nb = row_warps_blocks(g, g.N + 3);
         if (bytes && fs_bnd) k_smooth_span<1, 1, 0><<<nb + 1, 256, 0, s>>>(g, p, isU, out);
         else if (bytes) k_smooth_span<1, 0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
-        else if (budget) k_smooth_span<0, 0, 1><<<nb + 4, 256, 0, s>>>(g, p, isU, out);
+        else if (budget) k_smooth_span<0, 0, 1><<<nb + 4 * kEdgeCtas, 256, 0, s>>>(g, p, isU, out);
         else k_smooth_span<0, 0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
     }
     hyd_kernel_launches_add(1);
@@ -2105,16 +2254,35 @@ void launch_bed(const DevGrid& g, const DevParams& p, int startidx, int endidx, 
         return;
     }
     k_qb<1><<<grid2d(g.M - 1, g.N - 1, b), b, 0, s>>>(g, p);
-    if (endidx > startidx) k_bedload<1><<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
+    if (endidx > startidx) {
+        k_bedload<1><<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
+        k_bed_apply<<<grid2d(g.M - 1, endidx - startidx, b), b, 0, s>>>(g, p, startidx, endidx);
+        hyd_kernel_launches_add(2);
+    }
     k_bed_derive<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p);
     k_preprocess<<<1, 32, 0, s>>>(g, p);
-    hyd_kernel_launches_add(4);
+    hyd_kernel_launches_add(3);
 }
 
 void launch_bed_reset(const DevGrid& g, cudaStream_t s) {
     const dim3 b(32, 8);
     k_bed_reset<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g);
     hyd_kernel_launches_add(1);
+}
+
+void launch_add_levels(const DevGrid& g, const DevParams& p, const float* du, const float* dv, const float* dz,
+                       int i0, int j0, int rows, int cols, long long ld, cudaStream_t s) {
+    const dim3 b(32, 8);
+    k_add_levels<<<grid2d(cols, rows, b), b, 0, s>>>(g, p, du, dv, dz, i0, j0, rows, cols, ld);
+    k_add_levels_faces<<<grid2d(cols + 2, rows + 2, b), b, 0, s>>>(g, i0, j0, rows, cols);
+    hyd_kernel_launches_add(2);
+}
+
+void launch_steady_residual(const DevGrid& g, double* u0, double* v0, double* z0, int snapshot, double* part,
+                            int nblocks, double* out, cudaStream_t s) {
+    k_resid_partial<<<nblocks, 256, 0, s>>>(g, u0, v0, z0, snapshot, part);
+    k_resid_final<<<1, 32, 0, s>>>(part, nblocks, out);
+    hyd_kernel_launches_add(2);
 }
 
 // Up to kPutDoubles values carried in the launch's parameters into dst[0..n): a small

@@ -251,7 +251,8 @@ def meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=6.0, seed=20261203, amp=12
           np.full((1, total_time), cc_in), np.zeros((1, total_time))]
     nsteps = int(round((hours + spinup_h) * 3600 / dT))
     return Case(name, N, M, p, fields, bt, tables, cc, total_time, 0.0, nsteps,
-                notes={"wss": settling_velocity(p), "seed": seed, "spinup_steps": int(round(spinup_h * 3600 / dT))})
+                notes={"wss": settling_velocity(p), "seed": seed, "spinup_steps": int(round(spinup_h * 3600 / dT)),
+                       "end_cells": end_cells})
 
 
 def islands_case(N=48, M=36, dX=5.0, dT=1.0, seed=7, hours=1.0, sediment_start=0.0,
@@ -329,16 +330,85 @@ def config4_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE, hours=24.0, dT=1.0, end_
     and under that inflow the scheme's stage-edge velocity at the channel's bank cell
     grows without bound: the oracle reaches NaN by t = 1100 s (at dt = 0.5 s by
     t = 1600 s).  With the delay the run stays finite (checked for 4 h at dt = 1 s and
-    dt = 0.5 s).  The morphological factor 10 of this workload is not a
-    library parameter: the Exner step accumulates dH without feeding it back into the
-    bed (the reference's behaviour), so the factor scales the reported bed change only
-    and is kept in notes["morfac"]."""
+    dt = 0.5 s).  The morphological factor 10 of this workload is kept in
+    notes["morfac"]; the parity runs leave the bed unchanged (the reference's behaviour),
+    and the morphodynamic runs set bed_feedback with morfac = notes["morfac"]."""
     c = meander_case(N=4096, M=2048, dX=2.5, dT=dT, hours=hours, spinup_h=spinup_h, amp=240.0,
                      wavelength=3000.0, width=300.0, noise_len=100.0,
                      Q0=2000.0 * q_scale * 2.0, Q1=3500.0 * q_scale * 2.0, end_cells=end_cells,
                      tide_delay_h=spinup_h if tide_delay_h is None else tide_delay_h,
                      name="config4_large_meander")
     c.notes["morfac"] = 10.0
+    return c
+
+
+MORPHO_TOE = 1.0  # Pa: erosion threshold of the morphodynamic workloads' sediment
+
+
+def with_feedback(case, morfac=1.0, bed_period=600.0, fixed=None):
+    """The case made morphodynamic: the bed change fed back (bed_feedback) every
+    `bed_period` s at `morfac`, with the sediment set up for runs of days.
+
+    The parity cases' sediment (constant.cuh's erosion threshold Toe = 0.15 Pa and a
+    sediment-laden inflow of 0.2 kg/m3) is a parity set-up, not a long-run one: fed back,
+    its Exner rate moves the bed by centimetres per 10-min update (up to the 5 cm cap per
+    update within a few updates near the inflow, where the inflowing load settles), and
+    within two hours of config 4 the bed cuts lines into more than 20 wet segments.  So the
+    morphodynamic runs take a clear-water inflow (concentration 0), an erosion threshold of
+    MORPHO_TOE, and a fixed bed within `fixed` cells of the edges (default: twice the
+    meander's rectangular end sections, i.e. the inlet and outlet sections and their
+    blends).  On config 2 this gives mean bed changes of about 0.1 mm per update."""
+    p = case.params.copy()
+    p.bed_feedback = 1
+    p.morfac = float(morfac)
+    p.bed_period = float(bed_period)
+    p.Toe = MORPHO_TOE
+    p.bed_fixed = int(fixed if fixed is not None else 2 * case.notes.get("end_cells", 8))
+    case.params = p
+    for e in range(4):
+        case.cc[e] = np.zeros_like(case.cc[e])
+    return case
+
+
+CONFIG5_Q_MEAN, CONFIG5_Q_AMP = 687.5, 187.5  # config 2's scaled 500-875 m3/s range
+CONFIG5_Q_PERIOD_H, CONFIG5_STAGE_PERIOD_H, CONFIG5_STAGE_AMP = 240.0, 354.4, 0.3
+
+
+def config5_case(seed=20261205, days=30.0, spinup_h=1.0, bed_period=600.0, morfac=1.0, q_phase=None,
+                 stage_phase=None, feedback=True, name="config5_morpho"):
+    """Morphodynamic reach for the surrogate-assisted runs: the config-2 meander (1048 x 980,
+    5 m cells, dt = 1 s, the generator with this seed: bed noise and roughness), `days` of
+    hydraulics + sediment with the bed change fed back every `bed_period` s (bed_feedback,
+    morfac), sediment from 0.5 h and bed change from 1 h as in config 2.
+
+    Forcing (none is stated for this workload): over a 30-day run the hydraulics follow
+    the slow variations, so the upstream discharge is config 2's scaled 500-875 m3/s range
+    as a sine of 10-day period and the downstream stage a 0.3 m sine of the 14.77-day
+    spring-neap period (the 12.42 h tide is averaged out), both with phases drawn from the
+    seed unless given; the first `spinup_h` hours ramp the discharge linearly from rest.
+    Hourly tables, linearly interpolated like the reference's.  The sediment is
+    with_feedback's (clear-water inflow, erosion threshold MORPHO_TOE, a fixed bed in the
+    inlet and outlet sections); feedback=False keeps that sediment with the bed unchanged."""
+    rng = np.random.default_rng(seed + 1)
+    qph = rng.uniform(0, 2 * math.pi) if q_phase is None else q_phase
+    sph = rng.uniform(0, 2 * math.pi) if stage_phase is None else stage_phase
+    hours = days * 24.0
+    c = meander_case(N=1048, M=980, dX=5.0, dT=1.0, hours=hours, spinup_h=spinup_h, seed=seed,
+                     Q0=CONFIG5_Q_MEAN, Q1=CONFIG5_Q_MEAN, tide_amp=0.0, name=name)
+    th = np.arange(c.total_time, dtype=np.float64)
+    tr = np.maximum(th - spinup_h, 0.0)
+    q = CONFIG5_Q_MEAN + CONFIG5_Q_AMP * np.sin(2 * math.pi * tr / CONFIG5_Q_PERIOD_H + qph)
+    q = np.where(th < spinup_h, q[int(math.ceil(spinup_h))] * th / spinup_h, q) if spinup_h > 0 else q
+    zs = CONFIG5_STAGE_AMP * np.sin(2 * math.pi * tr / CONFIG5_STAGE_PERIOD_H + sph)
+    zs = np.where(th < spinup_h, 0.0, zs) if spinup_h > 0 else zs
+    c.tables[EDGE_LEFT] = q[None, :].copy()
+    c.tables[EDGE_RIGHT] = zs[None, :].copy()
+    with_feedback(c, morfac=morfac, bed_period=bed_period)
+    if not feedback:
+        p = c.params.copy()
+        p.bed_feedback = 0
+        c.params = p
+    c.notes.update({"q_phase": qph, "stage_phase": sph, "days": days})
     return c
 
 

@@ -62,6 +62,12 @@ def load():
         "hyd_synchronize": (ctypes.c_int, [H]),
         "hyd_mass_balance": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_int]),
         "hyd_mass_budget": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_int]),
+        "hyd_checkpoint": (ctypes.c_int, [H, ctypes.c_int]),
+        "hyd_get_field_device": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]),
+        "hyd_set_time": (ctypes.c_int, [H, ctypes.c_double]),
+        "hyd_steady_residual": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
+        "hyd_add_levels": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong]),
         "hyd_state_size": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_size_t)]),
         "hyd_get_state": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_size_t]),
         "hyd_set_state": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_size_t]),
@@ -284,10 +290,48 @@ class Simulation:
         through the edges, volumes of the cells opened and closed by the wet/dry resets, the
         volume fed-back bed changes added to the depths, and the net per edge (up, down,
         left, right)."""
-        out = np.zeros(10)
-        _check(self.lib.hyd_mass_budget(self.h, out.ctypes.data, 10))
+        out = np.zeros(11)
+        _check(self.lib.hyd_mass_budget(self.h, out.ctypes.data, 11))
         return {"net_in": out[0], "gross_in": out[1], "gross_out": out[2], "opened": out[3], "closed": out[4],
-                "bed": out[5], "edge_net": out[6:10].copy()}
+                "bed": out[5], "edge_net": out[6:10].copy(), "added": out[10]}
+
+    # quasi-steady support: device checkpoint, time, steady residual, level increments
+    def checkpoint(self):
+        """Save the whole device state in the handle's device slot (hyd_checkpoint)."""
+        _check(self.lib.hyd_checkpoint(self.h, 0))
+
+    def restore(self):
+        """Restore the state and time of the last checkpoint()."""
+        _check(self.lib.hyd_checkpoint(self.h, 1))
+
+    def get_device(self, name, out):
+        """Copy field `name` into the device tensor `out` (its packed shape and dtype)."""
+        shape, dtype = field_shape(name, self.N, self.M)
+        if tuple(out.shape) != shape or not out.is_contiguous() or not out.is_cuda or \
+                out.element_size() != np.dtype(dtype).itemsize:
+            raise ValueError("get_device needs a contiguous device tensor of shape %s" % (shape,))
+        _check(self.lib.hyd_get_field_device(self.h, name.encode(), out.data_ptr(), int(np.prod(shape))))
+        return out
+
+    def set_time(self, t):
+        _check(self.lib.hyd_set_time(self.h, float(t)))
+
+    def steady_residual(self, snapshot=True):
+        """(momentum, continuity) relative change since the last snapshot (hyd_steady_residual):
+        ||d(u, v)|| / ||(u, v)|| and ||dz|| / ||H|| over the wet cells; inf before the first."""
+        out = np.zeros(2)
+        _check(self.lib.hyd_steady_residual(self.h, 1 if snapshot else 0, out.ctypes.data, 2))
+        return float(out[0]), float(out[1])
+
+    def add_levels(self, du, dv, dz, i0, j0):
+        """Add FP32 device tensors du, dv, dz (rows x cols, contiguous) to u, v, z on the wet
+        cells of the rectangle starting at grid cell (i0, j0) (hyd_add_levels)."""
+        rows, cols = du.shape
+        for a in (du, dv, dz):
+            if tuple(a.shape) != (rows, cols) or not a.is_contiguous() or not a.is_cuda or a.element_size() != 4:
+                raise ValueError("add_levels takes three contiguous FP32 device tensors of one shape")
+        _check(self.lib.hyd_add_levels(self.h, du.data_ptr(), dv.data_ptr(), dz.data_ptr(), int(i0), int(j0), rows,
+                                       cols, cols))
 
     def get_state(self):
         n = ctypes.c_size_t()

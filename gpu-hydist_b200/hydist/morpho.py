@@ -1,0 +1,258 @@
+"""Quasi-steady morphodynamics with the surrogate's jump: the fast form of a long
+morphodynamic run (the 30-day, 10-minute bed-update workload).
+
+The plain run steps the hydraulics and the sediment every dT and feeds the bed change
+back every bed period (bed_feedback).  Between two bed updates the flow of a slowly
+forced reach stays close to the equilibrium of the current bed and forcing, and the bed
+update only reads the state at the period's end.  The quasi-steady form therefore
+replaces the period's steps by a jump to that equilibrium and a few plain steps:
+
+  1. checkpoint the device state (hyd_checkpoint);
+  2. the jump: the surrogate's predicted change of (u, v, z) from the last period's
+     (bed, forcing) to this one's, added on the wet cells (hyd_add_levels), or no jump
+     (the method without the network: the previous state is the warm start);
+  3. the clock moved to `warm` steps before the period's end (hyd_set_time) and plain
+     ADI steps taken, the steady residual (hyd_steady_residual: relative velocity change
+     per step, and level change per depth) read after each;
+  4. once both residuals are below the gate, the clock is moved to the last step of the
+     period and that step taken, which makes the period's bed update on the accepted
+     state; if the residual has not fallen below the gate within `warm` - 1 steps, the
+     checkpoint is restored and the period stepped plainly (the fallback).
+
+No reference counterpart (the reference steps every dT, Engine.py:144-366, and never
+feeds the bed back).  The surrogate's data are plain-solver snapshots of config-5-style
+reaches (other seeds of the same generator) along their slowly varying forcing.
+"""
+import math
+import time
+
+import numpy as np
+
+from . import cases
+from . import surrogate as S
+from .lib import Batch, Simulation
+
+H_REF, N_REF, Q_REF, STAGE_REF, DZ_REF = 8.0, 0.025, 700.0, 0.3, 0.1
+
+
+def forcing_at(case, t):
+    """(upstream discharge, downstream stage) of the case's hourly tables at time t
+    (linear between the hourly knots, as the library interpolates them)."""
+    k = int(t // 3600)
+    w = (t - 3600.0 * k) / 3600.0
+    q = case.tables[cases.EDGE_LEFT][0]
+    z = case.tables[cases.EDGE_RIGHT][0]
+    return float(q[k] + w * (q[k + 1] - q[k])), float(z[k] + w * (z[k + 1] - z[k]))
+
+
+def reach_crop(case, margin=6):
+    """Rows 1..N and the columns of the channel band (every column holding a bed cell below
+    the datum in any row, widened by `margin`): (i0, rows, j0, cols) in grid indices."""
+    N, M = case.N, case.M
+    h = case.fields["h"][1:N + 1, 1:M + 1] - case.params.NANGDAY
+    cols = np.nonzero((h > 0.0).any(axis=0))[0]
+    j0 = max(1, int(cols.min()) + 1 - margin)
+    j1 = min(M, int(cols.max()) + 1 + margin)
+    return 1, N, j0, j1 - j0 + 1
+
+
+class Features:
+    """The network's input of one reach on its crop, built on the device: bed depth,
+    roughness, upstream Q, downstream stage and the along-flow and cross coordinates
+    (normalised), padded to the first layer's 16 channels (BF16)."""
+
+    def __init__(self, case, crop, device):
+        import torch
+        self.crop = crop
+        self.dev = device
+        i0, rows, j0, cols = crop
+        N, M = case.N, case.M
+        self.nangday = case.params.NANGDAY
+        self.hbuf = torch.empty((N + 3, M + 3), dtype=torch.float64, device=device)
+        n = torch.from_numpy(np.ascontiguousarray(case.fields["hsnham"][i0:i0 + rows, j0:j0 + cols]))
+        self.static = torch.zeros((rows, cols, 3), dtype=torch.float32)
+        self.static[..., 0] = ((n - N_REF) / 0.01).float()
+        self.static[..., 1] = torch.linspace(0.0, 1.0, rows)[:, None]
+        self.static[..., 2] = torch.linspace(0.0, 1.0, cols)[None, :]
+        self.static = self.static.to(device)
+
+    def build(self, sim, Q, stage, out=None):
+        """(rows, cols, 16) BF16 on the device; written into `out` when given."""
+        import torch
+        i0, rows, j0, cols = self.crop
+        sim.get_device("h", self.hbuf)
+        h = (self.hbuf[i0:i0 + rows, j0:j0 + cols] - self.nangday) / H_REF
+        x = out if out is not None else torch.empty((rows, cols, 16), dtype=torch.bfloat16, device=self.dev)
+        x.zero_()
+        x[..., 0] = h.to(torch.bfloat16)
+        x[..., 1] = self.static[..., 0].to(torch.bfloat16)
+        x[..., 2] = Q / Q_REF
+        x[..., 3] = stage / STAGE_REF
+        x[..., 4] = self.static[..., 1].to(torch.bfloat16)
+        x[..., 5] = self.static[..., 2].to(torch.bfloat16)
+        return x
+
+
+class Targets:
+    """The state on the crop as network targets, on the device: u, v, (z - stage) / DZ_REF
+    and the wet mask."""
+
+    def __init__(self, case, crop, device):
+        import torch
+        N, M = case.N, case.M
+        self.crop = crop
+        self.buf = {f: torch.empty((N + 3, M + 3), dtype=torch.float64, device=device) for f in ("u", "v", "z")}
+        self.kh = torch.empty((N + 3, M + 3), dtype=torch.int32, device=device)
+
+    def build(self, sim, stage, y_out, w_out):
+        i0, rows, j0, cols = self.crop
+        for f, b in self.buf.items():
+            sim.get_device(f, b)
+        sim.get_device("khouot", self.kh)
+        sl = (slice(i0, i0 + rows), slice(j0, j0 + cols))
+        y_out[..., 0] = self.buf["u"][sl]
+        y_out[..., 1] = self.buf["v"][sl]
+        y_out[..., 2] = (self.buf["z"][sl] - stage) / DZ_REF
+        w_out.copy_((self.kh[sl] == 0).float())
+
+
+def generate(seeds, snapshots, every=600, settle_h=2.0, device=0, crop=None, log=None):
+    """Plain-solver quasi-steady snapshots of config-5-style reaches (config5_case with
+    each seed, the bed not fed back): the reaches run side by side as one batch (batched
+    launches), spun up for `settle_h` hours, then a snapshot of every reach every `every`
+    seconds, `snapshots` per reach.  Returns device tensors X (S, rows, cols, 16) BF16,
+    Y (S, rows, cols, 3) FP32, W (S, rows, cols) FP32 and the crop."""
+    import torch
+    dev = torch.device("cuda", device)
+    days = (settle_h * 3600 + snapshots * every) / 86400.0 + 0.1
+    cs = [cases.config5_case(seed=s, days=days, feedback=False) for s in seeds]
+    crop = crop or reach_crop(cs[0])
+    i0, rows, j0, cols = crop
+    n = len(cs) * snapshots
+    X = torch.empty((n, rows, cols, 16), dtype=torch.bfloat16, device=dev)
+    Y = torch.empty((n, rows, cols, 3), dtype=torch.float32, device=dev)
+    W = torch.empty((n, rows, cols), dtype=torch.float32, device=dev)
+    batch = Batch(cs, device=device)
+    batch.set_fused(True)
+    feats = [Features(c, crop, dev) for c in cs]
+    tgts = [Targets(c, crop, dev) for c in cs]
+    batch.step(int(round(settle_h * 3600)))
+    k = 0
+    t0 = time.perf_counter()
+    for s in range(snapshots):
+        batch.step(every)
+        for m, c, f, g in zip(batch.members, cs, feats, tgts):
+            Q, st = forcing_at(c, m.t)
+            f.build(m, Q, st, out=X[k])
+            g.build(m, st, Y[k], W[k])
+            k += 1
+        if log and s % max(1, snapshots // 5) == 0:
+            log("snapshot %d/%d, %.1f s" % (s + 1, snapshots, time.perf_counter() - t0))
+    batch.close()
+    return X, Y, W, crop
+
+
+def train(net, X, Y, W, iters=1500, batch=8, lr=2e-3, seed=0, log_every=0):
+    """Minibatch Adam on device tensors (as from generate), the forward and backward passes
+    on the tensor-core kernels.  Returns the loss of every iteration."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    losses = []
+    for it in range(iters):
+        idx = torch.randint(0, X.shape[0], (batch,), generator=g).to(X.device)
+        xb = X.index_select(0, idx).contiguous()
+        yb = Y.index_select(0, idx).contiguous()
+        wb = W.index_select(0, idx).contiguous()
+        pred, saved = net.forward(xb)
+        loss, dy = net.loss_grad(pred, yb, wb)
+        gw, gb = net.backward(saved, dy)
+        net.adam(gw + gb, lr=lr * 0.5 * (1 + math.cos(math.pi * it / iters)))
+        losses.append(loss)
+        if log_every and it % log_every == 0:
+            print("train %d loss %.4e" % (it, float(loss.item())))
+    net.check_errors()
+    return [float(l.item()) for l in losses]
+
+
+class SurrogateJump:
+    """The jump of the quasi-steady form: the network's predicted equilibrium for the
+    current (bed, forcing) minus its prediction for the previous period's, as FP32
+    increments of u, v, z on the crop."""
+
+    def __init__(self, net, case, crop):
+        self.net = net
+        self.crop = crop
+        self.feat = Features(case, crop, net.dev)
+        self.prev = None
+
+    def predict(self, sim, Q, stage):
+        x = self.feat.build(sim, Q, stage)[None]
+        y, _ = self.net.forward(x)
+        y = y[0]
+        return y[..., 0], y[..., 1], y[..., 2] * DZ_REF + stage
+
+    def increments(self, sim, Q, stage):
+        """(du, dv, dz) contiguous FP32 device tensors, or None on the first call; the
+        prediction is kept as the next call's reference."""
+        cur = self.predict(sim, Q, stage)
+        prev, self.prev = self.prev, cur
+        if prev is None:
+            return None
+        return tuple((a - b).contiguous() for a, b in zip(cur, prev))
+
+
+class QuasiSteady:
+    """The quasi-steady morphodynamic loop on one Simulation (see the module docstring).
+
+    period(): advance one bed period; returns (accepted, plain steps taken).  Counters:
+    accepted, fallbacks, steps."""
+
+    def __init__(self, sim, case, warm=20, gate=1e-4, jump=None):
+        self.sim = sim
+        self.case = case
+        self.warm = int(warm)
+        self.gate = float(gate)
+        self.jump = jump
+        self.period_s = float(case.params.bed_period)
+        self.accepted = 0
+        self.fallbacks = 0
+        self.steps = 0
+        self.residuals = []
+
+    def period(self):
+        sim = self.sim
+        dT = sim.params.dT
+        t0 = sim.t
+        t_end = t0 + self.period_s
+        nper = int(round(self.period_s / dT))
+        sim.checkpoint()
+        if self.jump is not None:
+            Q, st = forcing_at(self.case, t_end)
+            inc = self.jump.increments(sim, Q, st)
+            if inc is not None:
+                i0, _, j0, _ = self.jump.crop
+                sim.add_levels(*inc, i0, j0)
+        sim.set_time(t_end - self.warm * dT)
+        sim.steady_residual(snapshot=True)
+        r = (math.inf, math.inf)
+        for k in range(1, self.warm):
+            sim.step(1)
+            r = sim.steady_residual(snapshot=True)
+            if max(r) < self.gate:
+                sim.set_time(t_end - dT)
+                sim.step(1)  # the period's last step: the bed update on the accepted state
+                self.accepted += 1
+                self.steps += k + 1
+                self.residuals.append(max(r))
+                return True, k + 1
+        # not steady within the warm steps: back to the checkpoint, the period stepped plainly
+        sim.restore()
+        sim.step(nper)
+        self.fallbacks += 1
+        self.steps += self.warm - 1 + nper
+        self.residuals.append(max(r))
+        return False, self.warm - 1 + nper
+
+    def run_until(self, t_stop):
+        while self.sim.t + self.period_s <= t_stop + 1e-9:
+            self.period()

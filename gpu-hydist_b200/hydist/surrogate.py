@@ -228,11 +228,33 @@ class Surrogate:
             self.b[l].copy_(d["b"][l].to(self.dev))
 
 
-def reference_forward(w, b, x):
+def _bf16_rounding():
+    """An autograd function rounding its input to BF16 in the forward pass (out=True: the
+    value passes unrounded) and its gradient to BF16 in the backward pass: the points where
+    the kernels store BF16 (each layer's activation; each layer's pre-activation gradient,
+    which the data-gradient kernel writes after the ReLU mask; the loss gradient)."""
+    import torch
+
+    class RoundBF16(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, x, out):
+            return x if out else x.to(torch.bfloat16).float()
+
+        @staticmethod
+        def backward(ctx, g):
+            return g.to(torch.bfloat16).float(), None
+
+    return RoundBF16.apply
+
+
+def reference_forward(w, b, x, bf16=False):
     """The same network in plain PyTorch FP32 (any device; used on the CPU as the gradient
-    check): x [B][H][W][4] FP32, w[l] [cout][9][cin], b[l] [cout].  Returns [B][H][W][3]."""
+    check): x [B][H][W][IN_CH] FP32, w[l] [cout][9][cin], b[l] [cout].  Returns
+    [B][H][W][3].  bf16: round the activations and the gradients to BF16 where the kernels
+    store them, so that only the FP32 accumulation order differs from the GPU passes."""
     import torch
     import torch.nn.functional as F
+    rnd = _bf16_rounding() if bf16 else None
     B, H, W, _ = x.shape
     cur = x.permute(0, 3, 1, 2)
     for l, (mode, cin, cout, relu) in enumerate(LAYERS):
@@ -247,4 +269,6 @@ def reference_forward(w, b, x):
                                      output_padding=(H - (2 * hi - 1), W - (2 * wi - 1)))
         if relu:
             cur = F.relu(cur)
+        if rnd is not None:
+            cur = rnd(cur, l == len(LAYERS) - 1)
     return cur.permute(0, 2, 3, 1)

@@ -82,7 +82,8 @@ typedef struct HydCaseParams {
     double bed_period;       /* s; Exner update every bed_period s from bed_change_start on;
                                 0 = every bed_change_start s (Engine.py:364) */
     int bed_feedback;        /* 1 = apply each bed change to h and re-derive the depths */
-    int reserved1;
+    int bed_fixed;           /* the bed stays fixed within this many cells of the grid's edges
+                                (the open boundaries' inlet and outlet sections) */
 } HydCaseParams;
 
 /* precision_mode values */
@@ -147,6 +148,11 @@ int hyd_get_field(hyd_handle h, const char* name, void* host, size_t count);
  * synchronously, Engine.py:377-468).
  */
 int hyd_get_field_async(hyd_handle h, const char* name, void* host, size_t count);
+
+/* hyd_get_field into a DEVICE buffer of the handle's device (the same packed layout and
+ * count): a device-to-device copy on the handle's stream, synchronous.  For callers that
+ * keep their own device work (e.g. a network's input) beside the simulation. */
+int hyd_get_field_device(hyd_handle h, const char* name, void* dst, size_t count);
 int hyd_wait_fields(hyd_handle h);
 
 /*
@@ -273,11 +279,12 @@ int hyd_mass_balance(hyd_handle h, double* out, int n);
  *   out[5] water volume the fed-back bed changes added to the wet cells' depths (m^3;
  *          0 without bed_feedback)
  *   out[6..9] net volume in through the up, down, left, right edge (m^3)
+ *   out[10] water volume hyd_add_levels added (m^3; written when n >= 11)
  * Closure: between two times, the change of hyd_mass_balance's out[0] equals
- * d(out[0]) + d(out[3]) - d(out[4]) + d(out[5]).  n must be >= HYD_BUDGET_SLOTS.  No
- * reference counterpart.
+ * d(out[0]) + d(out[3]) - d(out[4]) + d(out[5]) + d(out[10]).  n must be >= 10
+ * (HYD_BUDGET_SLOTS for every slot).  No reference counterpart.
  */
-#define HYD_BUDGET_SLOTS 10
+#define HYD_BUDGET_SLOTS 11
 int hyd_mass_budget(hyd_handle h, double* out, int n);
 
 /*
@@ -310,6 +317,40 @@ int hyd_mass_balance_noalloc(hyd_handle h, int nblocks, double* out, int n);
 int hyd_state_size(hyd_handle h, size_t* bytes);
 int hyd_get_state(hyd_handle h, void* buf, size_t bytes);
 int hyd_set_state(hyd_handle h, const void* buf, size_t bytes);
+
+/*
+ * Quasi-steady support (no reference counterpart; the reference steps every dT through
+ * Engine.py:144-366).  A morphodynamic run that needs only the hydraulics' equilibrium
+ * between two bed updates can reach it by fewer steps from a predicted state, judged by
+ * the plain step: these calls keep that loop on the device.
+ *
+ * hyd_checkpoint(h, 0) saves the whole device state (every field, the mask, the segment
+ * tables, the spans, the water budget, the clock) into one device buffer of the handle
+ * (allocated at the first save; the arena's size); hyd_checkpoint(h, 1) restores it, with
+ * the time.  One slot per handle; a save replaces the previous one.
+ *
+ * hyd_set_time(h, t) moves the simulation time (the boundary tables' clock and the
+ * sediment, bed-update and hourly table schedules) to t without touching any field.
+ *
+ * hyd_steady_residual(h, snapshot, out, n >= 2) compares the state with the snapshot
+ * taken at the previous call with snapshot = 1, over the wet cells of [2,N] x [2,M]:
+ *   out[0] = ||(u, v) - (u0, v0)||_2 / ||(u, v)||_2   (momentum: relative velocity change)
+ *   out[1] = ||z - z0||_2 / ||H_moi||_2               (continuity: level change / depth)
+ * each an FP64 sum added in a fixed order; HUGE_VAL before the first snapshot.  With
+ * snapshot = 1 the current u, v, z become the snapshot.  Synchronous.
+ *
+ * hyd_add_levels(h, du, dv, dz, i0, j0, rows, cols, ld) adds DEVICE arrays of FP32
+ * increments (element r*ld + c belongs to cell (i0 + r, j0 + c) of the (N+3) x (M+3)
+ * grid) to u, v and z on the wet cells of [2,N] x [2,M] (a cell whose depth would fall to
+ * H_TINH or below keeps its level), and re-derives H_moi and the face depths Htdu, Htdv
+ * there (update_h_moi, support_funcs.cu:60-73; Htuongdoi 338-354).  The water it adds is
+ * kept in hyd_mass_budget's out[10].  Synchronous.
+ */
+int hyd_checkpoint(hyd_handle h, int restore);
+int hyd_set_time(hyd_handle h, double t);
+int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n);
+int hyd_add_levels(hyd_handle h, const float* du, const float* dv, const float* dz, int i0, int j0, int rows,
+                   int cols, long long ld);
 
 /* Device status bits accumulated since creation (waits for the stream):
  *   1 = a line had more than 20 wet segments (the reference overflows its tables),

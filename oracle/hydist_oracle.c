@@ -47,6 +47,7 @@ struct OraSim {
     double *h, *hsnham, *VISCOIDX, *Fw, *Tsxw, *Tsyw, *u, *v, *z, *t_u, *t_v, *t_z, *Htdu, *Htdv,
         *H_moi, *htaiz, *htaiz_bd, *Kx1, *Ky1, *FS, *tFS, *VTH, *Kx, *Ky, *Qbx, *Qby, *dH;
     double *h0, *dHc; /* morphodynamic feedback: h = h0 + dH, dH's Kahan compensation */
+    double* dHinc;    /* feedback: the update's unfiltered bed change (NaN where none) */
     int* khouot;
     int *daui, *cuoii, *moci, *dauj, *cuoij, *mocj;
     double *ubt, *ubp, *vbt, *vbd, *hi;
@@ -113,7 +114,7 @@ OraSim* ora_create(const HydCaseParams* p, int N, int M) {
                          &s->u,     &s->v,      &s->z,        &s->t_u,   &s->t_v,      &s->t_z,
                          &s->Htdu,  &s->Htdv,   &s->H_moi,    &s->htaiz, &s->htaiz_bd, &s->Kx1,
                          &s->Ky1,   &s->FS,     &s->tFS,      &s->VTH,   &s->Kx,       &s->Ky,
-                         &s->Qbx,   &s->Qby,    &s->dH,       &s->h0,    &s->dHc};
+                         &s->Qbx,   &s->Qby,    &s->dH,       &s->h0,    &s->dHc,      &s->dHinc};
     for (size_t k = 0; k < sizeof(fields) / sizeof(fields[0]); k++) {
         *fields[k] = (double*)ora_alloc(s, nf, sizeof(double), G);
         if (!*fields[k]) goto fail;
@@ -1602,9 +1603,9 @@ static void k_calculate_qb(OraSim* s) {
 
 /* BedLoad + _bed_load (Sediment_Transport.cu:630-639, 416-506): rows startidx..endidx-1.
  * With the library's bed_feedback option (no reference counterpart): the upwind test reads
- * t_u[pos] > 0 (quirk Q4), the increment is morfac * bed_period / (1 - Dorong) * rate
- * (0 if not finite) limited to BED_LIMIT of the depth and BED_CAP metres, added to dH as a Kahan sum and
- * applied to the bed, h = h0 + dH. */
+ * t_u[pos] > 0 (quirk Q4) and the update's raw bed change, morfac * bed_period / (1 - Dorong)
+ * * rate (0 if not finite), is stored in dHinc (NaN at the cells not computed) for
+ * bed_feedback_apply. */
 static void k_bedload(OraSim* s, int startidx, int endidx) {
     const int N = s->N, M = s->M, width = s->W;
     const HydCaseParams* P = &s->P;
@@ -1613,6 +1614,10 @@ static void k_bedload(OraSim* s, int startidx, int endidx) {
                  *Qby = s->Qby;
     const int* khouot = s->khouot;
     const double dX2 = P->dX2, dY2 = P->dY2, dXbp = P->dXbp, dYbp = P->dYbp;
+    if (P->bed_feedback) {
+        for (int i = startidx; i < endidx; i++)
+            for (int j = 2; j <= M; j++) s->dHinc[i * width + j] = NAN;
+    }
 #pragma omp parallel for schedule(static)
     for (int i = startidx; i < endidx; i++)
         for (int j = 2; j <= M + 2; j++) {
@@ -1666,20 +1671,56 @@ static void k_bedload(OraSim* s, int startidx, int endidx) {
                 s->dH[pos] += P->dT / (1 - P->Dorong) * (S + tH);
                 continue;
             }
-            {
+            if (j <= M) {
                 const double period = P->bed_period > 0 ? P->bed_period : P->bed_change_start;
                 double x = P->morfac * period / (1 - P->Dorong) * (S + tH);
                 if (!isfinite(x)) x = 0.0;
-                {
-                    const double lim = fmin(BED_LIMIT * H_moi[pos], BED_CAP);
-                    x = fmin(fmax(x, -lim), lim);
-                }
-                const double y = x - s->dHc[pos];
-                const double sum = s->dH[pos] + y;
-                s->dHc[pos] = (sum - s->dH[pos]) - y;
-                s->dH[pos] = sum;
-                s->h[pos] = s->h0[pos] + sum;
+                s->dHinc[pos] = x;
             }
+        }
+}
+
+/* The fed-back bed change of one update (no reference counterpart).  The explicit Exner
+ * rate from central bed-load and diffusion differences carries a grid-scale (2 dx)
+ * oscillation, which a morphological step of many minutes turns into a checkerboard bed
+ * that the hydraulics do not survive; so the raw change is filtered by the 3 x 3 binomial
+ * kernel (weights 1 2 1 x 1 2 1, renormalised over the computed neighbours in rows
+ * startidx..endidx-1, columns 2..M), which removes the 2 dx mode exactly and keeps smooth
+ * changes, then limited to BED_LIMIT of the depth and BED_CAP metres, added to dH as a
+ * Kahan sum and applied to the bed, h = h0 + dH.  Cells within bed_fixed cells of the
+ * grid's edges keep their bed. */
+static void bed_feedback_apply(OraSim* s, int startidx, int endidx) {
+    const int N = s->N, M = s->M, width = s->W;
+    const int F = s->P.bed_fixed > 0 ? s->P.bed_fixed : 0;
+    const double* inc = s->dHinc;
+#pragma omp parallel for schedule(static)
+    for (int i = startidx; i < endidx; i++)
+        for (int j = 2; j <= M; j++) {
+            const int pos = i * width + j;
+            if (i < 2 + F || i > N - F || j < 2 + F || j > M - F) continue;
+            if (!isfinite(inc[pos])) continue;
+            double num = 0.0, den = 0.0;
+            for (int di = -1; di <= 1; di++) {
+                const int ii = i + di;
+                if (ii < startidx || ii >= endidx) continue;
+                for (int dj = -1; dj <= 1; dj++) {
+                    const int jj = j + dj;
+                    if (jj < 2 || jj > M) continue;
+                    const double v = inc[ii * width + jj];
+                    if (!isfinite(v)) continue;
+                    const double w = (di == 0 ? 2.0 : 1.0) * (dj == 0 ? 2.0 : 1.0);
+                    num += w * v;
+                    den += w;
+                }
+            }
+            double x = num / den;
+            const double lim = fmin(BED_LIMIT * s->H_moi[pos], BED_CAP);
+            x = fmin(fmax(x, -lim), lim);
+            const double y = x - s->dHc[pos];
+            const double sum = s->dH[pos] + y;
+            s->dHc[pos] = (sum - s->dH[pos]) - y;
+            s->dH[pos] = sum;
+            s->h[pos] = s->h0[pos] + sum;
         }
 }
 
@@ -1802,7 +1843,10 @@ static void full_step(OraSim* s) {
         if (bed) {
             k_calculate_qb(s);
             k_bedload(s, start_idx, end_idx);
-            if (P->bed_feedback) bed_feedback_derive(s);
+            if (P->bed_feedback) {
+                bed_feedback_apply(s, start_idx, end_idx);
+                bed_feedback_derive(s);
+            }
         }
     }
     s->start_idx = start_idx;

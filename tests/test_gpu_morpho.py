@@ -4,9 +4,10 @@ over the large reach's stated 24 hours.
 The reference accumulates dH and never applies it (Sediment_Transport.cu:504, quirk Q5);
 with bed_feedback = 0 the library reproduces that (every parity test runs that way).
 With bed_feedback = 1 each Exner update (every bed_period s from bed_change_start on)
-adds morfac x bed_period / (1 - Dorong) x rate, limited to a tenth of the local depth and
-to 0.05 m, to dH as a Kahan sum and sets h = h0 + dH, and the set-up's depth-derived
-fields are re-derived.  The oracle restates
+takes the change morfac x bed_period / (1 - Dorong) x rate, filters it by the 3 x 3
+binomial kernel (which removes the grid-scale oscillation of the explicit rate), limits it
+to a tenth of the local depth and to 0.05 m, adds it to dH as a Kahan sum and sets
+h = h0 + dH, and the set-up's depth-derived fields are re-derived.  The oracle restates
 the same option, so the GPU is held to the parity tolerance against it.
 """
 import time
@@ -28,13 +29,16 @@ def _feedback(case, morfac, period):
     return case
 
 
-def test_feedback_matches_oracle(oracle_lib):
+@pytest.mark.parametrize("fixed", [0, 5])
+def test_feedback_matches_oracle(oracle_lib, fixed):
     """Islands reach with sediment from t = 0 and a fed-back bed update every 10 s at
-    morfac 10: 240 steps (23 updates) on the GPU and on the oracle."""
+    morfac 10: 240 steps (23 updates) on the GPU and on the oracle; with fixed = 5 the bed
+    of the cells within 5 cells of the edges stays put."""
     import oracle
     from hydist import cases
     from hydist.lib import Simulation
     c = _feedback(cases.islands_case(), 10.0, 10.0)
+    c.params.bed_fixed = fixed
     n = 240
     sim = Simulation.from_case(c)
     h_start = sim.get("h")
@@ -53,6 +57,11 @@ def test_feedback_matches_oracle(oracle_lib):
     assert np.isfinite(dH).all()
     assert np.abs(h - h_start).max() > 0
     assert np.allclose(h - h_start, dH, rtol=0, atol=1e-12)
+    if fixed:
+        N, M = c.N, c.M
+        band = np.ones_like(dH, dtype=bool)
+        band[2 + fixed:N - fixed + 1, 2 + fixed:M - fixed + 1] = False
+        assert np.array_equal(h[band], h_start[band])
     sim.close()
 
 
@@ -72,11 +81,11 @@ def test_feedback_off_keeps_the_bed():
 def test_config4_24h_morfac10():
     """The 4096 x 2048 reach over its stated 24 h (86 400 steps of 1 s) with hydraulics,
     sediment and the bed change fed back at morphological factor 10, the bed updated every
-    10 min: finite throughout, the water budget closed with the bed's share, and the
-    simulated hours per wall second reported."""
+    10 min (cases.with_feedback's long-run sediment): finite throughout, the water budget
+    closed with the bed's share, and the simulated hours per wall second reported."""
     from hydist import cases
     from hydist.lib import Simulation
-    c = _feedback(cases.config4_case(), 10.0, 600.0)
+    c = cases.with_feedback(cases.config4_case(), morfac=10.0, bed_period=600.0)
     sim = Simulation.from_case(c)
     sim.step(1)
     v0 = sim.mass_balance()["volume"]

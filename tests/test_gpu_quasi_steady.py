@@ -1,0 +1,107 @@
+"""The quasi-steady support entry points (GPU): device checkpoint and restore, the clock,
+the steady residual and the level increments, each against host-side arithmetic on the
+fields read back."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _case():
+    from hydist import cases
+    return cases.islands_case()
+
+
+def test_checkpoint_restore_is_exact():
+    """A restored checkpoint gives back every field, the time and the budget, and the run
+    continues bit for bit as it did from the saved state."""
+    from hydist.lib import Simulation
+    sim = Simulation.from_case(_case())
+    sim.step(30)
+    st0 = sim.get_state()
+    b0 = sim.mass_budget()
+    sim.checkpoint()
+    sim.step(25)
+    a = {f: sim.get(f) for f in ("z", "u", "v", "FS", "khouot")}
+    t_a = sim.t
+    sim.restore()
+    assert sim.t == 30 * sim.params.dT
+    assert np.array_equal(sim.get_state(), st0)
+    b1 = sim.mass_budget()
+    assert all(np.array_equal(np.asarray(b0[k]), np.asarray(b1[k])) for k in b0)
+    sim.step(25)
+    assert sim.t == t_a
+    for f, v in a.items():
+        assert np.array_equal(sim.get(f), v), f
+    sim.close()
+
+
+def test_steady_residual_matches_host():
+    from hydist.lib import Simulation
+    sim = Simulation.from_case(_case())
+    sim.step(20)
+    r = sim.steady_residual(snapshot=True)
+    assert r == (np.inf, np.inf) or (np.isinf(r[0]) and np.isinf(r[1]))
+    N, M = sim.N, sim.M
+    u0, v0, z0 = sim.get("u"), sim.get("v"), sim.get("z")
+    sim.step(1)
+    u, v, z, H, kh = sim.get("u"), sim.get("v"), sim.get("z"), sim.get("H_moi"), sim.get("khouot")
+    r = sim.steady_residual(snapshot=False)
+    w = np.zeros_like(kh, dtype=bool)
+    w[2:N + 1, 2:M + 1] = kh[2:N + 1, 2:M + 1] == 0
+    mom = np.sqrt(((u - u0)[w] ** 2 + (v - v0)[w] ** 2).sum() / (u[w] ** 2 + v[w] ** 2).sum())
+    con = np.sqrt(((z - z0)[w] ** 2).sum() / (H[w] ** 2).sum())
+    assert abs(r[0] - mom) <= 1e-12 * mom and abs(r[1] - con) <= 1e-12 * con, (r, mom, con)
+    # without a snapshot the reference state stays: the same residual again
+    assert sim.steady_residual(snapshot=False) == r
+    sim.close()
+
+
+def test_add_levels_and_set_time():
+    import torch
+    from hydist.lib import Simulation
+    sim = Simulation.from_case(_case())
+    sim.step(20)
+    N, M = sim.N, sim.M
+    before = {f: sim.get(f) for f in ("z", "u", "v", "t_z", "H_moi", "htaiz", "khouot", "h", "Htdu", "Htdv")}
+    b0 = sim.mass_budget()["added"]
+    i0, j0, rows, cols = 3, 4, N - 6, M - 8
+    g = torch.Generator().manual_seed(0)
+    du = (torch.randn((rows, cols), generator=g) * 0.01).float().cuda()
+    dv = (torch.randn((rows, cols), generator=g) * 0.01).float().cuda()
+    dz = (torch.randn((rows, cols), generator=g) * 0.005).float().cuda()
+    sim.add_levels(du, dv, dz, i0, j0)
+    after = {f: sim.get(f) for f in before}
+    kh = before["khouot"]
+    sl = (slice(i0, i0 + rows), slice(j0, j0 + cols))
+    wet = np.zeros_like(kh, dtype=bool)
+    wet[sl] = kh[sl] == 0
+    wet[:2, :] = False
+    wet[:, :2] = False
+    wet[N + 1:, :] = False
+    wet[:, M + 1:] = False
+    dz_full = np.zeros_like(before["z"])
+    dz_full[sl] = dz.double().cpu().numpy()
+    dz_full[~wet] = 0
+    keep = wet & (before["htaiz"] + (before["z"] + dz_full) <= sim.params.H_TINH)
+    dz_full[keep] = 0
+    assert np.array_equal(after["z"], before["z"] + dz_full)
+    assert np.array_equal(after["t_z"][wet], after["z"][wet])
+    assert np.array_equal(after["H_moi"][wet], (before["htaiz"] + after["z"])[wet])
+    du_full = np.zeros_like(before["u"])
+    du_full[sl] = du.double().cpu().numpy()
+    assert np.array_equal(after["u"][wet], (before["u"] + du_full)[wet])
+    assert np.array_equal(after["u"][~wet], before["u"][~wet])
+    # face depths of the changed rows (Htuongdoi)
+    h, z = after["h"], after["z"]
+    i, j = i0 + 2, j0 + 2
+    assert after["Htdu"][i, j] == (h[i, j - 1] + h[i, j] + z[i + 1, j] + z[i, j]) * 0.5
+    added = sim.mass_budget()["added"] - b0
+    area = sim.params.dX * sim.params.dY
+    assert abs(added - dz_full[wet].sum() * area) <= 1e-9 * max(1.0, abs(added))
+    # the clock: a step after set_time ends at the new time + dT
+    sim.set_time(100.0)
+    sim.step(1)
+    assert sim.t == 100.0 + sim.params.dT
+    assert np.isfinite(sim.get("z")).all()
+    sim.close()

@@ -5,8 +5,10 @@ network), then a short training run whose loss falls.
 
 Tolerances: the kernels take BF16 operands and accumulate in FP32, so a layer's output
 matches the FP32 convolution of the same rounded operands to the BF16 rounding of its
-own output (relative 1e-2 of the output's range); the network's gradients, whose
-activations are BF16 between layers, match the CPU's FP32 gradients to 5e-2 relative L2.
+own output (relative 1e-2 of the output's range).  The network's gradients match a CPU
+autograd that rounds to BF16 where the kernels store BF16 to 2e-2 relative L2 (the FP32
+accumulation order, and the BF16 roundings it flips, differ), and the CPU's FP32-only
+gradients to 1e-1 (the BF16 storage's own error).
 """
 import numpy as np
 import pytest
@@ -14,7 +16,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 LAYER_TOL = 1e-2
-GRAD_TOL = 5e-2
+BF16_REF_TOL = 2e-2
+GRAD_TOL = 1e-1
 
 
 def _rel(a, b):
@@ -102,9 +105,12 @@ def test_conv_wgrad_matches_torch(mode):
 
 
 def test_network_gradients_match_cpu():
-    """Loss and every weight and bias gradient of the six-layer network against PyTorch FP32
-    autograd of the same network on the CPU (the BF16 input and weights as the kernels see
-    them)."""
+    """Loss and every weight and bias gradient of the six-layer network against PyTorch
+    autograd of the same network on the CPU, from the BF16 input and weights the kernels
+    see: (1) with the activations and gradients rounded to BF16 where the kernels store
+    them (only the FP32 accumulation order differs: BF16_REF_TOL), (2) in FP32 throughout
+    (the BF16 storage's own error, largest in the first layer, whose gradient has passed
+    five BF16 data-gradient layers: GRAD_TOL)."""
     import torch
     from hydist import surrogate as S
     torch.manual_seed(3)
@@ -120,19 +126,20 @@ def test_network_gradients_match_cpu():
     gw, gb = net.backward(saved, dy)
     torch.cuda.synchronize()
     net.check_errors()
-    # the CPU reference: FP32 autograd on the BF16-rounded input and weights
-    wc = [w.detach().cpu().to(torch.bfloat16).float().requires_grad_(True) for w in net.w]
-    bc = [b.detach().cpu().clone().requires_grad_(True) for b in net.b]
-    out = S.reference_forward(wc, bc, xg.float().cpu()[..., :S.IN_CH])
-    ref_loss = ((out - tgt) ** 2).mean()
-    ref_loss.backward()
-    el = abs(float(loss.item()) - float(ref_loss)) / float(ref_loss)
-    print("loss %.6f vs CPU %.6f (rel %.2e)" % (float(loss.item()), float(ref_loss), el))
-    assert el <= 2e-2
-    for l in range(len(S.LAYERS)):
-        ew, eb = _rel(gw[l], wc[l].grad), _rel(gb[l], bc[l].grad)
-        print("layer %d: weight grad rel L2 %.2e, bias grad %.2e" % (l + 1, ew, eb))
-        assert ew <= GRAD_TOL and eb <= GRAD_TOL, (l, ew, eb)
+    for bf16, tol in ((True, BF16_REF_TOL), (False, GRAD_TOL)):
+        wc = [w.detach().cpu().to(torch.bfloat16).float().requires_grad_(True) for w in net.w]
+        bc = [b.detach().cpu().clone().requires_grad_(True) for b in net.b]
+        out = S.reference_forward(wc, bc, xg.float().cpu()[..., :S.IN_CH], bf16=bf16)
+        ref_loss = ((out - tgt) ** 2).mean()
+        ref_loss.backward()
+        el = abs(float(loss.item()) - float(ref_loss.detach())) / float(ref_loss.detach())
+        print("%s reference: loss %.6f vs %.6f (rel %.2e)" % ("BF16-rounding" if bf16 else "FP32",
+                                                               float(loss.item()), float(ref_loss.detach()), el))
+        assert el <= 2e-2
+        for l in range(len(S.LAYERS)):
+            ew, eb = _rel(gw[l], wc[l].grad), _rel(gb[l], bc[l].grad)
+            print("  layer %d: weight grad rel L2 %.2e, bias grad %.2e" % (l + 1, ew, eb))
+            assert ew <= tol and eb <= tol, (bf16, l, ew, eb)
 
 
 def test_training_reduces_loss():
