@@ -570,9 +570,10 @@ def run_ours(args, rank, world, local_rank, workload, secondary=False):
 
 def run_ensemble(args, local_rank):
     """Config 3: the 96-reach ensemble on one GPU as one batch, stepped with batched
-    launches (every phase one launch for all reaches, the batch step one CUDA graph) and,
-    for comparison, member by member (one graph and stream per reach).  Spun up past the
-    discharge ramp and the sediment start, then timed by CUDA events back to back."""
+    launches (every phase one launch for all reaches, the batch step one CUDA graph),
+    member by member (one graph and stream per reach), and as the autotuner chooses
+    between those and the members' sweep shapes (`value`).  Spun up past the discharge
+    ramp and the sediment start, then timed by CUDA events back to back."""
     import torch
     from hydist import cases
     from hydist.lib import Batch
@@ -609,9 +610,88 @@ def run_ensemble(args, local_rank):
         ms = timed(args.steps)
         out[label] = {"value": cells * args.steps / (ms / 1e3), "unit": "cell-updates/s",
                       "ms_per_step": ms / args.steps, "batched_steps": b.fused_steps() - f0}
-    out["value"] = out["batched"]["value"]
     out["speedup_vs_per_member"] = out["per_member"]["ms_per_step"] / out["batched"]["ms_per_step"]
+    # the autotuner's choice among per-member sweep shapes and the batched launches
+    from hydist.tune import DEFAULT_CANDIDATES, tune_batch
+    best, times = tune_batch(b, DEFAULT_CANDIDATES, steps=10)
+    b.step(max(args.warmup, 3), sync=True)
+    ms = timed(args.steps)
+    out["tuned"] = {"policy": "batched" if best == ("fused",) else "per_member d=%d wide=%d" % tuple(best),
+                    "value": cells * args.steps / (ms / 1e3), "unit": "cell-updates/s",
+                    "ms_per_step": ms / args.steps,
+                    "candidates_ms": {("batched" if k == ("fused",) else "d=%d wide=%d" % k): v * 1e3
+                                      for k, v in times.items()}}
+    out["value"] = out["tuned"]["value"]
     b.close()
+    return out
+
+
+def run_config5(args, local_rank, hours=12.0, seeds=8, snapshots=64, iters=800, warm=20, min_warm=1):
+    """Config 5, the morphodynamic reach (1048 x 980, bed fed back every 10 min, 30 days
+    stated): simulated hours per wall second of the plain FP64 run and of the quasi-steady
+    form (FP32-bulk mixed steps; each 10-min period replaced by the surrogate's jump and at
+    most `warm` plain steps judged by the steady residual, with fallback to plain stepping),
+    and the quasi-steady form's bed and level differences from the plain FP64 run, on a
+    bounded sample of `hours` hours after a 2 h spin-up (the spin-up and the surrogate's
+    data generation and training are not timed).  Timed by the host clock around
+    synchronised calls: the quasi-steady loop's decisions are taken on the host."""
+    import numpy as np
+    import torch
+    from hydist import cases, morpho as MO, surrogate as S
+    from hydist.lib import Simulation
+    from hydist.params import PRECISION_MIXED
+    spin = 7200
+    days = (spin / 3600 + hours) / 24 + 0.05
+    t0 = time.perf_counter()
+    X, Y, W, crop, dropped = MO.generate(list(range(500, 500 + seeds)), snapshots, every=600, device=local_rank)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    net = S.Surrogate(device=local_rank, seed=0)
+    t0 = time.perf_counter()
+    L = MO.train(net, X, Y, W, iters=iters, batch=8, lr=2e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    nsnap = int(X.shape[0])
+    del X, Y, W
+
+    def make(mixed):
+        c = cases.config5_case(days=days)
+        if mixed:
+            p = c.params.copy()
+            p.precision_mode = PRECISION_MIXED
+            c.params = p
+        sim = Simulation.from_case(c, device=local_rank)
+        sim.step(spin)
+        sim.synchronize()
+        return sim, c
+
+    ref, _ = make(False)
+    t0 = time.perf_counter()
+    ref.step(int(round(hours * 3600)))
+    plain_s = time.perf_counter() - t0
+    zr, dHr, wet = ref.get("z"), ref.get("dH"), ref.get("khouot") == 0
+    ref.close()
+    out = {"workload": "config5 morphodynamic reach 1048x980 dx=5m dt=1s, bed fed back every 600 s (morfac 1); "
+                       "sample of %.0f h after a 2 h spin-up (30 days stated)" % hours,
+           "sim_hours": hours,
+           "plain_fp64": {"sim_h_per_wall_s": hours / plain_s, "wall_s": plain_s,
+                          "steps": int(round(hours * 3600)), "bed_change_max_m": float(np.abs(dHr).max())},
+           "surrogate": {"snapshots": nsnap, "reaches_dropped": dropped, "iters": iters,
+                         "loss_first": L[0], "loss_last": float(np.mean(L[-20:])), "generate_s": gen_s,
+                         "train_s": train_s}}
+    for label, use_net in (("quasi_steady_surrogate", True), ("quasi_steady_no_network", False)):
+        sim, c = make(True)
+        jump = MO.SurrogateJump(net, c, crop) if use_net else None
+        q = MO.QuasiSteady(sim, c, warm=warm, gate=1e-4, jump=jump, min_warm=min_warm)
+        t0 = time.perf_counter()
+        q.run_until(spin + hours * 3600)
+        wall = time.perf_counter() - t0
+        z, dH = sim.get("z"), sim.get("dH")
+        out[label] = {"sim_h_per_wall_s": hours / wall, "wall_s": wall, "speedup_vs_plain_fp64": plain_s / wall,
+                      "periods_accepted": q.accepted, "periods_fallback": q.fallbacks, "steps": q.steps,
+                      "max_level_diff_m": float(np.abs(z - zr)[wet].max()),
+                      "max_bed_diff_m": float(np.abs(dH - dHr).max())}
+        sim.close()
     return out
 
 
@@ -683,6 +763,7 @@ def main():
     ap.add_argument("--workload", default="config2", choices=sorted(WORKLOADS),
                     help="config2 (the default: the 1048x980 reach) or config4 (the 4096x2048 reach)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the config-3 ensemble line")
+    ap.add_argument("--no-config5", action="store_true", help="skip the config-5 morphodynamic line")
     ap.add_argument("--secondary", default="config4", choices=sorted(WORKLOADS) + ["none"],
                     help="a second workload measured in the same run and printed under 'workloads' "
                          "(default config4; 'none' skips it)")
@@ -716,6 +797,10 @@ def main():
             ens = run_ensemble(args, local_rank)
             if res is not None:
                 res.setdefault("workloads", {})["config3"] = ens
+        if not args.no_config5 and args.secondary != "none" and world == 1:
+            c5 = run_config5(args, local_rank)
+            if res is not None:
+                res.setdefault("workloads", {})["config5"] = c5
     finally:
         if world > 1:
             import torch

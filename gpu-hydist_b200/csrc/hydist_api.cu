@@ -327,6 +327,7 @@ DevParams make_dev_params(const HydCaseParams& P) {
     d.channel = (P.kenhhepd || P.kenhhepng) ? 1 : 0;
     d.bed_feedback = P.bed_feedback ? 1 : 0;
     d.bed_fixed = P.bed_fixed > 0 ? P.bed_fixed : 0;
+    d.bed_min_depth = P.bed_min_depth > 0 ? P.bed_min_depth : 0.0;
     d.morfac = P.morfac;
     d.bed_period = P.bed_period > 0 ? P.bed_period : P.bed_change_start;
     d.mixed = P.precision_mode == HYD_PRECISION_MIXED ? 1 : 0;
@@ -1389,11 +1390,13 @@ int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n) {
     double sums[4];
     CUDA_TRY(cudaMemcpyAsync(sums, tot, sizeof sums, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    if (!h->res_valid) {
-        out[0] = out[1] = HUGE_VAL;
+    if (!h->res_valid || !(sums[1] > 0) || !(sums[3] > 0)) {
+        out[0] = out[1] = HUGE_VAL;  // no snapshot yet, no wet cell or no flow: not steady
     } else {
-        out[0] = sums[1] > 0 ? std::sqrt(sums[0] / sums[1]) : (sums[0] > 0 ? HUGE_VAL : 0.0);
-        out[1] = sums[3] > 0 ? std::sqrt(sums[2] / sums[3]) : (sums[2] > 0 ? HUGE_VAL : 0.0);
+        out[0] = std::sqrt(sums[0] / sums[1]);
+        out[1] = std::sqrt(sums[2] / sums[3]);
+        if (!std::isfinite(out[0])) out[0] = HUGE_VAL;
+        if (!std::isfinite(out[1])) out[1] = HUGE_VAL;
     }
     if (snapshot) h->res_valid = 1;
     return HYD_OK;

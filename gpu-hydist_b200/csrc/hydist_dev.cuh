@@ -30,7 +30,8 @@ struct DevParams {
     // morphodynamic feedback (off: the reference's step): each Exner update's bed change,
     // morfac x bed_period / (1 - Dorong) x rate, is applied to h and the depths re-derived
     int bed_feedback;
-    int bed_fixed;  // the bed stays fixed within bed_fixed cells of the grid's edges
+    int bed_fixed;         // the bed stays fixed within bed_fixed cells of the grid's edges
+    double bed_min_depth;  // and where the water is shallower than this
     double morfac, bed_period;  // bed_period: the Exner period in s (bed_change_start if unset)
     // precision_mode MIXED: coefficient assembly, the line sweeps, the explicit momentum and
     // the sediment transport in FP32; the water level's continuity update, the mass sums

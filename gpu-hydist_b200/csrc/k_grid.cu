@@ -1793,8 +1793,10 @@ __global__ void k_bedload(DevGrid g, DevParams p, int startidx, int endidx) {
 // 2 dx mode exactly and keeps smooth changes, then limited to kBedLimit of the water depth
 // and kBedCap metres (the step stays small against the depth it acts on), added to dH as a
 // Kahan sum and applied to the bed, h = h0 + dH.  Cells within bed_fixed cells of the
-// grid's edges (the inlet and outlet sections of the open boundaries) keep their bed.
-// Indexing as k_bedload.
+// grid's edges (the inlet and outlet sections of the open boundaries) and cells with less
+// than bed_min_depth of water (a threshold depth for the bed change, as morphodynamic
+// models keep: the banks' wet/dry fringe would otherwise break into patches) keep their
+// bed.  Indexing as k_bedload.
 __global__ void k_bed_apply(DevGrid g, DevParams p, int startidx, int endidx) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
     const int i = blockIdx.y * blockDim.y + threadIdx.y + startidx;
@@ -1802,6 +1804,7 @@ __global__ void k_bed_apply(DevGrid g, DevParams p, int startidx, int endidx) {
     if (i >= endidx || j > M) return;
     const int F = p.bed_fixed;
     if (i < 2 + F || i > N - F || j < 2 + F || j > M - F) return;
+    if (g.H_moi[i * width + j] < p.bed_min_depth) return;
     const int pos = i * width + j;
     const double* __restrict__ inc = g.dHinc;
     if (!isfinite(inc[pos])) return;
@@ -1846,14 +1849,18 @@ __global__ void k_bed_derive(DevGrid g, DevParams p) {
         const double old = g.htaiz[pos];
         g.htaiz[pos] = ht;
         g.htaiz_bd[pos] = ht;
-        // the face depths below datum taken no smaller than H_TINH: a raised bed must not
-        // give the friction factor a negative base (the set-up's formula is otherwise kept)
-        if (h[pos - 1] + h[pos] != 0)
-            g.Kx1[pos] = p.g * pow(fmax((h[pos - 1] + h[pos]) * 0.5, p.H_TINH), -2 * p.mu_mn) *
-                         pow((g.hsnham[pos - 1] + g.hsnham[pos]) * 0.5, 2);
-        if (h[pos - P] + h[pos] != 0)
-            g.Ky1[pos] = p.g * pow(fmax((h[pos - P] + h[pos]) * 0.5, p.H_TINH), -2 * p.mu_mn) *
-                         pow((g.hsnham[pos - P] + g.hsnham[pos]) * 0.5, 2);
+        // the set-up's formula; a face depth below datum that is not positive (a raised bed),
+        // where its pow has no real value, is taken as H_TINH.  Clamping every face depth to
+        // H_TINH instead would change the friction of the shallow faces that the set-up gave
+        // a depth between 0 and H_TINH at the first update, unbalancing the flow there.
+        if (h[pos - 1] + h[pos] != 0) {
+            const double d = (h[pos - 1] + h[pos]) * 0.5;
+            g.Kx1[pos] = p.g * pow(d > 0 ? d : p.H_TINH, -2 * p.mu_mn) * pow((g.hsnham[pos - 1] + g.hsnham[pos]) * 0.5, 2);
+        }
+        if (h[pos - P] + h[pos] != 0) {
+            const double d = (h[pos - P] + h[pos]) * 0.5;
+            g.Ky1[pos] = p.g * pow(d > 0 ? d : p.H_TINH, -2 * p.mu_mn) * pow((g.hsnham[pos - P] + g.hsnham[pos]) * 0.5, 2);
+        }
         if (g.khouot[pos] == 0) {
             g.H_moi[pos] = ht + g.z[pos];
             if (i >= 2 && j >= 2) dv = ht - old;

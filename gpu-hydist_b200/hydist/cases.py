@@ -313,7 +313,8 @@ def config2_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE):
                         Q0=2000.0 * q_scale, Q1=3500.0 * q_scale, name="config2_meander")
 
 
-def config4_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE, hours=24.0, dT=1.0, end_cells=32, tide_delay_h=None):
+def config4_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE, hours=24.0, dT=1.0, end_cells=32, tide_delay_h=None,
+                 tide_amp=1.0):
     """Large single reach 4096 x 2048, dx = 2.5 m, hydraulics + sediment + bed change.
 
     The config-2 meander scaled x2 in length and width: centreline amplitude 240 m,
@@ -336,13 +337,14 @@ def config4_case(spinup_h=1.0, q_scale=CONFIG2_Q_SCALE, hours=24.0, dT=1.0, end_
     c = meander_case(N=4096, M=2048, dX=2.5, dT=dT, hours=hours, spinup_h=spinup_h, amp=240.0,
                      wavelength=3000.0, width=300.0, noise_len=100.0,
                      Q0=2000.0 * q_scale * 2.0, Q1=3500.0 * q_scale * 2.0, end_cells=end_cells,
-                     tide_delay_h=spinup_h if tide_delay_h is None else tide_delay_h,
+                     tide_delay_h=spinup_h if tide_delay_h is None else tide_delay_h, tide_amp=tide_amp,
                      name="config4_large_meander")
     c.notes["morfac"] = 10.0
     return c
 
 
 MORPHO_TOE = 1.0  # Pa: erosion threshold of the morphodynamic workloads' sediment
+MORPHO_MIN_DEPTH = 0.5  # m: no bed change in shallower water
 
 
 def with_feedback(case, morfac=1.0, bed_period=600.0, fixed=None):
@@ -355,15 +357,17 @@ def with_feedback(case, morfac=1.0, bed_period=600.0, fixed=None):
     update within a few updates near the inflow, where the inflowing load settles), and
     within two hours of config 4 the bed cuts lines into more than 20 wet segments.  So the
     morphodynamic runs take a clear-water inflow (concentration 0), an erosion threshold of
-    MORPHO_TOE, and a fixed bed within `fixed` cells of the edges (default: twice the
+    MORPHO_TOE, a fixed bed within `fixed` cells of the edges (default: twice the
     meander's rectangular end sections, i.e. the inlet and outlet sections and their
-    blends).  On config 2 this gives mean bed changes of about 0.1 mm per update."""
+    blends) and where the water is shallower than MORPHO_MIN_DEPTH (the banks' fringe).
+    On config 2 this gives mean bed changes of about 0.1 mm per update."""
     p = case.params.copy()
     p.bed_feedback = 1
     p.morfac = float(morfac)
     p.bed_period = float(bed_period)
     p.Toe = MORPHO_TOE
     p.bed_fixed = int(fixed if fixed is not None else 2 * case.notes.get("end_cells", 8))
+    p.bed_min_depth = MORPHO_MIN_DEPTH
     case.params = p
     for e in range(4):
         case.cc[e] = np.zeros_like(case.cc[e])

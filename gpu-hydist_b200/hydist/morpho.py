@@ -14,10 +14,12 @@ replaces the period's steps by a jump to that equilibrium and a few plain steps:
   3. the clock moved to `warm` steps before the period's end (hyd_set_time) and plain
      ADI steps taken, the steady residual (hyd_steady_residual: relative velocity change
      per step, and level change per depth) read after each;
-  4. once both residuals are below the gate, the clock is moved to the last step of the
-     period and that step taken, which makes the period's bed update on the accepted
-     state; if the residual has not fallen below the gate within `warm` - 1 steps, the
-     checkpoint is restored and the period stepped plainly (the fallback).
+  4. once both residuals are below the gate (read from the `min_warm`-th warm step on)
+     and the state is finite,
+     the clock is moved to the last step of the period and that step taken, which makes
+     the period's bed update on the accepted state; if the residual has not fallen below
+     the gate within `warm` - 1 steps, the checkpoint is restored and the period stepped
+     plainly (the fallback).
 
 No reference counterpart (the reference steps every dT, Engine.py:144-366, and never
 feeds the bed back).  The surrogate's data are plain-solver snapshots of config-5-style
@@ -30,9 +32,14 @@ import numpy as np
 
 from . import cases
 from . import surrogate as S
-from .lib import Batch, Simulation
+from .lib import Simulation
 
 H_REF, N_REF, Q_REF, STAGE_REF, DZ_REF = 8.0, 0.025, 700.0, 0.3, 0.1
+# trust region of one jump: the surrogate's increments are clipped to these (m/s, m/s, m)
+JUMP_MAX = (0.1, 0.1, 0.05)
+# snapshot cells with a faster flow are left out of the training loss (a reach about to
+# fail the run's checks can carry a few runaway cells before it is dropped)
+TRAIN_MAX_SPEED = 3.0
 
 
 def forcing_at(case, t):
@@ -110,19 +117,26 @@ class Targets:
             sim.get_device(f, b)
         sim.get_device("khouot", self.kh)
         sl = (slice(i0, i0 + rows), slice(j0, j0 + cols))
-        y_out[..., 0] = self.buf["u"][sl]
-        y_out[..., 1] = self.buf["v"][sl]
-        y_out[..., 2] = (self.buf["z"][sl] - stage) / DZ_REF
-        w_out.copy_((self.kh[sl] == 0).float())
+        u, v, z = self.buf["u"][sl], self.buf["v"][sl], self.buf["z"][sl]
+        y_out[..., 0] = u
+        y_out[..., 1] = v
+        y_out[..., 2] = (z - stage) / DZ_REF
+        ok = (self.kh[sl] == 0) & (u.abs() <= TRAIN_MAX_SPEED) & (v.abs() <= TRAIN_MAX_SPEED) & z.isfinite()
+        y_out.nan_to_num_(0.0, 0.0, 0.0)
+        w_out.copy_(ok.float())
 
 
 def generate(seeds, snapshots, every=600, settle_h=2.0, device=0, crop=None, log=None):
     """Plain-solver quasi-steady snapshots of config-5-style reaches (config5_case with
-    each seed, the bed not fed back): the reaches run side by side as one batch (batched
-    launches), spun up for `settle_h` hours, then a snapshot of every reach every `every`
-    seconds, `snapshots` per reach.  Returns device tensors X (S, rows, cols, 16) BF16,
-    Y (S, rows, cols, 3) FP32, W (S, rows, cols) FP32 and the crop."""
+    each seed, the bed not fed back): every reach on its own handle and stream, all queued
+    together so that they step side by side on the device, spun up for `settle_h` hours,
+    then a snapshot of every reach every `every` seconds, `snapshots` per reach.  A reach
+    whose run fails (a device check, e.g. a line with more than 20 wet segments once its
+    floodplain starts to flood in patches) keeps the snapshots it gave and drops out.
+    Returns device tensors X (S, rows, cols, 16) BF16, Y (S, rows, cols, 3) FP32,
+    W (S, rows, cols) FP32, the crop and the number of reaches that dropped out."""
     import torch
+    from .lib import HydError
     dev = torch.device("cuda", device)
     days = (settle_h * 3600 + snapshots * every) / 86400.0 + 0.1
     cs = [cases.config5_case(seed=s, days=days, feedback=False) for s in seeds]
@@ -132,24 +146,39 @@ def generate(seeds, snapshots, every=600, settle_h=2.0, device=0, crop=None, log
     X = torch.empty((n, rows, cols, 16), dtype=torch.bfloat16, device=dev)
     Y = torch.empty((n, rows, cols, 3), dtype=torch.float32, device=dev)
     W = torch.empty((n, rows, cols), dtype=torch.float32, device=dev)
-    batch = Batch(cs, device=device)
-    batch.set_fused(True)
+    sims = [Simulation.from_case(c, device=device) for c in cs]
     feats = [Features(c, crop, dev) for c in cs]
     tgts = [Targets(c, crop, dev) for c in cs]
-    batch.step(int(round(settle_h * 3600)))
+    alive = list(range(len(cs)))
+
+    def advance(nsteps):
+        for m in alive:
+            sims[m].step(nsteps, sync=False)
+        ok = []
+        for m in alive:
+            try:
+                sims[m].synchronize()
+                ok.append(m)
+            except HydError as e:
+                if log:
+                    log("reach %d dropped at t = %.0f s: %s" % (seeds[m], sims[m].t, e))
+        alive[:] = ok
+
+    advance(int(round(settle_h * 3600)))
     k = 0
     t0 = time.perf_counter()
     for s in range(snapshots):
-        batch.step(every)
-        for m, c, f, g in zip(batch.members, cs, feats, tgts):
-            Q, st = forcing_at(c, m.t)
-            f.build(m, Q, st, out=X[k])
-            g.build(m, st, Y[k], W[k])
+        advance(every)
+        for m in alive:
+            Q, st = forcing_at(cs[m], sims[m].t)
+            feats[m].build(sims[m], Q, st, out=X[k])
+            tgts[m].build(sims[m], st, Y[k], W[k])
             k += 1
         if log and s % max(1, snapshots // 5) == 0:
-            log("snapshot %d/%d, %.1f s" % (s + 1, snapshots, time.perf_counter() - t0))
-    batch.close()
-    return X, Y, W, crop
+            log("snapshot %d/%d, %d reaches, %.1f s" % (s + 1, snapshots, len(alive), time.perf_counter() - t0))
+    for sim in sims:
+        sim.close()
+    return X[:k], Y[:k], W[:k], crop, len(cs) - len(alive)
 
 
 def train(net, X, Y, W, iters=1500, batch=8, lr=2e-3, seed=0, log_every=0):
@@ -179,9 +208,10 @@ class SurrogateJump:
     current (bed, forcing) minus its prediction for the previous period's, as FP32
     increments of u, v, z on the crop."""
 
-    def __init__(self, net, case, crop):
+    def __init__(self, net, case, crop, clip=True):
         self.net = net
         self.crop = crop
+        self.clip = clip
         self.feat = Features(case, crop, net.dev)
         self.prev = None
 
@@ -193,24 +223,32 @@ class SurrogateJump:
 
     def increments(self, sim, Q, stage):
         """(du, dv, dz) contiguous FP32 device tensors, or None on the first call; the
-        prediction is kept as the next call's reference."""
+        prediction is kept as the next call's reference.  Each increment is clipped to
+        JUMP_MAX (the jump's trust region; the gate judges the rest)."""
         cur = self.predict(sim, Q, stage)
         prev, self.prev = self.prev, cur
         if prev is None:
             return None
-        return tuple((a - b).contiguous() for a, b in zip(cur, prev))
+        return tuple((a - b).nan_to_num(0.0, 0.0, 0.0).clamp(-m if self.clip else -1e30, m if self.clip else 1e30)
+                     .contiguous() for a, b, m in zip(cur, prev, JUMP_MAX))
+
+    def reset(self, sim, Q, stage):
+        """Take the prediction for (Q, stage) as the reference of the next increments."""
+        self.prev = self.predict(sim, Q, stage)
 
 
 class QuasiSteady:
     """The quasi-steady morphodynamic loop on one Simulation (see the module docstring).
 
-    period(): advance one bed period; returns (accepted, plain steps taken).  Counters:
-    accepted, fallbacks, steps."""
+    period(): advance one bed period; returns (accepted, plain steps taken).  The gate is
+    read after each of the first `warm` - 1 warm steps from the `min_warm`-th on.
+    Counters: accepted, fallbacks, steps."""
 
-    def __init__(self, sim, case, warm=20, gate=1e-4, jump=None):
+    def __init__(self, sim, case, warm=20, gate=1e-4, jump=None, min_warm=1):
         self.sim = sim
         self.case = case
         self.warm = int(warm)
+        self.min_warm = max(1, min(int(min_warm), self.warm - 1))
         self.gate = float(gate)
         self.jump = jump
         self.period_s = float(case.params.bed_period)
@@ -238,7 +276,7 @@ class QuasiSteady:
         for k in range(1, self.warm):
             sim.step(1)
             r = sim.steady_residual(snapshot=True)
-            if max(r) < self.gate:
+            if k >= self.min_warm and max(r) < self.gate and sim.mass_balance()["nonfinite"] == 0:
                 sim.set_time(t_end - dT)
                 sim.step(1)  # the period's last step: the bed update on the accepted state
                 self.accepted += 1

@@ -23,7 +23,7 @@ _DOUBLE_FIELDS = [
 _INT_FIELDS = ["ketdinh", "kenhhepd", "kenhhepng", "precision_mode"]
 # morphodynamic feedback (no reference counterpart), after the reference's constants
 _MORPHO_FIELDS = [("morfac", ctypes.c_double), ("bed_period", ctypes.c_double), ("bed_feedback", ctypes.c_int),
-                  ("bed_fixed", ctypes.c_int)]
+                  ("bed_fixed", ctypes.c_int), ("bed_min_depth", ctypes.c_double)]
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -68,7 +68,7 @@ def default_params(**overrides):
         sohn=8.0, soha=3.0, sohn1=3.0, CORIOLIS_FORCE=0.0, g=9.81, Ks=2.5 * 0.00001,
         sediment_start=36000.0, bed_change_start=72000.0,
         ketdinh=1, kenhhepd=0, kenhhepng=0, precision_mode=PRECISION_FP64,
-        morfac=1.0, bed_period=0.0, bed_feedback=0, bed_fixed=0,
+        morfac=1.0, bed_period=0.0, bed_feedback=0, bed_fixed=0, bed_min_depth=0.0,
     )
     vals.update(overrides)
     for k, v in vals.items():

@@ -11,17 +11,28 @@ restored.
 
     tune_batch(batch, candidates, steps) -> (best policy, {policy: seconds per step})
 
-A policy (d, wide) gives member k ceil((max(N_k, M_k) + 3) / d) sweep CTAs (d lines per
-CTA: one per warp at d = 16) and the warp-tier choice `wide`.
+A policy (d, wide) steps every member on its own stream and graph and gives member k
+ceil((max(N_k, M_k) + 3) / d) sweep CTAs (d lines per CTA: one per warp at d = 16) and
+the warp-tier choice `wide`.  The policy FUSED steps the batch by batched launches
+(hyd_batch_set_fused: every phase one launch for all members, the lines of all members
+in one persistent sweep of one CTA per SM).  Which is faster depends on the batch: the
+batched launches wait, phase by phase, for the member with the longest chain, while the
+members' own streams overlap their phases.
 """
 import math
 import time
 
-DEFAULT_CANDIDATES = ((16, 1), (8, 1), (32, 1), (16, 0))
+FUSED = ("fused",)
+DEFAULT_CANDIDATES = ((16, 1), (8, 1), (32, 1), (16, 0), FUSED)
 
 
 def apply_policy(batch, policy):
-    """Set every member's sweep shape from the policy (d, wide)."""
+    """Set the batch's stepping from the policy: FUSED, or (d, wide) for every member."""
+    if tuple(policy) == FUSED:
+        batch.set_fused(True)
+        return
+    if hasattr(batch, "set_fused"):
+        batch.set_fused(False)
     d, wide = policy
     for sim in batch.members:
         sim.set_sweep_shape(max(1, math.ceil((max(sim.N, sim.M) + 3) / d)), wide)

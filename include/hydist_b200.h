@@ -84,6 +84,7 @@ typedef struct HydCaseParams {
     int bed_feedback;        /* 1 = apply each bed change to h and re-derive the depths */
     int bed_fixed;           /* the bed stays fixed within this many cells of the grid's edges
                                 (the open boundaries' inlet and outlet sections) */
+    double bed_min_depth;    /* m; the bed stays fixed where the water is shallower */
 } HydCaseParams;
 
 /* precision_mode values */
@@ -336,8 +337,9 @@ int hyd_set_state(hyd_handle h, const void* buf, size_t bytes);
  * taken at the previous call with snapshot = 1, over the wet cells of [2,N] x [2,M]:
  *   out[0] = ||(u, v) - (u0, v0)||_2 / ||(u, v)||_2   (momentum: relative velocity change)
  *   out[1] = ||z - z0||_2 / ||H_moi||_2               (continuity: level change / depth)
- * each an FP64 sum added in a fixed order; HUGE_VAL before the first snapshot.  With
- * snapshot = 1 the current u, v, z become the snapshot.  Synchronous.
+ * each an FP64 sum added in a fixed order; HUGE_VAL before the first snapshot, with no
+ * wet cell or no flow, and for a non-finite sum (so that such a state is never taken for
+ * steady).  With snapshot = 1 the current u, v, z become the snapshot.  Synchronous.
  *
  * hyd_add_levels(h, du, dv, dz, i0, j0, rows, cols, ld) adds DEVICE arrays of FP32
  * increments (element r*ld + c belongs to cell (i0 + r, j0 + c) of the (N+3) x (M+3)

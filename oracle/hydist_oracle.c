@@ -1688,7 +1688,7 @@ static void k_bedload(OraSim* s, int startidx, int endidx) {
  * startidx..endidx-1, columns 2..M), which removes the 2 dx mode exactly and keeps smooth
  * changes, then limited to BED_LIMIT of the depth and BED_CAP metres, added to dH as a
  * Kahan sum and applied to the bed, h = h0 + dH.  Cells within bed_fixed cells of the
- * grid's edges keep their bed. */
+ * grid's edges, and cells with less than bed_min_depth of water, keep their bed. */
 static void bed_feedback_apply(OraSim* s, int startidx, int endidx) {
     const int N = s->N, M = s->M, width = s->W;
     const int F = s->P.bed_fixed > 0 ? s->P.bed_fixed : 0;
@@ -1698,6 +1698,7 @@ static void bed_feedback_apply(OraSim* s, int startidx, int endidx) {
         for (int j = 2; j <= M; j++) {
             const int pos = i * width + j;
             if (i < 2 + F || i > N - F || j < 2 + F || j > M - F) continue;
+            if (s->H_moi[pos] < s->P.bed_min_depth) continue;
             if (!isfinite(inc[pos])) continue;
             double num = 0.0, den = 0.0;
             for (int di = -1; di <= 1; di++) {
@@ -1725,7 +1726,8 @@ static void bed_feedback_apply(OraSim* s, int startidx, int endidx) {
 }
 
 /* After a fed-back bed change (no reference counterpart): what the set-up derived from h
- * re-derived for the new bed: htaiz, htaiz_bd, Kx1, Ky1 (face depths no smaller than H_TINH)
+ * re-derived for the new bed: htaiz, htaiz_bd, Kx1, Ky1 (the set-up's formula; a face depth
+ * below datum that is not positive, where the set-up's pow has no real value, taken as H_TINH)
  * (Onetime_init,
  * support_funcs.cu:20-58), H_moi of the wet cells (update_h_moi, 60-73), Htuongdoi and
  * preprocess_data. */
@@ -1738,12 +1740,16 @@ static void bed_feedback_derive(OraSim* s) {
             const size_t ij = (size_t)i * W + j;
             s->htaiz[ij] = (h[(i - 1) * W + j - 1] + h[(i - 1) * W + j] + h[i * W + j - 1] + h[i * W + j]) * 0.25;
             s->htaiz_bd[ij] = s->htaiz[ij];
-            if (h[i * W + j - 1] + h[i * W + j] != 0)
-                s->Kx1[ij] = P->g * pow(fmax((h[i * W + j - 1] + h[i * W + j]) * 0.5, P->H_TINH), -2 * P->mu_mn) *
+            if (h[i * W + j - 1] + h[i * W + j] != 0) {
+                const double d = (h[i * W + j - 1] + h[i * W + j]) * 0.5;
+                s->Kx1[ij] = P->g * pow(d > 0 ? d : P->H_TINH, -2 * P->mu_mn) *
                              pow((s->hsnham[i * W + j - 1] + s->hsnham[i * W + j]) * 0.5, 2);
-            if (h[(i - 1) * W + j] + h[i * W + j] != 0)
-                s->Ky1[ij] = P->g * pow(fmax((h[(i - 1) * W + j] + h[i * W + j]) * 0.5, P->H_TINH), -2 * P->mu_mn) *
+            }
+            if (h[(i - 1) * W + j] + h[i * W + j] != 0) {
+                const double d = (h[(i - 1) * W + j] + h[i * W + j]) * 0.5;
+                s->Ky1[ij] = P->g * pow(d > 0 ? d : P->H_TINH, -2 * P->mu_mn) *
                              pow((s->hsnham[(i - 1) * W + j] + s->hsnham[i * W + j]) * 0.5, 2);
+            }
             if (s->khouot[ij] == 0) s->H_moi[ij] = s->htaiz[ij] + s->z[ij];
         }
     k_htuongdoi(s);

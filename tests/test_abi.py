@@ -36,7 +36,7 @@ def test_params_struct_layout():
     reference's constants and run options, then 2 doubles + 2 ints of the morphodynamic
     feedback)."""
     from hydist.params import HydCaseParams, default_params
-    assert ctypes.sizeof(HydCaseParams) == 46 * 8 + 6 * 4
+    assert ctypes.sizeof(HydCaseParams) == 47 * 8 + 6 * 4
     assert HydCaseParams.morfac.offset == 44 * 8 + 4 * 4
     p = default_params()
     assert p.dXbp == p.dX * p.dX and p.HaiChiadT == 2.0 / p.dT

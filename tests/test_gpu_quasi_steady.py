@@ -1,10 +1,17 @@
 """The quasi-steady support entry points (GPU): device checkpoint and restore, the clock,
 the steady residual and the level increments, each against host-side arithmetic on the
-fields read back."""
+fields read back; then the quasi-steady morphodynamic loop (hydist.morpho.QuasiSteady):
+its fallback path equal to plain stepping, and a sample of the morphodynamic reach against
+the plain FP64 run."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+# the quasi-steady form's stated difference from the plain FP64 run over the six-hour
+# sample (m): its approximation error, not rounding
+QS_LEVEL_TOL = 2e-2
+QS_BED_TOL = 5e-2
 
 
 def _case():
@@ -105,3 +112,70 @@ def test_add_levels_and_set_time():
     assert sim.t == 100.0 + sim.params.dT
     assert np.isfinite(sim.get("z")).all()
     sim.close()
+
+
+def _config5(hours):
+    from hydist import cases
+    from hydist.params import PRECISION_MIXED
+    c = cases.config5_case(days=(2.0 + hours) / 24 + 0.05)
+    p = c.params.copy()
+    p.precision_mode = PRECISION_MIXED
+    c.params = p
+    return c
+
+
+def test_quasi_steady_fallback_is_plain_stepping():
+    """With a gate no state can pass, every period falls back: restored from the device
+    checkpoint and stepped plainly, which must give the plain run bit for bit."""
+    from hydist import morpho as MO
+    from hydist.lib import Simulation
+    c = _config5(1.0)
+    a = Simulation.from_case(c)
+    a.step(7200)
+    b = Simulation.from_case(c)
+    b.step(7200)
+    q = MO.QuasiSteady(b, c, warm=20, gate=0.0)
+    q.run_until(7200 + 3600)
+    a.step(3600)
+    assert q.fallbacks == 6 and q.accepted == 0
+    assert a.t == b.t
+    for f in ("z", "u", "v", "FS", "dH", "h"):
+        assert np.array_equal(a.get(f), b.get(f)), f
+    a.close()
+    b.close()
+
+
+def test_quasi_steady_config5_sample():
+    """Six hours of the morphodynamic reach (bed fed back every 10 min) after a 2 h spin-up:
+    the quasi-steady form (FP32-bulk steps, no network: the previous state is the warm
+    start) against the plain FP64 run.  Most periods pass the gate within the warm steps,
+    the steps taken fall by more than 5x, and the level and bed stay within the stated
+    bounds of the FP64 run (QS_LEVEL_TOL, QS_BED_TOL: the quasi-steady approximation's own
+    error, the flow and the suspended sediment not following the period's forcing and bed
+    changes step by step)."""
+    from hydist import morpho as MO
+    from hydist.lib import Simulation
+    hours = 6.0
+    c = _config5(hours)
+    from hydist import cases
+    cref = cases.config5_case(days=(2.0 + hours) / 24 + 0.05)
+    ref = Simulation.from_case(cref)
+    ref.step(7200 + int(hours * 3600))
+    sim = Simulation.from_case(c)
+    sim.step(7200)
+    q = MO.QuasiSteady(sim, c, warm=20, gate=1e-4)
+    q.run_until(7200 + hours * 3600)
+    assert sim.t == ref.t
+    wet = ref.get("khouot") == 0
+    dz = float(np.abs(sim.get("z") - ref.get("z"))[wet].max())
+    db = float(np.abs(sim.get("dH") - ref.get("dH")).max())
+    nplain = int(hours * 3600)
+    print("quasi-steady %.0f h: %d of %d periods accepted, %d steps (plain %d), level diff %.2e m, bed diff %.2e m "
+          "(bed change up to %.3f m)" % (hours, q.accepted, q.accepted + q.fallbacks, q.steps, nplain, dz, db,
+                                         float(np.abs(ref.get("dH")).max())))
+    assert q.accepted >= 0.75 * (q.accepted + q.fallbacks)
+    assert q.steps * 5 < nplain
+    assert dz <= QS_LEVEL_TOL and db <= QS_BED_TOL
+    assert sim.mass_balance()["nonfinite"] == 0
+    sim.close()
+    ref.close()
