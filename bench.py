@@ -304,6 +304,11 @@ def run_ours(args, rank, world, local_rank, workload, secondary=False):
         torch.distributed.barrier()
     ms = float(t_max.item())
     value = world * cells * args.steps / (ms / 1e3)
+    if args.timed_only:  # profiling runs: the timed steps and nothing after them
+        sim.close()
+        return {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "timed_only": True,
+                "config": {"workload": WORKLOADS[workload][1]}}
 
     # the same steps back to back, L2 kept warm between them
     e0 = torch.cuda.Event(enable_timing=True)
@@ -764,6 +769,10 @@ def main():
                     help="config2 (the default: the 1048x980 reach) or config4 (the 4096x2048 reach)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the config-3 ensemble line")
     ap.add_argument("--no-config5", action="store_true", help="skip the config-5 morphodynamic line")
+    ap.add_argument("--timed-only", action="store_true",
+                    help="profiling runs: spin up, warm up, run the timed steps, print a short line and stop")
+    ap.add_argument("--config5-hours", type=float, default=12.0,
+                    help="simulated hours of the config-5 sample (720 = the stated 30 days)")
     ap.add_argument("--secondary", default="config4", choices=sorted(WORKLOADS) + ["none"],
                     help="a second workload measured in the same run and printed under 'workloads' "
                          "(default config4; 'none' skips it)")
@@ -798,7 +807,7 @@ def main():
             if res is not None:
                 res.setdefault("workloads", {})["config3"] = ens
         if not args.no_config5 and args.secondary != "none" and world == 1:
-            c5 = run_config5(args, local_rank)
+            c5 = run_config5(args, local_rank, hours=args.config5_hours)
             if res is not None:
                 res.setdefault("workloads", {})["config5"] = c5
     finally:

@@ -374,6 +374,29 @@ def with_feedback(case, morfac=1.0, bed_period=600.0, fixed=None):
     return case
 
 
+CONFIG4_MORPHO_Q = 800.0  # m3/s: the steady discharge of config 4's 24-hour morphodynamic run
+
+
+def config4_morpho_case(morfac=10.0, bed_period=600.0, dT=1.0, Q=CONFIG4_MORPHO_Q):
+    """Config 4's 24-hour morphodynamic run: the 4096 x 2048 reach with the bed fed back
+    every `bed_period` s at morphological factor `morfac` (with_feedback's long-run
+    sediment), a steady discharge Q after the one-hour ramp and a fixed stage of 0 m.
+
+    The workload states no forcing.  Under the parity case's tide (1 m) or its rising
+    hydrograph (to 1750 m3/s) the reference's scheme on this 2.5 m grid goes unstable after
+    2 to 10 hours, with or without the bed fed back (velocities past about 1.1 m/s at low
+    water, then a blow-up in the channel), at dt = 1 s and at 0.5 s alike.  A steady 800
+    m3/s with a fixed stage keeps the velocities below 0.9 m/s, and the run stays finite
+    over the 24 hours at morfac 10 (checked at dt = 1 s and 0.5 s; bed changes up to
+    1.2 m, about ten morphological days)."""
+    c = config4_case(dT=dT, tide_amp=0.0)
+    q = c.tables[EDGE_LEFT][0]
+    th = np.arange(q.size, dtype=np.float64)
+    q[:] = np.where(th < 1.0, Q * th, Q)
+    c.name = "config4_morpho"
+    return with_feedback(c, morfac=morfac, bed_period=bed_period)
+
+
 CONFIG5_Q_MEAN, CONFIG5_Q_AMP = 687.5, 187.5  # config 2's scaled 500-875 m3/s range
 CONFIG5_Q_PERIOD_H, CONFIG5_STAGE_PERIOD_H, CONFIG5_STAGE_AMP = 240.0, 354.4, 0.3
 

@@ -19,6 +19,11 @@ from helpers import REL_TOL, rel_linf
 
 pytestmark = pytest.mark.gpu
 
+# config 4's 24 h morphodynamic run, FP32-bulk mixed form against FP64: the bed's stated
+# bound (m) and the water budget's closure (relative to the volume)
+MIXED_24H_BED_TOL = 0.1
+MIXED_24H_CLOSURE = 1e-4
+
 
 def _feedback(case, morfac, period):
     p = case.params.copy()
@@ -80,14 +85,13 @@ def test_feedback_off_keeps_the_bed():
     sim.close()
 
 
-def test_config4_24h_morfac10():
-    """The 4096 x 2048 reach over its stated 24 h (86 400 steps of 1 s) with hydraulics,
-    sediment and the bed change fed back at morphological factor 10, the bed updated every
-    10 min (cases.with_feedback's long-run sediment): finite throughout, the water budget
-    closed with the bed's share, and the simulated hours per wall second reported."""
+def _run_24h(precision):
     from hydist import cases
     from hydist.lib import Simulation
-    c = cases.with_feedback(cases.config4_case(), morfac=10.0, bed_period=600.0)
+    c = cases.config4_morpho_case()
+    p = c.params.copy()
+    p.precision_mode = precision
+    c.params = p
     sim = Simulation.from_case(c)
     sim.step(1)
     v0 = sim.mass_balance()["volume"]
@@ -105,13 +109,34 @@ def test_config4_24h_morfac10():
         worst = max(worst, abs(dv - pred) / mb["volume"])
     wall = time.perf_counter() - t0
     assert sim.t == 86400.0
-    dH = sim.get("dH")
-    assert np.isfinite(dH).all()
-    mx = float(np.abs(dH).max())
-    b = sim.mass_budget()
-    print("config4 24 h morfac 10: %.1f s wall, %.2f sim-h/wall-s, max |dH| %.4f m, bed volume to the water "
-          "column %.1f m3, closure worst rel %.2e" % (wall, 24.0 / wall, mx, b["bed"], worst))
+    fields = {f: sim.get(f) for f in ("z", "u", "v", "FS", "dH", "khouot")}
+    bed_vol = sim.mass_budget()["bed"]
+    sim.close()
+    return fields, wall, worst, bed_vol
+
+
+def test_config4_24h_morfac10():
+    """The 4096 x 2048 reach over its stated 24 h (86 400 steps of 1 s) with hydraulics,
+    sediment and the bed change fed back at morphological factor 10, the bed updated every
+    10 min (cases.config4_morpho_case: steady discharge, fixed stage, with_feedback's
+    long-run sediment), in FP64 and in the FP32-bulk mixed form: each finite throughout,
+    its water budget closed with the bed's share (the cumulative drift stated), the
+    simulated hours per wall second reported, and the mixed form's per-field L-inf and L2
+    differences from FP64 at 24 h reported (bounded by MIXED_24H_BED_TOL on the bed)."""
+    from hydist.params import PRECISION_FP64, PRECISION_MIXED
+    ref, wall, worst, bed_vol = _run_24h(PRECISION_FP64)
+    mx = float(np.abs(ref["dH"]).max())
+    print("config4 24 h morfac 10, FP64: %.1f s wall, %.2f sim-h/wall-s, max |dH| %.4f m, bed volume to the water "
+          "column %.1f m3, closure worst rel %.2e" % (wall, 24.0 / wall, mx, bed_vol, worst))
     # each 10-min update moves a cell's bed by at most 0.05 m (the feedback's limit)
     assert 0 < mx <= 0.05 * 144 + 1e-9
     assert worst <= 1e-9
-    sim.close()
+    mix, wall_m, worst_m, _ = _run_24h(PRECISION_MIXED)
+    print("  mixed: %.1f s wall (%.2fx FP64), closure worst rel %.2e" % (wall_m, wall / wall_m, worst_m))
+    wet = (ref["khouot"] == 0) & (mix["khouot"] == 0)
+    for f in ("z", "u", "v", "FS", "dH"):
+        d = (mix[f] - ref[f])[wet]
+        print("  %-3s L-inf %.3e  L2 (RMS) %.3e" % (f, float(np.abs(d).max()), float(np.sqrt((d * d).mean()))))
+    print("  mask cells differing %d" % int((ref["khouot"] != mix["khouot"]).sum()))
+    assert worst_m <= MIXED_24H_CLOSURE
+    assert float(np.abs(mix["dH"] - ref["dH"]).max()) <= MIXED_24H_BED_TOL
