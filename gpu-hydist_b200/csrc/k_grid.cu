@@ -10,6 +10,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "hydist_dev.cuh"
 
@@ -968,36 +969,112 @@ __device__ __forceinline__ void mark_dirty(int* flags, int* list, unsigned* ctr,
     if (atomicExch(&flags[line], 1) == 0) list[atomicAdd(ctr, 1u)] = line;
 }
 
+struct WetBytes;
+struct WetGlobal;
+
+// The wet flags of cells a..b packed into 32-cell words by one warp: bit t of
+// words[w - w0] is cell origin + 32 w + t (cells outside [a, b] give 0), w = w0..w1.
+// Generic form: one cell per lane and word, origin 2.
+template <class Wet>
+__device__ __forceinline__ void pack_wet_words(const Wet& wet, int a, int b, int origin, unsigned* words, int w0,
+                                               int w1) {
+    const int lane = threadIdx.x & 31;
+    for (int w = w0; w <= w1; w++) {
+        const int k = origin + 32 * w + lane;
+        const bool z = (k >= a && k <= b) ? wet(k) : false;
+        const unsigned bits = __ballot_sync(0xffffffffu, z);
+        if (lane == 0) words[w - w0] = bits;
+    }
+}
+
+// Column-major mask bytes (origin 0): 16 consecutive bytes per lane (one 16-byte load),
+// 512 cells per pass, so that a 4096-cell column takes 8 dependent loads instead of 128.
+// Lanes 2m and 2m+1 hold the two halves of word (base >> 5) + m.  A column starts on a
+// 32-byte boundary and holds LT >= N + 3 bytes, LT a multiple of 32, so a lane's load at
+// c <= b <= N (c a multiple of 16) ends within the column.
+__device__ __forceinline__ void pack_wet_bytes(const unsigned char* col, int a, int b, unsigned* words, int w0,
+                                               int w1) {
+    const int lane = threadIdx.x & 31;
+    for (int base = w0 * 32; base <= w1 * 32 + 31; base += 512) {
+        const int c = base + lane * 16;
+        unsigned m = 0;
+        if (c <= b) {
+            const uint4 q = *reinterpret_cast<const uint4*>(col + c);
+            const unsigned v[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int t = 0; t < 16; t++) {
+                const int k = c + t;
+                if (((v[t >> 2] >> (8 * (t & 3))) & 3u) == 0u && k >= a && k <= b) m |= 1u << t;
+            }
+        }
+        const unsigned hi = __shfl_down_sync(0xffffffffu, m, 1);
+        const int w = (base >> 5) + (lane >> 1);
+        if ((lane & 1) == 0 && w <= w1) words[w - w0] = m | (hi << 16);
+    }
+}
+
+// A row of the int mask (origin 0): 4 consecutive cells per lane (one 16-byte load), 128
+// cells per pass; lanes 8m..8m+7 make word (base >> 5) + m.  A row starts on a 128-byte
+// boundary (the pitch is a multiple of 32 cells) and holds pitch >= M + 3 cells, so a
+// lane's load at c <= b <= M (c a multiple of 4) ends within the row.
+__device__ __forceinline__ void pack_wet_ints(const int* row, int a, int b, unsigned* words, int w0, int w1) {
+    const int lane = threadIdx.x & 31;
+    for (int base = w0 * 32; base <= w1 * 32 + 31; base += 128) {
+        const int c = base + lane * 4;
+        unsigned m = 0;
+        if (c <= b) {
+            const int4 q = *reinterpret_cast<const int4*>(row + c);
+            if (q.x == 0 && c >= a && c <= b) m |= 1u;
+            if (q.y == 0 && c + 1 >= a && c + 1 <= b) m |= 2u;
+            if (q.z == 0 && c + 2 >= a && c + 2 <= b) m |= 4u;
+            if (q.w == 0 && c + 3 >= a && c + 3 <= b) m |= 8u;
+        }
+        m <<= 4 * (lane & 7);
+        m |= __shfl_xor_sync(0xffffffffu, m, 1);
+        m |= __shfl_xor_sync(0xffffffffu, m, 2);
+        m |= __shfl_xor_sync(0xffffffffu, m, 4);
+        const int w = (base >> 5) + (lane >> 3);
+        if ((lane & 7) == 0 && w <= w1) words[w - w0] = m;
+    }
+}
+
 // Wet-segment scan of one line by one warp (Find_Calculation_limits_Horizontal/Vertical,
 // support_funcs.cu:230-335).  The serial while-loop there yields the maximal runs of
 // khouot == 0 within [2, L] in order, except runs starting at L-1 or L, which it skips.
 // Cells a..b are tested with wet(k); every other cell is dry.  The warp packs the wet
-// flags into 32-cell words (words: (b - a) / 32 + 2 entries of shared memory), then
-// lane 0 walks the run starts and ends word by word.
+// flags into 32-cell words (words: (b - a) / 32 + 2 entries of shared memory; mask bytes
+// and mask rows with wide loads), then lane 0 walks the run starts and ends word by word.
 template <class Wet>
 __device__ void warp_scan_line(const DevGrid& g, Wet wet, int a, int b, int L, unsigned* words, int* dau, int* cuoi,
                                int* moc) {
     const int lane = threadIdx.x & 31;
     if (a < 2) a = 2;
     if (b > L) b = L;
-    const int w0 = (a - 2) >> 5, w1 = (b - 2) >> 5;
-    for (int w = w0; w <= w1; w++) {
-        const int k = 2 + 32 * w + lane;
-        const bool z = (k >= a && k <= b) ? wet(k) : false;
-        const unsigned bits = __ballot_sync(0xffffffffu, z);
-        if (lane == 0) words[w - w0] = bits;
+    int origin = 2;
+    if constexpr (std::is_same<Wet, WetBytes>::value) origin = 0;
+    if constexpr (std::is_same<Wet, WetGlobal>::value) origin = wet.along == 1 ? 0 : 2;
+    const int w0 = (a - origin) >> 5, w1 = (b - origin) >> 5;
+    if (b >= a) {
+        if constexpr (std::is_same<Wet, WetBytes>::value) {
+            pack_wet_bytes(wet.col, a, b, words, w0, w1);
+        } else if constexpr (std::is_same<Wet, WetGlobal>::value) {
+            if (wet.along == 1) pack_wet_ints(wet.kh + wet.base, a, b, words, w0, w1);
+            else pack_wet_words(wet, a, b, origin, words, w0, w1);
+        } else {
+            pack_wet_words(wet, a, b, origin, words, w0, w1);
+        }
     }
     __syncwarp();
     if (lane == 0) {
         int nseg = 0;
         int open_start = -1;
-        for (int w = w0; w <= w1; w++) {
+        for (int w = w0; b >= a && w <= w1; w++) {
             const unsigned cur = words[w - w0];
             const unsigned prev = w > w0 ? words[w - w0 - 1] : 0u;
             const unsigned next = w < w1 ? words[w - w0 + 1] : 0u;
             unsigned starts = cur & ~((cur << 1) | (prev >> 31));
             unsigned ends = cur & ~((cur >> 1) | (next << 31));
-            const int c0 = 2 + 32 * w;
+            const int c0 = origin + 32 * w;
             // events in position order; a run's start precedes or equals its end
             while (starts | ends) {
                 if (open_start < 0) {
@@ -1554,6 +1631,66 @@ __global__ void k_vth_span(DevGrid g, DevParams p) {
     for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) vth_cell<FSI, R>(g, p, i, j);
 }
 
+// post_cell (with the state update) followed by vth_cell, for one cell of the extended
+// spans, with every load of the cell issued before its first store: the stores to z, u,
+// v, Htdu and Htdv would otherwise keep the compiler from hoisting the later loads (the
+// arrays may alias for all it knows), and a cell would take three memory round trips
+// instead of one.  Row and column 0 take the two calls as they are.  The values, and
+// the order of their operations, are those of the two calls.
+template <int VTH, int FSI, class R>
+__device__ __forceinline__ void post_vth_cell(const DevGrid& g, const DevParams& p, int i, int j) {
+    const int N = g.N, M = g.M, P = g.P;
+    if (i > N || j > M) return;
+    if (i < 1 || j < 1) {
+        post_cell(g, 1, i, j);
+        if (VTH) vth_cell<FSI, R>(g, p, i, j);
+        return;
+    }
+    const int gp = i * P + j;
+    const double tz = g.t_z[gp], tu = g.t_u[gp], tv = g.t_v[gp];
+    const double z_ip = i + 1 <= N ? g.t_z[gp + P] : g.z[gp + P];
+    const double z_jp = j + 1 <= M ? g.t_z[gp + 1] : g.z[gp + 1];
+    const double hw = g.h[gp - 1], hc = g.h[gp], hs = g.h[gp - P];
+    double htz = 0.0, Hm = 0.0, tu_s = 0.0, tv_w = 0.0;
+    int kh = 1;
+    if (VTH) {
+        htz = g.htaiz[gp];
+        Hm = g.H_moi[gp];
+        tu_s = g.t_u[gp - P];
+        tv_w = g.t_v[gp - 1];
+        if (FSI) kh = g.khouot[gp];
+    }
+    g.z[gp] = tz;
+    g.u[gp] = tu;
+    g.v[gp] = tv;
+    const double htdu = (hw + hc + z_ip + tz) * 0.5;
+    const double htdv = (hs + hc + z_jp + tz) * 0.5;
+    g.Htdu[gp] = htdu;
+    g.Htdv[gp] = htdv;
+    if (!VTH) return;
+    if (i >= 2 && j >= 2) {
+        R vth = 0;
+        if ((htz > p.NANGDAY) && (Hm > p.H_TINH)) {
+            const R ut = (R(tu) + R(tu_s)) * R(0.5);
+            const R vt = (R(tv) + R(tv_w)) * R(0.5);
+            vth = sqrt(ut * ut + vt * vt);
+        }
+        g.VTH[gp] = vth;
+        if (FSI && i >= 3 && i < N && kh == 0) fsi_cell_terms<R>(g, p, gp, vth, g.clock[1]);
+    }
+    const R sg = sqrt(R(p.g));
+    if (htdu > 0) {
+        const R Cz = 18 * log(12 * R(htdu) / R(p.Ks));
+        const R kx = R(5.93) * sg * (R(hw) + R(hc)) * R(0.25) * fabs(R(tu)) / Cz;
+        g.Kx[gp] = rmin(R(100.0), rmax(R(5.0), kx));
+    }
+    if (htdv > 0) {
+        const R Cz = 18 * log(12 * R(htdv) / R(p.Ks));
+        const R ky = R(5.93) * sg * (R(hs) + R(hc)) * R(0.25) * fabs(R(tv)) / Cz;
+        g.Ky[gp] = rmin(R(100.0), rmax(R(5.0), ky));
+    }
+}
+
 // After a half-step's reset, in one launch: the state update (update_uvz + Htuongdoi)
 // and, when VTH, Find_VTH + hesoK on the extended spans (CTAs [0, nbp), one warp per
 // row; both only read the cell's own new Htdu/Htdv); the rescan of the changed lines of
@@ -1570,10 +1707,8 @@ __device__ __forceinline__ void post_fused_body(const DevGrid& g, const DevParam
         const RowLane rl(g, 0, bx);
         const int i = rl.i;
         if (i > g.N) return;
-        for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
-            post_cell(g, 1, i, j);
-            if (VTH) vth_cell<ROWS, R>(g, p, i, j);  // rows: the second half-step, before FSi
-        }
+        // rows: the second half-step, with the FSi terms
+        for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) post_vth_cell<VTH, ROWS, R>(g, p, i, j);
         return;
     }
     if (b >= gx - kEdgeParts) {
