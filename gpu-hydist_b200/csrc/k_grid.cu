@@ -350,20 +350,24 @@ __device__ __forceinline__ void uz_cell_coeffs(const DevGrid& g, const DevParams
     f1 = dTx * u0 + L(g.VISC, pos) * dT / dXbp;
     f2 = -(2 + L(g.Kx1, pos) * dT * sqrt(u0 * u0 + vtb * vtb) / L(g.Htdu, pos) + (2 * dT * L(g.VISC, pos)) / dXbp);
     f3 = dT * L(g.VISC, pos) / dXbp - dTx * u0;
-    if (H[pos - 1] <= p.H_TINH) {
+    // the neighbours the branches below take, loaded before the depth tests that choose
+    // among them (one memory round trip; interior cells have two cells either side)
+    const R um1 = L(u, pos - 1), up1 = L(u, pos + 1), um2 = L(u, pos - 2), up2 = L(u, pos + 2);
+    const double Hm1 = H[pos - 1], Hp1 = H[pos + 1], Hm2 = H[pos - 2];
+    if (Hm1 <= p.H_TINH) {
         if (vtb < 0) {
-            pp = vtb * (-3 * u0 + 4 * L(u, pos + 1) - L(u, pos + 2)) / dY2;
-            qq = (u0 - 2 * L(u, pos + 1) + L(u, pos + 2)) / dYbp;
+            pp = vtb * (-3 * u0 + 4 * up1 - up2) / dY2;
+            qq = (u0 - 2 * up1 + up2) / dYbp;
         }
     } else {
-        if (H[pos + 1] <= p.H_TINH) {
-            if ((H[pos - 2] > p.H_TINH) && (vtb > 0)) {
-                pp = vtb * (3 * u0 - 4 * L(u, pos - 1) + L(u, pos - 2)) / dY2;
-                qq = (u0 - 2 * L(u, pos - 1) + L(u, pos - 2)) / dYbp;
+        if (Hp1 <= p.H_TINH) {
+            if ((Hm2 > p.H_TINH) && (vtb > 0)) {
+                pp = vtb * (3 * u0 - 4 * um1 + um2) / dY2;
+                qq = (u0 - 2 * um1 + um2) / dYbp;
             }
         } else {
-            pp = vtb * (L(u, pos + 1) - L(u, pos - 1)) / dY2;
-            qq = (L(u, pos + 1) - 2 * u0 + L(u, pos - 1)) / dYbp;
+            pp = vtb * (up1 - um1) / dY2;
+            qq = (up1 - 2 * u0 + um1) / dYbp;
         }
     }
     f5 = -2 * u0 + dT * pp - dT * R(p.CORIOLIS_FORCE) * vtb - dT * L(g.VISC, pos) * qq -
@@ -395,20 +399,23 @@ __device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams
     f1 = dTy * v0 + L(g.VISC, pos) * dT / dYbp;
     f2 = -(2 + L(g.Ky1, pos) * dT * sqrt(v0 * v0 + utb * utb) / L(g.Htdv, pos) + (2 * dT * L(g.VISC, pos)) / dYbp);
     f3 = dT * L(g.VISC, pos) / dYbp - dTy * v0;
-    if (H[pos - P] <= p.H_TINH) {
+    // as in uz_cell_coeffs: the branches' neighbours loaded first
+    const R vm1 = L(v, pos - P), vp1 = L(v, pos + P), vm2 = L(v, pos - 2 * P), vp2 = L(v, pos + 2 * P);
+    const double Hm1 = H[pos - P], Hp1 = H[pos + P], Hm2 = H[pos - 2 * P];
+    if (Hm1 <= p.H_TINH) {
         if (utb < 0) {
-            qq = utb * (-3 * v0 + 4 * L(v, pos + P) - L(v, pos + 2 * P)) / dX2;
-            pp = (v0 - 2 * L(v, pos + P) + L(v, pos + 2 * P)) / dXbp;
+            qq = utb * (-3 * v0 + 4 * vp1 - vp2) / dX2;
+            pp = (v0 - 2 * vp1 + vp2) / dXbp;
         }
     } else {
-        if (H[pos + P] <= p.H_TINH) {
-            if ((H[pos - 2 * P] > p.H_TINH) && (utb > 0)) {
-                qq = utb * (3 * v0 - 4 * L(v, pos - P) + L(v, pos - 2 * P)) / dX2;
-                pp = (v0 - 2 * L(v, pos - P) + L(v, pos - 2 * P)) / dXbp;
+        if (Hp1 <= p.H_TINH) {
+            if ((Hm2 > p.H_TINH) && (utb > 0)) {
+                qq = utb * (3 * v0 - 4 * vm1 + vm2) / dX2;
+                pp = (v0 - 2 * vm1 + vm2) / dXbp;
             }
         } else {
-            qq = utb * (L(v, pos + P) - L(v, pos - P)) / dX2;
-            pp = (L(v, pos + P) - 2 * v0 + L(v, pos - P)) / dXbp;
+            qq = utb * (vp1 - vm1) / dX2;
+            pp = (vp1 - 2 * v0 + vm1) / dXbp;
         }
     }
     f5 = -2 * v0 + dT * qq + dT * R(p.CORIOLIS_FORCE) * utb - dT * L(g.VISC, pos) * pp -
@@ -516,19 +523,32 @@ __device__ __forceinline__ void smooth_cell(const DevGrid& g, const DevParams& p
     if (i >= N + 3 || j >= M + 3) return;
     const double* val = isU ? g.t_u : g.t_v;
     const int gp = i * P + j;
+    const bool inner = !(i > N || j > M || i < 2 || j < 2);
+    const int close_d = isU ? P : 1, far_d = isU ? 1 : P;
+    // every load first (one memory round trip): the cell, its four neighbours and the
+    // mask of the two across the smoothing direction
     const double v0 = val[gp];
+    double vcm = 0.0, vcp = 0.0, vfm = 0.0, vfp = 0.0;
+    int kfm = 1, kfp = 1;
+    if (inner) {
+        vcm = val[gp - close_d];
+        vcp = val[gp + close_d];
+        vfm = val[gp - far_d];
+        vfp = val[gp + far_d];
+        kfm = g.khouot[gp - far_d];
+        kfp = g.khouot[gp + far_d];
+    }
     double r = v0;
     if (check_span && v0 != 0 && (j < g.elo[i] || j > g.ehi[i])) *g.span_wide = 1;
-    if (!(i > N || j > M || i < 2 || j < 2) && v0 != 0) {
-        const int close_d = isU ? P : 1, far_d = isU ? 1 : P;
+    if (inner && v0 != 0) {
         int count = 2;
-        double nb = val[gp - close_d] + val[gp + close_d];
-        if (g.khouot[gp - far_d] == 0) {
-            nb += val[gp - far_d];
+        double nb = vcm + vcp;
+        if (kfm == 0) {
+            nb += vfm;
             count++;
         }
-        if (g.khouot[gp + far_d] == 0) {
-            nb += val[gp + far_d];
+        if (kfp == 0) {
+            nb += vfp;
             count++;
         }
         r = v0 * p.heso + (1 - p.heso) * nb / count;
@@ -543,11 +563,11 @@ __device__ __forceinline__ void reset_byte_cell(const DevGrid& g, const DevParam
     if (i >= g.N + 3 || j >= g.M + 3) return;
     const int gp = i * g.P + j;
     const int kv = g.khouot[gp];
-    const double tz = g.t_z[gp];
+    const double tz = g.t_z[gp], zc = g.z[gp], ht = g.htaiz[gp];  // loads first
     unsigned b = (unsigned)kv;
-    if (i >= 2 && i <= g.N && tz > g.z[gp]) b |= 4u;
+    if (i >= 2 && i <= g.N && tz > zc) b |= 4u;
     if (kv == 0 && i >= 1 && i <= g.N && j >= 1 && j <= g.M) {
-        const double hv = g.htaiz[gp] + tz;
+        const double hv = ht + tz;
         g.H_moi[gp] = hv;
         if (i >= 2 && hv <= p.H_TINH) b |= 8u;
     }
