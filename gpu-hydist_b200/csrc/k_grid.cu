@@ -741,20 +741,24 @@ __device__ __forceinline__ R ev_cell(const DevGrid& g, const DevParams& p, int r
     const R t_utb = (L(t_u, (row - 1) * o + col) + L(t_u, row * o + col) + L(t_u, (row - 1) * o + col + 1) + L(t_u, row * o + col + 1)) * R(0.25);
     pp = (L(v, row * o + col + 1) - L(v, row * o + col - 1)) / R(p.dY2);
     pp = R(p.HaiChiadT) + pp + L(g.Ky1, row * o + col) * sqrt(utb * utb + v0 * v0) / L(g.Htdv, row * o + col);
-    if (H[(row - 1) * o + col] <= p.H_TINH) {
+    // the neighbours the branches take, loaded before the depth tests (one round trip)
+    const R vm1 = L(v, (row - 1) * o + col), vp1 = L(v, (row + 1) * o + col), vm2 = L(v, (row - 2) * o + col),
+            vp2 = L(v, (row + 2) * o + col);
+    const double Hm1 = H[(row - 1) * o + col], Hp1 = H[(row + 1) * o + col], Hm2 = H[(row - 2) * o + col];
+    if (Hm1 <= p.H_TINH) {
         if (utb < 0) {
-            q = t_utb * (-3 * v0 + 4 * L(v, (row + 1) * o + col) - L(v, (row + 2) * o + col)) / R(p.dX2);
-            tmp = (v0 - 2 * L(v, (row + 1) * o + col) + L(v, (row + 2) * o + col)) / R(p.dXbp);
+            q = t_utb * (-3 * v0 + 4 * vp1 - vp2) / R(p.dX2);
+            tmp = (v0 - 2 * vp1 + vp2) / R(p.dXbp);
         }
     } else {
-        if (H[(row + 1) * o + col] <= p.H_TINH) {
-            if ((H[(row - 2) * o + col] > p.H_TINH) && (utb > 0)) {
-                q = t_utb * (3 * v0 - 4 * L(v, (row - 1) * o + col) + L(v, (row - 2) * o + col)) / R(p.dX2);
-                tmp = (v0 - 2 * L(v, (row - 1) * o + col) + L(v, (row - 2) * o + col)) / R(p.dXbp);
+        if (Hp1 <= p.H_TINH) {
+            if ((Hm2 > p.H_TINH) && (utb > 0)) {
+                q = t_utb * (3 * v0 - 4 * vm1 + vm2) / R(p.dX2);
+                tmp = (v0 - 2 * vm1 + vm2) / R(p.dXbp);
             }
         } else {
-            q = t_utb * (L(v, (row + 1) * o + col) - L(v, (row - 1) * o + col)) / R(p.dX2);
-            tmp = (L(v, (row + 1) * o + col) - 2 * v0 + L(v, (row - 1) * o + col)) / R(p.dXbp);
+            q = t_utb * (vp1 - vm1) / R(p.dX2);
+            tmp = (vp1 - 2 * v0 + vm1) / R(p.dXbp);
         }
     }
     q = R(p.HaiChiadT) * v0 - q - R(p.CORIOLIS_FORCE) * t_utb;
@@ -851,20 +855,24 @@ __device__ __forceinline__ R eu_cell(const DevGrid& g, const DevParams& p, int r
     const R t_vtb = (L(t_v, row * o + col - 1) + L(t_v, row * o + col) + L(t_v, (row + 1) * o + col - 1) + L(t_v, (row + 1) * o + col)) * R(0.25);
     pp = (L(u, (row + 1) * o + col) - L(u, (row - 1) * o + col)) / R(p.dX2);
     pp = (R(p.HaiChiadT) + pp + L(g.Kx1, row * o + col) * sqrt(vtb * vtb + u0 * u0) / L(g.Htdu, row * o + col));
-    if (H[row * o + col - 1] <= p.H_TINH) {
+    // as in ev_cell: the branches' neighbours loaded first
+    const R um1 = L(u, row * o + col - 1), up1 = L(u, row * o + col + 1), um2 = L(u, row * o + col - 2),
+            up2 = L(u, row * o + col + 2);
+    const double Hm1 = H[row * o + col - 1], Hp1 = H[row * o + col + 1], Hm2 = H[row * o + col - 2];
+    if (Hm1 <= p.H_TINH) {
         if (vtb < 0) {
-            q = t_vtb * (-3 * u0 + 4 * L(u, row * o + col + 1) - L(u, row * o + col + 2)) / R(p.dY2);
-            tmp = (u0 - 2 * L(u, row * o + col + 1) + L(u, row * o + col + 2)) / R(p.dYbp);
+            q = t_vtb * (-3 * u0 + 4 * up1 - up2) / R(p.dY2);
+            tmp = (u0 - 2 * up1 + up2) / R(p.dYbp);
         }
     } else {
-        if (H[row * o + col + 1] <= p.H_TINH) {
-            if ((H[row * o + col - 2] > p.H_TINH) && (vtb > 0)) {
-                q = t_vtb * (3 * u0 - 4 * L(u, row * o + col - 1) + L(u, row * o + col - 2)) / R(p.dY2);
-                tmp = (u0 - 2 * L(u, row * o + col - 1) + L(u, row * o + col - 2)) / R(p.dYbp);
+        if (Hp1 <= p.H_TINH) {
+            if ((Hm2 > p.H_TINH) && (vtb > 0)) {
+                q = t_vtb * (3 * u0 - 4 * um1 + um2) / R(p.dY2);
+                tmp = (u0 - 2 * um1 + um2) / R(p.dYbp);
             }
         } else {
-            q = t_vtb * (L(u, row * o + col + 1) - L(u, row * o + col - 1)) / R(p.dY2);
-            tmp = (L(u, row * o + col + 1) - 2 * u0 + L(u, row * o + col - 1)) / R(p.dYbp);
+            q = t_vtb * (up1 - um1) / R(p.dY2);
+            tmp = (up1 - 2 * u0 + um1) / R(p.dYbp);
         }
     }
     q = R(p.HaiChiadT) * u0 - q + R(p.CORIOLIS_FORCE) * t_vtb;
