@@ -438,7 +438,10 @@ __device__ __forceinline__ void vz_cell_coeffs(const DevGrid& g, const DevParams
 // and gridDim.x of a launch for one grid; a member's share of a batched launch).
 template <int KIND, int TILE, class R>
 __device__ __forceinline__ void coef_bnd_body(const DevGrid& g, const DevParams& p, int writes, int bx, int gx) {
-    if (bx == gx - 1) {
+    // CTA 0 takes the clock and the boundary (a chain of dependent loads, started first
+    // so that it runs beside the coefficient CTAs instead of after them); the others the
+    // coefficients
+    if (bx == 0) {
         __shared__ double s_t;
         if (threadIdx.x == 0) {
             if (KIND == 0) {  // k_clock
@@ -457,6 +460,7 @@ __device__ __forceinline__ void coef_bnd_body(const DevGrid& g, const DevParams&
         else boundary_body(g, s_t, writes);
         return;
     }
+    bx -= 1;
     if constexpr (KIND == 0 && TILE) {
         R* const dst[7] = {colTr<R>(g, 0), colTr<R>(g, 1), colTr<R>(g, 2), colTr<R>(g, 3),
                            colTr<R>(g, 4), colTr<R>(g, 5), colTr<R>(g, 6)};
@@ -686,22 +690,28 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
     if (BYTES) reset_byte_cell(g, p, i, j);
 }
 
-// FSB: one more CTA (the last) applies the concentration part of the second half-step's
+// FSB: one more CTA (the first) applies the concentration part of the second half-step's
 // boundary (kBndFS), when the velocity/level part ran before the first half-step's
 // sediment sweep had finished.
-// BUD: 4 kEdgeCtas more CTAs (the last) add the half-step's open-edge volumes to the
+// BUD: 4 kEdgeCtas more CTAs (the first) add the half-step's open-edge volumes to the
 // budget (edge_budget; the smoothing of the swept velocity, isU = the UZ sweep's half-step).
 template <int BYTES, int FSB, int BUD>
 __device__ __forceinline__ void smooth_span_body(const DevGrid& g, const DevParams& p, int isU,
                                                  double* __restrict__ out, int bx, int gx) {
-    if (BUD && bx >= gx - 4 * kEdgeCtas) {
-        const int q = bx - (gx - 4 * kEdgeCtas);
-        edge_budget(g, p, isU, q / kEdgeCtas, q % kEdgeCtas);
-        return;
+    // the budget and boundary CTAs (chains of dependent loads) first, beside the smoothing
+    if (BUD) {
+        if (bx < 4 * kEdgeCtas) {
+            edge_budget(g, p, isU, bx / kEdgeCtas, bx % kEdgeCtas);
+            return;
+        }
+        bx -= 4 * kEdgeCtas;
     }
-    if (FSB && bx == gx - 1) {
-        boundary_body(g, g.clock[1], kBndFS);
-        return;
+    if (FSB) {
+        if (bx == 0) {
+            boundary_body(g, g.clock[1], kBndFS);
+            return;
+        }
+        bx -= 1;
     }
     const RowLane rl(g, 0, bx);
     const int i = rl.i;
@@ -1720,30 +1730,33 @@ __device__ __forceinline__ void post_vth_cell(const DevGrid& g, const DevParams&
 }
 
 // After a half-step's reset, in one launch: the state update (update_uvz + Htuongdoi)
-// and, when VTH, Find_VTH + hesoK on the extended spans (CTAs [0, nbp), one warp per
-// row; both only read the cell's own new Htdu/Htdv); the rescan of the changed lines of
-// the other direction (CTAs [nbp, nbp + nbs)); and the edge concentration interpolation
-// (the last kEdgeParts CTAs, reading t_u / t_v where the reference reads u / v after the
-// update).  None of the three writes what another reads.
+// and, when VTH, Find_VTH + hesoK on the extended spans (nbp CTAs, one warp per row; both
+// only read the cell's own new Htdu/Htdv); the rescan of the changed lines of the other
+// direction (nbs CTAs); and the edge concentration interpolation (kEdgeParts CTAs,
+// reading t_u / t_v where the reference reads u / v after the update).  None of the
+// three writes what another reads.
 constexpr int kEdgeParts = 8;
 template <int ROWS, int VTH, class R>
 __device__ __forceinline__ void post_fused_body(const DevGrid& g, const DevParams& p, int nbp, int nbs, int bx,
                                                 int gx) {
     extern __shared__ unsigned swords[];
+    // CTAs [0, kEdgeParts) the edge interpolation and [kEdgeParts, kEdgeParts + nbs) the
+    // rescans (chains of dependent loads, started first so that they run beside the state
+    // update), then the nbp state-update CTAs
     const int b = bx;
-    if (b < nbp) {
-        const RowLane rl(g, 0, bx);
+    if (b < kEdgeParts) {
+        fs_edges_part<0>(g, p, b, kEdgeParts);
+        return;
+    }
+    if (b >= kEdgeParts + nbs) {
+        const RowLane rl(g, 0, b - kEdgeParts - nbs);
         const int i = rl.i;
         if (i > g.N) return;
         // rows: the second half-step, with the FSi terms
         for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) post_vth_cell<VTH, ROWS, R>(g, p, i, j);
         return;
     }
-    if (b >= gx - kEdgeParts) {
-        fs_edges_part<0>(g, p, b - (gx - kEdgeParts), kEdgeParts);
-        return;
-    }
-    const int sb = b - nbp;
+    const int sb = b - kEdgeParts;
     {
         const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int n = *(volatile unsigned*)&g.dctr[ROWS ? 0 : 1];

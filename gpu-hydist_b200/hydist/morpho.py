@@ -32,7 +32,7 @@ import numpy as np
 
 from . import cases
 from . import surrogate as S
-from .lib import Simulation
+from .lib import HydError, Simulation
 
 H_REF, N_REF, Q_REF, STAGE_REF, DZ_REF = 8.0, 0.025, 700.0, 0.3, 0.1
 # trust region of one jump: the surrogate's increments are clipped to these (m/s, m/s, m)
@@ -273,16 +273,22 @@ class QuasiSteady:
         sim.set_time(t_end - self.warm * dT)
         sim.steady_residual(snapshot=True)
         r = (math.inf, math.inf)
-        for k in range(1, self.warm):
-            sim.step(1)
-            r = sim.steady_residual(snapshot=True)
-            if k >= self.min_warm and max(r) < self.gate and sim.mass_balance()["nonfinite"] == 0:
-                sim.set_time(t_end - dT)
-                sim.step(1)  # the period's last step: the bed update on the accepted state
-                self.accepted += 1
-                self.steps += k + 1
-                self.residuals.append(max(r))
-                return True, k + 1
+        try:
+            for k in range(1, self.warm):
+                sim.step(1)
+                r = sim.steady_residual(snapshot=True)
+                if k >= self.min_warm and max(r) < self.gate and sim.mass_balance()["nonfinite"] == 0:
+                    sim.set_time(t_end - dT)
+                    sim.step(1)  # the period's last step: the bed update on the accepted state
+                    self.accepted += 1
+                    self.steps += k + 1
+                    self.residuals.append(max(r))
+                    return True, k + 1
+        except HydError:
+            # a device check failed on the jumped state (e.g. its levels flooded a bank in
+            # patches and a line passed 20 wet segments): rejected like a state that is not
+            # steady; the checkpoint holds the device status of before the jump
+            r = (math.inf, math.inf)
         # not steady within the warm steps: back to the checkpoint, the period stepped plainly
         sim.restore()
         sim.step(nper)
