@@ -475,10 +475,14 @@ __device__ __forceinline__ void coef_bnd_body(const DevGrid& g, const DevParams&
             dst);
         return;
     }
-    const int i = 2 + ((bx * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    // rows 2..N, wpr warps per row (as many as the launch's CTAs give: g.wpr from
+    // launch_coef_bnd, one in a batched launch), lanes striding over the row's cells
+    const int wpr = max(1, ((gx - 1) * (int)(blockDim.x >> 5)) / max(g.N - 1, 1));
+    const int gw = (bx * (int)blockDim.x + (int)threadIdx.x) >> 5;
+    const int i = 2 + gw / wpr, off = (gw % wpr) * 32 + (threadIdx.x & 31), stride = wpr * 32;
     if (i > g.N) return;
     const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
-    for (int j = lo + lane; j <= hi; j += 32) {
+    for (int j = lo + off; j <= hi; j += stride) {
         const int pos = i * g.P + j;
         if (g.khouot[pos] != 0) continue;
         R a2, c2, d2, f1, f2, f3, f5;
@@ -2284,15 +2288,17 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
 
 
 void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
+    // the tiled form: kTileRows rows per CTA; the row form: g.wpr warps per row
     const int nb = ((g.N - 1) * 32 + 255) / 256 + 1;
+    const int nbr = row_warp_ctas(g, g.N - 1) + 1;
     if (p.mixed) {
-        if (half == 1) k_coef_bnd<1, 0, float><<<nb, 256, 0, s>>>(g, p, writes);
+        if (half == 1) k_coef_bnd<1, 0, float><<<nbr, 256, 0, s>>>(g, p, writes);
         else if (g.tile_cols) k_coef_bnd<0, 1, float><<<nb, 256, 0, s>>>(g, p, writes);
-        else k_coef_bnd<0, 0, float><<<nb, 256, 0, s>>>(g, p, writes);
+        else k_coef_bnd<0, 0, float><<<nbr, 256, 0, s>>>(g, p, writes);
     } else {
-        if (half == 1) k_coef_bnd<1, 0, double><<<nb, 256, 0, s>>>(g, p, writes);
+        if (half == 1) k_coef_bnd<1, 0, double><<<nbr, 256, 0, s>>>(g, p, writes);
         else if (g.tile_cols) k_coef_bnd<0, 1, double><<<nb, 256, 0, s>>>(g, p, writes);
-        else k_coef_bnd<0, 0, double><<<nb, 256, 0, s>>>(g, p, writes);
+        else k_coef_bnd<0, 0, double><<<nbr, 256, 0, s>>>(g, p, writes);
     }
     hyd_kernel_launches_add(1);
 }

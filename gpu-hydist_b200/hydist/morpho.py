@@ -241,35 +241,31 @@ class QuasiSteady:
     """The quasi-steady morphodynamic loop on one Simulation (see the module docstring).
 
     period(): advance one bed period; returns (accepted, plain steps taken).  The gate is
-    read after each of the first `warm` - 1 warm steps from the `min_warm`-th on.
-    Counters: accepted, fallbacks, steps."""
+    read after each of the first `warm` - 1 warm steps from the `min_warm`-th on.  With a
+    jump, a rejected jump is followed by one more try from the checkpoint without it
+    (`retry`), before the period is stepped plainly.  Counters: accepted (of them
+    jump_accepted with the jump), fallbacks, steps."""
 
-    def __init__(self, sim, case, warm=20, gate=1e-4, jump=None, min_warm=1):
+    def __init__(self, sim, case, warm=20, gate=1e-4, jump=None, min_warm=1, retry=True):
         self.sim = sim
         self.case = case
         self.warm = int(warm)
         self.min_warm = max(1, min(int(min_warm), self.warm - 1))
         self.gate = float(gate)
         self.jump = jump
+        self.retry = retry
         self.period_s = float(case.params.bed_period)
         self.accepted = 0
+        self.jump_accepted = 0
         self.fallbacks = 0
         self.steps = 0
         self.residuals = []
 
-    def period(self):
+    def _warm(self, t_end):
+        """The warm steps from the current state; True (and the period's last step taken)
+        once the gate passes; the residual reached otherwise."""
         sim = self.sim
         dT = sim.params.dT
-        t0 = sim.t
-        t_end = t0 + self.period_s
-        nper = int(round(self.period_s / dT))
-        sim.checkpoint()
-        if self.jump is not None:
-            Q, st = forcing_at(self.case, t_end)
-            inc = self.jump.increments(sim, Q, st)
-            if inc is not None:
-                i0, _, j0, _ = self.jump.crop
-                sim.add_levels(*inc, i0, j0)
         sim.set_time(t_end - self.warm * dT)
         sim.steady_residual(snapshot=True)
         r = (math.inf, math.inf)
@@ -280,22 +276,48 @@ class QuasiSteady:
                 if k >= self.min_warm and max(r) < self.gate and sim.mass_balance()["nonfinite"] == 0:
                     sim.set_time(t_end - dT)
                     sim.step(1)  # the period's last step: the bed update on the accepted state
-                    self.accepted += 1
                     self.steps += k + 1
                     self.residuals.append(max(r))
-                    return True, k + 1
+                    return True, r
         except HydError:
-            # a device check failed on the jumped state (e.g. its levels flooded a bank in
-            # patches and a line passed 20 wet segments): rejected like a state that is not
-            # steady; the checkpoint holds the device status of before the jump
+            # a device check failed on the warm-started state (e.g. jumped levels flooded a
+            # bank in patches and a line passed 20 wet segments): rejected like a state that
+            # is not steady; the checkpoint holds the device status of before the jump
             r = (math.inf, math.inf)
+        self.steps += self.warm - 1
+        return False, r
+
+    def period(self):
+        sim = self.sim
+        dT = sim.params.dT
+        t_end = sim.t + self.period_s
+        nper = int(round(self.period_s / dT))
+        steps0 = self.steps
+        sim.checkpoint()
+        jumped = False
+        if self.jump is not None:
+            Q, st = forcing_at(self.case, t_end)
+            inc = self.jump.increments(sim, Q, st)
+            if inc is not None:
+                i0, _, j0, _ = self.jump.crop
+                sim.add_levels(*inc, i0, j0)
+                jumped = True
+        ok, r = self._warm(t_end)
+        if not ok and jumped and self.retry:
+            sim.restore()  # the jump rejected: the previous state as the warm start
+            ok, r = self._warm(t_end)
+            jumped = False
+        if ok:
+            self.accepted += 1
+            self.jump_accepted += 1 if jumped else 0
+            return True, self.steps - steps0
         # not steady within the warm steps: back to the checkpoint, the period stepped plainly
         sim.restore()
         sim.step(nper)
         self.fallbacks += 1
-        self.steps += self.warm - 1 + nper
+        self.steps += nper
         self.residuals.append(max(r))
-        return False, self.warm - 1 + nper
+        return False, self.steps - steps0
 
     def run_until(self, t_stop):
         while self.sim.t + self.period_s <= t_stop + 1e-9:
