@@ -475,14 +475,12 @@ __device__ __forceinline__ void coef_bnd_body(const DevGrid& g, const DevParams&
             dst);
         return;
     }
-    // rows 2..N, wpr warps per row (as many as the launch's CTAs give: g.wpr from
-    // launch_coef_bnd, one in a batched launch), lanes striding over the row's cells
-    const int wpr = max(1, ((gx - 1) * (int)(blockDim.x >> 5)) / max(g.N - 1, 1));
-    const int gw = (bx * (int)blockDim.x + (int)threadIdx.x) >> 5;
-    const int i = 2 + gw / wpr, off = (gw % wpr) * 32 + (threadIdx.x & 31), stride = wpr * 32;
+    // rows 2..N, one warp per row (several warps per row measured slower on config 4:
+    // 46 -> 50 us), lanes striding over the row's cells
+    const int i = 2 + ((bx * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i > g.N) return;
     const int lo = max(g.rlo[i], 2), hi = min(g.rhi[i], g.M);
-    for (int j = lo + off; j <= hi; j += stride) {
+    for (int j = lo + lane; j <= hi; j += 32) {
         const int pos = i * g.P + j;
         if (g.khouot[pos] != 0) continue;
         R a2, c2, d2, f1, f2, f3, f5;
@@ -2288,9 +2286,9 @@ void launch_init_kernels(const DevGrid& g, const DevParams& p, const int* keep_m
 
 
 void launch_coef_bnd(const DevGrid& g, const DevParams& p, int half, int writes, cudaStream_t s) {
-    // the tiled form: kTileRows rows per CTA; the row form: g.wpr warps per row
+    // the tiled form: kTileRows rows per CTA; the row form: one warp per row (the same count)
     const int nb = ((g.N - 1) * 32 + 255) / 256 + 1;
-    const int nbr = row_warp_ctas(g, g.N - 1) + 1;
+    const int nbr = nb;
     if (p.mixed) {
         if (half == 1) k_coef_bnd<1, 0, float><<<nbr, 256, 0, s>>>(g, p, writes);
         else if (g.tile_cols) k_coef_bnd<0, 1, float><<<nb, 256, 0, s>>>(g, p, writes);
