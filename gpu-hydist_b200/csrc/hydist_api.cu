@@ -1469,7 +1469,6 @@ int hyd_mass_budget(hyd_handle h, double* out, int n) {
     out[4] = b[kBudClose] * area;
     out[5] = b[kBudBed] * area;
     if (n > 10) out[10] = b[kBudJump] * area;
-    if (n > 11) out[11] = b[kBudLeak];
     return HYD_OK;
 }
 

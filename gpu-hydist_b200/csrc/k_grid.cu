@@ -678,43 +678,6 @@ __device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int
     *count = 0u;  // ready for the next half-step (stream order separates the launches)
 }
 
-// The water a half-step's continuity rows move through interior faces between a cell the
-// sweep solved and one it did not (a dry or land cell, khouot != 0), for wet cell (i, j)
-// of [2,N] x [2,M] (m^3, out of the solved cells positive).  The faces across the sweep
-// direction carry the explicit velocity (UZ half-step: v at the y faces, VZ half-step: u
-// at the x faces); a row's term for such a face has no counterpart in the unsolved cell,
-// so the volume leaves (or enters) the wet set there.  The faces along the sweep have the
-// segment ends' boundary velocities (0 at a wall), and faces on the domain's edges are
-// edge_budget's.
-__device__ __forceinline__ double leak_cell(const DevGrid& g, const DevParams& p, int isU, int i, int j) {
-    const int N = g.N, M = g.M, P = g.P;
-    if (i < 2 || i > N || j < 2 || j > M) return 0.0;
-    const int gp = i * P + j;
-    if (g.khouot[gp] != 0) return 0.0;
-    double q = 0.0;
-    if (isU) {
-        if (j + 1 <= M && g.khouot[gp + 1] != 0) q += g.Htdv[gp] * g.v[gp];
-        if (j - 1 >= 2 && g.khouot[gp - 1] != 0) q -= g.Htdv[gp - 1] * g.v[gp - 1];
-        return q * p.dX * (p.dT * 0.5);
-    }
-    if (i + 1 <= N && g.khouot[gp + P] != 0) q += g.Htdu[gp] * g.u[gp];
-    if (i - 1 >= 2 && g.khouot[gp - P] != 0) q -= g.Htdu[gp - P] * g.u[gp - P];
-    return q * p.dY * (p.dT * 0.5);
-}
-
-// A warp's leak sum added to the budget (one atomic per warp that has one).
-__device__ __forceinline__ void add_leak(const DevGrid& g, double q) {
-    for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
-    if ((threadIdx.x & 31) == 0 && q != 0.0) atomicAdd(&g.budget[kBudLeak], q);
-}
-
-// The leak term over the whole grid (after a whole-grid smoothing pass).
-__global__ void k_leak_full(DevGrid g, DevParams p, int isU) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
-    add_leak(g, (i < g.N + 3 && j < g.M + 3) ? leak_cell(g, p, isU, i, j) : 0.0);
-}
-
 // The edge budget alone (after a whole-grid smoothing pass): kEdgeCtas CTAs per edge.
 __global__ void k_edge_budget(DevGrid g, DevParams p, int half1) {
     edge_budget(g, p, half1, blockIdx.x / kEdgeCtas, blockIdx.x % kEdgeCtas);
@@ -754,15 +717,11 @@ __device__ __forceinline__ void smooth_span_body(const DevGrid& g, const DevPara
     }
     const RowLane rl(g, 0, bx);
     const int i = rl.i;
-    double leak = 0.0;
-    if (i <= g.N + 2) {
-        for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
-            smooth_cell(g, p, isU, out, i, j, false);
-            if (BYTES) reset_byte_cell(g, p, i, j);
-            if (BUD) leak += leak_cell(g, p, isU, i, j);
-        }
+    if (i > g.N + 2) return;
+    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
+        smooth_cell(g, p, isU, out, i, j, false);
+        if (BYTES) reset_byte_cell(g, p, i, j);
     }
-    if (BUD) add_leak(g, leak);  // every lane of the warp takes part
 }
 
 template <int BYTES, int FSB, int BUD>
@@ -2353,8 +2312,7 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
         else k_smooth<0><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         if (budget) {  // the smoothing reads the swept velocity and writes elsewhere
             k_edge_budget<<<4 * kEdgeCtas, 256, 0, s>>>(g, p, isU);
-            k_leak_full<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU);
-            hyd_kernel_launches_add(2);
+            hyd_kernel_launches_add(1);
         }
     } else {
         const int nb = row_warps_blocks(g, g.N + 3);
