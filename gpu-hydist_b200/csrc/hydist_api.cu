@@ -1469,6 +1469,7 @@ int hyd_mass_budget(hyd_handle h, double* out, int n) {
     out[4] = b[kBudClose] * area;
     out[5] = b[kBudBed] * area;
     if (n > 10) out[10] = b[kBudJump] * area;
+    if (n > 11) out[11] = b[kBudLeak];
     return HYD_OK;
 }
 
@@ -1819,7 +1820,7 @@ int fused_build(HydBatch* b) {
         const int N = s->N, M = s->M;
         const int rw = row_warp_ctas(g0, N + 3);
         counts[BP_CB].push_back(((N - 1) * 32 + 255) / 256 + 1);
-        counts[BP_SM_BUD].push_back(rw + 4 * kEdgeCtas);
+        counts[BP_SM_BUD].push_back(rw + kBudCtas);
         counts[BP_SM].push_back(rw);
         counts[BP_SM_FSB].push_back(rw + 1);
         counts[BP_EV].push_back(N - 1);

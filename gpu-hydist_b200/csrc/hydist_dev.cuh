@@ -96,8 +96,10 @@ struct DevGrid {
 // 2 (e kEdgeCtas + c); the last CTA of the edge to finish (counted in the unsigned words
 // at kBudCount) adds the partials in CTA order to the edge's Kahan sums.
 constexpr int kBudNet = 0, kBudNetC = 4, kBudIn = 8, kBudInC = 12, kBudOut = 16, kBudOutC = 20;
-constexpr int kBudOpen = 24, kBudClose = 25, kBudBed = 26, kBudJump = 27;
+constexpr int kBudOpen = 24, kBudClose = 25, kBudBed = 26, kBudJump = 27, kBudLeak = 28;
 constexpr int kEdgeCtas = 8, kBudPart = 32, kBudCount = kBudPart + 8 * kEdgeCtas, kBudSlots = kBudCount + 4;
+// the budget CTAs of a half-step: kEdgeCtas per edge
+constexpr int kBudCtas = 4 * kEdgeCtas;
 
 __device__ __forceinline__ void flag_status(const DevGrid& g, unsigned bit) { atomicOr(g.status, bit); }
 

@@ -678,6 +678,50 @@ __device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int
     *count = 0u;  // ready for the next half-step (stream order separates the launches)
 }
 
+// The water a half-step's continuity rows move between a cell the sweep solved and a wet
+// cell it did not, for cell (i, j) of [2,N] x [2,M] (m^3, out of the solved cells
+// positive).  The segment scan skips a wet run that starts at the line's last two cells
+// (Find_Calculation_limits, support_funcs.cu:230-335), so a wet cell of rows N-1..N (the
+// UZ sweep's columns) or of columns M-1..M (the VZ sweep's rows) can lie in no segment;
+// its neighbours across the sweep still carry their face flux to it (the explicit v in the
+// UZ half-step, u in the VZ half-step), which the unsolved cell does not receive.  (The
+// same faces towards a dry or land cell carry no flux: the velocities there are zero.)
+// Faces on the domain's edges are edge_budget's.
+__device__ __forceinline__ double leak_cell(const DevGrid& g, const DevParams& p, int isU, int i, int j) {
+    const int N = g.N, M = g.M, P = g.P;
+    if (i < 2 || i > N || j < 2 || j > M) return 0.0;
+    if (isU ? i < N - 1 : j < M - 1) return 0.0;
+    const int gp = i * P + j;
+    if (g.khouot[gp] != 0) return 0.0;
+    int f, l;
+    double q = 0.0;
+    if (isU) {
+        if (find_seg_u(g, i, j, f, l) < 0) return 0.0;
+        if (j + 1 <= M && g.khouot[gp + 1] == 0 && find_seg_u(g, i, j + 1, f, l) < 0) q += g.Htdv[gp] * g.v[gp];
+        if (j - 1 >= 2 && g.khouot[gp - 1] == 0 && find_seg_u(g, i, j - 1, f, l) < 0)
+            q -= g.Htdv[gp - 1] * g.v[gp - 1];
+        return q * p.dX * (p.dT * 0.5);
+    }
+    if (find_seg_v(g, i, j, f, l) < 0) return 0.0;
+    if (i + 1 <= N && g.khouot[gp + P] == 0 && find_seg_v(g, i + 1, j, f, l) < 0) q += g.Htdu[gp] * g.u[gp];
+    if (i - 1 >= 2 && g.khouot[gp - P] == 0 && find_seg_v(g, i - 1, j, f, l) < 0) q -= g.Htdu[gp - P] * g.u[gp - P];
+    return q * p.dY * (p.dT * 0.5);
+}
+
+// A warp's leak sum added to the budget (one atomic per warp that has one).
+
+__device__ __forceinline__ void add_leak(const DevGrid& g, double q) {
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
+    if ((threadIdx.x & 31) == 0 && q != 0.0) atomicAdd(&g.budget[kBudLeak], q);
+}
+
+// The leak term over the whole grid (after a whole-grid smoothing pass).
+__global__ void k_leak_full(DevGrid g, DevParams p, int isU) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    add_leak(g, (i < g.N + 3 && j < g.M + 3) ? leak_cell(g, p, isU, i, j) : 0.0);
+}
+
 // The edge budget alone (after a whole-grid smoothing pass): kEdgeCtas CTAs per edge.
 __global__ void k_edge_budget(DevGrid g, DevParams p, int half1) {
     edge_budget(g, p, half1, blockIdx.x / kEdgeCtas, blockIdx.x % kEdgeCtas);
@@ -695,8 +739,9 @@ __global__ void k_smooth(DevGrid g, DevParams p, int isU, double* __restrict__ o
 // FSB: one more CTA (the first) applies the concentration part of the second half-step's
 // boundary (kBndFS), when the velocity/level part ran before the first half-step's
 // sediment sweep had finished.
-// BUD: 4 kEdgeCtas more CTAs (the first) add the half-step's open-edge volumes to the
-// budget (edge_budget; the smoothing of the swept velocity, isU = the UZ sweep's half-step).
+// BUD: kBudCtas more CTAs (the first) add the half-step's open-edge volumes to the budget
+// (edge_budget; the smoothing of the swept velocity, isU = the UZ sweep's half-step); the
+// smoothing warps add the flows to wet cells in no segment (leak_cell).
 template <int BYTES, int FSB, int BUD>
 __device__ __forceinline__ void smooth_span_body(const DevGrid& g, const DevParams& p, int isU,
                                                  double* __restrict__ out, int bx, int gx) {
@@ -706,7 +751,7 @@ __device__ __forceinline__ void smooth_span_body(const DevGrid& g, const DevPara
             edge_budget(g, p, isU, bx / kEdgeCtas, bx % kEdgeCtas);
             return;
         }
-        bx -= 4 * kEdgeCtas;
+        bx -= kBudCtas;
     }
     if (FSB) {
         if (bx == 0) {
@@ -717,11 +762,15 @@ __device__ __forceinline__ void smooth_span_body(const DevGrid& g, const DevPara
     }
     const RowLane rl(g, 0, bx);
     const int i = rl.i;
-    if (i > g.N + 2) return;
-    for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
-        smooth_cell(g, p, isU, out, i, j, false);
-        if (BYTES) reset_byte_cell(g, p, i, j);
+    double leak = 0.0;
+    if (i <= g.N + 2) {
+        for (int j = g.elo[i] + rl.off; j <= g.ehi[i]; j += rl.stride) {
+            smooth_cell(g, p, isU, out, i, j, false);
+            if (BYTES) reset_byte_cell(g, p, i, j);
+            if (BUD) leak += leak_cell(g, p, isU, i, j);
+        }
     }
+    if (BUD) add_leak(g, leak);  // every lane of the warp takes part
 }
 
 template <int BYTES, int FSB, int BUD>
@@ -2311,14 +2360,15 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
         if (bytes) k_smooth<1><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         else k_smooth<0><<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU, out);
         if (budget) {  // the smoothing reads the swept velocity and writes elsewhere
-            k_edge_budget<<<4 * kEdgeCtas, 256, 0, s>>>(g, p, isU);
-            hyd_kernel_launches_add(1);
+            k_edge_budget<<<kBudCtas, 256, 0, s>>>(g, p, isU);
+            k_leak_full<<<grid2d(g.M + 3, g.N + 3, b), b, 0, s>>>(g, p, isU);
+            hyd_kernel_launches_add(2);
         }
     } else {
         const int nb = row_warps_blocks(g, g.N + 3);
         if (bytes && fs_bnd) k_smooth_span<1, 1, 0><<<nb + 1, 256, 0, s>>>(g, p, isU, out);
         else if (bytes) k_smooth_span<1, 0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
-        else if (budget) k_smooth_span<0, 0, 1><<<nb + 4 * kEdgeCtas, 256, 0, s>>>(g, p, isU, out);
+        else if (budget) k_smooth_span<0, 0, 1><<<nb + kBudCtas, 256, 0, s>>>(g, p, isU, out);
         else k_smooth_span<0, 0, 0><<<nb, 256, 0, s>>>(g, p, isU, out);
     }
     hyd_kernel_launches_add(1);

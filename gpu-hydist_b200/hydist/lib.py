@@ -290,10 +290,10 @@ class Simulation:
         through the edges, volumes of the cells opened and closed by the wet/dry resets, the
         volume fed-back bed changes added to the depths, and the net per edge (up, down,
         left, right)."""
-        out = np.zeros(11)
-        _check(self.lib.hyd_mass_budget(self.h, out.ctypes.data, 11))
+        out = np.zeros(12)
+        _check(self.lib.hyd_mass_budget(self.h, out.ctypes.data, 12))
         return {"net_in": out[0], "gross_in": out[1], "gross_out": out[2], "opened": out[3], "closed": out[4],
-                "bed": out[5], "edge_net": out[6:10].copy(), "added": out[10]}
+                "bed": out[5], "edge_net": out[6:10].copy(), "added": out[10], "leak": out[11]}
 
     # quasi-steady support: device checkpoint, time, steady residual, level increments
     def checkpoint(self):

@@ -123,7 +123,8 @@ int main(void) {
     CHECK(hyd_mass_balance(sim, vol1, 5));
     CHECK(hyd_mass_budget(sim, b1, HYD_BUDGET_SLOTS));
     const double dv = vol1[0] - vol0[0];
-    const double pred = (b1[0] - b0[0]) + (b1[3] - b0[3]) - (b1[4] - b0[4]) + (b1[5] - b0[5]);
+    const double pred = (b1[0] - b0[0]) + (b1[3] - b0[3]) - (b1[4] - b0[4]) + (b1[5] - b0[5]) + (b1[10] - b0[10]) -
+                        (b1[11] - b0[11]);
     const double rel = fabs(dv - pred) / vol1[0];
     if (!(rel <= 1e-10) || vol1[4] != 0) {
         fprintf(stderr, "water budget: dV %.6e, budget %.6e, rel %.3e, non-finite %g\n", dv, pred, rel, vol1[4]);

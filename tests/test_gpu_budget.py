@@ -35,7 +35,8 @@ def _closure(sim, steps, chunk):
         b = sim.mass_budget()
         dv = mb["volume"] - v0
         net = b["net_in"] - b0["net_in"]
-        wd = (b["opened"] - b0["opened"]) - (b["closed"] - b0["closed"]) + (b["bed"] - b0["bed"])
+        wd = (b["opened"] - b0["opened"]) - (b["closed"] - b0["closed"]) + (b["bed"] - b0["bed"]) - (
+            b["leak"] - b0["leak"])
         err = abs(dv - net - wd) / mb["volume"]
         err_bnd = abs(dv - net) / mb["volume"]
         worst = max(worst, err)

@@ -104,7 +104,7 @@ def test_mixed_vs_fp64(name, steps):
     mb = b.mass_balance()
     bb = b.mass_budget()
     pred = (bb["net_in"] - b0["net_in"]) + (bb["opened"] - b0["opened"]) - (bb["closed"] - b0["closed"]) + (
-        bb["bed"] - b0["bed"])
+        bb["bed"] - b0["bed"]) - (bb["leak"] - b0["leak"])
     closure = abs(mb["volume"] - v0 - pred) / mb["volume"]
     vol_rel = abs(mb["volume"] - a.mass_balance()["volume"]) / a.mass_balance()["volume"]
     _report("%s mixed vs FP64 at t = %d s (closure %.2e, volume rel diff %.2e)" % (name, steps, closure, vol_rel),

@@ -110,7 +110,7 @@ def _run_24h(precision):
         b = sim.mass_budget()
         dv = mb["volume"] - v0
         pred = (b["net_in"] - b0["net_in"]) + (b["opened"] - b0["opened"]) - (b["closed"] - b0["closed"]) + (
-            b["bed"] - b0["bed"])
+            b["bed"] - b0["bed"]) - (b["leak"] - b0["leak"])
         worst = max(worst, abs(dv - pred) / mb["volume"])
     wall = time.perf_counter() - t0
     assert sim.t == 86400.0
