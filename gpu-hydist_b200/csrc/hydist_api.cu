@@ -1374,10 +1374,9 @@ int hyd_checkpoint(hyd_handle h, int restore) {
     return set_clock(h, h->t);  // synchronises the stream
 }
 
-int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n) {
-    if (!h || !out || n < 2) return fail(HYD_EINVAL, "need 2 output slots");
-    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_steady_residual");
-    CUDA_TRY(cudaSetDevice(h->device));
+// The steady residual; with `status`, the device status word is read back in the same
+// synchronisation (the quasi-steady period's warm steps run without a check of their own).
+static int steady_residual(HydSim* h, int snapshot, double* out, unsigned* status) {
     const size_t field = (size_t)(h->N + 3) * h->pitch;
     const int nb = 2 * 148;
     if (!h->res_buf) {
@@ -1389,6 +1388,7 @@ int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n) {
     CUDA_TRY(cudaGetLastError());
     double sums[4];
     CUDA_TRY(cudaMemcpyAsync(sums, tot, sizeof sums, cudaMemcpyDeviceToHost, h->stream));
+    if (status) CUDA_TRY(cudaMemcpyAsync(status, h->g.status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (!h->res_valid || !(sums[1] > 0) || !(sums[3] > 0)) {
         out[0] = out[1] = HUGE_VAL;  // no snapshot yet, no wet cell or no flow: not steady
@@ -1399,6 +1399,93 @@ int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n) {
         if (!std::isfinite(out[1])) out[1] = HUGE_VAL;
     }
     if (snapshot) h->res_valid = 1;
+    return HYD_OK;
+}
+
+int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n) {
+    if (!h || !out || n < 2) return fail(HYD_EINVAL, "need 2 output slots");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_steady_residual");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return steady_residual(h, snapshot, out, nullptr);
+}
+
+int hyd_quasi_steady_period(hyd_handle h, double period, int warm, int min_warm, double gate, const float* du,
+                            const float* dv, const float* dz, int i0, int j0, int rows, int cols, long long ld,
+                            int retry, int* result) {
+    if (!h || !result) return fail(HYD_EINVAL, "null argument");
+    if (!h->initialized) return fail(HYD_ESTATE, "hyd_init must precede hyd_quasi_steady_period");
+    const double dT = h->P.dT;
+    if (!(period > 0) || warm < 2) return fail(HYD_EINVAL, "period must be > 0 and warm >= 2");
+    const long long nper = llround(period / dT);
+    if (nper < warm || std::fabs((double)nper * dT - period) > 1e-9 * period)
+        return fail(HYD_EINVAL, "period must be a whole number of steps, at least warm");
+    if (min_warm < 1) min_warm = 1;
+    if (min_warm > warm - 1) min_warm = warm - 1;
+    const double t_end = h->t + period;
+    int rc = hyd_checkpoint(h, 0);
+    if (rc) return rc;
+    long long steps = 0;
+    // the warm steps from the current state: ok once the gate passes (and the period's last
+    // step, with its bed update, is taken); a device check that fails (e.g. a line with
+    // more than 20 wet segments) rejects the state like a residual above the gate
+    auto warm_phase = [&](int& ok) -> int {
+        ok = 0;
+        int e = hyd_set_time(h, t_end - warm * dT);
+        if (e) return e;
+        double r[2], t;
+        e = hyd_steady_residual(h, 1, r, 2);
+        if (e) return e;
+        for (int k = 1; k < warm; k++) {
+            e = hyd_step(h, 1, 0, &t);
+            if (e) return e;
+            unsigned st = 0;
+            e = steady_residual(h, 1, r, &st);
+            if (e) return e;
+            if (st & HYD_ST_SEG_OVERFLOW) break;
+            if (k >= min_warm && r[0] < gate && r[1] < gate) {
+                double mb[5];
+                e = hyd_mass_balance(h, mb, 5);
+                if (e) return e;
+                if (mb[4] != 0) continue;
+                e = hyd_set_time(h, t_end - dT);
+                if (e) return e;
+                e = hyd_step(h, 1, 1, &t);  // the period's last step: the bed update on the accepted state
+                if (e == HYD_EDEVICE) break;
+                if (e) return e;
+                steps += k + 1;
+                ok = 1;
+                return HYD_OK;
+            }
+        }
+        steps += warm - 1;
+        return HYD_OK;
+    };
+    int jumped = 0, ok = 0;
+    if (du && dv && dz && rows > 0 && cols > 0) {
+        rc = hyd_add_levels(h, du, dv, dz, i0, j0, rows, cols, ld);
+        if (rc) return rc;
+        jumped = 1;
+    }
+    rc = warm_phase(ok);
+    if (rc) return rc;
+    if (!ok && jumped && retry) {  // the jump rejected: the previous state as the warm start
+        rc = hyd_checkpoint(h, 1);
+        if (rc) return rc;
+        jumped = 0;
+        rc = warm_phase(ok);
+        if (rc) return rc;
+    }
+    if (!ok) {  // not steady within the warm steps: the period stepped plainly
+        rc = hyd_checkpoint(h, 1);
+        if (rc) return rc;
+        double t;
+        rc = hyd_step(h, (int)nper, 1, &t);
+        if (rc) return rc;
+        steps += nper;
+    }
+    result[0] = ok;
+    result[1] = ok && jumped;
+    result[2] = (int)steps;
     return HYD_OK;
 }
 

@@ -63,6 +63,10 @@ def load():
         "hyd_mass_balance": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_int]),
         "hyd_mass_budget": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_int]),
         "hyd_checkpoint": (ctypes.c_int, [H, ctypes.c_int]),
+        "hyd_quasi_steady_period": (ctypes.c_int, [H, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
+                                                   ctypes.c_int, ctypes.c_void_p]),
         "hyd_get_field_device": (ctypes.c_int, [H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]),
         "hyd_set_time": (ctypes.c_int, [H, ctypes.c_double]),
         "hyd_steady_residual": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
@@ -312,6 +316,24 @@ class Simulation:
             raise ValueError("get_device needs a contiguous device tensor of shape %s" % (shape,))
         _check(self.lib.hyd_get_field_device(self.h, name.encode(), out.data_ptr(), int(np.prod(shape))))
         return out
+
+    def quasi_steady_period(self, period, warm=20, min_warm=1, gate=1e-4, jump=None, i0=0, j0=0, retry=True):
+        """One bed period of the quasi-steady form in the library (hyd_quasi_steady_period);
+        jump: (du, dv, dz) FP32 device tensors of one shape, added at grid cell (i0, j0), or
+        None.  Returns (accepted, accepted with the jump, steps taken)."""
+        res = (ctypes.c_int * 3)()
+        if jump is None:
+            args = (None, None, None, 0, 0, 0, 0, 0)
+        else:
+            du, dv, dz = jump
+            rows, cols = du.shape
+            for a in (du, dv, dz):
+                if tuple(a.shape) != (rows, cols) or not a.is_contiguous() or not a.is_cuda or a.element_size() != 4:
+                    raise ValueError("the jump takes three contiguous FP32 device tensors of one shape")
+            args = (du.data_ptr(), dv.data_ptr(), dz.data_ptr(), int(i0), int(j0), rows, cols, cols)
+        _check(self.lib.hyd_quasi_steady_period(self.h, float(period), int(warm), int(min_warm), float(gate), *args,
+                                                1 if retry else 0, ctypes.cast(res, ctypes.c_void_p)))
+        return bool(res[0]), bool(res[1]), int(res[2])
 
     def set_time(self, t):
         _check(self.lib.hyd_set_time(self.h, float(t)))

@@ -244,9 +244,13 @@ class QuasiSteady:
     read after each of the first `warm` - 1 warm steps from the `min_warm`-th on.  With a
     jump, a rejected jump is followed by one more try from the checkpoint without it
     (`retry`), before the period is stepped plainly.  Counters: accepted (of them
-    jump_accepted with the jump), fallbacks, steps."""
+    jump_accepted with the jump), fallbacks, steps.
 
-    def __init__(self, sim, case, warm=20, gate=1e-4, jump=None, min_warm=1, retry=True):
+    native: the period's calls are made inside the library (hyd_quasi_steady_period: no
+    host round trip between the warm steps) when the simulation offers it; the same calls
+    in the same order as the loop written here, which runs otherwise."""
+
+    def __init__(self, sim, case, warm=20, gate=1e-4, jump=None, min_warm=1, retry=True, native=True):
         self.sim = sim
         self.case = case
         self.warm = int(warm)
@@ -254,12 +258,12 @@ class QuasiSteady:
         self.gate = float(gate)
         self.jump = jump
         self.retry = retry
+        self.native = bool(native) and hasattr(sim, "quasi_steady_period")
         self.period_s = float(case.params.bed_period)
         self.accepted = 0
         self.jump_accepted = 0
         self.fallbacks = 0
         self.steps = 0
-        self.residuals = []
 
     def _warm(self, t_end):
         """The warm steps from the current state; True (and the period's last step taken)
@@ -277,7 +281,6 @@ class QuasiSteady:
                     sim.set_time(t_end - dT)
                     sim.step(1)  # the period's last step: the bed update on the accepted state
                     self.steps += k + 1
-                    self.residuals.append(max(r))
                     return True, r
         except HydError:
             # a device check failed on the warm-started state (e.g. jumped levels flooded a
@@ -293,15 +296,27 @@ class QuasiSteady:
         t_end = sim.t + self.period_s
         nper = int(round(self.period_s / dT))
         steps0 = self.steps
-        sim.checkpoint()
-        jumped = False
+        inc = None
         if self.jump is not None:
             Q, st = forcing_at(self.case, t_end)
             inc = self.jump.increments(sim, Q, st)
+        if self.native:
+            i0 = j0 = 0
             if inc is not None:
                 i0, _, j0, _ = self.jump.crop
-                sim.add_levels(*inc, i0, j0)
-                jumped = True
+            ok, jumped, n = sim.quasi_steady_period(self.period_s, self.warm, self.min_warm, self.gate, jump=inc,
+                                                    i0=i0, j0=j0, retry=self.retry)
+            self.steps += n
+            self.accepted += 1 if ok else 0
+            self.jump_accepted += 1 if jumped else 0
+            self.fallbacks += 0 if ok else 1
+            return ok, n
+        sim.checkpoint()
+        jumped = False
+        if inc is not None:
+            i0, _, j0, _ = self.jump.crop
+            sim.add_levels(*inc, i0, j0)
+            jumped = True
         ok, r = self._warm(t_end)
         if not ok and jumped and self.retry:
             sim.restore()  # the jump rejected: the previous state as the warm start
@@ -316,7 +331,6 @@ class QuasiSteady:
         sim.step(nper)
         self.fallbacks += 1
         self.steps += nper
-        self.residuals.append(max(r))
         return False, self.steps - steps0
 
     def run_until(self, t_stop):

@@ -354,6 +354,22 @@ int hyd_set_state(hyd_handle h, const void* buf, size_t bytes);
  */
 int hyd_checkpoint(hyd_handle h, int restore);
 int hyd_set_time(hyd_handle h, double t);
+/*
+ * hyd_quasi_steady_period: one bed period of the quasi-steady form with the calls above,
+ * in the library (no host round trip between them): checkpoint; the optional jump
+ * (du/dv/dz device arrays as hyd_add_levels; null for none); the last `warm` steps of the
+ * period with the steady residual after each (from the min_warm-th on, both components
+ * below `gate` and no non-finite value accept, and the period's last step, which makes
+ * its bed update, is taken); a rejected jump retried once from the checkpoint without it
+ * when `retry`; otherwise the checkpoint restored and the period stepped plainly.  A
+ * failed device check in a warm step rejects the state.  result[0] = 1 if a warm start
+ * was accepted, result[1] = 1 if that was the jump, result[2] = steps taken.  `period`
+ * must be a whole number of steps, at least `warm`; the clock must stand on the period's
+ * start.
+ */
+int hyd_quasi_steady_period(hyd_handle h, double period, int warm, int min_warm, double gate, const float* du,
+                            const float* dv, const float* dz, int i0, int j0, int rows, int cols, long long ld,
+                            int retry, int* result);
 int hyd_steady_residual(hyd_handle h, int snapshot, double* out, int n);
 int hyd_add_levels(hyd_handle h, const float* du, const float* dv, const float* dz, int i0, int j0, int rows,
                    int cols, long long ld);

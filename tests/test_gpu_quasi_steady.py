@@ -179,3 +179,48 @@ def test_quasi_steady_config5_sample():
     assert sim.mass_balance()["nonfinite"] == 0
     sim.close()
     ref.close()
+
+
+class _AlternatingJump:
+    """A fixed level increment over the reach's crop, large on odd periods (for the gate
+    to reject, and the retry without it to run) and small on even ones."""
+
+    def __init__(self, crop):
+        self.crop = crop
+        self.k = 0
+
+    def increments(self, sim, Q, stage):
+        import torch
+        _, rows, _, cols = self.crop
+        self.k += 1
+        amp = 5e-2 if self.k % 2 else 1e-4
+        g = torch.Generator().manual_seed(self.k)
+        dz = (amp * torch.rand((rows, cols), generator=g)).float().cuda()
+        zero = torch.zeros_like(dz)
+        return zero, zero.clone(), dz
+
+
+def test_native_period_matches_the_host_loop():
+    """hyd_quasi_steady_period makes the calls of the host loop in the same order: both
+    give the same fields bit for bit and the same counters, with a jump that is accepted
+    on some periods and retried without on others."""
+    from hydist import morpho as MO
+    from hydist.lib import Simulation
+    c = _config5(1.0)
+    crop = MO.reach_crop(c)
+    out = []
+    for native in (False, True):
+        sim = Simulation.from_case(c)
+        sim.step(7200)
+        q = MO.QuasiSteady(sim, c, warm=20, gate=1e-4, jump=_AlternatingJump(crop), native=native)
+        assert q.native == native
+        q.run_until(7200 + 3600)
+        out.append(((q.accepted, q.jump_accepted, q.fallbacks, q.steps, sim.t),
+                    {f: sim.get(f) for f in ("z", "u", "v", "FS", "dH", "h")}))
+        sim.close()
+    (ca, fa), (cb, fb) = out
+    print("host loop: accepted %d (jump %d), fallbacks %d, steps %d" % ca[:4])
+    assert ca == cb
+    assert ca[0] + ca[2] == 6
+    for f in fa:
+        assert np.array_equal(fa[f], fb[f]), f
