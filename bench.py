@@ -640,7 +640,8 @@ def run_config5(args, local_rank, hours=12.0, seeds=8, snapshots=64, iters=800, 
     and the quasi-steady form's bed and level differences from the plain FP64 run, on a
     bounded sample of `hours` hours after a 2 h spin-up (the spin-up and the surrogate's
     data generation and training are not timed).  Timed by the host clock around
-    synchronised calls: the quasi-steady loop's decisions are taken on the host."""
+    synchronised calls: each period's decisions are taken on the host CPU, inside the
+    library (hyd_quasi_steady_period)."""
     import numpy as np
     import torch
     from hydist import cases, morpho as MO, surrogate as S
@@ -703,6 +704,85 @@ def run_config5(args, local_rank, hours=12.0, seeds=8, snapshots=64, iters=800, 
                       "nonfinite_cells": int((~np.isfinite(z)).sum() + (~np.isfinite(dH)).sum())}
         sim.close()
     return out
+
+
+def run_surrogate(args, local_rank, B=16, H=1048, W=89, reps=30):
+    """The surrogate's tensor-core kernels on a batch of B crops of the config-5 channel band
+    (H x W cells; the activations of one 48-channel layer, 16 x 1048 x 89 x 48 BF16, are
+    143 MB, above L2): the full-resolution 48 -> 48 convolution (`k_conv_tc`) alone, then
+    the network's forward pass and one training iteration (forward, loss, backward through
+    the data- and weight-gradient kernels, Adam), each timed with CUDA events on the
+    stream the kernels run on.  The convolution's roofline: its MMA FLOPs (2 x pixels x
+    9 taps x 48 x 48) against the measured BF16 peak and its activation bytes (48 channels
+    in, 48 out, BF16) against the measured HBM copy bandwidth."""
+    import torch
+    from hydist import surrogate as S
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    net = S.Surrogate(device=local_rank, seed=0)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    x = torch.zeros((B, H, W, S.CIN_PAD), dtype=torch.bfloat16)
+    x[..., :S.IN_CH] = torch.randn((B, H, W, S.IN_CH), generator=g).to(torch.bfloat16)
+    x = x.to(dev)
+    y = torch.randn((B, H, W, S.OUT_CH), generator=g).to(dev)
+    wgt = torch.ones((B, H, W), device=dev)
+    l = 4  # full resolution, 48 -> 48, ReLU
+    mode, cin, cout, relu = S.LAYERS[l]
+    act = (torch.randn((B, H, W, cin), generator=g) * 0.5).to(torch.bfloat16).to(dev)
+    wpk = S.pack_weights(net.w[l], S.pad16(cout), S.pad16(cin))
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / n
+
+    conv_ms = timed(lambda: net.conv(act, B, H, W, cin, wpk, net.b[l], S.pad16(cout), cout, mode, relu, H, W), reps)
+    fwd_ms = timed(lambda: net.forward(x), reps)
+
+    def train_iter():
+        pred, saved = net.forward(x)
+        loss, dy = net.loss_grad(pred, y, wgt)
+        gw, gb = net.backward(saved, dy)
+        net.adam(gw + gb, lr=1e-4)
+
+    train_ms = timed(train_iter, max(5, reps // 3))
+    net.check_errors()
+    npix = B * H * W
+    flops = 2.0 * npix * 9 * cin * cout
+    nbytes = npix * (cin + cout) * 2
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        peaks = {"tflops": float(d["bf16_tflops"]), "gbs": float(d["hbm_gbs"]), "kind": "measured"}
+    except Exception:
+        peaks = {"tflops": 1590.0, "gbs": 6650.0, "kind": "fallback"}
+    tf = flops / (conv_ms * 1e-3) / 1e12
+    gbs = nbytes / (conv_ms * 1e-3) / 1e9
+    t_tensor = flops / (peaks["tflops"] * 1e12)
+    t_hbm = nbytes / (peaks["gbs"] * 1e9)
+    bound = "tensor" if t_tensor >= t_hbm else "hbm"
+    return {"workload": "BF16 surrogate, batch %d x %d x %d cells (config-5 channel band), 6 conv layers width 48"
+                        % (B, H, W),
+            "conv_48x48": {"kernel": "k_conv_tc (SAME, 48 -> 48, ReLU)", "ms_per_launch": conv_ms,
+                           "tflops": tf, "gbs": gbs, "mma_flops_per_launch": flops, "bytes_per_launch": nbytes,
+                           "roofline": {"bound": bound, "achieved": tf if bound == "tensor" else gbs,
+                                        "peak": peaks["tflops"] if bound == "tensor" else peaks["gbs"],
+                                        "unit": "TFLOP/s" if bound == "tensor" else "GB/s",
+                                        "frac": (tf / peaks["tflops"]) if bound == "tensor" else (gbs / peaks["gbs"]),
+                                        "frac_tensor": tf / peaks["tflops"], "frac_hbm": gbs / peaks["gbs"],
+                                        "speed_of_light_ms": 1e3 * max(t_tensor, t_hbm),
+                                        "peak_kind": peaks["kind"]}},
+            "forward": {"ms": fwd_ms, "cells_per_s": npix / (fwd_ms * 1e-3)},
+            "train_iteration": {"ms": train_ms, "cells_per_s": npix / (train_ms * 1e-3)}}
 
 
 def run_reference(args, rank):
@@ -774,6 +854,9 @@ def main():
                     help="config2 (the default: the 1048x980 reach) or config4 (the 4096x2048 reach)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the config-3 ensemble line")
     ap.add_argument("--no-config5", action="store_true", help="skip the config-5 morphodynamic line")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate kernels' line")
+    ap.add_argument("--surrogate-only", action="store_true",
+                    help="time only the surrogate kernels (one JSON line; for profiling them)")
     ap.add_argument("--timed-only", action="store_true",
                     help="profiling runs: spin up, warm up, run the timed steps, print a short line and stop")
     ap.add_argument("--config5-hours", type=float, default=12.0,
@@ -797,6 +880,9 @@ def main():
         if res is not None:
             print(json.dumps(res))
         return
+    if args.surrogate_only:
+        print(json.dumps(run_surrogate(args, local_rank)))
+        return
     if world > 1:
         import datetime
         import torch
@@ -815,6 +901,10 @@ def main():
             c5 = run_config5(args, local_rank, hours=args.config5_hours)
             if res is not None:
                 res.setdefault("workloads", {})["config5"] = c5
+        if not args.no_surrogate and args.secondary != "none" and world == 1:
+            sg = run_surrogate(args, local_rank)
+            if res is not None:
+                res.setdefault("workloads", {})["surrogate"] = sg
     finally:
         if world > 1:
             import torch

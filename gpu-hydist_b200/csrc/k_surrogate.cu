@@ -117,6 +117,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
+// 16-byte asynchronous copy global -> shared, cached in L1 (the two halves of a 32-byte
+// sector and the taps of neighbouring pixels read the same lines); src_bytes 0 fills the
+// 16 bytes with zeros (nothing is read).  A thread's copies are waited for with
+// cp_async_wait_all.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Byte offset of element (row, k) of a K step block (row-major 8-row groups of two core
 // matrices, see the file comment).
 __device__ __forceinline__ uint32_t op_off(int row, int k) {
@@ -159,29 +169,76 @@ struct ConvArgs {
     int* err;
 };
 
+// This thread's row of A for `tile` (output pixel tile * kTile + tid): the 9 taps x CIN
+// channels of its input pixels, copied asynchronously into the K step blocks (zeros for
+// padding and for pixels past the end), one commit group.
+template <int MODE, int CIN>
+__device__ __forceinline__ void gather_row(const ConvArgs& a, uint32_t sA, long long tile, long long npix, int tid) {
+    constexpr int CB = CIN / 16;
+    constexpr int A_STEP = kTile * 32;
+    const long long p = tile * kTile + tid;
+    int b = 0, y = 0, x = 0;
+    const bool live = p < npix;
+    if (live) {  // the host keeps the pixel count below 2^31
+        const int pi = (int)p;
+        const int r = pi / a.Wout;
+        x = pi - r * a.Wout;
+        b = r / a.Hout;
+        y = r - b * a.Hout;
+    }
+#pragma unroll
+    for (int t = 0; t < 9; t++) {
+        const long long q = live ? map_pixel<MODE>(b, y, x, t, a.Hin, a.Win) : -1;
+        const __nv_bfloat16* src = a.x + (q < 0 ? 0 : q) * CIN;
+        const uint32_t n = q < 0 ? 0u : 16u;
+#pragma unroll
+        for (int cb = 0; cb < CB; cb++) {
+            const uint32_t blk = sA + (uint32_t)((t * CB + cb) * A_STEP);
+            cp_async16(blk + op_off(tid, 0), src + 16 * cb, n);
+            cp_async16(blk + op_off(tid, 8), src + 16 * cb + 8, n);
+        }
+    }
+    cp_async_commit();
+}
+
+// zero the BF16 halves of v whose mask value is not > 0
+__device__ __forceinline__ uint32_t mask_bf16x2(uint32_t v, uint32_t m) {
+    const bool lo = __uint_as_float(m << 16) > 0.0f, hi = __uint_as_float(m & 0xFFFF0000u) > 0.0f;
+    return (lo ? (v & 0xFFFFu) : 0u) | (hi ? (v & 0xFFFF0000u) : 0u);
+}
+
 // Forward / data-gradient convolution: CTA tiles of 128 output pixels, all output columns
 // (NCOL, a multiple of 16) at once.  CIN (16 or 48) input channels per pixel; the weights
-// for the whole K stay in shared memory, the tile's whole A (K x 128) is gathered at once,
-// then K/16 MMAs accumulate in tensor memory.
+// for the whole K stay in shared memory, the tile's whole A (K x 128) is copied in
+// asynchronously (every copy of a thread in flight at once), then K/16 MMAs accumulate in
+// tensor memory.  Once they have completed, the next tile's copies are issued and run
+// under this tile's epilogue, which stages the output tile (bias, ReLU) in shared memory
+// and writes it with coalesced 16-byte stores (the mask applied there).
 template <int MODE, int CIN, int NCOL>
 __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
     constexpr int KSTEPS = 9 * CIN / 16;
-    constexpr int CB = CIN / 16;                 // channel blocks per tap
     constexpr int A_STEP = kTile * 32;           // bytes of A per K step
     constexpr int B_STEP = NCOL * 32;            // bytes of B per K step
     constexpr uint32_t TCOLS = NCOL <= 32 ? 32 : (NCOL <= 64 ? 64 : (NCOL <= 128 ? 128 : 256));
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* sA = smem;
     unsigned char* sB = smem + KSTEPS * A_STEP;
+    unsigned char* sO = sB + KSTEPS * B_STEP;    // the output tile, kTile x nout, as in y
+    float* sBias = reinterpret_cast<float*>(sO + kTile * NCOL * 4);
     __shared__ uint64_t mbar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5;
-    // weights: a straight copy of the packed image
+    const long long npix = (long long)a.B * a.Hout * a.Wout;
+    const long long ntiles = (npix + kTile - 1) / kTile;
+    const uint32_t a0 = smem_u32(sA);
+    if ((long long)blockIdx.x < ntiles) gather_row<MODE, CIN>(a, a0, blockIdx.x, npix, tid);
+    // weights: a straight copy of the packed image; the bias (zero beyond nout)
     {
         const uint4* src = a.w;
         uint4* dst = reinterpret_cast<uint4*>(sB);
         for (int q = tid; q < KSTEPS * B_STEP / 16; q += kThreads) dst[q] = src[q];
+        for (int c = tid; c < NCOL; c += kThreads) sBias[c] = (a.bias && c < a.nout) ? a.bias[c] : 0.0f;
     }
     if (tid == 0) {
         mbar_init(&mbar);
@@ -192,42 +249,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    const long long npix = (long long)a.B * a.Hout * a.Wout;
-    const long long ntiles = (npix + kTile - 1) / kTile;
+    const int nout = a.nout, esz = a.out_f32 ? 4 : 2;
     uint32_t phase = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        // ---- gather this thread's row of A: K steps of 16 channels of one tap
-        const long long p = tile * kTile + tid;
-        int b = 0, y = 0, x = 0;
-        const bool live = p < npix;
-        if (live) {
-            x = (int)(p % a.Wout);
-            const long long r = p / a.Wout;
-            y = (int)(r % a.Hout);
-            b = (int)(r / a.Hout);
-        }
-#pragma unroll 3
-        for (int t = 0; t < 9; t++) {
-            const long long q = live ? map_pixel<MODE>(b, y, x, t, a.Hin, a.Win) : -1;
-            const uint4* src = reinterpret_cast<const uint4*>(a.x + (q < 0 ? 0 : q) * CIN);
-#pragma unroll
-            for (int cb = 0; cb < CB; cb++) {
-                uint4 lo = make_uint4(0, 0, 0, 0), hi = make_uint4(0, 0, 0, 0);
-                if (q >= 0) {
-                    lo = src[2 * cb];
-                    hi = src[2 * cb + 1];
-                }
-                unsigned char* blk = sA + (t * CB + cb) * A_STEP;
-                *reinterpret_cast<uint4*>(blk + op_off(tid, 0)) = lo;
-                *reinterpret_cast<uint4*>(blk + op_off(tid, 8)) = hi;
-            }
-        }
+        cp_async_wait_all();
         fence_async_smem();
         __syncthreads();
         // ---- the MMAs, issued by one thread; their completion arrives on the mbarrier
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            const uint32_t b0 = smem_u32(sB);
             constexpr uint32_t idesc = instr_desc(kTile, NCOL);
             for (int s = 0; s < KSTEPS; s++)
                 mma_bf16(tmem, smem_desc(a0 + s * A_STEP, 128, 256), smem_desc(b0 + s * B_STEP, 128, 256), idesc,
@@ -241,28 +272,87 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
             break;
         }
         tc_fence_after();
-        // ---- epilogue: this thread's row from tensor memory, bias, mask, activation (every
-        // thread of a warp takes part in tcgen05.ld, which is .sync.aligned)
+        // A has been read: the next tile's copies run under this epilogue
+        if (tile + gridDim.x < ntiles) gather_row<MODE, CIN>(a, a0, tile + gridDim.x, npix, tid);
+        const long long rem = npix - tile * kTile;
+        const int live_n = rem < kTile ? (int)rem : kTile;
+        // ---- this thread's row from tensor memory, bias and activation, into the staged
+        // tile (every thread of a warp takes part in tcgen05.ld, which is .sync.aligned)
 #pragma unroll
         for (int c0 = 0; c0 < NCOL; c0 += 16) {
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (live) {
+            if (tid < live_n) {
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
-                    const int c = c0 + k;
-                    if (c >= a.nout) break;
-                    float o = v[k] + (a.bias ? a.bias[c] : 0.0f);
-                    if (a.mask && !(__bfloat162float(a.mask[p * a.nout + c]) > 0.0f)) o = 0.0f;
-                    if (a.relu) o = fmaxf(o, 0.0f);
-                    if (a.out_f32) reinterpret_cast<float*>(a.y)[p * a.nout + c] = o;
-                    else reinterpret_cast<__nv_bfloat16*>(a.y)[p * a.nout + c] = __float2bfloat16_rn(o);
+                    v[k] += sBias[c0 + k];
+                    if (a.relu) v[k] = fmaxf(v[k], 0.0f);
+                }
+                if (!a.out_f32 && nout % 8 == 0 && c0 + 16 <= nout) {  // two 16-byte stores
+                    uint32_t w[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+                        w[k] = *reinterpret_cast<const uint32_t*>(&h);
+                    }
+                    uint4* d = reinterpret_cast<uint4*>(sO + ((size_t)tid * nout + c0) * 2);
+                    d[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                    d[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                } else if (a.out_f32 && nout % 4 == 0 && c0 + 16 <= nout) {  // four 16-byte stores
+                    float4* d = reinterpret_cast<float4*>(sO + ((size_t)tid * nout + c0) * 4);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) d[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        const int c = c0 + k;
+                        if (c >= nout) break;
+                        if (a.out_f32) reinterpret_cast<float*>(sO)[tid * nout + c] = v[k];
+                        else reinterpret_cast<__nv_bfloat16*>(sO)[tid * nout + c] = __float2bfloat16_rn(v[k]);
+                    }
                 }
             }
         }
         tc_fence_before();
-        __syncthreads();  // the tile's tensor memory and A are free for the next tile
+        __syncthreads();  // the staged tile is complete; the tensor memory has been read
+        // ---- the staged tile to y (it is contiguous there), the mask applied
+        const long long e0 = tile * kTile * nout;  // first element of the tile in y and the mask
+        const int nel = live_n * nout, nbytes = nel * esz;
+        unsigned char* yb = reinterpret_cast<unsigned char*>(a.y) + e0 * esz;
+        const __nv_bfloat16* mb = a.mask ? a.mask + e0 : nullptr;
+        const bool vec = (nbytes % 16 == 0) && !(reinterpret_cast<uintptr_t>(yb) & 15) &&
+                         !(reinterpret_cast<uintptr_t>(mb) & (a.out_f32 ? 7 : 15));
+        if (vec) {
+            for (int q = tid; q < nbytes / 16; q += kThreads) {
+                uint4 v = reinterpret_cast<const uint4*>(sO)[q];
+                if (mb) {
+                    if (a.out_f32) {
+                        const uint2 m = reinterpret_cast<const uint2*>(mb)[q];
+                        v.x = __uint_as_float(m.x << 16) > 0.0f ? v.x : 0u;
+                        v.y = __uint_as_float(m.x & 0xFFFF0000u) > 0.0f ? v.y : 0u;
+                        v.z = __uint_as_float(m.y << 16) > 0.0f ? v.z : 0u;
+                        v.w = __uint_as_float(m.y & 0xFFFF0000u) > 0.0f ? v.w : 0u;
+                    } else {
+                        const uint4 m = reinterpret_cast<const uint4*>(mb)[q];
+                        v.x = mask_bf16x2(v.x, m.x);
+                        v.y = mask_bf16x2(v.y, m.y);
+                        v.z = mask_bf16x2(v.z, m.z);
+                        v.w = mask_bf16x2(v.w, m.w);
+                    }
+                }
+                reinterpret_cast<uint4*>(yb)[q] = v;
+            }
+        } else {
+            for (int e = tid; e < nel; e += kThreads) {
+                const bool keep = !mb || __bfloat162float(mb[e]) > 0.0f;
+                if (a.out_f32) reinterpret_cast<float*>(yb)[e] = keep ? reinterpret_cast<const float*>(sO)[e] : 0.0f;
+                else
+                    reinterpret_cast<__nv_bfloat16*>(yb)[e] =
+                        keep ? reinterpret_cast<const __nv_bfloat16*>(sO)[e] : __float2bfloat16_rn(0.0f);
+            }
+        }
     }
+    cp_async_wait_all();  // no copy in flight past this point
     __syncthreads();
     if (s_fail) {
         if (tid == 0) atomicExch(a.err, 1);
@@ -287,6 +377,8 @@ struct WgradArgs {
 // Weight gradient: dW[n][t][ci] = sum_p dY[p][n] X[map(p, t)][ci].  An MMA with M = 128 rows
 // (t, ci) of the 9 x cin, N = NCOL output channels and K = output pixels; CTA (m-tile,
 // pixel chunk), the chunk's K steps gathered 8 at a time, the partial sums added to dw.
+// Each round's 128 pixels are mapped once (thread k: pixel k's input pixel for every tap,
+// kept in shared memory), so the gathers do no index division.
 template <int MODE, int NCOL>
 __global__ void __launch_bounds__(kThreads, 1) k_conv_wgrad_tc(WgradArgs a) {
     constexpr int KB = 8;                 // K steps per gather round
@@ -298,6 +390,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_wgrad_tc(WgradArgs a) {
     __shared__ uint64_t mbar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
+    __shared__ long long s_q[9][16 * KB];  // the round's input pixel per tap (-1: none)
     const int tid = threadIdx.x, warp = tid >> 5;
     const int rows = 9 * a.cin;
     const int mt = blockIdx.y;
@@ -319,7 +412,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_wgrad_tc(WgradArgs a) {
     const uint32_t tmem = s_tmem;
     uint32_t phase = 0;
     int issued = 0;
+    static_assert(16 * KB == kThreads, "one pixel of the round per thread");
     for (long long k0 = p0; k0 < p1; k0 += 16 * KB) {
+        {
+            const long long p = k0 + tid;
+            int x = 0, y = 0, b = 0;
+            if (p < p1) {
+                x = (int)(p % a.Wout);
+                const long long rr = p / a.Wout;
+                y = (int)(rr % a.Hout);
+                b = (int)(rr / a.Hout);
+            }
+#pragma unroll
+            for (int tt = 0; tt < 9; tt++) s_q[tt][tid] = p < p1 ? map_pixel<MODE>(b, y, x, tt, a.Hin, a.Win) : -1;
+        }
+        __syncthreads();
+        const long long* qrow = s_q[t];
         for (int s = 0; s < KB; s++) {
             // A row r over 16 pixels; B rows (channels) over the same pixels
             __align__(16) __nv_bfloat16 va[16];
@@ -330,11 +438,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_wgrad_tc(WgradArgs a) {
                 __nv_bfloat16 v = __float2bfloat16_rn(0.0f);
                 __nv_bfloat16 w = v;
                 if (p < p1) {
-                    const int x = (int)(p % a.Wout);
-                    const long long rr = p / a.Wout;
-                    const int y = (int)(rr % a.Hout), b = (int)(rr / a.Hout);
                     if (rlive) {
-                        const long long q = map_pixel<MODE>(b, y, x, t, a.Hin, a.Win);
+                        const long long q = qrow[s * 16 + k];
                         if (q >= 0) v = a.x[q * a.cin + ci];
                     }
                     if (tid < NCOL) w = a.dy[p * NCOL + tid];
@@ -434,7 +539,7 @@ __global__ void k_mse_grad(const float* pred, const float* tgt, const float* wgt
 template <int MODE, int CIN, int NCOL>
 cudaError_t launch_conv(const ConvArgs& a, cudaStream_t s) {
     constexpr int KSTEPS = 9 * CIN / 16;
-    const size_t smem = (size_t)KSTEPS * (kTile * 32 + NCOL * 32);
+    const size_t smem = (size_t)KSTEPS * (kTile * 32 + NCOL * 32) + (size_t)kTile * NCOL * 4 + NCOL * 4;
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc<MODE, CIN, NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -485,6 +590,7 @@ int hyd_conv_forward(const void* x, int B, int Hin, int Win, int cin, const void
                      int out_f32, int* err, void* stream) {
     if (!x || !w_packed || !y || !err || B < 1 || Hin < 1 || Win < 1 || Hout < 1 || Wout < 1) return HYD_EINVAL;
     if (nout < 1 || nout > ncol) return HYD_EINVAL;
+    if ((long long)B * Hout * Wout >= (1LL << 31)) return HYD_EINVAL;  // 32-bit pixel indices in the gather
     if ((reinterpret_cast<uintptr_t>(x) & 15) || (reinterpret_cast<uintptr_t>(w_packed) & 15)) return HYD_EINVAL;
     ConvArgs a{(const __nv_bfloat16*)x, B, Hin, Win, (const uint4*)w_packed, bias, (const __nv_bfloat16*)mask, y,
                Hout, Wout, nout, relu, out_f32, err};

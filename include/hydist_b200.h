@@ -467,6 +467,7 @@ int hyd_get_sweep_shape(hyd_handle h, int* ctas, int* wide);
  *   s = (t cin + c) / 16 a block of ncol x 16 BF16 in which element (n, k) lies at byte
  *   (n / 8) 256 + (k / 8) 128 + (n % 8) 16 + (k % 8) 2.  relu: max(0, .); out_f32: FP32
  *   output instead of BF16.  *err is set to 1 if a wait on the tensor cores timed out.
+ *   B x Hout x Wout must stay below 2^31 (HYD_EINVAL otherwise).
  * hyd_conv_wgrad: dw[n][t][c] += sum_p dy[p][n] x[map(p,t)][c] (FP32, n < nout), dy with
  *   ncol channels per pixel; map is the layer's forward mapping.
  * hyd_bias_grad: db[n] += sum_p dy[p][n].
