@@ -727,8 +727,19 @@ __device__ __forceinline__ void fsj_cell_coeffs(const DevGrid& g, const DevParam
     const int P = g.P;
     const double* FS = g.FS;
     const double* H = g.H_moi;
-    auto L = [](const double* a, int q) { return R(a[q]); };
-    const R Hp = L(H, pos), FSp = L(FS, pos), VTHp = L(g.VTH, pos);
+    // FSj runs right after the half-step's state update, which left u = t_u and v = t_v
+    // on every cell it reads; reading u and v lets it run beside the next half-step's
+    // sweeps, which write t_u and t_v
+    const double *u = g.u, *v = g.v;
+    // every operand first (one memory round trip; the branches below only select)
+    const double Hd = H[pos], FSd = FS[pos], VTHd = g.VTH[pos], Fwd = g.Fw[pos];
+    const double u0 = u[pos], u1 = u[pos - P], hu0 = g.Htdu[pos], hu1 = g.Htdu[pos - P], kx0 = g.Kx[pos],
+                 kx1 = g.Kx[pos - P];
+    const double Hm1 = H[pos - 1], Hp2 = H[pos + 2], Hm2 = H[pos - 2], Hp1 = H[pos + 1];
+    const double FSp1 = FS[pos + 1], FSm1 = FS[pos - 1];
+    const double hv0 = g.Htdv[pos], hv1 = g.Htdv[pos - 1], ky0 = g.Ky[pos], ky1 = g.Ky[pos - 1];
+    const double v0 = v[pos], v1 = v[pos - 1];
+    const R Hp = R(Hd), FSp = R(FSd), VTHp = R(VTHd);
     const double s_start = p.bed_change_start;
     const R sqrtg = sqrt(R(p.g));
     const R c = 18 * log(12 * Hp / R(p.Ks));
@@ -738,25 +749,20 @@ __device__ __forceinline__ void fsj_cell_coeffs(const DevGrid& g, const DevParam
     R Zf = 0;
     R S;
     const R gamav = R(0.98) - R(0.198) * Zf + R(0.032) * Zf * Zf;  // evaluated before Zf (Sediment_Transport.cu:236)
-    if (FS[pos] > 0.00001) Zf = wsm / (R(0.4) * (Uf + 2 * wsm));
-    if (p.ketdinh) S = source_chs<R>(p, wsm, Zf, FSp, L(g.Fw, pos), VTHp, Hp);
+    if (FSd > 0.00001) Zf = wsm / (R(0.4) * (Uf + 2 * wsm));
+    if (p.ketdinh) S = source_chs<R>(p, wsm, Zf, FSp, R(Fwd), VTHp, Hp);
     else S = source_nchs<R>(p, wsm, Zf, Uf, Hp, FSp);
     if (t < s_start) S = 0;
-    // FSj runs right after the half-step's state update, which left u = t_u and v = t_v
-    // on every cell it reads; reading u and v lets it run beside the next half-step's
-    // sweeps, which write t_u and t_v
-    const double *u = g.u, *v = g.v;
-    aa = -gamav * R(0.5) * (L(u, pos) + L(u, pos - P)) / R(p.dX2) -
-         L(g.Htdu, pos - P) * L(g.Kx, pos - P) / (Hp * (R(p.dXbp)));
-    cc = gamav * R(0.5) * (L(u, pos) + L(u, pos - P)) / R(p.dX2) - L(g.Htdu, pos) * L(g.Kx, pos) / (Hp * (R(p.dXbp)));
-    bb = R(p.HaiChiadT) + (L(g.Htdu, pos) * L(g.Kx, pos) + L(g.Htdu, pos - P) * L(g.Kx, pos - P)) / (Hp * (R(p.dXbp)));
+    aa = -gamav * R(0.5) * (R(u0) + R(u1)) / R(p.dX2) - R(hu1) * R(kx1) / (Hp * (R(p.dXbp)));
+    cc = gamav * R(0.5) * (R(u0) + R(u1)) / R(p.dX2) - R(hu0) * R(kx0) / (Hp * (R(p.dXbp)));
+    bb = R(p.HaiChiadT) + (R(hu0) * R(kx0) + R(hu1) * R(kx1)) / (Hp * (R(p.dXbp)));
     R pp = 0, qq = 0;
-    if ((H[pos - 1] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) pp = R(FS[pos + 1] - FS[pos]);
-    if ((H[pos - 2] > p.H_TINH) && (H[pos + 1] > p.H_TINH)) qq = R(FS[pos] - FS[pos - 1]);
-    pp = (1 / (Hp * R(p.dYbp))) * (L(g.Htdv, pos) * L(g.Ky, pos) * pp - L(g.Htdv, pos - 1) * L(g.Ky, pos - 1) * qq);
-    if ((H[pos - 2] > p.H_TINH) && (H[pos + 2] > p.H_TINH)) {
-        qq = R(FS[pos + 1] - FS[pos - 1]) / R(p.dY2);
-        qq = (L(v, pos) + L(v, pos - 1)) * R(0.5) * qq * gamav;
+    if ((Hm1 > p.H_TINH) && (Hp2 > p.H_TINH)) pp = R(FSp1 - FSd);
+    if ((Hm2 > p.H_TINH) && (Hp1 > p.H_TINH)) qq = R(FSd - FSm1);
+    pp = (1 / (Hp * R(p.dYbp))) * (R(hv0) * R(ky0) * pp - R(hv1) * R(ky1) * qq);
+    if ((Hm2 > p.H_TINH) && (Hp2 > p.H_TINH)) {
+        qq = R(FSp1 - FSm1) / R(p.dY2);
+        qq = (R(v0) + R(v1)) * R(0.5) * qq * gamav;
     } else
         qq = 0;
     dd = FSp / (R(p.dT) * R(0.5)) - qq + pp + (S / Hp);
@@ -772,23 +778,29 @@ __device__ __forceinline__ void fsi_cell_coeffs(const DevGrid& g, const DevParam
     const int P = g.P;
     const double* FS = g.FS;
     const double* H = g.H_moi;
-    auto L = [](const double* a, int q) { return R(a[q]); };
-    const R Hp = L(H, pos);
-    const R gamav = rowCr<R>(g, 0)[pos];
-    aa = -gamav * R(0.5) * (L(g.t_v, pos - 1) + L(g.t_v, pos)) / R(p.dY2) -
-         L(g.Htdv, pos - 1) * L(g.Ky, pos - 1) / (Hp * R(p.dYbp));
-    cc = gamav * R(0.5) * (L(g.t_v, pos - 1) + L(g.t_v, pos)) / R(p.dY2) - L(g.Htdv, pos) * L(g.Ky, pos) / (Hp * R(p.dYbp));
-    bb = R(p.HaiChiadT) + (L(g.Htdv, pos) * L(g.Ky, pos) + L(g.Htdv, pos - 1) * L(g.Ky, pos - 1)) / (Hp * R(p.dYbp));
+    // every operand first (one memory round trip; the branches below only select)
+    const double Hd = H[pos], FSd = FS[pos];
+    const R gamav = rowCr<R>(g, 0)[pos], src = rowCr<R>(g, 1)[pos];
+    const double tv0 = g.t_v[pos], tv1 = g.t_v[pos - 1], hv0 = g.Htdv[pos], hv1 = g.Htdv[pos - 1], ky0 = g.Ky[pos],
+                 ky1 = g.Ky[pos - 1];
+    const double Hp2 = H[pos + 2 * P], Hm1 = H[pos - P], Hm2 = H[pos - 2 * P], Hp1 = H[pos + P];
+    const double FSp1 = FS[pos + P], FSm1 = FS[pos - P];
+    const double hu0 = g.Htdu[pos], hu1 = g.Htdu[pos - P], kx0 = g.Kx[pos], kx1 = g.Kx[pos - P];
+    const double tu0 = g.t_u[pos], tu1 = g.t_u[pos - P];
+    const R Hp = R(Hd);
+    aa = -gamav * R(0.5) * (R(tv1) + R(tv0)) / R(p.dY2) - R(hv1) * R(ky1) / (Hp * R(p.dYbp));
+    cc = gamav * R(0.5) * (R(tv1) + R(tv0)) / R(p.dY2) - R(hv0) * R(ky0) / (Hp * R(p.dYbp));
+    bb = R(p.HaiChiadT) + (R(hv0) * R(ky0) + R(hv1) * R(ky1)) / (Hp * R(p.dYbp));
     R pp = 0, qq = 0;
-    if ((H[pos + 2 * P] > p.H_TINH) && (H[pos - P] > p.H_TINH)) pp = R(FS[pos + P] - FS[pos]);
-    if (H[pos - 2 * P] > p.H_TINH && H[pos + P] > p.H_TINH) qq = R(FS[pos] - FS[pos - P]);
-    pp = (1 / (Hp * R(p.dXbp))) * (L(g.Htdu, pos) * L(g.Kx, pos) * pp - L(g.Htdu, pos - P) * L(g.Kx, pos - P) * qq);
-    if (H[pos + 2 * P] > p.H_TINH && H[pos - 2 * P] > p.H_TINH) {
-        qq = R(FS[pos + P] - FS[pos - P]) / R(p.dX2);
-        qq = (L(g.t_u, pos) + L(g.t_u, pos - P)) * R(0.5) * qq * gamav;
+    if ((Hp2 > p.H_TINH) && (Hm1 > p.H_TINH)) pp = R(FSp1 - FSd);
+    if (Hm2 > p.H_TINH && Hp1 > p.H_TINH) qq = R(FSd - FSm1);
+    pp = (1 / (Hp * R(p.dXbp))) * (R(hu0) * R(kx0) * pp - R(hu1) * R(kx1) * qq);
+    if (Hp2 > p.H_TINH && Hm2 > p.H_TINH) {
+        qq = R(FSp1 - FSm1) / R(p.dX2);
+        qq = (R(tu0) + R(tu1)) * R(0.5) * qq * gamav;
     } else
         qq = 0;
-    dd = L(FS, pos) / (R(p.dT) * R(0.5)) - qq + pp + rowCr<R>(g, 1)[pos];
+    dd = R(FSd) / (R(p.dT) * R(0.5)) - qq + pp + src;
 }
 
 // FSj rows of every interior wet cell (columns 3..M-1), one warp per row of the grid over
