@@ -34,6 +34,8 @@ namespace {
 
 constexpr int kTile = 128;            // output pixels per CTA tile (MMA M)
 constexpr int kThreads = 128;         // four warps: one thread per tile row
+constexpr int kConvGroups = 3;        // the forward kernel's thread groups: a third of the taps
+constexpr int kConvThreads = kTile * kConvGroups;  // and of the output column blocks each
 constexpr unsigned kSpinLimit = 1u << 26;  // bounded waits (~seconds); then the error flag
 
 // pixel mappings of a layer (the input pixel that output pixel p, tap t reads)
@@ -169,14 +171,15 @@ struct ConvArgs {
     int* err;
 };
 
-// This thread's row of A for `tile` (output pixel tile * kTile + tid): the 9 taps x CIN
-// channels of its input pixels, copied asynchronously into the K step blocks (zeros for
-// padding and for pixels past the end), one commit group.
+// Taps t0..t0+2 of row `row` of A for `tile` (output pixel tile * kTile + row): CIN
+// channels of the input pixel of each tap, copied asynchronously into the K step blocks
+// (zeros for padding and for pixels past the end), one commit group.
 template <int MODE, int CIN>
-__device__ __forceinline__ void gather_row(const ConvArgs& a, uint32_t sA, long long tile, long long npix, int tid) {
+__device__ __forceinline__ void gather_row(const ConvArgs& a, uint32_t sA, long long tile, long long npix, int row,
+                                           int t0) {
     constexpr int CB = CIN / 16;
     constexpr int A_STEP = kTile * 32;
-    const long long p = tile * kTile + tid;
+    const long long p = tile * kTile + row;
     int b = 0, y = 0, x = 0;
     const bool live = p < npix;
     if (live) {  // the host keeps the pixel count below 2^31
@@ -187,15 +190,16 @@ __device__ __forceinline__ void gather_row(const ConvArgs& a, uint32_t sA, long 
         y = r - b * a.Hout;
     }
 #pragma unroll
-    for (int t = 0; t < 9; t++) {
+    for (int dt = 0; dt < 9 / kConvGroups; dt++) {
+        const int t = t0 + dt;
         const long long q = live ? map_pixel<MODE>(b, y, x, t, a.Hin, a.Win) : -1;
         const __nv_bfloat16* src = a.x + (q < 0 ? 0 : q) * CIN;
         const uint32_t n = q < 0 ? 0u : 16u;
 #pragma unroll
         for (int cb = 0; cb < CB; cb++) {
             const uint32_t blk = sA + (uint32_t)((t * CB + cb) * A_STEP);
-            cp_async16(blk + op_off(tid, 0), src + 16 * cb, n);
-            cp_async16(blk + op_off(tid, 8), src + 16 * cb + 8, n);
+            cp_async16(blk + op_off(row, 0), src + 16 * cb, n);
+            cp_async16(blk + op_off(row, 8), src + 16 * cb + 8, n);
         }
     }
     cp_async_commit();
@@ -213,9 +217,12 @@ __device__ __forceinline__ uint32_t mask_bf16x2(uint32_t v, uint32_t m) {
 // asynchronously (every copy of a thread in flight at once), then K/16 MMAs accumulate in
 // tensor memory.  Once they have completed, the next tile's copies are issued and run
 // under this tile's epilogue, which stages the output tile (bias, ReLU) in shared memory
-// and writes it with coalesced 16-byte stores (the mask applied there).
+// and writes it with coalesced 16-byte stores (the mask applied there).  Three groups of
+// 128 threads: thread (group g, row r) copies taps 3g..3g+2 of tile row r and, in the
+// epilogue, reads column blocks g, g + 3, ... of its row (warp w reads tensor-memory
+// lanes 32 (w % 4)..+31, the lanes its sub-partition may access).
 template <int MODE, int CIN, int NCOL>
-__global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
+__global__ void __launch_bounds__(kConvThreads, 1) k_conv_tc(ConvArgs a) {
     constexpr int KSTEPS = 9 * CIN / 16;
     constexpr int A_STEP = kTile * 32;           // bytes of A per K step
     constexpr int B_STEP = NCOL * 32;            // bytes of B per K step
@@ -229,16 +236,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = tid & (kTile - 1), grp = tid / kTile;
     const long long npix = (long long)a.B * a.Hout * a.Wout;
     const long long ntiles = (npix + kTile - 1) / kTile;
     const uint32_t a0 = smem_u32(sA);
-    if ((long long)blockIdx.x < ntiles) gather_row<MODE, CIN>(a, a0, blockIdx.x, npix, tid);
+    if ((long long)blockIdx.x < ntiles) gather_row<MODE, CIN>(a, a0, blockIdx.x, npix, row, 3 * grp);
     // weights: a straight copy of the packed image; the bias (zero beyond nout)
     {
         const uint4* src = a.w;
         uint4* dst = reinterpret_cast<uint4*>(sB);
-        for (int q = tid; q < KSTEPS * B_STEP / 16; q += kThreads) dst[q] = src[q];
-        for (int c = tid; c < NCOL; c += kThreads) sBias[c] = (a.bias && c < a.nout) ? a.bias[c] : 0.0f;
+        for (int q = tid; q < KSTEPS * B_STEP / 16; q += kConvThreads) dst[q] = src[q];
+        for (int c = tid; c < NCOL; c += kConvThreads) sBias[c] = (a.bias && c < a.nout) ? a.bias[c] : 0.0f;
     }
     if (tid == 0) {
         mbar_init(&mbar);
@@ -273,16 +281,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
         }
         tc_fence_after();
         // A has been read: the next tile's copies run under this epilogue
-        if (tile + gridDim.x < ntiles) gather_row<MODE, CIN>(a, a0, tile + gridDim.x, npix, tid);
+        if (tile + gridDim.x < ntiles) gather_row<MODE, CIN>(a, a0, tile + gridDim.x, npix, row, 3 * grp);
         const long long rem = npix - tile * kTile;
         const int live_n = rem < kTile ? (int)rem : kTile;
         // ---- this thread's row from tensor memory, bias and activation, into the staged
         // tile (every thread of a warp takes part in tcgen05.ld, which is .sync.aligned)
 #pragma unroll
-        for (int c0 = 0; c0 < NCOL; c0 += 16) {
+        for (int c0 = 16 * grp; c0 < NCOL; c0 += 16 * kConvGroups) {
             float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (tid < live_n) {
+            tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0, v);
+            if (row < live_n) {
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
                     v[k] += sBias[c0 + k];
@@ -295,11 +303,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
                         const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
                         w[k] = *reinterpret_cast<const uint32_t*>(&h);
                     }
-                    uint4* d = reinterpret_cast<uint4*>(sO + ((size_t)tid * nout + c0) * 2);
+                    uint4* d = reinterpret_cast<uint4*>(sO + ((size_t)row * nout + c0) * 2);
                     d[0] = make_uint4(w[0], w[1], w[2], w[3]);
                     d[1] = make_uint4(w[4], w[5], w[6], w[7]);
                 } else if (a.out_f32 && nout % 4 == 0 && c0 + 16 <= nout) {  // four 16-byte stores
-                    float4* d = reinterpret_cast<float4*>(sO + ((size_t)tid * nout + c0) * 4);
+                    float4* d = reinterpret_cast<float4*>(sO + ((size_t)row * nout + c0) * 4);
 #pragma unroll
                     for (int k = 0; k < 4; k++) d[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
                 } else {
@@ -307,8 +315,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
                     for (int k = 0; k < 16; k++) {
                         const int c = c0 + k;
                         if (c >= nout) break;
-                        if (a.out_f32) reinterpret_cast<float*>(sO)[tid * nout + c] = v[k];
-                        else reinterpret_cast<__nv_bfloat16*>(sO)[tid * nout + c] = __float2bfloat16_rn(v[k]);
+                        if (a.out_f32) reinterpret_cast<float*>(sO)[row * nout + c] = v[k];
+                        else reinterpret_cast<__nv_bfloat16*>(sO)[row * nout + c] = __float2bfloat16_rn(v[k]);
                     }
                 }
             }
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
         const bool vec = (nbytes % 16 == 0) && !(reinterpret_cast<uintptr_t>(yb) & 15) &&
                          !(reinterpret_cast<uintptr_t>(mb) & (a.out_f32 ? 7 : 15));
         if (vec) {
-            for (int q = tid; q < nbytes / 16; q += kThreads) {
+            for (int q = tid; q < nbytes / 16; q += kConvThreads) {
                 uint4 v = reinterpret_cast<const uint4*>(sO)[q];
                 if (mb) {
                     if (a.out_f32) {
@@ -343,7 +351,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_tc(ConvArgs a) {
                 reinterpret_cast<uint4*>(yb)[q] = v;
             }
         } else {
-            for (int e = tid; e < nel; e += kThreads) {
+            for (int e = tid; e < nel; e += kConvThreads) {
                 const bool keep = !mb || __bfloat162float(mb[e]) > 0.0f;
                 if (a.out_f32) reinterpret_cast<float*>(yb)[e] = keep ? reinterpret_cast<const float*>(sO)[e] : 0.0f;
                 else
@@ -548,7 +556,7 @@ cudaError_t launch_conv(const ConvArgs& a, cudaStream_t s) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const long long ntiles = ((long long)a.B * a.Hout * a.Wout + kTile - 1) / kTile;
     const int grid = (int)(ntiles < nsm ? ntiles : nsm);
-    k_conv_tc<MODE, CIN, NCOL><<<grid, kThreads, smem, s>>>(a);
+    k_conv_tc<MODE, CIN, NCOL><<<grid, kConvThreads, smem, s>>>(a);
     hyd_kernel_launches_add(1);
     return cudaGetLastError();
 }
