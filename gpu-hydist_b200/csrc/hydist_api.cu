@@ -113,6 +113,9 @@ struct HydSim {
     // second stream for work that runs beside the main chain (forked and joined by events)
     cudaStream_t side;
     cudaEvent_t ev_fork, ev_join;
+    // third stream: a half-step's water budget beside the launches that follow its sweep
+    cudaStream_t side2;
+    cudaEvent_t ev_bfork, ev_bjoin;
     // asynchronous field reads: two device snapshots, copied out on their own stream
     cudaStream_t copy_stream;
     cudaEvent_t ev_snap, ev_copied[2];
@@ -197,10 +200,16 @@ static int refresh_widths(HydSim* s) {
     const int tr = pick(lr), tc = pick(lc);
     int wpr = (le + 31) / 32;
     wpr = wpr < 1 ? 1 : (wpr > 8 ? 8 : wpr);
-    if (tr != s->thr_r || tc != s->thr_c || wpr != s->g.wpr) drop_graphs(s);
+    // a segment's cells are not land, so a staged line [first - 2, last + 1] spans at most
+    // the longest run of such cells plus 3
+    const int svc = std::min(lr + 3, s->M + 3), suc = std::min(lc + 3, s->N + 3);
+    if (tr != s->thr_r || tc != s->thr_c || wpr != s->g.wpr || svc != s->g.sv_cap || suc != s->g.su_cap)
+        drop_graphs(s);
     s->thr_r = tr;
     s->thr_c = tc;
     s->g.wpr = wpr;
+    s->g.sv_cap = svc;
+    s->g.su_cap = suc;
     return HYD_OK;
 }
 
@@ -340,6 +349,8 @@ int check_device_status(HydSim* s) {
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (st & HYD_ST_SEG_OVERFLOW)
         return fail(HYD_EDEVICE, "a grid line has more than 20 wet segments (segment_limit)");
+    if (st & HYD_ST_STAGE_RANGE)
+        return fail(HYD_EDEVICE, "a line's wet span exceeded the explicit kernels' staging bound");
     return HYD_OK;
 }
 
@@ -487,6 +498,8 @@ static void release(HydSim* s) {
     cudaFree(s->arena);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->ev_bfork) cudaEventDestroy(s->ev_bfork);
+    if (s->ev_bjoin) cudaEventDestroy(s->ev_bjoin);
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     cudaFree(s->snap[0]);
     cudaFree(s->snap[1]);
@@ -507,6 +520,7 @@ static void release(HydSim* s) {
     if (s->bnd_stage) cudaFreeHost(s->bnd_stage);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->side) cudaStreamDestroy(s->side);
+    if (s->side2) cudaStreamDestroy(s->side2);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -560,6 +574,9 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, prio_lo);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&s->side2, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_bfork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_bjoin, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_snap, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_copied[0], cudaEventDisableTiming);
@@ -601,6 +618,8 @@ int hyd_create(const HydCaseParams* p, int N, int M, int device, hyd_handle* out
     g.M = M;
     g.P = s->pitch;
     g.wpr = 1;
+    g.sv_cap = M + 3;
+    g.su_cap = N + 3;
     double** gd[] = {&g.h,   &g.hsnham, &g.VISC,  &g.Fw,   &g.Tsxw,  &g.Tsyw,     &g.u,   &g.v,   &g.z,
                      &g.t_u, &g.t_v,    &g.t_z,   &g.Htdu, &g.Htdv,  &g.H_moi,    &g.htaiz, &g.htaiz_bd,
                      &g.Kx1, &g.Ky1,    &g.FS,    &g.tFS,  &g.VTH,   &g.Kx,       &g.Ky,  &g.Qbx, &g.Qby,
@@ -1085,12 +1104,22 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
     }
     { PHASE(PH_COEF_UZ); launch_coef_bnd(g, p, 0, 3, st); }
     { PHASE(PH_SWEEP_UZ); launch_sweep_uz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, 0, 1, st); }
+    // span-limited passes: the half-step's water budget beside the smoothing and explicit v
+    // (joined before the row resets change the mask); whole-grid passes keep it in the
+    // smoothing's launches
+    if (!fh) {
+        cudaEventRecord(s->ev_bfork, st);
+        cudaStreamWaitEvent(s->side2, s->ev_bfork, 0);
+        launch_budget_half(g, p, 1, s->side2);
+        cudaEventRecord(s->ev_bjoin, s->side2);
+    }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 0, 0, fh, st); }
     std::swap(g.t_u, s->scratch_u);
     { PHASE(PH_EXPL_V); launch_explicit_v(g, p, s->thr_r, st); }
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, 0, st); }
     std::swap(g.t_v, s->scratch_v);
     if (force) launch_mark_all_cols(g, st);
+    if (!fh) cudaStreamWaitEvent(st, s->ev_bjoin, 0);
     { PHASE(PH_RESET_ROWS); launch_reset_rows(g, p, force, s->thr_r, st); }
     // after a span-limited pass the update, the column rescan and (with sediment) VTH/K
     // share one launch; whole-grid passes keep them apart
@@ -1132,13 +1161,20 @@ static void launch_step(HydSim* s, int sed1, int sed2, int bed, int force = 0, i
         end_idx = s->N;
     }
     { PHASE(PH_SWEEP_VZ); launch_sweep_vz(g, p, s->plan, start_idx, end_idx, s->solver, s->sweep_scratch, st); }
-    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, 1, st); }
+    if (!fh) {  // the budget beside the launches up to the column resets
+        cudaEventRecord(s->ev_bfork, st);
+        cudaStreamWaitEvent(s->side2, s->ev_bfork, 0);
+        launch_budget_half(g, p, 0, s->side2);
+        cudaEventRecord(s->ev_bjoin, s->side2);
+    }
+    { PHASE(PH_SMOOTH); launch_smooth(g, p, 0, s->scratch_v, fh, 0, 0, fh, st); }
     std::swap(g.t_v, s->scratch_v);
     { PHASE(PH_COEF_EU); launch_coef_eu(g, p, st); }
     { PHASE(PH_EXPL_U); launch_explicit_u(g, p, s->thr_c, st); }
     if (overlap) cudaStreamWaitEvent(st, s->ev_join, 0);
     { PHASE(PH_SMOOTH); launch_smooth(g, p, 1, s->scratch_u, fh, 1, overlap, 0, st); }
     std::swap(g.t_u, s->scratch_u);
+    if (!fh) cudaStreamWaitEvent(st, s->ev_bjoin, 0);
     { PHASE(PH_RESET_COLS); launch_reset_cols(g, p, 0, s->thr_c, st); }
     if (!fh) {
         PHASE(PH_POST);

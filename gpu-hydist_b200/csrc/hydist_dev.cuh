@@ -17,6 +17,7 @@
 #define HYD_ST_INTERP_RANGE 2u     // edge FS interpolation index left the grid
 #define HYD_ST_DEGENERATE 4u       // single-cell segment on an open edge (reference reads stale scratch)
 #define HYD_ST_EDGE_REACH 8u       // an edge FS interpolation read the opposite edge row (order-dependent)
+#define HYD_ST_STAGE_RANGE 16u     // a line's staged span exceeded its shared-memory bound (not run)
 
 struct DevParams {
     double dX, dY, dT, dXbp, dX2, dYbp, dY2, dTchia2dX, dTchia2dY, HaiChiadT;
@@ -79,6 +80,10 @@ struct DevGrid {
     size_t colT_stride;
     int LT;
     int wpr;  // warps per row of the extended-span kernels (1 until the spans are known)
+    // doubles of shared memory the explicit-momentum kernels stage a row (sv_cap) or column
+    // (su_cap) in: the longest span of cells that are not land, plus the three cells around
+    // the segments they read or write (M + 3 / N + 3 until the spans are known)
+    int sv_cap, su_cap;
     // column-major stores through shared-memory tiles (colmajor_tile): set for grids whose
     // column-major arrays are too large to stay in L2, where one 32-byte sector per stored
     // value costs DRAM traffic; smaller grids store straight from the per-row warps
@@ -347,6 +352,7 @@ void launch_sweep_vz(const DevGrid& g, const DevParams& p, const SweepPlan& sp, 
 // passes only)
 // budget: also add the half-step's open-edge volumes to the budget (the first smoothing
 // after each sweep: isU = 1 after the UZ sweep, isU = 0 after the VZ sweep)
+void launch_budget_half(const DevGrid& g, const DevParams& p, int isU, cudaStream_t s);
 void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, int full, int bytes, int fs_bnd,
                    int budget, cudaStream_t s);
 void launch_widen_spans(const DevGrid& g, cudaStream_t s);

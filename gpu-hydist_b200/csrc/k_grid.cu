@@ -727,6 +727,29 @@ __global__ void k_edge_budget(DevGrid g, DevParams p, int half1) {
     edge_budget(g, p, half1, blockIdx.x / kEdgeCtas, blockIdx.x % kEdgeCtas);
 }
 
+// The open-edge budget and the leak term of one half-step (isU: the UZ sweep's) as a launch
+// of its own, on a stream beside the smoothing and the explicit momentum that follow the
+// sweep (it reads the swept velocity, the other component, the face depths, the mask and
+// the sweep's segments, none of which those launches write; the resets that change the
+// mask wait for it): kBudCtas edge CTAs, then CTAs over the cells of the last two rows
+// (UZ) or columns (VZ), the only cells leak_cell counts.
+__global__ void k_budget_half(DevGrid g, DevParams p, int isU) {
+    if ((int)blockIdx.x < kBudCtas) {
+        edge_budget(g, p, isU, blockIdx.x / kEdgeCtas, blockIdx.x % kEdgeCtas);
+        return;
+    }
+    const int t = (blockIdx.x - kBudCtas) * blockDim.x + threadIdx.x;
+    double q = 0.0;
+    if (isU) {  // rows N-1, N; columns 2..M
+        const int n = g.M - 1;
+        if (t < 2 * n) q = leak_cell(g, p, 1, g.N - 1 + t / n, 2 + t % n);
+    } else {  // columns M-1, M; rows 2..N
+        const int n = g.N - 1;
+        if (t < 2 * n) q = leak_cell(g, p, 0, 2 + t % n, g.M - 1 + t / n);
+    }
+    add_leak(g, q);  // every lane of the warp takes part
+}
+
 // BYTES: also write the column reset bytes (the smoothing of u right before the column
 // resets; H_moi is not read in between).
 template <int BYTES>
@@ -842,6 +865,10 @@ __device__ __forceinline__ void explicit_v_body(const DevGrid& g, const DevParam
     // cells read or written: two before the first segment to one past the last
     const int k0 = max(g.daui[row * HYD_SEGL] - 2, 0);
     const int k1 = min(g.cuoii[row * HYD_SEGL + nseg - 1] + 1, M + 2);
+    if (k1 - k0 + 1 > g.sv_cap) {  // cannot happen while the spans hold (see refresh_widths)
+        if (threadIdx.x == 0) flag_status(g, HYD_ST_STAGE_RANGE);
+        return;
+    }
     for (int j = k0 + threadIdx.x; j <= k1; j += blockDim.x) sv[j - k0] = g.t_v[row * P + j];
     if ((int)threadIdx.x < nseg) {
         const int i = row, W = P, k = threadIdx.x;
@@ -994,6 +1021,10 @@ __device__ __forceinline__ void explicit_u_body(const DevGrid& g, const DevParam
     if (nseg == 0) return;
     const int k0 = max(g.dauj[col * HYD_SEGL] - 2, 0);
     const int k1 = min(g.cuoij[col * HYD_SEGL + nseg - 1] + 1, N + 2);
+    if (k1 - k0 + 1 > g.su_cap) {  // cannot happen while the spans hold (see refresh_widths)
+        if (threadIdx.x == 0) flag_status(g, HYD_ST_STAGE_RANGE);
+        return;
+    }
     for (int i = k0 + threadIdx.x; i <= k1; i += blockDim.x) su[i - k0] = g.t_u[i * P + col];
     if ((int)threadIdx.x < nseg) {
         const int j = col, W = P, k = threadIdx.x;
@@ -1208,9 +1239,9 @@ struct WetGlobal {  // mask in HBM: cell k at kh[base + k * along]
 // byte per cell instead of one 32-byte sector per 4-byte mask value of the pitched grid.
 // The resets keep those bits equal to the mask (they write the byte of every cell they
 // open or close; the smoothing pass before the column resets rewrites every byte).
+// warp_scan_line packs these bytes 16 at a time (pack_wet_bytes).
 struct WetBytes {
     const unsigned char* col;
-    __device__ bool operator()(int k) const { return (col[k] & 3u) == 0; }
 };
 
 // Words of each k_reset bitset: one bit per cell of a line.
@@ -2374,11 +2405,17 @@ void launch_smooth(const DevGrid& g, const DevParams& p, int isU, double* out, i
     hyd_kernel_launches_add(1);
 }
 
+void launch_budget_half(const DevGrid& g, const DevParams& p, int isU, cudaStream_t s) {
+    const int n = isU ? g.M - 1 : g.N - 1;
+    k_budget_half<<<kBudCtas + (2 * n + 255) / 256, 256, 0, s>>>(g, p, isU);
+    hyd_kernel_launches_add(1);
+}
+
 // The line kernels below take `threads` per CTA (a multiple of 32, at least 64), chosen
 // by the caller from the longest span of the direction.
 void launch_explicit_v(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s) {
-    if (p.mixed) k_explicit_v<float><<<g.N - 1, threads, sizeof(double) * (g.M + 3), s>>>(g, p);
-    else k_explicit_v<double><<<g.N - 1, threads, sizeof(double) * (g.M + 3), s>>>(g, p);
+    if (p.mixed) k_explicit_v<float><<<g.N - 1, threads, sizeof(double) * g.sv_cap, s>>>(g, p);
+    else k_explicit_v<double><<<g.N - 1, threads, sizeof(double) * g.sv_cap, s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
@@ -2395,8 +2432,8 @@ void launch_coef_eu(const DevGrid& g, const DevParams& p, cudaStream_t s) {
 }
 
 void launch_explicit_u(const DevGrid& g, const DevParams& p, int threads, cudaStream_t s) {
-    if (p.mixed) k_explicit_u<float><<<g.M - 1, threads, sizeof(double) * (g.N + 3), s>>>(g, p);
-    else k_explicit_u<double><<<g.M - 1, threads, sizeof(double) * (g.N + 3), s>>>(g, p);
+    if (p.mixed) k_explicit_u<float><<<g.M - 1, threads, sizeof(double) * g.su_cap, s>>>(g, p);
+    else k_explicit_u<double><<<g.M - 1, threads, sizeof(double) * g.su_cap, s>>>(g, p);
     hyd_kernel_launches_add(1);
 }
 
