@@ -94,7 +94,7 @@ NCU_TRAFFIC = {
 # timed steps; the summary, with its command, is the file named in "source".  Filled from
 # captures of the current kernels; absent workloads print no step_dram.
 STEP_DRAM = {
-    "config2": {"bytes_per_step": 46.33e6, "source": "profiles/launch_list_config2_timed.md (ncu, every launch "
+    "config2": {"bytes_per_step": 46.44e6, "source": "profiles/launch_list_config2_timed.md (ncu, every launch "
                 "of 20 timed steps run cold: an upper bound)"},
     "config4": {"bytes_per_step": 501.47e6, "source": "profiles/step_dram_config2_config4.md (ncu, every launch "
                 "of a timed step run cold: an upper bound)"},
