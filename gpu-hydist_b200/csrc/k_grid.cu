@@ -610,6 +610,30 @@ struct RowLane {
 // result does not depend on the CTAs' order.
 // half1: the UZ sweep (x faces t_u, y faces v); otherwise the VZ sweep (x faces u, y faces
 // t_v).
+// The volume a one-cell segment's continuity row took in through the edge face of edge e
+// (0 up: north face, 1 down: south, 2 left: west, 3 right: east) of cell (i, j): the
+// cell's level change less what its other three faces carried.  Extracting a one-cell
+// segment never writes the velocity of the face before it (_uzSolver/_vzSolver_extract_
+// solution, UVZSolver_multithread.cu:595-723: the branch that sets it runs for cells
+// before the last one), so where the segment starts on the edge that face keeps an older
+// velocity while the row used the boundary's; the face's own product would miss the
+// difference.  (A run starting at a line's last two cells is not a segment, so the far
+// edge has no such cell.)
+__device__ __forceinline__ double single_cell_edge_inflow(const DevGrid& g, const DevParams& p, int half1, int i, int j,
+                                                          int e) {
+    const int P = g.P, c = i * P + j;
+    const double* xu = half1 ? g.t_u : g.u;
+    const double* yv = half1 ? g.v : g.t_v;
+    const double h = p.dT * 0.5;
+    const double west = h * p.dY * g.Htdu[c - P] * xu[c - P], east = -h * p.dY * g.Htdu[c] * xu[c];
+    const double south = h * p.dX * g.Htdv[c - 1] * yv[c - 1], north = -h * p.dX * g.Htdv[c] * yv[c];
+    const double dv = (g.t_z[c] - g.z[c]) * p.dX * p.dY;
+    if (e == 0) return dv - (west + east + south);
+    if (e == 1) return dv - (west + east + north);
+    if (e == 2) return dv - (east + south + north);
+    return dv - (west + south + north);
+}
+
 __device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int e, int c) {
     __shared__ double s_in[32], s_out[32];
     __shared__ int s_last;
@@ -630,7 +654,10 @@ __device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int
         double q;
         if (e >= 2) q = g.Htdu[fp] * (half1 ? g.t_u[fp] : g.u[fp]) * p.dY;
         else q = g.Htdv[fp] * (half1 ? g.v[fp] : g.t_v[fp]) * p.dX;
-        const double vol = sgn * q * (p.dT * 0.5);
+        // the face before a one-cell segment that starts on the edge (the sweep's own
+        // direction: left edge for the UZ sweep's columns, down edge for the VZ sweep's rows)
+        const bool stale = f == l && (half1 ? e == 2 : e == 1);
+        const double vol = stale ? single_cell_edge_inflow(g, p, half1, i, j, e) : sgn * q * (p.dT * 0.5);
         if (vol > 0) vin += vol;
         else vout -= vol;
     }
@@ -686,6 +713,8 @@ __device__ void edge_budget(const DevGrid& g, const DevParams& p, int half1, int
 // its neighbours across the sweep still carry their face flux to it (the explicit v in the
 // UZ half-step, u in the VZ half-step), which the unsolved cell does not receive.  (The
 // same faces towards a dry or land cell carry no flux: the velocities there are zero.)
+// Such an unsolved cell may also lie on an edge whose stage the boundary imposes; the
+// level change that puts on it is returned for it (as water gained, a negative loss).
 // Faces on the domain's edges are edge_budget's.
 __device__ __forceinline__ double leak_cell(const DevGrid& g, const DevParams& p, int isU, int i, int j) {
     const int N = g.N, M = g.M, P = g.P;
@@ -695,14 +724,19 @@ __device__ __forceinline__ double leak_cell(const DevGrid& g, const DevParams& p
     if (g.khouot[gp] != 0) return 0.0;
     int f, l;
     double q = 0.0;
+    // a wet cell the sweep does not solve keeps its level unless the boundary set it
+    // (Update_Boundary_Value writes the stage of the edge's first segment into t_z,
+    // support_funcs.cu:622-668, whether or not the cell lies in a segment of this sweep):
+    // that level change adds water no face carried, entered here as a negative loss
+    const double imposed = -(g.t_z[gp] - g.z[gp]) * p.dX * p.dY;
     if (isU) {
-        if (find_seg_u(g, i, j, f, l) < 0) return 0.0;
+        if (find_seg_u(g, i, j, f, l) < 0) return imposed;
         if (j + 1 <= M && g.khouot[gp + 1] == 0 && find_seg_u(g, i, j + 1, f, l) < 0) q += g.Htdv[gp] * g.v[gp];
         if (j - 1 >= 2 && g.khouot[gp - 1] == 0 && find_seg_u(g, i, j - 1, f, l) < 0)
             q -= g.Htdv[gp - 1] * g.v[gp - 1];
         return q * p.dX * (p.dT * 0.5);
     }
-    if (find_seg_v(g, i, j, f, l) < 0) return 0.0;
+    if (find_seg_v(g, i, j, f, l) < 0) return imposed;
     if (i + 1 <= N && g.khouot[gp + P] == 0 && find_seg_v(g, i + 1, j, f, l) < 0) q += g.Htdu[gp] * g.u[gp];
     if (i - 1 >= 2 && g.khouot[gp - P] == 0 && find_seg_v(g, i - 1, j, f, l) < 0) q -= g.Htdu[gp - P] * g.u[gp - P];
     return q * p.dY * (p.dT * 0.5);

@@ -282,9 +282,11 @@ int hyd_mass_balance(hyd_handle h, double* out, int n);
  *   out[6..9] net volume in through the up, down, left, right edge (m^3)
  *   out[10] water volume hyd_add_levels added (m^3; written when n >= 11)
  *   out[11] water volume the continuity rows moved out of the solved cells to wet cells
- *           the sweep did not solve, net (m^3; written when n >= 12): the segment scan
- *           skips a run starting at a line's last two cells (support_funcs.cu:230-335),
- *           while the neighbours' rows carry their face flux to it
+ *           the sweep did not solve, net, less the level change the stage boundary put on
+ *           those cells (m^3; written when n >= 12): the segment scan skips a run starting
+ *           at a line's last two cells (support_funcs.cu:230-335), while the neighbours'
+ *           rows carry their face flux to it and the boundary still sets its level
+ *           (support_funcs.cu:622-668)
  * Closure: between two times, the change of hyd_mass_balance's out[0] equals
  * d(out[0]) + d(out[3]) - d(out[4]) + d(out[5]) + d(out[10]) - d(out[11]).  n must be >= 10
  * (HYD_BUDGET_SLOTS for every slot).  No reference counterpart.
