@@ -65,6 +65,11 @@ struct OraSim {
     double t;
     int start_idx, end_idx; /* Engine.py loop variables that reach BedLoad (Engine.py:366) */
     int overflow;
+    /* water account (ora_water_enable): caller-owned sums, the half-step's old levels and
+       the mask and depths before the reset */
+    double* water;
+    double *w_zold, *w_H;
+    int* w_kh;
     void* mem[96];
     int nmem;
 };
@@ -1777,6 +1782,114 @@ static void trace(const OraSim* s, const char* phase) {
 #define TRACE(name) trace(s, name)
 
 /* One iteration of the while loop of Engine.hydraulic_Calculation (Engine.py:144-366). */
+/* ------------------------------------------------------------ water account
+ * The terms of the library's water budget (hyd_mass_budget) restated on the oracle's step,
+ * so that their definitions can be checked against the volume of the oracle's own fields:
+ * water[0] volume in through the domain's edge faces, water[1] opened, water[2] closed,
+ * water[3] lost to wet cells a sweep leaves unsolved (flux into them, less the stage level
+ * the boundary puts on them), water[4] edge faces taken from a one-cell segment's
+ * continuity (count).  m^3, accumulated over the steps.  No reference counterpart. */
+static int in_seg(const OraSim* s, int isU, int i, int j, int* f, int* l) {
+    if (isU) {
+        for (int k = 0; k < s->mocj[j]; k++)
+            if (s->dauj[j * SEGL + k] <= i && i <= s->cuoij[j * SEGL + k]) {
+                *f = s->dauj[j * SEGL + k];
+                *l = s->cuoij[j * SEGL + k];
+                return 1;
+            }
+    } else {
+        for (int k = 0; k < s->moci[i]; k++)
+            if (s->daui[i * SEGL + k] <= j && j <= s->cuoii[i * SEGL + k]) {
+                *f = s->daui[i * SEGL + k];
+                *l = s->cuoii[i * SEGL + k];
+                return 1;
+            }
+    }
+    return 0;
+}
+
+static void water_sweep(OraSim* s, int isU) {
+    const int N = s->N, M = s->M, W = s->W;
+    const double dX = s->P.dX, dY = s->P.dY, h = s->P.dT * 0.5;
+    const double* xu = isU ? s->t_u : s->u;
+    const double* yv = isU ? s->v : s->t_v;
+    const double* zo = s->w_zold;
+    double edge = 0.0, leak = 0.0;
+    for (int e = 0; e < 4; e++) {
+        const int n = e >= 2 ? M : N;
+        for (int k = 2; k <= n; k++) {
+            int i, j, fp;
+            double sgn;
+            if (e == 0) { i = k; j = M; fp = i * W + M; sgn = -1.0; }
+            else if (e == 1) { i = k; j = 2; fp = i * W + 1; sgn = 1.0; }
+            else if (e == 2) { i = 2; j = k; fp = W + j; sgn = 1.0; }
+            else { i = N; j = k; fp = N * W + j; sgn = -1.0; }
+            const int c = i * W + j;
+            int f, l;
+            if (s->khouot[c] != 0 || !in_seg(s, isU, i, j, &f, &l)) continue;
+            if (f == l && (isU ? e == 2 : e == 1)) {
+                const double west = h * dY * s->Htdu[c - W] * xu[c - W], east = -h * dY * s->Htdu[c] * xu[c];
+                const double south = h * dX * s->Htdv[c - 1] * yv[c - 1], north = -h * dX * s->Htdv[c] * yv[c];
+                const double dv = (s->t_z[c] - zo[c]) * dX * dY;
+                edge += e == 2 ? dv - (east + south + north) : dv - (west + east + north);
+                s->water[4] += 1;
+            } else {
+                const double q = e >= 2 ? s->Htdu[fp] * xu[fp] * dY : s->Htdv[fp] * yv[fp] * dX;
+                edge += sgn * q * h;
+            }
+        }
+    }
+    for (int i = isU ? N - 1 : 2; i <= N; i++)
+        for (int j = isU ? 2 : M - 1; j <= M; j++) {
+            const int c = i * W + j;
+            int f, l;
+            if (s->khouot[c] != 0) continue;
+            if (!in_seg(s, isU, i, j, &f, &l)) {
+                leak -= (s->t_z[c] - zo[c]) * dX * dY;
+                continue;
+            }
+            double q = 0.0;
+            if (isU) {
+                if (j + 1 <= M && s->khouot[c + 1] == 0 && !in_seg(s, 1, i, j + 1, &f, &l)) q += s->Htdv[c] * s->v[c];
+                if (j - 1 >= 2 && s->khouot[c - 1] == 0 && !in_seg(s, 1, i, j - 1, &f, &l))
+                    q -= s->Htdv[c - 1] * s->v[c - 1];
+                leak += q * dX * h;
+            } else {
+                if (i + 1 <= N && s->khouot[c + W] == 0 && !in_seg(s, 0, i + 1, j, &f, &l)) q += s->Htdu[c] * s->u[c];
+                if (i - 1 >= 2 && s->khouot[c - W] == 0 && !in_seg(s, 0, i - 1, j, &f, &l))
+                    q -= s->Htdu[c - W] * s->u[c - W];
+                leak += q * dY * h;
+            }
+        }
+    s->water[0] += edge;
+    s->water[3] += leak;
+}
+
+static void water_reset(OraSim* s, int after) {
+    const int N = s->N, M = s->M, W = s->W;
+    const double area = s->P.dX * s->P.dY;
+    if (!after) {
+        memcpy(s->w_kh, s->khouot, sizeof(int) * s->nf);
+        memcpy(s->w_H, s->H_moi, sizeof(double) * s->nf);
+        return;
+    }
+    for (int i = 2; i <= N; i++)
+        for (int j = 2; j <= M; j++) {
+            const int c = i * W + j;
+            if (s->w_kh[c] != 0 && s->khouot[c] == 0) s->water[1] += s->H_moi[c] * area;
+            if (s->w_kh[c] == 0 && s->khouot[c] != 0) s->water[2] += s->w_H[c] * area;
+        }
+}
+
+void ora_water_enable(OraSim* s, double* acc) {
+    s->water = acc;
+    if (acc && !s->w_zold) {
+        s->w_zold = (double*)ora_alloc(s, s->nf, sizeof(double), 0);
+        s->w_H = (double*)ora_alloc(s, s->nf, sizeof(double), 0);
+        s->w_kh = (int*)ora_alloc(s, s->nf, sizeof(int), 0);
+    }
+}
+
 static void full_step(OraSim* s) {
     const int N = s->N, M = s->M;
     const HydCaseParams* P = &s->P;
@@ -1794,13 +1907,17 @@ static void full_step(OraSim* s) {
         start_idx = 3;
         end_idx = M - 1;
     }
+    if (s->water) memcpy(s->w_zold, s->z, sizeof(double) * s->nf);
     k_uz_sweep(s, start_idx, end_idx); TRACE("k_uz_sweep");
+    if (s->water) water_sweep(s, 1);
     k_normalize(s, 1); TRACE("normalize_u");
     k_solve_v(s); TRACE("k_solve_v");
     k_margin_v(s); TRACE("k_margin_v");
     k_normalize(s, 0); TRACE("normalize_v");
     k_update_h_moi(s); TRACE("k_update_h_moi");
+    if (s->water) water_reset(s, 0);
     k_reset_horizontal(s); TRACE("k_reset_horizontal");
+    if (s->water) water_reset(s, 1);
     k_update_uvz(s); TRACE("k_update_uvz");
     k_limits_horizontal(s);
     k_limits_vertical(s); TRACE("k_limits_vertical");
@@ -1823,13 +1940,17 @@ static void full_step(OraSim* s) {
         start_idx = 3;
         end_idx = N;
     }
+    if (s->water) memcpy(s->w_zold, s->z, sizeof(double) * s->nf);
     k_vz_sweep(s, start_idx, end_idx); TRACE("k_vz_sweep");
+    if (s->water) water_sweep(s, 0);
     k_normalize(s, 0); TRACE("normalize_v");
     k_solve_u(s); TRACE("k_solve_u");
     k_margin_u(s); TRACE("k_margin_u");
     k_normalize(s, 1); TRACE("normalize_u");
     k_update_h_moi(s); TRACE("k_update_h_moi");
+    if (s->water) water_reset(s, 0);
     k_reset_vertical(s); TRACE("k_reset_vertical");
+    if (s->water) water_reset(s, 1);
     k_update_uvz(s); TRACE("k_update_uvz");
     k_limits_horizontal(s);
     k_limits_vertical(s); TRACE("k_limits_vertical");

@@ -44,6 +44,10 @@ double ora_time(const OraSim* s);
 void ora_set_time(OraSim* s, double t);
 void ora_set_hmax(OraSim* s, const double* hmax4);
 void ora_set_threads(int n);
+/* Water account of the following steps into acc[0..4] (accumulated; null to stop): the
+ * library's budget terms restated on the oracle's step (edge inflow, opened, closed, loss
+ * to cells a sweep leaves unsolved, one-cell edge faces), m^3.  Not in the reference. */
+void ora_water_enable(OraSim* s, double* acc);
 /* Debug aid: print the first non-finite field value after each phase (stderr). */
 void ora_set_trace(int on);
 

@@ -1,0 +1,46 @@
+"""The water budget's terms checked on the oracle (CPU, no device).
+
+The library's budget (hyd_mass_budget) says that between two times the volume of the wet
+interior cells changes by the water through the domain's edge faces, plus the cells the
+wetting pass opened, minus those the drying pass closed, minus the water lost to wet cells
+a sweep leaves unsolved (the flux their solved neighbours send them, less the stage level
+the boundary puts on them), with the edge face of a one-cell segment that starts on the
+edge taken from the cell's continuity.  The oracle restates those terms on its own step
+(ora_water_enable); here they must account for the volume of the oracle's fields to FP64
+rounding on the islands reach, where a shelf wets and dries next to a stage edge, over a
+window that holds both the unsolved cells and a one-cell edge segment."""
+import ctypes
+
+import numpy as np
+
+CLOSURE_TOL = 1e-12  # relative to the volume
+
+
+def _volume(o, area):
+    kh, H = o.view("khouot"), o.view("H_moi")
+    return float(H[2:o.N + 1, 2:o.M + 1][kh[2:o.N + 1, 2:o.M + 1] == 0].sum()) * area
+
+
+def test_budget_terms_close_on_the_oracle(oracle_lib):
+    from hydist import cases
+    c = cases.islands_case()
+    o = oracle_lib.OracleSim(c)
+    o.lib.ora_water_enable.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    o.init()
+    o.step(1)  # the first step sets H_moi
+    area = c.params.dX * c.params.dY
+    acc = np.zeros(5)
+    o.lib.ora_water_enable(ctypes.c_void_p(o.h), acc.ctypes.data)
+    v0 = _volume(o, area)
+    worst = 0.0
+    for _ in range(6):
+        o.step(50)
+        v = _volume(o, area)
+        pred = acc[0] + acc[1] - acc[2] - acc[3]
+        worst = max(worst, abs(v - v0 - pred) / v)
+    o.lib.ora_water_enable(ctypes.c_void_p(o.h), None)
+    print("islands (oracle) closure worst rel %.2e: edge %.3f opened %.3f closed %.3f unsolved %.3f m3, "
+          "one-cell edge faces %d" % (worst, acc[0], acc[1], acc[2], acc[3], int(acc[4])))
+    assert worst <= CLOSURE_TOL
+    assert acc[3] != 0.0 and acc[4] >= 1  # both corrections were exercised
+    o.close()
